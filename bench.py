@@ -1,0 +1,457 @@
+"""Benchmark of the exact FP32 top-k search path on B200 (one JSON line on rank 0).
+
+Workload (default): exact FP32 cosine top-k in the memory-bound regime — a base of 1,000,000 ×
+768 float32 rows drawn from a 1,024-centre Gaussian mixture (centres ~ N(0, 1), points = centre
++ 0.3·N(0, 1)), unit-normalised and indexed with normalized=true; query batches of 16 drawn from
+the same mixture; k = 100. One step = one batch of queries through the fused scan (K1 query prep
+→ K2 scan with fused top-k → merge). Batches of 1 and 4 are reported beside it.
+
+  value : queries/s with queries and outputs resident in HBM (device C-ABI entry point);
+  e2e   : queries/s through nndex_cuda_search_batch with host buffers (H2D of the queries and
+          D2H of the results inside the timed region);
+  roofline : the scan kernel's algorithmic bytes per launch (N·D·4 + B·D·4 + B·k·12) ÷ its
+          CUDA-event duration, against the measured HBM copy bandwidth;
+  cpu_baseline : the CPU restatement of the reference's exact path (oracle/, its Gemm strategy
+          for batches, src/cpu.rs:256-284) on the host cores, on a bounded sample.
+
+`--impl reference` times that CPU restatement alone on the same workload (the reference is Rust
+and cannot be built here). Under torchrun each rank runs an independent replica on its own GPU
+(the path does not shard; one GPU per index), with a barrier around the timed region and the max
+of the per-rank times.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "top-k queries/s & % roofline; BF16/FP8+rerank vs FP32 at equal recall@k"
+
+
+def parse_args(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--rows", type=int, default=1_000_000)
+    p.add_argument("--dims", type=int, default=768)
+    p.add_argument("--centers", type=int, default=1024)
+    p.add_argument("--sigma", type=float, default=0.3)
+    p.add_argument("--batch", type=int, default=16)
+    p.add_argument("--k", type=int, default=100)
+    p.add_argument("--seed", type=int, default=42)
+    p.add_argument("--extra-batches", default="1,4", help="batch sizes reported beside the headline")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-batches", type=int, default=2)
+    return p.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------------------------
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def dist_init(backend: str):
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank, world, _ = dist_env()
+    if world > 1 and not dist.is_initialized():
+        dist.init_process_group(backend=backend, timeout=timedelta(seconds=120))
+    return rank, world
+
+
+def replica_seed(seed: int, rank: int) -> int:
+    """Each replica indexes its own synthetic base (independent objects, no exchange)."""
+    return seed + 1000003 * rank
+
+
+def aggregate(local_ms: float, local_queries: int, world: int, device=None):
+    """Max of the per-rank times and the sum of queries over ranks → (max_ms, total_queries)."""
+    if world == 1:
+        return local_ms, local_queries
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([local_ms], dtype=torch.float64, device=device)
+    q = torch.tensor([float(local_queries)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(q, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(q.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------------------------
+# synthetic data (seeded; generated on the GPU when one is present)
+# ---------------------------------------------------------------------------------------------
+
+def make_mixture(rows, dims, centers, sigma, seed, device, center_seed=None):
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(center_seed if center_seed is not None else seed)
+    c = torch.randn((centers, dims), generator=g, device=device, dtype=torch.float32)
+    g.manual_seed(seed + 1)
+    out = torch.empty((rows, dims), device=device, dtype=torch.float32)
+    step = 1 << 18
+    for r0 in range(0, rows, step):
+        r1 = min(rows, r0 + step)
+        a = torch.randint(0, centers, (r1 - r0,), generator=g, device=device)
+        x = torch.randn((r1 - r0, dims), generator=g, device=device, dtype=torch.float32)
+        x.mul_(sigma).add_(c[a])
+        x.div_(torch.linalg.vector_norm(x, dim=1, keepdim=True))
+        out[r0:r1] = x
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(rows, dims, batch, k):
+    """DRAM bytes per scan launch from the committed ncu summary, scaled to this workload."""
+    path = os.path.join(ROOT, "profiles", "scan_fp32_traffic.json")
+    try:
+        d = json.load(open(path))
+    except (OSError, ValueError):
+        return None
+    for e in d.get("captures", []):
+        if e.get("batch") == batch and e.get("dims") == dims and e.get("k") == k:
+            return e["dram_bytes_per_launch"] * rows / e["rows"]
+    return None
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU restatement timing (oracle port)
+# ---------------------------------------------------------------------------------------------
+
+def cpu_reference_time(base_np, queries_np, k, batches: int):
+    from oracle import oracle as O
+    O.lib()
+    threads = O.num_threads()
+    times = []
+    for b in range(batches):
+        q = queries_np[b % len(queries_np)]
+        t0 = time.perf_counter()
+        O.bench_search_batch(base_np, q, k)
+        times.append(time.perf_counter() - t0)
+    return times, threads
+
+
+# ---------------------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    from nndex_b200 import _lib, kernel_launch_count
+    from nndex_b200._lib import NNDEX_FLAG_NORMALIZED
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rank, world = dist_init("nccl")
+    dev = torch.device("cuda", local)
+    seed = replica_seed(args.seed, rank)
+    L = _lib.lib()
+
+    base = make_mixture(args.rows, args.dims, args.centers, args.sigma, seed, dev, center_seed=args.seed)
+    opts = _lib.Opts()
+    opts.device = local
+    h = C.c_void_p()
+    st = L.nndex_cuda_create_from_device(base.data_ptr(), base.numel(), args.rows, args.dims,
+                                         NNDEX_FLAG_NORMALIZED, C.byref(opts), C.byref(h))
+    if st != 0:
+        raise RuntimeError(_lib.last_error())
+    base_host = base.cpu().numpy() if (rank == 0 and not args.no_cpu_baseline) else None
+    del base
+    torch.cuda.empty_cache()
+
+    batches = [args.batch] + [int(b) for b in args.extra_batches.split(",") if b and int(b) != args.batch]
+    pool = 8
+    qall = make_mixture(pool * max(batches), args.dims, args.centers, args.sigma, seed + 7, dev,
+                        center_seed=args.seed)
+    k = min(args.k, args.rows)
+    stream = torch.cuda.current_stream(dev)
+    sptr = C.c_void_p(stream.cuda_stream)
+    out_i = torch.empty((max(batches), k), dtype=torch.int64, device=dev)
+    out_s = torch.empty((max(batches), k), dtype=torch.float32, device=dev)
+    out_c = torch.empty((max(batches),), dtype=torch.int32, device=dev)
+
+    def step(b, i):
+        q = qall[(i % pool) * b:(i % pool) * b + b]
+        r = L.nndex_cuda_search_batch_device(h, q.data_ptr(), b, args.dims, k, out_i.data_ptr(), out_s.data_ptr(),
+                                             out_c.data_ptr(), sptr, 0)
+        if r != 0:
+            raise RuntimeError(_lib.last_error())
+
+    results = {}
+    clocks = None
+    launches = 0
+    for bi, b in enumerate(batches):
+        for i in range(args.warmup):
+            step(b, i)
+        torch.cuda.synchronize(dev)
+        L.nndex_cuda_set_scan_timing(h, 1)
+        sampler = ClockSampler(local) if bi == 0 else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        n0 = kernel_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            step(b, i)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        n1 = kernel_launch_count()
+        barrier(world)
+        if sampler:
+            clocks = sampler.stop()
+        L.nndex_cuda_set_scan_timing(h, 0)
+        ms = e0.elapsed_time(e1)
+        scan_ms = C.c_double(0.0)
+        scan_n = C.c_uint64(0)
+        L.nndex_cuda_scan_timing(h, C.byref(scan_ms), C.byref(scan_n))
+        max_ms, total_q = aggregate(ms, b * args.steps, world, dev)
+        results[b] = {
+            "ms_per_step": max_ms / args.steps,
+            "queries_per_s": total_q / (max_ms / 1e3),
+            "scan_ms": scan_ms.value / max(scan_n.value, 1),
+            "launches": n1 - n0,
+        }
+        if bi == 0:
+            launches = n1 - n0
+
+    # e2e through the host-buffer C-ABI call (pinned staging inside the library)
+    b = args.batch
+    qhost = [qall[i * b:(i + 1) * b].cpu().numpy().copy() for i in range(pool)]
+    oi = np.zeros((b, k), np.uint64)
+    os_ = np.zeros((b, k), np.float32)
+    oc = np.zeros(b, np.uint64)
+
+    def host_step(i):
+        q = qhost[i % pool]
+        r = L.nndex_cuda_search_batch(h, q.ctypes.data, q.size, b, k, oi.ctypes.data, os_.ctypes.data,
+                                      oc.ctypes.data)
+        if r != 0:
+            raise RuntimeError(_lib.last_error())
+
+    for i in range(args.warmup):
+        host_step(i)
+    barrier(world)
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        host_step(i)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    ev_ms = e0.elapsed_time(e1)
+    e2e_ms = max(wall_ms, ev_ms)
+    e2e_max_ms, e2e_q = aggregate(e2e_ms, b * args.steps, world, dev)
+    barrier(world)
+
+    cpu = None
+    if rank == 0 and base_host is not None:
+        qs = [qall[i * b:(i + 1) * b].cpu().numpy() for i in range(args.cpu_sample_batches)]
+        times, threads = cpu_reference_time(base_host, qs, k, args.cpu_sample_batches)
+        cpu = {"value": b * len(times) / sum(times), "unit": "queries/s", "cores": threads, "kind": "port",
+               "sample": f"{len(times)} batches of {b} queries over the full {args.rows}x{args.dims} base "
+                         f"(oracle restatement of src/cpu.rs Gemm strategy, {threads} threads)"}
+
+    L.nndex_cuda_destroy(h)
+    if rank != 0:
+        return None
+    head = results[args.batch]
+    bytes_per_launch = args.rows * args.dims * 4 + args.batch * args.dims * 4 + args.batch * k * 12
+    achieved = bytes_per_launch / (head["scan_ms"] / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profiled_traffic(args.rows, args.dims, args.batch, k)
+    line = {
+        "metric": METRIC,
+        "value": head["queries_per_s"],
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": head["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"exact-fp32 top-k, base {args.rows}x{args.dims} f32 ({args.centers}-centre Gaussian "
+                        f"mixture, sigma={args.sigma}, unit rows, normalized=true), batch {args.batch}, k={k}",
+            "rows": args.rows, "dims": args.dims, "batch": args.batch, "k": k,
+            "parallelism": f"replicas{world}" if world > 1 else "single-gpu",
+            "l2": "inputs larger than L2 (base 3.07 GB per step vs 126 MB L2)",
+        },
+        "e2e": {"value": e2e_q / (e2e_max_ms / 1e3), "unit": "queries/s",
+                "h2d_bytes_per_step": b * args.dims * 4, "d2h_bytes_per_step": b * k * 12 + b * 8},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{peak_kind} hbm_gbs",
+                     "kernel": "scan_fp32_kernel",
+                     "bytes_per_launch": bytes_per_launch, "avg_launch_ms": head["scan_ms"]},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "batches": {str(bb): {"queries_per_s": r["queries_per_s"], "ms_per_step": r["ms_per_step"],
+                              "scan_ms": r["scan_ms"],
+                              "hbm_gbs": (args.rows * args.dims * 4 + bb * args.dims * 4 + bb * k * 12)
+                              / (r["scan_ms"] / 1e3) / 1e9}
+                    for bb, r in results.items()},
+    }
+    return line
+
+
+# ---------------------------------------------------------------------------------------------
+# reference arm: the CPU restatement of the reference's exact path on the host cores
+# ---------------------------------------------------------------------------------------------
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if world > 1 and rank != 0:
+        return None
+    import torch
+    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
+    base = make_mixture(args.rows, args.dims, args.centers, args.sigma, replica_seed(args.seed, 0), dev,
+                        center_seed=args.seed).cpu().numpy()
+    b = args.batch
+    k = min(args.k, args.rows)
+    qall = make_mixture(8 * b, args.dims, args.centers, args.sigma, args.seed + 7, dev,
+                        center_seed=args.seed).cpu().numpy()
+    qs = [qall[i * b:(i + 1) * b] for i in range(8)]
+    from oracle import oracle as O
+    O.lib()
+    threads = O.num_threads()
+    # Each step is a bounded sample: a row subsample when a full pass would exceed ~2 s.
+    t0 = time.perf_counter()
+    O.bench_search_batch(base, qs[0], k)
+    full = time.perf_counter() - t0
+    rows = args.rows if full <= 2.0 else max(100_000, int(args.rows * 2.0 / full))
+    sub = np.ascontiguousarray(base[:rows])
+    for i in range(args.warmup):
+        O.bench_search_batch(sub, qs[i % 8], k)
+    times = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        O.bench_search_batch(sub, qs[i % 8], k)
+        times.append(time.perf_counter() - t0)
+    scale = rows / args.rows
+    step_s = statistics.mean(times) / scale
+    value = b / step_s
+    sample = (f"each step: {b} queries over {rows} of {args.rows} rows, scaled to the full base"
+              if rows < args.rows else f"each step: {b} queries over the full {args.rows}-row base")
+    return {
+        "impl": "reference",
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"exact-fp32 top-k, base {args.rows}x{args.dims} f32 ({args.centers}-centre "
+                               f"Gaussian mixture, sigma={args.sigma}, unit rows, normalized=true), batch {b}, k={k}",
+                   "rows": args.rows, "dims": args.dims, "batch": b, "k": k, "parallelism": "host-cores"},
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "port",
+                         "sample": sample + " (CPU restatement of src/cpu.rs:256-341 + src/topk.rs, oracle/)"},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    line = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    rank, world, _ = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        if dist.is_initialized():
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,218 @@
+/*
+ * nndex_cuda.h — C ABI of the B200 (sm_100a) backend for nndex's cosine top-k search path.
+ *
+ * This is the seam a `BackendImpl::Cuda(Arc<CudaIndex>)` arm binds to in nndex
+ * (src/lib.rs:147-154 `enum BackendImpl`, src/lib.rs:246-269 `match options.backend`).
+ * Every entry point takes plain pointers and sizes; no C++ or CUDA runtime types cross it
+ * (streams are passed as `void*`). No exception or abort crosses the ABI: every call returns
+ * an `int` status (0 = OK) and leaves a thread-local message behind `nndex_cuda_last_error()`.
+ *
+ * Status codes map 1:1 onto nndex's `NNdexError` (src/lib.rs:107-145); the CUDA-specific
+ * failures map onto one new variant `NNdexError::Cuda(String)`, the analogue of
+ * `NNdexError::Gpu(#[from] GpuError)` (src/lib.rs:141-144).
+ *
+ * Results follow nndex's `Neighbor` contract (src/topk.rs:6-11): index as `uint64_t`,
+ * similarity as `float`, sorted by similarity descending and, for equal similarity,
+ * by index ascending (src/topk.rs:143-148, src/topk.rs:268-281).
+ */
+#ifndef NNDEX_CUDA_H
+#define NNDEX_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NNDEX_API __attribute__((visibility("default")))
+#else
+#define NNDEX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (NNdexError, src/lib.rs:107-145) ------------------------------------ */
+#define NNDEX_OK                   0
+#define NNDEX_ERR_SHAPE_MISMATCH   1  /* NNdexError::ShapeMismatch{rows,dims,values}      */
+#define NNDEX_ERR_QUERY_DIMS       2  /* NNdexError::QueryDimensionalityMismatch           */
+#define NNDEX_ERR_INVALID_TOPK     3  /* NNdexError::InvalidTopK                           */
+#define NNDEX_ERR_NON_FINITE       4  /* NNdexError::NonFiniteInput                        */
+#define NNDEX_ERR_ZERO_NORM        5  /* NNdexError::ZeroNorm                              */
+#define NNDEX_ERR_CUDA             6  /* NNdexError::Cuda: a CUDA runtime/driver failure   */
+#define NNDEX_ERR_OUT_OF_MEMORY    7  /* NNdexError::Cuda: device allocation failed        */
+#define NNDEX_ERR_TIMEOUT          8  /* NNdexError::Cuda: a bounded device wait ran out   */
+#define NNDEX_ERR_ADMISSION        9  /* NNdexError::Cuda: serving admission refused       */
+#define NNDEX_ERR_INVALID_ARGUMENT 10 /* NNdexError::Cuda: bad handle / pointer / option    */
+#define NNDEX_ERR_DEVICE_INDEX     11 /* GpuError::DeviceIndexOutOfRange (src/gpu.rs:46-52) */
+#define NNDEX_ERR_UNSUPPORTED      12 /* NNdexError::Cuda: request outside compiled limits  */
+
+/* ---- construction flags (IndexOptions, src/lib.rs:64-77) ------------------------------- */
+#define NNDEX_FLAG_NORMALIZED 0x1u /* IndexOptions::normalized: rows/queries already unit  */
+#define NNDEX_FLAG_APPROX     0x2u /* IndexOptions::approx: IVF prefilter + exact rerank    */
+#define NNDEX_FLAG_BF16       0x4u /* keep a BF16 scoring copy (tensor-core scan + rerank)  */
+#define NNDEX_FLAG_FP8        0x8u /* keep an FP8-E4M3 scoring copy with per-row scales     */
+
+/* ---- precision of the exact scan ------------------------------------------------------ */
+#define NNDEX_PRECISION_AUTO 0u /* autotuner: FP32 at small batches, low precision + rerank */
+#define NNDEX_PRECISION_FP32 1u /* plain FP32 scan (CUDA cores)                               */
+#define NNDEX_PRECISION_BF16 2u /* BF16 tensor-core scan + exact FP32 rerank                  */
+#define NNDEX_PRECISION_FP8  3u /* FP8-E4M3 tensor-core scan + exact FP32 rerank              */
+
+/* Hard limits of the compiled kernels. */
+#define NNDEX_MAX_DIMS 16384u       /* padded dimensionality                                 */
+#define NNDEX_MAX_ROWS 4294967295ull /* row indices travel as 32-bit inside the kernels      */
+
+typedef struct nndex_cuda_index nndex_cuda_index;
+
+/*
+ * Options that nndex's IndexOptions does not carry. All-zero means "reference policy":
+ *   nlist   = clamp(isqrt(rows), 16, 512)        (src/approx.rs:305-311 choose_nlist)
+ *   nprobe  = choose_nprobe(nlist, k, rows)      (src/approx.rs:318-336)
+ *   iters   = 12                                 (src/approx.rs:28 KMEANS_MAX_ITERS)
+ *   seed    = rows * 2654435761 + padded_dims    (src/approx.rs:359-361)
+ * `device` is IndexOptions::gpu_device_index (src/lib.rs:76); -1 selects device 0.
+ */
+typedef struct nndex_cuda_opts {
+    int32_t  device;          /* CUDA ordinal, -1 = default (0)                              */
+    uint32_t precision;       /* NNDEX_PRECISION_*                                           */
+    uint32_t nlist;           /* 0 = reference policy                                        */
+    uint32_t nprobe;          /* 0 = reference policy (per-search, depends on k)             */
+    uint32_t kmeans_iters;    /* 0 = 12                                                      */
+    uint32_t has_seed;        /* 1 = use `seed` as the k-means++ LCG start state             */
+    uint64_t seed;
+    uint32_t rerank_width;    /* k' for low-precision scans; 0 = autotuned                    */
+    uint32_t reserved[7];
+} nndex_cuda_opts;
+
+/* Device description (GpuDeviceInfo, src/gpu.rs:974-987), CUDA flavoured. */
+typedef struct nndex_cuda_devinfo {
+    uint64_t index;            /* CUDA ordinal                                              */
+    char     name[256];        /* cudaDeviceProp::name                                      */
+    char     driver[64];       /* "NVIDIA"                                                  */
+    char     driver_info[64];  /* driver and runtime versions                              */
+    char     backend[32];      /* "Cuda"                                                    */
+    char     device_type[32];  /* "DiscreteGpu"                                             */
+    uint32_t sm_count;
+    uint32_t cc_major, cc_minor;
+    uint64_t hbm_bytes;
+    uint64_t l2_bytes;
+} nndex_cuda_devinfo;
+
+/* Search-side statistics of the last call on this index (per index, not thread-local). */
+typedef struct nndex_cuda_search_stats {
+    uint32_t path;             /* 1 = FP32 scan, 2 = BF16 scan+rerank, 3 = FP8 scan+rerank,
+                                  4 = IVF probe + rerank                                     */
+    uint32_t kernel_launches;  /* kernels this library launched for the call                */
+    uint32_t rerank_width;     /* k' used by a low-precision scan (0 otherwise)             */
+    uint32_t certified;        /* 1 = every query's low-precision top-k passed the bound    */
+    uint32_t widenings;        /* k' doublings needed to certify                            */
+    uint32_t nprobe;           /* IVF lists probed per query                                */
+    uint64_t rows_scanned;     /* base rows scored (sum over queries for IVF)               */
+    double   device_ms;        /* CUDA-event time of the device part of the call            */
+} nndex_cuda_search_stats;
+
+/* ---- errors ---------------------------------------------------------------------------- */
+
+/* Message of the last failed call on this thread, formatted like NNdexError's Display
+ * (src/lib.rs:109-144). Never NULL; "" when the last call succeeded. */
+NNDEX_API const char* nndex_cuda_last_error(void);
+
+/* ---- devices --------------------------------------------------------------------------- */
+
+/* Replaces gpu::list_gpu_devices (src/gpu.rs:992-1010). Writes up to `capacity` entries. */
+NNDEX_API int nndex_cuda_list_devices(nndex_cuda_devinfo* out, uint32_t capacity, uint32_t* count);
+
+/* Replaces NNdex::gpu_info (src/lib.rs:302-318). */
+NNDEX_API int nndex_cuda_info(const nndex_cuda_index* index, nndex_cuda_devinfo* out);
+
+/* ---- lifetime -------------------------------------------------------------------------- */
+
+/*
+ * Replaces NNdex::new (src/lib.rs:185-278) + GpuIndex::new (src/gpu.rs:138-309).
+ * `host_matrix` is the caller's raw row-major f32 matrix of `n_values` values, read during the
+ * call only. Validation order is the reference's: shape (src/lib.rs:191, 433-442), then finite
+ * values, then zero-norm rows (src/lib.rs:239-244, 461-553). Normalisation, padding to a
+ * multiple of 8 dims and the low-precision copies are made on the device.
+ */
+NNDEX_API int nndex_cuda_create(const float* host_matrix, uint64_t n_values, uint64_t rows, uint64_t dims,
+                      uint32_t flags, const nndex_cuda_opts* opts, nndex_cuda_index** out);
+
+/* Same as nndex_cuda_create, but the raw matrix already lives in device memory on the
+ * selected device (no host copy). */
+NNDEX_API int nndex_cuda_create_from_device(const float* device_matrix, uint64_t n_values, uint64_t rows,
+                                  uint64_t dims, uint32_t flags, const nndex_cuda_opts* opts,
+                                  nndex_cuda_index** out);
+
+/* Rust `Drop` for CudaIndex. NULL is ignored. */
+NNDEX_API void nndex_cuda_destroy(nndex_cuda_index* index);
+
+NNDEX_API int nndex_cuda_rows(const nndex_cuda_index* index, uint64_t* rows, uint64_t* dims,
+                    uint64_t* padded_dims);
+
+/* ---- search ---------------------------------------------------------------------------- */
+
+/*
+ * Replaces NNdex::search (src/lib.rs:335-355) → GpuIndex::search (src/gpu.rs:321-349).
+ * Checks k > 0 (InvalidTopK) before query_len == dims (QueryDimensionalityMismatch), as the
+ * reference does. Writes capped_k = min(k, rows) results (fewer only in approx mode when the
+ * probed lists hold fewer rows; `count_out` receives the number written).
+ */
+NNDEX_API int nndex_cuda_search(nndex_cuda_index* index, const float* host_query, uint64_t query_len,
+                      uint64_t k, uint64_t* idx_out, float* sim_out, uint64_t* count_out);
+
+/*
+ * Replaces NNdex::search_batch (src/lib.rs:372-402) → GpuIndex::search_batch
+ * (src/gpu.rs:372-399). Checks the shape (ShapeMismatch) before k > 0 (InvalidTopK), as the
+ * reference does. Outputs are row-major [query_rows × min(k, rows)]; `counts_out[q]` holds the
+ * number of valid results of query q. Unused slots are (0, 0.0f), the padding
+ * batch_neighbors_to_numpy applies (src/python_bindings.rs:477-483).
+ */
+NNDEX_API int nndex_cuda_search_batch(nndex_cuda_index* index, const float* host_queries,
+                            uint64_t n_values, uint64_t query_rows, uint64_t k,
+                            uint64_t* idx_out, float* sim_out, uint64_t* counts_out);
+
+/*
+ * Device-resident variant of nndex_cuda_search_batch: queries and outputs are device pointers
+ * on the index's device, the work is enqueued on `stream` (a cudaStream_t, NULL = the index's
+ * own stream) and the call returns once it is enqueued when `synchronize` is 0. Query
+ * validation (finite, zero-norm) is reported through the returned status only when
+ * `synchronize` is 1; otherwise through nndex_cuda_stream_status after the stream drains.
+ */
+NNDEX_API int nndex_cuda_search_batch_device(nndex_cuda_index* index, const float* dev_queries,
+                                   uint64_t query_rows, uint64_t query_dims, uint64_t k,
+                                   uint64_t* dev_idx_out, float* dev_sim_out,
+                                   uint32_t* dev_counts_out, void* stream, int synchronize);
+
+/* Status word of the last asynchronous device call on this index (0 when clean). */
+NNDEX_API int nndex_cuda_stream_status(nndex_cuda_index* index);
+
+/* Statistics of the last search call on this index. */
+NNDEX_API int nndex_cuda_last_search_stats(const nndex_cuda_index* index, nndex_cuda_search_stats* out);
+
+/*
+ * Kernel timing for roofline reports: while enabled, the library brackets every launch of the
+ * dominant scan kernel with CUDA events on the stream it launches on. nndex_cuda_scan_timing
+ * waits for the recorded events and returns their summed duration and count, then clears them.
+ */
+NNDEX_API int nndex_cuda_set_scan_timing(nndex_cuda_index* index, int enable);
+NNDEX_API int nndex_cuda_scan_timing(nndex_cuda_index* index, double* total_ms, uint64_t* launches);
+
+/* Total kernels this library has launched in this process (all indexes, all devices). */
+NNDEX_API uint64_t nndex_cuda_kernel_launch_count(void);
+
+/* ---- FP64 oracle on the device (score-error report) ------------------------------------- */
+
+/*
+ * For `n` (query, row) pairs, computes the FP64 dot product of the stored (normalised, FP32)
+ * row with the query as normalised by the index (so the result is the exact score the FP32 path
+ * approximates). `dev_*` are device pointers; `rows_idx` are row indices into the index.
+ */
+NNDEX_API int nndex_cuda_fp64_scores(nndex_cuda_index* index, const float* dev_queries_normalized,
+                           uint64_t query_rows, const uint64_t* dev_pairs_query,
+                           const uint64_t* dev_pairs_row, uint64_t n, double* dev_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NNDEX_CUDA_H */

@@ -1,0 +1,299 @@
+"""nndex_b200 — B200 (sm_100a) backend for nndex's cosine top-k search, with nndex's Python API.
+
+``NNdex`` mirrors the reference's PyO3 class (src/python_bindings.rs:31-236): the same
+constructor keywords, the same ``search(query, k=10, dataframe=None)`` dispatch (1-D → single
+search, 2-D → batch search, one-row 2-D → single search), the same numpy outputs
+(``uint64`` indices, ``float32`` similarities, batch rows padded with (0, 0.0)) and the same
+exception types (constructor → ValueError, search → RuntimeError, dims mismatch → ValueError).
+The only backend is ``"cuda"``: every call goes through libnndex_cuda.so's C ABI
+(include/nndex_cuda.h). There is no CPU fallback; a missing library raises at import of the
+first index.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Any
+
+import numpy as np
+
+from . import _lib
+from ._lib import (NNDEX_FLAG_APPROX, NNDEX_FLAG_BF16, NNDEX_FLAG_FP8, NNDEX_FLAG_NORMALIZED,
+                   NNDEX_PRECISION_AUTO, NNDEX_PRECISION_BF16, NNDEX_PRECISION_FP8, NNDEX_PRECISION_FP32)
+
+__all__ = ["NNdex", "NNdexError", "list_gpu_devices", "kernel_launch_count"]
+
+_PRECISIONS = {
+    "auto": NNDEX_PRECISION_AUTO,
+    "fp32": NNDEX_PRECISION_FP32,
+    "bf16": NNDEX_PRECISION_BF16,
+    "fp8": NNDEX_PRECISION_FP8,
+}
+
+
+class NNdexError(RuntimeError):
+    """A failed C-ABI call: ``code`` is the NNDEX_ERR_* status, the message NNdexError's Display."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+def _parse_backend(raw: str) -> str:
+    """src/python_bindings.rs:300-308 parse_backend, with "cuda" as the one backend here."""
+    b = str(raw).lower()
+    if b == "cuda":
+        return b
+    raise ValueError(f"unsupported backend '{b}', expected one of: cuda")
+
+
+def _detect_dataframe_kind(value: Any) -> str | None:
+    """src/python_bindings.rs:404-418 detect_dataframe_kind."""
+    t = type(value)
+    if t.__name__ == "DataFrame" and "pandas" in (t.__module__ or ""):
+        return "pandas"
+    if t.__name__ == "DataFrame" and "polars" in (t.__module__ or ""):
+        return "polars"
+    return None
+
+
+def _parse_input(value: Any) -> np.ndarray:
+    """src/python_bindings.rs:311-400 parse_input → a C-contiguous float32 1-D or 2-D array."""
+    if hasattr(value, "to_numpy"):
+        arr = value.to_numpy()
+        if arr is not value:
+            return _parse_input(arr)
+    if isinstance(value, np.ndarray):
+        if value.dtype not in (np.float32, np.float64):
+            raise ValueError("unsupported input type: expected list, numpy array, pandas/polars Series, or DataFrame")
+        if value.ndim not in (1, 2):
+            raise ValueError("only 1D and 2D arrays are supported for inputs")
+        return np.ascontiguousarray(value, dtype=np.float32)
+    if isinstance(value, (list, tuple)):
+        if len(value) == 0:
+            raise ValueError("input vector must be non-empty")
+        if isinstance(value[0], (list, tuple, np.ndarray)):
+            rows = [list(r) for r in value]
+            if len(rows[0]) == 0:
+                raise ValueError("input matrix must be non-empty")
+            dims = len(rows[0])
+            if any(len(r) != dims for r in rows):
+                raise ValueError("2D list input must have consistent row lengths")
+            return np.ascontiguousarray(np.asarray(rows, dtype=np.float32))
+        return np.ascontiguousarray(np.asarray(value, dtype=np.float32))
+    raise ValueError("unsupported input type: expected list, numpy array, pandas/polars Series, or DataFrame")
+
+
+def _check(code: int) -> None:
+    if code != 0:
+        raise NNdexError(code, _lib.last_error())
+
+
+def list_gpu_devices() -> list[dict]:
+    """src/python_bindings.rs:273-289 list_gpu_devices, over CUDA devices."""
+    L = _lib.lib()
+    cnt = C.c_uint32(0)
+    _check(L.nndex_cuda_list_devices(None, 0, C.byref(cnt)))
+    n = cnt.value
+    if n == 0:
+        return []
+    arr = (_lib.DevInfo * n)()
+    _check(L.nndex_cuda_list_devices(arr, n, C.byref(cnt)))
+    return [_devinfo_dict(arr[i]) for i in range(n)]
+
+
+def kernel_launch_count() -> int:
+    """Kernels launched by libnndex_cuda.so in this process so far."""
+    return int(_lib.lib().nndex_cuda_kernel_launch_count())
+
+
+def _devinfo_dict(d: _lib.DevInfo) -> dict:
+    return {
+        "index": int(d.index),
+        "name": d.name.decode(),
+        "driver": d.driver.decode(),
+        "driver_info": d.driver_info.decode(),
+        "backend": d.backend.decode(),
+        "device_type": d.device_type.decode(),
+        "sm_count": int(d.sm_count),
+        "compute_capability": f"{d.cc_major}.{d.cc_minor}",
+        "hbm_bytes": int(d.hbm_bytes),
+        "l2_bytes": int(d.l2_bytes),
+    }
+
+
+class NNdex:
+    """In-memory cosine top-k index on one B200 (src/python_bindings.rs:31-66 PyNNdex)."""
+
+    def __init__(self, data: Any, normalized: bool = False, approx: bool = False, backend: str = "cuda",
+                 enable_cache: bool = True, gpu_device_index: int | None = None, *, precision: str = "fp32",
+                 nlist: int = 0, nprobe: int = 0, kmeans_iters: int = 0, seed: int | None = None,
+                 rerank_width: int = 0):
+        self._backend = _parse_backend(backend)
+        if precision not in _PRECISIONS:
+            raise ValueError(f"unsupported precision '{precision}', expected one of: {', '.join(_PRECISIONS)}")
+        self._h = None
+        arr = _parse_input(data)
+        if arr.ndim == 1:
+            arr = arr.reshape(1, -1)
+        rows, dims = arr.shape
+        self._enable_cache = enable_cache  # accepted for API parity; the CUDA backend keeps no result cache
+        flags = 0
+        if normalized:
+            flags |= NNDEX_FLAG_NORMALIZED
+        if approx:
+            flags |= NNDEX_FLAG_APPROX
+        if precision == "bf16":
+            flags |= NNDEX_FLAG_BF16
+        if precision == "fp8":
+            flags |= NNDEX_FLAG_FP8
+        opts = _lib.Opts()
+        opts.device = -1 if gpu_device_index is None else int(gpu_device_index)
+        opts.precision = _PRECISIONS[precision]
+        opts.nlist = nlist
+        opts.nprobe = nprobe
+        opts.kmeans_iters = kmeans_iters
+        opts.has_seed = 0 if seed is None else 1
+        opts.seed = 0 if seed is None else int(seed)
+        opts.rerank_width = rerank_width
+        h = C.c_void_p()
+        st = _lib.lib().nndex_cuda_create(arr.ctypes.data, arr.size, rows, dims, flags, C.byref(opts), C.byref(h))
+        if st != 0:
+            raise ValueError(_lib.last_error())
+        self._h = h
+        self._rows = rows
+        self._dims = dims
+        self._normalized = normalized
+        self._approx = approx
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().nndex_cuda_destroy(h)
+            self._h = None
+
+    # ---- getters (src/python_bindings.rs:88-123) ----
+    @property
+    def backend(self) -> str:
+        return self._backend
+
+    @property
+    def rows(self) -> int:
+        return self._rows
+
+    @property
+    def dims(self) -> int:
+        return self._dims
+
+    @property
+    def gpu_info(self) -> dict:
+        info = _lib.DevInfo()
+        _check(_lib.lib().nndex_cuda_info(self._h, C.byref(info)))
+        return _devinfo_dict(info)
+
+    @property
+    def handle(self) -> C.c_void_p:
+        """The opaque nndex_cuda_index* (for callers that drive the C ABI directly)."""
+        return self._h
+
+    def last_search_stats(self) -> dict:
+        s = _lib.SearchStats()
+        _check(_lib.lib().nndex_cuda_last_search_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in _lib.SearchStats._fields_}
+
+    # ---- search (src/python_bindings.rs:125-236) ----
+    def _search_single(self, q: np.ndarray, k: int):
+        k = int(k)
+        if k < 0:
+            raise OverflowError("can't convert negative int to unsigned")
+        kk = max(min(k, self._rows), 1)
+        idx = np.zeros(kk, dtype=np.uint64)
+        sim = np.zeros(kk, dtype=np.float32)
+        cnt = C.c_uint64(0)
+        st = _lib.lib().nndex_cuda_search(self._h, q.ctypes.data, q.size, k, idx.ctypes.data, sim.ctypes.data,
+                                          C.byref(cnt))
+        if st != 0:
+            raise NNdexError(st, _lib.last_error())
+        n = int(cnt.value)
+        return idx[:n], sim[:n]
+
+    def _search_batch(self, q: np.ndarray, k: int):
+        k = int(k)
+        if k < 0:
+            raise OverflowError("can't convert negative int to unsigned")
+        rows = q.shape[0]
+        kk = max(min(k, self._rows), 1)
+        idx = np.zeros((rows, kk), dtype=np.uint64)
+        sim = np.zeros((rows, kk), dtype=np.float32)
+        cnt = np.zeros(rows, dtype=np.uint64)
+        st = _lib.lib().nndex_cuda_search_batch(self._h, q.ctypes.data, q.size, rows, k, idx.ctypes.data,
+                                                sim.ctypes.data, cnt.ctypes.data)
+        if st != 0:
+            raise NNdexError(st, _lib.last_error())
+        # batch_neighbors_to_numpy (src/python_bindings.rs:465-497): width = first row's length;
+        # shorter rows padded with (0, 0.0), longer rows truncated.
+        cols = int(cnt[0]) if rows else 0
+        idx = np.ascontiguousarray(idx[:, :cols])
+        sim = np.ascontiguousarray(sim[:, :cols])
+        for r in range(rows):
+            n = int(cnt[r])
+            if n < cols:
+                idx[r, n:] = 0
+                sim[r, n:] = 0.0
+        return idx, sim
+
+    def search(self, query: Any, k: int = 10, dataframe: Any = None):
+        out_df = self._resolve_output_dataframe(dataframe)
+        query_is_df = _detect_dataframe_kind(query) is not None
+        q = _parse_input(query)
+        dims = q.shape[-1]
+        if q.ndim == 1:
+            if not query_is_df and dims != self._dims:
+                raise ValueError(f"query dims mismatch: expected {self._dims}, got {dims}")
+            if query_is_df and dims != self._dims:
+                raise ValueError(f"query dims mismatch: expected {self._dims}, got {dims}")
+            res = self._single_or_raise(q, k)
+            return self._to_df([res], *out_df) if out_df else res
+        if dims != self._dims:
+            raise ValueError(f"query dims mismatch: expected {self._dims}, got {dims}")
+        if q.shape[0] == 1:
+            res = self._single_or_raise(q.reshape(-1), k)
+            return self._to_df([res], *out_df) if out_df else res
+        try:
+            idx, sim = self._search_batch(q, k)
+        except NNdexError as e:
+            raise RuntimeError(str(e)) from e
+        if out_df:
+            return self._to_df([(idx[r], sim[r]) for r in range(idx.shape[0])], *out_df)
+        return idx, sim
+
+    def _single_or_raise(self, q: np.ndarray, k: int):
+        try:
+            return self._search_single(q, k)
+        except NNdexError as e:
+            raise RuntimeError(str(e)) from e
+
+    # ---- DataFrame output (src/python_bindings.rs:420-553) ----
+    def _resolve_output_dataframe(self, dataframe: Any):
+        if dataframe is None:
+            return None
+        kind = _detect_dataframe_kind(dataframe)
+        if kind is None:
+            raise ValueError("`dataframe` must be a pandas.DataFrame or polars.DataFrame")
+        n = int(dataframe.shape[0]) if kind == "pandas" else int(dataframe.height)
+        if n != self._rows:
+            raise ValueError(
+                f"provided dataframe row count must match index rows (index rows={self._rows}, dataframe rows={n})")
+        return (kind, dataframe)
+
+    @staticmethod
+    def _to_df(batch, kind, source):
+        frames = []
+        for idx, sim in batch:
+            rows = [int(i) for i in idx]
+            sims = [float(s) for s in sim]
+            if kind == "pandas":
+                frames.append(source.take(rows).assign(similarity=sims))
+            else:
+                import polars as pl  # noqa: PLC0415
+                frames.append(source[rows].with_columns(pl.Series("similarity", sims)))
+        return frames[0] if len(frames) == 1 else frames

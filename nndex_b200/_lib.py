@@ -1,0 +1,127 @@
+"""ctypes binding of the C ABI in include/nndex_cuda.h (libnndex_cuda.so, built in-tree).
+
+This is the Python-side counterpart of the `extern "C"` block a Rust `CudaIndex` would declare.
+Loading fails loudly when the shared object is missing: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnndex_cuda.so")
+
+NNDEX_OK = 0
+NNDEX_ERR_SHAPE_MISMATCH = 1
+NNDEX_ERR_QUERY_DIMS = 2
+NNDEX_ERR_INVALID_TOPK = 3
+NNDEX_ERR_NON_FINITE = 4
+NNDEX_ERR_ZERO_NORM = 5
+NNDEX_ERR_CUDA = 6
+NNDEX_ERR_OUT_OF_MEMORY = 7
+NNDEX_ERR_TIMEOUT = 8
+NNDEX_ERR_ADMISSION = 9
+NNDEX_ERR_INVALID_ARGUMENT = 10
+NNDEX_ERR_DEVICE_INDEX = 11
+NNDEX_ERR_UNSUPPORTED = 12
+
+NNDEX_FLAG_NORMALIZED = 0x1
+NNDEX_FLAG_APPROX = 0x2
+NNDEX_FLAG_BF16 = 0x4
+NNDEX_FLAG_FP8 = 0x8
+
+NNDEX_PRECISION_AUTO = 0
+NNDEX_PRECISION_FP32 = 1
+NNDEX_PRECISION_BF16 = 2
+NNDEX_PRECISION_FP8 = 3
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("precision", C.c_uint32),
+        ("nlist", C.c_uint32),
+        ("nprobe", C.c_uint32),
+        ("kmeans_iters", C.c_uint32),
+        ("has_seed", C.c_uint32),
+        ("seed", C.c_uint64),
+        ("rerank_width", C.c_uint32),
+        ("reserved", C.c_uint32 * 7),
+    ]
+
+
+class DevInfo(C.Structure):
+    _fields_ = [
+        ("index", C.c_uint64),
+        ("name", C.c_char * 256),
+        ("driver", C.c_char * 64),
+        ("driver_info", C.c_char * 64),
+        ("backend", C.c_char * 32),
+        ("device_type", C.c_char * 32),
+        ("sm_count", C.c_uint32),
+        ("cc_major", C.c_uint32),
+        ("cc_minor", C.c_uint32),
+        ("hbm_bytes", C.c_uint64),
+        ("l2_bytes", C.c_uint64),
+    ]
+
+
+class SearchStats(C.Structure):
+    _fields_ = [
+        ("path", C.c_uint32),
+        ("kernel_launches", C.c_uint32),
+        ("rerank_width", C.c_uint32),
+        ("certified", C.c_uint32),
+        ("widenings", C.c_uint32),
+        ("nprobe", C.c_uint32),
+        ("rows_scanned", C.c_uint64),
+        ("device_ms", C.c_double),
+    ]
+
+
+_vp = C.c_void_p
+_u64 = C.c_uint64
+_u32 = C.c_uint32
+_i32 = C.c_int
+
+# name → (restype, argtypes); every name here is declared in include/nndex_cuda.h.
+SIGNATURES = {
+    "nndex_cuda_last_error": (C.c_char_p, []),
+    "nndex_cuda_list_devices": (_i32, [C.POINTER(DevInfo), _u32, C.POINTER(_u32)]),
+    "nndex_cuda_info": (_i32, [_vp, C.POINTER(DevInfo)]),
+    "nndex_cuda_create": (_i32, [_vp, _u64, _u64, _u64, _u32, C.POINTER(Opts), C.POINTER(_vp)]),
+    "nndex_cuda_create_from_device": (_i32, [_vp, _u64, _u64, _u64, _u32, C.POINTER(Opts), C.POINTER(_vp)]),
+    "nndex_cuda_destroy": (None, [_vp]),
+    "nndex_cuda_rows": (_i32, [_vp, C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64)]),
+    "nndex_cuda_search": (_i32, [_vp, _vp, _u64, _u64, _vp, _vp, C.POINTER(_u64)]),
+    "nndex_cuda_search_batch": (_i32, [_vp, _vp, _u64, _u64, _u64, _vp, _vp, _vp]),
+    "nndex_cuda_search_batch_device": (_i32, [_vp, _vp, _u64, _u64, _u64, _vp, _vp, _vp, _vp, _i32]),
+    "nndex_cuda_stream_status": (_i32, [_vp]),
+    "nndex_cuda_last_search_stats": (_i32, [_vp, C.POINTER(SearchStats)]),
+    "nndex_cuda_kernel_launch_count": (_u64, []),
+    "nndex_cuda_set_scan_timing": (_i32, [_vp, _i32]),
+    "nndex_cuda_scan_timing": (_i32, [_vp, C.POINTER(C.c_double), C.POINTER(_u64)]),
+    "nndex_cuda_fp64_scores": (_i32, [_vp, _vp, _u64, _vp, _vp, _u64, _vp]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libnndex_cuda.so (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"{LIB_PATH} is missing: build it with `python -m nndex_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().nndex_cuda_last_error().decode("utf-8", "replace")

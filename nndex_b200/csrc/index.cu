@@ -1,0 +1,702 @@
+// index.cu — the CUDA backend object (CudaIndex) and the C ABI declared in include/nndex_cuda.h.
+//
+// Mirrors nndex's backend contract: GpuIndex::new / search / search_batch / adapter info
+// (src/gpu.rs:138-309, 321-430, 974-1010) behind NNdex::new / search / search_batch
+// (src/lib.rs:185-402), with the reference's validation order and error variants
+// (src/lib.rs:107-145, 433-450). The device holds the whole normalised base; queries are
+// normalised on the device (K1) and scored by the fused scan (K2) + merge.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "index.h"
+#include "internal.h"
+
+namespace nndex {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+static thread_local std::string t_error;
+
+int set_error(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    t_error = buf;
+    return code;
+}
+void clear_error() { t_error.clear(); }
+const char* last_error() { return t_error.c_str(); }
+
+int cuda_error(cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation)
+        return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: %s: out of device memory", what);
+    return set_error(NNDEX_ERR_CUDA, "cuda execution error: %s: %s", what, cudaGetErrorString(e));
+}
+
+// NNdexError Display strings (src/lib.rs:109-138).
+int err_shape(uint64_t rows, uint64_t dims, uint64_t values) {
+    return set_error(NNDEX_ERR_SHAPE_MISMATCH, "matrix shape mismatch: rows=%llu, dims=%llu, values=%llu",
+                     (unsigned long long)rows, (unsigned long long)dims, (unsigned long long)values);
+}
+int err_query_dims(uint64_t expected, uint64_t found) {
+    return set_error(NNDEX_ERR_QUERY_DIMS, "query dimensionality mismatch: expected %llu, found %llu",
+                     (unsigned long long)expected, (unsigned long long)found);
+}
+int err_topk() { return set_error(NNDEX_ERR_INVALID_TOPK, "top-k must be greater than zero"); }
+int err_code(int code) {
+    switch (code) {
+        case NNDEX_ERR_NON_FINITE: return set_error(code, "all input values must be finite");
+        case NNDEX_ERR_ZERO_NORM: return set_error(code, "encountered a zero-norm vector");
+        default: return set_error(code, "cuda execution error: device status %d", code);
+    }
+}
+
+// src/lib.rs:433-442 validate_matrix_shape (saturating multiply).
+bool shape_ok(uint64_t n_values, uint64_t rows, uint64_t dims) {
+    if (rows == 0 || dims == 0) return false;
+    unsigned __int128 p = static_cast<unsigned __int128>(rows) * dims;
+    const uint64_t sat = p > UINT64_MAX ? UINT64_MAX : static_cast<uint64_t>(p);
+    return sat == n_values;
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+bool encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, uint32_t elem_bytes, const void* base,
+                    uint64_t inner, uint64_t outer, uint64_t row_stride_bytes, uint32_t box_inner,
+                    uint32_t box_outer, CUtensorMapSwizzle swizzle) {
+    auto fn = get_encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {inner, outer};
+    cuuint64_t strides[1] = {row_stride_bytes};
+    cuuint32_t box[2] = {box_inner, box_outer};
+    cuuint32_t es[2] = {1, 1};
+    (void)elem_bytes;
+    CUresult r = fn(map, dtype, 2, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// ---- device buffers ------------------------------------------------------------------------
+
+template <class T>
+static int grow_device(T*& p, size_t& cap, size_t n, const char* what) {
+    if (n <= cap && p) return NNDEX_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return cuda_error(e, what);
+    }
+    cap = n;
+    return NNDEX_OK;
+}
+template <class T>
+static int grow_host(T*& p, size_t& cap, size_t n, const char* what) {
+    if (n <= cap && p) return NNDEX_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return cuda_error(e, what);
+    }
+    cap = n;
+    return NNDEX_OK;
+}
+
+void CudaIndex::scan_event_begin(cudaStream_t s, cudaEvent_t& a) {
+    a = nullptr;
+    if (!scan_timing) return;
+    if (scan_events_used == scan_events.size()) {
+        cudaEvent_t x, y;
+        if (cudaEventCreate(&x) != cudaSuccess) return;
+        if (cudaEventCreate(&y) != cudaSuccess) {
+            cudaEventDestroy(x);
+            return;
+        }
+        scan_events.emplace_back(x, y);
+    }
+    a = scan_events[scan_events_used].first;
+    cudaEventRecord(a, s);
+}
+
+void CudaIndex::scan_event_end(cudaStream_t s, cudaEvent_t a) {
+    if (!a) return;
+    cudaEventRecord(scan_events[scan_events_used].second, s);
+    ++scan_events_used;
+}
+
+CudaIndex::~CudaIndex() {
+    cudaSetDevice(device);
+    cudaStreamSynchronize(stream);
+    for (auto& p : scan_events) {
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
+    cudaFree(d_base);
+    cudaFree(d_qraw);
+    cudaFree(d_qn);
+    cudaFree(d_ws);
+    cudaFree(d_idx);
+    cudaFree(d_sim);
+    cudaFree(d_cnt);
+    cudaFree(d_err);
+    cudaFree(d_status);
+    cudaFreeHost(h_q);
+    cudaFreeHost(h_idx);
+    cudaFreeHost(h_sim);
+    cudaFreeHost(h_cnt);
+    cudaFreeHost(h_flags);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int CudaIndex::ensure_query_capacity(uint64_t nq) {
+    int st;
+    if ((st = grow_device(d_qraw, cap_qraw, nq * dims, "query buffer"))) return st;
+    if ((st = grow_device(d_qn, cap_qn, nq * ds, "query buffer"))) return st;
+    if ((st = grow_host(h_q, cap_hq, nq * dims, "pinned query buffer"))) return st;
+    return NNDEX_OK;
+}
+
+int CudaIndex::ensure_result_capacity(uint64_t nq, uint64_t kcap) {
+    int st;
+    if ((st = grow_device(d_idx, cap_idx, nq * kcap, "result buffer"))) return st;
+    if ((st = grow_device(d_sim, cap_sim, nq * kcap, "result buffer"))) return st;
+    if ((st = grow_device(d_cnt, cap_cnt, nq, "result buffer"))) return st;
+    if ((st = grow_host(h_idx, cap_hidx, nq * kcap, "pinned result buffer"))) return st;
+    if ((st = grow_host(h_sim, cap_hsim, nq * kcap, "pinned result buffer"))) return st;
+    if ((st = grow_host(h_cnt, cap_hcnt, nq, "pinned result buffer"))) return st;
+    return NNDEX_OK;
+}
+
+// Enqueue the exact FP32 top-k of `nq` normalised queries (d_queries, stride ds) into the
+// device outputs. Workspace is the index's own (grown on demand).
+int CudaIndex::enqueue_exact_fp32(const float* d_queries, uint32_t nq, uint32_t k, uint32_t out_stride,
+                                  uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s) {
+    ScanPlan plan;
+    if (!plan_scan_fp32(nq, static_cast<uint32_t>(ds), k, sm_count, smem_optin, plan))
+        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k=%u above the fused top-k limit %u", k,
+                         kMaxFusedK);
+    const uint64_t per_query = static_cast<uint64_t>(plan.ctas_per_group) * k;
+    int st = grow_device(d_ws, cap_ws, per_query * nq, "scan workspace");
+    if (st) return st;
+    ScanArgs a;
+    a.tmap = &tmap_f32;
+    a.queries = d_queries;
+    a.nq = nq;
+    a.dq = static_cast<uint32_t>(ds);
+    a.rows = rows;
+    a.k = k;
+    a.ws_keys = d_ws;
+    a.status = d_status;
+    cudaEvent_t ev_a = nullptr;
+    scan_event_begin(s, ev_a);
+    cudaError_t e = launch_scan_fp32(a, plan, s);
+    scan_event_end(s, ev_a);
+    if (e != cudaSuccess) return cuda_error(e, "scan launch");
+    MergeArgs m;
+    m.ws_keys = d_ws;
+    m.nq = nq;
+    m.per_query = per_query;
+    m.k = k;
+    m.out_stride = out_stride;
+    m.idx_out = o_idx;
+    m.sim_out = o_sim;
+    m.count_out = o_cnt;
+    e = launch_merge_topk(m, s);
+    if (e != cudaSuccess) return cuda_error(e, "merge launch");
+    stats.kernel_launches += 2;
+    stats.path = 1;
+    stats.rows_scanned += rows * nq;
+    return NNDEX_OK;
+}
+
+// Prepare `nq` raw queries already in d_qraw (mode per K1) into d_qn.
+int CudaIndex::enqueue_query_prep(uint64_t nq, int mode, cudaStream_t s) {
+    PrepArgs p;
+    p.src = d_qraw;
+    p.rows = nq;
+    p.dims = static_cast<uint32_t>(dims);
+    p.out = d_qn;
+    p.out_stride = static_cast<uint32_t>(ds);
+    p.mode = mode;
+    p.err = d_err;
+    p.sm_count = sm_count;
+    launch_prep_rows(p, s);
+    stats.kernel_launches += 1;
+    return NNDEX_OK;
+}
+
+int CudaIndex::check_device_words() {
+    // h_flags[0] = err word, h_flags[1] = status word (copied with the results).
+    const uint64_t err = h_flags[0];
+    const uint32_t status = static_cast<uint32_t>(h_flags[1]);
+    if (err != ~0ull) return err_code(static_cast<int>(err & 0xFF));
+    if (status == kStatusTimeout)
+        return set_error(NNDEX_ERR_TIMEOUT, "cuda execution error: a bounded device wait timed out");
+    if (status != 0) return set_error(NNDEX_ERR_CUDA, "cuda execution error: device status %u", status);
+    return NNDEX_OK;
+}
+
+int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mode, uint64_t* idx_out,
+                           float* sim_out, uint64_t* counts_out) {
+    std::lock_guard<std::mutex> lock(mu);
+    cudaSetDevice(device);
+    stats = nndex_cuda_search_stats{};
+    const uint64_t kcap = std::min<uint64_t>(k, rows);
+    if (kcap > kMaxFusedK)
+        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k=%llu above the fused top-k limit %u",
+                         (unsigned long long)kcap, kMaxFusedK);
+    cudaEventRecord(ev0, stream);
+    const uint64_t chunk = kMaxBatchChunk;
+    for (uint64_t q0 = 0; q0 < nq; q0 += chunk) {
+        const uint64_t n = std::min<uint64_t>(chunk, nq - q0);
+        int st;
+        if ((st = ensure_query_capacity(n))) return st;
+        if ((st = ensure_result_capacity(n, kcap))) return st;
+        std::memcpy(h_q, queries + q0 * dims, n * dims * sizeof(float));
+        cudaMemsetAsync(d_err, 0xFF, sizeof(unsigned long long), stream);
+        cudaMemsetAsync(d_status, 0, sizeof(uint32_t), stream);
+        cudaMemcpyAsync(d_qraw, h_q, n * dims * sizeof(float), cudaMemcpyHostToDevice, stream);
+        enqueue_query_prep(n, mode, stream);
+        if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
+                                     static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
+            return st;
+        cudaMemcpyAsync(h_idx, d_idx, n * kcap * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(h_sim, d_sim, n * kcap * sizeof(float), cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(h_cnt, d_cnt, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+        h_flags[1] = 0;
+        cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_error(e, "search");
+        if ((st = check_device_words())) return st;
+        std::memcpy(idx_out + q0 * kcap, h_idx, n * kcap * sizeof(uint64_t));
+        std::memcpy(sim_out + q0 * kcap, h_sim, n * kcap * sizeof(float));
+        if (counts_out)
+            for (uint64_t i = 0; i < n; ++i) counts_out[q0 + i] = h_cnt[i];
+    }
+    cudaEventRecord(ev1, stream);
+    cudaEventSynchronize(ev1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    stats.device_ms = ms;
+    return NNDEX_OK;
+}
+
+int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out,
+                             float* d_sim_out, uint32_t* d_cnt_out, cudaStream_t s, int synchronize) {
+    std::lock_guard<std::mutex> lock(mu);
+    cudaSetDevice(device);
+    stats = nndex_cuda_search_stats{};
+    if (!s) s = stream;
+    const uint64_t kcap = std::min<uint64_t>(k, rows);
+    int st;
+    if ((st = ensure_query_capacity(std::min<uint64_t>(nq, kMaxBatchChunk)))) return st;
+    cudaMemsetAsync(d_err, 0xFF, sizeof(unsigned long long), s);
+    cudaMemsetAsync(d_status, 0, sizeof(uint32_t), s);
+    for (uint64_t q0 = 0; q0 < nq; q0 += kMaxBatchChunk) {
+        const uint64_t n = std::min<uint64_t>(kMaxBatchChunk, nq - q0);
+        PrepArgs p;
+        p.src = d_queries + q0 * dims;
+        p.rows = n;
+        p.dims = static_cast<uint32_t>(dims);
+        p.row_base = q0;
+        p.out = d_qn;
+        p.out_stride = static_cast<uint32_t>(ds);
+        p.mode = normalized ? 2 : 0;
+        p.err = d_err;
+        p.sm_count = sm_count;
+        launch_prep_rows(p, s);
+        stats.kernel_launches += 1;
+        if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
+                                     static_cast<uint32_t>(kcap), d_idx_out + q0 * kcap, d_sim_out + q0 * kcap,
+                                     d_cnt_out ? d_cnt_out + q0 : nullptr, s)))
+            return st;
+    }
+    if (synchronize) {
+        h_flags[1] = 0;
+        cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_error(e, "search");
+        return check_device_words();
+    }
+    return NNDEX_OK;
+}
+
+int CudaIndex::stream_status() {
+    std::lock_guard<std::mutex> lock(mu);
+    cudaSetDevice(device);
+    h_flags[1] = 0;
+    cudaStreamSynchronize(stream);
+    cudaMemcpy(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    return check_device_words();
+}
+
+// ---- construction ----------------------------------------------------------------------------
+
+static int select_device(int32_t requested, int& device) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDeviceCount");
+    int d = requested < 0 ? 0 : requested;
+    if (d >= n)
+        return set_error(NNDEX_ERR_DEVICE_INDEX, "gpu device index %d is out of range (found %d adapter(s))", d, n);
+    device = d;
+    return NNDEX_OK;
+}
+
+int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_t rows, uint64_t dims,
+                 uint32_t flags, const nndex_cuda_opts* opts, CudaIndex** out) {
+    if (!out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null output handle");
+    *out = nullptr;
+    if (!shape_ok(n_values, rows, dims)) return err_shape(rows, dims, n_values);
+    if (!matrix) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null matrix");
+    if (rows >= (1ull << 31))
+        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: rows=%llu above the 2^31-1 row limit",
+                         (unsigned long long)rows);
+    const uint64_t dp = (dims + 7) / 8 * 8;
+    if (dp > NNDEX_MAX_DIMS)
+        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: dims=%llu above the %u limit",
+                         (unsigned long long)dims, NNDEX_MAX_DIMS);
+    nndex_cuda_opts o{};
+    o.device = -1;
+    if (opts) o = *opts;
+    int device = 0;
+    int st = select_device(o.device, device);
+    if (st) return st;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+
+    CudaIndex* ix = new (std::nothrow) CudaIndex();
+    if (!ix) return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: host allocation failed");
+    ix->device = device;
+    ix->rows = rows;
+    ix->dims = dims;
+    ix->dp = dp;
+    ix->ds = (dims + 31) / 32 * 32;
+    ix->rows_alloc = (rows + 127) / 128 * 128;
+    ix->flags = flags;
+    ix->normalized = (flags & NNDEX_FLAG_NORMALIZED) != 0;
+    ix->approx = (flags & NNDEX_FLAG_APPROX) != 0;
+    ix->opts = o;
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    ix->sm_count = prop.multiProcessorCount;
+    ix->smem_optin = prop.sharedMemPerBlockOptin;
+    auto fail = [&](int code) {
+        delete ix;
+        return code;
+    };
+    if ((e = cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(cuda_error(e, "cudaStreamCreate"));
+    cudaEventCreate(&ix->ev0);
+    cudaEventCreate(&ix->ev1);
+    if ((e = cudaMalloc(&ix->d_err, sizeof(unsigned long long))) != cudaSuccess) return fail(cuda_error(e, "alloc"));
+    if ((e = cudaMalloc(&ix->d_status, sizeof(uint32_t))) != cudaSuccess) return fail(cuda_error(e, "alloc"));
+    if ((e = cudaMallocHost(&ix->h_flags, 2 * sizeof(uint64_t))) != cudaSuccess) return fail(cuda_error(e, "alloc"));
+    const size_t base_bytes = ix->rows_alloc * ix->ds * sizeof(float);
+    if ((e = cudaMalloc(&ix->d_base, base_bytes)) != cudaSuccess) return fail(cuda_error(e, "base allocation"));
+    cudaMemsetAsync(ix->d_base + rows * ix->ds, 0, (ix->rows_alloc - rows) * ix->ds * sizeof(float), ix->stream);
+    cudaMemsetAsync(ix->d_err, 0xFF, sizeof(unsigned long long), ix->stream);
+
+    // K1: upload in chunks (≈256 MB of raw rows each), validate + normalise + pad on the device.
+    const int mode = ix->normalized ? 2 : 0;
+    if (on_device) {
+        PrepArgs p;
+        p.src = matrix;
+        p.rows = rows;
+        p.dims = static_cast<uint32_t>(dims);
+        p.out = ix->d_base;
+        p.out_stride = static_cast<uint32_t>(ix->ds);
+        p.mode = mode;
+        p.err = ix->d_err;
+        p.sm_count = ix->sm_count;
+        launch_prep_rows(p, ix->stream);
+    } else {
+        uint64_t chunk_rows = std::max<uint64_t>(1, (256ull << 20) / (dims * sizeof(float)));
+        chunk_rows = std::min(chunk_rows, rows);
+        float* d_raw[2] = {nullptr, nullptr};
+        cudaEvent_t done[2];
+        for (int b = 0; b < 2; ++b) {
+            if ((e = cudaMalloc(&d_raw[b], chunk_rows * dims * sizeof(float))) != cudaSuccess) {
+                cudaFree(d_raw[0]);
+                return fail(cuda_error(e, "upload staging"));
+            }
+            cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming);
+        }
+        int b = 0;
+        for (uint64_t r0 = 0; r0 < rows; r0 += chunk_rows, b ^= 1) {
+            const uint64_t n = std::min(chunk_rows, rows - r0);
+            cudaEventSynchronize(done[b]);
+            e = cudaMemcpyAsync(d_raw[b], matrix + r0 * dims, n * dims * sizeof(float), cudaMemcpyHostToDevice,
+                                ix->stream);
+            if (e != cudaSuccess) break;
+            PrepArgs p;
+            p.src = d_raw[b];
+            p.rows = n;
+            p.dims = static_cast<uint32_t>(dims);
+            p.row_base = r0;
+            p.out = ix->d_base + r0 * ix->ds;
+            p.out_stride = static_cast<uint32_t>(ix->ds);
+            p.mode = mode;
+            p.err = ix->d_err;
+            p.sm_count = ix->sm_count;
+            launch_prep_rows(p, ix->stream);
+            cudaEventRecord(done[b], ix->stream);
+        }
+        cudaStreamSynchronize(ix->stream);
+        for (int i = 0; i < 2; ++i) {
+            cudaFree(d_raw[i]);
+            cudaEventDestroy(done[i]);
+        }
+        if (e != cudaSuccess) return fail(cuda_error(e, "upload"));
+    }
+    cudaMemcpyAsync(&ix->h_flags[0], ix->d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, ix->stream);
+    if ((e = cudaStreamSynchronize(ix->stream)) != cudaSuccess) return fail(cuda_error(e, "upload"));
+    if (ix->h_flags[0] != ~0ull) return fail(err_code(static_cast<int>(ix->h_flags[0] & 0xFF)));
+    if (!encode_tmap_2d(&ix->tmap_f32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ix->d_base, ix->ds, ix->rows_alloc,
+                        ix->ds * sizeof(float), 32, 128, CU_TENSOR_MAP_SWIZZLE_128B))
+        return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed"));
+    *out = ix;
+    return NNDEX_OK;
+}
+
+int fill_devinfo(int device, nndex_cuda_devinfo* out) {
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDeviceProperties");
+    std::memset(out, 0, sizeof(*out));
+    out->index = static_cast<uint64_t>(device);
+    std::snprintf(out->name, sizeof(out->name), "%s", prop.name);
+    std::snprintf(out->driver, sizeof(out->driver), "NVIDIA");
+    int drv = 0, rt = 0;
+    cudaDriverGetVersion(&drv);
+    cudaRuntimeGetVersion(&rt);
+    std::snprintf(out->driver_info, sizeof(out->driver_info), "CUDA driver %d.%d, runtime %d.%d", drv / 1000,
+                  (drv % 1000) / 10, rt / 1000, (rt % 1000) / 10);
+    std::snprintf(out->backend, sizeof(out->backend), "Cuda");
+    std::snprintf(out->device_type, sizeof(out->device_type), prop.integrated ? "IntegratedGpu" : "DiscreteGpu");
+    out->sm_count = prop.multiProcessorCount;
+    out->cc_major = prop.major;
+    out->cc_minor = prop.minor;
+    out->hbm_bytes = prop.totalGlobalMem;
+    out->l2_bytes = prop.l2CacheSize;
+    return NNDEX_OK;
+}
+
+uint64_t launches() { return g_launches.load(); }
+
+}  // namespace nndex
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+using namespace nndex;
+
+struct nndex_cuda_index {
+    CudaIndex* impl;
+};
+
+extern "C" {
+
+const char* nndex_cuda_last_error(void) { return last_error(); }
+
+uint64_t nndex_cuda_kernel_launch_count(void) { return launches(); }
+
+int nndex_cuda_set_scan_timing(nndex_cuda_index* index, int enable) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    std::lock_guard<std::mutex> lock(index->impl->mu);
+    index->impl->scan_timing = enable != 0;
+    return NNDEX_OK;
+}
+
+int nndex_cuda_scan_timing(nndex_cuda_index* index, double* total_ms, uint64_t* launches_out) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    cudaSetDevice(ix->device);
+    double sum = 0.0;
+    for (size_t i = 0; i < ix->scan_events_used; ++i) {
+        cudaError_t e = cudaEventSynchronize(ix->scan_events[i].second);
+        if (e != cudaSuccess) return cuda_error(e, "scan timing");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ix->scan_events[i].first, ix->scan_events[i].second);
+        sum += ms;
+    }
+    if (total_ms) *total_ms = sum;
+    if (launches_out) *launches_out = ix->scan_events_used;
+    ix->scan_events_used = 0;
+    return NNDEX_OK;
+}
+
+int nndex_cuda_list_devices(nndex_cuda_devinfo* out, uint32_t capacity, uint32_t* count) {
+    clear_error();
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) n = 0;
+    else if (e != cudaSuccess) return cuda_error(e, "cudaGetDeviceCount");
+    if (count) *count = static_cast<uint32_t>(n);
+    for (int d = 0; d < n && static_cast<uint32_t>(d) < capacity && out; ++d) {
+        int st = fill_devinfo(d, &out[d]);
+        if (st) return st;
+    }
+    return NNDEX_OK;
+}
+
+int nndex_cuda_info(const nndex_cuda_index* index, nndex_cuda_devinfo* out) {
+    clear_error();
+    if (!index || !out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null argument");
+    return fill_devinfo(index->impl->device, out);
+}
+
+int nndex_cuda_create(const float* host_matrix, uint64_t n_values, uint64_t rows, uint64_t dims, uint32_t flags,
+                      const nndex_cuda_opts* opts, nndex_cuda_index** out) {
+    clear_error();
+    if (!out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null output handle");
+    CudaIndex* impl = nullptr;
+    int st = create_index(host_matrix, false, n_values, rows, dims, flags, opts, &impl);
+    if (st) return st;
+    *out = new nndex_cuda_index{impl};
+    return NNDEX_OK;
+}
+
+int nndex_cuda_create_from_device(const float* device_matrix, uint64_t n_values, uint64_t rows, uint64_t dims,
+                                  uint32_t flags, const nndex_cuda_opts* opts, nndex_cuda_index** out) {
+    clear_error();
+    if (!out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null output handle");
+    CudaIndex* impl = nullptr;
+    int st = create_index(device_matrix, true, n_values, rows, dims, flags, opts, &impl);
+    if (st) return st;
+    *out = new nndex_cuda_index{impl};
+    return NNDEX_OK;
+}
+
+void nndex_cuda_destroy(nndex_cuda_index* index) {
+    if (!index) return;
+    delete index->impl;
+    delete index;
+}
+
+int nndex_cuda_rows(const nndex_cuda_index* index, uint64_t* rows, uint64_t* dims, uint64_t* padded_dims) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    if (rows) *rows = index->impl->rows;
+    if (dims) *dims = index->impl->dims;
+    if (padded_dims) *padded_dims = index->impl->dp;
+    return NNDEX_OK;
+}
+
+int nndex_cuda_search(nndex_cuda_index* index, const float* host_query, uint64_t query_len, uint64_t k,
+                      uint64_t* idx_out, float* sim_out, uint64_t* count_out) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    CudaIndex* ix = index->impl;
+    // src/lib.rs:336-344: k == 0 first, then the dimensionality.
+    if (k == 0) return err_topk();
+    if (query_len != ix->dims) return err_query_dims(ix->dims, query_len);
+    if (!host_query || !idx_out || !sim_out)
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null buffer");
+    uint64_t cnt = 0;
+    int st = ix->search_host(host_query, 1, k, ix->normalized ? 2 : 1, idx_out, sim_out, &cnt);
+    if (st) return st;
+    if (count_out) *count_out = cnt;
+    return NNDEX_OK;
+}
+
+int nndex_cuda_search_batch(nndex_cuda_index* index, const float* host_queries, uint64_t n_values,
+                            uint64_t query_rows, uint64_t k, uint64_t* idx_out, float* sim_out,
+                            uint64_t* counts_out) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    CudaIndex* ix = index->impl;
+    // src/lib.rs:378-381: the shape first, then k == 0.
+    if (!shape_ok(n_values, query_rows, ix->dims)) return err_shape(query_rows, ix->dims, n_values);
+    if (k == 0) return err_topk();
+    if (!host_queries || !idx_out || !sim_out)
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null buffer");
+    return ix->search_host(host_queries, query_rows, k, ix->normalized ? 2 : 0, idx_out, sim_out, counts_out);
+}
+
+int nndex_cuda_search_batch_device(nndex_cuda_index* index, const float* dev_queries, uint64_t query_rows,
+                                   uint64_t query_dims, uint64_t k, uint64_t* dev_idx_out, float* dev_sim_out,
+                                   uint32_t* dev_counts_out, void* stream, int synchronize) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    CudaIndex* ix = index->impl;
+    if (query_rows == 0 || query_dims != ix->dims) return err_shape(query_rows, ix->dims, query_rows * query_dims);
+    if (k == 0) return err_topk();
+    if (!dev_queries || !dev_idx_out || !dev_sim_out)
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null buffer");
+    if (std::min<uint64_t>(k, ix->rows) > kMaxFusedK)
+        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k above the fused top-k limit %u",
+                         kMaxFusedK);
+    return ix->search_device(dev_queries, query_rows, k, dev_idx_out, dev_sim_out, dev_counts_out,
+                             static_cast<cudaStream_t>(stream), synchronize);
+}
+
+int nndex_cuda_stream_status(nndex_cuda_index* index) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    return index->impl->stream_status();
+}
+
+int nndex_cuda_last_search_stats(const nndex_cuda_index* index, nndex_cuda_search_stats* out) {
+    clear_error();
+    if (!index || !out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null argument");
+    *out = index->impl->stats;
+    return NNDEX_OK;
+}
+
+int nndex_cuda_fp64_scores(nndex_cuda_index* index, const float* dev_queries_normalized, uint64_t query_rows,
+                           const uint64_t* dev_pairs_query, const uint64_t* dev_pairs_row, uint64_t n,
+                           double* dev_out) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    CudaIndex* ix = index->impl;
+    (void)query_rows;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    cudaSetDevice(ix->device);
+    launch_fp64_pairs(ix->d_base, ix->ds, dev_queries_normalized, ix->dims, dev_pairs_query, dev_pairs_row, n, dev_out,
+                      ix->stream);
+    cudaError_t e = cudaStreamSynchronize(ix->stream);
+    if (e != cudaSuccess) return cuda_error(e, "fp64 scores");
+    return NNDEX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,89 @@
+// index.h — the CUDA backend object behind the C ABI (one per NNdex built with the Cuda backend).
+#pragma once
+
+#include <mutex>
+#include <utility>
+#include <vector>
+
+#include "internal.h"
+
+namespace nndex {
+
+// Queries handled per scan launch sequence; larger batches are processed in chunks.
+constexpr uint64_t kMaxBatchChunk = 16384;
+
+int set_error(int code, const char* fmt, ...);
+void clear_error();
+const char* last_error();
+int cuda_error(cudaError_t e, const char* what);
+
+struct CudaIndex {
+    int device = 0;
+    int sm_count = 148;
+    size_t smem_optin = 232448;
+    uint64_t rows = 0;        // stored rows
+    uint64_t rows_alloc = 0;  // rows rounded up to 128 (zero rows beyond `rows`)
+    uint64_t dims = 0;        // caller dimensionality
+    uint64_t dp = 0;          // nndex padded_dims (multiple of 8, src/lib.rs:192)
+    uint64_t ds = 0;          // device row stride: dims rounded up to 32 floats (one 128 B TMA slab)
+    uint32_t flags = 0;
+    bool normalized = false;
+    bool approx = false;
+    nndex_cuda_opts opts{};
+
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mutex mu;
+
+    float* d_base = nullptr;  // rows_alloc × ds FP32, normalised, zero padded
+    CUtensorMap tmap_f32{};
+
+    // per-search buffers (grown on demand)
+    float* d_qraw = nullptr;
+    size_t cap_qraw = 0;
+    float* d_qn = nullptr;
+    size_t cap_qn = 0;
+    uint64_t* d_ws = nullptr;
+    size_t cap_ws = 0;
+    uint64_t* d_idx = nullptr;
+    size_t cap_idx = 0;
+    float* d_sim = nullptr;
+    size_t cap_sim = 0;
+    uint32_t* d_cnt = nullptr;
+    size_t cap_cnt = 0;
+    unsigned long long* d_err = nullptr;
+    uint32_t* d_status = nullptr;
+    float* h_q = nullptr;
+    size_t cap_hq = 0;
+    uint64_t* h_idx = nullptr;
+    size_t cap_hidx = 0;
+    float* h_sim = nullptr;
+    size_t cap_hsim = 0;
+    uint32_t* h_cnt = nullptr;
+    size_t cap_hcnt = 0;
+    uint64_t* h_flags = nullptr;
+
+    nndex_cuda_search_stats stats{};
+
+    // scan-kernel timing (roofline reports)
+    bool scan_timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> scan_events;
+    size_t scan_events_used = 0;
+    void scan_event_begin(cudaStream_t s, cudaEvent_t& a);
+    void scan_event_end(cudaStream_t s, cudaEvent_t a);
+
+    ~CudaIndex();
+    int ensure_query_capacity(uint64_t nq);
+    int ensure_result_capacity(uint64_t nq, uint64_t kcap);
+    int enqueue_query_prep(uint64_t nq, int mode, cudaStream_t s);
+    int enqueue_exact_fp32(const float* d_queries, uint32_t nq, uint32_t k, uint32_t out_stride, uint64_t* o_idx,
+                           float* o_sim, uint32_t* o_cnt, cudaStream_t s);
+    int check_device_words();
+    int search_host(const float* queries, uint64_t nq, uint64_t k, int mode, uint64_t* idx_out, float* sim_out,
+                    uint64_t* counts_out);
+    int search_device(const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out, float* d_sim_out,
+                      uint32_t* d_cnt_out, cudaStream_t s, int synchronize);
+    int stream_status();
+};
+
+}  // namespace nndex

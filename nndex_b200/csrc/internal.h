@@ -1,0 +1,84 @@
+// internal.h — host-side declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/nndex_cuda.h"
+
+namespace nndex {
+
+// Number of kernels launched by this library (process-wide).
+void count_launch(uint32_t n = 1);
+
+struct PrepArgs {
+    const float* src = nullptr;  // rows × dims raw values (device)
+    uint64_t rows = 0;
+    uint32_t dims = 0;
+    uint64_t row_base = 0;       // global index of src row 0 (for error reporting)
+    float* out = nullptr;        // rows × out_stride
+    uint32_t out_stride = 0;
+    int mode = 0;                // 0 normalize_rows, 1 normalize_vector, 2 finite check + pad
+    unsigned long long* err = nullptr;  // (row << 8) | code, reduced with atomicMin
+    __nv_bfloat16* out_bf16 = nullptr;
+    uint32_t bf16_stride = 0;
+    uint8_t* out_fp8 = nullptr;
+    uint32_t fp8_stride = 0;
+    float* fp8_scale = nullptr;
+    float* resid_bf16 = nullptr;
+    float* resid_fp8 = nullptr;
+    int sm_count = 148;
+};
+void launch_prep_rows(const PrepArgs& a, cudaStream_t stream);
+
+// FP32 exact scan (K2) + cross-CTA merge.
+struct ScanPlan {
+    uint32_t qb = 16;          // queries per CTA (1, 2, 4, 8, 16)
+    uint32_t ctas_per_group = 148;
+    uint32_t groups = 1;
+    uint32_t cap = 512;        // candidate buffer capacity per query
+    uint32_t stages = 4;
+    size_t smem_bytes = 0;
+};
+
+struct ScanArgs {
+    const CUtensorMap* tmap = nullptr;  // base fp32 rows × dp, box {32, 128}, 128B swizzle
+    const float* queries = nullptr;     // nq × dq normalised, zero padded
+    uint32_t nq = 0;
+    uint32_t dq = 0;                    // multiple of 32
+    uint64_t rows = 0;
+    uint32_t k = 0;                     // capped k
+    const uint32_t* row_map = nullptr;  // optional: stored position → original row index
+    uint64_t* ws_keys = nullptr;        // nq × ctas_per_group × k
+    uint32_t* status = nullptr;
+};
+
+// Picks queries-per-CTA, grid and candidate capacity for (nq, dq, k) within the shared-memory
+// budget. Returns false when k is above what the fused kernel supports.
+bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t smem_limit, ScanPlan& plan);
+cudaError_t launch_scan_fp32(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream);
+
+struct MergeArgs {
+    const uint64_t* ws_keys = nullptr;  // nq × per_query candidate keys (0 = empty slot)
+    uint32_t nq = 0;
+    uint64_t per_query = 0;
+    uint32_t k = 0;
+    uint32_t out_stride = 0;            // result slots per query in the outputs
+    uint64_t* idx_out = nullptr;        // nq × out_stride
+    float* sim_out = nullptr;
+    uint32_t* count_out = nullptr;      // nq
+};
+cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream);
+
+// Maximum k the fused scan kernels select in shared memory.
+constexpr uint32_t kMaxFusedK = 2048;
+
+// FP64 scores of (query, row) pairs: base rows of stride ds, queries of stride dims.
+void launch_fp64_pairs(const float* base, uint64_t ds, const float* queries, uint64_t dims,
+                       const uint64_t* pq, const uint64_t* pr, uint64_t n, double* out,
+                       cudaStream_t stream);
+
+}  // namespace nndex

@@ -1,0 +1,399 @@
+// scan_fp32.cu — K2: exact FP32 scan of the base with a fused top-k, and the cross-CTA merge.
+//
+// Replaces the reference's exact scoring + top-k: the CPU strategies (src/cpu.rs:256-341,
+// 505-639), the wgpu shaders (src/shaders/dot_lowdim.wgsl, dot_highdim.wgsl) with their host
+// top-k over a read-back score matrix (src/gpu.rs:486-785), and TopKAccumulator /
+// topk_from_scores (src/topk.rs:44-210). Scores never reach HBM.
+//
+// Layout. The base is a row-major FP32 matrix [rows × dp] (dp = dims rounded up to 8, zero
+// padded). A TMA tensor map describes it with a box of 32 floats (128 B) × TR rows and the
+// 128-byte swizzle, so a tile of TR rows arrives in shared memory one 128 B column slab at a time
+// (nbox = dq / 32 slabs per tile). One producer warp issues the loads into a ring of `stages`
+// slabs guarded by full/empty mbarriers; NCW consumer warps compute.
+//
+// Consumer mapping. Warp w owns tile rows [32w, 32w+32); lane = (rg = lane/4, dg = lane%4) owns
+// rows rg + 8i (i < 4) and, inside each 128 B slab, 16 B chunks dg and dg + 4. With the 128 B
+// swizzle (chunk' = chunk ^ (row % 8) = chunk ^ rg) every base load is conflict-free and every
+// query load is a 4-address broadcast. Each lane keeps 4 rows × QB queries of FP32 partial sums
+// (a fixed FMA order per (row, query), independent of the batch's composition); the 4 dg lanes
+// combine with two xor shuffles at the end of a tile.
+//
+// Fused top-k. Per query, a shared-memory buffer of `cap` 64-bit keys (common.cuh) and the
+// current k-th best key `thr`. A score enters the buffer only if its key beats `thr`; when a
+// buffer could overflow on the next tile, a warp radix-selects its exact k best, compacts, and
+// raises `thr`. Each CTA writes its k best keys per query; merge_topk_kernel selects the global k
+// best and sorts them (similarity desc, index asc).
+#include "common.cuh"
+#include "internal.h"
+#include "select.cuh"
+
+namespace nndex {
+
+namespace {
+
+NNDEX_DEVICE_INLINE uint8_t* align_1024(uint8_t* p) {
+    const uint32_t a = smem_u32(p);
+    return p + ((1024u - (a & 1023u)) & 1023u);
+}
+
+template <int QB, int NCW>
+struct ScanSmem {
+    static constexpr int TR = NCW * 32;
+    static constexpr uint32_t kStageBytes = TR * 128;
+};
+
+}  // namespace
+
+template <int QB, int NCW>
+__global__ void __launch_bounds__((NCW + 1) * 32, 1)
+    scan_fp32_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restrict__ queries, uint32_t nq,
+                     uint32_t dq, uint64_t rows, uint32_t k, uint32_t cap, uint32_t stages,
+                     const uint32_t* __restrict__ row_map, uint64_t* __restrict__ ws_keys,
+                     uint32_t* __restrict__ status) {
+    constexpr int TR = ScanSmem<QB, NCW>::TR;
+    constexpr uint32_t kStageBytes = ScanSmem<QB, NCW>::kStageBytes;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = align_1024(smem_raw);
+    uint8_t* stage_base = smem;
+    float* q_s = reinterpret_cast<float*>(stage_base + static_cast<size_t>(stages) * kStageBytes);
+    uint64_t* cand = reinterpret_cast<uint64_t*>(q_s + static_cast<size_t>(QB) * dq);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(cand + static_cast<size_t>(QB) * cap);
+    uint64_t* thr = reinterpret_cast<uint64_t*>(hist + NCW * 256);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(thr + QB);
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(cnt + QB + (QB & 1));
+    uint64_t* empty_bar = full_bar + stages;
+    volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(empty_bar + stages);
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t warp = tid >> 5;
+    const uint32_t lane = tid & 31u;
+    const uint32_t G = gridDim.x;
+    const uint32_t c = blockIdx.x;
+    const uint32_t q0 = blockIdx.y * QB;
+    const uint32_t nqg = (nq - q0) < static_cast<uint32_t>(QB) ? (nq - q0) : static_cast<uint32_t>(QB);
+    const uint64_t row_begin = rows * c / G;
+    const uint64_t row_end = rows * (c + 1) / G;
+    const uint32_t ntiles = static_cast<uint32_t>((row_end - row_begin + TR - 1) / TR);
+    const uint32_t nbox = dq / 32;
+
+    if (tid == 0) {
+        for (uint32_t s = 0; s < stages; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], NCW);
+        }
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    for (uint32_t i = tid; i < static_cast<uint32_t>(QB) * dq; i += blockDim.x) {
+        const uint32_t b = i / dq, d = i - b * dq;
+        q_s[i] = b < nqg ? queries[static_cast<size_t>(q0 + b) * dq + d] : 0.0f;
+    }
+    if (tid < static_cast<uint32_t>(QB)) {
+        cnt[tid] = 0;
+        thr[tid] = 0ull;
+    }
+    __syncthreads();
+
+    if (warp == NCW) {
+        // ---------------- producer ----------------
+        if (lane == 0) {
+            tma_prefetch_desc(&tmap);
+            const uint64_t policy = l2_policy_evict_first();
+            uint32_t it = 0;
+            bool stop = false;
+            for (uint32_t t = 0; t < ntiles && !stop; ++t) {
+                const int32_t y = static_cast<int32_t>(row_begin + static_cast<uint64_t>(t) * TR);
+                for (uint32_t bx = 0; bx < nbox; ++bx) {
+                    const uint32_t s = it % stages, u = it / stages;
+                    if (u > 0 && !mbar_wait_bounded(&empty_bar[s], (u - 1) & 1u, kWaitBudgetCycles)) {
+                        *abort_flag = 1;
+                        record_status(status, kStatusTimeout);
+                        stop = true;
+                        break;
+                    }
+                    if (*abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&full_bar[s], kStageBytes);
+                    tma_load_2d_hint(stage_base + static_cast<size_t>(s) * kStageBytes, &tmap, &full_bar[s],
+                                     static_cast<int32_t>(bx * 32), y, policy);
+                    ++it;
+                }
+            }
+            // Drain: every issued copy has landed before the CTA may exit.
+            const uint32_t used = it < stages ? it : stages;
+            for (uint32_t s = 0; s < used; ++s) {
+                const uint32_t uses = (it - s + stages - 1) / stages;
+                if (!mbar_wait_bounded(&full_bar[s], (uses - 1) & 1u, kWaitBudgetCycles))
+                    record_status(status, kStatusTimeout);
+            }
+        }
+        return;
+    }
+
+    // ---------------- consumers ----------------
+    const uint32_t dg = lane & 3u, rg = lane >> 2;
+    float acc[4][QB];
+    uint32_t it = 0;
+    const uint32_t nthreads_c = NCW * 32;
+    for (uint32_t t = 0; t < ntiles; ++t) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int b = 0; b < QB; ++b) acc[i][b] = 0.0f;
+#pragma unroll 1
+        for (uint32_t bx = 0; bx < nbox; ++bx) {
+            const uint32_t s = it % stages, u = it / stages;
+            if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], u & 1u, kWaitBudgetCycles)) {
+                *abort_flag = 1;
+                record_status(status, kStatusTimeout);
+            }
+            const uint8_t* sb = stage_base + static_cast<size_t>(s) * kStageBytes + (warp * 32 + rg) * 128;
+            const float* qp = q_s + bx * 32;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t ch = dg + 4 * h;
+                const uint32_t phys = (ch ^ rg) * 16;
+                float4 x[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) x[i] = *reinterpret_cast<const float4*>(sb + i * 8 * 128 + phys);
+#pragma unroll
+                for (int b = 0; b < QB; ++b) {
+                    const float4 qv = *reinterpret_cast<const float4*>(qp + static_cast<size_t>(b) * dq + ch * 4);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        float a = acc[i][b];
+                        a = fmaf(x[i].x, qv.x, a);
+                        a = fmaf(x[i].y, qv.y, a);
+                        a = fmaf(x[i].z, qv.z, a);
+                        a = fmaf(x[i].w, qv.w, a);
+                        acc[i][b] = a;
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty_bar[s]);
+            ++it;
+        }
+        // Combine the four dg partial sums: ((p0 + p1) + (p2 + p3)) in every lane.
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int b = 0; b < QB; ++b) {
+                float v = acc[i][b];
+                v += __shfl_xor_sync(0xffffffffu, v, 1);
+                v += __shfl_xor_sync(0xffffffffu, v, 2);
+                acc[i][b] = v;
+            }
+        const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * TR + warp * 32 + rg;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint64_t r = tile_row0 + 8 * i;
+            if (r < row_end) {
+                const uint32_t orig = row_map ? row_map[r] : static_cast<uint32_t>(r);
+#pragma unroll
+                for (int b = 0; b < QB; ++b) {
+                    if ((b & 3) == static_cast<int>(dg) && static_cast<uint32_t>(b) < nqg) {
+                        const uint64_t key = make_key(acc[i][b], orig);
+                        if (key > thr[b]) {
+                            const uint32_t pos = atomicAdd(&cnt[b], 1u);
+                            if (pos < cap)
+                                cand[static_cast<size_t>(b) * cap + pos] = key;
+                            else
+                                record_status(status, kStatusOverflow);
+                        }
+                    }
+                }
+            }
+        }
+        named_bar_sync(1, nthreads_c);
+        bool need = false;
+        const bool last = (t + 1 == ntiles);
+#pragma unroll
+        for (int b = 0; b < QB; ++b)
+            if (static_cast<uint32_t>(b) < nqg) need |= last ? (cnt[b] > k) : (cnt[b] + TR > cap);
+        if (need) {
+            for (uint32_t b = warp; b < nqg; b += NCW) {
+                const uint32_t n = cnt[b] < cap ? cnt[b] : cap;
+                if (n > k) {
+                    uint64_t* buf = cand + static_cast<size_t>(b) * cap;
+                    const uint64_t kth = warp_radix_kth(buf, n, k, hist + warp * 256);
+                    const uint32_t m = warp_compact_ge(buf, n, kth);
+                    if (lane == 0) {
+                        cnt[b] = m;
+                        thr[b] = kth;
+                    }
+                }
+            }
+            named_bar_sync(1, nthreads_c);
+        }
+    }
+    // Write this CTA's k best keys per query (0 = empty slot).
+    for (uint32_t b = warp; b < nqg; b += NCW) {
+        const uint32_t n = cnt[b] < k ? cnt[b] : k;
+        uint64_t* dst = ws_keys + (static_cast<size_t>(q0 + b) * G + c) * k;
+        const uint64_t* src = cand + static_cast<size_t>(b) * cap;
+        for (uint32_t j = lane; j < k; j += 32) dst[j] = j < n ? src[j] : 0ull;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Cross-CTA merge: one block per query selects the k best of `per_query` candidate keys and
+// writes them sorted (similarity desc, index asc), padding the unused slots with (0, 0.0f)
+// (src/python_bindings.rs:477-483).
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restrict__ ws_keys, uint64_t per_query,
+                                                         uint32_t k, uint32_t out_stride,
+                                                         uint64_t* __restrict__ idx_out,
+                                                         float* __restrict__ sim_out,
+                                                         uint32_t* __restrict__ count_out) {
+    __shared__ BlockSelectScratch s;
+    extern __shared__ uint64_t sorted[];
+    const uint32_t q = blockIdx.x;
+    const uint64_t* keys = ws_keys + static_cast<size_t>(q) * per_query;
+    if (threadIdx.x == 0) s.count = 0;
+    __syncthreads();
+    uint32_t local = 0;
+    for (uint64_t i = threadIdx.x; i < per_query; i += blockDim.x) local += keys[i] != 0ull;
+    atomicAdd(&s.count, local);
+    __syncthreads();
+    const uint32_t nvalid = s.count;
+    const uint32_t kk = nvalid < k ? nvalid : k;
+    __syncthreads();
+    uint32_t p2 = 1;
+    while (p2 < kk) p2 <<= 1;
+    if (kk > 0) {
+        uint64_t kth = 1ull;
+        if (per_query > kk) kth = block_radix_kth(keys, per_query, kk, s);
+        if (threadIdx.x == 0) s.count = 0;
+        __syncthreads();
+        for (uint64_t i = threadIdx.x; i < per_query; i += blockDim.x) {
+            const uint64_t key = keys[i];
+            if (key != 0ull && key >= kth) {
+                const uint32_t pos = atomicAdd(&s.count, 1u);
+                if (pos < kk) sorted[pos] = key;
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = kk + threadIdx.x; i < p2; i += blockDim.x) sorted[i] = 0ull;
+        __syncthreads();
+        block_bitonic_sort_desc(sorted, p2);
+    }
+    for (uint32_t j = threadIdx.x; j < out_stride; j += blockDim.x) {
+        uint64_t idx = 0;
+        float sim = 0.0f;
+        if (j < kk) {
+            idx = key_row(sorted[j]);
+            sim = key_score(sorted[j]);
+        }
+        idx_out[static_cast<size_t>(q) * out_stride + j] = idx;
+        sim_out[static_cast<size_t>(q) * out_stride + j] = sim;
+    }
+    if (threadIdx.x == 0 && count_out) count_out[q] = kk;
+}
+
+// ------------------------------------------------------------------------------------------
+// FP64 oracle scores of (query, row) pairs — the score-error report.
+// ------------------------------------------------------------------------------------------
+// base rows have stride `ds`; queries have stride `dims`; both are read over `dims` values.
+__global__ void fp64_pairs_kernel(const float* __restrict__ base, uint64_t ds, const float* __restrict__ queries,
+                                  uint64_t dims, const uint64_t* __restrict__ pq, const uint64_t* __restrict__ pr,
+                                  uint64_t n, double* __restrict__ out) {
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (warp >= n) return;
+    const float* x = base + pr[warp] * ds;
+    const float* qv = queries + pq[warp] * dims;
+    double acc = 0.0;
+    for (uint64_t d = lane; d < dims; d += 32) acc = fma(static_cast<double>(x[d]), static_cast<double>(qv[d]), acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) out[warp] = acc;
+}
+
+// ------------------------------------------------------------------------------------------
+// Host side
+// ------------------------------------------------------------------------------------------
+namespace {
+constexpr int kNcw = 4;
+constexpr int kTileRows = kNcw * 32;
+
+size_t scan_smem_bytes(uint32_t qb, uint32_t dq, uint32_t cap, uint32_t stages) {
+    size_t b = 1024;  // alignment slack
+    b += static_cast<size_t>(stages) * kTileRows * 128;
+    b += static_cast<size_t>(qb) * dq * 4;
+    b += static_cast<size_t>(qb) * cap * 8;
+    b += kNcw * 256 * 4;
+    b += qb * 8 + (qb + (qb & 1)) * 4;
+    b += static_cast<size_t>(stages) * 16 + 16;
+    return b;
+}
+
+template <int QB>
+cudaError_t launch_qb(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
+    auto kern = scan_fp32_kernel<QB, kNcw>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(p.smem_bytes));
+    if (e != cudaSuccess) return e;
+    dim3 grid(p.ctas_per_group, p.groups);
+    kern<<<grid, (kNcw + 1) * 32, p.smem_bytes, stream>>>(*a.tmap, a.queries, a.nq, a.dq, a.rows, a.k, p.cap, p.stages,
+                                                          a.row_map, a.ws_keys, a.status);
+    count_launch();
+    return cudaGetLastError();
+}
+}  // namespace
+
+bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t smem_limit, ScanPlan& plan) {
+    if (k == 0 || k > kMaxFusedK || nq == 0) return false;
+    uint32_t qb = nq <= 1 ? 1 : nq <= 2 ? 2 : nq <= 4 ? 4 : nq <= 8 ? 8 : 16;
+    const uint32_t cap = ((k + 2 * kTileRows) + 31) / 32 * 32;
+    for (;;) {
+        uint32_t stages = 4;
+        while (stages >= 2 && scan_smem_bytes(qb, dq, cap, stages) > smem_limit) --stages;
+        if (stages >= 2) {
+            plan.qb = qb;
+            plan.cap = cap;
+            plan.stages = stages;
+            plan.smem_bytes = scan_smem_bytes(qb, dq, cap, stages);
+            break;
+        }
+        if (qb == 1) return false;
+        qb >>= 1;
+    }
+    plan.groups = (nq + plan.qb - 1) / plan.qb;
+    uint32_t per = static_cast<uint32_t>(sm_count) / plan.groups;
+    if (per < 1) per = 1;
+    plan.ctas_per_group = per;
+    return true;
+}
+
+cudaError_t launch_scan_fp32(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
+    switch (p.qb) {
+        case 1: return launch_qb<1>(a, p, stream);
+        case 2: return launch_qb<2>(a, p, stream);
+        case 4: return launch_qb<4>(a, p, stream);
+        case 8: return launch_qb<8>(a, p, stream);
+        case 16: return launch_qb<16>(a, p, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream) {
+    uint32_t p2 = 1;
+    while (p2 < a.k) p2 <<= 1;
+    merge_topk_kernel<<<a.nq, 512, p2 * sizeof(uint64_t), stream>>>(a.ws_keys, a.per_query, a.k, a.out_stride,
+                                                                    a.idx_out, a.sim_out, a.count_out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+void launch_fp64_pairs(const float* base, uint64_t ds, const float* queries, uint64_t dims, const uint64_t* pq,
+                       const uint64_t* pr, uint64_t n, double* out, cudaStream_t stream) {
+    if (n == 0) return;
+    const uint64_t blocks = (n * 32 + 255) / 256;
+    fp64_pairs_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(base, ds, queries, dims, pq, pr, n, out);
+    count_launch();
+}
+
+}  // namespace nndex

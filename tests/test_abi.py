@@ -1,0 +1,47 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares (no GPU needed)."""
+import ctypes as C
+import glob
+import os
+import re
+
+import pytest
+
+from nndex_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        names |= set(re.findall(r"NNDEX_API\s+[\w\s\*]+?\b(nndex_cuda_\w+)\s*\(", text))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = _declared_symbols()
+    assert {"nndex_cuda_create", "nndex_cuda_search", "nndex_cuda_search_batch", "nndex_cuda_destroy",
+            "nndex_cuda_last_error", "nndex_cuda_info", "nndex_cuda_list_devices"} <= names
+
+
+def test_library_exports_every_declared_symbol():
+    L = C.CDLL(_lib.LIB_PATH)
+    missing = [n for n in sorted(_declared_symbols()) if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_ctypes_signatures_cover_the_header():
+    assert set(_lib.SIGNATURES) == _declared_symbols()
+    _lib.lib()  # binds every signature
+
+
+def test_structs_match_header_layout():
+    # sizes of the C structs as the header lays them out (x86-64)
+    assert C.sizeof(_lib.Opts) == 4 + 4 * 5 + 8 + 4 + 4 * 7
+    assert C.sizeof(_lib.DevInfo) == 8 + 256 + 64 + 64 + 32 + 32 + 4 * 3 + 4 + 8 + 8
+    assert C.sizeof(_lib.SearchStats) == 4 * 6 + 8 + 8
+
+
+def test_last_error_is_empty_string_initially():
+    assert isinstance(_lib.last_error(), str)
