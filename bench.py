@@ -252,7 +252,9 @@ def run_ours(args):
     qall = make_mixture(pool * max(batches), args.dims, args.centers, args.sigma, seed + 7, dev,
                         center_seed=args.seed)
     k = min(args.k, args.rows)
-    stream = torch.cuda.current_stream(dev)
+    # A dedicated stream: the library launches on it and the CUDA events below are recorded on it.
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     sptr = C.c_void_p(stream.cuda_stream)
     out_i = torch.empty((max(batches), k), dtype=torch.int64, device=dev)
     out_s = torch.empty((max(batches), k), dtype=torch.float32, device=dev)

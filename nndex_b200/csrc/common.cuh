@@ -127,6 +127,14 @@ NNDEX_DEVICE_INLINE uint64_t l2_policy_evict_last() {
     return p;
 }
 
+// Shared-memory vector load by 32-bit shared address. Volatile: it keeps program order with the
+// (volatile) mbarrier waits and barriers, so it never reads a slab before the wait that publishes it.
+NNDEX_DEVICE_INLINE float4 lds128(uint32_t addr) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
+    return v;
+}
+
 // Named barrier over a subset of warps (id 1..15; id 0 is __syncthreads).
 NNDEX_DEVICE_INLINE void named_bar_sync(uint32_t id, uint32_t threads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");

@@ -11,18 +11,21 @@
 // (nbox = dq / 32 slabs per tile). One producer warp issues the loads into a ring of `stages`
 // slabs guarded by full/empty mbarriers; NCW consumer warps compute.
 //
-// Consumer mapping. Warp w owns tile rows [32w, 32w+32); lane = (rg = lane/4, dg = lane%4) owns
-// rows rg + 8i (i < 4) and, inside each 128 B slab, 16 B chunks dg and dg + 4. With the 128 B
-// swizzle (chunk' = chunk ^ (row % 8) = chunk ^ rg) every base load is conflict-free and every
-// query load is a 4-address broadcast. Each lane keeps 4 rows × QB queries of FP32 partial sums
-// (a fixed FMA order per (row, query), independent of the batch's composition); the 4 dg lanes
-// combine with two xor shuffles at the end of a tile.
+// Consumer mapping. 2·NCW consumer warps: warp = half·NCW + row group. The row group owns tile
+// rows [32·rgrp, 32·rgrp + 32); lane = (rg = lane/4, dg = lane%4) owns rows rg + 8i (i < 4) and,
+// inside each 128 B slab, the 16 B chunk 4·half + dg. With the 128 B swizzle
+// (chunk' = chunk ^ (row % 8) = chunk ^ rg) every base load is conflict-free and every query load
+// is a 4-address broadcast. Each lane keeps 4 rows × QB queries of FP32 partial sums (a fixed FMA
+// order per (row, query), independent of the batch's composition); the 4 dg lanes combine with
+// two xor shuffles, and the two halves add through shared memory, at the end of a tile.
 //
 // Fused top-k. Per query, a shared-memory buffer of `cap` 64-bit keys (common.cuh) and the
 // current k-th best key `thr`. A score enters the buffer only if its key beats `thr`; when a
 // buffer could overflow on the next tile, a warp radix-selects its exact k best, compacts, and
 // raises `thr`. Each CTA writes its k best keys per query; merge_topk_kernel selects the global k
 // best and sorts them (similarity desc, index asc).
+#include <cstdlib>
+
 #include "common.cuh"
 #include "internal.h"
 #include "select.cuh"
@@ -36,6 +39,11 @@ NNDEX_DEVICE_INLINE uint8_t* align_1024(uint8_t* p) {
     return p + ((1024u - (a & 1023u)) & 1023u);
 }
 
+// Values a consumer lane exchanges with its partner warp at the end of a tile:
+// 4 rows × the queries b ≡ dg (mod 4) it inserts.
+template <int QB>
+constexpr int kXchgPerLane = 4 * (QB < 4 ? 1 : QB / 4);
+
 template <int QB, int NCW>
 struct ScanSmem {
     static constexpr int TR = NCW * 32;
@@ -44,21 +52,25 @@ struct ScanSmem {
 
 }  // namespace
 
-template <int QB, int NCW>
-__global__ void __launch_bounds__((NCW + 1) * 32, 1)
+template <int QB, int NCW, int ST>
+__global__ void __launch_bounds__((2 * NCW + 1) * 32, 1)
     scan_fp32_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restrict__ queries, uint32_t nq,
-                     uint32_t dq, uint64_t rows, uint32_t k, uint32_t cap, uint32_t stages,
+                     uint32_t dq, uint64_t rows, uint32_t k, uint32_t cap,
                      const uint32_t* __restrict__ row_map, uint64_t* __restrict__ ws_keys,
                      uint32_t* __restrict__ status) {
     constexpr int TR = ScanSmem<QB, NCW>::TR;
     constexpr uint32_t kStageBytes = ScanSmem<QB, NCW>::kStageBytes;
+    constexpr uint32_t kConsumers = 2 * NCW;  // warp pairs split each slab's 8 chunks 4 + 4
+    constexpr uint32_t stages = ST;           // ring depth (power of two)
+    static_assert((ST & (ST - 1)) == 0, "ring depth must be a power of two");
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = align_1024(smem_raw);
     uint8_t* stage_base = smem;
     float* q_s = reinterpret_cast<float*>(stage_base + static_cast<size_t>(stages) * kStageBytes);
     uint64_t* cand = reinterpret_cast<uint64_t*>(q_s + static_cast<size_t>(QB) * dq);
-    uint32_t* hist = reinterpret_cast<uint32_t*>(cand + static_cast<size_t>(QB) * cap);
-    uint64_t* thr = reinterpret_cast<uint64_t*>(hist + NCW * 256);
+    float* xchg = reinterpret_cast<float*>(cand + static_cast<size_t>(QB) * cap);  // kConsumers × 32 × 4·QB/4
+    uint32_t* hist = reinterpret_cast<uint32_t*>(xchg + kConsumers * 32 * kXchgPerLane<QB>);
+    uint64_t* thr = reinterpret_cast<uint64_t*>(hist + kConsumers * 256);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(thr + QB);
     uint64_t* full_bar = reinterpret_cast<uint64_t*>(cnt + QB + (QB & 1));
     uint64_t* empty_bar = full_bar + stages;
@@ -79,7 +91,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1)
     if (tid == 0) {
         for (uint32_t s = 0; s < stages; ++s) {
             mbar_init(&full_bar[s], 1);
-            mbar_init(&empty_bar[s], NCW);
+            mbar_init(&empty_bar[s], kConsumers);
         }
         *abort_flag = 0;
         fence_mbar_init();
@@ -94,7 +106,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1)
     }
     __syncthreads();
 
-    if (warp == NCW) {
+    if (warp == kConsumers) {
         // ---------------- producer ----------------
         if (lane == 0) {
             tma_prefetch_desc(&tmap);
@@ -104,7 +116,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1)
             for (uint32_t t = 0; t < ntiles && !stop; ++t) {
                 const int32_t y = static_cast<int32_t>(row_begin + static_cast<uint64_t>(t) * TR);
                 for (uint32_t bx = 0; bx < nbox; ++bx) {
-                    const uint32_t s = it % stages, u = it / stages;
+                    const uint32_t s = it & (ST - 1), u = it / ST;
                     if (u > 0 && !mbar_wait_bounded(&empty_bar[s], (u - 1) & 1u, kWaitBudgetCycles)) {
                         *abort_flag = 1;
                         record_status(status, kStatusTimeout);
@@ -133,50 +145,62 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1)
     }
 
     // ---------------- consumers ----------------
+    // warp = half·NCW + row group; the row group owns tile rows [32·rgrp, 32·rgrp + 32), the half
+    // owns 16 B chunks 4·half + dg of every 128 B slab.
+    const uint32_t rgrp = warp % NCW, half = warp / NCW;
     const uint32_t dg = lane & 3u, rg = lane >> 2;
+    const uint32_t ch = dg + 4 * half;
+    const uint32_t phys = (ch ^ rg) * 16;
     float acc[4][QB];
     uint32_t it = 0;
-    const uint32_t nthreads_c = NCW * 32;
+    constexpr uint32_t nthreads_c = kConsumers * 32;
+    float* my_x = xchg + (warp * 32 + lane) * kXchgPerLane<QB>;
+    const float* peer_x = xchg + (((warp + NCW) % kConsumers) * 32 + lane) * kXchgPerLane<QB>;
+    const uint32_t x_base = smem_u32(stage_base) + (rgrp * 32 + rg) * 128 + phys;
+    const uint32_t q_base = smem_u32(q_s) + ch * 16;
+    const uint32_t q_stride = dq * 4;
     for (uint32_t t = 0; t < ntiles; ++t) {
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int b = 0; b < QB; ++b) acc[i][b] = 0.0f;
 #pragma unroll 1
-        for (uint32_t bx = 0; bx < nbox; ++bx) {
-            const uint32_t s = it % stages, u = it / stages;
-            if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], u & 1u, kWaitBudgetCycles)) {
+        for (uint32_t bx = 0; bx < nbox; ++bx, ++it) {
+            const uint32_t s = it & (ST - 1), parity = (it / ST) & 1u;
+            // Queries do not depend on the slab: load them before waiting for it.
+            float4 qv[QB];
+#pragma unroll
+            for (int b = 0; b < QB; ++b) qv[b] = lds128(q_base + b * q_stride + bx * 128);
+            if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], parity, kWaitBudgetCycles)) {
                 *abort_flag = 1;
                 record_status(status, kStatusTimeout);
             }
-            const uint8_t* sb = stage_base + static_cast<size_t>(s) * kStageBytes + (warp * 32 + rg) * 128;
-            const float* qp = q_s + bx * 32;
+            const uint32_t xa = x_base + s * kStageBytes;
+            float4 x[4];
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const uint32_t ch = dg + 4 * h;
-                const uint32_t phys = (ch ^ rg) * 16;
-                float4 x[4];
+            for (int i = 0; i < 4; ++i) x[i] = lds128(xa + i * 8 * 128);
+            // 4·QB independent accumulators per component: no FMA dependency stalls.
 #pragma unroll
-                for (int i = 0; i < 4; ++i) x[i] = *reinterpret_cast<const float4*>(sb + i * 8 * 128 + phys);
+            for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int b = 0; b < QB; ++b) {
-                    const float4 qv = *reinterpret_cast<const float4*>(qp + static_cast<size_t>(b) * dq + ch * 4);
+                for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].x, qv[b].x, acc[i][b]);
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        float a = acc[i][b];
-                        a = fmaf(x[i].x, qv.x, a);
-                        a = fmaf(x[i].y, qv.y, a);
-                        a = fmaf(x[i].z, qv.z, a);
-                        a = fmaf(x[i].w, qv.w, a);
-                        acc[i][b] = a;
-                    }
-                }
-            }
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].y, qv[b].y, acc[i][b]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].z, qv[b].z, acc[i][b]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].w, qv[b].w, acc[i][b]);
+            // The slab's values are consumed (the FMAs above read them): release it to the producer.
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty_bar[s]);
-            ++it;
         }
-        // Combine the four dg partial sums: ((p0 + p1) + (p2 + p3)) in every lane.
+        // Combine the four dg partial sums of this half: ((p0 + p1) + (p2 + p3)) in every lane.
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -186,26 +210,46 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1)
                 v += __shfl_xor_sync(0xffffffffu, v, 2);
                 acc[i][b] = v;
             }
-        const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * TR + warp * 32 + rg;
+        // Exchange with the other half: lane dg publishes the (i, b) it inserts, b ≡ dg (mod 4).
+        // Half 0 inserts rows i = 0, 1 and half 1 rows i = 2, 3; both add (half0 + half1).
+        {
+            int j = 0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const uint64_t r = tile_row0 + 8 * i;
-            if (r < row_end) {
-                const uint32_t orig = row_map ? row_map[r] : static_cast<uint32_t>(r);
+            for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int b = 0; b < QB; ++b) {
-                    if ((b & 3) == static_cast<int>(dg) && static_cast<uint32_t>(b) < nqg) {
-                        const uint64_t key = make_key(acc[i][b], orig);
-                        if (key > thr[b]) {
-                            const uint32_t pos = atomicAdd(&cnt[b], 1u);
-                            if (pos < cap)
-                                cand[static_cast<size_t>(b) * cap + pos] = key;
-                            else
-                                record_status(status, kStatusOverflow);
+                for (int b = 0; b < QB; ++b)
+                    if ((b & 3) == static_cast<int>(dg)) {
+                        my_x[j] = acc[i][b];
+                        ++j;
+                    }
+        }
+        named_bar_sync(1, nthreads_c);
+        const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * TR + rgrp * 32 + rg;
+        {
+            int j = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int b = 0; b < QB; ++b)
+                    if ((b & 3) == static_cast<int>(dg)) {
+                        const float other = peer_x[j];
+                        ++j;
+                        if ((i >> 1) == static_cast<int>(half) && static_cast<uint32_t>(b) < nqg) {
+                            const uint64_t r = tile_row0 + 8 * i;
+                            if (r < row_end) {
+                                const float v = half == 0 ? acc[i][b] + other : other + acc[i][b];
+                                const uint32_t orig = row_map ? row_map[r] : static_cast<uint32_t>(r);
+                                const uint64_t key = make_key(v, orig);
+                                if (key > thr[b]) {
+                                    const uint32_t pos = atomicAdd(&cnt[b], 1u);
+                                    if (pos < cap)
+                                        cand[static_cast<size_t>(b) * cap + pos] = key;
+                                    else
+                                        record_status(status, kStatusOverflow);
+                                }
+                            }
                         }
                     }
-                }
-            }
         }
         named_bar_sync(1, nthreads_c);
         bool need = false;
@@ -214,7 +258,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1)
         for (int b = 0; b < QB; ++b)
             if (static_cast<uint32_t>(b) < nqg) need |= last ? (cnt[b] > k) : (cnt[b] + TR > cap);
         if (need) {
-            for (uint32_t b = warp; b < nqg; b += NCW) {
+            for (uint32_t b = warp; b < nqg; b += kConsumers) {
                 const uint32_t n = cnt[b] < cap ? cnt[b] : cap;
                 if (n > k) {
                     uint64_t* buf = cand + static_cast<size_t>(b) * cap;
@@ -230,7 +274,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1)
         }
     }
     // Write this CTA's k best keys per query (0 = empty slot).
-    for (uint32_t b = warp; b < nqg; b += NCW) {
+    for (uint32_t b = warp; b < nqg; b += kConsumers) {
         const uint32_t n = cnt[b] < k ? cnt[b] : k;
         uint64_t* dst = ws_keys + (static_cast<size_t>(q0 + b) * G + c) * k;
         const uint64_t* src = cand + static_cast<size_t>(b) * cap;
@@ -324,33 +368,52 @@ size_t scan_smem_bytes(uint32_t qb, uint32_t dq, uint32_t cap, uint32_t stages) 
     b += static_cast<size_t>(stages) * kTileRows * 128;
     b += static_cast<size_t>(qb) * dq * 4;
     b += static_cast<size_t>(qb) * cap * 8;
-    b += kNcw * 256 * 4;
+    b += static_cast<size_t>(2 * kNcw) * 32 * 4 * (qb < 4 ? 1 : qb / 4) * 4;  // partner exchange
+    b += 2 * kNcw * 256 * 4;
     b += qb * 8 + (qb + (qb & 1)) * 4;
     b += static_cast<size_t>(stages) * 16 + 16;
     return b;
 }
 
-template <int QB>
-cudaError_t launch_qb(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
-    auto kern = scan_fp32_kernel<QB, kNcw>;
+template <int QB, int ST>
+cudaError_t launch_qb_st(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
+    auto kern = scan_fp32_kernel<QB, kNcw, ST>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(p.smem_bytes));
     if (e != cudaSuccess) return e;
     dim3 grid(p.ctas_per_group, p.groups);
-    kern<<<grid, (kNcw + 1) * 32, p.smem_bytes, stream>>>(*a.tmap, a.queries, a.nq, a.dq, a.rows, a.k, p.cap, p.stages,
-                                                          a.row_map, a.ws_keys, a.status);
+    kern<<<grid, (2 * kNcw + 1) * 32, p.smem_bytes, stream>>>(*a.tmap, a.queries, a.nq, a.dq, a.rows, a.k, p.cap,
+                                                              a.row_map, a.ws_keys, a.status);
     count_launch();
     return cudaGetLastError();
 }
+
+template <int QB>
+cudaError_t launch_qb(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
+    return p.stages >= 4 ? launch_qb_st<QB, 4>(a, p, stream) : launch_qb_st<QB, 2>(a, p, stream);
+}
 }  // namespace
+
+// Tile-shape overrides for the autotuner and for measurement sweeps (0 = default):
+//   NNDEX_SCAN_STAGES   ring depth (2 or 4)        NNDEX_SCAN_QB   max queries per CTA (1..16)
+//   NNDEX_SCAN_CTAS     CTAs per query group      NNDEX_SCAN_CAP  candidate slots beyond k
+static uint32_t env_u32(const char* name) {
+    const char* v = getenv(name);
+    return v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
+}
 
 bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t smem_limit, ScanPlan& plan) {
     if (k == 0 || k > kMaxFusedK || nq == 0) return false;
+    static const uint32_t o_stages = env_u32("NNDEX_SCAN_STAGES"), o_qb = env_u32("NNDEX_SCAN_QB"),
+                          o_ctas = env_u32("NNDEX_SCAN_CTAS"), o_cap = env_u32("NNDEX_SCAN_CAP");
     uint32_t qb = nq <= 1 ? 1 : nq <= 2 ? 2 : nq <= 4 ? 4 : nq <= 8 ? 8 : 16;
-    const uint32_t cap = ((k + 2 * kTileRows) + 31) / 32 * 32;
+    if (o_qb) while (qb > 1 && qb > o_qb) qb >>= 1;
+    const uint32_t extra = o_cap ? (o_cap > kTileRows ? o_cap : kTileRows + 32) : 2 * kTileRows;
+    const uint32_t cap = ((k + extra) + 31) / 32 * 32;
+    const uint32_t max_stages = (o_stages && o_stages < 4) ? 2 : 4;
     for (;;) {
-        uint32_t stages = 4;
-        while (stages >= 2 && scan_smem_bytes(qb, dq, cap, stages) > smem_limit) --stages;
+        uint32_t stages = max_stages;
+        while (stages >= 2 && scan_smem_bytes(qb, dq, cap, stages) > smem_limit) stages >>= 1;
         if (stages >= 2) {
             plan.qb = qb;
             plan.cap = cap;
@@ -364,6 +427,7 @@ bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t s
     plan.groups = (nq + plan.qb - 1) / plan.qb;
     uint32_t per = static_cast<uint32_t>(sm_count) / plan.groups;
     if (per < 1) per = 1;
+    if (o_ctas) per = o_ctas;
     plan.ctas_per_group = per;
     return true;
 }
