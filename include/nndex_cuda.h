@@ -200,6 +200,27 @@ NNDEX_API int nndex_cuda_scan_timing(nndex_cuda_index* index, double* total_ms, 
 /* Total kernels this library has launched in this process (all indexes, all devices). */
 NNDEX_API uint64_t nndex_cuda_kernel_launch_count(void);
 
+/* ---- search without allocation -------------------------------------------------------- */
+
+/* Size of the device array nndex_cuda_search_batch_device_noalloc works in (per GPU). */
+#define NNDEX_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/*
+ * Exact batch search that allocates no memory; no counterpart in the reference. For callers that
+ * cannot call cudaMalloc while searching: a process whose HBM is fully reserved by another
+ * allocator, or a latency-critical path that cannot take cudaMalloc/cudaFree's implicit
+ * synchronisation. Same arguments, results and validation as nndex_cuda_search_batch_device with
+ * synchronize = 1 (it returns after the results are written). Its scratch memory is one
+ * file-scope device array of NNDEX_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until exit; a batch whose normalised queries and candidate keys do not fit is rejected with
+ * NNDEX_ERR_UNSUPPORTED. The first call on a device looks up the array's address (make it before
+ * any stream capture). All calls share the array: calls that overlap on the GPU race.
+ */
+NNDEX_API int nndex_cuda_search_batch_device_noalloc(nndex_cuda_index* index, const float* dev_queries,
+                                                     uint64_t query_rows, uint64_t query_dims, uint64_t k,
+                                                     uint64_t* dev_idx_out, float* dev_sim_out,
+                                                     uint32_t* dev_counts_out, void* stream);
+
 /* ---- FP64 oracle on the device (score-error report) ------------------------------------- */
 
 /*

@@ -102,7 +102,10 @@ SIGNATURES = {
     "nndex_cuda_set_scan_timing": (_i32, [_vp, _i32]),
     "nndex_cuda_scan_timing": (_i32, [_vp, C.POINTER(C.c_double), C.POINTER(_u64)]),
     "nndex_cuda_fp64_scores": (_i32, [_vp, _vp, _u64, _vp, _vp, _u64, _vp]),
+    "nndex_cuda_search_batch_device_noalloc": (_i32, [_vp, _vp, _u64, _u64, _u64, _vp, _vp, _vp, _vp]),
 }
+
+NNDEX_NOALLOC_SCRATCH_BYTES = 16 << 20
 
 _lib = None
 

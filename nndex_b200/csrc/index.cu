@@ -527,10 +527,6 @@ uint64_t launches() { return g_launches.load(); }
 // =============================================================================================
 using namespace nndex;
 
-struct nndex_cuda_index {
-    CudaIndex* impl;
-};
-
 extern "C" {
 
 const char* nndex_cuda_last_error(void) { return last_error(); }

@@ -86,4 +86,12 @@ struct CudaIndex {
     int stream_status();
 };
 
+int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out,
+                          float* d_sim_out, uint32_t* d_cnt_out, cudaStream_t s);
+
 }  // namespace nndex
+
+// The opaque handle behind the C ABI.
+struct nndex_cuda_index {
+    nndex::CudaIndex* impl;
+};
