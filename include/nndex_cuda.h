@@ -183,6 +183,25 @@ NNDEX_API int nndex_cuda_search_batch_device(nndex_cuda_index* index, const floa
                                    uint64_t* dev_idx_out, float* dev_sim_out,
                                    uint32_t* dev_counts_out, void* stream, int synchronize);
 
+/*
+ * Selects the scan precision for later searches (NNDEX_PRECISION_*; BF16/FP8 need the index to have
+ * been created with NNDEX_FLAG_BF16/FP8) and the candidate width k' of the low-precision scan
+ * (0 = autotuned). Low-precision searches return the exact FP32 top-k: the k' candidates are
+ * re-scored in FP32 and queries whose exactness certificate fails are re-run on the FP32 scan.
+ * Tensor-core searches synchronise the stream (the certificate's fallback is decided on the host).
+ */
+NNDEX_API int nndex_cuda_set_precision(nndex_cuda_index* index, uint32_t precision, uint32_t rerank_width);
+
+/*
+ * Candidates of the last low-precision search on this index (diagnostics and error reports):
+ * for each of `query_rows` queries, the k' rows ranked by approximate (BF16/FP8) score, with those
+ * approximate scores, and the bound eps the exactness certificate used for this index's copy
+ * (max row residual). Host buffers of query_rows × k' entries; *kprime receives k'.
+ */
+NNDEX_API int nndex_cuda_last_candidates(nndex_cuda_index* index, uint64_t query_rows, uint64_t* idx_out,
+                                         float* approx_out, uint64_t capacity, uint32_t* kprime,
+                                         float* eps_rows);
+
 /* Status word of the last asynchronous device call on this index (0 when clean). */
 NNDEX_API int nndex_cuda_stream_status(nndex_cuda_index* index);
 

@@ -127,7 +127,7 @@ class NNdex:
     def __init__(self, data: Any, normalized: bool = False, approx: bool = False, backend: str = "cuda",
                  enable_cache: bool = True, gpu_device_index: int | None = None, *, precision: str = "fp32",
                  nlist: int = 0, nprobe: int = 0, kmeans_iters: int = 0, seed: int | None = None,
-                 rerank_width: int = 0):
+                 rerank_width: int = 0, low_precision_copies: tuple = ()):
         self._backend = _parse_backend(backend)
         if precision not in _PRECISIONS:
             raise ValueError(f"unsupported precision '{precision}', expected one of: {', '.join(_PRECISIONS)}")
@@ -142,10 +142,13 @@ class NNdex:
             flags |= NNDEX_FLAG_NORMALIZED
         if approx:
             flags |= NNDEX_FLAG_APPROX
-        if precision == "bf16":
+        # "bf16" / "fp8" keep that scoring copy; "auto" keeps a BF16 copy for large batches.
+        if precision in ("bf16", "auto"):
             flags |= NNDEX_FLAG_BF16
         if precision == "fp8":
             flags |= NNDEX_FLAG_FP8
+        for extra in low_precision_copies:
+            flags |= {"bf16": NNDEX_FLAG_BF16, "fp8": NNDEX_FLAG_FP8}[extra]
         opts = _lib.Opts()
         opts.device = -1 if gpu_device_index is None else int(gpu_device_index)
         opts.precision = _PRECISIONS[precision]
@@ -194,6 +197,24 @@ class NNdex:
     def handle(self) -> C.c_void_p:
         """The opaque nndex_cuda_index* (for callers that drive the C ABI directly)."""
         return self._h
+
+    def set_precision(self, precision: str, rerank_width: int = 0) -> None:
+        """Scan precision for later searches: "fp32", "bf16", "fp8" or "auto" (see __init__)."""
+        if precision not in _PRECISIONS:
+            raise ValueError(f"unsupported precision '{precision}', expected one of: {', '.join(_PRECISIONS)}")
+        _check(_lib.lib().nndex_cuda_set_precision(self._h, _PRECISIONS[precision], int(rerank_width)))
+
+    def last_candidates(self, query_rows: int):
+        """(rows, approximate scores, eps) of the last low-precision search's k′ candidates."""
+        kp = C.c_uint32(0)
+        eps = C.c_float(0.0)
+        st = self.last_search_stats()
+        kk = int(st["rerank_width"])
+        idx = np.zeros((query_rows, max(kk, 1)), dtype=np.uint64)
+        sim = np.zeros((query_rows, max(kk, 1)), dtype=np.float32)
+        _check(_lib.lib().nndex_cuda_last_candidates(self._h, query_rows, idx.ctypes.data, sim.ctypes.data, idx.size,
+                                                     C.byref(kp), C.byref(eps)))
+        return idx[:, :kp.value], sim[:, :kp.value], float(eps.value)
 
     def last_search_stats(self) -> dict:
         s = _lib.SearchStats()

@@ -176,6 +176,20 @@ CudaIndex::~CudaIndex() {
     cudaFreeHost(h_sim);
     cudaFreeHost(h_cnt);
     cudaFreeHost(h_flags);
+    cudaFree(d_base_bf16);
+    cudaFree(d_base_fp8);
+    cudaFree(d_row_scale);
+    cudaFree(d_q_bf16);
+    cudaFree(d_q_fp8);
+    cudaFree(d_q_scale);
+    cudaFree(d_q_resid);
+    cudaFree(d_thr);
+    cudaFree(d_cand_idx);
+    cudaFree(d_cand_sim);
+    cudaFree(d_cand_cnt);
+    cudaFree(d_cert);
+    cudaFree(d_qsub);
+    cudaFreeHost(h_cert);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -269,6 +283,208 @@ int CudaIndex::check_device_words() {
     return NNDEX_OK;
 }
 
+// ---- path choice (the autotuner's rules; see autotune notes in DESIGN) ---------------------
+
+int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
+    const bool has16 = d_base_bf16 != nullptr, has8 = d_base_fp8 != nullptr;
+    auto tc_ok = [&](bool fp8) {
+        const uint64_t kb = fp8 ? kf8 : kb16;
+        const uint32_t nchunks = static_cast<uint32_t>(kb * (fp8 ? 1 : 2) / 128);
+        const uint32_t kp = choose_kprime(kcap, fp8);
+        return kp >= kcap && kp > 0 && tc_smem_bytes(nchunks, kp) <= smem_optin;
+    };
+    switch (precision) {
+        case NNDEX_PRECISION_FP32: return 1;
+        case NNDEX_PRECISION_BF16: return (has16 && tc_ok(false)) ? 2 : 1;
+        case NNDEX_PRECISION_FP8: return (has8 && tc_ok(true)) ? 3 : 1;
+        default:
+            // FP32 streaming is HBM-bound at small batches; the tensor cores win from a few dozen
+            // queries per batch (the scan becomes compute-bound in FP32).
+            if (nq >= 64) {
+                if (has16 && tc_ok(false)) return 2;
+                if (has8 && tc_ok(true)) return 3;
+            }
+            return 1;
+    }
+}
+
+uint32_t CudaIndex::choose_kprime(uint64_t kcap, bool fp8) const {
+    const uint64_t kb = fp8 ? kf8 : kb16;
+    const uint32_t nchunks = static_cast<uint32_t>(kb * (fp8 ? 1 : 2) / 128);
+    // Largest k′ whose per-query heaps fit next to the resident query block and the base ring.
+    uint32_t kmax = 0;
+    for (uint32_t kp = 8; kp <= 256; kp += 8)
+        if (tc_smem_bytes(nchunks, kp) <= smem_optin) kmax = kp;
+    uint32_t kp = rerank_width ? rerank_width : static_cast<uint32_t>(std::max<uint64_t>(32, 3 * kcap));
+    if (kp > kmax) kp = kmax;
+    if (kp > rows) kp = static_cast<uint32_t>(rows);
+    return kp;
+}
+
+int CudaIndex::enqueue_prep_queries(const float* d_raw, uint64_t n, int mode, int path, cudaStream_t s) {
+    int st;
+    PrepArgs p;
+    p.src = d_raw;
+    p.rows = n;
+    p.dims = static_cast<uint32_t>(dims);
+    p.out = d_qn;
+    p.out_stride = static_cast<uint32_t>(ds);
+    p.mode = mode;
+    p.err = d_err;
+    p.sm_count = sm_count;
+    if (path >= 2) {
+        const uint64_t nq_alloc = (n + 127) / 128 * 128;
+        if ((st = grow_device(d_q_resid, cap_q_resid, n, "query buffer"))) return st;
+        if (path == 2) {
+            const bool grew = nq_alloc * kb16 > cap_q_bf16;
+            if ((st = grow_device(d_q_bf16, cap_q_bf16, nq_alloc * kb16, "query buffer"))) return st;
+            if (grew) cudaMemsetAsync(d_q_bf16, 0, cap_q_bf16 * sizeof(__nv_bfloat16), s);
+            p.out_bf16 = d_q_bf16;
+            p.bf16_stride = static_cast<uint32_t>(kb16);
+            p.resid_bf16 = d_q_resid;
+        } else {
+            const bool grew = nq_alloc * kf8 > cap_q_fp8;
+            if ((st = grow_device(d_q_fp8, cap_q_fp8, nq_alloc * kf8, "query buffer"))) return st;
+            if (grew) cudaMemsetAsync(d_q_fp8, 0, cap_q_fp8, s);
+            if ((st = grow_device(d_q_scale, cap_q_scale, n, "query buffer"))) return st;
+            p.out_fp8 = d_q_fp8;
+            p.fp8_stride = static_cast<uint32_t>(kf8);
+            p.fp8_scale = d_q_scale;
+            p.resid_fp8 = d_q_resid;
+        }
+    }
+    launch_prep_rows(p, s);
+    stats.kernel_launches += 1;
+    return NNDEX_OK;
+}
+
+int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                          cudaStream_t s) {
+    int st;
+    const uint32_t kp = choose_kprime(kcap, fp8);
+    const uint64_t kb = fp8 ? kf8 : kb16;
+    const uint32_t nchunks = static_cast<uint32_t>(kb * (fp8 ? 1 : 2) / 128);
+    const uint32_t nqb = (n + 127) / 128;
+    // Row ranges: about four waves of CTAs, each range a multiple of the 256-row tile.
+    uint64_t nranges = (4ull * sm_count + nqb - 1) / nqb;
+    nranges = std::max<uint64_t>(1, std::min<uint64_t>(nranges, (rows + 2047) / 2048));
+    uint64_t range_rows = (rows + nranges - 1) / nranges;
+    range_rows = (range_rows + 255) / 256 * 256;
+    nranges = (rows + range_rows - 1) / range_rows;
+    const uint64_t per_query = nranges * kp;
+    if ((st = grow_device(d_thr, cap_thr, n, "tc workspace"))) return st;
+    if ((st = grow_device(d_ws, cap_ws, per_query * n, "tc workspace"))) return st;
+    if ((st = grow_device(d_cand_idx, cap_cand_idx, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
+    if ((st = grow_device(d_cand_sim, cap_cand_sim, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
+    if ((st = grow_device(d_cand_cnt, cap_cand_cnt, n, "tc workspace"))) return st;
+    if ((st = grow_device(d_cert, cap_cert, n, "tc workspace"))) return st;
+    // Tensor map of the quantised query buffer (its address can change when it grows).
+    CUtensorMap tmap_q;
+    const uint64_t nq_alloc = (n + 127) / 128 * 128;
+    const bool ok = fp8 ? encode_tmap_2d(&tmap_q, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, d_q_fp8, kf8, nq_alloc, kf8, 128,
+                                         128, CU_TENSOR_MAP_SWIZZLE_128B)
+                        : encode_tmap_2d(&tmap_q, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, d_q_bf16, kb16, nq_alloc,
+                                         kb16 * 2, 64, 128, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (!ok) return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (queries)");
+    cudaMemsetAsync(d_thr, 0, n * sizeof(unsigned long long), s);
+    TcArgs a;
+    a.tmap_q = &tmap_q;
+    a.tmap_b = fp8 ? &tmap_fp8 : &tmap_bf16;
+    a.nq = n;
+    a.nchunks = nchunks;
+    a.rows = rows;
+    a.range_rows = range_rows;
+    a.nranges = static_cast<uint32_t>(nranges);
+    a.kprime = kp;
+    a.row_scale = fp8 ? d_row_scale : nullptr;
+    a.q_scale = fp8 ? d_q_scale : nullptr;
+    a.thr_global = d_thr;
+    a.ws_keys = d_ws;
+    a.status = d_status;
+    cudaEvent_t ev_a = nullptr;
+    scan_event_begin(s, ev_a);
+    cudaError_t e = launch_scan_tc(a, fp8, s);
+    scan_event_end(s, ev_a);
+    if (e != cudaSuccess) return cuda_error(e, "tensor-core scan launch");
+    MergeArgs m;
+    m.ws_keys = d_ws;
+    m.nq = n;
+    m.per_query = per_query;
+    m.k = kp;
+    m.out_stride = kp;
+    m.idx_out = d_cand_idx;
+    m.sim_out = d_cand_sim;
+    m.count_out = d_cand_cnt;
+    if ((e = launch_merge_topk(m, s)) != cudaSuccess) return cuda_error(e, "merge launch");
+    RerankArgs r;
+    r.base = d_base;
+    r.ds = static_cast<uint32_t>(ds);
+    r.queries = d_qn;
+    r.cand_idx = d_cand_idx;
+    r.cand_sim = d_cand_sim;
+    r.cand_cnt = d_cand_cnt;
+    r.nq = n;
+    r.kp = kp;
+    r.k = kcap;
+    r.q_resid = d_q_resid;
+    r.eps_rows = fp8 ? eps_fp8 : eps_bf16;
+    // FP32 accumulation of kb exact products (|Σ| ≤ 1 + ε): kb·2^-23, with a 4× margin.
+    r.eps_acc = 4.0f * static_cast<float>(kb) * 1.1920929e-07f;
+    r.idx_out = o_idx;
+    r.sim_out = o_sim;
+    r.cnt_out = o_cnt;
+    r.cert_out = d_cert;
+    if ((e = launch_rerank(r, s)) != cudaSuccess) return cuda_error(e, "rerank launch");
+    stats.kernel_launches += 3;
+    stats.path = fp8 ? 3 : 2;
+    stats.rerank_width = kp;
+    stats.rows_scanned += rows * n;
+    return NNDEX_OK;
+}
+
+int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                         cudaStream_t s) {
+    int st;
+    if ((st = grow_host(h_cert, cap_hcert, n, "pinned buffer"))) return st;
+    cudaMemcpyAsync(h_cert, d_cert, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    h_flags[1] = 0;
+    cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_error(e, "search");
+    if ((st = check_device_words())) return st;
+    std::vector<uint32_t> failed;
+    for (uint32_t i = 0; i < n; ++i)
+        if (!h_cert[i]) failed.push_back(i);
+    stats.certified = failed.empty() ? 1u : 0u;
+    stats.widenings = static_cast<uint32_t>(failed.size());  // queries re-run on the FP32 path
+    if (failed.empty()) return NNDEX_OK;
+    const uint32_t m = static_cast<uint32_t>(failed.size());
+    if ((st = grow_device(d_qsub, cap_qsub, static_cast<uint64_t>(m) * ds, "fallback buffer"))) return st;
+    for (uint32_t i = 0; i < m; ++i)
+        cudaMemcpyAsync(d_qsub + static_cast<uint64_t>(i) * ds, d_qn + static_cast<uint64_t>(failed[i]) * ds,
+                        ds * sizeof(float), cudaMemcpyDeviceToDevice, s);
+    // results of the re-run land in the candidate buffers, then move to their query's slots
+    if ((st = grow_device(d_cand_idx, cap_cand_idx, static_cast<uint64_t>(m) * kcap, "fallback buffer"))) return st;
+    if ((st = grow_device(d_cand_sim, cap_cand_sim, static_cast<uint64_t>(m) * kcap, "fallback buffer"))) return st;
+    if ((st = grow_device(d_cand_cnt, cap_cand_cnt, m, "fallback buffer"))) return st;
+    const uint32_t path = stats.path;
+    if ((st = enqueue_exact_fp32(d_qsub, m, kcap, kcap, d_cand_idx, d_cand_sim, d_cand_cnt, s))) return st;
+    stats.path = path;
+    for (uint32_t i = 0; i < m; ++i) {
+        const uint64_t q = failed[i];
+        cudaMemcpyAsync(o_idx + q * kcap, d_cand_idx + static_cast<uint64_t>(i) * kcap, kcap * sizeof(uint64_t),
+                        cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(o_sim + q * kcap, d_cand_sim + static_cast<uint64_t>(i) * kcap, kcap * sizeof(float),
+                        cudaMemcpyDeviceToDevice, s);
+        if (o_cnt)
+            cudaMemcpyAsync(o_cnt + q, d_cand_cnt + i, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+    }
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_error(e, "search");
+    return NNDEX_OK;
+}
+
 int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mode, uint64_t* idx_out,
                            float* sim_out, uint64_t* counts_out) {
     std::lock_guard<std::mutex> lock(mu);
@@ -282,6 +498,7 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
     const uint64_t chunk = kMaxBatchChunk;
     for (uint64_t q0 = 0; q0 < nq; q0 += chunk) {
         const uint64_t n = std::min<uint64_t>(chunk, nq - q0);
+        const int path = choose_path(n, kcap);
         int st;
         if ((st = ensure_query_capacity(n))) return st;
         if ((st = ensure_result_capacity(n, kcap))) return st;
@@ -289,10 +506,18 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         cudaMemsetAsync(d_err, 0xFF, sizeof(unsigned long long), stream);
         cudaMemsetAsync(d_status, 0, sizeof(uint32_t), stream);
         cudaMemcpyAsync(d_qraw, h_q, n * dims * sizeof(float), cudaMemcpyHostToDevice, stream);
-        enqueue_query_prep(n, mode, stream);
-        if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
-                                     static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
-            return st;
+        if ((st = enqueue_prep_queries(d_qraw, n, mode, path, stream))) return st;
+        if (path == 1) {
+            if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
+                                         static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
+                return st;
+        } else {
+            if ((st = enqueue_tc(path == 3, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim,
+                                 d_cnt, stream)))
+                return st;
+            if ((st = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
+                return st;
+        }
         cudaMemcpyAsync(h_idx, d_idx, n * kcap * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
         cudaMemcpyAsync(h_sim, d_sim, n * kcap * sizeof(float), cudaMemcpyDeviceToHost, stream);
         cudaMemcpyAsync(h_cnt, d_cnt, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
@@ -326,26 +551,27 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
     if ((st = ensure_query_capacity(std::min<uint64_t>(nq, kMaxBatchChunk)))) return st;
     cudaMemsetAsync(d_err, 0xFF, sizeof(unsigned long long), s);
     cudaMemsetAsync(d_status, 0, sizeof(uint32_t), s);
+    bool synced = false;
     for (uint64_t q0 = 0; q0 < nq; q0 += kMaxBatchChunk) {
         const uint64_t n = std::min<uint64_t>(kMaxBatchChunk, nq - q0);
-        PrepArgs p;
-        p.src = d_queries + q0 * dims;
-        p.rows = n;
-        p.dims = static_cast<uint32_t>(dims);
-        p.row_base = q0;
-        p.out = d_qn;
-        p.out_stride = static_cast<uint32_t>(ds);
-        p.mode = normalized ? 2 : 0;
-        p.err = d_err;
-        p.sm_count = sm_count;
-        launch_prep_rows(p, s);
-        stats.kernel_launches += 1;
-        if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
-                                     static_cast<uint32_t>(kcap), d_idx_out + q0 * kcap, d_sim_out + q0 * kcap,
-                                     d_cnt_out ? d_cnt_out + q0 : nullptr, s)))
-            return st;
+        const int path = choose_path(n, kcap);
+        if ((st = enqueue_prep_queries(d_queries + q0 * dims, n, normalized ? 2 : 0, path, s))) return st;
+        uint64_t* oi = d_idx_out + q0 * kcap;
+        float* os = d_sim_out + q0 * kcap;
+        uint32_t* oc = d_cnt_out ? d_cnt_out + q0 : nullptr;
+        if (path == 1) {
+            if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
+                                         static_cast<uint32_t>(kcap), oi, os, oc, s)))
+                return st;
+        } else {
+            // The certificate's fallback needs the host: tensor-core batches always synchronise.
+            if ((st = enqueue_tc(path == 3, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s)))
+                return st;
+            if ((st = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s))) return st;
+            synced = true;
+        }
     }
-    if (synchronize) {
+    if (synchronize || synced) {
         h_flags[1] = 0;
         cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
@@ -408,8 +634,10 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
     ix->dims = dims;
     ix->dp = dp;
     ix->ds = (dims + 31) / 32 * 32;
-    ix->rows_alloc = (rows + 127) / 128 * 128;
+    ix->rows_alloc = (rows + 255) / 256 * 256;  // whole 256-row tensor-core tiles
     ix->flags = flags;
+    ix->precision = o.precision;
+    ix->rerank_width = o.rerank_width;
     ix->normalized = (flags & NNDEX_FLAG_NORMALIZED) != 0;
     ix->approx = (flags & NNDEX_FLAG_APPROX) != 0;
     ix->opts = o;
@@ -432,6 +660,48 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
     if ((e = cudaMalloc(&ix->d_base, base_bytes)) != cudaSuccess) return fail(cuda_error(e, "base allocation"));
     cudaMemsetAsync(ix->d_base + rows * ix->ds, 0, (ix->rows_alloc - rows) * ix->ds * sizeof(float), ix->stream);
     cudaMemsetAsync(ix->d_err, 0xFF, sizeof(unsigned long long), ix->stream);
+    // Low-precision scoring copies (K1 writes them in the same pass) and their residual norms.
+    float* d_res16 = nullptr;
+    float* d_res8 = nullptr;
+    unsigned int* d_max = nullptr;
+    auto free_tmp = [&]() {
+        cudaFree(d_res16);
+        cudaFree(d_res8);
+        cudaFree(d_max);
+    };
+    if (flags & NNDEX_FLAG_BF16) {
+        ix->kb16 = (dims + 63) / 64 * 64;
+        if ((e = cudaMalloc(&ix->d_base_bf16, ix->rows_alloc * ix->kb16 * 2)) != cudaSuccess ||
+            (e = cudaMalloc(&d_res16, rows * sizeof(float))) != cudaSuccess) {
+            free_tmp();
+            return fail(cuda_error(e, "BF16 copy allocation"));
+        }
+        cudaMemsetAsync(ix->d_base_bf16, 0, ix->rows_alloc * ix->kb16 * 2, ix->stream);
+    }
+    if (flags & NNDEX_FLAG_FP8) {
+        ix->kf8 = (dims + 127) / 128 * 128;
+        if ((e = cudaMalloc(&ix->d_base_fp8, ix->rows_alloc * ix->kf8)) != cudaSuccess ||
+            (e = cudaMalloc(&ix->d_row_scale, ix->rows_alloc * sizeof(float))) != cudaSuccess ||
+            (e = cudaMalloc(&d_res8, rows * sizeof(float))) != cudaSuccess) {
+            free_tmp();
+            return fail(cuda_error(e, "FP8 copy allocation"));
+        }
+        cudaMemsetAsync(ix->d_base_fp8, 0, ix->rows_alloc * ix->kf8, ix->stream);
+        cudaMemsetAsync(ix->d_row_scale, 0, ix->rows_alloc * sizeof(float), ix->stream);
+    }
+    auto add_low_precision = [&](PrepArgs& p, uint64_t r0) {
+        if (ix->d_base_bf16) {
+            p.out_bf16 = ix->d_base_bf16 + r0 * ix->kb16;
+            p.bf16_stride = static_cast<uint32_t>(ix->kb16);
+            p.resid_bf16 = d_res16 + r0;
+        }
+        if (ix->d_base_fp8) {
+            p.out_fp8 = ix->d_base_fp8 + r0 * ix->kf8;
+            p.fp8_stride = static_cast<uint32_t>(ix->kf8);
+            p.fp8_scale = ix->d_row_scale + r0;
+            p.resid_fp8 = d_res8 + r0;
+        }
+    };
 
     // K1: upload in chunks (≈256 MB of raw rows each), validate + normalise + pad on the device.
     const int mode = ix->normalized ? 2 : 0;
@@ -445,6 +715,7 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
         p.mode = mode;
         p.err = ix->d_err;
         p.sm_count = ix->sm_count;
+        add_low_precision(p, 0);
         launch_prep_rows(p, ix->stream);
     } else {
         uint64_t chunk_rows = std::max<uint64_t>(1, (256ull << 20) / (dims * sizeof(float)));
@@ -454,6 +725,7 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
         for (int b = 0; b < 2; ++b) {
             if ((e = cudaMalloc(&d_raw[b], chunk_rows * dims * sizeof(float))) != cudaSuccess) {
                 cudaFree(d_raw[0]);
+                free_tmp();
                 return fail(cuda_error(e, "upload staging"));
             }
             cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming);
@@ -475,6 +747,7 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
             p.mode = mode;
             p.err = ix->d_err;
             p.sm_count = ix->sm_count;
+            add_low_precision(p, r0);
             launch_prep_rows(p, ix->stream);
             cudaEventRecord(done[b], ix->stream);
         }
@@ -483,14 +756,48 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
             cudaFree(d_raw[i]);
             cudaEventDestroy(done[i]);
         }
-        if (e != cudaSuccess) return fail(cuda_error(e, "upload"));
+        if (e != cudaSuccess) {
+            free_tmp();
+            return fail(cuda_error(e, "upload"));
+        }
     }
     cudaMemcpyAsync(&ix->h_flags[0], ix->d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, ix->stream);
-    if ((e = cudaStreamSynchronize(ix->stream)) != cudaSuccess) return fail(cuda_error(e, "upload"));
-    if (ix->h_flags[0] != ~0ull) return fail(err_code(static_cast<int>(ix->h_flags[0] & 0xFF)));
+    if ((e = cudaStreamSynchronize(ix->stream)) != cudaSuccess) {
+        free_tmp();
+        return fail(cuda_error(e, "upload"));
+    }
+    if (ix->h_flags[0] != ~0ull) {
+        free_tmp();
+        return fail(err_code(static_cast<int>(ix->h_flags[0] & 0xFF)));
+    }
+    if (d_res16 || d_res8) {
+        // ε of the certificate: the largest residual norm ‖x − x̂‖ over the rows.
+        if ((e = cudaMalloc(&d_max, 2 * sizeof(unsigned int))) != cudaSuccess) {
+            free_tmp();
+            return fail(cuda_error(e, "alloc"));
+        }
+        cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned int), ix->stream);
+        if (d_res16) launch_max_reduce(d_res16, rows, d_max, ix->stream);
+        if (d_res8) launch_max_reduce(d_res8, rows, d_max + 1, ix->stream);
+        unsigned int hm[2] = {0, 0};
+        cudaMemcpyAsync(hm, d_max, sizeof(hm), cudaMemcpyDeviceToHost, ix->stream);
+        e = cudaStreamSynchronize(ix->stream);
+        free_tmp();
+        if (e != cudaSuccess) return fail(cuda_error(e, "residual reduction"));
+        std::memcpy(&ix->eps_bf16, &hm[0], 4);
+        std::memcpy(&ix->eps_fp8, &hm[1], 4);
+    }
     if (!encode_tmap_2d(&ix->tmap_f32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ix->d_base, ix->ds, ix->rows_alloc,
                         ix->ds * sizeof(float), 32, 128, CU_TENSOR_MAP_SWIZZLE_128B))
         return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed"));
+    if (ix->d_base_bf16 &&
+        !encode_tmap_2d(&ix->tmap_bf16, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ix->d_base_bf16, ix->kb16, ix->rows_alloc,
+                        ix->kb16 * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B))
+        return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (BF16)"));
+    if (ix->d_base_fp8 &&
+        !encode_tmap_2d(&ix->tmap_fp8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ix->d_base_fp8, ix->kf8, ix->rows_alloc,
+                        ix->kf8, 128, 256, CU_TENSOR_MAP_SWIZZLE_128B))
+        return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (FP8)"));
     *out = ix;
     return NNDEX_OK;
 }
@@ -664,6 +971,44 @@ int nndex_cuda_search_batch_device(nndex_cuda_index* index, const float* dev_que
                          kMaxFusedK);
     return ix->search_device(dev_queries, query_rows, k, dev_idx_out, dev_sim_out, dev_counts_out,
                              static_cast<cudaStream_t>(stream), synchronize);
+}
+
+int nndex_cuda_set_precision(nndex_cuda_index* index, uint32_t precision, uint32_t rerank_width) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    if (precision > NNDEX_PRECISION_FP8)
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: unknown precision %u", precision);
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    if ((precision == NNDEX_PRECISION_BF16 && !ix->d_base_bf16) || (precision == NNDEX_PRECISION_FP8 && !ix->d_base_fp8))
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT,
+                         "cuda execution error: the index keeps no %s copy (create it with NNDEX_FLAG_%s)",
+                         precision == NNDEX_PRECISION_BF16 ? "BF16" : "FP8",
+                         precision == NNDEX_PRECISION_BF16 ? "BF16" : "FP8");
+    ix->precision = precision;
+    ix->rerank_width = rerank_width;
+    return NNDEX_OK;
+}
+
+int nndex_cuda_last_candidates(nndex_cuda_index* index, uint64_t query_rows, uint64_t* idx_out, float* approx_out,
+                               uint64_t capacity, uint32_t* kprime, float* eps_rows) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    cudaSetDevice(ix->device);
+    const uint32_t kp = ix->stats.rerank_width;
+    if (kprime) *kprime = kp;
+    if (eps_rows) *eps_rows = ix->stats.path == 3 ? ix->eps_fp8 : ix->eps_bf16;
+    if (kp == 0 || !ix->d_cand_idx) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: no low-precision search yet");
+    const uint64_t n = query_rows * kp;
+    if (n > capacity || n > ix->cap_cand_idx)
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: candidate buffer too small");
+    cudaError_t e = cudaStreamSynchronize(ix->stream);
+    if (e == cudaSuccess && idx_out) e = cudaMemcpy(idx_out, ix->d_cand_idx, n * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && approx_out) e = cudaMemcpy(approx_out, ix->d_cand_sim, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(e, "candidates");
+    return NNDEX_OK;
 }
 
 int nndex_cuda_stream_status(nndex_cuda_index* index) {

@@ -38,6 +38,40 @@ struct CudaIndex {
     float* d_base = nullptr;  // rows_alloc × ds FP32, normalised, zero padded
     CUtensorMap tmap_f32{};
 
+    // Low-precision scoring copies (NNDEX_FLAG_BF16 / NNDEX_FLAG_FP8), K3.
+    uint32_t precision = NNDEX_PRECISION_AUTO;
+    uint64_t kb16 = 0;                         // BF16 row length: dims rounded up to 64
+    uint64_t kf8 = 0;                          // FP8 row length: dims rounded up to 128
+    __nv_bfloat16* d_base_bf16 = nullptr;      // rows_alloc × kb16
+    uint8_t* d_base_fp8 = nullptr;             // rows_alloc × kf8 (E4M3)
+    float* d_row_scale = nullptr;              // rows_alloc: FP8 dequantisation scale per row
+    float eps_bf16 = 0.0f, eps_fp8 = 0.0f;     // max row residual norm ‖x − x̂‖
+    CUtensorMap tmap_bf16{}, tmap_fp8{};
+    // per-search buffers of the tensor-core path
+    __nv_bfloat16* d_q_bf16 = nullptr;
+    size_t cap_q_bf16 = 0;
+    uint8_t* d_q_fp8 = nullptr;
+    size_t cap_q_fp8 = 0;
+    float* d_q_scale = nullptr;
+    size_t cap_q_scale = 0;
+    float* d_q_resid = nullptr;
+    size_t cap_q_resid = 0;
+    unsigned long long* d_thr = nullptr;
+    size_t cap_thr = 0;
+    uint64_t* d_cand_idx = nullptr;
+    size_t cap_cand_idx = 0;
+    float* d_cand_sim = nullptr;
+    size_t cap_cand_sim = 0;
+    uint32_t* d_cand_cnt = nullptr;
+    size_t cap_cand_cnt = 0;
+    uint32_t* d_cert = nullptr;
+    size_t cap_cert = 0;
+    uint32_t* h_cert = nullptr;
+    size_t cap_hcert = 0;
+    float* d_qsub = nullptr;  // FP32 queries re-run after a failed certificate
+    size_t cap_qsub = 0;
+    uint32_t rerank_width = 0;  // k′ override (0 = autotuned)
+
     // per-search buffers (grown on demand)
     float* d_qraw = nullptr;
     size_t cap_qraw = 0;
@@ -83,6 +117,15 @@ struct CudaIndex {
                     uint64_t* counts_out);
     int search_device(const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out, float* d_sim_out,
                       uint32_t* d_cnt_out, cudaStream_t s, int synchronize);
+    // Path choice for a batch: 1 = FP32 scan, 2 = BF16 tensor-core scan, 3 = FP8 tensor-core scan.
+    int choose_path(uint64_t nq, uint64_t kcap) const;
+    uint32_t choose_kprime(uint64_t kcap, bool fp8) const;
+    int enqueue_prep_queries(const float* d_raw, uint64_t n, int mode, int path, cudaStream_t s);
+    int enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                   cudaStream_t s);
+    // After a tensor-core batch has completed: re-run the queries whose certificate failed on the
+    // FP32 path (device outputs are patched in place). Synchronises the stream.
+    int finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
     int stream_status();
 };
 

@@ -73,6 +73,43 @@ struct MergeArgs {
 };
 cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream);
 
+// K3 tensor-core scan (BF16 / FP8) with fused top-k′ filter, and K4 rerank.
+struct TcArgs {
+    const CUtensorMap* tmap_q = nullptr;  // quantised queries [nq_alloc × K], box {128 B, 128 rows}
+    const CUtensorMap* tmap_b = nullptr;  // quantised base [rows_alloc × K], box {128 B, 256 rows}
+    uint32_t nq = 0;
+    uint32_t nchunks = 0;                 // K bytes / 128
+    uint64_t rows = 0;
+    uint64_t range_rows = 0;              // rows per CTA range (multiple of 256)
+    uint32_t nranges = 0;
+    uint32_t kprime = 0;
+    const float* row_scale = nullptr;     // FP8 only
+    const float* q_scale = nullptr;       // FP8 only
+    unsigned long long* thr_global = nullptr;  // per query, zeroed before the launch
+    uint64_t* ws_keys = nullptr;          // nq × nranges × kprime
+    uint32_t* status = nullptr;
+};
+size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime);
+cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, cudaStream_t stream);
+
+struct RerankArgs {
+    const float* base = nullptr;  // FP32 base, stride ds
+    uint32_t ds = 0;
+    const float* queries = nullptr;  // FP32 normalised queries, stride ds
+    const uint64_t* cand_idx = nullptr;  // nq × kp, sorted by approximate score
+    const float* cand_sim = nullptr;
+    const uint32_t* cand_cnt = nullptr;
+    uint32_t nq = 0, kp = 0, k = 0;
+    const float* q_resid = nullptr;
+    float eps_rows = 0.0f, eps_acc = 0.0f;
+    uint64_t* idx_out = nullptr;
+    float* sim_out = nullptr;
+    uint32_t* cnt_out = nullptr;
+    uint32_t* cert_out = nullptr;
+};
+cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream);
+cudaError_t launch_max_reduce(const float* v, uint64_t n, unsigned int* out, cudaStream_t stream);
+
 // Maximum k the fused scan kernels select in shared memory.
 constexpr uint32_t kMaxFusedK = 2048;
 

@@ -1,0 +1,112 @@
+"""Tensor-core (BF16 / FP8) scan + exact FP32 rerank against the oracle (needs a B200).
+
+The low-precision paths must return the exact FP32 top-k (same acceptance rule as the FP32 path):
+candidates are re-scored in FP32 and queries whose certificate fails are re-run on the FP32 scan.
+The approximate candidate scores themselves must stay within the certificate's error bound.
+"""
+import numpy as np
+import pytest
+
+from nndex_b200 import NNdex
+from oracle import oracle as O
+from tests._parity import assert_topk_matches
+
+pytestmark = pytest.mark.gpu
+
+
+def mixture(rng, rows, dims, centers, sigma):
+    c = rng.normal(size=(centers, dims)).astype(np.float32)
+    a = rng.integers(0, centers, size=rows)
+    x = c[a] + np.float32(sigma) * rng.normal(size=(rows, dims)).astype(np.float32)
+    return x.astype(np.float32)
+
+
+def _check(index, m, queries, k, what):
+    st, base = O.prepare_index(m, False)
+    assert st == 0
+    idx, sim = index.search(queries, k=k)
+    _, qn = O.prepare_queries(queries, False, base.shape[1])
+    for i in range(queries.shape[0]):
+        assert_topk_matches(idx[i], sim[i], O.scores_f64(base, qn[i]), k, what=f"{what} q{i}")
+    return base, qn, idx, sim
+
+
+CASES = [
+    # precision, rows, dims, nq, k, data
+    ("bf16", 20_000, 128, 128, 10, "mixture"),
+    ("bf16", 50_000, 256, 300, 10, "mixture"),
+    ("bf16", 7_777, 100, 65, 5, "mixture"),
+    ("bf16", 30_000, 64, 129, 16, "gauss"),
+    ("fp8", 20_000, 128, 128, 10, "mixture"),
+    ("fp8", 40_000, 256, 200, 10, "mixture"),
+    ("fp8", 9_000, 200, 40, 8, "gauss"),
+]
+
+
+@pytest.mark.parametrize("precision,rows,dims,nq,k,data", CASES)
+def test_low_precision_exact_topk(precision, rows, dims, nq, k, data):
+    rng = np.random.default_rng(rows + dims + nq)
+    if data == "mixture":
+        m = mixture(rng, rows, dims, 256, 0.25)
+        q = mixture(np.random.default_rng(7), nq, dims, 256, 0.25)
+    else:
+        m = rng.normal(size=(rows, dims)).astype(np.float32)
+        q = rng.normal(size=(nq, dims)).astype(np.float32)
+    index = NNdex(m, precision=precision)
+    base, qn, idx, sim = _check(index, m, q, k, f"{precision} {rows}x{dims}")
+    st = index.last_search_stats()
+    assert st["path"] == (2 if precision == "bf16" else 3)
+    assert st["rerank_width"] >= k
+    # The certificate's premise: every candidate's approximate score is within eps of exact.
+    cidx, capprox, eps = index.last_candidates(nq)
+    assert eps > 0
+    for i in range(min(nq, 32)):
+        exact = O.scores_f64(base, qn[i])[cidx[i].astype(np.int64)]
+        err = np.abs(exact - capprox[i].astype(np.float64))
+        # per-row bound ≥ the approximation error; allow the query's own residual
+        assert err.max() <= 2.5 * eps + 1e-3, (precision, err.max(), eps)
+
+
+def test_bf16_certifies_on_clustered_data():
+    rng = np.random.default_rng(3)
+    m = mixture(rng, 60_000, 256, 512, 0.25)
+    q = mixture(np.random.default_rng(4), 256, 256, 512, 0.25)
+    index = NNdex(m, precision="bf16")
+    _check(index, m, q, 10, "bf16 certify")
+    st = index.last_search_stats()
+    assert st["certified"] == 1, st
+
+
+def test_fallback_restores_exactness_when_certificate_fails():
+    # Random isotropic data packs scores tightly: certificates fail and the FP32 re-run must
+    # still return the exact top-k.
+    rng = np.random.default_rng(11)
+    m = rng.normal(size=(20_000, 64)).astype(np.float32)
+    q = rng.normal(size=(64, 64)).astype(np.float32)
+    index = NNdex(m, precision="fp8")
+    _check(index, m, q, 10, "fp8 fallback")
+
+
+def test_tc_matches_fp32_path():
+    # the exact rerank and the FP32 scan select the same rows; scores agree within the tolerance
+    rng = np.random.default_rng(5)
+    m = mixture(rng, 30_000, 128, 128, 0.25)
+    q = mixture(np.random.default_rng(6), 150, 128, 128, 0.25)
+    index = NNdex(m, precision="bf16")
+    ti, ts = index.search(q, k=10)
+    index.set_precision("fp32")
+    fi, fs = index.search(q, k=10)
+    assert np.array_equal(ti, fi)
+    assert np.max(np.abs(ts - fs)) <= 1e-5
+
+
+def test_tc_alone_equals_in_batch():
+    rng = np.random.default_rng(8)
+    m = mixture(rng, 40_000, 128, 128, 0.25)
+    q = mixture(np.random.default_rng(9), 200, 128, 128, 0.25)
+    index = NNdex(m, precision="bf16")
+    bi, bs = index.search(q, k=10)
+    for lo in (0, 70, 190):
+        si, ss = index.search(q[lo:lo + 5].copy(), k=10)
+        assert np.array_equal(si, bi[lo:lo + 5])
+        assert np.array_equal(ss, bs[lo:lo + 5])
