@@ -195,12 +195,13 @@ NNDEX_API int nndex_cuda_set_precision(nndex_cuda_index* index, uint32_t precisi
 /*
  * Candidates of the last low-precision search on this index (diagnostics and error reports):
  * for each of `query_rows` queries, the k' rows ranked by approximate (BF16/FP8) score, with those
- * approximate scores, and the bound eps the exactness certificate used for this index's copy
- * (max row residual). Host buffers of query_rows × k' entries; *kprime receives k'.
+ * approximate scores, the bound eps the exactness certificate used for this index's copy (max row
+ * residual) and, per query, whether its certificate held (0 = re-run on the FP32 scan). Host
+ * buffers of query_rows × k' entries (certified_out: query_rows); *kprime receives k'.
  */
 NNDEX_API int nndex_cuda_last_candidates(nndex_cuda_index* index, uint64_t query_rows, uint64_t* idx_out,
                                          float* approx_out, uint64_t capacity, uint32_t* kprime,
-                                         float* eps_rows);
+                                         float* eps_rows, uint32_t* certified_out);
 
 /* Status word of the last asynchronous device call on this index (0 when clean). */
 NNDEX_API int nndex_cuda_stream_status(nndex_cuda_index* index);

@@ -205,16 +205,17 @@ class NNdex:
         _check(_lib.lib().nndex_cuda_set_precision(self._h, _PRECISIONS[precision], int(rerank_width)))
 
     def last_candidates(self, query_rows: int):
-        """(rows, approximate scores, eps) of the last low-precision search's k′ candidates."""
+        """(rows, approximate scores, eps, certified) of the last low-precision search's k′ candidates."""
         kp = C.c_uint32(0)
         eps = C.c_float(0.0)
         st = self.last_search_stats()
         kk = int(st["rerank_width"])
         idx = np.zeros((query_rows, max(kk, 1)), dtype=np.uint64)
         sim = np.zeros((query_rows, max(kk, 1)), dtype=np.float32)
+        cert = np.zeros(query_rows, dtype=np.uint32)
         _check(_lib.lib().nndex_cuda_last_candidates(self._h, query_rows, idx.ctypes.data, sim.ctypes.data, idx.size,
-                                                     C.byref(kp), C.byref(eps)))
-        return idx[:, :kp.value], sim[:, :kp.value], float(eps.value)
+                                                     C.byref(kp), C.byref(eps), cert.ctypes.data))
+        return idx[:, :kp.value], sim[:, :kp.value], float(eps.value), cert.astype(bool)
 
     def last_search_stats(self) -> dict:
         s = _lib.SearchStats()

@@ -98,7 +98,7 @@ SIGNATURES = {
     "nndex_cuda_search_batch_device": (_i32, [_vp, _vp, _u64, _u64, _u64, _vp, _vp, _vp, _vp, _i32]),
     "nndex_cuda_stream_status": (_i32, [_vp]),
     "nndex_cuda_set_precision": (_i32, [_vp, _u32, _u32]),
-    "nndex_cuda_last_candidates": (_i32, [_vp, _u64, _vp, _vp, _u64, C.POINTER(_u32), C.POINTER(C.c_float)]),
+    "nndex_cuda_last_candidates": (_i32, [_vp, _u64, _vp, _vp, _u64, C.POINTER(_u32), C.POINTER(C.c_float), _vp]),
     "nndex_cuda_last_search_stats": (_i32, [_vp, C.POINTER(SearchStats)]),
     "nndex_cuda_kernel_launch_count": (_u64, []),
     "nndex_cuda_set_scan_timing": (_i32, [_vp, _i32]),

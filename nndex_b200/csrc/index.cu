@@ -178,6 +178,8 @@ CudaIndex::~CudaIndex() {
     cudaFreeHost(h_flags);
     cudaFree(d_base_bf16);
     cudaFree(d_base_fp8);
+    cudaFree(d_res16);
+    cudaFree(d_res8);
     cudaFree(d_row_scale);
     cudaFree(d_q_bf16);
     cudaFree(d_q_fp8);
@@ -189,6 +191,9 @@ CudaIndex::~CudaIndex() {
     cudaFree(d_cand_cnt);
     cudaFree(d_cert);
     cudaFree(d_qsub);
+    cudaFree(d_fb_idx);
+    cudaFree(d_fb_sim);
+    cudaFree(d_fb_cnt);
     cudaFreeHost(h_cert);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -288,10 +293,8 @@ int CudaIndex::check_device_words() {
 int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
     const bool has16 = d_base_bf16 != nullptr, has8 = d_base_fp8 != nullptr;
     auto tc_ok = [&](bool fp8) {
-        const uint64_t kb = fp8 ? kf8 : kb16;
-        const uint32_t nchunks = static_cast<uint32_t>(kb * (fp8 ? 1 : 2) / 128);
         const uint32_t kp = choose_kprime(kcap, fp8);
-        return kp >= kcap && kp > 0 && tc_smem_bytes(nchunks, kp) <= smem_optin;
+        return kp >= kcap && kp > 0;
     };
     switch (precision) {
         case NNDEX_PRECISION_FP32: return 1;
@@ -308,14 +311,23 @@ int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
     }
 }
 
+uint32_t CudaIndex::tc_chunks(bool fp8) const {
+    return static_cast<uint32_t>((fp8 ? kf8 : kb16 * 2) / 128);
+}
+
+// k′ for a batch: the tuned width for this k (widened after batches whose certificates failed),
+// capped by the largest per-query heap that fits in shared memory with at least 2 ring stages.
 uint32_t CudaIndex::choose_kprime(uint64_t kcap, bool fp8) const {
-    const uint64_t kb = fp8 ? kf8 : kb16;
-    const uint32_t nchunks = static_cast<uint32_t>(kb * (fp8 ? 1 : 2) / 128);
-    // Largest k′ whose per-query heaps fit next to the resident query block and the base ring.
+    const uint32_t nchunks = tc_chunks(fp8);
     uint32_t kmax = 0;
     for (uint32_t kp = 8; kp <= 256; kp += 8)
-        if (tc_smem_bytes(nchunks, kp) <= smem_optin) kmax = kp;
-    uint32_t kp = rerank_width ? rerank_width : static_cast<uint32_t>(std::max<uint64_t>(32, 3 * kcap));
+        if (tc_stages_for(nchunks, kp, fp8, smem_optin) != 0) kmax = kp;
+    uint32_t kp = rerank_width;
+    if (!kp) {
+        kp = static_cast<uint32_t>(std::max<uint64_t>(32, 3 * kcap));
+        auto it = tuned_kprime.find((fp8 ? 1ull << 40 : 0ull) | kcap);
+        if (it != tuned_kprime.end()) kp = std::max(kp, it->second);
+    }
     if (kp > kmax) kp = kmax;
     if (kp > rows) kp = static_cast<uint32_t>(rows);
     return kp;
@@ -363,7 +375,10 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     int st;
     const uint32_t kp = choose_kprime(kcap, fp8);
     const uint64_t kb = fp8 ? kf8 : kb16;
-    const uint32_t nchunks = static_cast<uint32_t>(kb * (fp8 ? 1 : 2) / 128);
+    const uint32_t nchunks = tc_chunks(fp8);
+    // Prefer the deepest ring; give it up for k′ room only when the heaps need it.
+    const uint32_t stages = tc_stages_for(nchunks, kp, fp8, smem_optin);
+    if (!stages) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k'=%u does not fit", kp);
     const uint32_t nqb = (n + 127) / 128;
     // Row ranges: about four waves of CTAs, each range a multiple of the 256-row tile.
     uint64_t nranges = (4ull * sm_count + nqb - 1) / nqb;
@@ -396,8 +411,13 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     a.range_rows = range_rows;
     a.nranges = static_cast<uint32_t>(nranges);
     a.kprime = kp;
+    a.stages = stages;
     a.row_scale = fp8 ? d_row_scale : nullptr;
     a.q_scale = fp8 ? d_q_scale : nullptr;
+    a.row_resid = fp8 ? d_res8 : d_res16;
+    a.q_resid = d_q_resid;
+    // FP32 accumulation of kb exact products (|Σ| ≤ 1 + ε): kb·2^-23, with a 4× margin.
+    a.eps_acc = 4.0f * static_cast<float>(kb) * 1.1920929e-07f;
     a.thr_global = d_thr;
     a.ws_keys = d_ws;
     a.status = d_status;
@@ -426,10 +446,6 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     r.nq = n;
     r.kp = kp;
     r.k = kcap;
-    r.q_resid = d_q_resid;
-    r.eps_rows = fp8 ? eps_fp8 : eps_bf16;
-    // FP32 accumulation of kb exact products (|Σ| ≤ 1 + ε): kb·2^-23, with a 4× margin.
-    r.eps_acc = 4.0f * static_cast<float>(kb) * 1.1920929e-07f;
     r.idx_out = o_idx;
     r.sim_out = o_sim;
     r.cnt_out = o_cnt;
@@ -453,32 +469,39 @@ int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_si
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(e, "search");
     if ((st = check_device_words())) return st;
+    last_tc_n = n;
     std::vector<uint32_t> failed;
     for (uint32_t i = 0; i < n; ++i)
         if (!h_cert[i]) failed.push_back(i);
     stats.certified = failed.empty() ? 1u : 0u;
     stats.widenings = static_cast<uint32_t>(failed.size());  // queries re-run on the FP32 path
+    // Autotune k′: when more than 1 % of a batch fails, the next batch at this k searches twice as
+    // many candidates (up to the shared-memory cap).
+    if (failed.size() * 100 > n && stats.rerank_width) {
+        const bool fp8 = stats.path == 3;
+        uint64_t key = (fp8 ? 1ull << 40 : 0ull) | kcap;
+        tuned_kprime[key] = std::min<uint32_t>(stats.rerank_width * 2, 256);
+    }
     if (failed.empty()) return NNDEX_OK;
     const uint32_t m = static_cast<uint32_t>(failed.size());
     if ((st = grow_device(d_qsub, cap_qsub, static_cast<uint64_t>(m) * ds, "fallback buffer"))) return st;
     for (uint32_t i = 0; i < m; ++i)
         cudaMemcpyAsync(d_qsub + static_cast<uint64_t>(i) * ds, d_qn + static_cast<uint64_t>(failed[i]) * ds,
                         ds * sizeof(float), cudaMemcpyDeviceToDevice, s);
-    // results of the re-run land in the candidate buffers, then move to their query's slots
-    if ((st = grow_device(d_cand_idx, cap_cand_idx, static_cast<uint64_t>(m) * kcap, "fallback buffer"))) return st;
-    if ((st = grow_device(d_cand_sim, cap_cand_sim, static_cast<uint64_t>(m) * kcap, "fallback buffer"))) return st;
-    if ((st = grow_device(d_cand_cnt, cap_cand_cnt, m, "fallback buffer"))) return st;
+    // results of the re-run land in the fallback buffers, then move to their query's slots
+    if ((st = grow_device(d_fb_idx, cap_fb_idx, static_cast<uint64_t>(m) * kcap, "fallback buffer"))) return st;
+    if ((st = grow_device(d_fb_sim, cap_fb_sim, static_cast<uint64_t>(m) * kcap, "fallback buffer"))) return st;
+    if ((st = grow_device(d_fb_cnt, cap_fb_cnt, m, "fallback buffer"))) return st;
     const uint32_t path = stats.path;
-    if ((st = enqueue_exact_fp32(d_qsub, m, kcap, kcap, d_cand_idx, d_cand_sim, d_cand_cnt, s))) return st;
+    if ((st = enqueue_exact_fp32(d_qsub, m, kcap, kcap, d_fb_idx, d_fb_sim, d_fb_cnt, s))) return st;
     stats.path = path;
     for (uint32_t i = 0; i < m; ++i) {
         const uint64_t q = failed[i];
-        cudaMemcpyAsync(o_idx + q * kcap, d_cand_idx + static_cast<uint64_t>(i) * kcap, kcap * sizeof(uint64_t),
+        cudaMemcpyAsync(o_idx + q * kcap, d_fb_idx + static_cast<uint64_t>(i) * kcap, kcap * sizeof(uint64_t),
                         cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(o_sim + q * kcap, d_cand_sim + static_cast<uint64_t>(i) * kcap, kcap * sizeof(float),
+        cudaMemcpyAsync(o_sim + q * kcap, d_fb_sim + static_cast<uint64_t>(i) * kcap, kcap * sizeof(float),
                         cudaMemcpyDeviceToDevice, s);
-        if (o_cnt)
-            cudaMemcpyAsync(o_cnt + q, d_cand_cnt + i, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+        if (o_cnt) cudaMemcpyAsync(o_cnt + q, d_fb_cnt + i, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     }
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(e, "search");
@@ -661,13 +684,12 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
     cudaMemsetAsync(ix->d_base + rows * ix->ds, 0, (ix->rows_alloc - rows) * ix->ds * sizeof(float), ix->stream);
     cudaMemsetAsync(ix->d_err, 0xFF, sizeof(unsigned long long), ix->stream);
     // Low-precision scoring copies (K1 writes them in the same pass) and their residual norms.
-    float* d_res16 = nullptr;
-    float* d_res8 = nullptr;
+    float*& d_res16 = ix->d_res16;  // kept: the certificate's per-row bounds
+    float*& d_res8 = ix->d_res8;
     unsigned int* d_max = nullptr;
     auto free_tmp = [&]() {
-        cudaFree(d_res16);
-        cudaFree(d_res8);
         cudaFree(d_max);
+        d_max = nullptr;
     };
     if (flags & NNDEX_FLAG_BF16) {
         ix->kb16 = (dims + 63) / 64 * 64;
@@ -991,7 +1013,7 @@ int nndex_cuda_set_precision(nndex_cuda_index* index, uint32_t precision, uint32
 }
 
 int nndex_cuda_last_candidates(nndex_cuda_index* index, uint64_t query_rows, uint64_t* idx_out, float* approx_out,
-                               uint64_t capacity, uint32_t* kprime, float* eps_rows) {
+                               uint64_t capacity, uint32_t* kprime, float* eps_rows, uint32_t* certified_out) {
     clear_error();
     if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
     CudaIndex* ix = index->impl;
@@ -1007,6 +1029,11 @@ int nndex_cuda_last_candidates(nndex_cuda_index* index, uint64_t query_rows, uin
     cudaError_t e = cudaStreamSynchronize(ix->stream);
     if (e == cudaSuccess && idx_out) e = cudaMemcpy(idx_out, ix->d_cand_idx, n * sizeof(uint64_t), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && approx_out) e = cudaMemcpy(approx_out, ix->d_cand_sim, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && certified_out) {
+        if (query_rows > ix->last_tc_n)
+            return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: more rows than the last batch");
+        std::memcpy(certified_out, ix->h_cert, query_rows * sizeof(uint32_t));
+    }
     if (e != cudaSuccess) return cuda_error(e, "candidates");
     return NNDEX_OK;
 }

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <mutex>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -46,6 +47,8 @@ struct CudaIndex {
     uint8_t* d_base_fp8 = nullptr;             // rows_alloc × kf8 (E4M3)
     float* d_row_scale = nullptr;              // rows_alloc: FP8 dequantisation scale per row
     float eps_bf16 = 0.0f, eps_fp8 = 0.0f;     // max row residual norm ‖x − x̂‖
+    float* d_res16 = nullptr;                  // rows: ‖x − x̂‖ of the BF16 copy
+    float* d_res8 = nullptr;                   // rows: ‖x − x̂‖ of the FP8 copy
     CUtensorMap tmap_bf16{}, tmap_fp8{};
     // per-search buffers of the tensor-core path
     __nv_bfloat16* d_q_bf16 = nullptr;
@@ -70,7 +73,15 @@ struct CudaIndex {
     size_t cap_hcert = 0;
     float* d_qsub = nullptr;  // FP32 queries re-run after a failed certificate
     size_t cap_qsub = 0;
+    uint64_t* d_fb_idx = nullptr;  // their FP32 results before they move to the query's slots
+    size_t cap_fb_idx = 0;
+    float* d_fb_sim = nullptr;
+    size_t cap_fb_sim = 0;
+    uint32_t* d_fb_cnt = nullptr;
+    size_t cap_fb_cnt = 0;
+    uint32_t last_tc_n = 0;  // queries of the last tensor-core batch (diagnostics)
     uint32_t rerank_width = 0;  // k′ override (0 = autotuned)
+    std::unordered_map<uint64_t, uint32_t> tuned_kprime;  // (precision, k) → widened k′
 
     // per-search buffers (grown on demand)
     float* d_qraw = nullptr;
@@ -120,6 +131,7 @@ struct CudaIndex {
     // Path choice for a batch: 1 = FP32 scan, 2 = BF16 tensor-core scan, 3 = FP8 tensor-core scan.
     int choose_path(uint64_t nq, uint64_t kcap) const;
     uint32_t choose_kprime(uint64_t kcap, bool fp8) const;
+    uint32_t tc_chunks(bool fp8) const;
     int enqueue_prep_queries(const float* d_raw, uint64_t n, int mode, int path, cudaStream_t s);
     int enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
                    cudaStream_t s);

@@ -83,13 +83,19 @@ struct TcArgs {
     uint64_t range_rows = 0;              // rows per CTA range (multiple of 256)
     uint32_t nranges = 0;
     uint32_t kprime = 0;
+    uint32_t stages = 4;                  // base ring depth (2..4)
     const float* row_scale = nullptr;     // FP8 only
     const float* q_scale = nullptr;       // FP8 only
+    const float* row_resid = nullptr;     // ‖x − x̂‖ per row
+    const float* q_resid = nullptr;       // ‖q − q̂‖ per query
+    float eps_acc = 0.0f;                 // FP32 accumulation error bound
     unsigned long long* thr_global = nullptr;  // per query, zeroed before the launch
     uint64_t* ws_keys = nullptr;          // nq × nranges × kprime
     uint32_t* status = nullptr;
 };
-size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime);
+size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8);
+// Deepest base ring (4, 3 or 2 stages) that fits k′ heaps in `smem_limit`; 0 if none fits.
+uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, size_t smem_limit);
 cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, cudaStream_t stream);
 
 struct RerankArgs {
@@ -97,11 +103,9 @@ struct RerankArgs {
     uint32_t ds = 0;
     const float* queries = nullptr;  // FP32 normalised queries, stride ds
     const uint64_t* cand_idx = nullptr;  // nq × kp, sorted by approximate score
-    const float* cand_sim = nullptr;
+    const float* cand_sim = nullptr;     // upper bounds of the exact scores, sorted descending
     const uint32_t* cand_cnt = nullptr;
     uint32_t nq = 0, kp = 0, k = 0;
-    const float* q_resid = nullptr;
-    float eps_rows = 0.0f, eps_acc = 0.0f;
     uint64_t* idx_out = nullptr;
     float* sim_out = nullptr;
     uint32_t* cnt_out = nullptr;

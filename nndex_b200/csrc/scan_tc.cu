@@ -32,7 +32,6 @@ namespace nndex {
 namespace {
 constexpr int kM = 128;               // queries per CTA (TMEM lanes)
 constexpr int kN = 256;               // base rows per tile (MMA N)
-constexpr int kST = 4;                // ring depth for base slabs
 constexpr uint32_t kAChunk = kM * 128;
 constexpr uint32_t kBChunk = kN * 128;
 constexpr int kThreads = 192;         // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
@@ -44,21 +43,28 @@ NNDEX_DEVICE_INLINE uint8_t* align_1024(uint8_t* p) {
 }
 }  // namespace
 
-size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime) {
+size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8) {
     size_t b = 1024;
     b += static_cast<size_t>(nchunks) * kAChunk;
-    b += static_cast<size_t>(kST) * kBChunk;
+    b += static_cast<size_t>(stages) * kBChunk;
     b += static_cast<size_t>(kprime) * kM * 8;
-    b += 2 * kN * 4;
-    b += (2 * kST + 5) * 8 + 16;
+    b += 4 * kN * 4;
+    b += (2 * stages + 5) * 8 + 16;
     return b;
 }
 
-template <bool kFp8>
+uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, size_t smem_limit) {
+    for (uint32_t st = 4; st >= 2; --st)
+        if (tc_smem_bytes(nchunks, kprime, st, fp8) <= smem_limit) return st;
+    return 0;
+}
+
+template <bool kFp8, int kST>
 __global__ void __launch_bounds__(kThreads, 1)
     scan_tc_kernel(const __grid_constant__ CUtensorMap tmap_q, const __grid_constant__ CUtensorMap tmap_b,
                    uint32_t nq, uint32_t nchunks, uint64_t rows, uint64_t range_rows, uint32_t kprime,
                    const float* __restrict__ row_scale, const float* __restrict__ q_scale,
+                   const float* __restrict__ row_resid, const float* __restrict__ q_resid, float eps_acc,
                    unsigned long long* __restrict__ thr_global, uint64_t* __restrict__ ws_keys,
                    uint32_t* __restrict__ status) {
     constexpr uint32_t kElems = kFp8 ? 128 : 64;  // K elements per 128-byte slab
@@ -67,8 +73,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint8_t* a_smem = smem;
     uint8_t* b_smem = a_smem + static_cast<size_t>(nchunks) * kAChunk;
     uint64_t* heap = reinterpret_cast<uint64_t*>(b_smem + static_cast<size_t>(kST) * kBChunk);
-    float* scale_s = reinterpret_cast<float*>(heap + static_cast<size_t>(kprime) * kM);
-    uint64_t* full_bar = reinterpret_cast<uint64_t*>(scale_s + 2 * kN);
+    // Per-tile row data, double-buffered by tile parity: [parity][residual bound | FP8 scale][256].
+    float* rowinfo = reinterpret_cast<float*>(heap + static_cast<size_t>(kprime) * kM);
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(rowinfo + 4 * kN);
     uint64_t* empty_bar = full_bar + kST;
     uint64_t* a_full = empty_bar + kST;
     uint64_t* tfull = a_full + 1;
@@ -110,7 +117,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) {
             tma_prefetch_desc(&tmap_q);
             tma_prefetch_desc(&tmap_b);
-            const uint64_t policy = l2_policy_evict_first();
+            // Base tiles are read by every query block of the same row range at about the same
+            // time: keep them in L2 with the default policy (no evict-first hint).
             mbar_arrive_expect_tx(a_full, nchunks * kAChunk);
             for (uint32_t c = 0; c < nchunks; ++c)
                 tma_load_2d(a_smem + static_cast<size_t>(c) * kAChunk, &tmap_q, a_full, static_cast<int32_t>(c * kElems),
@@ -120,7 +128,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (uint32_t t = 0; t < ntiles && !stop; ++t) {
                 const int32_t y = static_cast<int32_t>(row_begin + static_cast<uint64_t>(t) * kN);
                 for (uint32_t c = 0; c < nchunks; ++c) {
-                    const uint32_t s = it & (kST - 1), u = it / kST;
+                    const uint32_t s = it % kST, u = it / kST;
                     if (u > 0 && !mbar_wait_bounded(&empty_bar[s], (u - 1) & 1u, kWaitBudgetCycles)) {
                         *abort_flag = 1;
                         record_status(status, kStatusTimeout);
@@ -132,8 +140,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     mbar_arrive_expect_tx(&full_bar[s], kBChunk);
-                    tma_load_2d_hint(b_smem + static_cast<size_t>(s) * kBChunk, &tmap_b, &full_bar[s],
-                                     static_cast<int32_t>(c * kElems), y, policy);
+                    tma_load_2d(b_smem + static_cast<size_t>(s) * kBChunk, &tmap_b, &full_bar[s],
+                                static_cast<int32_t>(c * kElems), y);
                     ++it;
                 }
             }
@@ -166,7 +174,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc::fence_after_sync();
                 const uint32_t d = tmem_base + buf * kN;
                 for (uint32_t c = 0; c < nchunks; ++c, ++it) {
-                    const uint32_t s = it & (kST - 1), u = it / kST;
+                    const uint32_t s = it % kST, u = it / kST;
                     if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], u & 1u, kWaitBudgetCycles)) {
                         *abort_flag = 1;
                         record_status(status, kStatusTimeout);
@@ -193,14 +201,22 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t et = threadIdx.x - 64;  // 0..127
         unsigned long long thr_key = valid_q ? thr_global[q] : ~0ull;
         const float qs = (kFp8 && valid_q) ? q_scale[q] : 1.0f;
+        // Candidates are ranked by an upper bound of the exact score: for row r,
+        //   s_r ≤ s̃_r + ‖δx_r‖(1 + ‖δq‖) + ‖δq‖ + ε_acc   (Cauchy–Schwarz on q·δx + δq·x̂, ‖q‖ = 1),
+        // so every row outside the final k′ has an exact score ≤ the k′-th bound.
+        const float rq = valid_q ? q_resid[q] : 0.0f;
+        const float b_mul = 1.0f + rq, b_add = rq + eps_acc;
         uint32_t n = 0;
         for (uint32_t t = 0; t < ntiles; ++t) {
             const uint32_t buf = t & 1u, ub = t >> 1;
             const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * kN;
-            if (kFp8) {
-                float* sc = scale_s + (t & 1u) * kN;
-                for (uint32_t j = et; j < static_cast<uint32_t>(kN); j += 128)
-                    sc[j] = (tile_row0 + j < row_end) ? row_scale[tile_row0 + j] * qs : 0.0f;
+            {
+                float* ri = rowinfo + (t & 1u) * 2 * kN;
+                for (uint32_t j = et; j < static_cast<uint32_t>(kN); j += 128) {
+                    const bool in = tile_row0 + j < row_end;
+                    ri[j] = in ? row_resid[tile_row0 + j] : 0.0f;
+                    if (kFp8) ri[kN + j] = in ? row_scale[tile_row0 + j] : 0.0f;
+                }
                 named_bar_sync(2, 128);
             }
             if (!*abort_flag && !mbar_wait_bounded(&tfull[buf], ub & 1u, kWaitBudgetCycles)) {
@@ -213,7 +229,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (g > thr_key) thr_key = g;
             }
             float thr_f = thr_key ? key_score(thr_key) : -INFINITY;
-            const float* sc = scale_s + (t & 1u) * kN;
+            const float* ri = rowinfo + (t & 1u) * 2 * kN;
 #pragma unroll 1
             for (uint32_t c = 0; c < kN / 32; ++c) {
                 uint32_t v[32];
@@ -223,10 +239,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     float s = __uint_as_float(v[j]);
-                    if (kFp8) s *= sc[c * 32 + j];
+                    if (kFp8) s = (s * ri[kN + c * 32 + j]) * qs;
+                    const float ub_s = fmaf(ri[c * 32 + j], b_mul, s + b_add);
                     const uint64_t row = tile_row0 + c * 32 + j;
-                    if (s >= thr_f && row < row_end) {
-                        const uint64_t key = make_key(s, static_cast<uint32_t>(row));
+                    if (ub_s >= thr_f && row < row_end) {
+                        const uint64_t key = make_key(ub_s, static_cast<uint32_t>(row));
                         if (key > thr_key) {
                             // min-heap insert (index-major layout: heap[i * 128 + lrow])
                             if (n < kprime) {
@@ -291,32 +308,49 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // ------------------------------------------------------------------------------------------
 // K4: exact FP32 rerank of the k′ candidates + top-k + certificate. One block per query.
+//
+// Each candidate's FP32 dot product is computed in exactly the order of the FP32 scan
+// (scan_fp32.cu): eight chains, one per 16-byte chunk position ch of each 128-byte slab, each
+// accumulating its chunk's four products slab by slab with FMA; then ((c0+c1)+(c2+c3)) +
+// ((c4+c5)+(c6+c7)). So a query's scores are bit-identical whichever path scored it.
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
     rerank_kernel(const float* __restrict__ base, uint32_t ds, const float* __restrict__ queries,
-                  const uint64_t* __restrict__ cand_idx, const float* __restrict__ cand_sim,
-                  const uint32_t* __restrict__ cand_cnt, uint32_t kp, uint32_t k, const float* __restrict__ q_resid,
-                  float eps_rows, float eps_acc, uint64_t* __restrict__ idx_out, float* __restrict__ sim_out,
-                  uint32_t* __restrict__ cnt_out, uint32_t* __restrict__ cert_out) {
+                  const uint64_t* __restrict__ cand_idx, const float* __restrict__ cand_bound,
+                  const uint32_t* __restrict__ cand_cnt, uint32_t kp, uint32_t k, uint64_t* __restrict__ idx_out,
+                  float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out, uint32_t* __restrict__ cert_out) {
     extern __shared__ uint64_t keys[];
     const uint32_t q = blockIdx.x;
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t ch = lane & 7u, slot = threadIdx.x >> 3;  // 8 lanes per candidate
+    const uint32_t nslots = blockDim.x >> 3;
     const uint32_t n = cand_cnt[q] < kp ? cand_cnt[q] : kp;
     uint32_t p2 = 1;
     while (p2 < kp) p2 <<= 1;
     const float* qv = queries + static_cast<size_t>(q) * ds;
-    for (uint32_t j = warp; j < p2; j += nw) {
-        uint64_t key = 0;
-        if (j < n) {
-            const uint64_t row = cand_idx[static_cast<size_t>(q) * kp + j];
-            const float* x = base + row * ds;
-            float acc = 0.0f;
-            for (uint32_t d = lane; d < ds; d += 32) acc = fmaf(x[d], qv[d], acc);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            key = make_key(acc, static_cast<uint32_t>(row));
+    const uint32_t nbox = ds / 32;
+    for (uint32_t j0 = 0; j0 < p2; j0 += nslots) {
+        const uint32_t j = j0 + slot;
+        const bool live = j < n;
+        float acc = 0.0f;
+        uint64_t row = 0;
+        if (live) {
+            row = cand_idx[static_cast<size_t>(q) * kp + j];
+            const float* x = base + row * ds + ch * 4;
+            const float* y = qv + ch * 4;
+            for (uint32_t bx = 0; bx < nbox; ++bx) {
+                const float4 a = *reinterpret_cast<const float4*>(x + bx * 32);
+                const float4 b = *reinterpret_cast<const float4*>(y + bx * 32);
+                acc = fmaf(a.x, b.x, acc);
+                acc = fmaf(a.y, b.y, acc);
+                acc = fmaf(a.z, b.z, acc);
+                acc = fmaf(a.w, b.w, acc);
+            }
         }
-        if (lane == 0) keys[j] = key;
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+        if (ch == 0 && j < p2) keys[j] = live ? make_key(acc, static_cast<uint32_t>(row)) : 0ull;
     }
     __syncthreads();
     block_bitonic_sort_desc(keys, p2);
@@ -327,15 +361,10 @@ __global__ void __launch_bounds__(256)
     }
     if (threadIdx.x == 0) {
         if (cnt_out) cnt_out[q] = kk;
-        // Every row outside the candidate set has an approximate score <= the k′-th candidate's,
-        // so its exact score is <= tau + eps. Exact k-th above that bound => the top-k is exact.
+        // Every row outside the k′ candidates has an exact score ≤ the k′-th upper bound; an exact
+        // k-th score above it proves the top-k exact.
         uint32_t ok = 1;
-        if (n >= kp && kk > 0) {
-            const float tau = cand_sim[static_cast<size_t>(q) * kp + kp - 1];
-            const float rq = q_resid ? q_resid[q] : 0.0f;
-            const float eps = eps_rows + rq * (1.0f + eps_rows) + eps_acc;
-            ok = key_score(keys[kk - 1]) > tau + eps ? 1u : 0u;
-        }
+        if (n >= kp && kk > 0) ok = key_score(keys[kk - 1]) > cand_bound[static_cast<size_t>(q) * kp + kp - 1] ? 1u : 0u;
         cert_out[q] = ok;
     }
 }
@@ -343,29 +372,40 @@ __global__ void __launch_bounds__(256)
 // ------------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------------
-template <bool kFp8>
+template <bool kFp8, int kST>
 static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
-    auto kern = scan_tc_kernel<kFp8>;
-    const size_t smem = tc_smem_bytes(a.nchunks, a.kprime);
+    auto kern = scan_tc_kernel<kFp8, kST>;
+    const size_t smem = tc_smem_bytes(a.nchunks, a.kprime, kST, kFp8);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     dim3 grid((a.nq + kM - 1) / kM, a.nranges);
     kern<<<grid, kThreads, smem, stream>>>(*a.tmap_q, *a.tmap_b, a.nq, a.nchunks, a.rows, a.range_rows, a.kprime,
-                                            a.row_scale, a.q_scale, a.thr_global, a.ws_keys, a.status);
+                                            a.row_scale, a.q_scale, a.row_resid, a.q_resid, a.eps_acc, a.thr_global,
+                                            a.ws_keys, a.status);
     count_launch();
     return cudaGetLastError();
 }
 
+template <bool kFp8>
+static cudaError_t launch_tc_stages(const TcArgs& a, cudaStream_t stream) {
+    switch (a.stages) {
+        case 4: return launch_tc_impl<kFp8, 4>(a, stream);
+        case 3: return launch_tc_impl<kFp8, 3>(a, stream);
+        case 2: return launch_tc_impl<kFp8, 2>(a, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, cudaStream_t stream) {
-    return fp8 ? launch_tc_impl<true>(a, stream) : launch_tc_impl<false>(a, stream);
+    return fp8 ? launch_tc_stages<true>(a, stream) : launch_tc_stages<false>(a, stream);
 }
 
 cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream) {
     uint32_t p2 = 1;
     while (p2 < a.kp) p2 <<= 1;
-    rerank_kernel<<<a.nq, 256, p2 * sizeof(uint64_t), stream>>>(
-        a.base, a.ds, a.queries, a.cand_idx, a.cand_sim, a.cand_cnt, a.kp, a.k, a.q_resid, a.eps_rows, a.eps_acc,
-        a.idx_out, a.sim_out, a.cnt_out, a.cert_out);
+    rerank_kernel<<<a.nq, 256, p2 * sizeof(uint64_t), stream>>>(a.base, a.ds, a.queries, a.cand_idx, a.cand_sim,
+                                                               a.cand_cnt, a.kp, a.k, a.idx_out, a.sim_out,
+                                                               a.cnt_out, a.cert_out);
     count_launch();
     return cudaGetLastError();
 }
