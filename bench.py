@@ -55,6 +55,16 @@ def parse_args(argv=None):
     p.add_argument("--extra-batches", default="1,4", help="batch sizes reported beside the headline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-batches", type=int, default=2)
+    p.add_argument("--mixed", choices=["on", "off", "only"], default="on",
+                   help="also measure the mixed-precision workload (BF16/FP8 scan + FP32 rerank vs FP32)")
+    p.add_argument("--mixed-rows", type=int, default=10_000_000)
+    p.add_argument("--mixed-dims", type=int, default=256)
+    p.add_argument("--mixed-centers", type=int, default=4096)
+    p.add_argument("--mixed-sigma", type=float, default=0.25)
+    p.add_argument("--mixed-batch", type=int, default=4096)
+    p.add_argument("--mixed-k", type=int, default=10)
+    p.add_argument("--mixed-steps", type=int, default=5)
+    p.add_argument("--mixed-oracle-queries", type=int, default=32)
     return p.parse_args(argv)
 
 
@@ -346,6 +356,9 @@ def run_ours(args):
                          f"(oracle restatement of src/cpu.rs Gemm strategy, {threads} threads)"}
 
     L.nndex_cuda_destroy(h)
+    del qall
+    torch.cuda.empty_cache()
+    mixed = run_mixed(args, dev, L, world) if args.mixed != "off" else None
     if rank != 0:
         return None
     head = results[args.batch]
@@ -382,6 +395,7 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
+        "mixed_precision": mixed,
         "batches": {str(bb): {"queries_per_s": r["queries_per_s"], "ms_per_step": r["ms_per_step"],
                               "scan_ms": r["scan_ms"],
                               "hbm_gbs": (args.rows * args.dims * 4 + bb * args.dims * 4 + bb * k * 12)
@@ -389,6 +403,128 @@ def run_ours(args):
                     for bb, r in results.items()},
     }
     return line
+
+
+# ---------------------------------------------------------------------------------------------
+# mixed-precision workload: BF16 / FP8 tensor-core scan + FP32 rerank vs the FP32 scan
+# ---------------------------------------------------------------------------------------------
+
+def fp64_topk(base, queries, k, chunk_rows=1 << 20):
+    """FP64 ground truth (verification only): top-k rows by float64 dot product, ties → lower row."""
+    import torch
+    qd = queries.double()
+    best_s = None
+    best_i = None
+    for r0 in range(0, base.shape[0], chunk_rows):
+        s = qd @ base[r0:r0 + chunk_rows].double().T
+        v, i = torch.topk(s, min(k + 1, s.shape[1]), dim=1)
+        i = i + r0
+        if best_s is None:
+            best_s, best_i = v, i
+        else:
+            cs = torch.cat([best_s, v], 1)
+            ci = torch.cat([best_i, i], 1)
+            v2, j = torch.topk(cs, k + 1, dim=1)
+            best_s, best_i = v2, torch.gather(ci, 1, j)
+    return best_i[:, :k], best_s
+
+
+def run_mixed(args, dev, L, world):
+    import torch
+    from nndex_b200 import _lib, kernel_launch_count
+    from nndex_b200._lib import (NNDEX_FLAG_BF16, NNDEX_FLAG_FP8, NNDEX_FLAG_NORMALIZED, NNDEX_PRECISION_BF16,
+                                 NNDEX_PRECISION_FP32, NNDEX_PRECISION_FP8)
+    rank, _, local = dist_env()
+    seed = replica_seed(args.seed + 100, rank)
+    rows, dims, nq, k = args.mixed_rows, args.mixed_dims, args.mixed_batch, args.mixed_k
+    base = make_mixture(rows, dims, args.mixed_centers, args.mixed_sigma, seed, dev, center_seed=args.seed + 100)
+    opts = _lib.Opts()
+    opts.device = local
+    h = C.c_void_p()
+    flags = NNDEX_FLAG_NORMALIZED | NNDEX_FLAG_BF16 | NNDEX_FLAG_FP8
+    st = L.nndex_cuda_create_from_device(base.data_ptr(), base.numel(), rows, dims, flags, C.byref(opts), C.byref(h))
+    if st != 0:
+        raise RuntimeError(_lib.last_error())
+    q = make_mixture(nq, dims, args.mixed_centers, args.mixed_sigma, seed + 7, dev, center_seed=args.seed + 100)
+    stream = torch.cuda.current_stream(dev)
+    sptr = C.c_void_p(stream.cuda_stream)
+    oi = torch.empty((nq, k), dtype=torch.int64, device=dev)
+    os_ = torch.empty((nq, k), dtype=torch.float32, device=dev)
+    stats = _lib.SearchStats()
+    out = {}
+    sample = min(args.mixed_oracle_queries, nq)
+    ref_i, ref_s = fp64_topk(base, q[:sample], k)
+    for name, prec in (("fp32", NNDEX_PRECISION_FP32), ("bf16", NNDEX_PRECISION_BF16), ("fp8", NNDEX_PRECISION_FP8)):
+        L.nndex_cuda_set_precision(h, prec, 0)
+        steps = max(1, min(args.mixed_steps, 2 if name == "fp32" else args.mixed_steps))
+        for _ in range(2):  # warm-up (the second also runs with the autotuned k′)
+            if L.nndex_cuda_search_batch_device(h, q.data_ptr(), nq, dims, k, oi.data_ptr(), os_.data_ptr(), None,
+                                                sptr, 1) != 0:
+                raise RuntimeError(_lib.last_error())
+        torch.cuda.synchronize(dev)
+        L.nndex_cuda_set_scan_timing(h, 1)
+        barrier(world)
+        n0 = kernel_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fallbacks = 0
+        for _ in range(steps):
+            if L.nndex_cuda_search_batch_device(h, q.data_ptr(), nq, dims, k, oi.data_ptr(), os_.data_ptr(), None,
+                                                sptr, 1) != 0:
+                raise RuntimeError(_lib.last_error())
+            L.nndex_cuda_last_search_stats(h, C.byref(stats))
+            fallbacks += stats.widenings if stats.path in (2, 3) else 0
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        n1 = kernel_launch_count()
+        L.nndex_cuda_set_scan_timing(h, 0)
+        ms = e0.elapsed_time(e1)
+        scan_ms = C.c_double(0.0)
+        scan_n = C.c_uint64(0)
+        L.nndex_cuda_scan_timing(h, C.byref(scan_ms), C.byref(scan_n))
+        max_ms, total_q = aggregate(ms, nq * steps, world, dev)
+        got = oi[:sample]
+        hits = sum(len(set(got[i].tolist()) & set(ref_i[i].tolist())) for i in range(sample))
+        # score error of the returned results against the FP64 oracle
+        ps = (q[:sample].double().unsqueeze(1) * base[got].double()).sum(-1)
+        err = (os_[:sample].double() - ps).abs().max().item()
+        scan_avg = scan_ms.value / max(scan_n.value, 1)
+        flops = 2.0 * rows * dims * nq
+        out[name] = {
+            "queries_per_s": total_q / (max_ms / 1e3),
+            "ms_per_batch": max_ms / steps,
+            "scan_ms": scan_avg,
+            "scan_tflops": flops / (scan_avg / 1e3) / 1e12,
+            "recall_at_k_vs_fp64": hits / (sample * k),
+            "max_score_error_vs_fp64": err,
+            "rerank_width": int(stats.rerank_width),
+            "fallback_queries_per_batch": fallbacks / steps,
+            "kernel_launches_per_batch": (n1 - n0) / steps,
+        }
+    L.nndex_cuda_destroy(h)
+    del base
+    torch.cuda.empty_cache()
+    fp32 = out["fp32"]["queries_per_s"]
+    for name in ("bf16", "fp8"):
+        out[name]["speedup_vs_fp32"] = out[name]["queries_per_s"] / fp32
+    bf16_peak = measured_bf16_peak()
+    return {
+        "workload": f"exact top-{k}, base {rows}x{dims} ({args.mixed_centers}-centre Gaussian mixture, "
+                    f"sigma={args.mixed_sigma}, unit rows), batch {nq}; BF16/FP8 tensor-core scan + FP32 rerank "
+                    f"vs the FP32 scan; recall on {sample} queries vs a float64 brute force",
+        "results": out,
+        "roofline": {"bound": "tensor", "achieved_bf16_tflops": out["bf16"]["scan_tflops"],
+                     "peak_bf16_tflops": bf16_peak[0], "frac_bf16": out["bf16"]["scan_tflops"] / bf16_peak[0],
+                     "peak_kind": bf16_peak[1], "flops_per_batch": 2.0 * rows * dims * nq},
+    }
+
+
+def measured_bf16_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["bf16_tflops"]), "measured bf16_tflops (burst)"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
 
 
 # ---------------------------------------------------------------------------------------------

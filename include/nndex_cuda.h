@@ -138,7 +138,8 @@ NNDEX_API int nndex_cuda_create(const float* host_matrix, uint64_t n_values, uin
                       uint32_t flags, const nndex_cuda_opts* opts, nndex_cuda_index** out);
 
 /* Same as nndex_cuda_create, but the raw matrix already lives in device memory on the
- * selected device (no host copy). */
+ * selected device (no host copy). The call first waits for all work on the device, so the matrix
+ * may still be in the making on any stream when it is called. */
 NNDEX_API int nndex_cuda_create_from_device(const float* device_matrix, uint64_t n_values, uint64_t rows,
                                   uint64_t dims, uint32_t flags, const nndex_cuda_opts* opts,
                                   nndex_cuda_index** out);
@@ -173,8 +174,9 @@ NNDEX_API int nndex_cuda_search_batch(nndex_cuda_index* index, const float* host
 
 /*
  * Device-resident variant of nndex_cuda_search_batch: queries and outputs are device pointers
- * on the index's device, the work is enqueued on `stream` (a cudaStream_t, NULL = the index's
- * own stream) and the call returns once it is enqueued when `synchronize` is 0. Query
+ * on the index's device, the work is enqueued on `stream` (a cudaStream_t, NULL = the legacy
+ * default stream) after any earlier call's work on this index, and the call returns once it is
+ * enqueued when `synchronize` is 0. Query
  * validation (finite, zero-norm) is reported through the returned status only when
  * `synchronize` is 1; otherwise through nndex_cuda_stream_status after the stream drains.
  */

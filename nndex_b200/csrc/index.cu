@@ -195,6 +195,7 @@ CudaIndex::~CudaIndex() {
     cudaFree(d_fb_sim);
     cudaFree(d_fb_cnt);
     cudaFreeHost(h_cert);
+    if (done_ev) cudaEventDestroy(done_ev);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -513,6 +514,7 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
     std::lock_guard<std::mutex> lock(mu);
     cudaSetDevice(device);
     stats = nndex_cuda_search_stats{};
+    order_after_previous(stream);
     const uint64_t kcap = std::min<uint64_t>(k, rows);
     if (kcap > kMaxFusedK)
         return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k=%llu above the fused top-k limit %u",
@@ -556,6 +558,7 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
             for (uint64_t i = 0; i < n; ++i) counts_out[q0 + i] = h_cnt[i];
     }
     cudaEventRecord(ev1, stream);
+    mark_done(stream);
     cudaEventSynchronize(ev1);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ev0, ev1);
@@ -568,7 +571,8 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
     std::lock_guard<std::mutex> lock(mu);
     cudaSetDevice(device);
     stats = nndex_cuda_search_stats{};
-    if (!s) s = stream;
+    if (!s) s = cudaStreamLegacy;
+    order_after_previous(s);
     const uint64_t kcap = std::min<uint64_t>(k, rows);
     int st;
     if ((st = ensure_query_capacity(std::min<uint64_t>(nq, kMaxBatchChunk)))) return st;
@@ -598,11 +602,24 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
         h_flags[1] = 0;
         cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        mark_done(s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_error(e, "search");
         return check_device_words();
     }
+    mark_done(s);
     return NNDEX_OK;
+}
+
+// The index's scratch buffers are shared by every call: work enqueued on one stream must not
+// overlap work of an earlier call on another stream.
+void CudaIndex::order_after_previous(cudaStream_t s) {
+    if (done_ev && done_stream && done_stream != s) cudaStreamWaitEvent(s, done_ev, 0);
+}
+void CudaIndex::mark_done(cudaStream_t s) {
+    if (!done_ev) cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming);
+    cudaEventRecord(done_ev, s);
+    done_stream = s;
 }
 
 int CudaIndex::stream_status() {
@@ -728,6 +745,11 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
     // K1: upload in chunks (≈256 MB of raw rows each), validate + normalise + pad on the device.
     const int mode = ix->normalized ? 2 : 0;
     if (on_device) {
+        // The caller may still be writing the matrix on any stream: wait for the device first.
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
+            free_tmp();
+            return fail(cuda_error(e, "cudaDeviceSynchronize"));
+        }
         PrepArgs p;
         p.src = matrix;
         p.rows = rows;

@@ -34,6 +34,8 @@ struct CudaIndex {
 
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t done_ev = nullptr;        // completion of the last call's device work
+    cudaStream_t done_stream = nullptr;   // the stream it ran on
     std::mutex mu;
 
     float* d_base = nullptr;  // rows_alloc × ds FP32, normalised, zero padded
@@ -139,6 +141,8 @@ struct CudaIndex {
     // FP32 path (device outputs are patched in place). Synchronises the stream.
     int finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
     int stream_status();
+    void order_after_previous(cudaStream_t s);
+    void mark_done(cudaStream_t s);
 };
 
 int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out,

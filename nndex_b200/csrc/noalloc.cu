@@ -57,7 +57,8 @@ int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, ui
     std::lock_guard<std::mutex> lock(ix->mu);
     cudaError_t e = cudaSetDevice(ix->device);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
-    if (!s) s = ix->stream;
+    if (!s) s = cudaStreamLegacy;
+    ix->order_after_previous(s);
     const uint64_t kcap = std::min<uint64_t>(k, ix->rows);
     ScanPlan plan;
     if (kcap > kMaxFusedK ||
@@ -122,6 +123,7 @@ int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, ui
     ix->h_flags[1] = 0;
     cudaMemcpyAsync(&ix->h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&ix->h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    ix->mark_done(s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "search");
     return ix->check_device_words();
 }

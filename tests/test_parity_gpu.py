@@ -366,3 +366,30 @@ def test_large_multi_cta_flushes():
     oi, osim = O.search_exact(base, qn, 100)
     for i in range(16):
         assert_topk_matches(idx[i], sim[i], O.scores_f64(base, qn[i]), 100, what=f"q{i}")
+
+
+def test_create_from_device_waits_for_pending_writes():
+    # The matrix is still being written asynchronously (no synchronize) when the index is built.
+    torch = pytest.importorskip("torch")
+    rows, dims = 2_000_000, 128
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    x = torch.randn((rows, dims), generator=g, device="cuda")
+    x = x / torch.linalg.vector_norm(x, dim=1, keepdim=True)
+    h = C.c_void_p()
+    opts = _lib.Opts()
+    opts.device = 0
+    st = _lib.lib().nndex_cuda_create_from_device(x.data_ptr(), x.numel(), rows, dims, _lib.NNDEX_FLAG_NORMALIZED,
+                                                  C.byref(opts), C.byref(h))
+    assert st == 0, _lib.last_error()
+    try:
+        q = x[[0, rows // 2, rows - 1]].clone()
+        pq = torch.arange(3, device="cuda", dtype=torch.int64)
+        pr = torch.tensor([0, rows // 2, rows - 1], device="cuda", dtype=torch.int64)
+        out = torch.zeros(3, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        assert _lib.lib().nndex_cuda_fp64_scores(h, q.data_ptr(), 3, pq.data_ptr(), pr.data_ptr(), 3,
+                                                 out.data_ptr()) == 0
+        assert np.allclose(out.cpu().numpy(), 1.0, atol=1e-5)
+    finally:
+        _lib.lib().nndex_cuda_destroy(h)
