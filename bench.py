@@ -467,13 +467,16 @@ def run_mixed(args, dev, L, world):
         n0 = kernel_launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
+        second = 0
         fallbacks = 0
         for _ in range(steps):
             if L.nndex_cuda_search_batch_device(h, q.data_ptr(), nq, dims, k, oi.data_ptr(), os_.data_ptr(), None,
                                                 sptr, 1) != 0:
                 raise RuntimeError(_lib.last_error())
             L.nndex_cuda_last_search_stats(h, C.byref(stats))
-            fallbacks += stats.widenings if stats.path in (2, 3) else 0
+            if stats.path in (2, 3):
+                second += stats.second_pass_queries
+                fallbacks += stats.fp32_fallback_queries
         e1.record(stream)
         torch.cuda.synchronize(dev)
         n1 = kernel_launch_count()
@@ -498,7 +501,8 @@ def run_mixed(args, dev, L, world):
             "recall_at_k_vs_fp64": hits / (sample * k),
             "max_score_error_vs_fp64": err,
             "rerank_width": int(stats.rerank_width),
-            "fallback_queries_per_batch": fallbacks / steps,
+            "second_pass_queries_per_batch": second / steps,
+            "fp32_fallback_queries_per_batch": fallbacks / steps,
             "kernel_launches_per_batch": (n1 - n0) / steps,
         }
     L.nndex_cuda_destroy(h)

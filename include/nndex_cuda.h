@@ -103,12 +103,14 @@ typedef struct nndex_cuda_search_stats {
     uint32_t path;             /* 1 = FP32 scan, 2 = BF16 scan+rerank, 3 = FP8 scan+rerank,
                                   4 = IVF probe + rerank                                     */
     uint32_t kernel_launches;  /* kernels this library launched for the call                */
-    uint32_t rerank_width;     /* k' used by a low-precision scan (0 otherwise)             */
-    uint32_t certified;        /* 1 = every query's low-precision top-k passed the bound    */
-    uint32_t widenings;        /* k' doublings needed to certify                            */
+    uint32_t rerank_width;     /* k' of a low-precision scan's first pass (0 otherwise)     */
+    uint32_t certified;        /* 1 = every query certified after the first pass            */
+    uint32_t second_pass_queries;   /* queries that took the threshold-collection pass     */
     uint32_t nprobe;           /* IVF lists probed per query                                */
     uint64_t rows_scanned;     /* base rows scored (sum over queries for IVF)               */
     double   device_ms;        /* CUDA-event time of the device part of the call            */
+    uint32_t fp32_fallback_queries; /* queries re-run on the FP32 scan (pass-2 overflow)   */
+    uint32_t reserved;
 } nndex_cuda_search_stats;
 
 /* ---- errors ---------------------------------------------------------------------------- */

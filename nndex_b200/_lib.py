@@ -72,10 +72,12 @@ class SearchStats(C.Structure):
         ("kernel_launches", C.c_uint32),
         ("rerank_width", C.c_uint32),
         ("certified", C.c_uint32),
-        ("widenings", C.c_uint32),
+        ("second_pass_queries", C.c_uint32),
         ("nprobe", C.c_uint32),
         ("rows_scanned", C.c_uint64),
         ("device_ms", C.c_double),
+        ("fp32_fallback_queries", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 

@@ -194,6 +194,17 @@ CudaIndex::~CudaIndex() {
     cudaFree(d_fb_idx);
     cudaFree(d_fb_sim);
     cudaFree(d_fb_cnt);
+    cudaFree(d_kth);
+    cudaFree(d_ids);
+    cudaFree(d_q2_lp);
+    cudaFree(d_q2_resid);
+    cudaFree(d_q2_scale);
+    cudaFree(d_q2_thr);
+    cudaFree(d_rows2);
+    cudaFree(d_cnt2);
+    cudaFree(d_ok2);
+    cudaFreeHost(h_ids);
+    cudaFreeHost(h_ok2);
     cudaFreeHost(h_cert);
     if (done_ev) cudaEventDestroy(done_ev);
     if (ev0) cudaEventDestroy(ev0);
@@ -316,20 +327,20 @@ uint32_t CudaIndex::tc_chunks(bool fp8) const {
     return static_cast<uint32_t>((fp8 ? kf8 : kb16 * 2) / 128);
 }
 
-// k′ for a batch: the tuned width for this k (widened after batches whose certificates failed),
-// capped by the largest per-query heap that fits in shared memory with at least 2 ring stages.
+// k′ of pass 1: enough candidates that most queries certify, but small enough that the heaps fit
+// beside a 4-deep base ring (queries that do not certify take the threshold pass).
 uint32_t CudaIndex::choose_kprime(uint64_t kcap, bool fp8) const {
     const uint32_t nchunks = tc_chunks(fp8);
-    uint32_t kmax = 0;
-    for (uint32_t kp = 8; kp <= 256; kp += 8)
-        if (tc_stages_for(nchunks, kp, fp8, smem_optin) != 0) kmax = kp;
-    uint32_t kp = rerank_width;
-    if (!kp) {
-        kp = static_cast<uint32_t>(std::max<uint64_t>(32, 3 * kcap));
-        auto it = tuned_kprime.find((fp8 ? 1ull << 40 : 0ull) | kcap);
-        if (it != tuned_kprime.end()) kp = std::max(kp, it->second);
+    uint32_t kmax4 = 0, kmax = 0;
+    for (uint32_t kp = 8; kp <= 2048; kp += 8) {
+        const uint32_t stg = tc_stages_for(nchunks, kp, fp8, smem_optin);
+        if (stg == 4) kmax4 = kp;
+        if (stg != 0) kmax = kp;
     }
+    uint32_t kp = rerank_width ? rerank_width : static_cast<uint32_t>(std::max<uint64_t>(32, 2 * kcap));
+    if (kp > kmax4 && kcap <= kmax4 && !rerank_width) kp = kmax4;
     if (kp > kmax) kp = kmax;
+    if (kp < kcap) kp = static_cast<uint32_t>(std::min<uint64_t>(kcap, kmax));
     if (kp > rows) kp = static_cast<uint32_t>(rows);
     return kp;
 }
@@ -375,18 +386,12 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
                           cudaStream_t s) {
     int st;
     const uint32_t kp = choose_kprime(kcap, fp8);
-    const uint64_t kb = fp8 ? kf8 : kb16;
     const uint32_t nchunks = tc_chunks(fp8);
-    // Prefer the deepest ring; give it up for k′ room only when the heaps need it.
     const uint32_t stages = tc_stages_for(nchunks, kp, fp8, smem_optin);
     if (!stages) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k'=%u does not fit", kp);
     const uint32_t nqb = (n + 127) / 128;
-    // Row ranges: about four waves of CTAs, each range a multiple of the 256-row tile.
-    uint64_t nranges = (4ull * sm_count + nqb - 1) / nqb;
-    nranges = std::max<uint64_t>(1, std::min<uint64_t>(nranges, (rows + 2047) / 2048));
-    uint64_t range_rows = (rows + nranges - 1) / nranges;
-    range_rows = (range_rows + 255) / 256 * 256;
-    nranges = (rows + range_rows - 1) / range_rows;
+    uint64_t nranges = 0, range_rows = 0;
+    tc_ranges(nqb, nranges, range_rows);
     const uint64_t per_query = nranges * kp;
     if ((st = grow_device(d_thr, cap_thr, n, "tc workspace"))) return st;
     if ((st = grow_device(d_ws, cap_ws, per_query * n, "tc workspace"))) return st;
@@ -394,37 +399,25 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     if ((st = grow_device(d_cand_sim, cap_cand_sim, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
     if ((st = grow_device(d_cand_cnt, cap_cand_cnt, n, "tc workspace"))) return st;
     if ((st = grow_device(d_cert, cap_cert, n, "tc workspace"))) return st;
-    // Tensor map of the quantised query buffer (its address can change when it grows).
+    if ((st = grow_device(d_kth, cap_kth, n, "tc workspace"))) return st;
     CUtensorMap tmap_q;
-    const uint64_t nq_alloc = (n + 127) / 128 * 128;
-    const bool ok = fp8 ? encode_tmap_2d(&tmap_q, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, d_q_fp8, kf8, nq_alloc, kf8, 128,
-                                         128, CU_TENSOR_MAP_SWIZZLE_128B)
-                        : encode_tmap_2d(&tmap_q, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, d_q_bf16, kb16, nq_alloc,
-                                         kb16 * 2, 64, 128, CU_TENSOR_MAP_SWIZZLE_128B);
-    if (!ok) return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (queries)");
+    if ((st = encode_query_tmap(fp8, fp8 ? static_cast<void*>(d_q_fp8) : static_cast<void*>(d_q_bf16), n, &tmap_q)))
+        return st;
     cudaMemsetAsync(d_thr, 0, n * sizeof(unsigned long long), s);
     TcArgs a;
     a.tmap_q = &tmap_q;
     a.tmap_b = fp8 ? &tmap_fp8 : &tmap_bf16;
-    a.nq = n;
-    a.nchunks = nchunks;
-    a.rows = rows;
-    a.range_rows = range_rows;
     a.nranges = static_cast<uint32_t>(nranges);
-    a.kprime = kp;
     a.stages = stages;
-    a.row_scale = fp8 ? d_row_scale : nullptr;
-    a.q_scale = fp8 ? d_q_scale : nullptr;
-    a.row_resid = fp8 ? d_res8 : d_res16;
-    a.q_resid = d_q_resid;
-    // FP32 accumulation of kb exact products (|Σ| ≤ 1 + ε): kb·2^-23, with a 4× margin.
-    a.eps_acc = 4.0f * static_cast<float>(kb) * 1.1920929e-07f;
-    a.thr_global = d_thr;
-    a.ws_keys = d_ws;
-    a.status = d_status;
+    fill_tc_params(fp8, n, range_rows, a.p);
+    a.p.q_resid = d_q_resid;
+    a.p.q_scale = fp8 ? d_q_scale : nullptr;
+    a.p.kprime = kp;
+    a.p.thr_global = d_thr;
+    a.p.ws_keys = d_ws;
     cudaEvent_t ev_a = nullptr;
     scan_event_begin(s, ev_a);
-    cudaError_t e = launch_scan_tc(a, fp8, s);
+    cudaError_t e = launch_scan_tc(a, fp8, 0, s);
     scan_event_end(s, ev_a);
     if (e != cudaSuccess) return cuda_error(e, "tensor-core scan launch");
     MergeArgs m;
@@ -451,6 +444,7 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     r.sim_out = o_sim;
     r.cnt_out = o_cnt;
     r.cert_out = d_cert;
+    r.kth_out = d_kth;
     if ((e = launch_rerank(r, s)) != cudaSuccess) return cuda_error(e, "rerank launch");
     stats.kernel_launches += 3;
     stats.path = fp8 ? 3 : 2;
@@ -459,6 +453,43 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     return NNDEX_OK;
 }
 
+// Row ranges of the tensor-core grid: about four waves of CTAs, each range a multiple of the
+// 256-row tile. Concurrent CTAs share ranges, so a base tile is read from HBM about once.
+void CudaIndex::tc_ranges(uint32_t nqb, uint64_t& nranges, uint64_t& range_rows) const {
+    nranges = (4ull * sm_count + nqb - 1) / nqb;
+    nranges = std::max<uint64_t>(1, std::min<uint64_t>(nranges, (rows + 2047) / 2048));
+    range_rows = (rows + nranges - 1) / nranges;
+    range_rows = (range_rows + 255) / 256 * 256;
+    nranges = (rows + range_rows - 1) / range_rows;
+}
+
+void CudaIndex::fill_tc_params(bool fp8, uint32_t n, uint64_t range_rows, TcParams& p) const {
+    const uint64_t kb = fp8 ? kf8 : kb16;
+    p.nq = n;
+    p.nchunks = tc_chunks(fp8);
+    p.rows = rows;
+    p.range_rows = range_rows;
+    p.row_scale = fp8 ? d_row_scale : nullptr;
+    p.row_resid = fp8 ? d_res8 : d_res16;
+    p.eps_rows = fp8 ? eps_fp8 : eps_bf16;
+    // FP32 accumulation of kb exact products (|Σ| ≤ 1 + ε): kb·2^-23, with a 4× margin.
+    p.eps_acc = 4.0f * static_cast<float>(kb) * 1.1920929e-07f;
+    p.status = d_status;
+}
+
+int CudaIndex::encode_query_tmap(bool fp8, void* buf, uint32_t n, CUtensorMap* map) const {
+    const uint64_t nq_alloc = (n + 127) / 128 * 128;
+    const bool ok = fp8 ? encode_tmap_2d(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, buf, kf8, nq_alloc, kf8, 128, 128,
+                                         CU_TENSOR_MAP_SWIZZLE_128B)
+                        : encode_tmap_2d(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, buf, kb16, nq_alloc, kb16 * 2, 64,
+                                         128, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (!ok) return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (queries)");
+    return NNDEX_OK;
+}
+
+// After pass 1: queries whose certificate held are final. The others run pass 2 (collect every row
+// whose upper bound reaches their exact k-th score, rerank exactly); a query whose collected set
+// overflows is re-run on the FP32 scan. Synchronises the stream.
 int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
                          cudaStream_t s) {
     int st;
@@ -471,32 +502,84 @@ int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_si
     if (e != cudaSuccess) return cuda_error(e, "search");
     if ((st = check_device_words())) return st;
     last_tc_n = n;
-    std::vector<uint32_t> failed;
+    const bool fp8 = stats.path == 3;
+    uint32_t m = 0;
+    if ((st = grow_host(h_ids, cap_hids, n, "pinned buffer"))) return st;
     for (uint32_t i = 0; i < n; ++i)
-        if (!h_cert[i]) failed.push_back(i);
-    stats.certified = failed.empty() ? 1u : 0u;
-    stats.widenings = static_cast<uint32_t>(failed.size());  // queries re-run on the FP32 path
-    // Autotune k′: when more than 1 % of a batch fails, the next batch at this k searches twice as
-    // many candidates (up to the shared-memory cap).
-    if (failed.size() * 100 > n && stats.rerank_width) {
-        const bool fp8 = stats.path == 3;
-        uint64_t key = (fp8 ? 1ull << 40 : 0ull) | kcap;
-        tuned_kprime[key] = std::min<uint32_t>(stats.rerank_width * 2, 256);
-    }
-    if (failed.empty()) return NNDEX_OK;
-    const uint32_t m = static_cast<uint32_t>(failed.size());
-    if ((st = grow_device(d_qsub, cap_qsub, static_cast<uint64_t>(m) * ds, "fallback buffer"))) return st;
+        if (!h_cert[i]) h_ids[m++] = i;
+    stats.certified = m == 0 ? 1u : 0u;
+    stats.second_pass_queries = m;
+    if (m == 0) return NNDEX_OK;
+
+    // ---- pass 2 ----
+    const uint32_t cap2 = kSecondPassCap;
+    const uint64_t row_bytes = fp8 ? kf8 : kb16 * 2;
+    const uint64_t m_alloc = (m + 127) / 128 * 128;
+    if ((st = grow_device(d_ids, cap_ids, m, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_q2_lp, cap_q2_lp, m_alloc * row_bytes, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_q2_resid, cap_q2_resid, m, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_q2_scale, cap_q2_scale, m, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_q2_thr, cap_q2_thr, m, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_rows2, cap_rows2, static_cast<uint64_t>(m) * cap2, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_cnt2, cap_cnt2, m, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_ok2, cap_ok2, m, "pass-2 buffer"))) return st;
+    cudaMemcpyAsync(d_ids, h_ids, m * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    e = launch_gather_queries(d_ids, m, fp8 ? static_cast<const void*>(d_q_fp8) : static_cast<const void*>(d_q_bf16),
+                              static_cast<uint32_t>(row_bytes), d_q2_lp, d_q_resid, d_q2_resid,
+                              fp8 ? d_q_scale : nullptr, d_q2_scale, d_kth, d_q2_thr, s);
+    if (e != cudaSuccess) return cuda_error(e, "gather launch");
+    cudaMemsetAsync(d_cnt2, 0, m * sizeof(uint32_t), s);
+    CUtensorMap tmap_q2;
+    if ((st = encode_query_tmap(fp8, d_q2_lp, m, &tmap_q2))) return st;
+    uint64_t nranges = 0, range_rows = 0;
+    tc_ranges((m + 127) / 128, nranges, range_rows);
+    TcArgs a;
+    a.tmap_q = &tmap_q2;
+    a.tmap_b = fp8 ? &tmap_fp8 : &tmap_bf16;
+    a.nranges = static_cast<uint32_t>(nranges);
+    a.stages = tc_stages_for(tc_chunks(fp8), 0, fp8, smem_optin);
+    fill_tc_params(fp8, m, range_rows, a.p);
+    a.p.q_resid = d_q2_resid;
+    a.p.q_scale = fp8 ? d_q2_scale : nullptr;
+    a.p.q_thr = d_q2_thr;
+    a.p.cand_rows = d_rows2;
+    a.p.cand_cnt = d_cnt2;
+    a.p.cap2 = cap2;
+    cudaEvent_t ev_a = nullptr;
+    scan_event_begin(s, ev_a);
+    e = launch_scan_tc(a, fp8, 1, s);
+    scan_event_end(s, ev_a);
+    if (e != cudaSuccess) return cuda_error(e, "tensor-core scan launch (pass 2)");
+    e = launch_rerank_collected(d_base, static_cast<uint32_t>(ds), d_qn, d_ids, m, d_rows2, d_cnt2, cap2, kcap, o_idx,
+                                o_sim, o_cnt, d_ok2, s);
+    if (e != cudaSuccess) return cuda_error(e, "rerank launch (pass 2)");
+    stats.kernel_launches += 3;
+    if ((st = grow_host(h_ok2, cap_hok2, m, "pinned buffer"))) return st;
+    cudaMemcpyAsync(h_ok2, d_ok2, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    h_flags[1] = 0;
+    cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_error(e, "search");
+    if ((st = check_device_words())) return st;
+    std::vector<uint32_t> failed;
     for (uint32_t i = 0; i < m; ++i)
+        if (!h_ok2[i]) failed.push_back(h_ids[i]);
+    stats.fp32_fallback_queries = static_cast<uint32_t>(failed.size());
+    if (failed.empty()) return NNDEX_OK;
+
+    // ---- FP32 scan for queries whose collected set overflowed ----
+    const uint32_t mf = static_cast<uint32_t>(failed.size());
+    if ((st = grow_device(d_qsub, cap_qsub, static_cast<uint64_t>(mf) * ds, "fallback buffer"))) return st;
+    for (uint32_t i = 0; i < mf; ++i)
         cudaMemcpyAsync(d_qsub + static_cast<uint64_t>(i) * ds, d_qn + static_cast<uint64_t>(failed[i]) * ds,
                         ds * sizeof(float), cudaMemcpyDeviceToDevice, s);
-    // results of the re-run land in the fallback buffers, then move to their query's slots
-    if ((st = grow_device(d_fb_idx, cap_fb_idx, static_cast<uint64_t>(m) * kcap, "fallback buffer"))) return st;
-    if ((st = grow_device(d_fb_sim, cap_fb_sim, static_cast<uint64_t>(m) * kcap, "fallback buffer"))) return st;
-    if ((st = grow_device(d_fb_cnt, cap_fb_cnt, m, "fallback buffer"))) return st;
+    if ((st = grow_device(d_fb_idx, cap_fb_idx, static_cast<uint64_t>(mf) * kcap, "fallback buffer"))) return st;
+    if ((st = grow_device(d_fb_sim, cap_fb_sim, static_cast<uint64_t>(mf) * kcap, "fallback buffer"))) return st;
+    if ((st = grow_device(d_fb_cnt, cap_fb_cnt, mf, "fallback buffer"))) return st;
     const uint32_t path = stats.path;
-    if ((st = enqueue_exact_fp32(d_qsub, m, kcap, kcap, d_fb_idx, d_fb_sim, d_fb_cnt, s))) return st;
+    if ((st = enqueue_exact_fp32(d_qsub, mf, kcap, kcap, d_fb_idx, d_fb_sim, d_fb_cnt, s))) return st;
     stats.path = path;
-    for (uint32_t i = 0; i < m; ++i) {
+    for (uint32_t i = 0; i < mf; ++i) {
         const uint64_t q = failed[i];
         cudaMemcpyAsync(o_idx + q * kcap, d_fb_idx + static_cast<uint64_t>(i) * kcap, kcap * sizeof(uint64_t),
                         cudaMemcpyDeviceToDevice, s);

@@ -12,6 +12,8 @@ namespace nndex {
 
 // Queries handled per scan launch sequence; larger batches are processed in chunks.
 constexpr uint64_t kMaxBatchChunk = 16384;
+// Rows a pass-2 query may collect before it is re-run on the FP32 scan.
+constexpr uint32_t kSecondPassCap = 8192;
 
 int set_error(int code, const char* fmt, ...);
 void clear_error();
@@ -82,8 +84,31 @@ struct CudaIndex {
     uint32_t* d_fb_cnt = nullptr;
     size_t cap_fb_cnt = 0;
     uint32_t last_tc_n = 0;  // queries of the last tensor-core batch (diagnostics)
+    float* d_kth = nullptr;  // pass 1: exact k-th score per query
+    size_t cap_kth = 0;
+    // pass 2 (threshold collection) buffers
+    uint32_t* d_ids = nullptr;
+    size_t cap_ids = 0;
+    uint8_t* d_q2_lp = nullptr;
+    size_t cap_q2_lp = 0;
+    float* d_q2_resid = nullptr;
+    size_t cap_q2_resid = 0;
+    float* d_q2_scale = nullptr;
+    size_t cap_q2_scale = 0;
+    float* d_q2_thr = nullptr;
+    size_t cap_q2_thr = 0;
+    uint32_t* d_rows2 = nullptr;
+    size_t cap_rows2 = 0;
+    uint32_t* d_cnt2 = nullptr;
+    size_t cap_cnt2 = 0;
+    uint32_t* d_ok2 = nullptr;
+    size_t cap_ok2 = 0;
+    uint32_t* h_ids = nullptr;
+    size_t cap_hids = 0;
+    uint32_t* h_ok2 = nullptr;
+    size_t cap_hok2 = 0;
     uint32_t rerank_width = 0;  // k′ override (0 = autotuned)
-    std::unordered_map<uint64_t, uint32_t> tuned_kprime;  // (precision, k) → widened k′
+
 
     // per-search buffers (grown on demand)
     float* d_qraw = nullptr;
@@ -134,6 +159,9 @@ struct CudaIndex {
     int choose_path(uint64_t nq, uint64_t kcap) const;
     uint32_t choose_kprime(uint64_t kcap, bool fp8) const;
     uint32_t tc_chunks(bool fp8) const;
+    void tc_ranges(uint32_t nqb, uint64_t& nranges, uint64_t& range_rows) const;
+    void fill_tc_params(bool fp8, uint32_t n, uint64_t range_rows, TcParams& p) const;
+    int encode_query_tmap(bool fp8, void* buf, uint32_t n, CUtensorMap* map) const;
     int enqueue_prep_queries(const float* d_raw, uint64_t n, int mode, int path, cudaStream_t s);
     int enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
                    cudaStream_t s);

@@ -73,36 +73,44 @@ struct MergeArgs {
 };
 cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream);
 
-// K3 tensor-core scan (BF16 / FP8) with fused top-k′ filter, and K4 rerank.
-struct TcArgs {
-    const CUtensorMap* tmap_q = nullptr;  // quantised queries [nq_alloc × K], box {128 B, 128 rows}
-    const CUtensorMap* tmap_b = nullptr;  // quantised base [rows_alloc × K], box {128 B, 256 rows}
+// K3 tensor-core scan (BF16 / FP8), two passes, and K4 rerank.
+struct TcParams {
     uint32_t nq = 0;
     uint32_t nchunks = 0;                 // K bytes / 128
+    uint32_t kprime = 0;                  // pass 1 heap size
+    uint32_t cap2 = 0;                    // pass 2 rows collected per query
     uint64_t rows = 0;
     uint64_t range_rows = 0;              // rows per CTA range (multiple of 256)
-    uint32_t nranges = 0;
-    uint32_t kprime = 0;
-    uint32_t stages = 4;                  // base ring depth (2..4)
     const float* row_scale = nullptr;     // FP8 only
     const float* q_scale = nullptr;       // FP8 only
     const float* row_resid = nullptr;     // ‖x − x̂‖ per row
     const float* q_resid = nullptr;       // ‖q − q̂‖ per query
     float eps_acc = 0.0f;                 // FP32 accumulation error bound
-    unsigned long long* thr_global = nullptr;  // per query, zeroed before the launch
-    uint64_t* ws_keys = nullptr;          // nq × nranges × kprime
+    float eps_rows = 0.0f;                // max ‖x − x̂‖ over the rows
+    unsigned long long* thr_global = nullptr;  // pass 1: per query, zeroed before the launch
+    uint64_t* ws_keys = nullptr;          // pass 1: nq × nranges × kprime
+    const float* q_thr = nullptr;         // pass 2: per query T (exact k-th score of pass 1)
+    uint32_t* cand_rows = nullptr;        // pass 2: nq × cap2
+    uint32_t* cand_cnt = nullptr;         // pass 2: nq, zeroed before the launch
     uint32_t* status = nullptr;
+};
+struct TcArgs {
+    const CUtensorMap* tmap_q = nullptr;  // quantised queries [nq_alloc × K], box {128 B, 128 rows}
+    const CUtensorMap* tmap_b = nullptr;  // quantised base [rows_alloc × K], box {128 B, 256 rows}
+    TcParams p;
+    uint32_t nranges = 0;
+    uint32_t stages = 4;                  // base ring depth (2..4)
 };
 size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8);
 // Deepest base ring (4, 3 or 2 stages) that fits k′ heaps in `smem_limit`; 0 if none fits.
 uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, size_t smem_limit);
-cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, cudaStream_t stream);
+cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t stream);
 
 struct RerankArgs {
     const float* base = nullptr;  // FP32 base, stride ds
     uint32_t ds = 0;
     const float* queries = nullptr;  // FP32 normalised queries, stride ds
-    const uint64_t* cand_idx = nullptr;  // nq × kp, sorted by approximate score
+    const uint64_t* cand_idx = nullptr;  // nq × kp, sorted by upper bound
     const float* cand_sim = nullptr;     // upper bounds of the exact scores, sorted descending
     const uint32_t* cand_cnt = nullptr;
     uint32_t nq = 0, kp = 0, k = 0;
@@ -110,8 +118,16 @@ struct RerankArgs {
     float* sim_out = nullptr;
     uint32_t* cnt_out = nullptr;
     uint32_t* cert_out = nullptr;
+    float* kth_out = nullptr;            // exact k-th score per query (pass-2 threshold)
 };
 cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream);
+cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q_lp, uint32_t row_bytes, void* q2_lp,
+                                  const float* resid, float* resid2, const float* scale, float* scale2,
+                                  const float* kth, float* thr2, cudaStream_t stream);
+cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float* queries, const uint32_t* ids,
+                                    uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
+                                    uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
+                                    cudaStream_t stream);
 cudaError_t launch_max_reduce(const float* v, uint64_t n, unsigned int* out, cudaStream_t stream);
 
 // Maximum k the fused scan kernels select in shared memory.

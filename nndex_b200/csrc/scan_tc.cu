@@ -1,25 +1,31 @@
-// scan_tc.cu — K3: tensor-core (tcgen05) scan of the BF16 / FP8-E4M3 base with a fused top-k′
-// filter, and K4: exact FP32 rerank of the k′ candidates with the exactness certificate.
+// scan_tc.cu — K3: tensor-core (tcgen05) scan of the BF16 / FP8-E4M3 base, and K4: exact FP32 rerank.
 //
 // This is the large-batch path of nndex's exact search (the reference's GEMM strategies,
-// src/cpu.rs:256-341): S = Q̂·X̂ᵀ on the 5th-generation tensor cores, FP32 accumulation in TMEM, and
-// a per-query top-k′ of the approximate scores kept in shared memory, so scores never reach HBM.
-// The k′ candidates are re-scored exactly in FP32 (K4) and the top-k returned. The result is exact
-// (identical to the FP32 path's selection rule) whenever the certificate holds:
-//     exact k-th score  >  approximate k′-th score + ε,
-// where ε bounds |q·x − q̂·x̂| for every row (quantisation residual norms from K1, Cauchy–Schwarz,
-// plus the FP32 accumulation error). Queries whose certificate fails are re-run on the FP32 path.
+// src/cpu.rs:256-341): S = Q̂·X̂ᵀ on the 5th-generation tensor cores with FP32 accumulation in TMEM.
+// Scores never reach HBM. The result is the exact FP32 top-k, proven per query:
+//
+//   Every row r gets an upper bound of its exact score from its approximate score:
+//       s_r ≤ u_r = s̃_r + ‖δx_r‖(1 + ‖δq‖) + ‖δq‖ + ε_acc
+//   (q·x − q̂·x̂ = q·δx + δq·x̂, ‖q‖ = 1, Cauchy–Schwarz; ε_acc bounds the FP32 accumulation).
+//   Pass 1 (kMode 0) keeps, per query, the k′ rows with the largest u_r (a min-heap per query in
+//   shared memory, thresholds shared across CTAs through a global per-query key). K4 re-scores the
+//   k′ candidates exactly in FP32; the exact k-th score T is a lower bound of the true k-th score.
+//   If T > the k′-th upper bound, no other row can enter the top-k: the query is done.
+//   Pass 2 (kMode 1), for the other queries only: collect every row with u_r ≥ T (no row with
+//   u_r < T can reach the top-k, since k rows already score ≥ T), and re-score them exactly.
+//   Only a query whose pass-2 set overflows its buffer is re-run on the FP32 scan.
 //
 // K3 layout. One CTA = 128 queries (one TMEM lane each; the query block is the MMA's A operand,
 // resident in shared memory) × one range of base rows. Warp 0 issues TMA loads of 256-row base
 // tiles, one 128-byte K slab per ring stage (128 B swizzle); warp 1 issues tcgen05.mma (M = 128,
 // N = 256, 4 instructions per slab) into one of two 256-column FP32 accumulators in TMEM; warps 2-5
-// read the finished accumulator with tcgen05.ld (each thread one query's 256 scores), scale them
-// (FP8: per-row × per-query scale) and push keys that beat the query's running k′-th key into a
-// per-query min-heap in shared memory. The k′-th key of each finished range is published to a
-// global per-query threshold (atomicMax), which later ranges start from. No TMA multicast.
+// read the finished accumulator with tcgen05.ld (each thread: one query's 256 scores, in 32-column
+// chunks, loads double-buffered), reject almost every score with one compare against
+// (threshold − largest possible bound slack), and bound/insert the rare survivors. Base tiles stay
+// in L2 for the other query blocks of the same row range. No TMA multicast.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstdlib>
 
 #include "common.cuh"
@@ -41,6 +47,26 @@ NNDEX_DEVICE_INLINE uint8_t* align_1024(uint8_t* p) {
     const uint32_t a = smem_u32(p);
     return p + ((1024u - (a & 1023u)) & 1023u);
 }
+
+// tcgen05.wait::ld that also ties the 32 registers of the completed load, so no use of them can be
+// scheduled before the wait.
+NNDEX_DEVICE_INLINE void tmem_wait_ld_regs(uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.wait::ld.sync.aligned;"
+        : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+          "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15]),
+          "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]), "+r"(v[22]), "+r"(v[23]),
+          "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]), "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
+        :
+        : "memory");
+}
+
+NNDEX_DEVICE_INLINE float pick(const uint32_t (&v)[32], uint32_t j) {
+    uint32_t r = 0;
+#pragma unroll
+    for (uint32_t jj = 0; jj < 32; ++jj) r = (jj == j) ? v[jj] : r;
+    return __uint_as_float(r);
+}
 }  // namespace
 
 size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8) {
@@ -48,7 +74,7 @@ size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp
     b += static_cast<size_t>(nchunks) * kAChunk;
     b += static_cast<size_t>(stages) * kBChunk;
     b += static_cast<size_t>(kprime) * kM * 8;
-    b += 4 * kN * 4;
+    b += fp8 ? 2 * kN * 4 : 0;
     b += (2 * stages + 5) * 8 + 16;
     return b;
 }
@@ -59,23 +85,81 @@ uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, size_t smem_
     return 0;
 }
 
-template <bool kFp8, int kST>
+// Per-query epilogue state.
+struct EpiState {
+    uint32_t n;                  // heap size (pass 1)
+    unsigned long long thr_key;  // pass 1: key a candidate must beat
+    float thr_f;                 // pass 1: score of thr_key; pass 2: T
+    float cut;                   // thr_f − largest bound slack: scores below cannot survive
+};
+
+// A score that passed the cheap filter: apply its exact bound, then insert (pass 1) or collect
+// (pass 2).
+template <int kMode>
+NNDEX_DEVICE_INLINE void epi_survivor(const TcParams& p, EpiState& st, uint64_t* heap, uint32_t lrow, uint32_t q,
+                                      float u, uint64_t row, float slack) {
+    if (u < st.thr_f) return;
+    if (kMode == 0) {
+        const uint64_t key = make_key(u, static_cast<uint32_t>(row));
+        if (key <= st.thr_key) return;
+        const uint32_t kp = p.kprime;
+        if (st.n < kp) {
+            uint32_t i = st.n++;
+            while (i > 0) {
+                const uint32_t pp = (i - 1) >> 1;
+                const uint64_t hp = heap[pp * kM + lrow];
+                if (hp <= key) break;
+                heap[i * kM + lrow] = hp;
+                i = pp;
+            }
+            heap[i * kM + lrow] = key;
+        } else {
+            uint32_t i = 0;
+            for (;;) {
+                const uint32_t l = 2 * i + 1;
+                if (l >= st.n) break;
+                const uint32_t r = l + 1;
+                uint64_t hm = heap[l * kM + lrow];
+                uint32_t m = l;
+                if (r < st.n) {
+                    const uint64_t hr = heap[r * kM + lrow];
+                    if (hr < hm) {
+                        hm = hr;
+                        m = r;
+                    }
+                }
+                if (hm >= key) break;
+                heap[i * kM + lrow] = hm;
+                i = m;
+            }
+            heap[i * kM + lrow] = key;
+        }
+        if (st.n == kp) {
+            const uint64_t mn = heap[lrow];
+            if (mn > st.thr_key) {
+                st.thr_key = mn;
+                st.thr_f = key_score(mn);
+                st.cut = st.thr_f - slack;
+            }
+        }
+    } else {
+        const uint32_t pos = atomicAdd(&p.cand_cnt[q], 1u);
+        if (pos < p.cap2) p.cand_rows[static_cast<size_t>(q) * p.cap2 + pos] = static_cast<uint32_t>(row);
+    }
+}
+
+template <bool kFp8, int kST, int kMode>
 __global__ void __launch_bounds__(kThreads, 1)
     scan_tc_kernel(const __grid_constant__ CUtensorMap tmap_q, const __grid_constant__ CUtensorMap tmap_b,
-                   uint32_t nq, uint32_t nchunks, uint64_t rows, uint64_t range_rows, uint32_t kprime,
-                   const float* __restrict__ row_scale, const float* __restrict__ q_scale,
-                   const float* __restrict__ row_resid, const float* __restrict__ q_resid, float eps_acc,
-                   unsigned long long* __restrict__ thr_global, uint64_t* __restrict__ ws_keys,
-                   uint32_t* __restrict__ status) {
+                   const TcParams p) {
     constexpr uint32_t kElems = kFp8 ? 128 : 64;  // K elements per 128-byte slab
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = align_1024(smem_raw);
     uint8_t* a_smem = smem;
-    uint8_t* b_smem = a_smem + static_cast<size_t>(nchunks) * kAChunk;
+    uint8_t* b_smem = a_smem + static_cast<size_t>(p.nchunks) * kAChunk;
     uint64_t* heap = reinterpret_cast<uint64_t*>(b_smem + static_cast<size_t>(kST) * kBChunk);
-    // Per-tile row data, double-buffered by tile parity: [parity][residual bound | FP8 scale][256].
-    float* rowinfo = reinterpret_cast<float*>(heap + static_cast<size_t>(kprime) * kM);
-    uint64_t* full_bar = reinterpret_cast<uint64_t*>(rowinfo + 4 * kN);
+    float* scale_s = reinterpret_cast<float*>(heap + static_cast<size_t>(p.kprime) * kM);  // FP8: [2][256]
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(scale_s + (kFp8 ? 2 * kN : 0));
     uint64_t* empty_bar = full_bar + kST;
     uint64_t* a_full = empty_bar + kST;
     uint64_t* tfull = a_full + 1;
@@ -86,9 +170,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t q0 = blockIdx.x * kM;
     const uint32_t range = blockIdx.y, nranges = gridDim.y;
-    const uint64_t row_begin = static_cast<uint64_t>(range) * range_rows;
-    const uint64_t row_end = (row_begin + range_rows) < rows ? (row_begin + range_rows) : rows;
+    const uint64_t row_begin = static_cast<uint64_t>(range) * p.range_rows;
+    const uint64_t row_end = (row_begin + p.range_rows) < p.rows ? (row_begin + p.range_rows) : p.rows;
     const uint32_t ntiles = row_end > row_begin ? static_cast<uint32_t>((row_end - row_begin + kN - 1) / kN) : 0;
+    const uint32_t nchunks = p.nchunks;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kST; ++s) {
@@ -131,7 +216,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint32_t s = it % kST, u = it / kST;
                     if (u > 0 && !mbar_wait_bounded(&empty_bar[s], (u - 1) & 1u, kWaitBudgetCycles)) {
                         *abort_flag = 1;
-                        record_status(status, kStatusTimeout);
+                        record_status(p.status, kStatusTimeout);
                         stop = true;
                         break;
                     }
@@ -146,12 +231,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             }
             // Drain every copy this thread issued before the CTA may exit.
-            if (!mbar_wait_bounded(a_full, 0, kWaitBudgetCycles)) record_status(status, kStatusTimeout);
+            if (!mbar_wait_bounded(a_full, 0, kWaitBudgetCycles)) record_status(p.status, kStatusTimeout);
             const uint32_t used = it < static_cast<uint32_t>(kST) ? it : kST;
             for (uint32_t s = 0; s < used; ++s) {
                 const uint32_t uses = (it - s + kST - 1) / kST;
                 if (!mbar_wait_bounded(&full_bar[s], (uses - 1) & 1u, kWaitBudgetCycles))
-                    record_status(status, kStatusTimeout);
+                    record_status(p.status, kStatusTimeout);
             }
         }
     } else if (warp == 1) {
@@ -160,7 +245,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             constexpr uint32_t idesc = tc::instr_desc<kFp8, kM, kN>();
             if (!mbar_wait_bounded(a_full, 0, kWaitBudgetCycles)) {
                 *abort_flag = 1;
-                record_status(status, kStatusTimeout);
+                record_status(p.status, kStatusTimeout);
             }
             tc::fence_after_sync();
             const uint32_t a_addr0 = smem_u32(a_smem), b_addr0 = smem_u32(b_smem);
@@ -169,7 +254,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const uint32_t buf = t & 1u, ub = t >> 1;
                 if (ub > 0 && !*abort_flag && !mbar_wait_bounded(&tempty[buf], (ub - 1) & 1u, kWaitBudgetCycles)) {
                     *abort_flag = 1;
-                    record_status(status, kStatusTimeout);
+                    record_status(p.status, kStatusTimeout);
                 }
                 tc::fence_after_sync();
                 const uint32_t d = tmem_base + buf * kN;
@@ -177,7 +262,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint32_t s = it % kST, u = it / kST;
                     if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], u & 1u, kWaitBudgetCycles)) {
                         *abort_flag = 1;
-                        record_status(status, kStatusTimeout);
+                        record_status(p.status, kStatusTimeout);
                     }
                     tc::fence_after_sync();
                     if (!*abort_flag) {
@@ -197,103 +282,92 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t quarter = warp & 3u;
         const uint32_t lrow = quarter * 32 + lane;
         const uint32_t q = q0 + lrow;
-        const bool valid_q = q < nq;
+        const bool valid_q = q < p.nq;
         const uint32_t et = threadIdx.x - 64;  // 0..127
-        unsigned long long thr_key = valid_q ? thr_global[q] : ~0ull;
-        const float qs = (kFp8 && valid_q) ? q_scale[q] : 1.0f;
-        // Candidates are ranked by an upper bound of the exact score: for row r,
-        //   s_r ≤ s̃_r + ‖δx_r‖(1 + ‖δq‖) + ‖δq‖ + ε_acc   (Cauchy–Schwarz on q·δx + δq·x̂, ‖q‖ = 1),
-        // so every row outside the final k′ has an exact score ≤ the k′-th bound.
-        const float rq = valid_q ? q_resid[q] : 0.0f;
-        const float b_mul = 1.0f + rq, b_add = rq + eps_acc;
-        uint32_t n = 0;
+        const float qs = (kFp8 && valid_q) ? p.q_scale[q] : 1.0f;
+        const float rq = valid_q ? p.q_resid[q] : 0.0f;
+        const float b_mul = 1.0f + rq, b_add = rq + p.eps_acc;
+        const float slack = fmaf(p.eps_rows, b_mul, b_add);  // the largest u_r − s̃_r over all rows
+        EpiState st;
+        st.n = 0;
+        if (kMode == 0) {
+            st.thr_key = valid_q ? p.thr_global[q] : ~0ull;
+            st.thr_f = !valid_q ? INFINITY : (st.thr_key ? key_score(st.thr_key) : -INFINITY);
+        } else {
+            st.thr_key = 0;
+            st.thr_f = valid_q ? p.q_thr[q] : INFINITY;
+        }
+        st.cut = st.thr_f - slack;
+        const uint32_t taddr0 = tmem_base + ((quarter * 32u) << 16);
         for (uint32_t t = 0; t < ntiles; ++t) {
             const uint32_t buf = t & 1u, ub = t >> 1;
             const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * kN;
-            {
-                float* ri = rowinfo + (t & 1u) * 2 * kN;
-                for (uint32_t j = et; j < static_cast<uint32_t>(kN); j += 128) {
-                    const bool in = tile_row0 + j < row_end;
-                    ri[j] = in ? row_resid[tile_row0 + j] : 0.0f;
-                    if (kFp8) ri[kN + j] = in ? row_scale[tile_row0 + j] : 0.0f;
-                }
+            const float* sc = scale_s + (t & 1u) * kN;
+            if (kFp8) {
+                // Row scales of this tile, shared by the 128 queries (each applies its own scale).
+                float* w = scale_s + (t & 1u) * kN;
+                for (uint32_t j = et; j < static_cast<uint32_t>(kN); j += 128)
+                    w[j] = (tile_row0 + j < row_end) ? p.row_scale[tile_row0 + j] : 0.0f;
                 named_bar_sync(2, 128);
             }
             if (!*abort_flag && !mbar_wait_bounded(&tfull[buf], ub & 1u, kWaitBudgetCycles)) {
                 *abort_flag = 1;
-                record_status(status, kStatusTimeout);
+                record_status(p.status, kStatusTimeout);
             }
             tc::fence_after_sync();
-            if ((t & 15u) == 15u && valid_q) {
-                const unsigned long long g = thr_global[q];
-                if (g > thr_key) thr_key = g;
-            }
-            float thr_f = thr_key ? key_score(thr_key) : -INFINITY;
-            const float* ri = rowinfo + (t & 1u) * 2 * kN;
-#pragma unroll 1
-            for (uint32_t c = 0; c < kN / 32; ++c) {
-                uint32_t v[32];
-                __syncwarp();
-                tc::tmem_ld32(tmem_base + ((quarter * 32u) << 16) + buf * kN + c * 32, v);
-                tc::tmem_wait_ld();
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    float s = __uint_as_float(v[j]);
-                    if (kFp8) s = (s * ri[kN + c * 32 + j]) * qs;
-                    const float ub_s = fmaf(ri[c * 32 + j], b_mul, s + b_add);
-                    const uint64_t row = tile_row0 + c * 32 + j;
-                    if (ub_s >= thr_f && row < row_end) {
-                        const uint64_t key = make_key(ub_s, static_cast<uint32_t>(row));
-                        if (key > thr_key) {
-                            // min-heap insert (index-major layout: heap[i * 128 + lrow])
-                            if (n < kprime) {
-                                uint32_t i = n++;
-                                while (i > 0) {
-                                    const uint32_t p = (i - 1) >> 1;
-                                    const uint64_t hp = heap[p * kM + lrow];
-                                    if (hp <= key) break;
-                                    heap[i * kM + lrow] = hp;
-                                    i = p;
-                                }
-                                heap[i * kM + lrow] = key;
-                            } else {
-                                uint32_t i = 0;
-                                for (;;) {
-                                    const uint32_t l = 2 * i + 1;
-                                    if (l >= n) break;
-                                    const uint32_t r = l + 1;
-                                    uint64_t hm = heap[l * kM + lrow];
-                                    uint32_t m = l;
-                                    if (r < n) {
-                                        const uint64_t hr = heap[r * kM + lrow];
-                                        if (hr < hm) {
-                                            hm = hr;
-                                            m = r;
-                                        }
-                                    }
-                                    if (hm >= key) break;
-                                    heap[i * kM + lrow] = hm;
-                                    i = m;
-                                }
-                                heap[i * kM + lrow] = key;
-                            }
-                            if (n == kprime) {
-                                const uint64_t mn = heap[lrow];
-                                if (mn > thr_key) thr_key = mn;
-                                thr_f = key_score(thr_key);
-                            }
-                        }
-                    }
+            if (kMode == 0 && (t & 15u) == 15u && valid_q) {
+                const unsigned long long g = p.thr_global[q];
+                if (g > st.thr_key) {
+                    st.thr_key = g;
+                    st.thr_f = key_score(g);
+                    st.cut = st.thr_f - slack;
                 }
+            }
+            const uint32_t taddr = taddr0 + buf * kN;
+            uint32_t va[32], vb[32];
+            __syncwarp();
+            tc::tmem_ld32(taddr, va);
+            tmem_wait_ld_regs(va);
+            auto process = [&](const uint32_t(&v)[32], uint32_t c) {
+                uint32_t mask = 0;
+#pragma unroll
+                for (uint32_t j = 0; j < 32; ++j) {
+                    float s = __uint_as_float(v[j]);
+                    if (kFp8) s = (s * sc[c * 32 + j]) * qs;
+                    mask |= (s >= st.cut ? 1u : 0u) << j;
+                }
+                while (mask) {  // survivors are rare once a threshold exists
+                    const uint32_t j = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const uint64_t row = tile_row0 + c * 32 + j;
+                    if (row >= row_end) continue;
+                    float s = pick(v, j);
+                    if (kFp8) s = (s * sc[c * 32 + j]) * qs;
+                    const float u = fmaf(p.row_resid[row], b_mul, s + b_add);
+                    epi_survivor<kMode>(p, st, heap, lrow, q, u, row, slack);
+                }
+            };
+#pragma unroll
+            for (uint32_t c = 0; c < kN / 32; c += 2) {
+                __syncwarp();
+                tc::tmem_ld32(taddr + (c + 1) * 32, vb);
+                process(va, c);
+                tmem_wait_ld_regs(vb);
+                if (c + 2 < kN / 32) {
+                    __syncwarp();
+                    tc::tmem_ld32(taddr + (c + 2) * 32, va);
+                }
+                process(vb, c + 1);
+                if (c + 2 < kN / 32) tmem_wait_ld_regs(va);
             }
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[buf]);
         }
-        if (valid_q) {
-            uint64_t* dst = ws_keys + (static_cast<size_t>(q) * nranges + range) * kprime;
-            for (uint32_t i = 0; i < kprime; ++i) dst[i] = i < n ? heap[i * kM + lrow] : 0ull;
-            if (n == kprime) atomicMax(&thr_global[q], static_cast<unsigned long long>(heap[lrow]));
+        if (kMode == 0 && valid_q) {
+            uint64_t* dst = p.ws_keys + (static_cast<size_t>(q) * nranges + range) * p.kprime;
+            for (uint32_t i = 0; i < p.kprime; ++i) dst[i] = i < st.n ? heap[i * kM + lrow] : 0ull;
+            if (st.n == p.kprime) atomicMax(&p.thr_global[q], static_cast<unsigned long long>(heap[lrow]));
         }
     }
     // ---------------- teardown: release TMEM ----------------
@@ -307,22 +381,44 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // ------------------------------------------------------------------------------------------
-// K4: exact FP32 rerank of the k′ candidates + top-k + certificate. One block per query.
-//
-// Each candidate's FP32 dot product is computed in exactly the order of the FP32 scan
-// (scan_fp32.cu): eight chains, one per 16-byte chunk position ch of each 128-byte slab, each
-// accumulating its chunk's four products slab by slab with FMA; then ((c0+c1)+(c2+c3)) +
-// ((c4+c5)+(c6+c7)). So a query's scores are bit-identical whichever path scored it.
+// Exact FP32 dot product in the order of the FP32 scan (scan_fp32.cu): eight chains, one per
+// 16-byte chunk position ch of each 128-byte slab, each accumulating its chunk's four products slab
+// by slab with FMA; then ((c0+c1)+(c2+c3)) + ((c4+c5)+(c6+c7)). Called by 8 consecutive lanes (one
+// per ch); every lane returns the full sum. So a query's scores are bit-identical on every path.
+// ------------------------------------------------------------------------------------------
+NNDEX_DEVICE_INLINE float dot_scan_order(const float* __restrict__ x, const float* __restrict__ y, uint32_t nbox,
+                                         uint32_t ch, bool live) {
+    float acc = 0.0f;
+    if (live) {
+        const float* xa = x + ch * 4;
+        const float* ya = y + ch * 4;
+        for (uint32_t bx = 0; bx < nbox; ++bx) {
+            const float4 a = *reinterpret_cast<const float4*>(xa + bx * 32);
+            const float4 b = *reinterpret_cast<const float4*>(ya + bx * 32);
+            acc = fmaf(a.x, b.x, acc);
+            acc = fmaf(a.y, b.y, acc);
+            acc = fmaf(a.z, b.z, acc);
+            acc = fmaf(a.w, b.w, acc);
+        }
+    }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+    return acc;
+}
+
+// ------------------------------------------------------------------------------------------
+// K4 (pass 1): exact FP32 rerank of the k′ candidates + top-k + certificate + T. One block per query.
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
     rerank_kernel(const float* __restrict__ base, uint32_t ds, const float* __restrict__ queries,
                   const uint64_t* __restrict__ cand_idx, const float* __restrict__ cand_bound,
                   const uint32_t* __restrict__ cand_cnt, uint32_t kp, uint32_t k, uint64_t* __restrict__ idx_out,
-                  float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out, uint32_t* __restrict__ cert_out) {
+                  float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out, uint32_t* __restrict__ cert_out,
+                  float* __restrict__ kth_out) {
     extern __shared__ uint64_t keys[];
     const uint32_t q = blockIdx.x;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t ch = lane & 7u, slot = threadIdx.x >> 3;  // 8 lanes per candidate
+    const uint32_t ch = threadIdx.x & 7u, slot = threadIdx.x >> 3;  // 8 lanes per candidate
     const uint32_t nslots = blockDim.x >> 3;
     const uint32_t n = cand_cnt[q] < kp ? cand_cnt[q] : kp;
     uint32_t p2 = 1;
@@ -332,24 +428,8 @@ __global__ void __launch_bounds__(256)
     for (uint32_t j0 = 0; j0 < p2; j0 += nslots) {
         const uint32_t j = j0 + slot;
         const bool live = j < n;
-        float acc = 0.0f;
-        uint64_t row = 0;
-        if (live) {
-            row = cand_idx[static_cast<size_t>(q) * kp + j];
-            const float* x = base + row * ds + ch * 4;
-            const float* y = qv + ch * 4;
-            for (uint32_t bx = 0; bx < nbox; ++bx) {
-                const float4 a = *reinterpret_cast<const float4*>(x + bx * 32);
-                const float4 b = *reinterpret_cast<const float4*>(y + bx * 32);
-                acc = fmaf(a.x, b.x, acc);
-                acc = fmaf(a.y, b.y, acc);
-                acc = fmaf(a.z, b.z, acc);
-                acc = fmaf(a.w, b.w, acc);
-            }
-        }
-        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+        const uint64_t row = live ? cand_idx[static_cast<size_t>(q) * kp + j] : 0;
+        const float acc = dot_scan_order(base + row * ds, qv, nbox, ch, live);
         if (ch == 0 && j < p2) keys[j] = live ? make_key(acc, static_cast<uint32_t>(row)) : 0ull;
     }
     __syncthreads();
@@ -366,38 +446,120 @@ __global__ void __launch_bounds__(256)
         uint32_t ok = 1;
         if (n >= kp && kk > 0) ok = key_score(keys[kk - 1]) > cand_bound[static_cast<size_t>(q) * kp + kp - 1] ? 1u : 0u;
         cert_out[q] = ok;
+        kth_out[q] = kk > 0 ? key_score(keys[kk - 1]) : -INFINITY;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Pass-2 helpers: gather the uncertified queries into a compact block, then rerank their
+// threshold-collected rows exactly and write the top-k into their own output slots.
+// ------------------------------------------------------------------------------------------
+__global__ void gather_queries_kernel(const uint32_t* __restrict__ ids, uint32_t m, const uint8_t* __restrict__ q_lp,
+                                      uint32_t row_bytes, uint8_t* __restrict__ q2_lp, const float* __restrict__ resid,
+                                      float* __restrict__ resid2, const float* __restrict__ scale,
+                                      float* __restrict__ scale2, const float* __restrict__ kth,
+                                      float* __restrict__ thr2) {
+    const uint32_t i = blockIdx.x;
+    if (i >= m) return;
+    const uint32_t src = ids[i];
+    const uint4* a = reinterpret_cast<const uint4*>(q_lp + static_cast<size_t>(src) * row_bytes);
+    uint4* b = reinterpret_cast<uint4*>(q2_lp + static_cast<size_t>(i) * row_bytes);
+    for (uint32_t t = threadIdx.x; t < row_bytes / 16; t += blockDim.x) b[t] = a[t];
+    if (threadIdx.x == 0) {
+        resid2[i] = resid[src];
+        if (scale) scale2[i] = scale[src];
+        thr2[i] = kth[src];
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    rerank_collected_kernel(const float* __restrict__ base, uint32_t ds, const float* __restrict__ queries,
+                            const uint32_t* __restrict__ ids, const uint32_t* __restrict__ rows2,
+                            const uint32_t* __restrict__ cnt2, uint32_t cap2, uint32_t k, uint64_t* __restrict__ idx_out,
+                            float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out,
+                            uint32_t* __restrict__ ok_out) {
+    extern __shared__ uint64_t keys[];
+    __shared__ BlockSelectScratch sel;
+    const uint32_t i = blockIdx.x;
+    const uint32_t q = ids[i];
+    const uint32_t total = cnt2[i];
+    if (total > cap2) {  // the collected set overflowed: this query goes to the FP32 scan
+        if (threadIdx.x == 0) ok_out[i] = 0;
+        return;
+    }
+    const uint32_t n = total;
+    const uint32_t ch = threadIdx.x & 7u, slot = threadIdx.x >> 3, nslots = blockDim.x >> 3;
+    const float* qv = queries + static_cast<size_t>(q) * ds;
+    const uint32_t nbox = ds / 32;
+    for (uint32_t j0 = 0; j0 < n; j0 += nslots) {
+        const uint32_t j = j0 + slot;
+        const bool live = j < n;
+        const uint64_t row = live ? rows2[static_cast<size_t>(i) * cap2 + j] : 0;
+        const float acc = dot_scan_order(base + row * ds, qv, nbox, ch, live);
+        if (ch == 0 && live) keys[j] = make_key(acc, static_cast<uint32_t>(row));
+    }
+    __syncthreads();
+    const uint32_t kk = n < k ? n : k;
+    uint64_t kth = 1;
+    if (n > kk && kk > 0) kth = block_radix_kth(keys, n, kk, sel);
+    // Keep the kk best in place (order does not matter yet), then sort them.
+    if (threadIdx.x == 0) sel.count = 0;
+    __syncthreads();
+    for (uint32_t j0 = 0; j0 < n; j0 += blockDim.x) {
+        const uint32_t j = j0 + threadIdx.x;
+        const uint64_t key = j < n ? keys[j] : 0ull;
+        __syncthreads();
+        if (j < n && key >= kth) {
+            const uint32_t pos = atomicAdd(&sel.count, 1u);
+            keys[pos] = key;  // pos ≤ j: never overwrites a key not yet read
+        }
+        __syncthreads();
+    }
+    uint32_t p2 = 1;
+    while (p2 < kk) p2 <<= 1;
+    for (uint32_t j = kk + threadIdx.x; j < p2; j += blockDim.x) keys[j] = 0ull;
+    block_bitonic_sort_desc(keys, p2);
+    for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
+        idx_out[static_cast<size_t>(q) * k + j] = j < kk ? key_row(keys[j]) : 0;
+        sim_out[static_cast<size_t>(q) * k + j] = j < kk ? key_score(keys[j]) : 0.0f;
+    }
+    if (threadIdx.x == 0) {
+        if (cnt_out) cnt_out[q] = kk;
+        ok_out[i] = 1;
     }
 }
 
 // ------------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------------
-template <bool kFp8, int kST>
+template <bool kFp8, int kST, int kMode>
 static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
-    auto kern = scan_tc_kernel<kFp8, kST>;
-    const size_t smem = tc_smem_bytes(a.nchunks, a.kprime, kST, kFp8);
+    auto kern = scan_tc_kernel<kFp8, kST, kMode>;
+    const uint32_t kp = kMode == 0 ? a.p.kprime : 0;
+    const size_t smem = tc_smem_bytes(a.p.nchunks, kp, kST, kFp8);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    dim3 grid((a.nq + kM - 1) / kM, a.nranges);
-    kern<<<grid, kThreads, smem, stream>>>(*a.tmap_q, *a.tmap_b, a.nq, a.nchunks, a.rows, a.range_rows, a.kprime,
-                                            a.row_scale, a.q_scale, a.row_resid, a.q_resid, a.eps_acc, a.thr_global,
-                                            a.ws_keys, a.status);
+    dim3 grid((a.p.nq + kM - 1) / kM, a.nranges);
+    TcParams p = a.p;
+    p.kprime = kp;
+    kern<<<grid, kThreads, smem, stream>>>(*a.tmap_q, *a.tmap_b, p);
     count_launch();
     return cudaGetLastError();
 }
 
-template <bool kFp8>
+template <bool kFp8, int kMode>
 static cudaError_t launch_tc_stages(const TcArgs& a, cudaStream_t stream) {
     switch (a.stages) {
-        case 4: return launch_tc_impl<kFp8, 4>(a, stream);
-        case 3: return launch_tc_impl<kFp8, 3>(a, stream);
-        case 2: return launch_tc_impl<kFp8, 2>(a, stream);
+        case 4: return launch_tc_impl<kFp8, 4, kMode>(a, stream);
+        case 3: return launch_tc_impl<kFp8, 3, kMode>(a, stream);
+        case 2: return launch_tc_impl<kFp8, 2, kMode>(a, stream);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, cudaStream_t stream) {
-    return fp8 ? launch_tc_stages<true>(a, stream) : launch_tc_stages<false>(a, stream);
+cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t stream) {
+    if (mode == 0) return fp8 ? launch_tc_stages<true, 0>(a, stream) : launch_tc_stages<false, 0>(a, stream);
+    return fp8 ? launch_tc_stages<true, 1>(a, stream) : launch_tc_stages<false, 1>(a, stream);
 }
 
 cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream) {
@@ -405,7 +567,33 @@ cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream) {
     while (p2 < a.kp) p2 <<= 1;
     rerank_kernel<<<a.nq, 256, p2 * sizeof(uint64_t), stream>>>(a.base, a.ds, a.queries, a.cand_idx, a.cand_sim,
                                                                a.cand_cnt, a.kp, a.k, a.idx_out, a.sim_out,
-                                                               a.cnt_out, a.cert_out);
+                                                               a.cnt_out, a.cert_out, a.kth_out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q_lp, uint32_t row_bytes, void* q2_lp,
+                                  const float* resid, float* resid2, const float* scale, float* scale2,
+                                  const float* kth, float* thr2, cudaStream_t stream) {
+    if (m == 0) return cudaSuccess;
+    gather_queries_kernel<<<m, 128, 0, stream>>>(ids, m, static_cast<const uint8_t*>(q_lp), row_bytes,
+                                                 static_cast<uint8_t*>(q2_lp), resid, resid2, scale, scale2, kth, thr2);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float* queries, const uint32_t* ids,
+                                    uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
+                                    uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
+                                    cudaStream_t stream) {
+    if (m == 0) return cudaSuccess;
+    uint32_t p2 = 1;
+    while (p2 < cap2) p2 <<= 1;
+    const size_t smem = std::max<size_t>(p2, 2 * k) * sizeof(uint64_t);
+    auto kern = rerank_collected_kernel;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    kern<<<m, 256, smem, stream>>>(base, ds, queries, ids, rows2, cnt2, cap2, k, idx_out, sim_out, cnt_out, ok_out);
     count_launch();
     return cudaGetLastError();
 }
