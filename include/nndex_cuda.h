@@ -110,7 +110,7 @@ typedef struct nndex_cuda_search_stats {
     uint64_t rows_scanned;     /* base rows scored (sum over queries for IVF)               */
     double   device_ms;        /* CUDA-event time of the device part of the call            */
     uint32_t fp32_fallback_queries; /* queries re-run on the FP32 scan (pass-2 overflow)   */
-    uint32_t reserved;
+    uint32_t pass1_tile_stride;     /* first pass scanned every n-th 256-row tile (1 = all) */
 } nndex_cuda_search_stats;
 
 /* ---- errors ---------------------------------------------------------------------------- */

@@ -77,7 +77,7 @@ class SearchStats(C.Structure):
         ("rows_scanned", C.c_uint64),
         ("device_ms", C.c_double),
         ("fp32_fallback_queries", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("pass1_tile_stride", C.c_uint32),
     ]
 
 

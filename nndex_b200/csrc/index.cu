@@ -393,6 +393,9 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     uint64_t nranges = 0, range_rows = 0;
     tc_ranges(nqb, nranges, range_rows);
     const uint64_t per_query = nranges * kp;
+    // Autotuned: when the last batch rarely certified in pass 1, pass 1 only has to produce each
+    // query's threshold T, and a sample of the rows (every 8th tile) gives a valid one.
+    const uint32_t stride = (tc_sample_stride > 1 && rows >= 256ull * 64) ? tc_sample_stride : 1;
     if ((st = grow_device(d_thr, cap_thr, n, "tc workspace"))) return st;
     if ((st = grow_device(d_ws, cap_ws, per_query * n, "tc workspace"))) return st;
     if ((st = grow_device(d_cand_idx, cap_cand_idx, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
@@ -415,6 +418,9 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     a.p.kprime = kp;
     a.p.thr_global = d_thr;
     a.p.ws_keys = d_ws;
+    a.p.tile_stride = stride;
+    last_tc_stride = stride;
+    stats.pass1_tile_stride = stride;
     cudaEvent_t ev_a = nullptr;
     scan_event_begin(s, ev_a);
     cudaError_t e = launch_scan_tc(a, fp8, 0, s);
@@ -445,6 +451,7 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     r.cnt_out = o_cnt;
     r.cert_out = d_cert;
     r.kth_out = d_kth;
+    r.certify = stride == 1;
     if ((e = launch_rerank(r, s)) != cudaSuccess) return cuda_error(e, "rerank launch");
     stats.kernel_launches += 3;
     stats.path = fp8 ? 3 : 2;
@@ -509,6 +516,9 @@ int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_si
         if (!h_cert[i]) h_ids[m++] = i;
     stats.certified = m == 0 ? 1u : 0u;
     stats.second_pass_queries = m;
+    // Autotune pass 1 for the next batch: a full pass 1 pays off only when it certifies most queries.
+    if (last_tc_stride == 1) tc_sample_stride = (m * 2 > n) ? 8u : 1u;
+    else if (m * 2 <= n) tc_sample_stride = 1;
     if (m == 0) return NNDEX_OK;
 
     // ---- pass 2 ----

@@ -84,6 +84,8 @@ struct CudaIndex {
     uint32_t* d_fb_cnt = nullptr;
     size_t cap_fb_cnt = 0;
     uint32_t last_tc_n = 0;  // queries of the last tensor-core batch (diagnostics)
+    uint32_t tc_sample_stride = 1;  // autotuned pass-1 tile stride (1 = full pass 1)
+    uint32_t last_tc_stride = 1;
     float* d_kth = nullptr;  // pass 1: exact k-th score per query
     size_t cap_kth = 0;
     // pass 2 (threshold collection) buffers

@@ -81,6 +81,7 @@ struct TcParams {
     uint32_t cap2 = 0;                    // pass 2 rows collected per query
     uint64_t rows = 0;
     uint64_t range_rows = 0;              // rows per CTA range (multiple of 256)
+    uint32_t tile_stride = 1;             // scan every tile_stride-th 256-row tile (pass-1 sampling)
     const float* row_scale = nullptr;     // FP8 only
     const float* q_scale = nullptr;       // FP8 only
     const float* row_resid = nullptr;     // ‖x − x̂‖ per row
@@ -119,6 +120,7 @@ struct RerankArgs {
     uint32_t* cnt_out = nullptr;
     uint32_t* cert_out = nullptr;
     float* kth_out = nullptr;            // exact k-th score per query (pass-2 threshold)
+    bool certify = true;                 // false when pass 1 scanned a sample of the rows
 };
 cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream);
 cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q_lp, uint32_t row_bytes, void* q2_lp,

@@ -172,7 +172,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t range = blockIdx.y, nranges = gridDim.y;
     const uint64_t row_begin = static_cast<uint64_t>(range) * p.range_rows;
     const uint64_t row_end = (row_begin + p.range_rows) < p.rows ? (row_begin + p.range_rows) : p.rows;
-    const uint32_t ntiles = row_end > row_begin ? static_cast<uint32_t>((row_end - row_begin + kN - 1) / kN) : 0;
+    const uint64_t tile_step = static_cast<uint64_t>(kN) * p.tile_stride;
+    const uint32_t ntiles =
+        row_end > row_begin ? static_cast<uint32_t>((row_end - row_begin + tile_step - 1) / tile_step) : 0;
     const uint32_t nchunks = p.nchunks;
 
     if (threadIdx.x == 0) {
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint32_t it = 0;
             bool stop = false;
             for (uint32_t t = 0; t < ntiles && !stop; ++t) {
-                const int32_t y = static_cast<int32_t>(row_begin + static_cast<uint64_t>(t) * kN);
+                const int32_t y = static_cast<int32_t>(row_begin + static_cast<uint64_t>(t) * tile_step);
                 for (uint32_t c = 0; c < nchunks; ++c) {
                     const uint32_t s = it % kST, u = it / kST;
                     if (u > 0 && !mbar_wait_bounded(&empty_bar[s], (u - 1) & 1u, kWaitBudgetCycles)) {
@@ -301,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t taddr0 = tmem_base + ((quarter * 32u) << 16);
         for (uint32_t t = 0; t < ntiles; ++t) {
             const uint32_t buf = t & 1u, ub = t >> 1;
-            const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * kN;
+            const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * tile_step;
             const float* sc = scale_s + (t & 1u) * kN;
             if (kFp8) {
                 // Row scales of this tile, shared by the 128 queries (each applies its own scale).
@@ -415,7 +417,7 @@ __global__ void __launch_bounds__(256)
                   const uint64_t* __restrict__ cand_idx, const float* __restrict__ cand_bound,
                   const uint32_t* __restrict__ cand_cnt, uint32_t kp, uint32_t k, uint64_t* __restrict__ idx_out,
                   float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out, uint32_t* __restrict__ cert_out,
-                  float* __restrict__ kth_out) {
+                  float* __restrict__ kth_out, int certify) {
     extern __shared__ uint64_t keys[];
     const uint32_t q = blockIdx.x;
     const uint32_t ch = threadIdx.x & 7u, slot = threadIdx.x >> 3;  // 8 lanes per candidate
@@ -443,8 +445,9 @@ __global__ void __launch_bounds__(256)
         if (cnt_out) cnt_out[q] = kk;
         // Every row outside the k′ candidates has an exact score ≤ the k′-th upper bound; an exact
         // k-th score above it proves the top-k exact.
-        uint32_t ok = 1;
-        if (n >= kp && kk > 0) ok = key_score(keys[kk - 1]) > cand_bound[static_cast<size_t>(q) * kp + kp - 1] ? 1u : 0u;
+        uint32_t ok = certify ? 1u : 0u;
+        if (certify && n >= kp && kk > 0)
+            ok = key_score(keys[kk - 1]) > cand_bound[static_cast<size_t>(q) * kp + kp - 1] ? 1u : 0u;
         cert_out[q] = ok;
         kth_out[q] = kk > 0 ? key_score(keys[kk - 1]) : -INFINITY;
     }
@@ -567,7 +570,7 @@ cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream) {
     while (p2 < a.kp) p2 <<= 1;
     rerank_kernel<<<a.nq, 256, p2 * sizeof(uint64_t), stream>>>(a.base, a.ds, a.queries, a.cand_idx, a.cand_sim,
                                                                a.cand_cnt, a.kp, a.k, a.idx_out, a.sim_out,
-                                                               a.cnt_out, a.cert_out, a.kth_out);
+                                                               a.cnt_out, a.cert_out, a.kth_out, a.certify ? 1 : 0);
     count_launch();
     return cudaGetLastError();
 }
