@@ -244,6 +244,10 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     seed = replica_seed(args.seed, rank)
     L = _lib.lib()
+    if args.mixed == "only":
+        # the mixed-precision section alone (profiling runs of the tensor-core scan)
+        mixed = run_mixed(args, dev, L, world)
+        return {"mixed_precision": mixed} if rank == 0 else None
 
     base = make_mixture(args.rows, args.dims, args.centers, args.sigma, seed, dev, center_seed=args.seed)
     opts = _lib.Opts()
