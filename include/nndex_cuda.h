@@ -113,6 +113,20 @@ typedef struct nndex_cuda_search_stats {
     uint32_t pass1_tile_stride;     /* first pass scanned every n-th 256-row tile (1 = all) */
 } nndex_cuda_search_stats;
 
+/* IVF build statistics (approximate mode; zero when the index has no IVF). */
+typedef struct nndex_cuda_ivf_stats {
+    uint64_t nlist;            /* clusters                                                   */
+    uint64_t iters;            /* k-means iterations run                                     */
+    uint64_t max_list;         /* rows of the largest cluster                                */
+    double   build_ms;         /* whole build, device time                                   */
+    double   seed_ms;          /* medoid + k-means++ seeding                                 */
+    double   kmeans_ms;        /* the k-means iterations                                     */
+    double   layout_ms;        /* list layout: reordered rows, row map, offsets              */
+    uint64_t seed_exact_rows;  /* rows whose seeding distance was computed exactly           */
+    uint64_t ambiguous_rows;   /* assignments resolved by the exact FP64 pass (all iters)    */
+    uint64_t reserved[4];
+} nndex_cuda_ivf_stats;
+
 /* ---- errors ---------------------------------------------------------------------------- */
 
 /* Message of the last failed call on this thread, formatted like NNdexError's Display
@@ -238,12 +252,26 @@ NNDEX_API uint64_t nndex_cuda_kernel_launch_count(void);
  * file-scope device array of NNDEX_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
  * until exit; a batch whose normalised queries and candidate keys do not fit is rejected with
  * NNDEX_ERR_UNSUPPORTED. The first call on a device looks up the array's address (make it before
- * any stream capture). All calls share the array: calls that overlap on the GPU race.
+ * any stream capture). All calls share the array: calls that overlap on the GPU race. Indexes that
+ * answer through an IVF (NNDEX_FLAG_APPROX) are rejected with NNDEX_ERR_UNSUPPORTED.
  */
 NNDEX_API int nndex_cuda_search_batch_device_noalloc(nndex_cuda_index* index, const float* dev_queries,
                                                      uint64_t query_rows, uint64_t query_dims, uint64_t k,
                                                      uint64_t* dev_idx_out, float* dev_sim_out,
                                                      uint32_t* dev_counts_out, void* stream);
+
+/* ---- IVF layout (approximate mode) --------------------------------------------------------- */
+
+/*
+ * The IVF built for an index created with NNDEX_FLAG_APPROX, as ApproxIndex holds it
+ * (src/approx.rs:11-25). *nlist_out is always written (0 = no IVF: the index answers approx
+ * searches exactly, as the reference does when the IVF gives no speedup, src/cpu.rs:399-407).
+ * Each array may be NULL; otherwise it must hold: centroids nlist × padded_dims floats,
+ * offsets nlist + 1, original_indices rows, init_rows nlist (the rows k-means++ picked).
+ */
+NNDEX_API int nndex_cuda_ivf_layout(nndex_cuda_index* index, uint64_t* nlist_out, float* centroids,
+                                    uint64_t* offsets, uint64_t* original_indices, uint64_t* init_rows);
+NNDEX_API int nndex_cuda_ivf_stats_get(const nndex_cuda_index* index, nndex_cuda_ivf_stats* out);
 
 /* ---- FP64 oracle on the device (score-error report) ------------------------------------- */
 

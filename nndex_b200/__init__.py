@@ -222,6 +222,32 @@ class NNdex:
         _check(_lib.lib().nndex_cuda_last_search_stats(self._h, C.byref(s)))
         return {f: getattr(s, f) for f, _ in _lib.SearchStats._fields_}
 
+    def ivf_layout(self) -> dict | None:
+        """The IVF of an approx index as ApproxIndex holds it (src/approx.rs:11-25), or None.
+
+        Keys: centroids [nlist × padded_dims] f32, cluster_offsets [nlist + 1], original_indices
+        [rows] (reordered position → original row), init_rows [nlist] (the rows k-means++ picked).
+        """
+        L = _lib.lib()
+        n = C.c_uint64(0)
+        _check(L.nndex_cuda_ivf_layout(self._h, C.byref(n), None, None, None, None))
+        if n.value == 0:
+            return None
+        nl = n.value
+        pd = (self._dims + 7) // 8 * 8
+        cent = np.zeros((nl, pd), dtype=np.float32)
+        off = np.zeros(nl + 1, dtype=np.uint64)
+        orig = np.zeros(self._rows, dtype=np.uint64)
+        init = np.zeros(nl, dtype=np.uint64)
+        _check(L.nndex_cuda_ivf_layout(self._h, C.byref(n), cent.ctypes.data, off.ctypes.data, orig.ctypes.data,
+                                       init.ctypes.data))
+        return {"centroids": cent, "cluster_offsets": off, "original_indices": orig, "init_rows": init}
+
+    def ivf_stats(self) -> dict:
+        s = _lib.IvfStats()
+        _check(_lib.lib().nndex_cuda_ivf_stats_get(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in _lib.IvfStats._fields_ if f != "reserved"}
+
     # ---- search (src/python_bindings.rs:125-236) ----
     def _search_single(self, q: np.ndarray, k: int):
         k = int(k)

@@ -81,6 +81,21 @@ class SearchStats(C.Structure):
     ]
 
 
+class IvfStats(C.Structure):
+    _fields_ = [
+        ("nlist", C.c_uint64),
+        ("iters", C.c_uint64),
+        ("max_list", C.c_uint64),
+        ("build_ms", C.c_double),
+        ("seed_ms", C.c_double),
+        ("kmeans_ms", C.c_double),
+        ("layout_ms", C.c_double),
+        ("seed_exact_rows", C.c_uint64),
+        ("ambiguous_rows", C.c_uint64),
+        ("reserved", C.c_uint64 * 4),
+    ]
+
+
 _vp = C.c_void_p
 _u64 = C.c_uint64
 _u32 = C.c_uint32
@@ -107,6 +122,8 @@ SIGNATURES = {
     "nndex_cuda_scan_timing": (_i32, [_vp, C.POINTER(C.c_double), C.POINTER(_u64)]),
     "nndex_cuda_fp64_scores": (_i32, [_vp, _vp, _u64, _vp, _vp, _u64, _vp]),
     "nndex_cuda_search_batch_device_noalloc": (_i32, [_vp, _vp, _u64, _u64, _u64, _vp, _vp, _vp, _vp]),
+    "nndex_cuda_ivf_layout": (_i32, [_vp, C.POINTER(_u64), _vp, _vp, _vp, _vp]),
+    "nndex_cuda_ivf_stats_get": (_i32, [_vp, C.POINTER(IvfStats)]),
 }
 
 NNDEX_NOALLOC_SCRATCH_BYTES = 16 << 20

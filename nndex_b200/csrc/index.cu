@@ -356,7 +356,7 @@ int CudaIndex::enqueue_prep_queries(const float* d_raw, uint64_t n, int mode, in
     p.mode = mode;
     p.err = d_err;
     p.sm_count = sm_count;
-    if (path >= 2) {
+    if (path == 2 || path == 3) {
         const uint64_t nq_alloc = (n + 127) / 128 * 128;
         if ((st = grow_device(d_q_resid, cap_q_resid, n, "query buffer"))) return st;
         if (path == 2) {
@@ -616,7 +616,7 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
     const uint64_t chunk = kMaxBatchChunk;
     for (uint64_t q0 = 0; q0 < nq; q0 += chunk) {
         const uint64_t n = std::min<uint64_t>(chunk, nq - q0);
-        const int path = choose_path(n, kcap);
+        const int path = uses_ivf() ? 4 : choose_path(n, kcap);
         int st;
         if ((st = ensure_query_capacity(n))) return st;
         if ((st = ensure_result_capacity(n, kcap))) return st;
@@ -625,7 +625,11 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         cudaMemsetAsync(d_status, 0, sizeof(uint32_t), stream);
         cudaMemcpyAsync(d_qraw, h_q, n * dims * sizeof(float), cudaMemcpyHostToDevice, stream);
         if ((st = enqueue_prep_queries(d_qraw, n, mode, path, stream))) return st;
-        if (path == 1) {
+        if (path == 4) {
+            if ((st = ivf_search(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
+                                 stream)))
+                return st;
+        } else if (path == 1) {
             if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
                                          static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
                 return st;
@@ -645,6 +649,7 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_error(e, "search");
         if ((st = check_device_words())) return st;
+        if (path == 4) stats.rows_scanned += *ivf->h_probed;
         std::memcpy(idx_out + q0 * kcap, h_idx, n * kcap * sizeof(uint64_t));
         std::memcpy(sim_out + q0 * kcap, h_sim, n * kcap * sizeof(float));
         if (counts_out)
@@ -674,12 +679,14 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
     bool synced = false;
     for (uint64_t q0 = 0; q0 < nq; q0 += kMaxBatchChunk) {
         const uint64_t n = std::min<uint64_t>(kMaxBatchChunk, nq - q0);
-        const int path = choose_path(n, kcap);
+        const int path = uses_ivf() ? 4 : choose_path(n, kcap);
         if ((st = enqueue_prep_queries(d_queries + q0 * dims, n, normalized ? 2 : 0, path, s))) return st;
         uint64_t* oi = d_idx_out + q0 * kcap;
         float* os = d_sim_out + q0 * kcap;
         uint32_t* oc = d_cnt_out ? d_cnt_out + q0 : nullptr;
-        if (path == 1) {
+        if (path == 4) {
+            if ((st = ivf_search(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s))) return st;
+        } else if (path == 1) {
             if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
                                          static_cast<uint32_t>(kcap), oi, os, oc, s)))
                 return st;
@@ -698,6 +705,7 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
         mark_done(s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_error(e, "search");
+        if (uses_ivf()) stats.rows_scanned = *ivf->h_probed;
         return check_device_words();
     }
     mark_done(s);
@@ -935,6 +943,10 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
         !encode_tmap_2d(&ix->tmap_fp8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ix->d_base_fp8, ix->kf8, ix->rows_alloc,
                         ix->kf8, 128, 256, CU_TENSOR_MAP_SWIZZLE_128B))
         return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (FP8)"));
+    if (ix->approx) {
+        // src/approx.rs:46-100, built once at construction instead of on the first approx search.
+        if ((st = ivf_build(*ix)) != NNDEX_OK) return fail(st);
+    }
     *out = ix;
     return NNDEX_OK;
 }
@@ -1163,6 +1175,40 @@ int nndex_cuda_last_search_stats(const nndex_cuda_index* index, nndex_cuda_searc
     clear_error();
     if (!index || !out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null argument");
     *out = index->impl->stats;
+    return NNDEX_OK;
+}
+
+int nndex_cuda_ivf_layout(nndex_cuda_index* index, uint64_t* nlist_out, float* centroids, uint64_t* offsets,
+                          uint64_t* original_indices, uint64_t* init_rows) {
+    clear_error();
+    if (!index || !nlist_out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null argument");
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    *nlist_out = 0;
+    if (!ix->ivf) return NNDEX_OK;
+    const IvfIndex& v = *ix->ivf;
+    *nlist_out = v.nlist;
+    cudaSetDevice(ix->device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && centroids)
+        e = cudaMemcpy2D(centroids, ix->dp * sizeof(float), v.d_centroids, ix->ds * sizeof(float), ix->dp * sizeof(float),
+                         v.nlist, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && original_indices) {
+        std::vector<uint32_t> m(ix->rows);
+        e = cudaMemcpy(m.data(), v.d_row_map, ix->rows * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        for (uint64_t i = 0; i < ix->rows; ++i) original_indices[i] = m[i];
+    }
+    if (e != cudaSuccess) return cuda_error(e, "IVF layout copy");
+    if (offsets) std::copy(v.h_offsets.begin(), v.h_offsets.end(), offsets);
+    if (init_rows) std::copy(v.h_init_rows.begin(), v.h_init_rows.end(), init_rows);
+    return NNDEX_OK;
+}
+
+int nndex_cuda_ivf_stats_get(const nndex_cuda_index* index, nndex_cuda_ivf_stats* out) {
+    clear_error();
+    if (!index || !out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null argument");
+    const CudaIndex* ix = index->impl;
+    *out = ix->ivf ? ix->ivf->stats : nndex_cuda_ivf_stats{};
     return NNDEX_OK;
 }
 

@@ -1,12 +1,14 @@
 // index.h — the CUDA backend object behind the C ABI (one per NNdex built with the Cuda backend).
 #pragma once
 
+#include <memory>
 #include <mutex>
 #include <unordered_map>
 #include <utility>
 #include <vector>
 
 #include "internal.h"
+#include "ivf.h"
 
 namespace nndex {
 
@@ -138,6 +140,7 @@ struct CudaIndex {
     uint64_t* h_flags = nullptr;
 
     nndex_cuda_search_stats stats{};
+    std::unique_ptr<IvfIndex> ivf;  // approximate mode (NNDEX_FLAG_APPROX), built at creation
 
     // scan-kernel timing (roofline reports)
     bool scan_timing = false;
@@ -171,6 +174,8 @@ struct CudaIndex {
     // FP32 path (device outputs are patched in place). Synchronises the stream.
     int finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
     int stream_status();
+    // Approximate mode with an IVF that gives a speedup (src/approx.rs:35-37 provides_speedup).
+    bool uses_ivf() const { return approx && ivf && rows >= 256 && ivf->nlist >= 4; }
     void order_after_previous(cudaStream_t s);
     void mark_done(cudaStream_t s);
 };

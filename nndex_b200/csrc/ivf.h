@@ -1,0 +1,67 @@
+// ivf.h — the IVF (inverted file) index of nndex's approximate mode, built and searched on the GPU.
+//
+// Reference: ApproxIndex (src/approx.rs:11-25) — centroids [nlist × dims], the matrix reordered so
+// every cluster's rows are contiguous, original_indices (position → original row) and
+// cluster_offsets [nlist + 1]. Built by k-means++ seeding (src/approx.rs:357-429) and spherical
+// k-means (src/approx.rs:434-535); searched by probing the nprobe best clusters and reranking
+// their rows exactly (src/approx.rs:159-215, src/cpu.rs:425-502).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/nndex_cuda.h"
+
+namespace nndex {
+
+struct CudaIndex;
+
+struct IvfIndex {
+    uint64_t nlist = 0;          // clusters (1 = single-list index, never probed)
+    uint64_t iters = 0;          // k-means iterations
+    uint64_t nlist_pad = 0;      // nlist rounded up to 256 (assignment GEMM tiles, dims-major stride)
+    float* d_centroids = nullptr;  // nlist × ds FP32, final centroids (zero padded)
+    float* d_cent_t = nullptr;     // ds × nlist_pad FP32, the same centroids dims-major (probe)
+    float* d_reordered = nullptr;  // rows_alloc × ds FP32, cluster-contiguous copy of the base
+    uint32_t* d_row_map = nullptr; // rows: reordered position → original row
+    uint32_t* d_offsets = nullptr; // nlist + 1
+    std::vector<uint64_t> h_offsets;
+    std::vector<uint64_t> h_init_rows;  // rows chosen by k-means++ (diagnostics / parity)
+    uint64_t max_list = 0;
+    CUtensorMap tmap_reordered{};
+    nndex_cuda_ivf_stats stats{};
+
+    // search scratch (grown on demand)
+    uint32_t* d_probes = nullptr;       size_t cap_probes = 0;
+    uint32_t* d_list_cnt = nullptr;     size_t cap_list_cnt = 0;   // nlist: queries probing each list
+    uint32_t* d_list_fill = nullptr;    size_t cap_list_fill = 0;
+    uint32_t* d_list_qoff = nullptr;    size_t cap_list_qoff = 0;  // nlist + 1
+    uint32_t* d_item_off = nullptr;     size_t cap_item_off = 0;   // nlist + 1
+    uint32_t* d_list_q = nullptr;       size_t cap_list_q = 0;     // B·nprobe: query of each (list, query) pair
+    uint32_t* d_list_slot = nullptr;    size_t cap_list_slot = 0;  // B·nprobe: its first output slot
+    uint32_t* d_q_slot_off = nullptr;   size_t cap_q_slot_off = 0; // B + 1
+    unsigned long long* d_counters = nullptr; size_t cap_counters = 0;  // work counter, totals, rows probed
+    uint64_t* d_ws = nullptr;           size_t cap_ws = 0;         // slots × k keys
+    unsigned long long* h_probed = nullptr;  // pinned: Σ rows probed by the last search
+
+    ~IvfIndex();
+};
+
+// Builds the IVF of `ix` (k-means++ + spherical k-means + list layout) on the GPU. nlist, iters
+// and the seed come from ix.opts (0 = the reference's policy). Returns an NNDEX status.
+int ivf_build(CudaIndex& ix);
+
+// Enqueues the IVF search of `nq` normalised queries (ix.d_qn, stride ds) with capped k into the
+// device outputs (rows of `k` slots). Returns an NNDEX status.
+int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+               cudaStream_t s);
+
+// src/approx.rs:305-311 choose_nlist and 318-336 choose_nprobe.
+uint64_t ivf_choose_nlist(uint64_t rows);
+uint64_t ivf_choose_nprobe(uint64_t nlist, uint64_t k, uint64_t rows);
+
+}  // namespace nndex

@@ -57,6 +57,9 @@ int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, ui
     std::lock_guard<std::mutex> lock(ix->mu);
     cudaError_t e = cudaSetDevice(ix->device);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    if (ix->uses_ivf())
+        return set_error(NNDEX_ERR_UNSUPPORTED,
+                         "cuda execution error: the no-allocation entry point serves exact indexes only");
     if (!s) s = cudaStreamLegacy;
     ix->order_after_previous(s);
     const uint64_t kcap = std::min<uint64_t>(k, ix->rows);
