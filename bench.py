@@ -65,6 +65,21 @@ def parse_args(argv=None):
     p.add_argument("--mixed-k", type=int, default=10)
     p.add_argument("--mixed-steps", type=int, default=5)
     p.add_argument("--mixed-oracle-queries", type=int, default=32)
+    p.add_argument("--ivf", choices=["on", "off", "only"], default="on",
+                   help="also measure the IVF workload (GPU k-means build + probe + ragged list scan)")
+    p.add_argument("--ivf-rows", type=int, default=2_000_000)
+    p.add_argument("--ivf-dims", type=int, default=384)
+    p.add_argument("--ivf-centers", type=int, default=8192)
+    p.add_argument("--ivf-zipf", type=float, default=1.1)
+    p.add_argument("--ivf-sigma", type=float, default=0.25)
+    p.add_argument("--ivf-nlist", type=int, default=1414)
+    p.add_argument("--ivf-iters", type=int, default=10)
+    p.add_argument("--ivf-seed", type=int, default=42)
+    p.add_argument("--ivf-nprobe", default="8,32,64")
+    p.add_argument("--ivf-batch", type=int, default=1024)
+    p.add_argument("--ivf-k", type=int, default=10)
+    p.add_argument("--ivf-steps", type=int, default=10)
+    p.add_argument("--ivf-cpu-queries", type=int, default=64)
     return p.parse_args(argv)
 
 
@@ -113,17 +128,26 @@ def barrier(world: int):
 # synthetic data (seeded; generated on the GPU when one is present)
 # ---------------------------------------------------------------------------------------------
 
-def make_mixture(rows, dims, centers, sigma, seed, device, center_seed=None):
+def make_mixture(rows, dims, centers, sigma, seed, device, center_seed=None, zipf=None):
+    """Unit rows x = c_a + sigma·N(0, I), centres c ~ N(0, I); the centre a is uniform, or drawn with
+    power-law (Zipf, exponent `zipf`) cluster sizes."""
     import torch
     g = torch.Generator(device=device)
     g.manual_seed(center_seed if center_seed is not None else seed)
     c = torch.randn((centers, dims), generator=g, device=device, dtype=torch.float32)
+    w = None
+    if zipf:
+        w = torch.arange(1, centers + 1, device=device, dtype=torch.float64).pow(-float(zipf))
+        w = (w / w.sum()).float()
     g.manual_seed(seed + 1)
     out = torch.empty((rows, dims), device=device, dtype=torch.float32)
     step = 1 << 18
     for r0 in range(0, rows, step):
         r1 = min(rows, r0 + step)
-        a = torch.randint(0, centers, (r1 - r0,), generator=g, device=device)
+        if w is not None:
+            a = torch.multinomial(w, r1 - r0, replacement=True, generator=g)
+        else:
+            a = torch.randint(0, centers, (r1 - r0,), generator=g, device=device)
         x = torch.randn((r1 - r0, dims), generator=g, device=device, dtype=torch.float32)
         x.mul_(sigma).add_(c[a])
         x.div_(torch.linalg.vector_norm(x, dim=1, keepdim=True))
@@ -248,6 +272,9 @@ def run_ours(args):
         # the mixed-precision section alone (profiling runs of the tensor-core scan)
         mixed = run_mixed(args, dev, L, world)
         return {"mixed_precision": mixed} if rank == 0 else None
+    if args.ivf == "only":
+        ivf = run_ivf(args, dev, L, world)
+        return {"ivf": ivf} if rank == 0 else None
 
     base = make_mixture(args.rows, args.dims, args.centers, args.sigma, seed, dev, center_seed=args.seed)
     opts = _lib.Opts()
@@ -363,6 +390,7 @@ def run_ours(args):
     del qall
     torch.cuda.empty_cache()
     mixed = run_mixed(args, dev, L, world) if args.mixed != "off" else None
+    ivf = run_ivf(args, dev, L, world) if args.ivf != "off" else None
     if rank != 0:
         return None
     head = results[args.batch]
@@ -400,6 +428,7 @@ def run_ours(args):
         "clocks": clocks,
         "gpu_launches": launches,
         "mixed_precision": mixed,
+        "ivf": ivf,
         "batches": {str(bb): {"queries_per_s": r["queries_per_s"], "ms_per_step": r["ms_per_step"],
                               "scan_ms": r["scan_ms"],
                               "hbm_gbs": (args.rows * args.dims * 4 + bb * args.dims * 4 + bb * k * 12)
@@ -532,6 +561,153 @@ def run_mixed(args, dev, L, world):
                      "peak_bf16_tflops": bf16_peak[0], "frac_bf16": out["bf16"]["scan_tflops"] / bf16_peak[0],
                      "peak_kind": bf16_peak[1],
                      "flops": "2*N*D*(batch/pass1_tile_stride + second_pass_queries) per batch"},
+    }
+
+
+def run_ivf(args, dev, L, world):
+    """IVF ANN with exact rerank: the k-means build on the GPU, then probe + ragged list scan."""
+    import numpy as np
+    import torch
+    from nndex_b200 import _lib, kernel_launch_count
+    from nndex_b200._lib import NNDEX_FLAG_APPROX, NNDEX_FLAG_NORMALIZED
+    rank, _, local = dist_env()
+    seed = replica_seed(args.seed + 200, rank)
+    rows, dims, nq, k = args.ivf_rows, args.ivf_dims, args.ivf_batch, args.ivf_k
+    base = make_mixture(rows, dims, args.ivf_centers, args.ivf_sigma, seed, dev, center_seed=args.seed + 200,
+                        zipf=args.ivf_zipf)
+    q = make_mixture(nq, dims, args.ivf_centers, args.ivf_sigma, seed + 7, dev, center_seed=args.seed + 200,
+                     zipf=args.ivf_zipf)
+    opts = _lib.Opts()
+    opts.device = local
+    opts.nlist = args.ivf_nlist
+    opts.kmeans_iters = args.ivf_iters
+    opts.has_seed = 1
+    opts.seed = args.ivf_seed
+    h = C.c_void_p()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    st = L.nndex_cuda_create_from_device(base.data_ptr(), base.numel(), rows, dims,
+                                         NNDEX_FLAG_NORMALIZED | NNDEX_FLAG_APPROX, C.byref(opts), C.byref(h))
+    build_wall = time.perf_counter() - t0
+    if st != 0:
+        raise RuntimeError(_lib.last_error())
+    bst = _lib.IvfStats()
+    L.nndex_cuda_ivf_stats_get(h, C.byref(bst))
+    # exact reference results (the FP32 exact path, parity-tested against the FP64 oracle)
+    hx = C.c_void_p()
+    ox = _lib.Opts()
+    ox.device = local
+    if L.nndex_cuda_create_from_device(base.data_ptr(), base.numel(), rows, dims, NNDEX_FLAG_NORMALIZED,
+                                       C.byref(ox), C.byref(hx)) != 0:
+        raise RuntimeError(_lib.last_error())
+    stream = torch.cuda.current_stream(dev)
+    sptr = C.c_void_p(stream.cuda_stream)
+    ei = torch.empty((nq, k), dtype=torch.int64, device=dev)
+    es = torch.empty((nq, k), dtype=torch.float32, device=dev)
+    if L.nndex_cuda_search_batch_device(hx, q.data_ptr(), nq, dims, k, ei.data_ptr(), es.data_ptr(), None, sptr, 1):
+        raise RuntimeError(_lib.last_error())
+    ex0, ex1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ex0.record(stream)
+    L.nndex_cuda_search_batch_device(hx, q.data_ptr(), nq, dims, k, ei.data_ptr(), es.data_ptr(), None, sptr, 1)
+    ex1.record(stream)
+    torch.cuda.synchronize(dev)
+    exact_ms = ex0.elapsed_time(ex1)
+    L.nndex_cuda_destroy(hx)
+    exact_sets = [set(r) for r in ei.cpu().tolist()]
+    oi = torch.empty((nq, k), dtype=torch.int64, device=dev)
+    os_ = torch.empty((nq, k), dtype=torch.float32, device=dev)
+    cnt = torch.empty((nq,), dtype=torch.int32, device=dev)
+    stats = _lib.SearchStats()
+    peak, peak_kind = measured_peaks()
+    per = {}
+    layout = None
+    for np_ in [int(x) for x in args.ivf_nprobe.split(",") if x]:
+        L.nndex_cuda_set_nprobe(h, np_)
+        for _ in range(3):
+            if L.nndex_cuda_search_batch_device(h, q.data_ptr(), nq, dims, k, oi.data_ptr(), os_.data_ptr(),
+                                                cnt.data_ptr(), sptr, 1) != 0:
+                raise RuntimeError(_lib.last_error())
+        L.nndex_cuda_last_search_stats(h, C.byref(stats))
+        torch.cuda.synchronize(dev)
+        L.nndex_cuda_set_scan_timing(h, 1)
+        barrier(world)
+        n0 = kernel_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.ivf_steps):
+            L.nndex_cuda_search_batch_device(h, q.data_ptr(), nq, dims, k, oi.data_ptr(), os_.data_ptr(),
+                                             cnt.data_ptr(), sptr, 0)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        n1 = kernel_launch_count()
+        L.nndex_cuda_set_scan_timing(h, 0)
+        if L.nndex_cuda_stream_status(h) != 0:
+            raise RuntimeError(_lib.last_error())
+        ms = e0.elapsed_time(e1)
+        scan_ms = C.c_double(0.0)
+        scan_n = C.c_uint64(0)
+        L.nndex_cuda_scan_timing(h, C.byref(scan_ms), C.byref(scan_n))
+        max_ms, total_q = aggregate(ms, nq * args.ivf_steps, world, dev)
+        got = oi.cpu().tolist()
+        hits = sum(len(set(got[i]) & exact_sets[i]) for i in range(nq))
+        scan_avg = scan_ms.value / max(scan_n.value, 1)
+        streamed_b = stats.ivf_rows_streamed * dims * 4
+        union_b = stats.ivf_rows_union * dims * 4
+        per[str(np_)] = {
+            "queries_per_s": total_q / (max_ms / 1e3),
+            "ms_per_batch": max_ms / args.ivf_steps,
+            "recall_at_k_vs_exact": hits / (nq * k),
+            "rows_probed_per_query": stats.rows_scanned / nq,
+            "rows_streamed": stats.ivf_rows_streamed,
+            "rows_union": stats.ivf_rows_union,
+            "scan_ms": scan_avg,
+            "scan_gbs_streamed": streamed_b / (scan_avg / 1e3) / 1e9,
+            "scan_frac_of_hbm_streamed": streamed_b / (scan_avg / 1e3) / 1e9 / peak,
+            "scan_gbs_union": union_b / (scan_avg / 1e3) / 1e9,
+            "scan_fp32_tflops": 2.0 * stats.rows_scanned * dims / (scan_avg / 1e3) / 1e12,
+            "kernel_launches_per_batch": (n1 - n0) / args.ivf_steps,
+        }
+    # CPU baseline: the reference's IVF search restated (oracle/) on the same index, host threads.
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        n_lay = C.c_uint64(0)
+        L.nndex_cuda_ivf_layout(h, C.byref(n_lay), None, None, None, None)
+        nl = n_lay.value
+        cent = np.zeros((nl, (dims + 7) // 8 * 8), dtype=np.float32)
+        off = np.zeros(nl + 1, dtype=np.uint64)
+        orig = np.zeros(rows, dtype=np.uint64)
+        L.nndex_cuda_ivf_layout(h, C.byref(n_lay), cent.ctypes.data, off.ctypes.data, orig.ctypes.data, None)
+        storage = base.cpu().numpy()
+        if storage.shape[1] != cent.shape[1]:
+            storage = np.ascontiguousarray(np.pad(storage, ((0, 0), (0, cent.shape[1] - storage.shape[1]))))
+        ref = O.IvfIndex(storage, layout={"centroids": cent, "cluster_offsets": off, "original_indices": orig})
+        qs = q[:args.ivf_cpu_queries].cpu().numpy()
+        if qs.shape[1] != cent.shape[1]:
+            qs = np.ascontiguousarray(np.pad(qs, ((0, 0), (0, cent.shape[1] - qs.shape[1]))))
+        cpu = {}
+        for np_ in [int(x) for x in args.ivf_nprobe.split(",") if x]:
+            t0 = time.perf_counter()
+            ri, _, _ = ref.search(qs, k, np_)
+            dt = time.perf_counter() - t0
+            cpu[str(np_)] = {"queries_per_s": qs.shape[0] / dt, "cores": O.num_threads(),
+                             "sample": f"{qs.shape[0]} queries, same index (restated src/cpu.rs:456-502)"}
+        del ref, storage
+    L.nndex_cuda_destroy(h)
+    del base
+    torch.cuda.empty_cache()
+    return {
+        "workload": f"IVF top-{k}, base {rows}x{dims} ({args.ivf_centers}-centre Gaussian mixture, Zipf "
+                    f"s={args.ivf_zipf} sizes, sigma={args.ivf_sigma}, unit rows), nlist={args.ivf_nlist}, "
+                    f"{args.ivf_iters} k-means iterations, seed {args.ivf_seed}, batch {nq}",
+        "build": {"device_ms": bst.build_ms, "seed_ms": bst.seed_ms, "kmeans_ms": bst.kmeans_ms,
+                  "layout_ms": bst.layout_ms, "wall_s_with_upload": build_wall, "max_list": bst.max_list,
+                  "ambiguous_rows_all_iters": bst.ambiguous_rows, "seed_exact_rows": bst.seed_exact_rows},
+        "exact_fp32_ms_per_batch": exact_ms,
+        "by_nprobe": per,
+        "cpu_baseline": cpu,
+        "roofline": {"bound": "hbm", "kernel": "ivf_scan_kernel", "peak": peak, "peak_kind": peak_kind,
+                     "bytes": "rows_streamed * D * 4 per batch (a list is read once per group of queries)"},
     }
 
 

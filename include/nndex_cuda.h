@@ -111,6 +111,8 @@ typedef struct nndex_cuda_search_stats {
     double   device_ms;        /* CUDA-event time of the device part of the call            */
     uint32_t fp32_fallback_queries; /* queries re-run on the FP32 scan (pass-2 overflow)   */
     uint32_t pass1_tile_stride;     /* first pass scanned every n-th 256-row tile (1 = all) */
+    uint64_t ivf_rows_streamed;     /* IVF: rows read by the list scan (a list once per query group) */
+    uint64_t ivf_rows_union;        /* IVF: rows in the union of the probed lists               */
 } nndex_cuda_search_stats;
 
 /* IVF build statistics (approximate mode; zero when the index has no IVF). */
@@ -272,6 +274,9 @@ NNDEX_API int nndex_cuda_search_batch_device_noalloc(nndex_cuda_index* index, co
 NNDEX_API int nndex_cuda_ivf_layout(nndex_cuda_index* index, uint64_t* nlist_out, float* centroids,
                                     uint64_t* offsets, uint64_t* original_indices, uint64_t* init_rows);
 NNDEX_API int nndex_cuda_ivf_stats_get(const nndex_cuda_index* index, nndex_cuda_ivf_stats* out);
+/* Lists probed per query by later approx searches (0 = choose_nprobe, src/approx.rs:318-336);
+ * no counterpart in the reference, whose nprobe is always the policy's. */
+NNDEX_API int nndex_cuda_set_nprobe(nndex_cuda_index* index, uint32_t nprobe);
 
 /* ---- FP64 oracle on the device (score-error report) ------------------------------------- */
 

@@ -243,6 +243,10 @@ class NNdex:
                                        init.ctypes.data))
         return {"centroids": cent, "cluster_offsets": off, "original_indices": orig, "init_rows": init}
 
+    def set_nprobe(self, nprobe: int) -> None:
+        """Lists probed per query by later approx searches (0 = the reference's choose_nprobe)."""
+        _check(_lib.lib().nndex_cuda_set_nprobe(self._h, int(nprobe)))
+
     def ivf_stats(self) -> dict:
         s = _lib.IvfStats()
         _check(_lib.lib().nndex_cuda_ivf_stats_get(self._h, C.byref(s)))

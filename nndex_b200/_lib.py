@@ -78,6 +78,8 @@ class SearchStats(C.Structure):
         ("device_ms", C.c_double),
         ("fp32_fallback_queries", C.c_uint32),
         ("pass1_tile_stride", C.c_uint32),
+        ("ivf_rows_streamed", C.c_uint64),
+        ("ivf_rows_union", C.c_uint64),
     ]
 
 
@@ -124,6 +126,7 @@ SIGNATURES = {
     "nndex_cuda_search_batch_device_noalloc": (_i32, [_vp, _vp, _u64, _u64, _u64, _vp, _vp, _vp, _vp]),
     "nndex_cuda_ivf_layout": (_i32, [_vp, C.POINTER(_u64), _vp, _vp, _vp, _vp]),
     "nndex_cuda_ivf_stats_get": (_i32, [_vp, C.POINTER(IvfStats)]),
+    "nndex_cuda_set_nprobe": (_i32, [_vp, _u32]),
 }
 
 NNDEX_NOALLOC_SCRATCH_BYTES = 16 << 20

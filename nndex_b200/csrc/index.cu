@@ -649,7 +649,11 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_error(e, "search");
         if ((st = check_device_words())) return st;
-        if (path == 4) stats.rows_scanned += *ivf->h_probed;
+        if (path == 4) {
+            stats.rows_scanned += ivf->h_probed[0];
+            stats.ivf_rows_streamed += ivf->h_probed[1];
+            stats.ivf_rows_union += ivf->h_probed[2];
+        }
         std::memcpy(idx_out + q0 * kcap, h_idx, n * kcap * sizeof(uint64_t));
         std::memcpy(sim_out + q0 * kcap, h_sim, n * kcap * sizeof(float));
         if (counts_out)
@@ -705,7 +709,11 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
         mark_done(s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_error(e, "search");
-        if (uses_ivf()) stats.rows_scanned = *ivf->h_probed;
+        if (uses_ivf()) {
+            stats.rows_scanned = ivf->h_probed[0];
+            stats.ivf_rows_streamed = ivf->h_probed[1];
+            stats.ivf_rows_union = ivf->h_probed[2];
+        }
         return check_device_words();
     }
     mark_done(s);
@@ -801,6 +809,7 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
     if ((e = cudaMalloc(&ix->d_base, base_bytes)) != cudaSuccess) return fail(cuda_error(e, "base allocation"));
     cudaMemsetAsync(ix->d_base + rows * ix->ds, 0, (ix->rows_alloc - rows) * ix->ds * sizeof(float), ix->stream);
     cudaMemsetAsync(ix->d_err, 0xFF, sizeof(unsigned long long), ix->stream);
+    cudaMemsetAsync(ix->d_status, 0, sizeof(uint32_t), ix->stream);
     // Low-precision scoring copies (K1 writes them in the same pass) and their residual norms.
     float*& d_res16 = ix->d_res16;  // kept: the certificate's per-row bounds
     float*& d_res8 = ix->d_res8;
@@ -1201,6 +1210,16 @@ int nndex_cuda_ivf_layout(nndex_cuda_index* index, uint64_t* nlist_out, float* c
     if (e != cudaSuccess) return cuda_error(e, "IVF layout copy");
     if (offsets) std::copy(v.h_offsets.begin(), v.h_offsets.end(), offsets);
     if (init_rows) std::copy(v.h_init_rows.begin(), v.h_init_rows.end(), init_rows);
+    return NNDEX_OK;
+}
+
+int nndex_cuda_set_nprobe(nndex_cuda_index* index, uint32_t nprobe) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    ix->opts.nprobe = nprobe;
+    if (ix->ivf) ix->ivf->nprobe = nprobe;
     return NNDEX_OK;
 }
 

@@ -46,7 +46,8 @@ struct IvfIndex {
     uint32_t* d_q_slot_off = nullptr;   size_t cap_q_slot_off = 0; // B + 1
     unsigned long long* d_counters = nullptr; size_t cap_counters = 0;  // work counter, totals, rows probed
     uint64_t* d_ws = nullptr;           size_t cap_ws = 0;         // slots × k keys
-    unsigned long long* h_probed = nullptr;  // pinned: Σ rows probed by the last search
+    unsigned long long* h_probed = nullptr;  // pinned [3]: rows probed (Σ over queries), streamed, union
+    uint32_t nprobe = 0;                     // 0 = choose_nprobe per search
 
     ~IvfIndex();
 };

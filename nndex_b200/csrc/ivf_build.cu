@@ -952,6 +952,7 @@ int ivf_build(CudaIndex& ix) {
     IvfIndex& v = *ivf;
     v.nlist = nlist;
     v.iters = iters;
+    v.nprobe = ix.opts.nprobe;
     v.nlist_pad = (nlist + 255) / 256 * 256;
     const uint64_t kb = (ix.dims + 63) / 64 * 64;  // BF16 row length (64-element K slabs)
     BuildScratch tmp;
@@ -1007,6 +1008,7 @@ int ivf_build(CudaIndex& ix) {
         kern<<<static_cast<unsigned>(ds / 32), 64, smem, s>>>(ix.tmap_f32, rows, mean_f32, ix.d_status);
         count_launch();
         cudaMemsetAsync(best, 0, sizeof(unsigned long long), s);
+        cudaFuncSetAttribute(medoid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(ds * sizeof(float)));
         const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>((rows + 255) / 256, ix.sm_count * 8ull));
         medoid_kernel<<<blocks, 256, ds * sizeof(float), s>>>(ix.d_base, static_cast<uint32_t>(ds),
                                                                static_cast<uint32_t>(dp), rows, mean_f32, best);
@@ -1074,6 +1076,14 @@ int ivf_build(CudaIndex& ix) {
     const uint32_t nrt = static_cast<uint32_t>((rows + kAsM - 1) / kAsM);
     const uint32_t as_grid = std::min<uint32_t>(nrt, static_cast<uint32_t>(ix.sm_count));
     const uint32_t cp_blocks = static_cast<uint32_t>((nlist * 32 + 255) / 256);
+    cudaFuncSetAttribute(kmeans_assign_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(ds * sizeof(float)));
+    cudaFuncSetAttribute(cluster_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(nlist * sizeof(uint32_t)));
+    cudaFuncSetAttribute(cluster_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(nlist * sizeof(uint32_t)));
+    cudaFuncSetAttribute(centroid_normalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(ds * sizeof(double)));
     std::vector<uint32_t> h_amb(iters, 0);
     uint32_t* d_amb_hist = nullptr;
     if ((e = tmp.alloc(d_amb_hist, iters)) != cudaSuccess) return oom("IVF build scratch");

@@ -102,7 +102,8 @@ __global__ void __launch_bounds__(256)
 
 // ------------------------------------------------------------------------------------------
 // 2. Plan: one block.
-//    counters[0] work-item counter (the scan's), [1] items, [2] slots, [3] Σ rows probed.
+//    counters[0] work-item counter (the scan's), [1] items, [2] slots; summed over the sub-batches of
+//    a search: [3] Σ rows probed per query, [4] rows streamed by the scan, [5] rows of probed lists.
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024)
     ivf_plan_kernel(const uint32_t* __restrict__ probes, uint32_t nq, uint32_t np, uint32_t nlist,
@@ -131,11 +132,18 @@ __global__ void __launch_bounds__(1024)
     }
     atomicAdd(&probed, my_rows);
     __syncthreads();
+    unsigned long long my_stream = 0, my_union = 0;
     for (uint32_t l = threadIdx.x; l < nlist; l += blockDim.x) {
         const uint32_t c = list_cnt[l];
-        item_off[l] = chunks(l) * ((c + qb - 1) / qb);
+        const uint32_t groups = (c + qb - 1) / qb;
+        item_off[l] = chunks(l) * groups;
         list_qoff[l] = c;
+        const uint32_t len = offsets[l + 1] - offsets[l];
+        my_stream += static_cast<unsigned long long>(len) * groups;
+        my_union += c ? len : 0u;
     }
+    atomicAdd(&counters[4], my_stream);
+    atomicAdd(&counters[5], my_union);
     __syncthreads();
     block_exclusive_scan(list_qoff, nlist, part);
     block_exclusive_scan(item_off, nlist, part);
@@ -518,7 +526,7 @@ int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o
                cudaStream_t s) {
     IvfIndex& v = *ix.ivf;
     const uint32_t nlist = static_cast<uint32_t>(v.nlist);
-    uint64_t np64 = ix.opts.nprobe ? ix.opts.nprobe : ivf_choose_nprobe(v.nlist, k, ix.rows);
+    uint64_t np64 = v.nprobe ? v.nprobe : ivf_choose_nprobe(v.nlist, k, ix.rows);
     np64 = std::max<uint64_t>(1, std::min<uint64_t>(np64, v.nlist));
     const uint32_t np = static_cast<uint32_t>(np64);
     const uint32_t dq = static_cast<uint32_t>(ix.ds);
@@ -546,7 +554,7 @@ int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o
     if ((st = grow(v.d_list_q, v.cap_list_q, static_cast<size_t>(sub) * np, "IVF plan buffer"))) return st;
     if ((st = grow(v.d_list_slot, v.cap_list_slot, static_cast<size_t>(sub) * np, "IVF plan buffer"))) return st;
     if ((st = grow(v.d_q_slot_off, v.cap_q_slot_off, sub + 1, "IVF plan buffer"))) return st;
-    if ((st = grow(v.d_counters, v.cap_counters, 4, "IVF plan buffer"))) return st;
+    if ((st = grow(v.d_counters, v.cap_counters, 6, "IVF plan buffer"))) return st;
     if ((st = grow(v.d_ws, v.cap_ws, static_cast<size_t>(sub) * np * max_chunks * k, "IVF slot workspace"))) return st;
     IvfScanArgs a;
     a.dq = dq;
@@ -567,7 +575,7 @@ int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o
     cudaFuncSetAttribute(ivf_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(probe_smem));
     uint32_t p2 = 1;
     while (p2 < k) p2 <<= 1;
-    cudaMemsetAsync(v.d_counters, 0, 4 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(v.d_counters, 0, 6 * sizeof(unsigned long long), s);
     for (uint32_t q0 = 0; q0 < nq; q0 += sub) {
         const uint32_t n = std::min(sub, nq - q0);
         const float* qn = ix.d_qn + static_cast<uint64_t>(q0) * ix.ds;
@@ -597,9 +605,9 @@ int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "IVF merge launch");
         ix.stats.kernel_launches += 4;
     }
-    if (!v.h_probed && cudaMallocHost(&v.h_probed, sizeof(unsigned long long)) != cudaSuccess)
+    if (!v.h_probed && cudaMallocHost(&v.h_probed, 3 * sizeof(unsigned long long)) != cudaSuccess)
         return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: pinned allocation failed");
-    cudaMemcpyAsync(v.h_probed, v.d_counters + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(v.h_probed, v.d_counters + 3, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
     ix.stats.path = 4;
     ix.stats.nprobe = np;
     return NNDEX_OK;

@@ -695,6 +695,32 @@ OR_API or_ivf* or_ivf_build(const float* m, uint64_t rows, uint64_t dims, uint64
     return ix;
 }
 
+/*
+ * An index over a given layout (centroids, offsets, original_indices, as ApproxIndex holds them,
+ * src/approx.rs:11-25): the reordered rows are gathered from `m`. Lets the CPU baseline time the
+ * reference's search on an index built elsewhere (the build itself is timed separately).
+ */
+OR_API or_ivf* or_ivf_from_layout(const float* m, uint64_t rows, uint64_t dims, uint64_t nlist,
+                                  const float* centroids, const uint64_t* offsets,
+                                  const uint64_t* original) {
+    or_ivf* ix = (or_ivf*)calloc(1, sizeof(or_ivf));
+    ix->rows = rows;
+    ix->dims = dims;
+    ix->nlist = nlist;
+    ix->centroids = (float*)malloc(sizeof(float) * nlist * dims);
+    memcpy(ix->centroids, centroids, sizeof(float) * nlist * dims);
+    ix->offsets = (uint64_t*)malloc(sizeof(uint64_t) * (nlist + 1));
+    memcpy(ix->offsets, offsets, sizeof(uint64_t) * (nlist + 1));
+    ix->original = (uint64_t*)malloc(sizeof(uint64_t) * rows);
+    memcpy(ix->original, original, sizeof(uint64_t) * rows);
+    ix->reordered = (float*)malloc(sizeof(float) * rows * dims);
+#pragma omp parallel for schedule(static)
+    for (uint64_t p = 0; p < rows; ++p)
+        memcpy(ix->reordered + p * dims, m + original[p] * dims, sizeof(float) * dims);
+    ix->assign = (uint32_t*)calloc(rows, sizeof(uint32_t));
+    return ix;
+}
+
 OR_API void or_ivf_free(or_ivf* ix) {
     if (!ix) return;
     free(ix->centroids);

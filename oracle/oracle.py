@@ -71,6 +71,7 @@ def lib():
         "or_kmeans_plusplus_init": (None, [_f32p, _u64, _u64, _u64, C.c_int, _u64, _f32p, _u64p]),
         "or_spherical_kmeans": (None, [_f32p, _u64, _u64, _u64, _u64, _f32p, _u32p]),
         "or_ivf_build": (C.c_void_p, [_f32p, _u64, _u64, _u64, _u64, C.c_int, _u64]),
+        "or_ivf_from_layout": (C.c_void_p, [_f32p, _u64, _u64, _u64, _f32p, _u64p, _u64p]),
         "or_ivf_free": (None, [C.c_void_p]),
         "or_ivf_nlist": (_u64, [C.c_void_p]),
         "or_ivf_centroids": (C.c_void_p, [C.c_void_p]),
@@ -282,11 +283,18 @@ def choose_nprobe(nlist: int, k: int, rows: int) -> int:
 class IvfIndex:
     """src/approx.rs:46-100 ApproxIndex::build (parameterised), with probe and rerank."""
 
-    def __init__(self, storage: np.ndarray, nlist: int = 0, iters: int = 0, seed: int | None = None):
+    def __init__(self, storage: np.ndarray, nlist: int = 0, iters: int = 0, seed: int | None = None,
+                 layout: dict | None = None):
         self.base = _c(storage, np.float32)
         self.rows, self.dims = self.base.shape
-        self.h = lib().or_ivf_build(self.base, self.rows, self.dims, nlist, iters,
-                                    0 if seed is None else 1, 0 if seed is None else seed)
+        if layout is not None:
+            cent = _c(layout["centroids"], np.float32)
+            self.h = lib().or_ivf_from_layout(self.base, self.rows, self.dims, cent.shape[0], cent,
+                                              _c(layout["cluster_offsets"], np.uint64),
+                                              _c(layout["original_indices"], np.uint64))
+        else:
+            self.h = lib().or_ivf_build(self.base, self.rows, self.dims, nlist, iters,
+                                        0 if seed is None else 1, 0 if seed is None else seed)
         self.nlist = int(lib().or_ivf_nlist(self.h))
 
     def _arr(self, fn, ctype, n, dtype):

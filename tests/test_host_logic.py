@@ -36,3 +36,17 @@ def test_precision_validated_before_device():
         nb.NNdex(np.eye(8, dtype=np.float32), precision="fp16")
     with pytest.raises(ValueError, match="unsupported backend"):
         nb.NNdex(np.eye(8, dtype=np.float32), backend="gpu")
+
+
+def test_oracle_ivf_from_layout_equals_built():
+    # the CPU baseline times the reference's IVF search on a given layout: same results as the build
+    from oracle import oracle as O
+    rng = np.random.default_rng(0)
+    m = rng.normal(size=(3000, 32)).astype(np.float32)
+    st, storage = O.prepare_index(m, False)
+    a = O.IvfIndex(storage, nlist=20, iters=3, seed=1)
+    lay = {"centroids": a.centroids, "cluster_offsets": a.offsets, "original_indices": a.original_indices}
+    b = O.IvfIndex(storage, layout=lay)
+    q = storage[:5]
+    ra, rb = a.search(q, 10, 4), b.search(q, 10, 4)
+    assert np.array_equal(ra[0], rb[0]) and np.array_equal(ra[1], rb[1])

@@ -107,15 +107,14 @@ def test_ivf_search_matches_oracle(name, nprobe, k):
     case = next(c for c in BUILD_CASES if c[0] == name)
     m, index, storage, ref = built(case)
     q = make_data("mixture" if name != "policy" else "gauss", 37, m.shape[1], seed=5)
-    if nprobe:
-        # nprobe is an index option (the reference's IndexOptions has none): a fresh index, same build
-        idx_obj = NNdex(m, normalized=case[6], approx=True, nlist=case[3], kmeans_iters=case[4], seed=case[5],
-                        nprobe=nprobe)
-    else:
-        idx_obj = index
-    gi, gs = idx_obj.search(q, k=k)
-    st = idx_obj.last_search_stats()
+    index.set_nprobe(nprobe)
+    try:
+        gi, gs = index.search(q, k=k)
+        st = index.last_search_stats()
+    finally:
+        index.set_nprobe(0)
     assert st["path"] == 4
+    assert st["ivf_rows_union"] <= st["ivf_rows_streamed"] and st["rows_scanned"] > 0
     eff_np = nprobe if nprobe else O.choose_nprobe(ref.nlist, min(k, m.shape[0]), m.shape[0])
     assert st["nprobe"] == min(eff_np, ref.nlist)
     _, qn = O.prepare_queries(q, False, storage.shape[1])
@@ -150,21 +149,35 @@ def test_ivf_batch_equals_single():
     bi, bs = index.search(q, k=10)
     for i in range(q.shape[0]):
         si, ss = index.search(q[i], k=10)
+        # same rows in the same order; scores within the reference's 1e-4 (a single query is
+        # normalised by normalize_vector, a batch by normalize_rows: they may differ by an ulp)
         np.testing.assert_array_equal(si, bi[i])
-        np.testing.assert_array_equal(ss, bs[i])
+        assert np.max(np.abs(ss - bs[i])) < 1e-4
 
 
-def test_ivf_recall_floor_like_reference():
-    # src/lib.rs:962-1021: 4096 × 64, k = 20, approx keeps most of the exact top-k (≥ 14 of 20)
-    rng = np.random.default_rng(42)
-    m = rng.normal(size=(4096, 64)).astype(np.float32)
-    q = rng.normal(size=(64,)).astype(np.float32)
-    approx = NNdex(m, approx=True)
-    exact = NNdex(m)
-    ai, _ = approx.search(q, k=20)
-    ei, _ = exact.search(q, k=20)
-    assert len(set(ai.tolist()) & set(ei.tolist())) >= 14
-    assert ai[0] in set(ei.tolist())
+def test_ivf_recall_equals_reference_approx():
+    # src/lib.rs:962-1021 (4096 × 64 uniform(-1, 1), k = 20, reference nlist/nprobe policy). The
+    # reference asserts ≥ 14 of 20 for one ChaCha8 draw, which numpy cannot reproduce; on numpy draws
+    # of the same distribution the restated reference IVF keeps ≈ 11 of 20 on average. The GPU index
+    # is the same index, so its overlap equals the restatement's on every draw (
+    # recall no lower than the reference approx mode at the same nlist/nprobe/seed).
+    gpu, ref_ov = [], []
+    for seed in range(6):
+        rng = np.random.default_rng(seed)
+        m = rng.uniform(-1, 1, size=(4096, 64)).astype(np.float32)
+        q = rng.uniform(-1, 1, size=(64,)).astype(np.float32)
+        ai, _ = NNdex(m, approx=True).search(q, k=20)
+        ei, _ = NNdex(m).search(q, k=20)
+        st, storage = O.prepare_index(m, False)
+        ref = O.IvfIndex(storage)
+        _, qn = O.prepare_queries(q.reshape(1, -1), False, storage.shape[1])
+        ri, _, _ = ref.search(qn, 20, 0)
+        exact = set(ei.tolist())
+        gpu.append(len(set(ai.tolist()) & exact))
+        ref_ov.append(len(set(ri[0].tolist()) & exact))
+        assert ai[0] in exact
+    assert gpu == ref_ov, (gpu, ref_ov)
+    assert np.mean(gpu) >= 10
 
 
 def test_ivf_small_index_answers_exactly():
@@ -185,6 +198,7 @@ def test_ivf_probed_fewer_rows_than_k():
     # one probed list smaller than k: the result holds the probed rows only (count < k)
     case = BUILD_CASES[0]
     m, _, storage, ref = built(case)
+    # nprobe given at construction (an option the reference's IndexOptions does not have)
     idx_obj = NNdex(m, approx=True, nlist=case[3], kmeans_iters=case[4], seed=case[5], nprobe=1)
     sizes = np.diff(ref.offsets.astype(np.int64))
     k = int(sizes.max()) + 5
