@@ -577,6 +577,8 @@ def run_ivf(args, dev, L, world):
                         zipf=args.ivf_zipf)
     q = make_mixture(nq, dims, args.ivf_centers, args.ivf_sigma, seed + 7, dev, center_seed=args.seed + 200,
                      zipf=args.ivf_zipf)
+    # fingerprint of the synthetic base (a strided sample), so runs on different boxes can be compared
+    data_fp = float(base[::997].double().sum().item())
     opts = _lib.Opts()
     opts.device = local
     opts.nlist = args.ivf_nlist
@@ -702,7 +704,9 @@ def run_ivf(args, dev, L, world):
                     f"{args.ivf_iters} k-means iterations, seed {args.ivf_seed}, batch {nq}",
         "build": {"device_ms": bst.build_ms, "seed_ms": bst.seed_ms, "kmeans_ms": bst.kmeans_ms,
                   "layout_ms": bst.layout_ms, "wall_s_with_upload": build_wall, "max_list": bst.max_list,
-                  "ambiguous_rows_all_iters": bst.ambiguous_rows, "seed_exact_rows": bst.seed_exact_rows},
+                  "ambiguous_rows_all_iters": bst.ambiguous_rows,
+                  "candidate_rows_all_iters": bst.candidate_rows, "seed_exact_rows": bst.seed_exact_rows},
+        "data_fingerprint": data_fp,
         "exact_fp32_ms_per_batch": exact_ms,
         "by_nprobe": per,
         "cpu_baseline": cpu,

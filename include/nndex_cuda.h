@@ -125,8 +125,9 @@ typedef struct nndex_cuda_ivf_stats {
     double   kmeans_ms;        /* the k-means iterations                                     */
     double   layout_ms;        /* list layout: reordered rows, row map, offsets              */
     uint64_t seed_exact_rows;  /* rows whose seeding distance was computed exactly           */
-    uint64_t ambiguous_rows;   /* assignments resolved by the exact FP64 pass (all iters)    */
-    uint64_t reserved[4];
+    uint64_t ambiguous_rows;   /* assignments re-scored against every centroid (all iters)   */
+    uint64_t candidate_rows;   /* assignments decided exactly among <= 3 candidates (all iters) */
+    uint64_t reserved[3];
 } nndex_cuda_ivf_stats;
 
 /* ---- errors ---------------------------------------------------------------------------- */

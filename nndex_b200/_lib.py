@@ -94,7 +94,8 @@ class IvfStats(C.Structure):
         ("layout_ms", C.c_double),
         ("seed_exact_rows", C.c_uint64),
         ("ambiguous_rows", C.c_uint64),
-        ("reserved", C.c_uint64 * 4),
+        ("candidate_rows", C.c_uint64),
+        ("reserved", C.c_uint64 * 3),
     ]
 
 

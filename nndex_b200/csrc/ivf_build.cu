@@ -8,19 +8,24 @@
 // value: products of two f32 are exact in FP64, and the sum is accumulated in index order.
 //
 // Where the time goes and how it is spent on B200:
-//   * seeding: nlist − 1 sequential passes over the rows. Each pass screens every row with a BF16
+//   * seeding: nlist − 1 sequential passes over the rows. Each pass screens every row with an FP16
 //     dot (half the bytes of FP32) and a rigorous error bound; only rows whose distance could drop
 //     below their running minimum are re-scored exactly (FP64 sequential dot). The running sum of
 //     the minima and the threshold search are exact: every distance is a multiple of 2^-24, so FP64
 //     sums below 2^29 carry no rounding and any summation order gives the reference's value.
-//   * assignment: a tcgen05 BF16 GEMM rows × centroids (M = 128 rows in TMEM lanes, N = 256
-//     centroids) whose epilogue keeps each row's best two approximate scores. A row whose gap
-//     exceeds twice its error bound has a certain argmax; the rest are re-scored exactly against
-//     every centroid (FP64, index order) with the reference's tie rule.
+//   * assignment: a tcgen05 FP16 GEMM rows × centroids (M = 128 rows in TMEM lanes, N = 256
+//     centroids) whose epilogue keeps each row's best four approximate scores. A row whose runner-up
+//     trails by more than twice its error bound has a certain argmax; a row with at most three
+//     scores inside that window is decided by exact dots with those candidates; the rest are
+//     re-scored exactly against every centroid (FP64, index order) with the reference's tie rule.
+//     FP16 (11-bit significand) suits unit rows and centroids: its error bound is 8× tighter than
+//     BF16's. Values in FP16's subnormal range count as lost in the residual, so the bound holds
+//     whether the tensor core keeps or flushes them; an overflow makes the bound infinite (or NaN),
+//     which sends the row to the exact pass.
 //   * update: a stable counting sort by cluster (row order kept inside each cluster) and FP64 sums
 //     in that order — the reference's summation order — then the reference's normalisation, each
 //     operation rounded as in Rust (no contraction).
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cfloat>
@@ -82,6 +87,15 @@ NNDEX_DEVICE_INLINE double warp_sum_d(double v) {
     return v;
 }
 
+// FP16 copy of v, and the residual the error bounds use: v − half(v) when half(v) is a normal FP16
+// value; a value in the subnormal range (or zero) counts as entirely lost.
+NNDEX_DEVICE_INLINE __half to_f16(float v, float& resid) {
+    const __half h = __float2half_rn(v);
+    const float hf = __half2float(h);
+    resid = fabsf(hf) >= 6.103515625e-05f ? v - hf : v;  // 2^-14: the smallest normal FP16
+    return h;
+}
+
 // Upper bound of sqrt(v) as f32 for v ≥ 0 accumulated in FP64 (relative slack for its rounding).
 NNDEX_DEVICE_INLINE float sqrt_up(double v) {
     return __double2float_ru(__dsqrt_ru(v * (1.0 + 1e-12)));
@@ -90,11 +104,11 @@ NNDEX_DEVICE_INLINE float sqrt_up(double v) {
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
-// Row preparation: BF16 copy (when the index does not keep one), and per row upper bounds of
-// ‖x‖ and of the BF16 residual ‖x − bf16(x)‖. One warp per row.
+// Row preparation: FP16 copy and per row upper bounds of ‖x‖ and of the residual ‖x − x̂‖. One
+// warp per row.
 // ------------------------------------------------------------------------------------------
 __global__ void ivf_row_prep_kernel(const float* __restrict__ src, uint32_t ds, uint64_t rows,
-                                    __nv_bfloat16* __restrict__ out16, uint32_t kb, float* __restrict__ norm_up,
+                                    __half* __restrict__ out16, uint32_t kb, float* __restrict__ norm_up,
                                     float* __restrict__ res_up) {
     const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
@@ -104,11 +118,11 @@ __global__ void ivf_row_prep_kernel(const float* __restrict__ src, uint32_t ds, 
         double n2 = 0.0, r2 = 0.0;
         for (uint32_t d = lane; d < kb; d += 32) {
             const float v = d < ds ? x[d] : 0.0f;
-            const __nv_bfloat16 b = __float2bfloat16_rn(v);
-            const float e = v - __bfloat162float(b);  // exact: the rounding residual
+            float e;
+            const __half b = to_f16(v, e);
             n2 = fma(static_cast<double>(v), static_cast<double>(v), n2);
             r2 = fma(static_cast<double>(e), static_cast<double>(e), r2);
-            if (out16) out16[r * kb + d] = b;
+            out16[r * kb + d] = b;
         }
         n2 = warp_sum_d(n2);
         r2 = warp_sum_d(r2);
@@ -230,14 +244,14 @@ constexpr uint32_t kKppScanChunk = 2048;
 }  // namespace
 
 __global__ void __launch_bounds__(kKppThreads)
-    kpp_step_kernel(const float* __restrict__ base, const __nv_bfloat16* __restrict__ b16, uint32_t ds, uint32_t kb,
+    kpp_step_kernel(const float* __restrict__ base, const __half* __restrict__ b16, uint32_t ds, uint32_t kb,
                     uint32_t dp, uint64_t rows, uint64_t rows_per_block, const float* __restrict__ norm_up,
                     const float* __restrict__ res_up, float gamma, float* __restrict__ min_d,
                     double* __restrict__ partial, KppState* __restrict__ st, uint32_t* __restrict__ chosen,
                     uint32_t c) {
     extern __shared__ uint8_t smem_raw[];
     float* cf = reinterpret_cast<float*>(smem_raw);                        // ds
-    __nv_bfloat16* cb = reinterpret_cast<__nv_bfloat16*>(cf + ds);        // kb
+    __half* cb = reinterpret_cast<__half*>(cf + ds);                      // kb
     float* scan_buf = reinterpret_cast<float*>(cb + kb);                   // kKppScanChunk (last block)
     __shared__ double wsum[kKppThreads / 32];
     __shared__ unsigned int is_last;
@@ -258,39 +272,56 @@ __global__ void __launch_bounds__(kKppThreads)
     const uint32_t nch = kb / 8;                    // 16-byte chunks of a BF16 row
     double acc = 0.0;
     uint32_t exact_here = 0;
+    const uint4* cr = reinterpret_cast<const uint4*>(cb);
     for (uint64_t rb = r0 + warp * 4; rb < r1; rb += (kKppThreads / 32) * 4) {
         const uint64_t r = rb + g;
         const bool live = r < r1;
-        float sd = 0.0f;
-        if (live) {
-            const uint4* xr = reinterpret_cast<const uint4*>(b16 + r * kb);
-            const uint4* cr = reinterpret_cast<const uint4*>(cb);
-            for (uint32_t ch = j; ch < nch; ch += 8) {
-                const uint4 a = xr[ch], b = cr[ch];
-                const __nv_bfloat162* a2 = reinterpret_cast<const __nv_bfloat162*>(&a);
-                const __nv_bfloat162* b2 = reinterpret_cast<const __nv_bfloat162*>(&b);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const float2 fa = __bfloat1622float2(a2[i]), fb = __bfloat1622float2(b2[i]);
-                    sd = fmaf(fa.x, fb.x, sd);
-                    sd = fmaf(fa.y, fb.y, sd);
-                }
-            }
+        // Every load of the row first (its FP16 chunks; lane 0 of the group: min_d and the row's
+        // bounds), so a row costs one memory round trip.
+        float m = 0.0f, nr = 0.0f, rr = 0.0f;
+        if (live && j == 0) {
+            m = min_d[r];
+            nr = norm_up[r];
+            rr = res_up[r];
         }
+        constexpr int kPre = 8;  // chunks per lane in flight (rows up to 512 FP16 values)
+        const uint4* xr = reinterpret_cast<const uint4*>(b16 + (live ? r : r0) * kb);
+        uint4 xa[kPre];
+#pragma unroll
+        for (int u = 0; u < kPre; ++u) {
+            const uint32_t ch = j + 8u * u;
+            xa[u] = (live && ch < nch) ? xr[ch] : make_uint4(0u, 0u, 0u, 0u);
+        }
+        float sd = 0.0f;
+        auto dot_chunk = [&](const uint4& a, const uint4& b) {
+            const __half2* a2 = reinterpret_cast<const __half2*>(&a);
+            const __half2* b2 = reinterpret_cast<const __half2*>(&b);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const float2 fa = __half22float2(a2[i]), fb = __half22float2(b2[i]);
+                sd = fmaf(fa.x, fb.x, sd);
+                sd = fmaf(fa.y, fb.y, sd);
+            }
+        };
+#pragma unroll
+        for (int u = 0; u < kPre; ++u) {
+            const uint32_t ch = j + 8u * u;
+            if (ch < nch) dot_chunk(xa[u], cr[ch]);
+        }
+        if (live)
+            for (uint32_t ch = j + 8u * kPre; ch < nch; ch += 8) dot_chunk(xr[ch], cr[ch]);
         sd += __shfl_xor_sync(0xffffffffu, sd, 1);
         sd += __shfl_xor_sync(0xffffffffu, sd, 2);
         sd += __shfl_xor_sync(0xffffffffu, sd, 4);
         if (live && j == 0) {
-            float m = min_d[r];
             bool need = m > 0.0f;
             if (need && m < FLT_MAX) {
                 // |x·c − x̂·ĉ| ≤ ‖δx‖‖c‖ + ‖x̂‖‖δc‖; + FP32 accumulation of the screen; + the f32
                 // rounding of the exact dot and of 1 − dot.
-                const float nr = norm_up[r], rr = res_up[r];
                 const float xh = nr + rr, chn = nc + rc;
                 const float e = (rr * nc + xh * rc + gamma * xh * chn + 2.4e-7f * fmaxf(1.0f, nr * nc)) * 1.001f;
                 const double lb = 1.0 - (static_cast<double>(sd) + static_cast<double>(e));
-                need = static_cast<double>(m) > lb;
+                need = !(static_cast<double>(m) <= lb);  // a NaN bound (overflowed copy) scores exactly
             }
             if (need) {
                 const float dot = dot_f64_seq(base + r * ds, cf, dp);
@@ -429,12 +460,12 @@ __global__ void gather_rows_kernel(const float* __restrict__ src, uint32_t ds, c
 }
 
 // ------------------------------------------------------------------------------------------
-// Centroid preparation for one assignment: BF16 copy (rows ≥ nlist stay zero), dims-major FP32
-// copy, and the largest ‖c‖ and ‖c − bf16(c)‖ (upper bounds, as f32 bits; non-negative floats
-// order as unsigned integers). One warp per centroid.
+// Centroid preparation for one assignment: FP16 copy (rows ≥ nlist stay zero), dims-major FP32
+// copy, and the largest ‖c‖ and ‖c − ĉ‖ (upper bounds, as f32 bits; non-negative floats order as
+// unsigned integers; a NaN bound compares above every finite one). One warp per centroid.
 // ------------------------------------------------------------------------------------------
 __global__ void centroid_prep_kernel(const float* __restrict__ cent, uint32_t ds, uint32_t nlist,
-                                     __nv_bfloat16* __restrict__ c16, uint32_t kb, float* __restrict__ cent_t,
+                                     __half* __restrict__ c16, uint32_t kb, float* __restrict__ cent_t,
                                      uint64_t ct_stride, unsigned int* __restrict__ cmax) {
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
@@ -443,8 +474,8 @@ __global__ void centroid_prep_kernel(const float* __restrict__ cent, uint32_t ds
     double n2 = 0.0, r2 = 0.0;
     for (uint32_t d = lane; d < kb; d += 32) {
         const float v = d < ds ? x[d] : 0.0f;
-        const __nv_bfloat16 b = __float2bfloat16_rn(v);
-        const float e = v - __bfloat162float(b);
+        float e;
+        const __half b = to_f16(v, e);
         n2 = fma(static_cast<double>(v), static_cast<double>(v), n2);
         r2 = fma(static_cast<double>(e), static_cast<double>(e), r2);
         if (c16) c16[static_cast<uint64_t>(warp) * kb + d] = b;
@@ -475,6 +506,7 @@ constexpr int kAsStages = 4;
 constexpr uint32_t kAsThreads = 192;
 constexpr uint32_t kAsTmemCols = 512;
 constexpr size_t kAsSmem = 1024 + kAsStages * kAsStage + (2 * kAsStages + 4) * 8 + 16;
+constexpr uint32_t kCandCap = 32;  // candidates a row may keep (one warp lane each)
 
 NNDEX_DEVICE_INLINE void tmem_wait_ld_regs(uint32_t (&v)[32]) {
     asm volatile(
@@ -497,12 +529,21 @@ struct AssignParams {
     const float* res_up = nullptr;
     const unsigned int* cmax = nullptr;  // max ‖c‖, max ‖δc‖ (f32 bits)
     float gamma = 0.0f;                  // FP32 accumulation bound factor
+    float* smax = nullptr;          // pass A output: the best approximate score of each row
     uint32_t* assign = nullptr;
-    uint32_t* amb = nullptr;
+    uint32_t* amb = nullptr;        // rows re-scored against every centroid
     uint32_t* amb_cnt = nullptr;
+    uint32_t* cand_list = nullptr;  // rows × kCandCap: the centroids inside a row's window
+    uint2* cand = nullptr;          // (row, candidates) of the rows decided among their candidates
+    uint32_t* cand_cnt = nullptr;
     uint32_t* status = nullptr;
 };
 
+// kMode 0 (pass A): each row's best approximate score s1 → smax. kMode 1 (pass B): the same GEMM;
+// every centroid whose approximate score reaches s1 − 2e is a candidate (any other scores strictly
+// lower than the best, exactly). One candidate: assigned. Up to kCandCap: queued for the exact
+// decision among them. More (or a non-finite bound): queued for the all-centroid exact pass.
+template <int kMode>
 __global__ void __launch_bounds__(kAsThreads, 1)
     kmeans_assign_tc_kernel(const __grid_constant__ CUtensorMap tmap_rows, const __grid_constant__ CUtensorMap tmap_cent,
                             const AssignParams p) {
@@ -576,7 +617,7 @@ __global__ void __launch_bounds__(kAsThreads, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            constexpr uint32_t idesc = tc::instr_desc<false, kAsM, kAsN>();
+            constexpr uint32_t idesc = tc::instr_desc_f16<kAsM, kAsN>();
             const uint32_t ring0 = smem_u32(ring);
             uint32_t it = 0, seq = 0;
             for (uint32_t rt = blockIdx.x; rt < nrt; rt += gridDim.x)
@@ -615,8 +656,19 @@ __global__ void __launch_bounds__(kAsThreads, 1)
         const float cn = __uint_as_float(p.cmax[0]), cr = __uint_as_float(p.cmax[1]);
         uint32_t seq = 0;
         for (uint32_t rt = blockIdx.x; rt < nrt; rt += gridDim.x) {
-            float s1 = -INFINITY, s2 = -INFINITY;
-            uint32_t i1 = 0;
+            const uint64_t r = static_cast<uint64_t>(rt) * kAsM + lrow;
+            const bool live = r < p.rows;
+            // |s̃ − fl32(s)| ≤ ‖δx‖‖c‖ + ‖x̂‖‖δc‖ + accumulation + the f32 rounding of s.
+            float thr = INFINITY;
+            if (kMode == 1 && live) {
+                const float nr = p.norm_up[r], rr = p.res_up[r];
+                const float xh = nr + rr;
+                const float e = (rr * cn + xh * cr + p.gamma * xh * (cn + cr) + 2.4e-7f * fmaxf(1.0f, nr * cn)) * 1.001f;
+                thr = p.smax[r] - 2.0f * e;
+            }
+            float s1 = -INFINITY;
+            uint32_t ncand = 0, first = 0;
+            uint32_t* my_list = p.cand_list + (live ? r : 0) * kCandCap;
             for (uint32_t ct = 0; ct < nct; ++ct, ++seq) {
                 const uint32_t buf = seq & 1u, ub = seq >> 1;
                 if (!*abort_flag && !mbar_wait_bounded(&tfull[buf], ub & 1u, kWaitBudgetCycles)) {
@@ -631,14 +683,12 @@ __global__ void __launch_bounds__(kAsThreads, 1)
 #pragma unroll
                     for (uint32_t jj = 0; jj < 32; ++jj) {
                         const float sv = __uint_as_float(v[jj]);
-                        if (sv > s2 && id0 + jj < p.nlist) {
-                            if (sv > s1) {
-                                s2 = s1;
-                                s1 = sv;
-                                i1 = id0 + jj;
-                            } else {
-                                s2 = sv;
-                            }
+                        if (kMode == 0) {
+                            if (sv > s1 && id0 + jj < p.nlist) s1 = sv;
+                        } else if (sv >= thr && id0 + jj < p.nlist) {
+                            if (ncand == 0) first = id0 + jj;
+                            if (ncand < kCandCap) my_list[ncand] = id0 + jj;
+                            ++ncand;
                         }
                     }
                 };
@@ -662,15 +712,15 @@ __global__ void __launch_bounds__(kAsThreads, 1)
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&tempty[buf]);
             }
-            const uint64_t r = static_cast<uint64_t>(rt) * kAsM + lrow;
-            if (r < p.rows && !*abort_flag) {
-                // |s̃ − fl32(s)| ≤ ‖δx‖‖c‖ + ‖x̂‖‖δc‖ + accumulation + the f32 rounding of s.
-                const float nr = p.norm_up[r], rr = p.res_up[r];
-                const float xh = nr + rr;
-                const float e = (rr * cn + xh * cr + p.gamma * xh * (cn + cr) + 2.4e-7f * fmaxf(1.0f, nr * cn)) * 1.001f;
-                if (s1 - s2 > 2.0f * e) {
-                    p.assign[r] = i1;
-                } else {
+            if (live && !*abort_flag) {
+                if (kMode == 0) {
+                    p.smax[r] = s1;
+                } else if (ncand == 1) {
+                    p.assign[r] = first;  // every other centroid scores strictly lower, exactly
+                } else if (ncand >= 2 && ncand <= kCandCap) {
+                    const uint32_t pos = atomicAdd(p.cand_cnt, 1u);
+                    p.cand[pos] = make_uint2(static_cast<uint32_t>(r), ncand);
+                } else {  // too many candidates, or a non-finite bound (no candidate passed)
                     const uint32_t pos = atomicAdd(p.amb_cnt, 1u);
                     p.amb[pos] = static_cast<uint32_t>(r);
                 }
@@ -683,6 +733,30 @@ __global__ void __launch_bounds__(kAsThreads, 1)
         __syncwarp();
         tc::fence_after_sync();
         tc::tmem_dealloc(tmem_base, kAsTmemCols);
+    }
+}
+
+// Exact assignment among a row's candidates (every other centroid scores certainly lower): the
+// highest dot_small, the lowest centroid index on a tie. One warp per queued row, one lane per
+// candidate.
+__global__ void kmeans_assign_cand_kernel(const float* __restrict__ base, uint32_t ds, uint32_t dp,
+                                          const float* __restrict__ cent, const uint32_t* __restrict__ cand_list,
+                                          const uint2* __restrict__ cand, const uint32_t* __restrict__ cand_cnt,
+                                          uint32_t* __restrict__ assign) {
+    const uint32_t n = *cand_cnt;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+        const uint2 e = cand[i];
+        unsigned long long best = 0;
+        if (lane < e.y) {
+            const uint32_t c = cand_list[static_cast<uint64_t>(e.x) * kCandCap + lane];
+            const float sc = fold_zero(dot_f64_seq(base + static_cast<uint64_t>(e.x) * ds,
+                                                   cent + static_cast<uint64_t>(c) * ds, dp));
+            best = make_key(sc, c);
+        }
+        best = warp_max_u64(best);
+        if (lane == 0) assign[e.x] = key_row(best);
     }
 }
 
@@ -967,28 +1041,30 @@ int ivf_build(CudaIndex& ix) {
     cudaMemsetAsync(v.d_cent_t, 0, ds * v.nlist_pad * sizeof(float), s);
 
     // ---- scratch ----
-    __nv_bfloat16* b16 = ix.d_base_bf16;
-    const bool own16 = (b16 == nullptr) || (ix.kb16 != kb);
-    if (own16) {
-        if ((e = tmp.alloc(b16, ix.rows_alloc * kb)) != cudaSuccess) return oom("IVF BF16 rows");
-        cudaMemsetAsync(b16, 0, ix.rows_alloc * kb * sizeof(__nv_bfloat16), s);
-    }
+    __half* b16 = nullptr;  // FP16 rows of the build (screens and the assignment GEMM)
+    if ((e = tmp.alloc(b16, ix.rows_alloc * kb)) != cudaSuccess) return oom("IVF FP16 rows");
+    cudaMemsetAsync(b16, 0, ix.rows_alloc * kb * sizeof(__half), s);
     float *norm_up, *res_up, *min_d, *mean_f32;
     uint32_t *chosen, *assign, *amb, *amb_cnt, *hist, *perm;
     unsigned int* cmax;
     unsigned long long* best;
     double *partial, *sums;
     KppState* kst;
-    __nv_bfloat16* c16;
+    __half* c16;
+    uint2* cand;
+    uint32_t *cand_cnt, *cand_list;
+    float* smax;
     const uint32_t nblk_sort = static_cast<uint32_t>((rows + kSortRows - 1) / kSortRows);
     if ((e = tmp.alloc(norm_up, rows)) || (e = tmp.alloc(res_up, rows)) || (e = tmp.alloc(min_d, rows)) ||
         (e = tmp.alloc(mean_f32, ds)) || (e = tmp.alloc(chosen, nlist)) || (e = tmp.alloc(assign, rows)) ||
         (e = tmp.alloc(amb, rows)) || (e = tmp.alloc(amb_cnt, 1)) ||
         (e = tmp.alloc(hist, nlist * nblk_sort + 1)) || (e = tmp.alloc(cmax, 2)) || (e = tmp.alloc(best, 1)) ||
-        (e = tmp.alloc(sums, nlist * ds)) || (e = tmp.alloc(kst, 1)) || (e = tmp.alloc(c16, v.nlist_pad * kb)))
+        (e = tmp.alloc(sums, nlist * ds)) || (e = tmp.alloc(kst, 1)) || (e = tmp.alloc(c16, v.nlist_pad * kb)) ||
+        (e = tmp.alloc(cand, rows)) || (e = tmp.alloc(cand_cnt, 1)) || (e = tmp.alloc(smax, rows)) ||
+        (e = tmp.alloc(cand_list, rows * kCandCap)))
         return oom("IVF build scratch");
     perm = v.d_row_map;
-    cudaMemsetAsync(c16, 0, v.nlist_pad * kb * sizeof(__nv_bfloat16), s);
+    cudaMemsetAsync(c16, 0, v.nlist_pad * kb * sizeof(__half), s);
 
     Timer t_all, t_seed, t_km, t_lay;
     cudaEventRecord(t_all.a, s);
@@ -996,7 +1072,7 @@ int ivf_build(CudaIndex& ix) {
     // Row bounds (and the BF16 copy when the index keeps none).
     {
         const uint32_t blocks = static_cast<uint32_t>(std::min<uint64_t>((rows + 7) / 8, ix.sm_count * 16ull));
-        ivf_row_prep_kernel<<<blocks, 256, 0, s>>>(ix.d_base, static_cast<uint32_t>(ds), rows, own16 ? b16 : nullptr,
+        ivf_row_prep_kernel<<<blocks, 256, 0, s>>>(ix.d_base, static_cast<uint32_t>(ds), rows, b16,
                                                    static_cast<uint32_t>(kb), norm_up, res_up);
         count_launch();
     }
@@ -1026,7 +1102,13 @@ int ivf_build(CudaIndex& ix) {
         KppState h{};
         h.rng = ix.opts.has_seed ? ix.opts.seed : rows * 2654435761ull + dp;
         cudaMemcpyAsync(kst, &h, sizeof(h), cudaMemcpyHostToDevice, s);
-        const uint32_t blocks_target = static_cast<uint32_t>(ix.sm_count) * 8u;
+        const size_t smem = ds * sizeof(float) + kb * sizeof(__half) + kKppScanChunk * sizeof(float);
+        auto kern = kpp_step_kernel;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        // One resident wave: every block streams its row range once, none waits for a second wave.
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kKppThreads, smem);
+        const uint32_t blocks_target = static_cast<uint32_t>(ix.sm_count) * static_cast<uint32_t>(std::max(per_sm, 1));
         uint64_t rpb = (rows + blocks_target - 1) / blocks_target;
         rpb = (rpb + 31) / 32 * 32;
         const uint32_t nb = static_cast<uint32_t>((rows + rpb - 1) / rpb);
@@ -1035,9 +1117,6 @@ int ivf_build(CudaIndex& ix) {
         fill_f32_kernel<<<static_cast<unsigned>(std::min<uint64_t>((rows + 255) / 256, 65535)), 256, 0, s>>>(
             min_d, rows, FLT_MAX);
         count_launch();
-        const size_t smem = ds * sizeof(float) + kb * sizeof(__nv_bfloat16) + kKppScanChunk * sizeof(float);
-        auto kern = kpp_step_kernel;
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         for (uint64_t c = 1; c < nlist; ++c) {
             kern<<<nb, kKppThreads, smem, s>>>(ix.d_base, b16, static_cast<uint32_t>(ds), static_cast<uint32_t>(kb),
                                                static_cast<uint32_t>(dp), rows, rpb, norm_up, res_up, gamma, min_d,
@@ -1054,9 +1133,9 @@ int ivf_build(CudaIndex& ix) {
     // Spherical k-means.
     cudaEventRecord(t_km.a, s);
     CUtensorMap tmap_rows{}, tmap_cent{};
-    if (!encode_tmap_2d(&tmap_rows, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, b16, kb, ix.rows_alloc, kb * 2, 64, 128,
+    if (!encode_tmap_2d(&tmap_rows, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, b16, kb, ix.rows_alloc, kb * 2, 64, 128,
                         CU_TENSOR_MAP_SWIZZLE_128B) ||
-        !encode_tmap_2d(&tmap_cent, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, c16, kb, v.nlist_pad, kb * 2, 64, 256,
+        !encode_tmap_2d(&tmap_cent, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, c16, kb, v.nlist_pad, kb * 2, 64, 256,
                         CU_TENSOR_MAP_SWIZZLE_128B))
         return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (IVF)");
     AssignParams ap;
@@ -1071,8 +1150,13 @@ int ivf_build(CudaIndex& ix) {
     ap.assign = assign;
     ap.amb = amb;
     ap.amb_cnt = amb_cnt;
+    ap.smax = smax;
+    ap.cand_list = cand_list;
+    ap.cand = cand;
+    ap.cand_cnt = cand_cnt;
     ap.status = ix.d_status;
-    cudaFuncSetAttribute(kmeans_assign_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kAsSmem));
+    cudaFuncSetAttribute(kmeans_assign_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kAsSmem));
+    cudaFuncSetAttribute(kmeans_assign_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kAsSmem));
     const uint32_t nrt = static_cast<uint32_t>((rows + kAsM - 1) / kAsM);
     const uint32_t as_grid = std::min<uint32_t>(nrt, static_cast<uint32_t>(ix.sm_count));
     const uint32_t cp_blocks = static_cast<uint32_t>((nlist * 32 + 255) / 256);
@@ -1084,20 +1168,26 @@ int ivf_build(CudaIndex& ix) {
                          static_cast<int>(nlist * sizeof(uint32_t)));
     cudaFuncSetAttribute(centroid_normalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(ds * sizeof(double)));
-    std::vector<uint32_t> h_amb(iters, 0);
-    uint32_t* d_amb_hist = nullptr;
-    if ((e = tmp.alloc(d_amb_hist, iters)) != cudaSuccess) return oom("IVF build scratch");
+    std::vector<uint32_t> h_amb(2 * iters, 0);
+    uint32_t* d_amb_hist = nullptr;  // per iteration: rows of the full exact pass, rows decided among candidates
+    if ((e = tmp.alloc(d_amb_hist, 2 * iters)) != cudaSuccess) return oom("IVF build scratch");
     for (uint64_t it = 0; it < iters; ++it) {
         cudaMemsetAsync(cmax, 0, 2 * sizeof(unsigned int), s);
         cudaMemsetAsync(amb_cnt, 0, sizeof(uint32_t), s);
+        cudaMemsetAsync(cand_cnt, 0, sizeof(uint32_t), s);
         centroid_prep_kernel<<<cp_blocks, 256, 0, s>>>(v.d_centroids, static_cast<uint32_t>(ds),
                                                         static_cast<uint32_t>(nlist), c16, static_cast<uint32_t>(kb),
                                                         v.d_cent_t, v.nlist_pad, cmax);
-        kmeans_assign_tc_kernel<<<as_grid, kAsThreads, kAsSmem, s>>>(tmap_rows, tmap_cent, ap);
+        kmeans_assign_tc_kernel<0><<<as_grid, kAsThreads, kAsSmem, s>>>(tmap_rows, tmap_cent, ap);
+        kmeans_assign_tc_kernel<1><<<as_grid, kAsThreads, kAsSmem, s>>>(tmap_rows, tmap_cent, ap);
         kmeans_assign_exact_kernel<<<ix.sm_count * 4, 256, ds * sizeof(float), s>>>(
             ix.d_base, static_cast<uint32_t>(ds), static_cast<uint32_t>(dp), v.d_cent_t, v.nlist_pad,
             static_cast<uint32_t>(nlist), amb, amb_cnt, assign);
-        cudaMemcpyAsync(d_amb_hist + it, amb_cnt, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+        kmeans_assign_cand_kernel<<<ix.sm_count * 8, 256, 0, s>>>(ix.d_base, static_cast<uint32_t>(ds),
+                                                                  static_cast<uint32_t>(dp), v.d_centroids, cand_list,
+                                                                  cand, cand_cnt, assign);
+        cudaMemcpyAsync(d_amb_hist + 2 * it, amb_cnt, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(d_amb_hist + 2 * it + 1, cand_cnt, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
         // Lists of this assignment (stable by row).
         cluster_hist_kernel<<<nblk_sort, 256, nlist * sizeof(uint32_t), s>>>(assign, rows, static_cast<uint32_t>(nlist),
                                                                              nblk_sort, hist);
@@ -1111,7 +1201,7 @@ int ivf_build(CudaIndex& ix) {
             ix.d_base, static_cast<uint32_t>(ds), perm, v.d_offsets, sums);
         centroid_normalize_kernel<<<static_cast<unsigned>(nlist), 128, ds * sizeof(double), s>>>(
             sums, static_cast<uint32_t>(ds), static_cast<uint32_t>(dp), v.d_offsets, v.d_centroids);
-        count_launch(9);
+        count_launch(11);
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "IVF k-means launch");
     }
     // Dims-major copy of the final centroids for the probe.
@@ -1136,7 +1226,7 @@ int ivf_build(CudaIndex& ix) {
     KppState h_st{};
     cudaMemcpyAsync(h_off.data(), v.d_offsets, (nlist + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(h_chosen.data(), chosen, nlist * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(h_amb.data(), d_amb_hist, iters * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h_amb.data(), d_amb_hist, 2 * iters * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&h_st, kst, sizeof(h_st), cudaMemcpyDeviceToHost, s);
     uint32_t h_status = 0;
     cudaMemcpyAsync(&h_status, ix.d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
@@ -1164,7 +1254,10 @@ int ivf_build(CudaIndex& ix) {
     cudaEventElapsedTime(&ms, t_lay.a, t_lay.b);
     v.stats.layout_ms = ms;
     v.stats.seed_exact_rows = h_st.exact_rows;
-    for (uint32_t a : h_amb) v.stats.ambiguous_rows += a;
+    for (uint64_t i = 0; i < iters; ++i) {
+        v.stats.ambiguous_rows += h_amb[2 * i];
+        v.stats.candidate_rows += h_amb[2 * i + 1];
+    }
     ix.ivf = std::move(ivf);
     return NNDEX_OK;
 }

@@ -8,7 +8,7 @@
 //   with the 128-byte swizzle, consecutive 8-row groups are 1024 bytes apart (SBO = 1024) and the
 //   leading offset is unused (1). Advancing along K inside the 128-byte row moves the start address.
 //   instruction descriptor (32 bit): D format in [4,6) (1 = F32), A format in [7,10), B format in
-//   [10,13) (kind::f16: 1 = BF16; kind::f8f6f4: 0 = E4M3), A/B major bits 15/16 (0 = K-major),
+//   [10,13) (kind::f16: 0 = F16, 1 = BF16; kind::f8f6f4: 0 = E4M3), A/B major bits 15/16 (0 = K-major),
 //   N >> 3 in [17,23), M >> 4 in [24,29).
 #pragma once
 
@@ -32,6 +32,12 @@ template <bool kFp8, int M, int N>
 __host__ __device__ constexpr uint32_t instr_desc() {
     return (1u << 4) | ((kFp8 ? 0u : 1u) << 7) | ((kFp8 ? 0u : 1u) << 10) |
            (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+// kind::f16 with FP16 inputs (format 0), F32 accumulate, both K-major.
+template <int M, int N>
+__host__ __device__ constexpr uint32_t instr_desc_f16() {
+    return (1u << 4) | (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
 }
 
 // D[tmem] (+)= A[smem] · B[smem]ᵀ, issued by one thread.
