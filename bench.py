@@ -80,6 +80,16 @@ def parse_args(argv=None):
     p.add_argument("--ivf-k", type=int, default=10)
     p.add_argument("--ivf-steps", type=int, default=10)
     p.add_argument("--ivf-cpu-queries", type=int, default=64)
+    p.add_argument("--serve", choices=["on", "off", "only"], default="on",
+                   help="also measure the serving loop (Poisson arrivals, continuous batching)")
+    p.add_argument("--serve-rows", type=int, default=5_000_000)
+    p.add_argument("--serve-dims", type=int, default=512)
+    p.add_argument("--serve-centers", type=int, default=2048)
+    p.add_argument("--serve-sigma", type=float, default=0.25)
+    p.add_argument("--serve-rates", default="20000,50000,100000,200000", help="offered queries/s")
+    p.add_argument("--serve-seconds", type=float, default=2.0)
+    p.add_argument("--serve-slots", type=int, default=3)
+    p.add_argument("--serve-nprobe", type=int, default=32)
     return p.parse_args(argv)
 
 
@@ -275,6 +285,9 @@ def run_ours(args):
     if args.ivf == "only":
         ivf = run_ivf(args, dev, L, world)
         return {"ivf": ivf} if rank == 0 else None
+    if args.serve == "only":
+        serve = run_serve(args, dev, L, world)
+        return {"serving": serve} if rank == 0 else None
 
     base = make_mixture(args.rows, args.dims, args.centers, args.sigma, seed, dev, center_seed=args.seed)
     opts = _lib.Opts()
@@ -391,6 +404,7 @@ def run_ours(args):
     torch.cuda.empty_cache()
     mixed = run_mixed(args, dev, L, world) if args.mixed != "off" else None
     ivf = run_ivf(args, dev, L, world) if args.ivf != "off" else None
+    serve = run_serve(args, dev, L, world) if args.serve != "off" else None
     if rank != 0:
         return None
     head = results[args.batch]
@@ -429,6 +443,7 @@ def run_ours(args):
         "gpu_launches": launches,
         "mixed_precision": mixed,
         "ivf": ivf,
+        "serving": serve,
         "batches": {str(bb): {"queries_per_s": r["queries_per_s"], "ms_per_step": r["ms_per_step"],
                               "scan_ms": r["scan_ms"],
                               "hbm_gbs": (args.rows * args.dims * 4 + bb * args.dims * 4 + bb * k * 12)
@@ -712,6 +727,126 @@ def run_ivf(args, dev, L, world):
         "cpu_baseline": cpu,
         "roofline": {"bound": "hbm", "kernel": "ivf_scan_kernel", "peak": peak, "peak_kind": peak_kind,
                      "bytes": "rows_streamed * D * 4 per batch (a list is read once per group of queries)"},
+    }
+
+
+def run_serve(args, dev, L, world):
+    """Serving loop: Poisson arrivals of mixed requests against a device-resident index."""
+    import numpy as np
+    import torch
+    from nndex_b200 import _lib
+    from nndex_b200._lib import NNDEX_FLAG_APPROX, NNDEX_FLAG_BF16, NNDEX_FLAG_NORMALIZED, NNDEX_PENDING
+    rank, _, local = dist_env()
+    seed = replica_seed(args.seed + 300, rank)
+    rows, dims = args.serve_rows, args.serve_dims
+    base = make_mixture(rows, dims, args.serve_centers, args.serve_sigma, seed, dev, center_seed=args.seed + 300)
+    pool = make_mixture(1 << 16, dims, args.serve_centers, args.serve_sigma, seed + 7, dev,
+                        center_seed=args.seed + 300).cpu().numpy()
+    opts = _lib.Opts()
+    opts.device = local
+    h = C.c_void_p()
+    t0 = time.perf_counter()
+    if L.nndex_cuda_create_from_device(base.data_ptr(), base.numel(), rows, dims,
+                                       NNDEX_FLAG_NORMALIZED | NNDEX_FLAG_APPROX | NNDEX_FLAG_BF16, C.byref(opts),
+                                       C.byref(h)) != 0:
+        raise RuntimeError(_lib.last_error())
+    create_s = time.perf_counter() - t0
+    del base
+    torch.cuda.empty_cache()
+    bst = _lib.IvfStats()
+    L.nndex_cuda_ivf_stats_get(h, C.byref(bst))
+    so = _lib.ServerOpts()
+    so.slots = args.serve_slots
+    srv = C.c_void_p()
+    if L.nndex_cuda_server_start(h, C.byref(so), C.byref(srv)) != 0:
+        raise RuntimeError(_lib.last_error())
+    rng = np.random.default_rng(seed)
+    mean_size = (1 + 256) / 2
+    out = {}
+    rates = [float(x) for x in args.serve_rates.split(",") if x]
+    # a warm-up phase first (not reported): every slot meets every request kind and grows its scratch
+    phases = [(None, max(rates), 0.5)] + [(str(int(r)), r, args.serve_seconds) for r in rates]
+    for name, rate, seconds in phases:
+        nreq = max(1, int(rate * seconds / mean_size))
+        gaps = rng.exponential(mean_size / rate, size=nreq)
+        sizes = rng.integers(1, 257, size=nreq)
+        ks = rng.choice([1, 10, 100], size=nreq)
+        approx = rng.integers(0, 2, size=nreq).astype(bool)
+        starts = rng.integers(0, pool.shape[0] - 256, size=nreq)
+        tickets = [None] * nreq
+        lat = []
+        done_q = [0]
+        refused = [0]
+        first_last = [None, None]
+        ready = threading.Semaphore(0)
+
+        def collect():
+            for i in range(nreq):
+                ready.acquire()
+                t = tickets[i]
+                if t is None:
+                    continue
+                n, k = int(sizes[i]), int(ks[i])
+                idx = np.empty((n, k), dtype=np.uint64)
+                sim = np.empty((n, k), dtype=np.float32)
+                cnt = np.empty(n, dtype=np.uint64)
+                info = _lib.RequestInfo()
+                st = L.nndex_cuda_server_poll(srv, t, -1, idx.ctypes.data, sim.ctypes.data, cnt.ctypes.data,
+                                              C.byref(info))
+                if st != 0:
+                    raise RuntimeError(_lib.last_error())
+                lat.append((info.done_ns - info.submit_ns) / 1e6)
+                done_q[0] += n
+                first_last[0] = info.submit_ns if first_last[0] is None else min(first_last[0], info.submit_ns)
+                first_last[1] = info.done_ns if first_last[1] is None else max(first_last[1], info.done_ns)
+
+        th = threading.Thread(target=collect)
+        th.start()
+        tk = C.c_uint64(0)
+        t_begin = time.perf_counter()
+        due = t_begin
+        for i in range(nreq):
+            due += gaps[i]
+            while time.perf_counter() < due:
+                pass
+            q = pool[starts[i]:starts[i] + sizes[i]]
+            st = L.nndex_cuda_server_submit(srv, q.ctypes.data, int(sizes[i]), dims, int(ks[i]),
+                                            NNDEX_FLAG_APPROX if approx[i] else 0,
+                                            args.serve_nprobe if approx[i] else 0, C.byref(tk))
+            if st == 0:
+                tickets[i] = tk.value
+            else:
+                refused[0] += 1
+            ready.release()
+        th.join()
+        elapsed = (first_last[1] - first_last[0]) / 1e9 if first_last[1] else float("nan")
+        lat_a = np.array(lat) if lat else np.array([float("nan")])
+        if name is None:
+            continue
+        out[name] = {
+            "offered_queries_per_s": rate,
+            "requests": nreq,
+            "refused": refused[0],
+            "queries_per_s": done_q[0] / elapsed if elapsed > 0 else None,
+            "latency_ms_p50": float(np.percentile(lat_a, 50)),
+            "latency_ms_p99": float(np.percentile(lat_a, 99)),
+            "latency_ms_max": float(lat_a.max()),
+        }
+    sst = _lib.ServerStats()
+    L.nndex_cuda_server_stats_get(srv, C.byref(sst))
+    L.nndex_cuda_server_stop(srv)
+    L.nndex_cuda_destroy(h)
+    return {
+        "workload": f"serving: base {rows}x{dims} ({args.serve_centers}-centre mixture, sigma={args.serve_sigma}, "
+                    f"unit rows; FP32 + BF16 copies + IVF nlist={bst.nlist}), Poisson arrivals, requests of "
+                    f"U{{1..256}} queries, k in {{1,10,100}}, 50/50 exact / IVF(nprobe={args.serve_nprobe}), "
+                    f"{args.serve_slots} slots, admission by free HBM",
+        "create_s_with_ivf_build": create_s,
+        "by_offered_rate": out,
+        "batches": sst.batches,
+        "mean_batch_queries": sst.queries_done / max(sst.batches, 1),
+        "max_queued_queries": sst.max_queued_queries,
+        "slot_bytes": sst.slot_bytes,
     }
 
 

@@ -45,6 +45,7 @@ extern "C" {
 #define NNDEX_ERR_INVALID_ARGUMENT 10 /* NNdexError::Cuda: bad handle / pointer / option    */
 #define NNDEX_ERR_DEVICE_INDEX     11 /* GpuError::DeviceIndexOutOfRange (src/gpu.rs:46-52) */
 #define NNDEX_ERR_UNSUPPORTED      12 /* NNdexError::Cuda: request outside compiled limits  */
+#define NNDEX_PENDING              13 /* serving: the request has not finished (not an error) */
 
 /* ---- construction flags (IndexOptions, src/lib.rs:64-77) ------------------------------- */
 #define NNDEX_FLAG_NORMALIZED 0x1u /* IndexOptions::normalized: rows/queries already unit  */
@@ -278,6 +279,61 @@ NNDEX_API int nndex_cuda_ivf_stats_get(const nndex_cuda_index* index, nndex_cuda
 /* Lists probed per query by later approx searches (0 = choose_nprobe, src/approx.rs:318-336);
  * no counterpart in the reference, whose nprobe is always the policy's. */
 NNDEX_API int nndex_cuda_set_nprobe(nndex_cuda_index* index, uint32_t nprobe);
+
+/* ---- serving: continuous batching (replaces the query caches, src/cpu.rs:16-89, src/gpu.rs:21-25) ----
+ *
+ * A server owns `slots` views of one index (each: its own stream and scratch, the index's device
+ * data shared) and one worker thread per slot. Submitted requests wait in a queue; whenever a slot
+ * is free its worker takes every queued request of the same kind (exact, or approx with the same
+ * nprobe) that fits the slot, in arrival order, and runs them as one batch at their largest k (each
+ * request receives its own k; a query's result does not depend on the batch it ran in). Requests
+ * that arrive while batches are on the GPU join the next batch of the first slot to free up; slots
+ * run concurrently on the device.
+ * Admission by memory: every slot may hold at most `slot_bytes` of per-batch device memory
+ * (0 = free HBM × 0.5 / slots at start), estimated per query from k; a request that cannot fit a
+ * slot, or that would take the queue above `queue_capacity` queries, is refused with
+ * NNDEX_ERR_ADMISSION (the caller may retry later). The index must outlive its servers.
+ */
+typedef struct nndex_cuda_server nndex_cuda_server;
+typedef struct nndex_cuda_server_opts {
+    uint32_t slots;              /* concurrent batches (worker threads), 0 = 2                  */
+    uint32_t max_batch_queries;  /* queries per batch, 0 = 4096                                 */
+    uint64_t queue_capacity;     /* queries waiting, 0 = 1 << 20                                */
+    uint64_t slot_bytes;         /* device memory per slot, 0 = free HBM × 0.5 / slots          */
+    uint32_t reserved[8];
+} nndex_cuda_server_opts;
+typedef struct nndex_cuda_request_info {
+    uint64_t submit_ns, start_ns, done_ns;   /* steady-clock times: queued, batch launched, done */
+    uint64_t batch_id;
+    uint32_t batch_queries;                  /* queries in the batch it ran in                  */
+    uint32_t slot;
+    uint32_t path;                           /* nndex_cuda_search_stats::path of the batch      */
+    uint32_t reserved;
+} nndex_cuda_request_info;
+typedef struct nndex_cuda_server_stats {
+    uint64_t requests_done, queries_done, batches, refused;
+    uint64_t queued_queries, max_queued_queries;
+    uint32_t slots, max_batch_queries;
+    uint64_t slot_bytes;
+} nndex_cuda_server_stats;
+
+NNDEX_API int nndex_cuda_server_start(nndex_cuda_index* index, const nndex_cuda_server_opts* opts,
+                                      nndex_cuda_server** out);
+/* Queues `query_rows` raw queries (copied before the call returns). flags: NNDEX_FLAG_APPROX for
+ * an IVF search (the index must have one; otherwise the request is answered exactly, as the
+ * reference does). nprobe: 0 = the index's setting. */
+NNDEX_API int nndex_cuda_server_submit(nndex_cuda_server* server, const float* host_queries,
+                                       uint64_t query_rows, uint64_t query_dims, uint64_t k,
+                                       uint32_t flags, uint32_t nprobe, uint64_t* ticket);
+/* NNDEX_OK with the results (idx/sim: query_rows × min(k, rows); counts: query_rows) once the
+ * request has finished (the ticket is then retired), NNDEX_PENDING if it has not within
+ * `timeout_ms` (0 = do not wait, negative = wait until it finishes), or the request's error. */
+NNDEX_API int nndex_cuda_server_poll(nndex_cuda_server* server, uint64_t ticket, int32_t timeout_ms,
+                                     uint64_t* idx_out, float* sim_out, uint64_t* counts_out,
+                                     nndex_cuda_request_info* info);
+NNDEX_API int nndex_cuda_server_stats_get(nndex_cuda_server* server, nndex_cuda_server_stats* out);
+/* Finishes the queued requests, joins the workers and frees the slots. */
+NNDEX_API void nndex_cuda_server_stop(nndex_cuda_server* server);
 
 /* ---- FP64 oracle on the device (score-error report) ------------------------------------- */
 

@@ -349,3 +349,84 @@ class NNdex:
                 import polars as pl  # noqa: PLC0415
                 frames.append(source[rows].with_columns(pl.Series("similarity", sims)))
         return frames[0] if len(frames) == 1 else frames
+
+
+class Server:
+    """Continuous-batching request loop over one index (nndex_cuda_server_*; see include/nndex_cuda.h).
+
+    ``submit`` queues a request and returns a ticket at once; ``poll`` returns ``(indices, scores)``
+    (or ``None`` while the request runs); ``result`` waits for it. Results have the shape the
+    index's own ``search`` gives for a batch (rows × min(k, rows), padded like search_batch).
+    The index must outlive the server.
+    """
+
+    def __init__(self, index: NNdex, slots: int = 2, max_batch_queries: int = 4096,
+                 queue_capacity: int = 1 << 20, slot_bytes: int = 0):
+        self._index = index  # keeps the index alive while the server runs
+        o = _lib.ServerOpts()
+        o.slots = slots
+        o.max_batch_queries = max_batch_queries
+        o.queue_capacity = queue_capacity
+        o.slot_bytes = slot_bytes
+        h = C.c_void_p()
+        _check(_lib.lib().nndex_cuda_server_start(index.handle, C.byref(o), C.byref(h)))
+        self._h = h
+        self._shapes = {}
+
+    def submit(self, queries: Any, k: int = 10, approx: bool = False, nprobe: int = 0) -> int:
+        q = _parse_input(queries)
+        if q.ndim == 1:
+            q = q.reshape(1, -1)
+        t = C.c_uint64(0)
+        st = _lib.lib().nndex_cuda_server_submit(self._h, q.ctypes.data, q.shape[0], q.shape[1], int(k),
+                                                 NNDEX_FLAG_APPROX if approx else 0, int(nprobe), C.byref(t))
+        if st != 0:
+            raise NNdexError(st, _lib.last_error())
+        self._shapes[t.value] = (q.shape[0], max(min(int(k), self._index.rows), 1))
+        return t.value
+
+    def poll(self, ticket: int, timeout: float | None = 0.0, with_info: bool = False):
+        rows, kk = self._shapes[ticket]
+        idx = np.zeros((rows, kk), dtype=np.uint64)
+        sim = np.zeros((rows, kk), dtype=np.float32)
+        cnt = np.zeros(rows, dtype=np.uint64)
+        info = _lib.RequestInfo()
+        ms = -1 if timeout is None else int(timeout * 1000)
+        st = _lib.lib().nndex_cuda_server_poll(self._h, ticket, ms, idx.ctypes.data, sim.ctypes.data, cnt.ctypes.data,
+                                               C.byref(info))
+        if st == _lib.NNDEX_PENDING:
+            return None
+        del self._shapes[ticket]
+        if st != 0:
+            raise NNdexError(st, _lib.last_error())
+        for r in range(rows):
+            n = int(cnt[r])
+            idx[r, n:] = 0
+            sim[r, n:] = 0.0
+        out = (idx, sim)
+        if with_info:
+            return out, {f: getattr(info, f) for f, _ in _lib.RequestInfo._fields_ if f != "reserved"}
+        return out
+
+    def result(self, ticket: int, with_info: bool = False):
+        return self.poll(ticket, timeout=None, with_info=with_info)
+
+    def stats(self) -> dict:
+        s = _lib.ServerStats()
+        _check(_lib.lib().nndex_cuda_server_stats_get(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in _lib.ServerStats._fields_}
+
+    def stop(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.lib().nndex_cuda_server_stop(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.stop()
+
+    def __del__(self):
+        self.stop()
+

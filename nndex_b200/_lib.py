@@ -24,6 +24,7 @@ NNDEX_ERR_ADMISSION = 9
 NNDEX_ERR_INVALID_ARGUMENT = 10
 NNDEX_ERR_DEVICE_INDEX = 11
 NNDEX_ERR_UNSUPPORTED = 12
+NNDEX_PENDING = 13  # serving: the request has not finished (not an error)
 
 NNDEX_FLAG_NORMALIZED = 0x1
 NNDEX_FLAG_APPROX = 0x2
@@ -99,6 +100,43 @@ class IvfStats(C.Structure):
     ]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [
+        ("slots", C.c_uint32),
+        ("max_batch_queries", C.c_uint32),
+        ("queue_capacity", C.c_uint64),
+        ("slot_bytes", C.c_uint64),
+        ("reserved", C.c_uint32 * 8),
+    ]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [
+        ("submit_ns", C.c_uint64),
+        ("start_ns", C.c_uint64),
+        ("done_ns", C.c_uint64),
+        ("batch_id", C.c_uint64),
+        ("batch_queries", C.c_uint32),
+        ("slot", C.c_uint32),
+        ("path", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("requests_done", C.c_uint64),
+        ("queries_done", C.c_uint64),
+        ("batches", C.c_uint64),
+        ("refused", C.c_uint64),
+        ("queued_queries", C.c_uint64),
+        ("max_queued_queries", C.c_uint64),
+        ("slots", C.c_uint32),
+        ("max_batch_queries", C.c_uint32),
+        ("slot_bytes", C.c_uint64),
+    ]
+
+
 _vp = C.c_void_p
 _u64 = C.c_uint64
 _u32 = C.c_uint32
@@ -128,6 +166,11 @@ SIGNATURES = {
     "nndex_cuda_ivf_layout": (_i32, [_vp, C.POINTER(_u64), _vp, _vp, _vp, _vp]),
     "nndex_cuda_ivf_stats_get": (_i32, [_vp, C.POINTER(IvfStats)]),
     "nndex_cuda_set_nprobe": (_i32, [_vp, _u32]),
+    "nndex_cuda_server_start": (_i32, [_vp, C.POINTER(ServerOpts), C.POINTER(_vp)]),
+    "nndex_cuda_server_submit": (_i32, [_vp, _vp, _u64, _u64, _u64, _u32, _u32, C.POINTER(_u64)]),
+    "nndex_cuda_server_poll": (_i32, [_vp, _u64, C.c_int32, _vp, _vp, _vp, C.POINTER(RequestInfo)]),
+    "nndex_cuda_server_stats_get": (_i32, [_vp, C.POINTER(ServerStats)]),
+    "nndex_cuda_server_stop": (None, [_vp]),
 }
 
 NNDEX_NOALLOC_SCRATCH_BYTES = 16 << 20

@@ -162,7 +162,7 @@ CudaIndex::~CudaIndex() {
         cudaEventDestroy(p.first);
         cudaEventDestroy(p.second);
     }
-    cudaFree(d_base);
+    if (owns_base) cudaFree(d_base);
     cudaFree(d_qraw);
     cudaFree(d_qn);
     cudaFree(d_ws);
@@ -176,11 +176,11 @@ CudaIndex::~CudaIndex() {
     cudaFreeHost(h_sim);
     cudaFreeHost(h_cnt);
     cudaFreeHost(h_flags);
-    cudaFree(d_base_bf16);
-    cudaFree(d_base_fp8);
-    cudaFree(d_res16);
-    cudaFree(d_res8);
-    cudaFree(d_row_scale);
+    if (owns_base) cudaFree(d_base_bf16);
+    if (owns_base) cudaFree(d_base_fp8);
+    if (owns_base) cudaFree(d_res16);
+    if (owns_base) cudaFree(d_res8);
+    if (owns_base) cudaFree(d_row_scale);
     cudaFree(d_q_bf16);
     cudaFree(d_q_fp8);
     cudaFree(d_q_scale);
@@ -305,8 +305,8 @@ int CudaIndex::check_device_words() {
 int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
     const bool has16 = d_base_bf16 != nullptr, has8 = d_base_fp8 != nullptr;
     auto tc_ok = [&](bool fp8) {
-        const uint32_t kp = choose_kprime(kcap, fp8);
-        return kp >= kcap && kp > 0;
+        const TcPlan p1 = plan_tc(kcap, fp8);
+        return p1.kp >= kcap && p1.kp > 0 && plan_tc(0, fp8).stages > 0;
     };
     switch (precision) {
         case NNDEX_PRECISION_FP32: return 1;
@@ -327,22 +327,47 @@ uint32_t CudaIndex::tc_chunks(bool fp8) const {
     return static_cast<uint32_t>((fp8 ? kf8 : kb16 * 2) / 128);
 }
 
-// k′ of pass 1: enough candidates that most queries certify, but small enough that the heaps fit
-// beside a 4-deep base ring (queries that do not certify take the threshold pass).
-uint32_t CudaIndex::choose_kprime(uint64_t kcap, bool fp8) const {
+// Shared-memory plan of a tensor-core pass. kcap = 0 plans pass 2 (no heaps). Pass 1 wants
+// k′ = max(32, 2k) heap entries per query (enough that most queries certify) beside a 4-deep ring
+// with the query block resident; it gives up, in order: the ring depth for a k′ that still holds k
+// (queries that do not certify take the threshold pass), then the resident query block (its slabs
+// then travel with every ring stage), then the k′ margin (k′ = k).
+CudaIndex::TcPlan CudaIndex::plan_tc(uint64_t kcap, bool fp8) const {
     const uint32_t nchunks = tc_chunks(fp8);
-    uint32_t kmax4 = 0, kmax = 0;
-    for (uint32_t kp = 8; kp <= 2048; kp += 8) {
-        const uint32_t stg = tc_stages_for(nchunks, kp, fp8, smem_optin);
-        if (stg == 4) kmax4 = kp;
-        if (stg != 0) kmax = kp;
+    TcPlan out;
+    if (kcap == 0) {
+        out.stages = tc_stages_for(nchunks, 0, fp8, false, smem_optin);
+        if (!out.stages) {
+            out.stream_a = true;
+            out.stages = tc_stages_for(nchunks, 0, fp8, true, smem_optin);
+        }
+        return out;
     }
-    uint32_t kp = rerank_width ? rerank_width : static_cast<uint32_t>(std::max<uint64_t>(32, 2 * kcap));
+    auto largest = [&](bool stream_a, bool four) {
+        uint32_t best = 0;
+        for (uint32_t kp = 8; kp <= 2048; kp += 8) {
+            const uint32_t stg = tc_stages_for(nchunks, kp, fp8, stream_a, smem_optin);
+            if (four ? stg == 4 : stg != 0) best = kp;
+        }
+        return best;
+    };
+    const uint32_t kmax4 = largest(false, true), kmax = largest(false, false), kmax_s = largest(true, false);
+    uint32_t want = rerank_width ? rerank_width : static_cast<uint32_t>(std::max<uint64_t>(32, 2 * kcap));
+    if (want > rows) want = static_cast<uint32_t>(rows);
+    uint32_t kp = want;
     if (kp > kmax4 && kcap <= kmax4 && !rerank_width) kp = kmax4;
     if (kp > kmax) kp = kmax;
-    if (kp < kcap) kp = static_cast<uint32_t>(std::min<uint64_t>(kcap, kmax));
-    if (kp > rows) kp = static_cast<uint32_t>(rows);
-    return kp;
+    if (kp >= kcap && kp > 0) {
+        out.kp = kp;
+        out.stages = tc_stages_for(nchunks, kp, fp8, false, smem_optin);
+        return out;
+    }
+    kp = std::min(want, kmax_s);  // streamed query slabs
+    if (kp < kcap) return out;    // no tensor-core plan: the FP32 scan serves this k
+    out.kp = kp;
+    out.stream_a = true;
+    out.stages = tc_stages_for(nchunks, kp, fp8, true, smem_optin);
+    return out;
 }
 
 int CudaIndex::enqueue_prep_queries(const float* d_raw, uint64_t n, int mode, int path, cudaStream_t s) {
@@ -385,10 +410,9 @@ int CudaIndex::enqueue_prep_queries(const float* d_raw, uint64_t n, int mode, in
 int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
                           cudaStream_t s) {
     int st;
-    const uint32_t kp = choose_kprime(kcap, fp8);
-    const uint32_t nchunks = tc_chunks(fp8);
-    const uint32_t stages = tc_stages_for(nchunks, kp, fp8, smem_optin);
-    if (!stages) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k'=%u does not fit", kp);
+    const TcPlan plan = plan_tc(kcap, fp8);
+    const uint32_t kp = plan.kp, stages = plan.stages;
+    if (!stages || kp < kcap) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k'=%u does not fit", kp);
     const uint32_t nqb = (n + 127) / 128;
     uint64_t nranges = 0, range_rows = 0;
     tc_ranges(nqb, nranges, range_rows);
@@ -412,6 +436,7 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     a.tmap_b = fp8 ? &tmap_fp8 : &tmap_bf16;
     a.nranges = static_cast<uint32_t>(nranges);
     a.stages = stages;
+    a.stream_a = plan.stream_a;
     fill_tc_params(fp8, n, range_rows, a.p);
     a.p.q_resid = d_q_resid;
     a.p.q_scale = fp8 ? d_q_scale : nullptr;
@@ -547,7 +572,9 @@ int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_si
     a.tmap_q = &tmap_q2;
     a.tmap_b = fp8 ? &tmap_fp8 : &tmap_bf16;
     a.nranges = static_cast<uint32_t>(nranges);
-    a.stages = tc_stages_for(tc_chunks(fp8), 0, fp8, smem_optin);
+    const TcPlan plan2 = plan_tc(0, fp8);
+    a.stages = plan2.stages;
+    a.stream_a = plan2.stream_a;
     fill_tc_params(fp8, m, range_rows, a.p);
     a.p.q_resid = d_q2_resid;
     a.p.q_scale = fp8 ? d_q2_scale : nullptr;
@@ -650,9 +677,9 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         if (e != cudaSuccess) return cuda_error(e, "search");
         if ((st = check_device_words())) return st;
         if (path == 4) {
-            stats.rows_scanned += ivf->h_probed[0];
-            stats.ivf_rows_streamed += ivf->h_probed[1];
-            stats.ivf_rows_union += ivf->h_probed[2];
+            stats.rows_scanned += ivf_scratch.h_probed[0];
+            stats.ivf_rows_streamed += ivf_scratch.h_probed[1];
+            stats.ivf_rows_union += ivf_scratch.h_probed[2];
         }
         std::memcpy(idx_out + q0 * kcap, h_idx, n * kcap * sizeof(uint64_t));
         std::memcpy(sim_out + q0 * kcap, h_sim, n * kcap * sizeof(float));
@@ -710,9 +737,9 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_error(e, "search");
         if (uses_ivf()) {
-            stats.rows_scanned = ivf->h_probed[0];
-            stats.ivf_rows_streamed = ivf->h_probed[1];
-            stats.ivf_rows_union = ivf->h_probed[2];
+            stats.rows_scanned = ivf_scratch.h_probed[0];
+            stats.ivf_rows_streamed = ivf_scratch.h_probed[1];
+            stats.ivf_rows_union = ivf_scratch.h_probed[2];
         }
         return check_device_words();
     }
@@ -957,6 +984,61 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
         if ((st = ivf_build(*ix)) != NNDEX_OK) return fail(st);
     }
     *out = ix;
+    return NNDEX_OK;
+}
+
+// A second handle on the same device-resident index: it shares the read-only data (base copies,
+// tensor maps, the IVF) and owns its stream, status words and per-search scratch, so several can
+// search concurrently (server slots).
+int make_view(const CudaIndex& src, CudaIndex** out) {
+    *out = nullptr;
+    cudaSetDevice(src.device);
+    CudaIndex* v = new (std::nothrow) CudaIndex();
+    if (!v) return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: host allocation failed");
+    v->owns_base = false;
+    v->device = src.device;
+    v->sm_count = src.sm_count;
+    v->smem_optin = src.smem_optin;
+    v->rows = src.rows;
+    v->rows_alloc = src.rows_alloc;
+    v->dims = src.dims;
+    v->dp = src.dp;
+    v->ds = src.ds;
+    v->flags = src.flags;
+    v->normalized = src.normalized;
+    v->approx = src.approx;
+    v->opts = src.opts;
+    v->d_base = src.d_base;
+    v->tmap_f32 = src.tmap_f32;
+    v->precision = src.precision;
+    v->kb16 = src.kb16;
+    v->kf8 = src.kf8;
+    v->d_base_bf16 = src.d_base_bf16;
+    v->d_base_fp8 = src.d_base_fp8;
+    v->d_row_scale = src.d_row_scale;
+    v->eps_bf16 = src.eps_bf16;
+    v->eps_fp8 = src.eps_fp8;
+    v->d_res16 = src.d_res16;
+    v->d_res8 = src.d_res8;
+    v->tmap_bf16 = src.tmap_bf16;
+    v->tmap_fp8 = src.tmap_fp8;
+    v->rerank_width = src.rerank_width;
+    v->tc_sample_stride = src.tc_sample_stride;
+    v->ivf = src.ivf;
+    v->ivf_scratch.nprobe = src.ivf_scratch.nprobe;
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&v->ev0)) != cudaSuccess || (e = cudaEventCreate(&v->ev1)) != cudaSuccess ||
+        (e = cudaMalloc(&v->d_err, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMalloc(&v->d_status, sizeof(uint32_t))) != cudaSuccess ||
+        (e = cudaMallocHost(&v->h_flags, 2 * sizeof(uint64_t))) != cudaSuccess) {
+        delete v;
+        return cuda_error(e, "index view");
+    }
+    cudaMemsetAsync(v->d_err, 0xFF, sizeof(unsigned long long), v->stream);
+    cudaMemsetAsync(v->d_status, 0, sizeof(uint32_t), v->stream);
+    cudaStreamSynchronize(v->stream);
+    *out = v;
     return NNDEX_OK;
 }
 
@@ -1219,7 +1301,7 @@ int nndex_cuda_set_nprobe(nndex_cuda_index* index, uint32_t nprobe) {
     CudaIndex* ix = index->impl;
     std::lock_guard<std::mutex> lock(ix->mu);
     ix->opts.nprobe = nprobe;
-    if (ix->ivf) ix->ivf->nprobe = nprobe;
+    ix->ivf_scratch.nprobe = nprobe;
     return NNDEX_OK;
 }
 

@@ -23,6 +23,7 @@ const char* last_error();
 int cuda_error(cudaError_t e, const char* what);
 
 struct CudaIndex {
+    bool owns_base = true;    // false for a view (make_view): the device data belongs to another handle
     int device = 0;
     int sm_count = 148;
     size_t smem_optin = 232448;
@@ -140,7 +141,9 @@ struct CudaIndex {
     uint64_t* h_flags = nullptr;
 
     nndex_cuda_search_stats stats{};
-    std::unique_ptr<IvfIndex> ivf;  // approximate mode (NNDEX_FLAG_APPROX), built at creation
+    std::shared_ptr<const IvfIndex> ivf;  // approximate mode (NNDEX_FLAG_APPROX), built at creation
+    IvfScratch ivf_scratch;
+    int approx_override = -1;   // -1: the index's mode; 0: exact; 1: approx (server batches)
 
     // scan-kernel timing (roofline reports)
     bool scan_timing = false;
@@ -162,7 +165,12 @@ struct CudaIndex {
                       uint32_t* d_cnt_out, cudaStream_t s, int synchronize);
     // Path choice for a batch: 1 = FP32 scan, 2 = BF16 tensor-core scan, 3 = FP8 tensor-core scan.
     int choose_path(uint64_t nq, uint64_t kcap) const;
-    uint32_t choose_kprime(uint64_t kcap, bool fp8) const;
+    struct TcPlan {
+        uint32_t kp = 0;        // pass-1 heap entries per query (0: no plan)
+        uint32_t stages = 0;    // ring depth
+        bool stream_a = false;  // query slabs staged per ring stage instead of resident
+    };
+    TcPlan plan_tc(uint64_t kcap, bool fp8) const;
     uint32_t tc_chunks(bool fp8) const;
     void tc_ranges(uint32_t nqb, uint64_t& nranges, uint64_t& range_rows) const;
     void fill_tc_params(bool fp8, uint32_t n, uint64_t range_rows, TcParams& p) const;
@@ -175,11 +183,15 @@ struct CudaIndex {
     int finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
     int stream_status();
     // Approximate mode with an IVF that gives a speedup (src/approx.rs:35-37 provides_speedup).
-    bool uses_ivf() const { return approx && ivf && rows >= 256 && ivf->nlist >= 4; }
+    bool uses_ivf() const {
+        const bool want = approx_override < 0 ? approx : approx_override == 1;
+        return want && ivf && rows >= 256 && ivf->nlist >= 4;
+    }
     void order_after_previous(cudaStream_t s);
     void mark_done(cudaStream_t s);
 };
 
+int make_view(const CudaIndex& src, CudaIndex** out);
 int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out,
                           float* d_sim_out, uint32_t* d_cnt_out, cudaStream_t s);
 

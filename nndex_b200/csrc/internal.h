@@ -101,10 +101,11 @@ struct TcArgs {
     TcParams p;
     uint32_t nranges = 0;
     uint32_t stages = 4;                  // base ring depth (2..4)
+    bool stream_a = false;                // pass 1: query slabs staged per ring stage, not resident
 };
-size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8);
+size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8, bool stream_a);
 // Deepest base ring (4, 3 or 2 stages) that fits k′ heaps in `smem_limit`; 0 if none fits.
-uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, size_t smem_limit);
+uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, bool stream_a, size_t smem_limit);
 cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t stream);
 
 struct RerankArgs {

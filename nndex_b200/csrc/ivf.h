@@ -20,6 +20,7 @@ namespace nndex {
 
 struct CudaIndex;
 
+// The built index: read-only once built, shared by every view of the CudaIndex (server slots).
 struct IvfIndex {
     uint64_t nlist = 0;          // clusters (1 = single-list index, never probed)
     uint64_t iters = 0;          // k-means iterations
@@ -35,7 +36,12 @@ struct IvfIndex {
     CUtensorMap tmap_reordered{};
     nndex_cuda_ivf_stats stats{};
 
-    // search scratch (grown on demand)
+    ~IvfIndex();
+};
+
+// Per-search scratch of the IVF path (one per CudaIndex view; grown on demand).
+struct IvfScratch {
+    uint32_t nprobe = 0;                // 0 = choose_nprobe per search
     uint32_t* d_probes = nullptr;       size_t cap_probes = 0;
     uint32_t* d_list_cnt = nullptr;     size_t cap_list_cnt = 0;   // nlist: queries probing each list
     uint32_t* d_list_fill = nullptr;    size_t cap_list_fill = 0;
@@ -47,9 +53,8 @@ struct IvfIndex {
     unsigned long long* d_counters = nullptr; size_t cap_counters = 0;  // work counter, totals, rows probed
     uint64_t* d_ws = nullptr;           size_t cap_ws = 0;         // slots × k keys
     unsigned long long* h_probed = nullptr;  // pinned [3]: rows probed (Σ over queries), streamed, union
-    uint32_t nprobe = 0;                     // 0 = choose_nprobe per search
 
-    ~IvfIndex();
+    ~IvfScratch();
 };
 
 // Builds the IVF of `ix` (k-means++ + spherical k-means + list layout) on the GPU. nlist, iters

@@ -937,6 +937,9 @@ IvfIndex::~IvfIndex() {
     cudaFree(d_reordered);
     cudaFree(d_row_map);
     cudaFree(d_offsets);
+}
+
+IvfScratch::~IvfScratch() {
     cudaFree(d_probes);
     cudaFree(d_list_cnt);
     cudaFree(d_list_fill);
@@ -1022,11 +1025,11 @@ int ivf_build(CudaIndex& ix) {
     if (nlist > 16384)
         return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: nlist=%llu above the 16384 limit",
                          (unsigned long long)nlist);
-    auto ivf = std::make_unique<IvfIndex>();
+    auto ivf = std::make_shared<IvfIndex>();
     IvfIndex& v = *ivf;
     v.nlist = nlist;
     v.iters = iters;
-    v.nprobe = ix.opts.nprobe;
+    ix.ivf_scratch.nprobe = ix.opts.nprobe;
     v.nlist_pad = (nlist + 255) / 256 * 256;
     const uint64_t kb = (ix.dims + 63) / 64 * 64;  // BF16 row length (64-element K slabs)
     BuildScratch tmp;

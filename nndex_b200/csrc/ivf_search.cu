@@ -524,9 +524,10 @@ cudaError_t launch_scan(const CUtensorMap& tmap, const IvfScanArgs& a, uint32_t 
 
 int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
                cudaStream_t s) {
-    IvfIndex& v = *ix.ivf;
+    const IvfIndex& v = *ix.ivf;
+    IvfScratch& w = ix.ivf_scratch;
     const uint32_t nlist = static_cast<uint32_t>(v.nlist);
-    uint64_t np64 = v.nprobe ? v.nprobe : ivf_choose_nprobe(v.nlist, k, ix.rows);
+    uint64_t np64 = w.nprobe ? w.nprobe : ivf_choose_nprobe(v.nlist, k, ix.rows);
     np64 = std::max<uint64_t>(1, std::min<uint64_t>(np64, v.nlist));
     const uint32_t np = static_cast<uint32_t>(np64);
     const uint32_t dq = static_cast<uint32_t>(ix.ds);
@@ -546,16 +547,16 @@ int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o
     const uint64_t ws_budget = 256ull << 20;
     uint64_t per_query = std::max<uint64_t>(1, static_cast<uint64_t>(np) * max_chunks * k * 8);
     uint32_t sub = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(nq, ws_budget / per_query)));
-    if ((st = grow(v.d_probes, v.cap_probes, static_cast<size_t>(sub) * np, "IVF probe buffer"))) return st;
-    if ((st = grow(v.d_list_cnt, v.cap_list_cnt, nlist, "IVF plan buffer"))) return st;
-    if ((st = grow(v.d_list_fill, v.cap_list_fill, nlist, "IVF plan buffer"))) return st;
-    if ((st = grow(v.d_list_qoff, v.cap_list_qoff, nlist + 1, "IVF plan buffer"))) return st;
-    if ((st = grow(v.d_item_off, v.cap_item_off, nlist + 1, "IVF plan buffer"))) return st;
-    if ((st = grow(v.d_list_q, v.cap_list_q, static_cast<size_t>(sub) * np, "IVF plan buffer"))) return st;
-    if ((st = grow(v.d_list_slot, v.cap_list_slot, static_cast<size_t>(sub) * np, "IVF plan buffer"))) return st;
-    if ((st = grow(v.d_q_slot_off, v.cap_q_slot_off, sub + 1, "IVF plan buffer"))) return st;
-    if ((st = grow(v.d_counters, v.cap_counters, 6, "IVF plan buffer"))) return st;
-    if ((st = grow(v.d_ws, v.cap_ws, static_cast<size_t>(sub) * np * max_chunks * k, "IVF slot workspace"))) return st;
+    if ((st = grow(w.d_probes, w.cap_probes, static_cast<size_t>(sub) * np, "IVF probe buffer"))) return st;
+    if ((st = grow(w.d_list_cnt, w.cap_list_cnt, nlist, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_list_fill, w.cap_list_fill, nlist, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_list_qoff, w.cap_list_qoff, nlist + 1, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_item_off, w.cap_item_off, nlist + 1, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_list_q, w.cap_list_q, static_cast<size_t>(sub) * np, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_list_slot, w.cap_list_slot, static_cast<size_t>(sub) * np, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_q_slot_off, w.cap_q_slot_off, sub + 1, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_counters, w.cap_counters, 6, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_ws, w.cap_ws, static_cast<size_t>(sub) * np * max_chunks * k, "IVF slot workspace"))) return st;
     IvfScanArgs a;
     a.dq = dq;
     a.k = k;
@@ -563,29 +564,29 @@ int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o
     a.nlist = nlist;
     a.offsets = v.d_offsets;
     a.row_map = v.d_row_map;
-    a.list_cnt = v.d_list_cnt;
-    a.list_qoff = v.d_list_qoff;
-    a.item_off = v.d_item_off;
-    a.list_q = v.d_list_q;
-    a.list_slot = v.d_list_slot;
-    a.counters = v.d_counters;
-    a.ws = v.d_ws;
+    a.list_cnt = w.d_list_cnt;
+    a.list_qoff = w.d_list_qoff;
+    a.item_off = w.d_item_off;
+    a.list_q = w.d_list_q;
+    a.list_slot = w.d_list_slot;
+    a.counters = w.d_counters;
+    a.ws = w.d_ws;
     a.status = ix.d_status;
     const size_t probe_smem = static_cast<size_t>(ix.ds) * 4 + static_cast<size_t>(nlist) * 8;
     cudaFuncSetAttribute(ivf_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(probe_smem));
     uint32_t p2 = 1;
     while (p2 < k) p2 <<= 1;
-    cudaMemsetAsync(v.d_counters, 0, 6 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(w.d_counters, 0, 6 * sizeof(unsigned long long), s);
     for (uint32_t q0 = 0; q0 < nq; q0 += sub) {
         const uint32_t n = std::min(sub, nq - q0);
         const float* qn = ix.d_qn + static_cast<uint64_t>(q0) * ix.ds;
-        cudaMemsetAsync(v.d_list_cnt, 0, nlist * sizeof(uint32_t), s);
-        cudaMemsetAsync(v.d_list_fill, 0, nlist * sizeof(uint32_t), s);
+        cudaMemsetAsync(w.d_list_cnt, 0, nlist * sizeof(uint32_t), s);
+        cudaMemsetAsync(w.d_list_fill, 0, nlist * sizeof(uint32_t), s);
         ivf_probe_kernel<<<n, 256, probe_smem, s>>>(qn, dq, static_cast<uint32_t>(ix.dp), v.d_cent_t, v.nlist_pad, nlist,
-                                                    np, v.d_probes);
-        ivf_plan_kernel<<<1, 1024, 0, s>>>(v.d_probes, n, np, nlist, v.d_offsets, qb, v.d_list_cnt, v.d_list_fill,
-                                           v.d_list_qoff, v.d_item_off, v.d_list_q, v.d_list_slot, v.d_q_slot_off,
-                                           v.d_counters);
+                                                    np, w.d_probes);
+        ivf_plan_kernel<<<1, 1024, 0, s>>>(w.d_probes, n, np, nlist, v.d_offsets, qb, w.d_list_cnt, w.d_list_fill,
+                                           w.d_list_qoff, w.d_item_off, w.d_list_q, w.d_list_slot, w.d_q_slot_off,
+                                           w.d_counters);
         count_launch(2);
         a.queries = qn;
         cudaError_t e;
@@ -598,16 +599,16 @@ int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o
         }
         ix.scan_event_end(s, ev_a);
         if (e != cudaSuccess) return cuda_error(e, "IVF scan launch");
-        ivf_merge_kernel<<<n, 512, p2 * sizeof(uint64_t), s>>>(v.d_ws, v.d_q_slot_off, k, o_idx + static_cast<uint64_t>(q0) * k,
+        ivf_merge_kernel<<<n, 512, p2 * sizeof(uint64_t), s>>>(w.d_ws, w.d_q_slot_off, k, o_idx + static_cast<uint64_t>(q0) * k,
                                                                o_sim + static_cast<uint64_t>(q0) * k,
                                                                o_cnt ? o_cnt + q0 : nullptr);
         count_launch();
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "IVF merge launch");
         ix.stats.kernel_launches += 4;
     }
-    if (!v.h_probed && cudaMallocHost(&v.h_probed, 3 * sizeof(unsigned long long)) != cudaSuccess)
+    if (!w.h_probed && cudaMallocHost(&w.h_probed, 3 * sizeof(unsigned long long)) != cudaSuccess)
         return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: pinned allocation failed");
-    cudaMemcpyAsync(v.h_probed, v.d_counters + 3, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(w.h_probed, w.d_counters + 3, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
     ix.stats.path = 4;
     ix.stats.nprobe = np;
     return NNDEX_OK;

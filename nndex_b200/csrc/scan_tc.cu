@@ -69,19 +69,19 @@ NNDEX_DEVICE_INLINE float pick(const uint32_t (&v)[32], uint32_t j) {
 }
 }  // namespace
 
-size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8) {
+size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8, bool stream_a) {
     size_t b = 1024;
-    b += static_cast<size_t>(nchunks) * kAChunk;
-    b += static_cast<size_t>(stages) * kBChunk;
+    b += stream_a ? static_cast<size_t>(stages) * (kAChunk + kBChunk)
+                  : static_cast<size_t>(nchunks) * kAChunk + static_cast<size_t>(stages) * kBChunk;
     b += static_cast<size_t>(kprime) * kM * 8;
     b += fp8 ? 2 * kN * 4 : 0;
     b += (2 * stages + 5) * 8 + 16;
     return b;
 }
 
-uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, size_t smem_limit) {
+uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, bool stream_a, size_t smem_limit) {
     for (uint32_t st = 4; st >= 2; --st)
-        if (tc_smem_bytes(nchunks, kprime, st, fp8) <= smem_limit) return st;
+        if (tc_smem_bytes(nchunks, kprime, st, fp8, stream_a) <= smem_limit) return st;
     return 0;
 }
 
@@ -148,16 +148,20 @@ NNDEX_DEVICE_INLINE void epi_survivor(const TcParams& p, EpiState& st, uint64_t*
     }
 }
 
-template <bool kFp8, int kST, int kMode>
+// kStreamA: the query block's K slabs are not resident; each ring stage carries the matching query
+// slab beside the base slab (re-read from L2 per tile). It frees nchunks × 16 KB of shared memory
+// for the pass-1 heaps, which large D × large k needs (D = 512, k = 100: 128 KB of queries).
+template <bool kFp8, int kST, int kMode, bool kStreamA>
 __global__ void __launch_bounds__(kThreads, 1)
     scan_tc_kernel(const __grid_constant__ CUtensorMap tmap_q, const __grid_constant__ CUtensorMap tmap_b,
                    const TcParams p) {
     constexpr uint32_t kElems = kFp8 ? 128 : 64;  // K elements per 128-byte slab
+    constexpr uint32_t kStage = kStreamA ? kAChunk + kBChunk : kBChunk;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = align_1024(smem_raw);
-    uint8_t* a_smem = smem;
-    uint8_t* b_smem = a_smem + static_cast<size_t>(p.nchunks) * kAChunk;
-    uint64_t* heap = reinterpret_cast<uint64_t*>(b_smem + static_cast<size_t>(kST) * kBChunk);
+    uint8_t* a_smem = smem;  // resident query slabs (kStreamA: none)
+    uint8_t* b_smem = a_smem + (kStreamA ? 0 : static_cast<size_t>(p.nchunks) * kAChunk);
+    uint64_t* heap = reinterpret_cast<uint64_t*>(b_smem + static_cast<size_t>(kST) * kStage);
     float* scale_s = reinterpret_cast<float*>(heap + static_cast<size_t>(p.kprime) * kM);  // FP8: [2][256]
     uint64_t* full_bar = reinterpret_cast<uint64_t*>(scale_s + (kFp8 ? 2 * kN : 0));
     uint64_t* empty_bar = full_bar + kST;
@@ -206,10 +210,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             tma_prefetch_desc(&tmap_b);
             // Base tiles are read by every query block of the same row range at about the same
             // time: keep them in L2 with the default policy (no evict-first hint).
-            mbar_arrive_expect_tx(a_full, nchunks * kAChunk);
-            for (uint32_t c = 0; c < nchunks; ++c)
-                tma_load_2d(a_smem + static_cast<size_t>(c) * kAChunk, &tmap_q, a_full, static_cast<int32_t>(c * kElems),
-                            static_cast<int32_t>(q0));
+            if (!kStreamA) {
+                mbar_arrive_expect_tx(a_full, nchunks * kAChunk);
+                for (uint32_t c = 0; c < nchunks; ++c)
+                    tma_load_2d(a_smem + static_cast<size_t>(c) * kAChunk, &tmap_q, a_full,
+                                static_cast<int32_t>(c * kElems), static_cast<int32_t>(q0));
+            }
             uint32_t it = 0;
             bool stop = false;
             for (uint32_t t = 0; t < ntiles && !stop; ++t) {
@@ -226,14 +232,17 @@ __global__ void __launch_bounds__(kThreads, 1)
                         stop = true;
                         break;
                     }
-                    mbar_arrive_expect_tx(&full_bar[s], kBChunk);
-                    tma_load_2d(b_smem + static_cast<size_t>(s) * kBChunk, &tmap_b, &full_bar[s],
-                                static_cast<int32_t>(c * kElems), y);
+                    uint8_t* stage = b_smem + static_cast<size_t>(s) * kStage;
+                    mbar_arrive_expect_tx(&full_bar[s], kStage);
+                    if (kStreamA)
+                        tma_load_2d(stage + kBChunk, &tmap_q, &full_bar[s], static_cast<int32_t>(c * kElems),
+                                    static_cast<int32_t>(q0));
+                    tma_load_2d(stage, &tmap_b, &full_bar[s], static_cast<int32_t>(c * kElems), y);
                     ++it;
                 }
             }
             // Drain every copy this thread issued before the CTA may exit.
-            if (!mbar_wait_bounded(a_full, 0, kWaitBudgetCycles)) record_status(p.status, kStatusTimeout);
+            if (!kStreamA && !mbar_wait_bounded(a_full, 0, kWaitBudgetCycles)) record_status(p.status, kStatusTimeout);
             const uint32_t used = it < static_cast<uint32_t>(kST) ? it : kST;
             for (uint32_t s = 0; s < used; ++s) {
                 const uint32_t uses = (it - s + kST - 1) / kST;
@@ -245,7 +254,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             constexpr uint32_t idesc = tc::instr_desc<kFp8, kM, kN>();
-            if (!mbar_wait_bounded(a_full, 0, kWaitBudgetCycles)) {
+            if (!kStreamA && !mbar_wait_bounded(a_full, 0, kWaitBudgetCycles)) {
                 *abort_flag = 1;
                 record_status(p.status, kStatusTimeout);
             }
@@ -268,7 +277,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     tc::fence_after_sync();
                     if (!*abort_flag) {
-                        const uint32_t a_addr = a_addr0 + c * kAChunk, b_addr = b_addr0 + s * kBChunk;
+                        const uint32_t b_addr = b_addr0 + s * kStage;
+                        const uint32_t a_addr = kStreamA ? b_addr + kBChunk : a_addr0 + c * kAChunk;
 #pragma unroll
                         for (uint32_t kk = 0; kk < 4; ++kk)
                             tc::mma<kFp8>(d, tc::smem_desc_sw128(a_addr + kk * 32), tc::smem_desc_sw128(b_addr + kk * 32),
@@ -535,11 +545,11 @@ __global__ void __launch_bounds__(256)
 // ------------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------------
-template <bool kFp8, int kST, int kMode>
+template <bool kFp8, int kST, int kMode, bool kStreamA>
 static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
-    auto kern = scan_tc_kernel<kFp8, kST, kMode>;
+    auto kern = scan_tc_kernel<kFp8, kST, kMode, kStreamA>;
     const uint32_t kp = kMode == 0 ? a.p.kprime : 0;
-    const size_t smem = tc_smem_bytes(a.p.nchunks, kp, kST, kFp8);
+    const size_t smem = tc_smem_bytes(a.p.nchunks, kp, kST, kFp8, kStreamA);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     dim3 grid((a.p.nq + kM - 1) / kM, a.nranges);
@@ -550,19 +560,23 @@ static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-template <bool kFp8, int kMode>
+template <bool kFp8, int kMode, bool kStreamA>
 static cudaError_t launch_tc_stages(const TcArgs& a, cudaStream_t stream) {
     switch (a.stages) {
-        case 4: return launch_tc_impl<kFp8, 4, kMode>(a, stream);
-        case 3: return launch_tc_impl<kFp8, 3, kMode>(a, stream);
-        case 2: return launch_tc_impl<kFp8, 2, kMode>(a, stream);
+        case 4: return launch_tc_impl<kFp8, 4, kMode, kStreamA>(a, stream);
+        case 3: return launch_tc_impl<kFp8, 3, kMode, kStreamA>(a, stream);
+        case 2: return launch_tc_impl<kFp8, 2, kMode, kStreamA>(a, stream);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t stream) {
-    if (mode == 0) return fp8 ? launch_tc_stages<true, 0>(a, stream) : launch_tc_stages<false, 0>(a, stream);
-    return fp8 ? launch_tc_stages<true, 1>(a, stream) : launch_tc_stages<false, 1>(a, stream);
+    if (mode == 0) {
+        if (a.stream_a) return fp8 ? launch_tc_stages<true, 0, true>(a, stream) : launch_tc_stages<false, 0, true>(a, stream);
+        return fp8 ? launch_tc_stages<true, 0, false>(a, stream) : launch_tc_stages<false, 0, false>(a, stream);
+    }
+    if (a.stream_a) return fp8 ? launch_tc_stages<true, 1, true>(a, stream) : launch_tc_stages<false, 1, true>(a, stream);
+    return fp8 ? launch_tc_stages<true, 1, false>(a, stream) : launch_tc_stages<false, 1, false>(a, stream);
 }
 
 cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream) {

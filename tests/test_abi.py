@@ -45,3 +45,41 @@ def test_structs_match_header_layout():
 
 def test_last_error_is_empty_string_initially():
     assert isinstance(_lib.last_error(), str)
+
+
+STRUCTS = {
+    "nndex_cuda_opts": "Opts",
+    "nndex_cuda_devinfo": "DevInfo",
+    "nndex_cuda_search_stats": "SearchStats",
+    "nndex_cuda_ivf_stats": "IvfStats",
+    "nndex_cuda_server_opts": "ServerOpts",
+    "nndex_cuda_request_info": "RequestInfo",
+    "nndex_cuda_server_stats": "ServerStats",
+}
+
+
+def test_ctypes_structs_match_the_c_compiler(tmp_path):
+    # sizeof and every field offset as gcc lays the header out, against the ctypes mirrors
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{ROOT}/include/nndex_cuda.h"', "int main(void) {"]
+    for cname, pyname in STRUCTS.items():
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for field, _ in getattr(_lib, pyname)._fields_:
+            lines.append(f'printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(_lib, pyname)
+        assert got[(cname, "sizeof")] == C.sizeof(cls), cname
+        for field, _ in cls._fields_:
+            assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)
+

@@ -41,6 +41,11 @@ CASES = [
     ("fp8", 20_000, 128, 128, 10, "mixture"),
     ("fp8", 40_000, 256, 200, 10, "mixture"),
     ("fp8", 9_000, 200, 40, 8, "gauss"),
+    # large D × large k: the pass-1 heaps only fit with the query slabs streamed per ring stage
+    ("bf16", 20_000, 512, 100, 100, "mixture"),
+    ("fp8", 20_000, 512, 100, 100, "mixture"),
+    # D = 768: pass 2 streams the query slabs too
+    ("bf16", 12_000, 768, 70, 100, "mixture"),
 ]
 
 
