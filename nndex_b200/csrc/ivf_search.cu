@@ -20,6 +20,7 @@
 #include "index.h"
 #include "internal.h"
 #include "ivf.h"
+#include "scan_core.cuh"
 #include "select.cuh"
 
 namespace nndex {
@@ -37,9 +38,6 @@ NNDEX_DEVICE_INLINE uint8_t* align_1024(uint8_t* p) {
 }
 
 NNDEX_DEVICE_INLINE float fold_zero(float f) { return f == 0.0f ? 0.0f : f; }
-
-template <int QB>
-constexpr int kXchg = 4 * (QB < 4 ? 1 : QB / 4);
 
 // In-place exclusive scan of v[0..n) by one block; v[n] = total.
 NNDEX_DEVICE_INLINE void block_exclusive_scan(uint32_t* v, uint32_t n, uint32_t* part) {
@@ -189,16 +187,18 @@ struct IvfScanArgs {
 };
 
 template <int QB>
-__global__ void __launch_bounds__((2 * kNcw + 1) * 32, 1)
+__global__ void __launch_bounds__(ScanShape<QB, kNcw>::kThreads, 1)
     ivf_scan_kernel(const __grid_constant__ CUtensorMap tmap, const IvfScanArgs a) {
-    constexpr uint32_t kConsumers = 2 * kNcw;
+    using S = ScanShape<QB, kNcw>;
+    using Consumer = ScanConsumer<QB, kNcw, kStages>;
+    constexpr uint32_t kConsumers = S::kConsumers;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* stage_base = align_1024(smem_raw);
     const uint32_t dq = a.dq, cap = a.cap, k = a.k;
     float* q_s = reinterpret_cast<float*>(stage_base + static_cast<size_t>(kStages) * kStageBytes);
     uint64_t* cand = reinterpret_cast<uint64_t*>(q_s + static_cast<size_t>(QB) * dq);
     float* xchg = reinterpret_cast<float*>(cand + static_cast<size_t>(QB) * cap);
-    uint32_t* hist = reinterpret_cast<uint32_t*>(xchg + kConsumers * 32 * kXchg<QB>);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(xchg + kConsumers * 32 * S::kXchg);
     uint64_t* thr = reinterpret_cast<uint64_t*>(hist + kConsumers * 256);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(thr + QB);
     uint32_t* qid = cnt + QB;
@@ -221,17 +221,9 @@ __global__ void __launch_bounds__((2 * kNcw + 1) * 32, 1)
     }
     __syncthreads();
 
-    // consumer constants
-    const uint32_t rgrp = warp % kNcw, half = warp / kNcw;
-    const uint32_t dg = lane & 3u, rg = lane >> 2;
-    const uint32_t ch = dg + 4 * half;
-    const uint32_t phys = (ch ^ rg) * 16;
     constexpr uint32_t nthreads_c = kConsumers * 32;
-    float* my_x = xchg + (warp * 32 + lane) * kXchg<QB>;
-    const float* peer_x = xchg + (((warp + kNcw) % kConsumers) * 32 + lane) * kXchg<QB>;
-    const uint32_t x_base = smem_u32(stage_base) + (rgrp * 32 + rg) * 128 + phys;
-    const uint32_t q_base = smem_u32(q_s) + ch * 16;
-    const uint32_t q_stride = dq * 4;
+    const Consumer con(warp < kConsumers ? warp : 0, lane, stage_base, q_s, dq, xchg);
+    auto row_key = [&](uint64_t r) { return a.row_map[r]; };
 
     uint32_t it = 0;  // ring position (producer and consumers walk the same sequence)
     for (;;) {
@@ -309,113 +301,12 @@ __global__ void __launch_bounds__((2 * kNcw + 1) * 32, 1)
                 thr[tid] = 0ull;
             }
             named_bar_sync(1, nthreads_c);
-            float acc[4][QB];
+            float acc[4][Consumer::QW];
             for (uint32_t t = 0; t < ntiles; ++t) {
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int b = 0; b < QB; ++b) acc[i][b] = 0.0f;
-#pragma unroll 1
-                for (uint32_t bx = 0; bx < nbox; ++bx, ++it) {
-                    const uint32_t s = it & (kStages - 1), parity = (it / kStages) & 1u;
-                    float4 qv[QB];
-#pragma unroll
-                    for (int b = 0; b < QB; ++b) qv[b] = lds128(q_base + b * q_stride + bx * 128);
-                    if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], parity, kWaitBudgetCycles)) {
-                        *abort_flag = 1;
-                        record_status(a.status, kStatusTimeout);
-                    }
-                    const uint32_t xa = x_base + s * kStageBytes;
-                    float4 x[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) x[i] = lds128(xa + i * 8 * 128);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].x, qv[b].x, acc[i][b]);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].y, qv[b].y, acc[i][b]);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].z, qv[b].z, acc[i][b]);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].w, qv[b].w, acc[i][b]);
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&empty_bar[s]);
-                }
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int b = 0; b < QB; ++b) {
-                        float v = acc[i][b];
-                        v += __shfl_xor_sync(0xffffffffu, v, 1);
-                        v += __shfl_xor_sync(0xffffffffu, v, 2);
-                        acc[i][b] = v;
-                    }
-                {
-                    int j = 0;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int b = 0; b < QB; ++b)
-                            if ((b & 3) == static_cast<int>(dg)) {
-                                my_x[j] = acc[i][b];
-                                ++j;
-                            }
-                }
-                named_bar_sync(1, nthreads_c);
-                const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * kTileRows + rgrp * 32 + rg;
-                {
-                    int j = 0;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int b = 0; b < QB; ++b)
-                            if ((b & 3) == static_cast<int>(dg)) {
-                                const float other = peer_x[j];
-                                ++j;
-                                if ((i >> 1) == static_cast<int>(half) && static_cast<uint32_t>(b) < nqg) {
-                                    const uint64_t r = tile_row0 + 8 * i;
-                                    if (r < row_end) {
-                                        const float v = half == 0 ? acc[i][b] + other : other + acc[i][b];
-                                        const uint64_t key = make_key(v, a.row_map[r]);
-                                        if (key > thr[b]) {
-                                            const uint32_t pos = atomicAdd(&cnt[b], 1u);
-                                            if (pos < cap)
-                                                cand[static_cast<size_t>(b) * cap + pos] = key;
-                                            else
-                                                record_status(a.status, kStatusOverflow);
-                                        }
-                                    }
-                                }
-                            }
-                }
-                named_bar_sync(1, nthreads_c);
-                bool need = false;
-                const bool last = (t + 1 == ntiles);
-#pragma unroll
-                for (int b = 0; b < QB; ++b)
-                    if (static_cast<uint32_t>(b) < nqg) need |= last ? (cnt[b] > k) : (cnt[b] + kTileRows > cap);
-                if (need) {
-                    for (uint32_t b = warp; b < nqg; b += kConsumers) {
-                        const uint32_t n = cnt[b] < cap ? cnt[b] : cap;
-                        if (n > k) {
-                            uint64_t* buf = cand + static_cast<size_t>(b) * cap;
-                            const uint64_t kth = warp_radix_kth(buf, n, k, hist + warp * 256);
-                            const uint32_t m = warp_compact_ge(buf, n, kth);
-                            if (lane == 0) {
-                                cnt[b] = m;
-                                thr[b] = kth;
-                            }
-                        }
-                    }
-                    named_bar_sync(1, nthreads_c);
-                }
+                con.accumulate(acc, nbox, it, full_bar, empty_bar, abort_flag, a.status);
+                con.insert(acc, row_begin + static_cast<uint64_t>(t) * kTileRows, row_end, nqg, row_key, thr, cnt, cand,
+                           cap, a.status);
+                scan_flush<QB, kNcw>(t + 1 == ntiles, nqg, k, cap, warp, lane, cnt, thr, cand, hist);
             }
             for (uint32_t b = warp; b < nqg; b += kConsumers) {
                 const uint32_t n = cnt[b] < k ? cnt[b] : k;
@@ -499,12 +390,13 @@ int grow(T*& p, size_t& cap, size_t n, const char* what) {
 }
 
 size_t ivf_scan_smem(uint32_t qb, uint32_t dq, uint32_t cap) {
+    const size_t consumers = scan_consumers(qb, kNcw);
     size_t b = 1024;
     b += static_cast<size_t>(kStages) * kStageBytes;
     b += static_cast<size_t>(qb) * dq * 4;
     b += static_cast<size_t>(qb) * cap * 8;
-    b += static_cast<size_t>(2 * kNcw) * 32 * 4 * (qb < 4 ? 1 : qb / 4) * 4;
-    b += 2 * kNcw * 256 * 4;
+    b += consumers * 32 * scan_xchg_per_lane(qb) * 4;
+    b += consumers * 256 * 4;
     b += qb * 8 + (3 * qb + (qb & 1)) * 4;
     b += 4 * 8 + kStages * 16 + 16;
     return b;
@@ -515,7 +407,7 @@ cudaError_t launch_scan(const CUtensorMap& tmap, const IvfScanArgs& a, uint32_t 
     auto kern = ivf_scan_kernel<QB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    kern<<<grid, (2 * kNcw + 1) * 32, smem, s>>>(tmap, a);
+    kern<<<grid, ScanShape<QB, kNcw>::kThreads, smem, s>>>(tmap, a);
     count_launch();
     return cudaGetLastError();
 }

@@ -11,13 +11,9 @@
 // (nbox = dq / 32 slabs per tile). One producer warp issues the loads into a ring of `stages`
 // slabs guarded by full/empty mbarriers; NCW consumer warps compute.
 //
-// Consumer mapping. 2·NCW consumer warps: warp = half·NCW + row group. The row group owns tile
-// rows [32·rgrp, 32·rgrp + 32); lane = (rg = lane/4, dg = lane%4) owns rows rg + 8i (i < 4) and,
-// inside each 128 B slab, the 16 B chunk 4·half + dg. With the 128 B swizzle
-// (chunk' = chunk ^ (row % 8) = chunk ^ rg) every base load is conflict-free and every query load
-// is a 4-address broadcast. Each lane keeps 4 rows × QB queries of FP32 partial sums (a fixed FMA
-// order per (row, query), independent of the batch's composition); the 4 dg lanes combine with
-// two xor shuffles, and the two halves add through shared memory, at the end of a tile.
+// Consumers (scan_core.cuh): 2·NCW warps per group of up to 8 queries (16 warps at 16 queries per
+// CTA), each lane a 4-row × 8-query block of FP32 partial sums in a fixed FMA order per (row, query),
+// independent of the batch's composition.
 //
 // Fused top-k. Per query, a shared-memory buffer of `cap` 64-bit keys (common.cuh) and the
 // current k-th best key `thr`. A score enters the buffer only if its key beats `thr`; when a
@@ -28,6 +24,7 @@
 
 #include "common.cuh"
 #include "internal.h"
+#include "scan_core.cuh"
 #include "select.cuh"
 
 namespace nndex {
@@ -39,37 +36,27 @@ NNDEX_DEVICE_INLINE uint8_t* align_1024(uint8_t* p) {
     return p + ((1024u - (a & 1023u)) & 1023u);
 }
 
-// Values a consumer lane exchanges with its partner warp at the end of a tile:
-// 4 rows × the queries b ≡ dg (mod 4) it inserts.
-template <int QB>
-constexpr int kXchgPerLane = 4 * (QB < 4 ? 1 : QB / 4);
-
-template <int QB, int NCW>
-struct ScanSmem {
-    static constexpr int TR = NCW * 32;
-    static constexpr uint32_t kStageBytes = TR * 128;
-};
-
 }  // namespace
 
 template <int QB, int NCW, int ST>
-__global__ void __launch_bounds__((2 * NCW + 1) * 32, 1)
+__global__ void __launch_bounds__(ScanShape<QB, NCW>::kThreads, 1)
     scan_fp32_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restrict__ queries, uint32_t nq,
                      uint32_t dq, uint64_t rows, uint32_t k, uint32_t cap,
                      const uint32_t* __restrict__ row_map, uint64_t* __restrict__ ws_keys,
                      uint32_t* __restrict__ status) {
-    constexpr int TR = ScanSmem<QB, NCW>::TR;
-    constexpr uint32_t kStageBytes = ScanSmem<QB, NCW>::kStageBytes;
-    constexpr uint32_t kConsumers = 2 * NCW;  // warp pairs split each slab's 8 chunks 4 + 4
-    constexpr uint32_t stages = ST;           // ring depth (power of two)
-    static_assert((ST & (ST - 1)) == 0, "ring depth must be a power of two");
+    using S = ScanShape<QB, NCW>;
+    using Consumer = ScanConsumer<QB, NCW, ST>;
+    constexpr int TR = S::kTileRows;
+    constexpr uint32_t kStageBytes = S::kStageBytes;
+    constexpr uint32_t kConsumers = S::kConsumers;
+    constexpr uint32_t stages = ST;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = align_1024(smem_raw);
     uint8_t* stage_base = smem;
     float* q_s = reinterpret_cast<float*>(stage_base + static_cast<size_t>(stages) * kStageBytes);
     uint64_t* cand = reinterpret_cast<uint64_t*>(q_s + static_cast<size_t>(QB) * dq);
-    float* xchg = reinterpret_cast<float*>(cand + static_cast<size_t>(QB) * cap);  // kConsumers × 32 × 4·QB/4
-    uint32_t* hist = reinterpret_cast<uint32_t*>(xchg + kConsumers * 32 * kXchgPerLane<QB>);
+    float* xchg = reinterpret_cast<float*>(cand + static_cast<size_t>(QB) * cap);  // kConsumers × 32 × kXchg
+    uint32_t* hist = reinterpret_cast<uint32_t*>(xchg + kConsumers * 32 * S::kXchg);
     uint64_t* thr = reinterpret_cast<uint64_t*>(hist + kConsumers * 256);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(thr + QB);
     uint64_t* full_bar = reinterpret_cast<uint64_t*>(cnt + QB + (QB & 1));
@@ -145,133 +132,14 @@ __global__ void __launch_bounds__((2 * NCW + 1) * 32, 1)
     }
 
     // ---------------- consumers ----------------
-    // warp = half·NCW + row group; the row group owns tile rows [32·rgrp, 32·rgrp + 32), the half
-    // owns 16 B chunks 4·half + dg of every 128 B slab.
-    const uint32_t rgrp = warp % NCW, half = warp / NCW;
-    const uint32_t dg = lane & 3u, rg = lane >> 2;
-    const uint32_t ch = dg + 4 * half;
-    const uint32_t phys = (ch ^ rg) * 16;
-    float acc[4][QB];
+    const Consumer con(warp, lane, stage_base, q_s, dq, xchg);
+    auto row_key = [&](uint64_t r) { return row_map ? row_map[r] : static_cast<uint32_t>(r); };
+    float acc[4][Consumer::QW];
     uint32_t it = 0;
-    constexpr uint32_t nthreads_c = kConsumers * 32;
-    float* my_x = xchg + (warp * 32 + lane) * kXchgPerLane<QB>;
-    const float* peer_x = xchg + (((warp + NCW) % kConsumers) * 32 + lane) * kXchgPerLane<QB>;
-    const uint32_t x_base = smem_u32(stage_base) + (rgrp * 32 + rg) * 128 + phys;
-    const uint32_t q_base = smem_u32(q_s) + ch * 16;
-    const uint32_t q_stride = dq * 4;
     for (uint32_t t = 0; t < ntiles; ++t) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int b = 0; b < QB; ++b) acc[i][b] = 0.0f;
-#pragma unroll 1
-        for (uint32_t bx = 0; bx < nbox; ++bx, ++it) {
-            const uint32_t s = it & (ST - 1), parity = (it / ST) & 1u;
-            // Queries do not depend on the slab: load them before waiting for it.
-            float4 qv[QB];
-#pragma unroll
-            for (int b = 0; b < QB; ++b) qv[b] = lds128(q_base + b * q_stride + bx * 128);
-            if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], parity, kWaitBudgetCycles)) {
-                *abort_flag = 1;
-                record_status(status, kStatusTimeout);
-            }
-            const uint32_t xa = x_base + s * kStageBytes;
-            float4 x[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) x[i] = lds128(xa + i * 8 * 128);
-            // 4·QB independent accumulators per component: no FMA dependency stalls.
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].x, qv[b].x, acc[i][b]);
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].y, qv[b].y, acc[i][b]);
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].z, qv[b].z, acc[i][b]);
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int b = 0; b < QB; ++b) acc[i][b] = fmaf(x[i].w, qv[b].w, acc[i][b]);
-            // The slab's values are consumed (the FMAs above read them): release it to the producer.
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty_bar[s]);
-        }
-        // Combine the four dg partial sums of this half: ((p0 + p1) + (p2 + p3)) in every lane.
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int b = 0; b < QB; ++b) {
-                float v = acc[i][b];
-                v += __shfl_xor_sync(0xffffffffu, v, 1);
-                v += __shfl_xor_sync(0xffffffffu, v, 2);
-                acc[i][b] = v;
-            }
-        // Exchange with the other half: lane dg publishes the (i, b) it inserts, b ≡ dg (mod 4).
-        // Half 0 inserts rows i = 0, 1 and half 1 rows i = 2, 3; both add (half0 + half1).
-        {
-            int j = 0;
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int b = 0; b < QB; ++b)
-                    if ((b & 3) == static_cast<int>(dg)) {
-                        my_x[j] = acc[i][b];
-                        ++j;
-                    }
-        }
-        named_bar_sync(1, nthreads_c);
-        const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * TR + rgrp * 32 + rg;
-        {
-            int j = 0;
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int b = 0; b < QB; ++b)
-                    if ((b & 3) == static_cast<int>(dg)) {
-                        const float other = peer_x[j];
-                        ++j;
-                        if ((i >> 1) == static_cast<int>(half) && static_cast<uint32_t>(b) < nqg) {
-                            const uint64_t r = tile_row0 + 8 * i;
-                            if (r < row_end) {
-                                const float v = half == 0 ? acc[i][b] + other : other + acc[i][b];
-                                const uint32_t orig = row_map ? row_map[r] : static_cast<uint32_t>(r);
-                                const uint64_t key = make_key(v, orig);
-                                if (key > thr[b]) {
-                                    const uint32_t pos = atomicAdd(&cnt[b], 1u);
-                                    if (pos < cap)
-                                        cand[static_cast<size_t>(b) * cap + pos] = key;
-                                    else
-                                        record_status(status, kStatusOverflow);
-                                }
-                            }
-                        }
-                    }
-        }
-        named_bar_sync(1, nthreads_c);
-        bool need = false;
-        const bool last = (t + 1 == ntiles);
-#pragma unroll
-        for (int b = 0; b < QB; ++b)
-            if (static_cast<uint32_t>(b) < nqg) need |= last ? (cnt[b] > k) : (cnt[b] + TR > cap);
-        if (need) {
-            for (uint32_t b = warp; b < nqg; b += kConsumers) {
-                const uint32_t n = cnt[b] < cap ? cnt[b] : cap;
-                if (n > k) {
-                    uint64_t* buf = cand + static_cast<size_t>(b) * cap;
-                    const uint64_t kth = warp_radix_kth(buf, n, k, hist + warp * 256);
-                    const uint32_t m = warp_compact_ge(buf, n, kth);
-                    if (lane == 0) {
-                        cnt[b] = m;
-                        thr[b] = kth;
-                    }
-                }
-            }
-            named_bar_sync(1, nthreads_c);
-        }
+        con.accumulate(acc, nbox, it, full_bar, empty_bar, abort_flag, status);
+        con.insert(acc, row_begin + static_cast<uint64_t>(t) * TR, row_end, nqg, row_key, thr, cnt, cand, cap, status);
+        scan_flush<QB, NCW>(t + 1 == ntiles, nqg, k, cap, warp, lane, cnt, thr, cand, hist);
     }
     // Write this CTA's k best keys per query (0 = empty slot).
     for (uint32_t b = warp; b < nqg; b += kConsumers) {
@@ -364,12 +232,13 @@ constexpr int kNcw = 4;
 constexpr int kTileRows = kNcw * 32;
 
 size_t scan_smem_bytes(uint32_t qb, uint32_t dq, uint32_t cap, uint32_t stages) {
+    const size_t consumers = scan_consumers(qb, kNcw);
     size_t b = 1024;  // alignment slack
     b += static_cast<size_t>(stages) * kTileRows * 128;
     b += static_cast<size_t>(qb) * dq * 4;
     b += static_cast<size_t>(qb) * cap * 8;
-    b += static_cast<size_t>(2 * kNcw) * 32 * 4 * (qb < 4 ? 1 : qb / 4) * 4;  // partner exchange
-    b += 2 * kNcw * 256 * 4;
+    b += consumers * 32 * scan_xchg_per_lane(qb) * 4;  // partner exchange
+    b += consumers * 256 * 4;
     b += qb * 8 + (qb + (qb & 1)) * 4;
     b += static_cast<size_t>(stages) * 16 + 16;
     return b;
@@ -382,7 +251,7 @@ cudaError_t launch_qb_st(const ScanArgs& a, const ScanPlan& p, cudaStream_t stre
                                          static_cast<int>(p.smem_bytes));
     if (e != cudaSuccess) return e;
     dim3 grid(p.ctas_per_group, p.groups);
-    kern<<<grid, (2 * kNcw + 1) * 32, p.smem_bytes, stream>>>(*a.tmap, a.queries, a.nq, a.dq, a.rows, a.k, p.cap,
+    kern<<<grid, ScanShape<QB, kNcw>::kThreads, p.smem_bytes, stream>>>(*a.tmap, a.queries, a.nq, a.dq, a.rows, a.k, p.cap,
                                                               a.row_map, a.ws_keys, a.status);
     count_launch();
     return cudaGetLastError();
