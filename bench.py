@@ -145,17 +145,20 @@ def make_mixture(rows, dims, centers, sigma, seed, device, center_seed=None, zip
     g = torch.Generator(device=device)
     g.manual_seed(center_seed if center_seed is not None else seed)
     c = torch.randn((centers, dims), generator=g, device=device, dtype=torch.float32)
-    w = None
+    cdf = None
     if zipf:
+        # cluster sizes ∝ rank^-zipf; each row's centre from one uniform draw through the CDF
+        # (a plain inverse-CDF lookup: the same rows on every run and GPU configuration)
         w = torch.arange(1, centers + 1, device=device, dtype=torch.float64).pow(-float(zipf))
-        w = (w / w.sum()).float()
+        cdf = torch.cumsum(w / w.sum(), 0)
     g.manual_seed(seed + 1)
     out = torch.empty((rows, dims), device=device, dtype=torch.float32)
     step = 1 << 18
     for r0 in range(0, rows, step):
         r1 = min(rows, r0 + step)
-        if w is not None:
-            a = torch.multinomial(w, r1 - r0, replacement=True, generator=g)
+        if cdf is not None:
+            u = torch.rand((r1 - r0,), generator=g, device=device, dtype=torch.float64)
+            a = torch.searchsorted(cdf, u).clamp_(max=centers - 1)
         else:
             a = torch.randint(0, centers, (r1 - r0,), generator=g, device=device)
         x = torch.randn((r1 - r0, dims), generator=g, device=device, dtype=torch.float32)
@@ -592,8 +595,8 @@ def run_ivf(args, dev, L, world):
                         zipf=args.ivf_zipf)
     q = make_mixture(nq, dims, args.ivf_centers, args.ivf_sigma, seed + 7, dev, center_seed=args.seed + 200,
                      zipf=args.ivf_zipf)
-    # fingerprint of the synthetic base (a strided sample), so runs on different boxes can be compared
-    data_fp = float(base[::997].double().sum().item())
+    # exact checksum of the synthetic base (its bits as integers), so runs can be compared
+    data_fp = int(base.view(torch.int32).to(torch.int64).sum().item())
     opts = _lib.Opts()
     opts.device = local
     opts.nlist = args.ivf_nlist
@@ -638,8 +641,12 @@ def run_ivf(args, dev, L, world):
     peak, peak_kind = measured_peaks()
     per = {}
     layout = None
-    for np_ in [int(x) for x in args.ivf_nprobe.split(",") if x]:
+    from nndex_b200._lib import NNDEX_PRECISION_AUTO, NNDEX_PRECISION_FP32
+    runs = [(str(n), n, NNDEX_PRECISION_AUTO) for n in [int(x) for x in args.ivf_nprobe.split(",") if x]]
+    runs += [(f"{n}_fp32_list_scan", n, NNDEX_PRECISION_FP32) for n in [int(x) for x in args.ivf_nprobe.split(",") if x]]
+    for name, np_, prec in runs:
         L.nndex_cuda_set_nprobe(h, np_)
+        L.nndex_cuda_set_precision(h, prec, 0)
         for _ in range(3):
             if L.nndex_cuda_search_batch_device(h, q.data_ptr(), nq, dims, k, oi.data_ptr(), os_.data_ptr(),
                                                 cnt.data_ptr(), sptr, 1) != 0:
@@ -667,10 +674,15 @@ def run_ivf(args, dev, L, world):
         max_ms, total_q = aggregate(ms, nq * args.ivf_steps, world, dev)
         got = oi.cpu().tolist()
         hits = sum(len(set(got[i]) & exact_sets[i]) for i in range(nq))
-        scan_avg = scan_ms.value / max(scan_n.value, 1)
-        streamed_b = stats.ivf_rows_streamed * dims * 4
+        tc = stats.path == 5
+        scan_avg = scan_ms.value / args.ivf_steps  # all scan launches of a batch (the tensor-core scan: 2 passes)
+        passes = (scan_n.value / args.ivf_steps) if tc else 1.0
+        streamed_b = stats.ivf_rows_streamed * dims * (2 if tc else 4) * passes
         union_b = stats.ivf_rows_union * dims * 4
-        per[str(np_)] = {
+        per[name] = {
+            "path": "tensor-core list scan" if stats.path == 5 else "FP32 list scan",
+            "second_pass_queries": stats.second_pass_queries,
+            "fp32_fallback_queries": stats.fp32_fallback_queries,
             "queries_per_s": total_q / (max_ms / 1e3),
             "ms_per_batch": max_ms / args.ivf_steps,
             "recall_at_k_vs_exact": hits / (nq * k),
@@ -681,7 +693,10 @@ def run_ivf(args, dev, L, world):
             "scan_gbs_streamed": streamed_b / (scan_avg / 1e3) / 1e9,
             "scan_frac_of_hbm_streamed": streamed_b / (scan_avg / 1e3) / 1e9 / peak,
             "scan_gbs_union": union_b / (scan_avg / 1e3) / 1e9,
-            "scan_fp32_tflops": 2.0 * stats.rows_scanned * dims / (scan_avg / 1e3) / 1e12,
+            "scan_fp32_tflops": None if tc else 2.0 * stats.rows_scanned * dims / (scan_avg / 1e3) / 1e12,
+            # tensor-core scan: executed MMA work, 128-query blocks × streamed rows × D, per pass
+            "scan_tensor_tflops": (2.0 * 128 * stats.ivf_rows_streamed * dims * passes / (scan_avg / 1e3) / 1e12
+                                   if tc else None),
             "kernel_launches_per_batch": (n1 - n0) / args.ivf_steps,
         }
     # CPU baseline: the reference's IVF search restated (oracle/) on the same index, host threads.

@@ -323,6 +323,14 @@ int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
     }
 }
 
+// IVF batches: the tensor-core list scan (5) from a few dozen queries, when the index's precision
+// allows low-precision scoring and k fits its pass-1 heaps; else the FP32 list scan (4).
+int CudaIndex::ivf_path(uint64_t nq, uint64_t kcap) const {
+    if (precision == NNDEX_PRECISION_FP32 || nq < 64 || !ivf || !ivf->d_reordered16) return 4;
+    const TcPlan p1 = plan_tc(kcap, false);
+    return (p1.kp >= kcap && p1.kp > 0 && plan_tc(0, false).stages > 0) ? 5 : 4;
+}
+
 uint32_t CudaIndex::tc_chunks(bool fp8) const {
     return static_cast<uint32_t>((fp8 ? kf8 : kb16 * 2) / 128);
 }
@@ -381,10 +389,10 @@ int CudaIndex::enqueue_prep_queries(const float* d_raw, uint64_t n, int mode, in
     p.mode = mode;
     p.err = d_err;
     p.sm_count = sm_count;
-    if (path == 2 || path == 3) {
+    if (path == 2 || path == 3 || path == 5) {
         const uint64_t nq_alloc = (n + 127) / 128 * 128;
         if ((st = grow_device(d_q_resid, cap_q_resid, n, "query buffer"))) return st;
-        if (path == 2) {
+        if (path == 2 || path == 5) {
             const bool grew = nq_alloc * kb16 > cap_q_bf16;
             if ((st = grow_device(d_q_bf16, cap_q_bf16, nq_alloc * kb16, "query buffer"))) return st;
             if (grew) cudaMemsetAsync(d_q_bf16, 0, cap_q_bf16 * sizeof(__nv_bfloat16), s);
@@ -643,7 +651,7 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
     const uint64_t chunk = kMaxBatchChunk;
     for (uint64_t q0 = 0; q0 < nq; q0 += chunk) {
         const uint64_t n = std::min<uint64_t>(chunk, nq - q0);
-        const int path = uses_ivf() ? 4 : choose_path(n, kcap);
+        const int path = uses_ivf() ? ivf_path(n, kcap) : choose_path(n, kcap);
         int st;
         if ((st = ensure_query_capacity(n))) return st;
         if ((st = ensure_result_capacity(n, kcap))) return st;
@@ -653,8 +661,12 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         cudaMemcpyAsync(d_qraw, h_q, n * dims * sizeof(float), cudaMemcpyHostToDevice, stream);
         if ((st = enqueue_prep_queries(d_qraw, n, mode, path, stream))) return st;
         if (path == 4) {
-            if ((st = ivf_search(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
-                                 stream)))
+            if ((st = ivf_search(*this, d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim,
+                                 d_cnt, stream)))
+                return st;
+        } else if (path == 5) {
+            if ((st = ivf_search_tc(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
+                                    stream)))
                 return st;
         } else if (path == 1) {
             if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
@@ -710,13 +722,18 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
     bool synced = false;
     for (uint64_t q0 = 0; q0 < nq; q0 += kMaxBatchChunk) {
         const uint64_t n = std::min<uint64_t>(kMaxBatchChunk, nq - q0);
-        const int path = uses_ivf() ? 4 : choose_path(n, kcap);
+        const int path = uses_ivf() ? ivf_path(n, kcap) : choose_path(n, kcap);
         if ((st = enqueue_prep_queries(d_queries + q0 * dims, n, normalized ? 2 : 0, path, s))) return st;
         uint64_t* oi = d_idx_out + q0 * kcap;
         float* os = d_sim_out + q0 * kcap;
         uint32_t* oc = d_cnt_out ? d_cnt_out + q0 : nullptr;
         if (path == 4) {
-            if ((st = ivf_search(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s))) return st;
+            if ((st = ivf_search(*this, d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s)))
+                return st;
+        } else if (path == 5) {
+            if ((st = ivf_search_tc(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s)))
+                return st;
+            synced = true;
         } else if (path == 1) {
             if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
                                          static_cast<uint32_t>(kcap), oi, os, oc, s)))
@@ -736,7 +753,7 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
         mark_done(s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_error(e, "search");
-        if (uses_ivf()) {
+        if (stats.path == 4) {
             stats.rows_scanned = ivf_scratch.h_probed[0];
             stats.ivf_rows_streamed = ivf_scratch.h_probed[1];
             stats.ivf_rows_union = ivf_scratch.h_probed[2];

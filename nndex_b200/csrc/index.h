@@ -165,6 +165,7 @@ struct CudaIndex {
                       uint32_t* d_cnt_out, cudaStream_t s, int synchronize);
     // Path choice for a batch: 1 = FP32 scan, 2 = BF16 tensor-core scan, 3 = FP8 tensor-core scan.
     int choose_path(uint64_t nq, uint64_t kcap) const;
+    int ivf_path(uint64_t nq, uint64_t kcap) const;
     struct TcPlan {
         uint32_t kp = 0;        // pass-1 heap entries per query (0: no plan)
         uint32_t stages = 0;    // ring depth

@@ -94,6 +94,17 @@ struct TcParams {
     uint32_t* cand_rows = nullptr;        // pass 2: nq × cap2
     uint32_t* cand_cnt = nullptr;         // pass 2: nq, zeroed before the launch
     uint32_t* status = nullptr;
+    // IVF item mode (the list scan on the tensor cores): CTA b runs work item b of the IVF plan —
+    // one chunk of one list's reordered rows against one gathered block of ≤ 128 queries probing it.
+    const uint32_t* it_item_off = nullptr;    // nlist + 1: first work item of each list
+    const uint32_t* it_list_cnt = nullptr;    // nlist: queries probing each list
+    const uint32_t* it_offsets = nullptr;     // nlist + 1: each list's reordered row range
+    const uint32_t* it_qblock_off = nullptr;  // nlist + 1: first gathered query block of each list
+    const uint32_t* it_lane_qid = nullptr;    // blocks × 128: query of each lane (0xFFFFFFFF = none)
+    const uint32_t* it_lane_slot = nullptr;   // blocks × 128: the query's output slot for chunk 0
+    const uint32_t* row_map = nullptr;        // reordered row → original row
+    uint32_t it_nlist = 0;
+    uint32_t it_chunk_rows = 0;
 };
 struct TcArgs {
     const CUtensorMap* tmap_q = nullptr;  // quantised queries [nq_alloc × K], box {128 B, 128 rows}
@@ -102,6 +113,7 @@ struct TcArgs {
     uint32_t nranges = 0;
     uint32_t stages = 4;                  // base ring depth (2..4)
     bool stream_a = false;                // pass 1: query slabs staged per ring stage, not resident
+    uint32_t items = 0;                   // IVF item mode: number of work items (grid), 0 = off
 };
 size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8, bool stream_a);
 // Deepest base ring (4, 3 or 2 stages) that fits k′ heaps in `smem_limit`; 0 if none fits.
@@ -130,7 +142,7 @@ cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q
 cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float* queries, const uint32_t* ids,
                                     uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
                                     uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
-                                    cudaStream_t stream);
+                                    cudaStream_t stream, bool by_query = false);
 cudaError_t launch_max_reduce(const float* v, uint64_t n, unsigned int* out, cudaStream_t stream);
 
 // Maximum k the fused scan kernels select in shared memory.

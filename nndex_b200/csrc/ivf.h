@@ -34,6 +34,13 @@ struct IvfIndex {
     std::vector<uint64_t> h_init_rows;  // rows chosen by k-means++ (diagnostics / parity)
     uint64_t max_list = 0;
     CUtensorMap tmap_reordered{};
+    // BF16 copy of the reordered rows for the tensor-core list scan: kb16 = dims rounded up to 64,
+    // per row an upper bound of ‖x − bf16(x)‖, and the largest of them.
+    uint64_t kb16 = 0;
+    __nv_bfloat16* d_reordered16 = nullptr;  // rows_alloc × kb16
+    float* d_res16 = nullptr;                // rows (reordered order)
+    float eps16 = 0.0f;
+    CUtensorMap tmap_reordered16{};
     nndex_cuda_ivf_stats stats{};
 
     ~IvfIndex();
@@ -42,6 +49,7 @@ struct IvfIndex {
 // Per-search scratch of the IVF path (one per CudaIndex view; grown on demand).
 struct IvfScratch {
     uint32_t nprobe = 0;                // 0 = choose_nprobe per search
+    uint32_t tc_stride = 1;             // tensor-core scan: pass 1 on every n-th tile (autotuned)
     uint32_t* d_probes = nullptr;       size_t cap_probes = 0;
     uint32_t* d_list_cnt = nullptr;     size_t cap_list_cnt = 0;   // nlist: queries probing each list
     uint32_t* d_list_fill = nullptr;    size_t cap_list_fill = 0;
@@ -52,7 +60,11 @@ struct IvfScratch {
     uint32_t* d_q_slot_off = nullptr;   size_t cap_q_slot_off = 0; // B + 1
     unsigned long long* d_counters = nullptr; size_t cap_counters = 0;  // work counter, totals, rows probed
     uint64_t* d_ws = nullptr;           size_t cap_ws = 0;         // slots × k keys
-    unsigned long long* h_probed = nullptr;  // pinned [3]: rows probed (Σ over queries), streamed, union
+    uint32_t* d_qblock_off = nullptr;   size_t cap_qblock_off = 0; // nlist + 1 (tensor-core scan)
+    __nv_bfloat16* d_g16 = nullptr;     size_t cap_g16 = 0;        // gathered query blocks × 128 × kb16
+    uint32_t* d_lane_qid = nullptr;     size_t cap_lane_qid = 0;   // gathered blocks × 128
+    uint32_t* d_lane_slot = nullptr;    size_t cap_lane_slot = 0;
+    unsigned long long* h_probed = nullptr;  // pinned [8]: FP32 scan: rows probed (Σ over queries), streamed, union
 
     ~IvfScratch();
 };
@@ -61,10 +73,14 @@ struct IvfScratch {
 // and the seed come from ix.opts (0 = the reference's policy). Returns an NNDEX status.
 int ivf_build(CudaIndex& ix);
 
-// Enqueues the IVF search of `nq` normalised queries (ix.d_qn, stride ds) with capped k into the
-// device outputs (rows of `k` slots). Returns an NNDEX status.
-int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
-               cudaStream_t s);
+// Enqueues the IVF search of `nq` normalised queries (stride ds) with capped k into the device
+// outputs (rows of `k` slots), on the FP32 list scan. Returns an NNDEX status.
+int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim,
+               uint32_t* o_cnt, cudaStream_t s);
+// The same result on the tensor cores: BF16 list scan with certified candidates, exact FP32 rerank
+// (the queries of ix.d_qn and their BF16 copies ix.d_q_bf16 / ix.d_q_resid). Synchronises the stream.
+int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                  cudaStream_t s);
 
 // src/approx.rs:305-311 choose_nlist and 318-336 choose_nprobe.
 uint64_t ivf_choose_nlist(uint64_t rows);

@@ -25,6 +25,7 @@
 //   * update: a stable counting sort by cluster (row order kept inside each cluster) and FP64 sums
 //     in that order — the reference's summation order — then the reference's normalisation, each
 //     operation rounded as in Rust (no contraction).
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -444,6 +445,27 @@ __global__ void fill_f32_kernel(float* __restrict__ p, uint64_t n, float v) {
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
         p[i] = v;
+}
+
+// BF16 copy of FP32 rows (round to nearest, as the index's own BF16 copy) with an upper bound of
+// each row's residual norm ‖x − bf16(x)‖. One warp per row.
+__global__ void bf16_rows_kernel(const float* __restrict__ src, uint32_t ds, uint64_t rows, __nv_bfloat16* __restrict__ out,
+                                 uint32_t kb, float* __restrict__ res_up) {
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t r = warp; r < rows; r += nwarps) {
+        double r2 = 0.0;
+        for (uint32_t d = lane; d < kb; d += 32) {
+            const float v = d < ds ? src[r * ds + d] : 0.0f;
+            const __nv_bfloat16 b = __float2bfloat16_rn(v);
+            const float e = v - __bfloat162float(b);  // exact: the rounding residual
+            r2 = fma(static_cast<double>(e), static_cast<double>(e), r2);
+            out[r * kb + d] = b;
+        }
+        r2 = warp_sum_d(r2);
+        if (lane == 0) res_up[r] = sqrt_up(r2);
+    }
 }
 
 // Rows → centroid slots (the seeded centroids are copies of rows).
@@ -932,6 +954,8 @@ __global__ void centroid_normalize_kernel(const double* __restrict__ sums, uint3
 // ------------------------------------------------------------------------------------------
 
 IvfIndex::~IvfIndex() {
+    cudaFree(d_reordered16);
+    cudaFree(d_res16);
     cudaFree(d_centroids);
     cudaFree(d_cent_t);
     cudaFree(d_reordered);
@@ -940,6 +964,10 @@ IvfIndex::~IvfIndex() {
 }
 
 IvfScratch::~IvfScratch() {
+    cudaFree(d_qblock_off);
+    cudaFree(d_g16);
+    cudaFree(d_lane_qid);
+    cudaFree(d_lane_slot);
     cudaFree(d_probes);
     cudaFree(d_list_cnt);
     cudaFree(d_list_fill);
@@ -1031,7 +1059,8 @@ int ivf_build(CudaIndex& ix) {
     v.iters = iters;
     ix.ivf_scratch.nprobe = ix.opts.nprobe;
     v.nlist_pad = (nlist + 255) / 256 * 256;
-    const uint64_t kb = (ix.dims + 63) / 64 * 64;  // BF16 row length (64-element K slabs)
+    const uint64_t kb = (ix.dims + 63) / 64 * 64;  // FP16 / BF16 row length (64-element K slabs)
+    const uint64_t kb16 = kb;
     BuildScratch tmp;
     cudaError_t e = cudaSuccess;
     auto oom = [&](const char* what) { return cuda_error(e, what); };
@@ -1221,6 +1250,17 @@ int ivf_build(CudaIndex& ix) {
         const uint32_t gb = static_cast<uint32_t>(std::min<uint64_t>((rows * 32 + 255) / 256, ix.sm_count * 16ull));
         gather_rows_kernel<<<gb, 256, 0, s>>>(ix.d_base, static_cast<uint32_t>(ds), perm, rows, v.d_reordered);
         count_launch();
+        // BF16 copy for the tensor-core list scan, and the bound of its residuals
+        v.kb16 = kb16;
+        if ((e = cudaMalloc(&v.d_reordered16, ix.rows_alloc * kb16 * sizeof(__nv_bfloat16))) != cudaSuccess ||
+            (e = cudaMalloc(&v.d_res16, rows * sizeof(float))) != cudaSuccess)
+            return oom("IVF BF16 rows");
+        cudaMemsetAsync(v.d_reordered16 + rows * kb16, 0, (ix.rows_alloc - rows) * kb16 * sizeof(__nv_bfloat16), s);
+        bf16_rows_kernel<<<gb, 256, 0, s>>>(v.d_reordered, static_cast<uint32_t>(ds), rows, v.d_reordered16,
+                                            static_cast<uint32_t>(kb16), v.d_res16);
+        count_launch();
+        cudaMemsetAsync(cmax, 0, sizeof(unsigned int), s);
+        if ((e = launch_max_reduce(v.d_res16, rows, cmax, s)) != cudaSuccess) return cuda_error(e, "IVF residual bound");
     }
     cudaEventRecord(t_lay.b, s);
     cudaEventRecord(t_all.b, s);
@@ -1232,7 +1272,9 @@ int ivf_build(CudaIndex& ix) {
     cudaMemcpyAsync(h_amb.data(), d_amb_hist, 2 * iters * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&h_st, kst, sizeof(h_st), cudaMemcpyDeviceToHost, s);
     uint32_t h_status = 0;
+    unsigned int h_eps = 0;
     cudaMemcpyAsync(&h_status, ix.d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&h_eps, cmax, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "IVF build");
     if (h_status == kStatusTimeout)
         return set_error(NNDEX_ERR_TIMEOUT, "cuda execution error: a bounded device wait timed out (IVF build)");
@@ -1242,8 +1284,12 @@ int ivf_build(CudaIndex& ix) {
     v.h_init_rows.assign(h_chosen.begin(), h_chosen.end());
     for (uint64_t c = 0; c < nlist; ++c) v.max_list = std::max<uint64_t>(v.max_list, h_off[c + 1] - h_off[c]);
     if (!encode_tmap_2d(&v.tmap_reordered, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, v.d_reordered, ds, ix.rows_alloc,
-                        ds * sizeof(float), 32, 128, CU_TENSOR_MAP_SWIZZLE_128B))
+                        ds * sizeof(float), 32, 128, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !encode_tmap_2d(&v.tmap_reordered16, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, v.d_reordered16, kb16, ix.rows_alloc,
+                        kb16 * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B))
         return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (IVF rows)");
+    std::memcpy(&v.eps16, &h_eps, sizeof(float));
+    if (ix.kb16 == 0) ix.kb16 = kb16;  // BF16 query copies for the tensor-core list scan
     float ms = 0.0f;
     v.stats.nlist = nlist;
     v.stats.iters = iters;

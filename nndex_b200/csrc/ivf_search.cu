@@ -101,14 +101,16 @@ __global__ void __launch_bounds__(256)
 // ------------------------------------------------------------------------------------------
 // 2. Plan: one block.
 //    counters[0] work-item counter (the scan's), [1] items, [2] slots; summed over the sub-batches of
-//    a search: [3] Σ rows probed per query, [4] rows streamed by the scan, [5] rows of probed lists.
+//    a search: [3] Σ rows probed per query, [4] rows streamed by the scan, [5] rows of probed lists;
+//    [6] gathered query blocks (qblock_off given: the tensor-core scan's groups of qb queries).
+//    Groups of a list are consecutive blocks from qblock_off[l].
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024)
     ivf_plan_kernel(const uint32_t* __restrict__ probes, uint32_t nq, uint32_t np, uint32_t nlist,
                     const uint32_t* __restrict__ offsets, uint32_t qb, uint32_t* __restrict__ list_cnt,
                     uint32_t* __restrict__ list_fill, uint32_t* __restrict__ list_qoff, uint32_t* __restrict__ item_off,
                     uint32_t* __restrict__ list_q, uint32_t* __restrict__ list_slot, uint32_t* __restrict__ q_slot_off,
-                    unsigned long long* __restrict__ counters) {
+                    unsigned long long* __restrict__ counters, uint32_t* __restrict__ qblock_off) {
     __shared__ uint32_t part[1024];
     __shared__ unsigned long long probed;
     if (threadIdx.x == 0) probed = 0;
@@ -136,6 +138,7 @@ __global__ void __launch_bounds__(1024)
         const uint32_t groups = (c + qb - 1) / qb;
         item_off[l] = chunks(l) * groups;
         list_qoff[l] = c;
+        if (qblock_off) qblock_off[l] = groups;
         const uint32_t len = offsets[l + 1] - offsets[l];
         my_stream += static_cast<unsigned long long>(len) * groups;
         my_union += c ? len : 0u;
@@ -146,6 +149,7 @@ __global__ void __launch_bounds__(1024)
     block_exclusive_scan(list_qoff, nlist, part);
     block_exclusive_scan(item_off, nlist, part);
     block_exclusive_scan(q_slot_off, nq, part);
+    if (qblock_off) block_exclusive_scan(qblock_off, nlist, part);
     for (uint32_t q = threadIdx.x; q < nq; q += blockDim.x) {
         uint32_t rel = q_slot_off[q];
         for (uint32_t j = 0; j < np; ++j) {
@@ -161,6 +165,7 @@ __global__ void __launch_bounds__(1024)
         counters[1] = item_off[nlist];
         counters[2] = q_slot_off[nq];
         counters[3] += probed;  // zeroed once per search: Σ over sub-batches
+        if (qblock_off) counters[6] = qblock_off[nlist];
     }
 }
 
@@ -373,6 +378,54 @@ __global__ void __launch_bounds__(512)
 }
 
 // ------------------------------------------------------------------------------------------
+// Tensor-core list scan helpers.
+// ------------------------------------------------------------------------------------------
+// One block per list: its probing queries in groups of 128 (one gathered block each, consecutive from
+// qblock_off[l]): their BF16 rows (zero past the group's end), query ids (0xFFFFFFFF: none) and the
+// query's output slot for the list's chunk 0.
+__global__ void __launch_bounds__(256)
+    ivf_gather_tc_kernel(const __nv_bfloat16* __restrict__ q16, uint32_t kb, const uint32_t* __restrict__ list_cnt,
+                         const uint32_t* __restrict__ list_qoff, const uint32_t* __restrict__ list_q,
+                         const uint32_t* __restrict__ list_slot, const uint32_t* __restrict__ qblock_off,
+                         __nv_bfloat16* __restrict__ g16, uint32_t* __restrict__ lane_qid,
+                         uint32_t* __restrict__ lane_slot) {
+    const uint32_t l = blockIdx.x;
+    const uint32_t cnt = list_cnt[l];
+    if (cnt == 0) return;
+    const uint32_t n = (cnt + 127) / 128 * 128;
+    const uint64_t row0 = static_cast<uint64_t>(qblock_off[l]) * 128;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
+    const uint32_t chunks = kb / 8;  // 16-byte chunks of a row
+    for (uint32_t j = warp; j < n; j += nwarps) {
+        const uint64_t row = row0 + j;
+        uint4* dst = reinterpret_cast<uint4*>(g16 + row * kb);
+        if (j < cnt) {
+            const uint32_t src = list_qoff[l] + j;
+            const uint32_t q = list_q[src];
+            const uint4* from = reinterpret_cast<const uint4*>(q16 + static_cast<uint64_t>(q) * kb);
+            for (uint32_t c = lane; c < chunks; c += 32) dst[c] = from[c];
+            if (lane == 0) {
+                lane_qid[row] = q;
+                lane_slot[row] = list_slot[src];
+            }
+        } else {
+            for (uint32_t c = lane; c < chunks; c += 32) dst[c] = make_uint4(0u, 0u, 0u, 0u);
+            if (lane == 0) {
+                lane_qid[row] = 0xFFFFFFFFu;
+                lane_slot[row] = 0;
+            }
+        }
+    }
+}
+
+// Pass-2 thresholds by query: the exact k-th score of pass 1, or +inf for a certified query.
+__global__ void ivf_pass2_thr_kernel(const uint32_t* __restrict__ cert, const float* __restrict__ kth, uint32_t n,
+                                     float* __restrict__ thr) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) thr[q] = cert[q] ? INFINITY : kth[q];
+}
+
+// ------------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------------
 namespace {
@@ -412,10 +465,22 @@ cudaError_t launch_scan(const CUtensorMap& tmap, const IvfScanArgs& a, uint32_t 
     return cudaGetLastError();
 }
 
+template <class T>
+int grow_pinned(T*& p, size_t& cap, size_t n, const char* what) {
+    if (n <= cap && p) return NNDEX_OK;
+    cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return cuda_error(e, what);
+    cap = n;
+    return NNDEX_OK;
+}
+
 }  // namespace
 
-int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
-               cudaStream_t s) {
+int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim,
+               uint32_t* o_cnt, cudaStream_t s) {
     const IvfIndex& v = *ix.ivf;
     IvfScratch& w = ix.ivf_scratch;
     const uint32_t nlist = static_cast<uint32_t>(v.nlist);
@@ -447,7 +512,7 @@ int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o
     if ((st = grow(w.d_list_q, w.cap_list_q, static_cast<size_t>(sub) * np, "IVF plan buffer"))) return st;
     if ((st = grow(w.d_list_slot, w.cap_list_slot, static_cast<size_t>(sub) * np, "IVF plan buffer"))) return st;
     if ((st = grow(w.d_q_slot_off, w.cap_q_slot_off, sub + 1, "IVF plan buffer"))) return st;
-    if ((st = grow(w.d_counters, w.cap_counters, 6, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_counters, w.cap_counters, 8, "IVF plan buffer"))) return st;
     if ((st = grow(w.d_ws, w.cap_ws, static_cast<size_t>(sub) * np * max_chunks * k, "IVF slot workspace"))) return st;
     IvfScanArgs a;
     a.dq = dq;
@@ -468,17 +533,17 @@ int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o
     cudaFuncSetAttribute(ivf_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(probe_smem));
     uint32_t p2 = 1;
     while (p2 < k) p2 <<= 1;
-    cudaMemsetAsync(w.d_counters, 0, 6 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(w.d_counters, 0, 8 * sizeof(unsigned long long), s);
     for (uint32_t q0 = 0; q0 < nq; q0 += sub) {
         const uint32_t n = std::min(sub, nq - q0);
-        const float* qn = ix.d_qn + static_cast<uint64_t>(q0) * ix.ds;
+        const float* qn = queries + static_cast<uint64_t>(q0) * ix.ds;
         cudaMemsetAsync(w.d_list_cnt, 0, nlist * sizeof(uint32_t), s);
         cudaMemsetAsync(w.d_list_fill, 0, nlist * sizeof(uint32_t), s);
         ivf_probe_kernel<<<n, 256, probe_smem, s>>>(qn, dq, static_cast<uint32_t>(ix.dp), v.d_cent_t, v.nlist_pad, nlist,
                                                     np, w.d_probes);
         ivf_plan_kernel<<<1, 1024, 0, s>>>(w.d_probes, n, np, nlist, v.d_offsets, qb, w.d_list_cnt, w.d_list_fill,
                                            w.d_list_qoff, w.d_item_off, w.d_list_q, w.d_list_slot, w.d_q_slot_off,
-                                           w.d_counters);
+                                           w.d_counters, nullptr);
         count_launch(2);
         a.queries = qn;
         cudaError_t e;
@@ -498,11 +563,228 @@ int ivf_search(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "IVF merge launch");
         ix.stats.kernel_launches += 4;
     }
-    if (!w.h_probed && cudaMallocHost(&w.h_probed, 3 * sizeof(unsigned long long)) != cudaSuccess)
+    if (!w.h_probed && cudaMallocHost(&w.h_probed, 8 * sizeof(unsigned long long)) != cudaSuccess)
         return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: pinned allocation failed");
     cudaMemcpyAsync(w.h_probed, w.d_counters + 3, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
     ix.stats.path = 4;
     ix.stats.nprobe = np;
+    return NNDEX_OK;
+}
+
+// Tensor-core list scan (path 5). Pass 1: the plan groups the queries probing each list by 128;
+// each work item (list chunk × query group) runs the tensor-core scan in item mode over the list's
+// reordered BF16 rows and leaves the k′ best upper bounds per (query, chunk) in its slot; the merge
+// keeps the k′ best per query over its slots and K4 re-scores them exactly in FP32: the exact k-th
+// score T, and a certificate when T beats the k′-th bound (no other probed row can reach the top k).
+// Pass 2, for the other queries: every probed row whose bound reaches T, re-scored exactly; a query
+// whose collection overflows runs on the FP32 list scan. The result equals the FP32 list scan's
+// (the same probed rows, the same exact scores, bit for bit).
+int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                  cudaStream_t s) {
+    const IvfIndex& v = *ix.ivf;
+    IvfScratch& w = ix.ivf_scratch;
+    const uint32_t nlist = static_cast<uint32_t>(v.nlist);
+    uint64_t np64 = w.nprobe ? w.nprobe : ivf_choose_nprobe(v.nlist, k, ix.rows);
+    np64 = std::max<uint64_t>(1, std::min<uint64_t>(np64, v.nlist));
+    const uint32_t np = static_cast<uint32_t>(np64);
+    const CudaIndex::TcPlan plan = ix.plan_tc(k, false), plan2 = ix.plan_tc(0, false);
+    if (plan.kp < k || !plan.stages || !plan2.stages) return ivf_search(ix, ix.d_qn, nq, k, o_idx, o_sim, o_cnt, s);
+    const uint32_t kp = plan.kp;
+    if (static_cast<size_t>(ix.ds) * 4 + static_cast<size_t>(nlist) * 8 > ix.smem_optin)
+        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF probe shared memory above the limit");
+    const uint64_t max_chunks = (v.max_list + kChunkRows - 1) / kChunkRows;
+    const uint64_t pairs = static_cast<uint64_t>(nq) * np;
+    const uint64_t max_blocks = nlist + (pairs + 127) / 128;
+    int st;
+    if ((st = grow(w.d_probes, w.cap_probes, pairs, "IVF probe buffer"))) return st;
+    if ((st = grow(w.d_list_cnt, w.cap_list_cnt, nlist, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_list_fill, w.cap_list_fill, nlist, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_list_qoff, w.cap_list_qoff, nlist + 1, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_item_off, w.cap_item_off, nlist + 1, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_qblock_off, w.cap_qblock_off, nlist + 1, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_list_q, w.cap_list_q, pairs, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_list_slot, w.cap_list_slot, pairs, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_q_slot_off, w.cap_q_slot_off, nq + 1, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_counters, w.cap_counters, 8, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_ws, w.cap_ws, pairs * max_chunks * kp, "IVF slot workspace"))) return st;
+    if ((st = grow(w.d_g16, w.cap_g16, max_blocks * 128 * v.kb16, "IVF query blocks"))) return st;
+    if ((st = grow(w.d_lane_qid, w.cap_lane_qid, max_blocks * 128, "IVF query blocks"))) return st;
+    if ((st = grow(w.d_lane_slot, w.cap_lane_slot, max_blocks * 128, "IVF query blocks"))) return st;
+    if ((st = grow(ix.d_thr, ix.cap_thr, nq, "tc workspace"))) return st;
+    if ((st = grow(ix.d_cand_idx, ix.cap_cand_idx, static_cast<size_t>(nq) * kp, "tc workspace"))) return st;
+    if ((st = grow(ix.d_cand_sim, ix.cap_cand_sim, static_cast<size_t>(nq) * kp, "tc workspace"))) return st;
+    if ((st = grow(ix.d_cand_cnt, ix.cap_cand_cnt, nq, "tc workspace"))) return st;
+    if ((st = grow(ix.d_cert, ix.cap_cert, nq, "tc workspace"))) return st;
+    if ((st = grow(ix.d_kth, ix.cap_kth, nq, "tc workspace"))) return st;
+    if (!w.h_probed && cudaMallocHost(&w.h_probed, 8 * sizeof(unsigned long long)) != cudaSuccess)
+        return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: pinned allocation failed");
+
+    // ---- probe + plan (groups of 128 queries) + gathered query blocks ----
+    const size_t probe_smem = static_cast<size_t>(ix.ds) * 4 + static_cast<size_t>(nlist) * 8;
+    cudaFuncSetAttribute(ivf_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(probe_smem));
+    cudaMemsetAsync(w.d_counters, 0, 8 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(w.d_list_cnt, 0, nlist * sizeof(uint32_t), s);
+    cudaMemsetAsync(w.d_list_fill, 0, nlist * sizeof(uint32_t), s);
+    ivf_probe_kernel<<<nq, 256, probe_smem, s>>>(ix.d_qn, static_cast<uint32_t>(ix.ds), static_cast<uint32_t>(ix.dp),
+                                                 v.d_cent_t, v.nlist_pad, nlist, np, w.d_probes);
+    ivf_plan_kernel<<<1, 1024, 0, s>>>(w.d_probes, nq, np, nlist, v.d_offsets, 128, w.d_list_cnt, w.d_list_fill,
+                                       w.d_list_qoff, w.d_item_off, w.d_list_q, w.d_list_slot, w.d_q_slot_off,
+                                       w.d_counters, w.d_qblock_off);
+    ivf_gather_tc_kernel<<<nlist, 256, 0, s>>>(ix.d_q_bf16, static_cast<uint32_t>(v.kb16), w.d_list_cnt, w.d_list_qoff,
+                                               w.d_list_q, w.d_list_slot, w.d_qblock_off, w.d_g16, w.d_lane_qid,
+                                               w.d_lane_slot);
+    count_launch(3);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_error(e, "IVF plan launch");
+    cudaMemcpyAsync(w.h_probed, w.d_counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "IVF plan");
+    const uint64_t items = w.h_probed[1], blocks = w.h_probed[6];
+    const unsigned long long rows_probed = w.h_probed[3], streamed = w.h_probed[4], uni = w.h_probed[5];
+    if (items == 0 || blocks > max_blocks)
+        return set_error(NNDEX_ERR_CUDA, "cuda execution error: IVF plan produced %llu items, %llu query blocks",
+                         (unsigned long long)items, (unsigned long long)blocks);
+
+    // ---- pass 1 ----
+    CUtensorMap tmap_q;
+    if ((st = ix.encode_query_tmap(false, w.d_g16, static_cast<uint32_t>(blocks * 128), &tmap_q))) return st;
+    cudaMemsetAsync(ix.d_thr, 0, nq * sizeof(unsigned long long), s);
+    TcArgs a;
+    a.tmap_q = &tmap_q;
+    a.tmap_b = &v.tmap_reordered16;
+    a.nranges = 1;
+    a.stages = plan.stages;
+    a.stream_a = plan.stream_a;
+    a.items = static_cast<uint32_t>(items);
+    ix.fill_tc_params(false, nq, 0, a.p);
+    a.p.row_resid = v.d_res16;
+    a.p.eps_rows = v.eps16;
+    a.p.q_resid = ix.d_q_resid;
+    a.p.kprime = kp;
+    a.p.thr_global = ix.d_thr;
+    a.p.ws_keys = w.d_ws;
+    // Autotuned like the exact path's pass 1: when pass 1 rarely certifies, it only has to give each
+    // query its threshold T, and every 4th tile of its lists gives a valid one.
+    const uint32_t stride = w.tc_stride;
+    a.p.tile_stride = stride;
+    a.p.it_item_off = w.d_item_off;
+    a.p.it_list_cnt = w.d_list_cnt;
+    a.p.it_offsets = v.d_offsets;
+    a.p.it_qblock_off = w.d_qblock_off;
+    a.p.it_lane_qid = w.d_lane_qid;
+    a.p.it_lane_slot = w.d_lane_slot;
+    a.p.row_map = v.d_row_map;
+    a.p.it_nlist = nlist;
+    a.p.it_chunk_rows = kChunkRows;
+    cudaEvent_t ev_a = nullptr;
+    ix.scan_event_begin(s, ev_a);
+    e = launch_scan_tc(a, false, 0, s);
+    ix.scan_event_end(s, ev_a);
+    if (e != cudaSuccess) return cuda_error(e, "IVF tensor-core scan launch");
+    uint32_t p2 = 1;
+    while (p2 < kp) p2 <<= 1;
+    ivf_merge_kernel<<<nq, 512, p2 * sizeof(uint64_t), s>>>(w.d_ws, w.d_q_slot_off, kp, ix.d_cand_idx, ix.d_cand_sim,
+                                                            ix.d_cand_cnt);
+    count_launch();
+    RerankArgs r;
+    r.base = ix.d_base;
+    r.ds = static_cast<uint32_t>(ix.ds);
+    r.queries = ix.d_qn;
+    r.cand_idx = ix.d_cand_idx;
+    r.cand_sim = ix.d_cand_sim;
+    r.cand_cnt = ix.d_cand_cnt;
+    r.nq = nq;
+    r.kp = kp;
+    r.k = k;
+    r.idx_out = o_idx;
+    r.sim_out = o_sim;
+    r.cnt_out = o_cnt;
+    r.cert_out = ix.d_cert;
+    r.kth_out = ix.d_kth;
+    r.certify = stride == 1;
+    if ((e = launch_rerank(r, s)) != cudaSuccess) return cuda_error(e, "rerank launch");
+    if ((st = grow_pinned(ix.h_cert, ix.cap_hcert, nq, "pinned buffer"))) return st;
+    cudaMemcpyAsync(ix.h_cert, ix.d_cert, nq * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    ix.h_flags[1] = 0;
+    cudaMemcpyAsync(&ix.h_flags[1], ix.d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "IVF search");
+    if (ix.h_flags[1] != 0) return ix.check_device_words();
+    ix.stats.kernel_launches += 6;
+    ix.stats.path = 5;
+    ix.stats.nprobe = np;
+    ix.stats.rerank_width = kp;
+    ix.stats.rows_scanned = rows_probed;
+    ix.stats.ivf_rows_streamed = streamed;
+    ix.stats.ivf_rows_union = uni;
+    if ((st = grow_pinned(ix.h_ids, ix.cap_hids, nq, "pinned buffer"))) return st;
+    uint32_t m = 0;
+    for (uint32_t i = 0; i < nq; ++i)
+        if (!ix.h_cert[i]) ix.h_ids[m++] = i;
+    ix.stats.certified = m == 0 ? 1u : 0u;
+    ix.stats.second_pass_queries = m;
+    ix.stats.pass1_tile_stride = stride;
+    if (stride == 1 && m * 2 > nq) w.tc_stride = 4;
+    if (m == 0) return NNDEX_OK;
+
+    // ---- pass 2: every probed row whose bound reaches T, for the uncertified queries ----
+    const uint32_t cap2 = kSecondPassCap;
+    if ((st = grow(ix.d_ids, ix.cap_ids, m, "pass-2 buffer"))) return st;
+    if ((st = grow(ix.d_q2_thr, ix.cap_q2_thr, nq, "pass-2 buffer"))) return st;
+    if ((st = grow(ix.d_rows2, ix.cap_rows2, static_cast<size_t>(nq) * cap2, "pass-2 buffer"))) return st;
+    if ((st = grow(ix.d_cnt2, ix.cap_cnt2, nq, "pass-2 buffer"))) return st;
+    if ((st = grow(ix.d_ok2, ix.cap_ok2, m, "pass-2 buffer"))) return st;
+    cudaMemcpyAsync(ix.d_ids, ix.h_ids, m * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    ivf_pass2_thr_kernel<<<(nq + 255) / 256, 256, 0, s>>>(ix.d_cert, ix.d_kth, nq, ix.d_q2_thr);
+    count_launch();
+    cudaMemsetAsync(ix.d_cnt2, 0, nq * sizeof(uint32_t), s);
+    a.stages = plan2.stages;
+    a.stream_a = plan2.stream_a;
+    a.p.tile_stride = 1;
+    a.p.kprime = 0;
+    a.p.q_thr = ix.d_q2_thr;
+    a.p.cand_rows = ix.d_rows2;
+    a.p.cand_cnt = ix.d_cnt2;
+    a.p.cap2 = cap2;
+    ix.scan_event_begin(s, ev_a);
+    e = launch_scan_tc(a, false, 1, s);
+    ix.scan_event_end(s, ev_a);
+    if (e != cudaSuccess) return cuda_error(e, "IVF tensor-core scan launch (pass 2)");
+    e = launch_rerank_collected(ix.d_base, static_cast<uint32_t>(ix.ds), ix.d_qn, ix.d_ids, m, ix.d_rows2, ix.d_cnt2,
+                                cap2, k, o_idx, o_sim, o_cnt, ix.d_ok2, s, true);
+    if (e != cudaSuccess) return cuda_error(e, "rerank launch (pass 2)");
+    ix.stats.kernel_launches += 3;
+    if ((st = grow_pinned(ix.h_ok2, ix.cap_hok2, m, "pinned buffer"))) return st;
+    cudaMemcpyAsync(ix.h_ok2, ix.d_ok2, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    ix.h_flags[1] = 0;
+    cudaMemcpyAsync(&ix.h_flags[1], ix.d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "IVF search");
+    if (ix.h_flags[1] != 0) return ix.check_device_words();
+    std::vector<uint32_t> failed;
+    for (uint32_t i = 0; i < m; ++i)
+        if (!ix.h_ok2[i]) failed.push_back(ix.h_ids[i]);
+    ix.stats.fp32_fallback_queries = static_cast<uint32_t>(failed.size());
+    if (failed.empty()) return NNDEX_OK;
+
+    // ---- FP32 list scan for the queries whose collection overflowed ----
+    const uint32_t mf = static_cast<uint32_t>(failed.size());
+    if ((st = grow(ix.d_qsub, ix.cap_qsub, static_cast<size_t>(mf) * ix.ds, "fallback buffer"))) return st;
+    for (uint32_t i = 0; i < mf; ++i)
+        cudaMemcpyAsync(ix.d_qsub + static_cast<uint64_t>(i) * ix.ds, ix.d_qn + static_cast<uint64_t>(failed[i]) * ix.ds,
+                        ix.ds * sizeof(float), cudaMemcpyDeviceToDevice, s);
+    if ((st = grow(ix.d_fb_idx, ix.cap_fb_idx, static_cast<size_t>(mf) * k, "fallback buffer"))) return st;
+    if ((st = grow(ix.d_fb_sim, ix.cap_fb_sim, static_cast<size_t>(mf) * k, "fallback buffer"))) return st;
+    if ((st = grow(ix.d_fb_cnt, ix.cap_fb_cnt, mf, "fallback buffer"))) return st;
+    const nndex_cuda_search_stats keep = ix.stats;
+    if ((st = ivf_search(ix, ix.d_qsub, mf, k, ix.d_fb_idx, ix.d_fb_sim, ix.d_fb_cnt, s))) return st;
+    ix.stats = keep;
+    for (uint32_t i = 0; i < mf; ++i) {
+        const uint64_t q = failed[i];
+        cudaMemcpyAsync(o_idx + q * k, ix.d_fb_idx + static_cast<uint64_t>(i) * k, k * sizeof(uint64_t),
+                        cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(o_sim + q * k, ix.d_fb_sim + static_cast<uint64_t>(i) * k, k * sizeof(float),
+                        cudaMemcpyDeviceToDevice, s);
+        if (o_cnt) cudaMemcpyAsync(o_cnt + q, ix.d_fb_cnt + i, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+    }
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "IVF search");
     return NNDEX_OK;
 }
 

@@ -151,7 +151,10 @@ NNDEX_DEVICE_INLINE void epi_survivor(const TcParams& p, EpiState& st, uint64_t*
 // kStreamA: the query block's K slabs are not resident; each ring stage carries the matching query
 // slab beside the base slab (re-read from L2 per tile). It frees nchunks × 16 KB of shared memory
 // for the pass-1 heaps, which large D × large k needs (D = 512, k = 100: 128 KB of queries).
-template <bool kFp8, int kST, int kMode, bool kStreamA>
+// kItems: the IVF list scan (TcParams' item fields): the CTA's queries are a gathered block of the
+// queries probing one list and its rows one chunk of that list's reordered rows; keys and collected
+// rows carry original row indices, and pass-1 heaps go to the (query, chunk) output slots.
+template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems>
 __global__ void __launch_bounds__(kThreads, 1)
     scan_tc_kernel(const __grid_constant__ CUtensorMap tmap_q, const __grid_constant__ CUtensorMap tmap_b,
                    const TcParams p) {
@@ -172,10 +175,26 @@ __global__ void __launch_bounds__(kThreads, 1)
     volatile uint32_t* abort_flag = tmem_slot + 1;
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    const uint32_t q0 = blockIdx.x * kM;
+    uint32_t q0 = blockIdx.x * kM;
     const uint32_t range = blockIdx.y, nranges = gridDim.y;
-    const uint64_t row_begin = static_cast<uint64_t>(range) * p.range_rows;
-    const uint64_t row_end = (row_begin + p.range_rows) < p.rows ? (row_begin + p.range_rows) : p.rows;
+    uint64_t row_begin = static_cast<uint64_t>(range) * p.range_rows;
+    uint64_t row_end = (row_begin + p.range_rows) < p.rows ? (row_begin + p.range_rows) : p.rows;
+    uint32_t chunk = 0;  // item mode: the chunk of the list (its output slot offset)
+    if (kItems) {
+        const uint32_t wi = blockIdx.x;
+        uint32_t lo = 0, hi = p.it_nlist;  // the last list whose first item is ≤ wi
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (p.it_item_off[mid] <= wi) lo = mid; else hi = mid;
+        }
+        const uint32_t groups = (p.it_list_cnt[lo] + kM - 1) / kM;
+        const uint32_t local = wi - p.it_item_off[lo];
+        chunk = local / groups;
+        q0 = (p.it_qblock_off[lo] + local % groups) * kM;
+        row_begin = p.it_offsets[lo] + static_cast<uint64_t>(chunk) * p.it_chunk_rows;
+        const uint64_t le = p.it_offsets[lo + 1];
+        row_end = (row_begin + p.it_chunk_rows) < le ? (row_begin + p.it_chunk_rows) : le;
+    }
     const uint64_t tile_step = static_cast<uint64_t>(kN) * p.tile_stride;
     const uint32_t ntiles =
         row_end > row_begin ? static_cast<uint32_t>((row_end - row_begin + tile_step - 1) / tile_step) : 0;
@@ -293,8 +312,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ---------------- epilogue: 4 warps, one query per thread ----------------
         const uint32_t quarter = warp & 3u;
         const uint32_t lrow = quarter * 32 + lane;
-        const uint32_t q = q0 + lrow;
-        const bool valid_q = q < p.nq;
+        const uint32_t q = kItems ? p.it_lane_qid[q0 + lrow] : q0 + lrow;
+        const bool valid_q = kItems ? q != 0xFFFFFFFFu : q < p.nq;
         const uint32_t et = threadIdx.x - 64;  // 0..127
         const float qs = (kFp8 && valid_q) ? p.q_scale[q] : 1.0f;
         const float rq = valid_q ? p.q_resid[q] : 0.0f;
@@ -356,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     float s = pick(v, j);
                     if (kFp8) s = (s * sc[c * 32 + j]) * qs;
                     const float u = fmaf(p.row_resid[row], b_mul, s + b_add);
-                    epi_survivor<kMode>(p, st, heap, lrow, q, u, row, slack);
+                    epi_survivor<kMode>(p, st, heap, lrow, q, u, kItems ? p.row_map[row] : row, slack);
                 }
             };
 #pragma unroll
@@ -377,7 +396,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (lane == 0) mbar_arrive(&tempty[buf]);
         }
         if (kMode == 0 && valid_q) {
-            uint64_t* dst = p.ws_keys + (static_cast<size_t>(q) * nranges + range) * p.kprime;
+            uint64_t* dst = kItems ? p.ws_keys + static_cast<size_t>(p.it_lane_slot[q0 + lrow] + chunk) * p.kprime
+                                   : p.ws_keys + (static_cast<size_t>(q) * nranges + range) * p.kprime;
             for (uint32_t i = 0; i < p.kprime; ++i) dst[i] = i < st.n ? heap[i * kM + lrow] : 0ull;
             if (st.n == p.kprime) atomicMax(&p.thr_global[q], static_cast<unsigned long long>(heap[lrow]));
         }
@@ -459,7 +479,9 @@ __global__ void __launch_bounds__(256)
         if (certify && n >= kp && kk > 0)
             ok = key_score(keys[kk - 1]) > cand_bound[static_cast<size_t>(q) * kp + kp - 1] ? 1u : 0u;
         cert_out[q] = ok;
-        kth_out[q] = kk > 0 ? key_score(keys[kk - 1]) : -INFINITY;
+        // T: the exact k-th score among the candidates, a lower bound of the true k-th; with fewer
+        // than k candidates (a sampled pass 1 over few rows) there is no bound.
+        kth_out[q] = kk == k ? key_score(keys[kk - 1]) : -INFINITY;
     }
 }
 
@@ -490,12 +512,13 @@ __global__ void __launch_bounds__(256)
                             const uint32_t* __restrict__ ids, const uint32_t* __restrict__ rows2,
                             const uint32_t* __restrict__ cnt2, uint32_t cap2, uint32_t k, uint64_t* __restrict__ idx_out,
                             float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out,
-                            uint32_t* __restrict__ ok_out) {
+                            uint32_t* __restrict__ ok_out, int by_query) {
     extern __shared__ uint64_t keys[];
     __shared__ BlockSelectScratch sel;
     const uint32_t i = blockIdx.x;
     const uint32_t q = ids[i];
-    const uint32_t total = cnt2[i];
+    const uint32_t qrow = by_query ? q : i;  // collected rows indexed by query, or by position in ids
+    const uint32_t total = cnt2[qrow];
     if (total > cap2) {  // the collected set overflowed: this query goes to the FP32 scan
         if (threadIdx.x == 0) ok_out[i] = 0;
         return;
@@ -507,7 +530,7 @@ __global__ void __launch_bounds__(256)
     for (uint32_t j0 = 0; j0 < n; j0 += nslots) {
         const uint32_t j = j0 + slot;
         const bool live = j < n;
-        const uint64_t row = live ? rows2[static_cast<size_t>(i) * cap2 + j] : 0;
+        const uint64_t row = live ? rows2[static_cast<size_t>(qrow) * cap2 + j] : 0;
         const float acc = dot_scan_order(base + row * ds, qv, nbox, ch, live);
         if (ch == 0 && live) keys[j] = make_key(acc, static_cast<uint32_t>(row));
     }
@@ -545,14 +568,14 @@ __global__ void __launch_bounds__(256)
 // ------------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------------
-template <bool kFp8, int kST, int kMode, bool kStreamA>
+template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems = false>
 static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
-    auto kern = scan_tc_kernel<kFp8, kST, kMode, kStreamA>;
+    auto kern = scan_tc_kernel<kFp8, kST, kMode, kStreamA, kItems>;
     const uint32_t kp = kMode == 0 ? a.p.kprime : 0;
     const size_t smem = tc_smem_bytes(a.p.nchunks, kp, kST, kFp8, kStreamA);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    dim3 grid((a.p.nq + kM - 1) / kM, a.nranges);
+    dim3 grid = kItems ? dim3(a.items, 1) : dim3((a.p.nq + kM - 1) / kM, a.nranges);
     TcParams p = a.p;
     p.kprime = kp;
     kern<<<grid, kThreads, smem, stream>>>(*a.tmap_q, *a.tmap_b, p);
@@ -570,7 +593,23 @@ static cudaError_t launch_tc_stages(const TcArgs& a, cudaStream_t stream) {
     }
 }
 
+// IVF item mode (BF16 only).
+template <int kMode, bool kStreamA>
+static cudaError_t launch_tc_items(const TcArgs& a, cudaStream_t stream) {
+    switch (a.stages) {
+        case 4: return launch_tc_impl<false, 4, kMode, kStreamA, true>(a, stream);
+        case 3: return launch_tc_impl<false, 3, kMode, kStreamA, true>(a, stream);
+        case 2: return launch_tc_impl<false, 2, kMode, kStreamA, true>(a, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t stream) {
+    if (a.items) {
+        if (fp8 || a.items > 0x7FFFFFFFu) return cudaErrorInvalidValue;
+        if (mode == 0) return a.stream_a ? launch_tc_items<0, true>(a, stream) : launch_tc_items<0, false>(a, stream);
+        return a.stream_a ? launch_tc_items<1, true>(a, stream) : launch_tc_items<1, false>(a, stream);
+    }
     if (mode == 0) {
         if (a.stream_a) return fp8 ? launch_tc_stages<true, 0, true>(a, stream) : launch_tc_stages<false, 0, true>(a, stream);
         return fp8 ? launch_tc_stages<true, 0, false>(a, stream) : launch_tc_stages<false, 0, false>(a, stream);
@@ -602,7 +641,7 @@ cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q
 cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float* queries, const uint32_t* ids,
                                     uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
                                     uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
-                                    cudaStream_t stream) {
+                                    cudaStream_t stream, bool by_query) {
     if (m == 0) return cudaSuccess;
     uint32_t p2 = 1;
     while (p2 < cap2) p2 <<= 1;
@@ -610,7 +649,8 @@ cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float*
     auto kern = rerank_collected_kernel;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    kern<<<m, 256, smem, stream>>>(base, ds, queries, ids, rows2, cnt2, cap2, k, idx_out, sim_out, cnt_out, ok_out);
+    kern<<<m, 256, smem, stream>>>(base, ds, queries, ids, rows2, cnt2, cap2, k, idx_out, sim_out, cnt_out, ok_out,
+                                   by_query ? 1 : 0);
     count_launch();
     return cudaGetLastError();
 }

@@ -79,7 +79,13 @@ struct Server {
         uint64_t per = (ix->dims + ix->ds) * 4 + kcap * 12;
         per += 160 * kcap * 8;                      // FP32 scan: one k-key slot per CTA and query
         per += 64 * std::max<uint64_t>(32, 2 * kcap) * 8;  // tensor-core pass 1 (k′ keys per row range)
-        if (approx) per += (static_cast<uint64_t>(nprobe) * max_chunks * kcap + 4ull * nprobe) * 8;
+        if (approx) {
+            // FP32 list scan: k keys per (probed list, chunk); tensor-core list scan: k′ keys per
+            // (probed list, chunk), the gathered BF16 query blocks, and the pass-2 row collection.
+            const uint64_t kp = std::max<uint64_t>(32, 2 * kcap);
+            per += (static_cast<uint64_t>(nprobe) * max_chunks * std::max(kp, kcap) + 4ull * nprobe) * 8;
+            per += ix->ds * 2 + 8192ull * 4;
+        }
         return nq * per;
     }
     void worker(uint32_t slot);

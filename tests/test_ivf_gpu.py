@@ -210,3 +210,40 @@ def test_ivf_probed_fewer_rows_than_k():
         n = int(rc[i])
         assert n < k and gi.shape[0] == n
         check_against_probed(ref, storage, qn[i], gi, gs, n, k, 1, f"small-list q{i}")
+
+
+TC_CASES = [
+    # name, rows, dims, nlist, nq, k, nprobe
+    ("mixture", 20_000, 64, 64, 200, 10, 0),
+    ("mixture", 20_000, 64, 64, 150, 1, 9),
+    ("zipf", 30_000, 96, 150, 300, 100, 0),
+    ("multichunk", 60_000, 128, 8, 96, 10, 3),  # lists of ≈ 7,500 rows: two 4,096-row chunks each
+]
+
+
+@pytest.mark.parametrize("name,rows,dims,nlist,nq,k,nprobe", TC_CASES)
+def test_ivf_tensor_core_scan_equals_fp32_scan(name, rows, dims, nlist, nq, k, nprobe):
+    # the tensor-core list scan (certified BF16 candidates + exact FP32 rerank) returns the FP32 list
+    # scan's result: the same probed rows, the same exact scores, bit for bit
+    m = make_data("zipf" if name == "zipf" else "mixture", rows, dims)
+    index = NNdex(m, approx=True, precision="auto", nlist=nlist, kmeans_iters=3, seed=42, nprobe=nprobe)
+    q = make_data("mixture", nq, dims, seed=13)
+    ti, ts = index.search(q, k=k)
+    st = index.last_search_stats()
+    assert st["path"] == 5, st
+    # again: pass 1 may now run on a sample of each list's tiles (autotuned); same result
+    ti2, ts2 = index.search(q, k=k)
+    index.set_precision("fp32")
+    fi, fs = index.search(q, k=k)
+    assert index.last_search_stats()["path"] == 4
+    for gi, gs in ((ti, ts), (ti2, ts2)):
+        np.testing.assert_array_equal(gi, fi)
+        np.testing.assert_array_equal(gs.view(np.uint32), fs.view(np.uint32))
+    # and against the oracle's probed lists
+    st_, storage = O.prepare_index(m, False)
+    ref = O.IvfIndex(storage, nlist=nlist, iters=3, seed=42)
+    _, qn = O.prepare_queries(q, False, storage.shape[1])
+    eff = nprobe if nprobe else O.choose_nprobe(ref.nlist, k, rows)
+    _, _, rc = ref.search(qn, k, nprobe)
+    for i in range(0, nq, 7):
+        check_against_probed(ref, storage, qn[i], ti[i], ts[i], int(rc[i]), k, min(eff, ref.nlist), f"{name} q{i}")
