@@ -164,6 +164,35 @@ NNDEX_API int nndex_cuda_create_from_device(const float* device_matrix, uint64_t
                                   uint64_t dims, uint32_t flags, const nndex_cuda_opts* opts,
                                   nndex_cuda_index** out);
 
+/* ---- streaming construction and file loading ----------------------------------------------
+ * The reference reads a .npy / .npz / .parquet matrix into one host Vec<f32> (load_matrix_from_disk,
+ * src/python_io.rs:80-377) and then calls NNdex::new (src/python_bindings.rs:69-86). These entry
+ * points let a loader hand the rows over in pieces instead: every piece is copied into pinned
+ * staging and uploaded while the next one is read, and K1 (validation, normalisation, padding,
+ * low-precision copies) runs on the device per piece. The finished index is identical to
+ * nndex_cuda_create on the concatenated values, with the same errors in the same order. */
+typedef struct nndex_cuda_builder nndex_cuda_builder;
+
+/* Starts an index of rows × dims (both > 0, else NNDEX_ERR_SHAPE_MISMATCH). */
+NNDEX_API int nndex_cuda_builder_begin(uint64_t rows, uint64_t dims, uint32_t flags, const nndex_cuda_opts* opts,
+                             nndex_cuda_builder** out);
+/* Appends the next `n_values` row-major values (any count, need not end on a row). Appending past
+ * rows × dims fails with NNDEX_ERR_SHAPE_MISMATCH; the builder then only accepts finish/abort. */
+NNDEX_API int nndex_cuda_builder_append(nndex_cuda_builder* builder, const float* host_values, uint64_t n_values);
+/* Completes the index (shape check, then the first non-finite / zero-norm row, then the IVF when
+ * approximate) and frees the builder, whatever the outcome. */
+NNDEX_API int nndex_cuda_builder_finish(nndex_cuda_builder* builder, nndex_cuda_index** out);
+/* Frees an unfinished builder. NULL is ignored. */
+NNDEX_API void nndex_cuda_builder_abort(nndex_cuda_builder* builder);
+
+/* Replaces load_npy + NNdex::new (src/python_io.rs:112-120): a little-endian float32, C-order,
+ * 2-D .npy file (format 1.0-3.0), memory-mapped and streamed through the builder. Other .npy
+ * layouts fail with NNDEX_ERR_INVALID_ARGUMENT ("failed to read .npy matrix from ..."); a 0-row or
+ * 0-column array with NNDEX_ERR_SHAPE_MISMATCH ("matrix loaded from ... is empty or has zero
+ * dimensions", src/python_io.rs:75-76). */
+NNDEX_API int nndex_cuda_create_from_npy(const char* path, uint32_t flags, const nndex_cuda_opts* opts,
+                               nndex_cuda_index** out);
+
 /* Rust `Drop` for CudaIndex. NULL is ignored. */
 NNDEX_API void nndex_cuda_destroy(nndex_cuda_index* index);
 

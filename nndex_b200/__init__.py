@@ -128,15 +128,44 @@ class NNdex:
                  enable_cache: bool = True, gpu_device_index: int | None = None, *, precision: str = "fp32",
                  nlist: int = 0, nprobe: int = 0, kmeans_iters: int = 0, seed: int | None = None,
                  rerank_width: int = 0, low_precision_copies: tuple = ()):
-        self._backend = _parse_backend(backend)
-        if precision not in _PRECISIONS:
-            raise ValueError(f"unsupported precision '{precision}', expected one of: {', '.join(_PRECISIONS)}")
         self._h = None
+        flags, opts = self._options(backend, normalized, approx, gpu_device_index, precision, nlist, nprobe,
+                                    kmeans_iters, seed, rerank_width, low_precision_copies)
         arr = _parse_input(data)
         if arr.ndim == 1:
             arr = arr.reshape(1, -1)
         rows, dims = arr.shape
-        self._enable_cache = enable_cache  # accepted for API parity; the CUDA backend keeps no result cache
+        h = C.c_void_p()
+        st = _lib.lib().nndex_cuda_create(arr.ctypes.data, arr.size, rows, dims, flags, C.byref(opts), C.byref(h))
+        if st != 0:
+            raise ValueError(_lib.last_error())
+        self._adopt(h, rows, dims, normalized, approx, enable_cache)
+
+    @classmethod
+    def from_file(cls, path: str, *, key: str | None = None, normalized: bool = False, approx: bool = False,
+                  backend: str = "cuda", enable_cache: bool = True, gpu_device_index: int | None = None,
+                  precision: str = "fp32", nlist: int = 0, nprobe: int = 0, kmeans_iters: int = 0,
+                  seed: int | None = None, rerank_width: int = 0, low_precision_copies: tuple = ()) -> "NNdex":
+        """src/python_bindings.rs:67-86 from_file: a .npy, .npz (``key`` names the array) or .parquet
+        (``key`` names a list<float32> column) matrix, streamed to the device piece by piece
+        (nndex_b200/_files.py); the errors of load_matrix_from_disk (src/python_io.rs:20-77) and of
+        NNdex::new, as ValueError."""
+        from . import _files
+        self = cls.__new__(cls)
+        self._h = None
+        flags, opts = cls._options(backend, normalized, approx, gpu_device_index, precision, nlist, nprobe,
+                                   kmeans_iters, seed, rerank_width, low_precision_copies)
+        h, rows, dims = _files.load(str(path), key, flags, opts)
+        self._adopt(h, rows, dims, normalized, approx, enable_cache)
+        return self
+
+    @staticmethod
+    def _options(backend, normalized, approx, gpu_device_index, precision, nlist, nprobe, kmeans_iters, seed,
+                 rerank_width, low_precision_copies):
+        """Construction flags and options (parse_index_options, src/python_bindings.rs:239-262)."""
+        _parse_backend(backend)
+        if precision not in _PRECISIONS:
+            raise ValueError(f"unsupported precision '{precision}', expected one of: {', '.join(_PRECISIONS)}")
         flags = 0
         if normalized:
             flags |= NNDEX_FLAG_NORMALIZED
@@ -158,13 +187,14 @@ class NNdex:
         opts.has_seed = 0 if seed is None else 1
         opts.seed = 0 if seed is None else int(seed)
         opts.rerank_width = rerank_width
-        h = C.c_void_p()
-        st = _lib.lib().nndex_cuda_create(arr.ctypes.data, arr.size, rows, dims, flags, C.byref(opts), C.byref(h))
-        if st != 0:
-            raise ValueError(_lib.last_error())
+        return flags, opts
+
+    def _adopt(self, h, rows, dims, normalized, approx, enable_cache):
+        self._backend = "cuda"
+        self._enable_cache = enable_cache  # accepted for API parity; the CUDA backend keeps no result cache
         self._h = h
-        self._rows = rows
-        self._dims = dims
+        self._rows = int(rows)
+        self._dims = int(dims)
         self._normalized = normalized
         self._approx = approx
 

@@ -150,6 +150,11 @@ SIGNATURES = {
     "nndex_cuda_create": (_i32, [_vp, _u64, _u64, _u64, _u32, C.POINTER(Opts), C.POINTER(_vp)]),
     "nndex_cuda_create_from_device": (_i32, [_vp, _u64, _u64, _u64, _u32, C.POINTER(Opts), C.POINTER(_vp)]),
     "nndex_cuda_destroy": (None, [_vp]),
+    "nndex_cuda_builder_begin": (_i32, [_u64, _u64, _u32, C.POINTER(Opts), C.POINTER(_vp)]),
+    "nndex_cuda_builder_append": (_i32, [_vp, _vp, _u64]),
+    "nndex_cuda_builder_finish": (_i32, [_vp, C.POINTER(_vp)]),
+    "nndex_cuda_builder_abort": (None, [_vp]),
+    "nndex_cuda_create_from_npy": (_i32, [C.c_char_p, _u32, C.POINTER(Opts), C.POINTER(_vp)]),
     "nndex_cuda_rows": (_i32, [_vp, C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64)]),
     "nndex_cuda_search": (_i32, [_vp, _vp, _u64, _u64, _vp, _vp, C.POINTER(_u64)]),
     "nndex_cuda_search_batch": (_i32, [_vp, _vp, _u64, _u64, _u64, _vp, _vp, _vp]),

@@ -798,12 +798,12 @@ static int select_device(int32_t requested, int& device) {
     return NNDEX_OK;
 }
 
-int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_t rows, uint64_t dims,
-                 uint32_t flags, const nndex_cuda_opts* opts, CudaIndex** out) {
-    if (!out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null output handle");
+// Construction in three steps (create_index below, and the streaming builder in builder.cu):
+// index_begin allocates the device copies for rows × dims; index_prep_rows runs K1 (validate,
+// normalise, pad, low-precision copies) over raw rows already on the device; index_finish checks
+// the error word and completes the index (residual bounds, tensor maps, the IVF).
+int index_begin(uint64_t rows, uint64_t dims, uint32_t flags, const nndex_cuda_opts* opts, CudaIndex** out) {
     *out = nullptr;
-    if (!shape_ok(n_values, rows, dims)) return err_shape(rows, dims, n_values);
-    if (!matrix) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null matrix");
     if (rows >= (1ull << 31))
         return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: rows=%llu above the 2^31-1 row limit",
                          (unsigned long long)rows);
@@ -855,132 +855,71 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
     cudaMemsetAsync(ix->d_err, 0xFF, sizeof(unsigned long long), ix->stream);
     cudaMemsetAsync(ix->d_status, 0, sizeof(uint32_t), ix->stream);
     // Low-precision scoring copies (K1 writes them in the same pass) and their residual norms.
-    float*& d_res16 = ix->d_res16;  // kept: the certificate's per-row bounds
-    float*& d_res8 = ix->d_res8;
-    unsigned int* d_max = nullptr;
-    auto free_tmp = [&]() {
-        cudaFree(d_max);
-        d_max = nullptr;
-    };
     if (flags & NNDEX_FLAG_BF16) {
         ix->kb16 = (dims + 63) / 64 * 64;
         if ((e = cudaMalloc(&ix->d_base_bf16, ix->rows_alloc * ix->kb16 * 2)) != cudaSuccess ||
-            (e = cudaMalloc(&d_res16, rows * sizeof(float))) != cudaSuccess) {
-            free_tmp();
+            (e = cudaMalloc(&ix->d_res16, rows * sizeof(float))) != cudaSuccess)
             return fail(cuda_error(e, "BF16 copy allocation"));
-        }
         cudaMemsetAsync(ix->d_base_bf16, 0, ix->rows_alloc * ix->kb16 * 2, ix->stream);
     }
     if (flags & NNDEX_FLAG_FP8) {
         ix->kf8 = (dims + 127) / 128 * 128;
         if ((e = cudaMalloc(&ix->d_base_fp8, ix->rows_alloc * ix->kf8)) != cudaSuccess ||
             (e = cudaMalloc(&ix->d_row_scale, ix->rows_alloc * sizeof(float))) != cudaSuccess ||
-            (e = cudaMalloc(&d_res8, rows * sizeof(float))) != cudaSuccess) {
-            free_tmp();
+            (e = cudaMalloc(&ix->d_res8, rows * sizeof(float))) != cudaSuccess)
             return fail(cuda_error(e, "FP8 copy allocation"));
-        }
         cudaMemsetAsync(ix->d_base_fp8, 0, ix->rows_alloc * ix->kf8, ix->stream);
         cudaMemsetAsync(ix->d_row_scale, 0, ix->rows_alloc * sizeof(float), ix->stream);
     }
-    auto add_low_precision = [&](PrepArgs& p, uint64_t r0) {
-        if (ix->d_base_bf16) {
-            p.out_bf16 = ix->d_base_bf16 + r0 * ix->kb16;
-            p.bf16_stride = static_cast<uint32_t>(ix->kb16);
-            p.resid_bf16 = d_res16 + r0;
-        }
-        if (ix->d_base_fp8) {
-            p.out_fp8 = ix->d_base_fp8 + r0 * ix->kf8;
-            p.fp8_stride = static_cast<uint32_t>(ix->kf8);
-            p.fp8_scale = ix->d_row_scale + r0;
-            p.resid_fp8 = d_res8 + r0;
-        }
-    };
+    *out = ix;
+    return NNDEX_OK;
+}
 
-    // K1: upload in chunks (≈256 MB of raw rows each), validate + normalise + pad on the device.
-    const int mode = ix->normalized ? 2 : 0;
-    if (on_device) {
-        // The caller may still be writing the matrix on any stream: wait for the device first.
-        if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
-            free_tmp();
-            return fail(cuda_error(e, "cudaDeviceSynchronize"));
-        }
-        PrepArgs p;
-        p.src = matrix;
-        p.rows = rows;
-        p.dims = static_cast<uint32_t>(dims);
-        p.out = ix->d_base;
-        p.out_stride = static_cast<uint32_t>(ix->ds);
-        p.mode = mode;
-        p.err = ix->d_err;
-        p.sm_count = ix->sm_count;
-        add_low_precision(p, 0);
-        launch_prep_rows(p, ix->stream);
-    } else {
-        uint64_t chunk_rows = std::max<uint64_t>(1, (256ull << 20) / (dims * sizeof(float)));
-        chunk_rows = std::min(chunk_rows, rows);
-        float* d_raw[2] = {nullptr, nullptr};
-        cudaEvent_t done[2];
-        for (int b = 0; b < 2; ++b) {
-            if ((e = cudaMalloc(&d_raw[b], chunk_rows * dims * sizeof(float))) != cudaSuccess) {
-                cudaFree(d_raw[0]);
-                free_tmp();
-                return fail(cuda_error(e, "upload staging"));
-            }
-            cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming);
-        }
-        int b = 0;
-        for (uint64_t r0 = 0; r0 < rows; r0 += chunk_rows, b ^= 1) {
-            const uint64_t n = std::min(chunk_rows, rows - r0);
-            cudaEventSynchronize(done[b]);
-            e = cudaMemcpyAsync(d_raw[b], matrix + r0 * dims, n * dims * sizeof(float), cudaMemcpyHostToDevice,
-                                ix->stream);
-            if (e != cudaSuccess) break;
-            PrepArgs p;
-            p.src = d_raw[b];
-            p.rows = n;
-            p.dims = static_cast<uint32_t>(dims);
-            p.row_base = r0;
-            p.out = ix->d_base + r0 * ix->ds;
-            p.out_stride = static_cast<uint32_t>(ix->ds);
-            p.mode = mode;
-            p.err = ix->d_err;
-            p.sm_count = ix->sm_count;
-            add_low_precision(p, r0);
-            launch_prep_rows(p, ix->stream);
-            cudaEventRecord(done[b], ix->stream);
-        }
-        cudaStreamSynchronize(ix->stream);
-        for (int i = 0; i < 2; ++i) {
-            cudaFree(d_raw[i]);
-            cudaEventDestroy(done[i]);
-        }
-        if (e != cudaSuccess) {
-            free_tmp();
-            return fail(cuda_error(e, "upload"));
-        }
+void index_prep_rows(CudaIndex* ix, const float* d_src, uint64_t row0, uint64_t n) {
+    PrepArgs p;
+    p.src = d_src;
+    p.rows = n;
+    p.dims = static_cast<uint32_t>(ix->dims);
+    p.row_base = row0;
+    p.out = ix->d_base + row0 * ix->ds;
+    p.out_stride = static_cast<uint32_t>(ix->ds);
+    p.mode = ix->normalized ? 2 : 0;
+    p.err = ix->d_err;
+    p.sm_count = ix->sm_count;
+    if (ix->d_base_bf16) {
+        p.out_bf16 = ix->d_base_bf16 + row0 * ix->kb16;
+        p.bf16_stride = static_cast<uint32_t>(ix->kb16);
+        p.resid_bf16 = ix->d_res16 + row0;
     }
+    if (ix->d_base_fp8) {
+        p.out_fp8 = ix->d_base_fp8 + row0 * ix->kf8;
+        p.fp8_stride = static_cast<uint32_t>(ix->kf8);
+        p.fp8_scale = ix->d_row_scale + row0;
+        p.resid_fp8 = ix->d_res8 + row0;
+    }
+    launch_prep_rows(p, ix->stream);
+}
+
+int index_finish(CudaIndex* ix) {
+    auto fail = [&](int code) {
+        delete ix;
+        return code;
+    };
+    cudaError_t e;
     cudaMemcpyAsync(&ix->h_flags[0], ix->d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, ix->stream);
-    if ((e = cudaStreamSynchronize(ix->stream)) != cudaSuccess) {
-        free_tmp();
-        return fail(cuda_error(e, "upload"));
-    }
-    if (ix->h_flags[0] != ~0ull) {
-        free_tmp();
-        return fail(err_code(static_cast<int>(ix->h_flags[0] & 0xFF)));
-    }
-    if (d_res16 || d_res8) {
+    if ((e = cudaStreamSynchronize(ix->stream)) != cudaSuccess) return fail(cuda_error(e, "upload"));
+    if (ix->h_flags[0] != ~0ull) return fail(err_code(static_cast<int>(ix->h_flags[0] & 0xFF)));
+    if (ix->d_res16 || ix->d_res8) {
         // ε of the certificate: the largest residual norm ‖x − x̂‖ over the rows.
-        if ((e = cudaMalloc(&d_max, 2 * sizeof(unsigned int))) != cudaSuccess) {
-            free_tmp();
-            return fail(cuda_error(e, "alloc"));
-        }
+        unsigned int* d_max = nullptr;
+        if ((e = cudaMalloc(&d_max, 2 * sizeof(unsigned int))) != cudaSuccess) return fail(cuda_error(e, "alloc"));
         cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned int), ix->stream);
-        if (d_res16) launch_max_reduce(d_res16, rows, d_max, ix->stream);
-        if (d_res8) launch_max_reduce(d_res8, rows, d_max + 1, ix->stream);
+        if (ix->d_res16) launch_max_reduce(ix->d_res16, ix->rows, d_max, ix->stream);
+        if (ix->d_res8) launch_max_reduce(ix->d_res8, ix->rows, d_max + 1, ix->stream);
         unsigned int hm[2] = {0, 0};
         cudaMemcpyAsync(hm, d_max, sizeof(hm), cudaMemcpyDeviceToHost, ix->stream);
         e = cudaStreamSynchronize(ix->stream);
-        free_tmp();
+        cudaFree(d_max);
         if (e != cudaSuccess) return fail(cuda_error(e, "residual reduction"));
         std::memcpy(&ix->eps_bf16, &hm[0], 4);
         std::memcpy(&ix->eps_fp8, &hm[1], 4);
@@ -998,8 +937,64 @@ int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_
         return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (FP8)"));
     if (ix->approx) {
         // src/approx.rs:46-100, built once at construction instead of on the first approx search.
-        if ((st = ivf_build(*ix)) != NNDEX_OK) return fail(st);
+        const int st = ivf_build(*ix);
+        if (st != NNDEX_OK) return fail(st);
     }
+    return NNDEX_OK;
+}
+
+int create_index(const float* matrix, bool on_device, uint64_t n_values, uint64_t rows, uint64_t dims,
+                 uint32_t flags, const nndex_cuda_opts* opts, CudaIndex** out) {
+    if (!out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null output handle");
+    *out = nullptr;
+    if (!shape_ok(n_values, rows, dims)) return err_shape(rows, dims, n_values);
+    if (!matrix) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null matrix");
+    CudaIndex* ix = nullptr;
+    int st = index_begin(rows, dims, flags, opts, &ix);
+    if (st) return st;
+    cudaError_t e = cudaSuccess;
+    // K1: upload in chunks (≈256 MB of raw rows each), validate + normalise + pad on the device.
+    if (on_device) {
+        // The caller may still be writing the matrix on any stream: wait for the device first.
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
+            delete ix;
+            return cuda_error(e, "cudaDeviceSynchronize");
+        }
+        index_prep_rows(ix, matrix, 0, rows);
+    } else {
+        uint64_t chunk_rows = std::max<uint64_t>(1, (256ull << 20) / (dims * sizeof(float)));
+        chunk_rows = std::min(chunk_rows, rows);
+        float* d_raw[2] = {nullptr, nullptr};
+        cudaEvent_t done[2];
+        for (int b = 0; b < 2; ++b) {
+            if ((e = cudaMalloc(&d_raw[b], chunk_rows * dims * sizeof(float))) != cudaSuccess) {
+                cudaFree(d_raw[0]);
+                delete ix;
+                return cuda_error(e, "upload staging");
+            }
+            cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming);
+        }
+        int b = 0;
+        for (uint64_t r0 = 0; r0 < rows; r0 += chunk_rows, b ^= 1) {
+            const uint64_t n = std::min(chunk_rows, rows - r0);
+            cudaEventSynchronize(done[b]);
+            e = cudaMemcpyAsync(d_raw[b], matrix + r0 * dims, n * dims * sizeof(float), cudaMemcpyHostToDevice,
+                                ix->stream);
+            if (e != cudaSuccess) break;
+            index_prep_rows(ix, d_raw[b], r0, n);
+            cudaEventRecord(done[b], ix->stream);
+        }
+        cudaStreamSynchronize(ix->stream);
+        for (int i = 0; i < 2; ++i) {
+            cudaFree(d_raw[i]);
+            cudaEventDestroy(done[i]);
+        }
+        if (e != cudaSuccess) {
+            delete ix;
+            return cuda_error(e, "upload");
+        }
+    }
+    if ((st = index_finish(ix))) return st;
     *out = ix;
     return NNDEX_OK;
 }

@@ -21,6 +21,8 @@ int set_error(int code, const char* fmt, ...);
 void clear_error();
 const char* last_error();
 int cuda_error(cudaError_t e, const char* what);
+// NNdexError::ShapeMismatch (src/lib.rs:109-112).
+int err_shape(uint64_t rows, uint64_t dims, uint64_t values);
 
 struct CudaIndex {
     bool owns_base = true;    // false for a view (make_view): the device data belongs to another handle
@@ -193,6 +195,9 @@ struct CudaIndex {
 };
 
 int make_view(const CudaIndex& src, CudaIndex** out);
+int index_begin(uint64_t rows, uint64_t dims, uint32_t flags, const nndex_cuda_opts* opts, CudaIndex** out);
+void index_prep_rows(CudaIndex* ix, const float* d_src, uint64_t row0, uint64_t n);
+int index_finish(CudaIndex* ix);  // deletes ix on failure
 int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out,
                           float* d_sim_out, uint32_t* d_cnt_out, cudaStream_t s);
 
