@@ -725,6 +725,37 @@ def run_ivf(args, dev, L, world):
             cpu[str(np_)] = {"queries_per_s": qs.shape[0] / dt, "cores": O.num_threads(),
                              "sample": f"{qs.shape[0]} queries, same index (restated src/cpu.rs:456-502)"}
         del ref, storage
+    # The saved layout installed into a second index over the same rows instead of building it.
+    n_lay = C.c_uint64(0)
+    L.nndex_cuda_ivf_layout(h, C.byref(n_lay), None, None, None, None)
+    nl = n_lay.value
+    r_cent = np.zeros((nl, (dims + 7) // 8 * 8), dtype=np.float32)
+    r_off, r_orig, r_init = (np.zeros(nl + 1, dtype=np.uint64), np.zeros(rows, dtype=np.uint64),
+                             np.zeros(nl, dtype=np.uint64))
+    L.nndex_cuda_ivf_layout(h, C.byref(n_lay), r_cent.ctypes.data, r_off.ctypes.data, r_orig.ctypes.data,
+                            r_init.ctypes.data)
+    hr = C.c_void_p()
+    if L.nndex_cuda_create_from_device(base.data_ptr(), base.numel(), rows, dims, NNDEX_FLAG_NORMALIZED,
+                                       C.byref(opts), C.byref(hr)) != 0:
+        raise RuntimeError(_lib.last_error())
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    if L.nndex_cuda_ivf_restore(hr, nl, r_cent.ctypes.data, r_off.ctypes.data, r_orig.ctypes.data,
+                                r_init.ctypes.data) != 0:
+        raise RuntimeError(_lib.last_error())
+    restore_wall = time.perf_counter() - t0
+    rst = _lib.IvfStats()
+    L.nndex_cuda_ivf_stats_get(hr, C.byref(rst))
+    restored_equal = True
+    ri_, rs_ = torch.empty_like(oi), torch.empty_like(os_)
+    for np_ in [int(x) for x in args.ivf_nprobe.split(",") if x]:
+        for hh in (h, hr):
+            L.nndex_cuda_set_nprobe(hh, np_)
+            L.nndex_cuda_set_precision(hh, NNDEX_PRECISION_AUTO, 0)
+        L.nndex_cuda_search_batch_device(h, q.data_ptr(), nq, dims, k, oi.data_ptr(), os_.data_ptr(), None, sptr, 1)
+        L.nndex_cuda_search_batch_device(hr, q.data_ptr(), nq, dims, k, ri_.data_ptr(), rs_.data_ptr(), None, sptr, 1)
+        restored_equal &= bool(torch.equal(oi, ri_)) and bool(torch.equal(os_.view(torch.int32), rs_.view(torch.int32)))
+    L.nndex_cuda_destroy(hr)
     L.nndex_cuda_destroy(h)
     del base
     torch.cuda.empty_cache()
@@ -736,6 +767,8 @@ def run_ivf(args, dev, L, world):
                   "layout_ms": bst.layout_ms, "wall_s_with_upload": build_wall, "max_list": bst.max_list,
                   "ambiguous_rows_all_iters": bst.ambiguous_rows,
                   "candidate_rows_all_iters": bst.candidate_rows, "seed_exact_rows": bst.seed_exact_rows},
+        "restore_saved_layout": {"device_ms": rst.build_ms, "wall_s": restore_wall,
+                                 "results_equal_built_index": restored_equal},
         "data_fingerprint": data_fp,
         "exact_fp32_ms_per_batch": exact_ms,
         "by_nprobe": per,

@@ -305,6 +305,26 @@ NNDEX_API int nndex_cuda_search_batch_device_noalloc(nndex_cuda_index* index, co
 NNDEX_API int nndex_cuda_ivf_layout(nndex_cuda_index* index, uint64_t* nlist_out, float* centroids,
                                     uint64_t* offsets, uint64_t* original_indices, uint64_t* init_rows);
 NNDEX_API int nndex_cuda_ivf_stats_get(const nndex_cuda_index* index, nndex_cuda_ivf_stats* out);
+/*
+ * Installs a saved IVF instead of building one (the build, src/approx.rs:46-100, is the most
+ * expensive one-off of approximate mode). The arrays are the ones nndex_cuda_ivf_layout exports
+ * from an index over the same matrix: centroids [nlist × padded_dims] f32, offsets [nlist + 1],
+ * original_indices [rows] (reordered position → row), init_rows [nlist] or NULL. nlist 0 installs
+ * "no IVF" (the reference answers such indexes exactly). Checks offsets (0 … rows, non-decreasing),
+ * that original_indices is a permutation and that the centroids are finite
+ * (NNDEX_ERR_INVALID_ARGUMENT otherwise); it cannot check that the layout was made from THIS
+ * matrix: compare nndex_cuda_base_checksum values for that. Afterwards the index is in approximate
+ * mode and answers as the index the layout was exported from. Waits for the device; not while a
+ * server runs on the index.
+ */
+NNDEX_API int nndex_cuda_ivf_restore(nndex_cuda_index* index, uint64_t nlist, const float* centroids,
+                                     const uint64_t* offsets, const uint64_t* original_indices,
+                                     const uint64_t* init_rows);
+
+/* 64-bit fingerprint of the stored (validated, normalised, padded) rows: Σ over positions i of
+ * splitmix64(i · 2^32 + bits of value i), mod 2^64. Equal matrices give equal values on any GPU. */
+NNDEX_API int nndex_cuda_base_checksum(nndex_cuda_index* index, uint64_t* checksum);
+
 /* Lists probed per query by later approx searches (0 = choose_nprobe, src/approx.rs:318-336);
  * no counterpart in the reference, whose nprobe is always the policy's. */
 NNDEX_API int nndex_cuda_set_nprobe(nndex_cuda_index* index, uint32_t nprobe);

@@ -30,6 +30,9 @@ _PRECISIONS = {
 }
 
 
+_IVF_FORMAT = "nndex-cuda-ivf/1"
+
+
 class NNdexError(RuntimeError):
     """A failed C-ABI call: ``code`` is the NNDEX_ERR_* status, the message NNdexError's Display."""
 
@@ -127,10 +130,10 @@ class NNdex:
     def __init__(self, data: Any, normalized: bool = False, approx: bool = False, backend: str = "cuda",
                  enable_cache: bool = True, gpu_device_index: int | None = None, *, precision: str = "fp32",
                  nlist: int = 0, nprobe: int = 0, kmeans_iters: int = 0, seed: int | None = None,
-                 rerank_width: int = 0, low_precision_copies: tuple = ()):
+                 rerank_width: int = 0, low_precision_copies: tuple = (), ivf: Any = None):
         self._h = None
         flags, opts = self._options(backend, normalized, approx, gpu_device_index, precision, nlist, nprobe,
-                                    kmeans_iters, seed, rerank_width, low_precision_copies)
+                                    kmeans_iters, seed, rerank_width, low_precision_copies, ivf)
         arr = _parse_input(data)
         if arr.ndim == 1:
             arr = arr.reshape(1, -1)
@@ -140,12 +143,15 @@ class NNdex:
         if st != 0:
             raise ValueError(_lib.last_error())
         self._adopt(h, rows, dims, normalized, approx, enable_cache)
+        if ivf is not None:
+            self.load_ivf(ivf)
 
     @classmethod
     def from_file(cls, path: str, *, key: str | None = None, normalized: bool = False, approx: bool = False,
                   backend: str = "cuda", enable_cache: bool = True, gpu_device_index: int | None = None,
                   precision: str = "fp32", nlist: int = 0, nprobe: int = 0, kmeans_iters: int = 0,
-                  seed: int | None = None, rerank_width: int = 0, low_precision_copies: tuple = ()) -> "NNdex":
+                  seed: int | None = None, rerank_width: int = 0, low_precision_copies: tuple = (),
+                  ivf: Any = None) -> "NNdex":
         """src/python_bindings.rs:67-86 from_file: a .npy, .npz (``key`` names the array) or .parquet
         (``key`` names a list<float32> column) matrix, streamed to the device piece by piece
         (nndex_b200/_files.py); the errors of load_matrix_from_disk (src/python_io.rs:20-77) and of
@@ -154,22 +160,27 @@ class NNdex:
         self = cls.__new__(cls)
         self._h = None
         flags, opts = cls._options(backend, normalized, approx, gpu_device_index, precision, nlist, nprobe,
-                                   kmeans_iters, seed, rerank_width, low_precision_copies)
+                                   kmeans_iters, seed, rerank_width, low_precision_copies, ivf)
         h, rows, dims = _files.load(str(path), key, flags, opts)
         self._adopt(h, rows, dims, normalized, approx, enable_cache)
+        if ivf is not None:
+            self.load_ivf(ivf)
         return self
 
     @staticmethod
     def _options(backend, normalized, approx, gpu_device_index, precision, nlist, nprobe, kmeans_iters, seed,
-                 rerank_width, low_precision_copies):
-        """Construction flags and options (parse_index_options, src/python_bindings.rs:239-262)."""
+                 rerank_width, low_precision_copies, ivf=None):
+        """Construction flags and options (parse_index_options, src/python_bindings.rs:239-262).
+        With a saved IVF (``ivf``) the index is created without building one."""
         _parse_backend(backend)
         if precision not in _PRECISIONS:
             raise ValueError(f"unsupported precision '{precision}', expected one of: {', '.join(_PRECISIONS)}")
+        if ivf is not None and not approx:
+            raise ValueError("a saved IVF (ivf=...) needs approx=True")
         flags = 0
         if normalized:
             flags |= NNDEX_FLAG_NORMALIZED
-        if approx:
+        if approx and ivf is None:
             flags |= NNDEX_FLAG_APPROX
         # "bf16" / "fp8" keep that scoring copy; "auto" keeps a BF16 copy for large batches.
         if precision in ("bf16", "auto"):
@@ -276,6 +287,57 @@ class NNdex:
     def set_nprobe(self, nprobe: int) -> None:
         """Lists probed per query by later approx searches (0 = the reference's choose_nprobe)."""
         _check(_lib.lib().nndex_cuda_set_nprobe(self._h, int(nprobe)))
+
+    def checksum(self) -> int:
+        """64-bit fingerprint of the stored (validated, normalised) rows (nndex_cuda_base_checksum)."""
+        out = C.c_uint64(0)
+        _check(_lib.lib().nndex_cuda_base_checksum(self._h, C.byref(out)))
+        return int(out.value)
+
+    def save_ivf(self, path: str) -> None:
+        """Writes the IVF (ivf_layout) with the matrix's shape and checksum to an .npz file, so that
+        a later index over the same matrix can skip the build (``NNdex(..., approx=True, ivf=path)``)."""
+        if not self._approx:
+            raise ValueError("save_ivf needs an approx index")
+        lay = self.ivf_layout()
+        if lay is None:
+            pd = (self._dims + 7) // 8 * 8
+            lay = {"centroids": np.zeros((0, pd), np.float32), "cluster_offsets": np.zeros(0, np.uint64),
+                   "original_indices": np.zeros(0, np.uint64), "init_rows": np.zeros(0, np.uint64)}
+        with open(path, "wb") as f:
+            np.savez(f, format=np.array(_IVF_FORMAT), rows=np.uint64(self._rows), dims=np.uint64(self._dims),
+                     normalized=np.bool_(self._normalized), checksum=np.uint64(self.checksum()),
+                     nlist=np.uint64(len(lay["init_rows"])), **lay)
+
+    def load_ivf(self, source: Any) -> None:
+        """Installs a saved IVF (a path written by save_ivf, or an ivf_layout() dict) instead of
+        building one; the index answers approx searches as the index it was saved from."""
+        if isinstance(source, dict):
+            lay = source
+            nl = len(lay["init_rows"]) if lay.get("init_rows") is not None else len(lay["cluster_offsets"]) - 1
+        else:
+            with np.load(source, allow_pickle=False) as z:
+                if "format" not in z.files or str(z["format"]) != _IVF_FORMAT:
+                    raise ValueError(f"'{source}' is not a saved nndex IVF")
+                if int(z["rows"]) != self._rows or int(z["dims"]) != self._dims:
+                    raise ValueError(f"the IVF in '{source}' was saved for a {int(z['rows'])} x {int(z['dims'])} "
+                                     f"matrix, this index is {self._rows} x {self._dims}")
+                if int(z["checksum"]) != self.checksum():
+                    raise ValueError(f"the IVF in '{source}' was saved for a different matrix (checksum mismatch)")
+                lay = {k: z[k] for k in ("centroids", "cluster_offsets", "original_indices", "init_rows")}
+                nl = int(z["nlist"])
+        pd = (self._dims + 7) // 8 * 8
+        cent = np.ascontiguousarray(lay["centroids"], dtype=np.float32).reshape(nl, pd) if nl else None
+        off = np.ascontiguousarray(lay["cluster_offsets"], dtype=np.uint64)
+        orig = np.ascontiguousarray(lay["original_indices"], dtype=np.uint64)
+        init = lay.get("init_rows")
+        init = np.ascontiguousarray(init, dtype=np.uint64) if init is not None else None
+        if nl and (len(off) != nl + 1 or len(orig) != self._rows or (init is not None and len(init) != nl)):
+            raise ValueError("IVF layout arrays do not match nlist and the index's rows")
+        ptr = lambda a: a.ctypes.data if a is not None else None  # noqa: E731
+        _check(_lib.lib().nndex_cuda_ivf_restore(self._h, nl, ptr(cent), ptr(off) if nl else None,
+                                                 ptr(orig) if nl else None, ptr(init) if nl else None))
+        self._approx = True
 
     def ivf_stats(self) -> dict:
         s = _lib.IvfStats()

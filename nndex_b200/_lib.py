@@ -171,6 +171,8 @@ SIGNATURES = {
     "nndex_cuda_ivf_layout": (_i32, [_vp, C.POINTER(_u64), _vp, _vp, _vp, _vp]),
     "nndex_cuda_ivf_stats_get": (_i32, [_vp, C.POINTER(IvfStats)]),
     "nndex_cuda_set_nprobe": (_i32, [_vp, _u32]),
+    "nndex_cuda_ivf_restore": (_i32, [_vp, _u64, _vp, _vp, _vp, _vp]),
+    "nndex_cuda_base_checksum": (_i32, [_vp, C.POINTER(_u64)]),
     "nndex_cuda_server_start": (_i32, [_vp, C.POINTER(ServerOpts), C.POINTER(_vp)]),
     "nndex_cuda_server_submit": (_i32, [_vp, _vp, _u64, _u64, _u64, _u32, _u32, C.POINTER(_u64)]),
     "nndex_cuda_server_poll": (_i32, [_vp, _u64, C.c_int32, _vp, _vp, _vp, C.POINTER(RequestInfo)]),

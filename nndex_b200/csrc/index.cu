@@ -1307,6 +1307,33 @@ int nndex_cuda_ivf_layout(nndex_cuda_index* index, uint64_t* nlist_out, float* c
     return NNDEX_OK;
 }
 
+int nndex_cuda_ivf_restore(nndex_cuda_index* index, uint64_t nlist, const float* centroids, const uint64_t* offsets,
+                           const uint64_t* original_indices, const uint64_t* init_rows) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    if (!ix->owns_base)
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: cannot restore an IVF into a view");
+    cudaSetDevice(ix->device);
+    cudaError_t e = cudaDeviceSynchronize();  // searches in flight on any stream read the old IVF
+    if (e != cudaSuccess) return cuda_error(e, "IVF restore");
+    const int st = ivf_restore(*ix, nlist, centroids, offsets, original_indices, init_rows);
+    if (st == NNDEX_OK) ix->approx = true;
+    return st;
+}
+
+int nndex_cuda_base_checksum(nndex_cuda_index* index, uint64_t* checksum) {
+    clear_error();
+    if (!index || !checksum) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null argument");
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    cudaSetDevice(ix->device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_error(e, "checksum");
+    return base_checksum(*ix, checksum);
+}
+
 int nndex_cuda_set_nprobe(nndex_cuda_index* index, uint32_t nprobe) {
     clear_error();
     if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");

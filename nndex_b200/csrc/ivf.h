@@ -73,6 +73,14 @@ struct IvfScratch {
 // and the seed come from ix.opts (0 = the reference's policy). Returns an NNDEX status.
 int ivf_build(CudaIndex& ix);
 
+// Installs a saved IVF layout (the arrays nndex_cuda_ivf_layout exports: centroids nlist ×
+// padded dims, offsets nlist + 1, original indices rows, k-means++ rows nlist or NULL) instead of
+// building one; nlist 0 removes the IVF. Validates the arrays. Synchronises ix.stream.
+int ivf_restore(CudaIndex& ix, uint64_t nlist, const float* centroids, const uint64_t* offsets,
+                const uint64_t* original_indices, const uint64_t* init_rows);
+// Position-sensitive 64-bit fingerprint of the stored (normalised, padded) rows.
+int base_checksum(CudaIndex& ix, uint64_t* out);
+
 // Enqueues the IVF search of `nq` normalised queries (stride ds) with capped k into the device
 // outputs (rows of `k` slots), on the FP32 list scan. Returns an NNDEX status.
 int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim,

@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <cstring>
 
 #include "common.cuh"
@@ -1044,6 +1045,46 @@ struct Timer {
 
 }  // namespace
 
+// Cluster-contiguous copies of the rows for the list scans, in the order of v.d_row_map: the FP32
+// rows and their BF16 copy with per-row residual bounds, whose maximum is raised into *d_eps.
+// Enqueued on ix.stream.
+static cudaError_t ivf_enqueue_layout(CudaIndex& ix, IvfIndex& v, unsigned int* d_eps) {
+    const uint64_t rows = ix.rows, ds = ix.ds;
+    const cudaStream_t s = ix.stream;
+    const uint64_t kb16 = (ix.dims + 63) / 64 * 64;
+    cudaError_t e;
+    if ((e = cudaMalloc(&v.d_reordered, ix.rows_alloc * ds * sizeof(float))) != cudaSuccess) return e;
+    cudaMemsetAsync(v.d_reordered + rows * ds, 0, (ix.rows_alloc - rows) * ds * sizeof(float), s);
+    const uint32_t gb = static_cast<uint32_t>(std::min<uint64_t>((rows * 32 + 255) / 256, ix.sm_count * 16ull));
+    gather_rows_kernel<<<gb, 256, 0, s>>>(ix.d_base, static_cast<uint32_t>(ds), v.d_row_map, rows, v.d_reordered);
+    count_launch();
+    v.kb16 = kb16;
+    if ((e = cudaMalloc(&v.d_reordered16, ix.rows_alloc * kb16 * sizeof(__nv_bfloat16))) != cudaSuccess ||
+        (e = cudaMalloc(&v.d_res16, rows * sizeof(float))) != cudaSuccess)
+        return e;
+    cudaMemsetAsync(v.d_reordered16 + rows * kb16, 0, (ix.rows_alloc - rows) * kb16 * sizeof(__nv_bfloat16), s);
+    bf16_rows_kernel<<<gb, 256, 0, s>>>(v.d_reordered, static_cast<uint32_t>(ds), rows, v.d_reordered16,
+                                        static_cast<uint32_t>(kb16), v.d_res16);
+    count_launch();
+    if ((e = launch_max_reduce(v.d_res16, rows, d_eps, s)) != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+// Once the layout has completed (v.h_offsets set): the longest list, the BF16 residual bound and
+// the tensor maps of the reordered copies.
+static int ivf_complete_layout(CudaIndex& ix, IvfIndex& v, unsigned int eps_bits) {
+    v.max_list = 0;
+    for (uint64_t c = 0; c < v.nlist; ++c) v.max_list = std::max<uint64_t>(v.max_list, v.h_offsets[c + 1] - v.h_offsets[c]);
+    if (!encode_tmap_2d(&v.tmap_reordered, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, v.d_reordered, ix.ds, ix.rows_alloc,
+                        ix.ds * sizeof(float), 32, 128, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !encode_tmap_2d(&v.tmap_reordered16, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, v.d_reordered16, v.kb16,
+                        ix.rows_alloc, v.kb16 * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B))
+        return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (IVF rows)");
+    std::memcpy(&v.eps16, &eps_bits, sizeof(float));
+    if (ix.kb16 == 0) ix.kb16 = v.kb16;  // BF16 query copies for the tensor-core list scan
+    return NNDEX_OK;
+}
+
 int ivf_build(CudaIndex& ix) {
     const uint64_t rows = ix.rows, ds = ix.ds, dp = ix.dp;
     const cudaStream_t s = ix.stream;
@@ -1060,7 +1101,6 @@ int ivf_build(CudaIndex& ix) {
     ix.ivf_scratch.nprobe = ix.opts.nprobe;
     v.nlist_pad = (nlist + 255) / 256 * 256;
     const uint64_t kb = (ix.dims + 63) / 64 * 64;  // FP16 / BF16 row length (64-element K slabs)
-    const uint64_t kb16 = kb;
     BuildScratch tmp;
     cudaError_t e = cudaSuccess;
     auto oom = [&](const char* what) { return cuda_error(e, what); };
@@ -1242,26 +1282,10 @@ int ivf_build(CudaIndex& ix) {
     count_launch();
     cudaEventRecord(t_km.b, s);
 
-    // List layout: the reordered FP32 rows.
+    // List layout: the reordered FP32 rows and their BF16 copy.
     cudaEventRecord(t_lay.a, s);
-    if ((e = cudaMalloc(&v.d_reordered, ix.rows_alloc * ds * sizeof(float))) != cudaSuccess) return oom("IVF reordered rows");
-    cudaMemsetAsync(v.d_reordered + rows * ds, 0, (ix.rows_alloc - rows) * ds * sizeof(float), s);
-    {
-        const uint32_t gb = static_cast<uint32_t>(std::min<uint64_t>((rows * 32 + 255) / 256, ix.sm_count * 16ull));
-        gather_rows_kernel<<<gb, 256, 0, s>>>(ix.d_base, static_cast<uint32_t>(ds), perm, rows, v.d_reordered);
-        count_launch();
-        // BF16 copy for the tensor-core list scan, and the bound of its residuals
-        v.kb16 = kb16;
-        if ((e = cudaMalloc(&v.d_reordered16, ix.rows_alloc * kb16 * sizeof(__nv_bfloat16))) != cudaSuccess ||
-            (e = cudaMalloc(&v.d_res16, rows * sizeof(float))) != cudaSuccess)
-            return oom("IVF BF16 rows");
-        cudaMemsetAsync(v.d_reordered16 + rows * kb16, 0, (ix.rows_alloc - rows) * kb16 * sizeof(__nv_bfloat16), s);
-        bf16_rows_kernel<<<gb, 256, 0, s>>>(v.d_reordered, static_cast<uint32_t>(ds), rows, v.d_reordered16,
-                                            static_cast<uint32_t>(kb16), v.d_res16);
-        count_launch();
-        cudaMemsetAsync(cmax, 0, sizeof(unsigned int), s);
-        if ((e = launch_max_reduce(v.d_res16, rows, cmax, s)) != cudaSuccess) return cuda_error(e, "IVF residual bound");
-    }
+    cudaMemsetAsync(cmax, 0, sizeof(unsigned int), s);
+    if ((e = ivf_enqueue_layout(ix, v, cmax)) != cudaSuccess) return oom("IVF reordered rows");
     cudaEventRecord(t_lay.b, s);
     cudaEventRecord(t_all.b, s);
 
@@ -1282,14 +1306,8 @@ int ivf_build(CudaIndex& ix) {
 
     v.h_offsets.assign(h_off.begin(), h_off.end());
     v.h_init_rows.assign(h_chosen.begin(), h_chosen.end());
-    for (uint64_t c = 0; c < nlist; ++c) v.max_list = std::max<uint64_t>(v.max_list, h_off[c + 1] - h_off[c]);
-    if (!encode_tmap_2d(&v.tmap_reordered, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, v.d_reordered, ds, ix.rows_alloc,
-                        ds * sizeof(float), 32, 128, CU_TENSOR_MAP_SWIZZLE_128B) ||
-        !encode_tmap_2d(&v.tmap_reordered16, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, v.d_reordered16, kb16, ix.rows_alloc,
-                        kb16 * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B))
-        return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (IVF rows)");
-    std::memcpy(&v.eps16, &h_eps, sizeof(float));
-    if (ix.kb16 == 0) ix.kb16 = kb16;  // BF16 query copies for the tensor-core list scan
+    const int st = ivf_complete_layout(ix, v, h_eps);
+    if (st != NNDEX_OK) return st;
     float ms = 0.0f;
     v.stats.nlist = nlist;
     v.stats.iters = iters;
@@ -1308,6 +1326,129 @@ int ivf_build(CudaIndex& ix) {
         v.stats.candidate_rows += h_amb[2 * i + 1];
     }
     ix.ivf = std::move(ivf);
+    return NNDEX_OK;
+}
+
+int ivf_restore(CudaIndex& ix, uint64_t nlist, const float* centroids, const uint64_t* offsets,
+                const uint64_t* original_indices, const uint64_t* init_rows) {
+    const uint64_t rows = ix.rows, ds = ix.ds, dp = ix.dp;
+    const cudaStream_t s = ix.stream;
+    auto bad = [](const char* why) {
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: invalid IVF layout: %s", why);
+    };
+    if (nlist == 0) {  // the layout of an index the reference answers exactly (src/approx.rs:49-59)
+        ix.ivf.reset();
+        return NNDEX_OK;
+    }
+    if (nlist == 1) return bad("nlist must be 0 or at least 2");
+    if (nlist > 16384)
+        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: nlist=%llu above the 16384 limit",
+                         (unsigned long long)nlist);
+    if (!centroids || !offsets || !original_indices) return bad("null array");
+    // Lists: offsets from 0 to rows, non-decreasing; original_indices a permutation of the rows.
+    if (offsets[0] != 0 || offsets[nlist] != rows) return bad("cluster offsets must run from 0 to rows");
+    for (uint64_t c = 0; c < nlist; ++c)
+        if (offsets[c + 1] < offsets[c]) return bad("cluster offsets must be non-decreasing");
+    std::vector<uint32_t> map(rows);
+    {
+        std::vector<uint8_t> seen(rows, 0);
+        for (uint64_t i = 0; i < rows; ++i) {
+            const uint64_t r = original_indices[i];
+            if (r >= rows || seen[r]) return bad("original indices must be a permutation of the rows");
+            seen[r] = 1;
+            map[i] = static_cast<uint32_t>(r);
+        }
+    }
+    for (uint64_t i = 0; i < nlist * dp; ++i)
+        if (!std::isfinite(centroids[i])) return bad("non-finite centroid value");
+    if (init_rows)
+        for (uint64_t c = 0; c < nlist; ++c)
+            if (init_rows[c] >= rows) return bad("k-means++ row out of range");
+
+    auto ivf = std::make_shared<IvfIndex>();
+    IvfIndex& v = *ivf;
+    v.nlist = nlist;
+    v.nlist_pad = (nlist + 255) / 256 * 256;
+    cudaError_t e;
+    Timer t_all;
+    cudaEventRecord(t_all.a, s);
+    if ((e = cudaMalloc(&v.d_centroids, nlist * ds * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&v.d_cent_t, ds * v.nlist_pad * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&v.d_row_map, rows * sizeof(uint32_t))) != cudaSuccess ||
+        (e = cudaMalloc(&v.d_offsets, (nlist + 1) * sizeof(uint32_t))) != cudaSuccess)
+        return cuda_error(e, "IVF layout");
+    std::vector<uint32_t> off32(offsets, offsets + nlist + 1);
+    unsigned int* d_eps = nullptr;
+    if ((e = cudaMalloc(&d_eps, sizeof(unsigned int))) != cudaSuccess) return cuda_error(e, "IVF layout");
+    BuildScratch tmp;
+    tmp.ptrs.push_back(d_eps);
+    cudaMemsetAsync(d_eps, 0, sizeof(unsigned int), s);
+    cudaMemsetAsync(v.d_centroids, 0, nlist * ds * sizeof(float), s);
+    cudaMemsetAsync(v.d_cent_t, 0, ds * v.nlist_pad * sizeof(float), s);
+    if ((e = cudaMemcpy2DAsync(v.d_centroids, ds * sizeof(float), centroids, dp * sizeof(float), dp * sizeof(float),
+                               nlist, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(v.d_row_map, map.data(), rows * sizeof(uint32_t), cudaMemcpyHostToDevice, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(v.d_offsets, off32.data(), (nlist + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s)) !=
+            cudaSuccess)
+        return cuda_error(e, "IVF layout upload");
+    const uint64_t kb = (ix.dims + 63) / 64 * 64;
+    centroid_prep_kernel<<<static_cast<unsigned>((nlist * 32 + 255) / 256), 256, 0, s>>>(
+        v.d_centroids, static_cast<uint32_t>(ds), static_cast<uint32_t>(nlist), nullptr, static_cast<uint32_t>(kb),
+        v.d_cent_t, v.nlist_pad, nullptr);
+    count_launch();
+    if ((e = ivf_enqueue_layout(ix, v, d_eps)) != cudaSuccess) return cuda_error(e, "IVF reordered rows");
+    cudaEventRecord(t_all.b, s);
+    unsigned int h_eps = 0;
+    cudaMemcpyAsync(&h_eps, d_eps, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
+    // the host arrays above are read by the copies until the stream drains
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "IVF layout");
+    v.h_offsets.assign(offsets, offsets + nlist + 1);
+    if (init_rows) v.h_init_rows.assign(init_rows, init_rows + nlist);
+    else v.h_init_rows.assign(nlist, 0);
+    const int st = ivf_complete_layout(ix, v, h_eps);
+    if (st != NNDEX_OK) return st;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, t_all.a, t_all.b);
+    v.stats.nlist = nlist;
+    v.stats.max_list = v.max_list;
+    v.stats.build_ms = ms;
+    v.stats.layout_ms = ms;
+    ix.ivf_scratch.nprobe = ix.opts.nprobe;
+    ix.ivf = std::move(ivf);
+    return NNDEX_OK;
+}
+
+// Σ over the stored values (row-major, rows × ds) of splitmix64(position · 2^32 + bits): a
+// position-sensitive fingerprint, identical for identical stored matrices whatever the launch.
+__global__ void base_checksum_kernel(const uint32_t* __restrict__ bits, uint64_t n, unsigned long long* out) {
+    uint64_t acc = 0;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t z = (i << 32) + bits[i] + 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        acc += z ^ (z >> 31);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(out, static_cast<unsigned long long>(acc));
+}
+
+int base_checksum(CudaIndex& ix, uint64_t* out) {
+    unsigned long long* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(unsigned long long));
+    if (e != cudaSuccess) return cuda_error(e, "checksum");
+    cudaMemsetAsync(d, 0, sizeof(unsigned long long), ix.stream);
+    const uint64_t n = ix.rows * ix.ds;
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, ix.sm_count * 8ull));
+    base_checksum_kernel<<<blocks, 256, 0, ix.stream>>>(reinterpret_cast<const uint32_t*>(ix.d_base), n, d);
+    count_launch();
+    unsigned long long h = 0;
+    cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, ix.stream);
+    e = cudaStreamSynchronize(ix.stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_error(e, "checksum");
+    *out = h;
     return NNDEX_OK;
 }
 
