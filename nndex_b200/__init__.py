@@ -373,8 +373,13 @@ class NNdex:
                                                 sim.ctypes.data, cnt.ctypes.data)
         if st != 0:
             raise NNdexError(st, _lib.last_error())
-        # batch_neighbors_to_numpy (src/python_bindings.rs:465-497): width = first row's length;
-        # shorter rows padded with (0, 0.0), longer rows truncated.
+        return idx, sim, cnt
+
+    @staticmethod
+    def _rectangular(idx, sim, cnt):
+        """batch_neighbors_to_numpy (src/python_bindings.rs:465-497): width = the first row's
+        length; shorter rows padded with (0, 0.0), longer rows truncated."""
+        rows = idx.shape[0]
         cols = int(cnt[0]) if rows else 0
         idx = np.ascontiguousarray(idx[:, :cols])
         sim = np.ascontiguousarray(sim[:, :cols])
@@ -399,16 +404,22 @@ class NNdex:
             return self._to_df([res], *out_df) if out_df else res
         if dims != self._dims:
             raise ValueError(f"query dims mismatch: expected {self._dims}, got {dims}")
-        if q.shape[0] == 1:
+        # A one-row float32 matrix that is not contiguous takes the batch path in the reference
+        # (src/python_bindings.rs:170-198: the single search needs `as_slice`).
+        strided_f32 = (not query_is_df and isinstance(query, np.ndarray) and query.dtype == np.float32
+                       and query.ndim == 2 and not query.flags.c_contiguous)
+        if q.shape[0] == 1 and not strided_f32:
             res = self._single_or_raise(q.reshape(-1), k)
             return self._to_df([res], *out_df) if out_df else res
         try:
-            idx, sim = self._search_batch(q, k)
+            idx, sim, cnt = self._search_batch(q, k)
         except NNdexError as e:
             raise RuntimeError(str(e)) from e
         if out_df:
-            return self._to_df([(idx[r], sim[r]) for r in range(idx.shape[0])], *out_df)
-        return idx, sim
+            # every query's own neighbours (neighbors_to_source_dataframe, src/python_bindings.rs:500-553)
+            n = [int(c) for c in cnt]
+            return self._to_df([(idx[r, :n[r]], sim[r, :n[r]]) for r in range(idx.shape[0])], *out_df)
+        return self._rectangular(idx, sim, cnt)
 
     def _single_or_raise(self, q: np.ndarray, k: int):
         try:
