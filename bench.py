@@ -354,12 +354,16 @@ def run_ours(args):
         scan_ms = C.c_double(0.0)
         scan_n = C.c_uint64(0)
         L.nndex_cuda_scan_timing(h, C.byref(scan_ms), C.byref(scan_n))
+        sst = _lib.SearchStats()
+        L.nndex_cuda_last_search_stats(h, C.byref(sst))
         max_ms, total_q = aggregate(ms, b * args.steps, world, dev)
         results[b] = {
             "ms_per_step": max_ms / args.steps,
             "queries_per_s": total_q / (max_ms / 1e3),
             "scan_ms": scan_ms.value / max(scan_n.value, 1),
             "launches": n1 - n0,
+            "kernel": (f"scan_fp32_wide_kernel<{sst.scan_qb},{sst.scan_wide}>" if sst.scan_wide
+                       else f"scan_fp32_kernel<{sst.scan_qb},4>"),
         }
         if bi == 0:
             launches = n1 - n0
@@ -433,13 +437,13 @@ def run_ours(args):
                         f"mixture, sigma={args.sigma}, unit rows, normalized=true), batch {args.batch}, k={k}",
             "rows": args.rows, "dims": args.dims, "batch": args.batch, "k": k,
             "parallelism": f"replicas{world}" if world > 1 else "single-gpu",
-            "l2": "inputs larger than L2 (base 3.07 GB per step vs 126 MB L2)",
+            "l2": f"inputs larger than L2 (base {args.rows * args.dims * 4 / 1e9:.2f} GB per step vs 126 MB L2)",
         },
         "e2e": {"value": e2e_q / (e2e_max_ms / 1e3), "unit": "queries/s",
                 "h2d_bytes_per_step": b * args.dims * 4, "d2h_bytes_per_step": b * k * 12 + b * 8},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{peak_kind} hbm_gbs",
-                     "kernel": "scan_fp32_kernel",
+                     "kernel": head["kernel"],
                      "bytes_per_launch": bytes_per_launch, "avg_launch_ms": head["scan_ms"]},
         "cpu_baseline": cpu,
         "clocks": clocks,
@@ -448,7 +452,7 @@ def run_ours(args):
         "ivf": ivf,
         "serving": serve,
         "batches": {str(bb): {"queries_per_s": r["queries_per_s"], "ms_per_step": r["ms_per_step"],
-                              "scan_ms": r["scan_ms"],
+                              "scan_ms": r["scan_ms"], "kernel": r["kernel"],
                               "hbm_gbs": (args.rows * args.dims * 4 + bb * args.dims * 4 + bb * k * 12)
                               / (r["scan_ms"] / 1e3) / 1e9}
                     for bb, r in results.items()},

@@ -114,6 +114,9 @@ typedef struct nndex_cuda_search_stats {
     uint32_t pass1_tile_stride;     /* first pass scanned every n-th 256-row tile (1 = all) */
     uint64_t ivf_rows_streamed;     /* IVF: rows read by the list scan (a list once per query group) */
     uint64_t ivf_rows_union;        /* IVF: rows in the union of the probed lists               */
+    uint32_t scan_qb;               /* FP32 scan: queries per CTA of its last launch            */
+    uint32_t scan_wide;             /* FP32 scan: 0 = 4-row × 8-query warps, 8 / 16 = consumer
+                                       warps of 16 rows × all queries (the wide consumer)       */
 } nndex_cuda_search_stats;
 
 /* IVF build statistics (approximate mode; zero when the index has no IVF). */

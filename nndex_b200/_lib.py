@@ -81,6 +81,8 @@ class SearchStats(C.Structure):
         ("pass1_tile_stride", C.c_uint32),
         ("ivf_rows_streamed", C.c_uint64),
         ("ivf_rows_union", C.c_uint64),
+        ("scan_qb", C.c_uint32),
+        ("scan_wide", C.c_uint32),
     ]
 
 

@@ -76,6 +76,30 @@ NNDEX_DEVICE_INLINE bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
+// try_wait that may suspend the thread for up to `ns` nanoseconds while the phase is incomplete
+// (a producer that mostly waits then takes no issue slots from the warps it shares a scheduler with).
+NNDEX_DEVICE_INLINE bool mbar_try_wait_suspend(uint64_t* bar, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait with suspension: as mbar_wait_bounded, each try suspending for up to `ns`.
+NNDEX_DEVICE_INLINE bool mbar_wait_bounded_suspend(uint64_t* bar, uint32_t parity, long long budget, uint32_t ns) {
+    if (mbar_try_wait_suspend(bar, parity, ns)) return true;
+    long long start = clock64();
+    while (!mbar_try_wait_suspend(bar, parity, ns)) {
+        if (clock64() - start > budget) return false;
+    }
+    return true;
+}
+
 // Bounded wait: spins on try_wait until the phase with `parity` completes or `budget` clock
 // cycles pass. Returns false on timeout (the caller records kStatusTimeout and drains).
 NNDEX_DEVICE_INLINE bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long budget) {

@@ -270,6 +270,8 @@ int CudaIndex::enqueue_exact_fp32(const float* d_queries, uint32_t nq, uint32_t 
     stats.kernel_launches += 2;
     stats.path = 1;
     stats.rows_scanned += rows * nq;
+    stats.scan_qb = plan.qb;
+    stats.scan_wide = plan.wide;
     return NNDEX_OK;
 }
 

@@ -42,6 +42,7 @@ struct ScanPlan {
     uint32_t cap = 512;        // candidate buffer capacity per query
     uint32_t stages = 4;
     size_t smem_bytes = 0;
+    uint32_t wide = 0;         // 0, or the consumer warps of the wide scan (8 or 16)
 };
 
 struct ScanArgs {

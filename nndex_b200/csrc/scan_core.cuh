@@ -177,19 +177,198 @@ struct ScanConsumer {
     }
 };
 
+// The wide consumer (K2 at 8 or 16 queries per CTA): each of the W consumer warps owns 16 tile rows
+// and ALL of the CTA's QB queries, so every row value is read from shared memory once. Lane
+// (rg = lane / 8, dg = lane % 8) keeps rows 16w + rg + 4i (i < 4) × QB queries of partial sums for
+// chunk position dg (16 bytes) of every slab: a row load is one 128-byte row per 8 lanes
+// (conflict-free under the 128-byte swizzle) and a query load is 8 consecutive chunks, one full
+// wavefront broadcast to the 4 row groups. The next slab's rows are loaded before the current one
+// is multiplied, and the queries are loaded four at a time between their FMAs, so shared-memory
+// traffic is spread over the FMA stream instead of bursting after each barrier.
+//
+// The FMA order per (row, query) is ScanConsumer's: per chunk position the slab's 4 products in
+// order, slab after slab, then ((p0 + p1) + (p2 + p3)) + ((p4 + p5) + (p6 + p7)) over the 8
+// positions. The tile's scores are completed by a reduce-scatter butterfly over the 8 lanes of a
+// row group (xor 1, 2, 4, halving the values a lane keeps at each step): the same addition tree,
+// and IEEE addition commutes, so every score has ScanConsumer's bits. Each lane ends with one row
+// × QB/2 queries and inserts those; no shared-memory exchange is needed.
+template <int QB, int W, int ST>
+struct ScanConsumerWide {
+    static_assert(QB == 8 || QB == 16, "the wide consumer takes 8 or 16 queries");
+    static constexpr int kTileRows = 16 * W;
+    static constexpr uint32_t kStageBytes = kTileRows * 128;
+    static constexpr int kHalf = QB / 2;
+    // Queries in shared memory slab-major: [dq / 32][QB][32] floats, so a slab's query chunks sit
+    // at fixed offsets (b · 128 bytes) from the slab's base.
+    static constexpr uint32_t kQSlabBytes = QB * 128;
+
+    uint32_t lane, rg, dg, warp;
+    uint32_t x_base0, x_base1;  // row chunk address (stage 0) for rows i = 0, 2 and i = 1, 3
+    const float4* q_base;       // this lane's chunk of query 0 in slab 0
+
+    NNDEX_DEVICE_INLINE ScanConsumerWide(uint32_t warp_, uint32_t lane_, const uint8_t* stage_base, const float* q_s)
+        : lane(lane_), warp(warp_) {
+        rg = lane >> 3;
+        dg = lane & 7u;
+        // row 16w + rg + 4i: (row % 8) = rg + 4·(i % 2), the 128-byte swizzle's chunk xor
+        const uint32_t row0 = warp * 16 + rg;
+        x_base0 = smem_u32(stage_base) + row0 * 128 + ((dg ^ rg) * 16);
+        x_base1 = smem_u32(stage_base) + (row0 + 4) * 128 + ((dg ^ (rg + 4)) * 16);
+        q_base = reinterpret_cast<const float4*>(q_s) + dg;
+    }
+
+    NNDEX_DEVICE_INLINE void load_rows(float4 (&x)[4], uint32_t it) const {
+        const uint32_t off = (it % ST) * kStageBytes;
+        x[0] = lds128(x_base0 + off);
+        x[1] = lds128(x_base1 + off);
+        x[2] = lds128(x_base0 + off + 8 * 128);
+        x[3] = lds128(x_base1 + off + 8 * 128);
+    }
+
+    NNDEX_DEVICE_INLINE void wait_full(uint64_t* full_bar, uint32_t it, volatile uint32_t* abort_flag,
+                                       uint32_t* status) const {
+        const uint32_t s = it % ST, parity = (it / ST) & 1u;
+        if (mbar_try_wait(&full_bar[s], parity)) return;
+        if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], parity, kWaitBudgetCycles)) {
+            *abort_flag = 1;
+            record_status(status, kStatusTimeout);
+        }
+    }
+
+    // acc += the slab's products of rows x and the queries at q (chunk dg), in component order.
+    // The queries are written once before the consumers start: plain loads, which the compiler
+    // may schedule among the FMAs. Four queries at a time: 16 independent FMAs separate the
+    // dependent ones of an accumulator.
+    NNDEX_DEVICE_INLINE static void fma_slab(float (&acc)[4][QB], const float4 (&x)[4], const float4* q) {
+#pragma unroll
+        for (int b0 = 0; b0 < QB; b0 += 4) {
+            float4 qv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) qv[j] = q[(b0 + j) * 8];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][b0 + j] = fmaf(x[i].x, qv[j].x, acc[i][b0 + j]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][b0 + j] = fmaf(x[i].y, qv[j].y, acc[i][b0 + j]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][b0 + j] = fmaf(x[i].z, qv[j].z, acc[i][b0 + j]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][b0 + j] = fmaf(x[i].w, qv[j].w, acc[i][b0 + j]);
+        }
+    }
+
+    NNDEX_DEVICE_INLINE void release(uint64_t* empty_bar, uint32_t it) const {
+        // the slab's row values were used by the FMAs before this (their loads have completed)
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty_bar[it % ST]);
+    }
+
+    // One tile: nbox slabs from the ring (starting at ring position `it`, advanced), each released
+    // to the producer once its row values have been used. The next slab's rows are loaded before
+    // the current slab is multiplied (two register sets, alternating).
+    NNDEX_DEVICE_INLINE void accumulate(float (&acc)[4][QB], uint32_t nbox, uint32_t& it, uint64_t* full_bar,
+                                        uint64_t* empty_bar, volatile uint32_t* abort_flag, uint32_t* status) const {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int b = 0; b < QB; ++b) acc[i][b] = 0.0f;
+        float4 xa[4], xb[4];
+        wait_full(full_bar, it, abort_flag, status);
+        load_rows(xa, it);
+        const float4* q = q_base;
+#pragma unroll 1
+        for (uint32_t bx = 0; bx < nbox; bx += 2) {
+            if (bx + 1 < nbox) {
+                wait_full(full_bar, it + 1, abort_flag, status);
+                load_rows(xb, it + 1);
+            }
+            fma_slab(acc, xa, q);
+            release(empty_bar, it);
+            ++it;
+            q += kQSlabBytes / 16;
+            if (bx + 1 >= nbox) break;
+            if (bx + 2 < nbox) {
+                wait_full(full_bar, it + 1, abort_flag, status);
+                load_rows(xa, it + 1);
+            }
+            fma_slab(acc, xb, q);
+            release(empty_bar, it);
+            ++it;
+            q += kQSlabBytes / 16;
+        }
+    }
+
+    // One butterfly step over lanes xor m: a lane whose bit m is clear keeps the first half of its
+    // values and receives the partner's share of them; the other lane keeps the second half.
+    template <int N>
+    NNDEX_DEVICE_INLINE static void halve(const float (&v)[N], float (&out)[N / 2], uint32_t m, bool upper) {
+#pragma unroll
+        for (int j = 0; j < N / 2; ++j) {
+            const float send = upper ? v[j] : v[j + N / 2];
+            const float keep = upper ? v[j + N / 2] : v[j];
+            out[j] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+        }
+    }
+
+    // Completes the tile's scores and appends every key that beats its query's running k-th key.
+    // row_key(r) maps a tile row to the row index the key carries. Ends with the consumers
+    // synchronised.
+    template <class RowKey>
+    NNDEX_DEVICE_INLINE void insert(const float (&acc)[4][QB], uint64_t tile_row0, uint64_t row_end, uint32_t nqg,
+                                    RowKey row_key, const uint64_t* thr, uint32_t* cnt, uint64_t* cand, uint32_t cap,
+                                    uint32_t* status) const {
+        float v4[4 * QB];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int b = 0; b < QB; ++b) v4[i * QB + b] = acc[i][b];
+        float v2[2 * QB], v1[QB], v0[kHalf];
+        halve<4 * QB>(v4, v2, 1, (dg & 1u) != 0);   // keeps rows {0,1} or {2,3}
+        halve<2 * QB>(v2, v1, 2, (dg & 2u) != 0);   // keeps one row of those two
+        halve<QB>(v1, v0, 4, (dg & 4u) != 0);       // keeps queries [0, QB/2) or [QB/2, QB)
+        const uint32_t i_l = 2 * (dg & 1u) + ((dg >> 1) & 1u);
+        const uint64_t r = tile_row0 + warp * 16 + rg + 4 * i_l;
+        const uint32_t b0 = kHalf * (dg >> 2);
+        if (r < row_end) {
+            const uint32_t rk = row_key(r);
+#pragma unroll
+            for (int t = 0; t < kHalf; ++t) {
+                const uint32_t bq = b0 + t;
+                if (bq < nqg) {
+                    const uint64_t key = make_key(v0[t], rk);
+                    if (key > thr[bq]) {
+                        const uint32_t pos = atomicAdd(&cnt[bq], 1u);
+                        if (pos < cap)
+                            cand[static_cast<size_t>(bq) * cap + pos] = key;
+                        else
+                            record_status(status, kStatusOverflow);
+                    }
+                }
+            }
+        }
+        named_bar_sync(1, W * 32);
+    }
+};
+
 // When a query's buffer could overflow on the next tile (or, after the last tile, holds more than
 // k), one warp radix-selects its exact k best, compacts, and raises its threshold. Called by every
 // consumer thread after insert(); ends synchronised when it did any work.
-template <int QB, int NCW>
-NNDEX_DEVICE_INLINE void scan_flush(bool last, uint32_t nqg, uint32_t k, uint32_t cap, uint32_t warp, uint32_t lane,
-                                    uint32_t* cnt, uint64_t* thr, uint64_t* cand, uint32_t* hist) {
-    using S = ScanShape<QB, NCW>;
+template <int QB, int kConsumers, int kTileRows>
+NNDEX_DEVICE_INLINE void scan_flush_g(bool last, uint32_t nqg, uint32_t k, uint32_t cap, uint32_t warp,
+                                      uint32_t lane, uint32_t* cnt, uint64_t* thr, uint64_t* cand, uint32_t* hist) {
     bool need = false;
 #pragma unroll
     for (int b = 0; b < QB; ++b)
-        if (static_cast<uint32_t>(b) < nqg) need |= last ? (cnt[b] > k) : (cnt[b] + S::kTileRows > cap);
+        if (static_cast<uint32_t>(b) < nqg) need |= last ? (cnt[b] > k) : (cnt[b] + kTileRows > cap);
     if (!need) return;
-    for (uint32_t b = warp; b < nqg; b += S::kConsumers) {
+    for (uint32_t b = warp; b < nqg; b += kConsumers) {
         const uint32_t n = cnt[b] < cap ? cnt[b] : cap;
         if (n > k) {
             uint64_t* buf = cand + static_cast<size_t>(b) * cap;
@@ -201,7 +380,14 @@ NNDEX_DEVICE_INLINE void scan_flush(bool last, uint32_t nqg, uint32_t k, uint32_
             }
         }
     }
-    named_bar_sync(1, S::kConsumers * 32);
+    named_bar_sync(1, kConsumers * 32);
+}
+
+template <int QB, int NCW>
+NNDEX_DEVICE_INLINE void scan_flush(bool last, uint32_t nqg, uint32_t k, uint32_t cap, uint32_t warp, uint32_t lane,
+                                    uint32_t* cnt, uint64_t* thr, uint64_t* cand, uint32_t* hist) {
+    using S = ScanShape<QB, NCW>;
+    scan_flush_g<QB, S::kConsumers, S::kTileRows>(last, nqg, k, cap, warp, lane, cnt, thr, cand, hist);
 }
 
 }  // namespace nndex

@@ -150,6 +150,120 @@ __global__ void __launch_bounds__(ScanShape<QB, NCW>::kThreads, 1)
     }
 }
 
+// The same scan with the wide consumer (scan_core.cuh ScanConsumerWide): W consumer warps of 16
+// rows × all QB (8 or 16) queries, a tile of 16·W rows arriving as 128-row TMA boxes per slab.
+template <int QB, int W, int ST>
+__global__ void __launch_bounds__((W + 1) * 32, 1)
+    scan_fp32_wide_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restrict__ queries, uint32_t nq,
+                          uint32_t dq, uint64_t rows, uint32_t k, uint32_t cap,
+                          const uint32_t* __restrict__ row_map, uint64_t* __restrict__ ws_keys,
+                          uint32_t* __restrict__ status) {
+    using Consumer = ScanConsumerWide<QB, W, ST>;
+    constexpr int TR = Consumer::kTileRows;
+    constexpr uint32_t kStageBytes = Consumer::kStageBytes;
+    constexpr uint32_t kBoxes = TR / 128;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = align_1024(smem_raw);
+    uint8_t* stage_base = smem;
+    float* q_s = reinterpret_cast<float*>(stage_base + static_cast<size_t>(ST) * kStageBytes);
+    uint64_t* cand = reinterpret_cast<uint64_t*>(q_s + static_cast<size_t>(QB) * dq);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(cand + static_cast<size_t>(QB) * cap);
+    uint64_t* thr = reinterpret_cast<uint64_t*>(hist + W * 256);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(thr + QB);
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(cnt + QB);
+    uint64_t* empty_bar = full_bar + ST;
+    volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(empty_bar + ST);
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t warp = tid >> 5;
+    const uint32_t lane = tid & 31u;
+    const uint32_t G = gridDim.x;
+    const uint32_t c = blockIdx.x;
+    const uint32_t q0 = blockIdx.y * QB;
+    const uint32_t nqg = (nq - q0) < static_cast<uint32_t>(QB) ? (nq - q0) : static_cast<uint32_t>(QB);
+    const uint64_t row_begin = rows * c / G;
+    const uint64_t row_end = rows * (c + 1) / G;
+    const uint32_t ntiles = static_cast<uint32_t>((row_end - row_begin + TR - 1) / TR);
+    const uint32_t nbox = dq / 32;
+
+    if (tid == 0) {
+        for (uint32_t s = 0; s < ST; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], W);
+        }
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    // queries slab-major: [dq / 32][QB][32]
+    for (uint32_t i = tid; i < static_cast<uint32_t>(QB) * dq; i += blockDim.x) {
+        const uint32_t b = i / dq, d = i - b * dq;
+        q_s[((d >> 5) * QB + b) * 32 + (d & 31u)] = b < nqg ? queries[static_cast<size_t>(q0 + b) * dq + d] : 0.0f;
+    }
+    if (tid < static_cast<uint32_t>(QB)) {
+        cnt[tid] = 0;
+        thr[tid] = 0ull;
+    }
+    __syncthreads();
+
+    if (warp == W) {
+        // ---------------- producer ----------------
+        if (lane == 0) {
+            tma_prefetch_desc(&tmap);
+            const uint64_t policy = l2_policy_evict_first();
+            uint32_t it = 0;
+            bool stop = false;
+            for (uint32_t t = 0; t < ntiles && !stop; ++t) {
+                const int32_t y = static_cast<int32_t>(row_begin + static_cast<uint64_t>(t) * TR);
+                for (uint32_t bx = 0; bx < nbox; ++bx) {
+                    const uint32_t s = it % ST, u = it / ST;
+                    if (u > 0 && !mbar_wait_bounded_suspend(&empty_bar[s], (u - 1) & 1u, kWaitBudgetCycles, 20000)) {
+                        *abort_flag = 1;
+                        record_status(status, kStatusTimeout);
+                        stop = true;
+                        break;
+                    }
+                    if (*abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&full_bar[s], kStageBytes);
+#pragma unroll
+                    for (uint32_t h = 0; h < kBoxes; ++h)
+                        tma_load_2d_hint(stage_base + static_cast<size_t>(s) * kStageBytes + h * 128 * 128, &tmap,
+                                         &full_bar[s], static_cast<int32_t>(bx * 32), y + static_cast<int32_t>(h * 128),
+                                         policy);
+                    ++it;
+                }
+            }
+            // Drain: every issued copy has landed before the CTA may exit.
+            const uint32_t used = it < ST ? it : ST;
+            for (uint32_t s = 0; s < used; ++s) {
+                const uint32_t uses = (it - s + ST - 1) / ST;
+                if (!mbar_wait_bounded(&full_bar[s], (uses - 1) & 1u, kWaitBudgetCycles))
+                    record_status(status, kStatusTimeout);
+            }
+        }
+        return;
+    }
+
+    // ---------------- consumers ----------------
+    const Consumer con(warp, lane, stage_base, q_s);
+    auto row_key = [&](uint64_t r) { return row_map ? row_map[r] : static_cast<uint32_t>(r); };
+    float acc[4][QB];
+    uint32_t it = 0;
+    for (uint32_t t = 0; t < ntiles; ++t) {
+        con.accumulate(acc, nbox, it, full_bar, empty_bar, abort_flag, status);
+        con.insert(acc, row_begin + static_cast<uint64_t>(t) * TR, row_end, nqg, row_key, thr, cnt, cand, cap, status);
+        scan_flush_g<QB, W, TR>(t + 1 == ntiles, nqg, k, cap, warp, lane, cnt, thr, cand, hist);
+    }
+    for (uint32_t b = warp; b < nqg; b += W) {
+        const uint32_t n = cnt[b] < k ? cnt[b] : k;
+        uint64_t* dst = ws_keys + (static_cast<size_t>(q0 + b) * G + c) * k;
+        const uint64_t* src = cand + static_cast<size_t>(b) * cap;
+        for (uint32_t j = lane; j < k; j += 32) dst[j] = j < n ? src[j] : 0ull;
+    }
+}
+
 // ------------------------------------------------------------------------------------------
 // Cross-CTA merge: one block per query selects the k best of `per_query` candidate keys and
 // writes them sorted (similarity desc, index asc), padding the unused slots with (0, 0.0f)
@@ -261,11 +375,54 @@ template <int QB>
 cudaError_t launch_qb(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
     return p.stages >= 4 ? launch_qb_st<QB, 4>(a, p, stream) : launch_qb_st<QB, 2>(a, p, stream);
 }
+
+size_t wide_smem_bytes(uint32_t qb, uint32_t w, uint32_t dq, uint32_t cap, uint32_t stages) {
+    size_t b = 1024;
+    b += static_cast<size_t>(stages) * w * 16 * 128;
+    b += static_cast<size_t>(qb) * dq * 4;
+    b += static_cast<size_t>(qb) * cap * 8;
+    b += static_cast<size_t>(w) * 256 * 4;
+    b += qb * 8 + qb * 4;
+    b += static_cast<size_t>(stages) * 16 + 16;
+    return b;
+}
+
+template <int QB, int W, int ST>
+cudaError_t launch_wide_st(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
+    auto kern = scan_fp32_wide_kernel<QB, W, ST>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(p.smem_bytes));
+    if (e != cudaSuccess) return e;
+    dim3 grid(p.ctas_per_group, p.groups);
+    kern<<<grid, (W + 1) * 32, p.smem_bytes, stream>>>(*a.tmap, a.queries, a.nq, a.dq, a.rows, a.k, p.cap, a.row_map,
+                                                       a.ws_keys, a.status);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <int QB>
+cudaError_t launch_wide(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
+    if (p.wide == 16) {
+        switch (p.stages) {
+            case 2: return launch_wide_st<QB, 16, 2>(a, p, stream);
+            case 3: return launch_wide_st<QB, 16, 3>(a, p, stream);
+            default: return launch_wide_st<QB, 16, 4>(a, p, stream);
+        }
+    }
+    switch (p.stages) {
+        case 2: return launch_wide_st<QB, 8, 2>(a, p, stream);
+        case 3: return launch_wide_st<QB, 8, 3>(a, p, stream);
+        case 6: return launch_wide_st<QB, 8, 6>(a, p, stream);
+        case 8: return launch_wide_st<QB, 8, 8>(a, p, stream);
+        default: return launch_wide_st<QB, 8, 4>(a, p, stream);
+    }
+}
 }  // namespace
 
 // Tile-shape overrides for the autotuner and for measurement sweeps (0 = default):
 //   NNDEX_SCAN_STAGES   ring depth (2 or 4)        NNDEX_SCAN_QB   max queries per CTA (1..16)
 //   NNDEX_SCAN_CTAS     CTAs per query group      NNDEX_SCAN_CAP  candidate slots beyond k
+//   NNDEX_SCAN_WIDE     wide consumer warps at 8 / 16 queries per CTA: 8 (default) or 16; 1 = off
 static uint32_t env_u32(const char* name) {
     const char* v = getenv(name);
     return v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
@@ -293,6 +450,33 @@ bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t s
         if (qb == 1) return false;
         qb >>= 1;
     }
+    // 8 or 16 queries per CTA: the wide consumer (16 rows × all queries per warp) when it fits.
+    static const uint32_t o_wide = env_u32("NNDEX_SCAN_WIDE");
+    plan.wide = 0;
+    if ((plan.qb == 8 || plan.qb == 16) && o_wide != 1) {
+        // 16 consumer warps at 8 queries (96 registers, 4 warps per scheduler); 8 at 16 queries (the
+        // 64 accumulators need more than the 96 registers 17 warps leave)
+        const uint32_t w = o_wide ? (o_wide == 16 ? 16 : 8) : (plan.qb == 8 ? 16 : 8);
+        const uint32_t tr = 16 * w;
+        const uint32_t wcap = ((k + (o_cap ? (o_cap > tr ? o_cap : tr + 32) : 2 * tr)) + 31) / 32 * 32;
+        // ring depths with a kernel instance: 16 warps {4, 3, 2}, 8 warps {6, 4, 3, 2}
+        static const uint32_t kDepth16[] = {4, 3, 2, 0}, kDepth8[] = {8, 6, 4, 3, 2, 0};
+        const uint32_t* depths = w == 16 ? kDepth16 : kDepth8;
+        uint32_t st = 0;
+        for (const uint32_t* d = depths; *d; ++d) {
+            if (o_stages && *d > o_stages) continue;
+            if (wide_smem_bytes(plan.qb, w, dq, wcap, *d) <= smem_limit) {
+                st = *d;
+                break;
+            }
+        }
+        if (st >= 2) {
+            plan.wide = w;
+            plan.cap = wcap;
+            plan.stages = st;
+            plan.smem_bytes = wide_smem_bytes(plan.qb, w, dq, wcap, st);
+        }
+    }
     plan.groups = (nq + plan.qb - 1) / plan.qb;
     uint32_t per = static_cast<uint32_t>(sm_count) / plan.groups;
     if (per < 1) per = 1;
@@ -302,6 +486,7 @@ bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t s
 }
 
 cudaError_t launch_scan_fp32(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
+    if (p.wide) return p.qb == 16 ? launch_wide<16>(a, p, stream) : launch_wide<8>(a, p, stream);
     switch (p.qb) {
         case 1: return launch_qb<1>(a, p, stream);
         case 2: return launch_qb<2>(a, p, stream);
