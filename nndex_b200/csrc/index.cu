@@ -244,6 +244,8 @@ int CudaIndex::enqueue_exact_fp32(const float* d_queries, uint32_t nq, uint32_t 
     if (st) return st;
     ScanArgs a;
     a.tmap = &tmap_f32;
+    a.tmap_tile = &tmap_f32_176;
+    a.tmap_112 = &tmap_f32_112;
     a.queries = d_queries;
     a.nq = nq;
     a.dq = static_cast<uint32_t>(ds);
@@ -927,7 +929,11 @@ int index_finish(CudaIndex* ix) {
         std::memcpy(&ix->eps_fp8, &hm[1], 4);
     }
     if (!encode_tmap_2d(&ix->tmap_f32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ix->d_base, ix->ds, ix->rows_alloc,
-                        ix->ds * sizeof(float), 32, 128, CU_TENSOR_MAP_SWIZZLE_128B))
+                        ix->ds * sizeof(float), 32, 128, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !encode_tmap_2d(&ix->tmap_f32_176, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ix->d_base, ix->ds, ix->rows_alloc,
+                        ix->ds * sizeof(float), 32, 176, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !encode_tmap_2d(&ix->tmap_f32_112, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ix->d_base, ix->ds, ix->rows_alloc,
+                        ix->ds * sizeof(float), 32, 112, CU_TENSOR_MAP_SWIZZLE_128B))
         return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed"));
     if (ix->d_base_bf16 &&
         !encode_tmap_2d(&ix->tmap_bf16, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ix->d_base_bf16, ix->kb16, ix->rows_alloc,
@@ -1024,6 +1030,8 @@ int make_view(const CudaIndex& src, CudaIndex** out) {
     v->opts = src.opts;
     v->d_base = src.d_base;
     v->tmap_f32 = src.tmap_f32;
+    v->tmap_f32_176 = src.tmap_f32_176;
+    v->tmap_f32_112 = src.tmap_f32_112;
     v->precision = src.precision;
     v->kb16 = src.kb16;
     v->kf8 = src.kf8;

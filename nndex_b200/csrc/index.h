@@ -47,6 +47,8 @@ struct CudaIndex {
 
     float* d_base = nullptr;  // rows_alloc × ds FP32, normalised, zero padded
     CUtensorMap tmap_f32{};
+    CUtensorMap tmap_f32_176{};  // box {32 floats, 176 rows}: the 11-warp wide FP32 scan's tiles
+    CUtensorMap tmap_f32_112{};  // box {32 floats, 112 rows}: the 7-warp wide FP32 scan's tiles
 
     // Low-precision scoring copies (NNDEX_FLAG_BF16 / NNDEX_FLAG_FP8), K3.
     uint32_t precision = NNDEX_PRECISION_AUTO;

@@ -47,6 +47,8 @@ struct ScanPlan {
 
 struct ScanArgs {
     const CUtensorMap* tmap = nullptr;  // base fp32 rows × dp, box {32, 128}, 128B swizzle
+    const CUtensorMap* tmap_tile = nullptr;  // the same rows, box {32, 176}: the 11-warp wide scan's tiles
+    const CUtensorMap* tmap_112 = nullptr;   // the same rows, box {32, 112}: the 7-warp wide scan's tiles
     const float* queries = nullptr;     // nq × dq normalised, zero padded
     uint32_t nq = 0;
     uint32_t dq = 0;                    // multiple of 32

@@ -104,6 +104,8 @@ int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, ui
     launch_prep_rows(p, s);
     ScanArgs a;
     a.tmap = &ix->tmap_f32;
+    a.tmap_tile = &ix->tmap_f32_176;
+    a.tmap_112 = &ix->tmap_f32_112;
     a.queries = d_qn;
     a.nq = static_cast<uint32_t>(nq);
     a.dq = static_cast<uint32_t>(ix->ds);

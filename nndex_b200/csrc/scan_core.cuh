@@ -192,6 +192,20 @@ struct ScanConsumer {
 // row group (xor 1, 2, 4, halving the values a lane keeps at each step): the same addition tree,
 // and IEEE addition commutes, so every score has ScanConsumer's bits. Each lane ends with one row
 // × QB/2 queries and inserts those; no shared-memory exchange is needed.
+// A position in a ring of ST stages: the stage and the parity of its current phase.
+template <int ST>
+struct RingPos {
+    uint32_t s = 0, phase = 0;
+    NNDEX_DEVICE_INLINE RingPos next() const {
+        RingPos n = *this;
+        if (++n.s == ST) {
+            n.s = 0;
+            n.phase ^= 1u;
+        }
+        return n;
+    }
+};
+
 template <int QB, int W, int ST>
 struct ScanConsumerWide {
     static_assert(QB == 8 || QB == 16, "the wide consumer takes 8 or 16 queries");
@@ -201,6 +215,7 @@ struct ScanConsumerWide {
     // Queries in shared memory slab-major: [dq / 32][QB][32] floats, so a slab's query chunks sit
     // at fixed offsets (b · 128 bytes) from the slab's base.
     static constexpr uint32_t kQSlabBytes = QB * 128;
+    NNDEX_DEVICE_INLINE static uint32_t q_slab_index(uint32_t b, uint32_t d) { return ((d >> 5) * QB + b) * 32 + (d & 31u); }
 
     uint32_t lane, rg, dg, warp;
     uint32_t x_base0, x_base1;  // row chunk address (stage 0) for rows i = 0, 2 and i = 1, 3
@@ -217,31 +232,31 @@ struct ScanConsumerWide {
         q_base = reinterpret_cast<const float4*>(q_s) + dg;
     }
 
-    NNDEX_DEVICE_INLINE void load_rows(float4 (&x)[4], uint32_t it) const {
-        const uint32_t off = (it % ST) * kStageBytes;
+    NNDEX_DEVICE_INLINE void load_rows(float4 (&x)[4], RingPos<ST> r) const {
+        const uint32_t off = r.s * kStageBytes;
         x[0] = lds128(x_base0 + off);
         x[1] = lds128(x_base1 + off);
         x[2] = lds128(x_base0 + off + 8 * 128);
         x[3] = lds128(x_base1 + off + 8 * 128);
     }
 
-    NNDEX_DEVICE_INLINE void wait_full(uint64_t* full_bar, uint32_t it, volatile uint32_t* abort_flag,
+    NNDEX_DEVICE_INLINE void wait_full(uint64_t* full_bar, RingPos<ST> r, volatile uint32_t* abort_flag,
                                        uint32_t* status) const {
-        const uint32_t s = it % ST, parity = (it / ST) & 1u;
-        if (mbar_try_wait(&full_bar[s], parity)) return;
-        if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], parity, kWaitBudgetCycles)) {
+        if (mbar_try_wait(&full_bar[r.s], r.phase)) return;
+        if (!*abort_flag && !mbar_wait_bounded(&full_bar[r.s], r.phase, kWaitBudgetCycles)) {
             *abort_flag = 1;
             record_status(status, kStatusTimeout);
         }
     }
 
-    // acc += the slab's products of rows x and the queries at q (chunk dg), in component order.
+    // acc += the products of rows x and queries [4·G0, 4·G1) at q (chunk dg), in component order.
     // The queries are written once before the consumers start: plain loads, which the compiler
     // may schedule among the FMAs. Four queries at a time: 16 independent FMAs separate the
     // dependent ones of an accumulator.
-    NNDEX_DEVICE_INLINE static void fma_slab(float (&acc)[4][QB], const float4 (&x)[4], const float4* q) {
+    template <int G0, int G1>
+    NNDEX_DEVICE_INLINE static void fma_groups(float (&acc)[4][QB], const float4 (&x)[4], const float4* q) {
 #pragma unroll
-        for (int b0 = 0; b0 < QB; b0 += 4) {
+        for (int b0 = 4 * G0; b0 < 4 * G1; b0 += 4) {
             float4 qv[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) qv[j] = q[(b0 + j) * 8];
@@ -264,43 +279,52 @@ struct ScanConsumerWide {
         }
     }
 
-    NNDEX_DEVICE_INLINE void release(uint64_t* empty_bar, uint32_t it) const {
-        // the slab's row values were used by the FMAs before this (their loads have completed)
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty_bar[it % ST]);
+    // Every lane arrives (the empty barriers count W·32 arrivals) once its FMAs have used the
+    // slab's row values, i.e. once its loads of the stage have completed.
+    NNDEX_DEVICE_INLINE void release(uint64_t* empty_bar, RingPos<ST> r) const { mbar_arrive(&empty_bar[r.s]); }
+
+    // One slab with the rows in x (ring position it) while the next slab's rows go to xn: the
+    // next stage's barrier is tested before the first query group's FMAs and the branch on it
+    // (and the row loads it guards) comes after them, so neither the test nor the loads' latency
+    // holds up the FMA stream.
+    NNDEX_DEVICE_INLINE void slab(float (&acc)[4][QB], const float4 (&x)[4], float4 (&xn)[4], bool more,
+                                  RingPos<ST> cur, const float4* q, uint64_t* full_bar, uint64_t* empty_bar,
+                                  volatile uint32_t* abort_flag, uint32_t* status) const {
+        const RingPos<ST> nxt = cur.next();
+        const bool ready = !more || mbar_try_wait(&full_bar[nxt.s], nxt.phase);
+        fma_groups<0, 1>(acc, x, q);
+        if (more) {
+            if (!ready && !*abort_flag &&
+                !mbar_wait_bounded_suspend(&full_bar[nxt.s], nxt.phase, kWaitBudgetCycles, 20000)) {
+                *abort_flag = 1;
+                record_status(status, kStatusTimeout);
+            }
+            load_rows(xn, nxt);
+        }
+        fma_groups<1, QB / 4>(acc, x, q);
+        release(empty_bar, cur);
     }
 
-    // One tile: nbox slabs from the ring (starting at ring position `it`, advanced), each released
-    // to the producer once its row values have been used. The next slab's rows are loaded before
-    // the current slab is multiplied (two register sets, alternating).
-    NNDEX_DEVICE_INLINE void accumulate(float (&acc)[4][QB], uint32_t nbox, uint32_t& it, uint64_t* full_bar,
+    // One tile: nbox slabs from the ring (starting at ring position `pos`, advanced), each released
+    // to the producer once its row values have been used (two register sets, alternating).
+    NNDEX_DEVICE_INLINE void accumulate(float (&acc)[4][QB], uint32_t nbox, RingPos<ST>& pos, uint64_t* full_bar,
                                         uint64_t* empty_bar, volatile uint32_t* abort_flag, uint32_t* status) const {
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int b = 0; b < QB; ++b) acc[i][b] = 0.0f;
         float4 xa[4], xb[4];
-        wait_full(full_bar, it, abort_flag, status);
-        load_rows(xa, it);
+        wait_full(full_bar, pos, abort_flag, status);
+        load_rows(xa, pos);
         const float4* q = q_base;
 #pragma unroll 1
         for (uint32_t bx = 0; bx < nbox; bx += 2) {
-            if (bx + 1 < nbox) {
-                wait_full(full_bar, it + 1, abort_flag, status);
-                load_rows(xb, it + 1);
-            }
-            fma_slab(acc, xa, q);
-            release(empty_bar, it);
-            ++it;
+            slab(acc, xa, xb, bx + 1 < nbox, pos, q, full_bar, empty_bar, abort_flag, status);
+            pos = pos.next();
             q += kQSlabBytes / 16;
             if (bx + 1 >= nbox) break;
-            if (bx + 2 < nbox) {
-                wait_full(full_bar, it + 1, abort_flag, status);
-                load_rows(xa, it + 1);
-            }
-            fma_slab(acc, xb, q);
-            release(empty_bar, it);
-            ++it;
+            slab(acc, xb, xa, bx + 2 < nbox, pos, q, full_bar, empty_bar, abort_flag, status);
+            pos = pos.next();
             q += kQSlabBytes / 16;
         }
     }

@@ -161,7 +161,9 @@ __global__ void __launch_bounds__((W + 1) * 32, 1)
     using Consumer = ScanConsumerWide<QB, W, ST>;
     constexpr int TR = Consumer::kTileRows;
     constexpr uint32_t kStageBytes = Consumer::kStageBytes;
-    constexpr uint32_t kBoxes = TR / 128;
+    // one box per 128 rows, or a single box of the whole tile (tensor map with box rows = TR)
+    constexpr uint32_t kBoxRows = (TR % 128 == 0) ? 128 : TR;
+    constexpr uint32_t kBoxes = TR / kBoxRows;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = align_1024(smem_raw);
     uint8_t* stage_base = smem;
@@ -189,15 +191,15 @@ __global__ void __launch_bounds__((W + 1) * 32, 1)
     if (tid == 0) {
         for (uint32_t s = 0; s < ST; ++s) {
             mbar_init(&full_bar[s], 1);
-            mbar_init(&empty_bar[s], W);
+            mbar_init(&empty_bar[s], W * 32);
         }
         *abort_flag = 0;
         fence_mbar_init();
     }
-    // queries slab-major: [dq / 32][QB][32]
+    // queries slab-major (ScanConsumerWide::q_slab_index)
     for (uint32_t i = tid; i < static_cast<uint32_t>(QB) * dq; i += blockDim.x) {
         const uint32_t b = i / dq, d = i - b * dq;
-        q_s[((d >> 5) * QB + b) * 32 + (d & 31u)] = b < nqg ? queries[static_cast<size_t>(q0 + b) * dq + d] : 0.0f;
+        q_s[Consumer::q_slab_index(b, d)] = b < nqg ? queries[static_cast<size_t>(q0 + b) * dq + d] : 0.0f;
     }
     if (tid < static_cast<uint32_t>(QB)) {
         cnt[tid] = 0;
@@ -229,9 +231,9 @@ __global__ void __launch_bounds__((W + 1) * 32, 1)
                     mbar_arrive_expect_tx(&full_bar[s], kStageBytes);
 #pragma unroll
                     for (uint32_t h = 0; h < kBoxes; ++h)
-                        tma_load_2d_hint(stage_base + static_cast<size_t>(s) * kStageBytes + h * 128 * 128, &tmap,
-                                         &full_bar[s], static_cast<int32_t>(bx * 32), y + static_cast<int32_t>(h * 128),
-                                         policy);
+                        tma_load_2d_hint(stage_base + static_cast<size_t>(s) * kStageBytes + h * kBoxRows * 128, &tmap,
+                                         &full_bar[s], static_cast<int32_t>(bx * 32),
+                                         y + static_cast<int32_t>(h * kBoxRows), policy);
                     ++it;
                 }
             }
@@ -250,9 +252,9 @@ __global__ void __launch_bounds__((W + 1) * 32, 1)
     const Consumer con(warp, lane, stage_base, q_s);
     auto row_key = [&](uint64_t r) { return row_map ? row_map[r] : static_cast<uint32_t>(r); };
     float acc[4][QB];
-    uint32_t it = 0;
+    RingPos<ST> pos;
     for (uint32_t t = 0; t < ntiles; ++t) {
-        con.accumulate(acc, nbox, it, full_bar, empty_bar, abort_flag, status);
+        con.accumulate(acc, nbox, pos, full_bar, empty_bar, abort_flag, status);
         con.insert(acc, row_begin + static_cast<uint64_t>(t) * TR, row_end, nqg, row_key, thr, cnt, cand, cap, status);
         scan_flush_g<QB, W, TR>(t + 1 == ntiles, nqg, k, cap, warp, lane, cnt, thr, cand, hist);
     }
@@ -393,8 +395,11 @@ cudaError_t launch_wide_st(const ScanArgs& a, const ScanPlan& p, cudaStream_t st
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(p.smem_bytes));
     if (e != cudaSuccess) return e;
+    // tiles of 16·W rows: 128-row boxes, or one box of the tile (a tensor map of that box height)
+    const CUtensorMap* tm = (16 * W) % 128 == 0 ? a.tmap : (W == 7 ? a.tmap_112 : a.tmap_tile);
+    if (!tm) return cudaErrorInvalidValue;
     dim3 grid(p.ctas_per_group, p.groups);
-    kern<<<grid, (W + 1) * 32, p.smem_bytes, stream>>>(*a.tmap, a.queries, a.nq, a.dq, a.rows, a.k, p.cap, a.row_map,
+    kern<<<grid, (W + 1) * 32, p.smem_bytes, stream>>>(*tm, a.queries, a.nq, a.dq, a.rows, a.k, p.cap, a.row_map,
                                                        a.ws_keys, a.status);
     count_launch();
     return cudaGetLastError();
@@ -402,6 +407,22 @@ cudaError_t launch_wide_st(const ScanArgs& a, const ScanPlan& p, cudaStream_t st
 
 template <int QB>
 cudaError_t launch_wide(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
+    if (p.wide == 11) {
+        switch (p.stages) {
+            case 2: return launch_wide_st<QB, 11, 2>(a, p, stream);
+            case 3: return launch_wide_st<QB, 11, 3>(a, p, stream);
+            case 5: return launch_wide_st<QB, 11, 5>(a, p, stream);
+            default: return launch_wide_st<QB, 11, 4>(a, p, stream);
+        }
+    }
+    if (p.wide == 7) {
+        switch (p.stages) {
+            case 2: return launch_wide_st<QB, 7, 2>(a, p, stream);
+            case 4: return launch_wide_st<QB, 7, 4>(a, p, stream);
+            case 6: return launch_wide_st<QB, 7, 6>(a, p, stream);
+            default: return launch_wide_st<QB, 7, 8>(a, p, stream);
+        }
+    }
     if (p.wide == 16) {
         switch (p.stages) {
             case 2: return launch_wide_st<QB, 16, 2>(a, p, stream);
@@ -422,7 +443,8 @@ cudaError_t launch_wide(const ScanArgs& a, const ScanPlan& p, cudaStream_t strea
 // Tile-shape overrides for the autotuner and for measurement sweeps (0 = default):
 //   NNDEX_SCAN_STAGES   ring depth (2 or 4)        NNDEX_SCAN_QB   max queries per CTA (1..16)
 //   NNDEX_SCAN_CTAS     CTAs per query group      NNDEX_SCAN_CAP  candidate slots beyond k
-//   NNDEX_SCAN_WIDE     wide consumer warps at 8 / 16 queries per CTA: 8 (default) or 16; 1 = off
+//   NNDEX_SCAN_WIDE     wide consumer warps at 8 / 16 queries per CTA: 7, 8, 11 or 16 (default 16
+//                       at 8 queries, 11 at 16); 1 = the 4-row × 8-query consumer instead
 static uint32_t env_u32(const char* name) {
     const char* v = getenv(name);
     return v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
@@ -454,14 +476,17 @@ bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t s
     static const uint32_t o_wide = env_u32("NNDEX_SCAN_WIDE");
     plan.wide = 0;
     if ((plan.qb == 8 || plan.qb == 16) && o_wide != 1) {
-        // 16 consumer warps at 8 queries (96 registers, 4 warps per scheduler); 8 at 16 queries (the
-        // 64 accumulators need more than the 96 registers 17 warps leave)
-        const uint32_t w = o_wide ? (o_wide == 16 ? 16 : 8) : (plan.qb == 8 ? 16 : 8);
+        // 16 consumer warps at 8 queries (96 registers, 4 warps per scheduler); 11 at 16 queries (3
+        // per scheduler at up to 168 registers: the 64 accumulators need more than the 96 registers
+        // that 17 warps leave)
+        const uint32_t w = o_wide ? (o_wide == 16 || o_wide == 11 || o_wide == 7 ? o_wide : 8)
+                                  : (plan.qb == 8 ? 16 : 11);
         const uint32_t tr = 16 * w;
         const uint32_t wcap = ((k + (o_cap ? (o_cap > tr ? o_cap : tr + 32) : 2 * tr)) + 31) / 32 * 32;
         // ring depths with a kernel instance: 16 warps {4, 3, 2}, 8 warps {6, 4, 3, 2}
-        static const uint32_t kDepth16[] = {4, 3, 2, 0}, kDepth8[] = {8, 6, 4, 3, 2, 0};
-        const uint32_t* depths = w == 16 ? kDepth16 : kDepth8;
+        static const uint32_t kDepth16[] = {4, 3, 2, 0}, kDepth11[] = {5, 4, 3, 2, 0},
+                              kDepth8[] = {8, 6, 4, 3, 2, 0}, kDepth7[] = {8, 6, 4, 2, 0};
+        const uint32_t* depths = w == 16 ? kDepth16 : w == 11 ? kDepth11 : w == 7 ? kDepth7 : kDepth8;
         uint32_t st = 0;
         for (const uint32_t* d = depths; *d; ++d) {
             if (o_stages && *d > o_stages) continue;
