@@ -115,8 +115,11 @@ typedef struct nndex_cuda_search_stats {
     uint64_t ivf_rows_streamed;     /* IVF: rows read by the list scan (a list once per query group) */
     uint64_t ivf_rows_union;        /* IVF: rows in the union of the probed lists               */
     uint32_t scan_qb;               /* FP32 scan: queries per CTA of its last launch            */
-    uint32_t scan_wide;             /* FP32 scan: 0 = 4-row × 8-query warps, 8 / 16 = consumer
-                                       warps of 16 rows × all queries (the wide consumer)       */
+    uint32_t scan_wide;             /* FP32 scan: 0 = 4-row × 8-query warps, 7 / 8 / 11 / 16 =
+                                       consumer warps of 16 rows × all queries (wide consumer)  */
+    uint32_t graph;                 /* host-buffer search: 0 = direct launches, 1 = captured as a
+                                       CUDA graph by this call, 2 = a cached graph replayed      */
+    uint32_t reserved;
 } nndex_cuda_search_stats;
 
 /* IVF build statistics (approximate mode; zero when the index has no IVF). */
@@ -327,6 +330,14 @@ NNDEX_API int nndex_cuda_ivf_restore(nndex_cuda_index* index, uint64_t nlist, co
 /* 64-bit fingerprint of the stored (validated, normalised, padded) rows: Σ over positions i of
  * splitmix64(i · 2^32 + bits of value i), mod 2^64. Equal matrices give equal values on any GPU. */
 NNDEX_API int nndex_cuda_base_checksum(nndex_cuda_index* index, uint64_t* checksum);
+
+/* CUDA graphs for nndex_cuda_search / nndex_cuda_search_batch (on by default): the per-batch
+ * sequence of an exact FP32 or IVF list-scan batch (status resets, query upload, prep, scan, merge,
+ * result download) is captured the second time a (path, batch size, k) shape comes in a row and
+ * replayed as one launch afterwards; results are identical either way. Any reallocation of a
+ * scratch buffer, nndex_cuda_set_precision, nndex_cuda_set_nprobe or nndex_cuda_ivf_restore drops
+ * the cached graphs. enable = 0 turns capture off (and drops them). */
+NNDEX_API int nndex_cuda_set_graphs(nndex_cuda_index* index, int enable);
 
 /* Lists probed per query by later approx searches (0 = choose_nprobe, src/approx.rs:318-336);
  * no counterpart in the reference, whose nprobe is always the policy's. */

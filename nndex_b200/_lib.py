@@ -83,6 +83,8 @@ class SearchStats(C.Structure):
         ("ivf_rows_union", C.c_uint64),
         ("scan_qb", C.c_uint32),
         ("scan_wide", C.c_uint32),
+        ("graph", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 
@@ -173,6 +175,7 @@ SIGNATURES = {
     "nndex_cuda_ivf_layout": (_i32, [_vp, C.POINTER(_u64), _vp, _vp, _vp, _vp]),
     "nndex_cuda_ivf_stats_get": (_i32, [_vp, C.POINTER(IvfStats)]),
     "nndex_cuda_set_nprobe": (_i32, [_vp, _u32]),
+    "nndex_cuda_set_graphs": (_i32, [_vp, _i32]),
     "nndex_cuda_ivf_restore": (_i32, [_vp, _u64, _vp, _vp, _vp, _vp]),
     "nndex_cuda_base_checksum": (_i32, [_vp, C.POINTER(_u64)]),
     "nndex_cuda_server_start": (_i32, [_vp, C.POINTER(ServerOpts), C.POINTER(_vp)]),

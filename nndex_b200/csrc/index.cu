@@ -25,7 +25,11 @@
 namespace nndex {
 
 static std::atomic<uint64_t> g_launches{0};
+static std::atomic<uint64_t> g_alloc_epoch{0};
+uint64_t alloc_epoch() { return g_alloc_epoch.load(std::memory_order_acquire); }
+void bump_alloc_epoch() { g_alloc_epoch.fetch_add(1, std::memory_order_acq_rel); }
 void count_launch(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t kernel_launches_total() { return g_launches.load(std::memory_order_relaxed); }
 
 static thread_local std::string t_error;
 
@@ -107,6 +111,7 @@ bool encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, uint32_t elem_b
 template <class T>
 static int grow_device(T*& p, size_t& cap, size_t n, const char* what) {
     if (n <= cap && p) return NNDEX_OK;
+    bump_alloc_epoch();
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
@@ -121,6 +126,7 @@ static int grow_device(T*& p, size_t& cap, size_t n, const char* what) {
 template <class T>
 static int grow_host(T*& p, size_t& cap, size_t n, const char* what) {
     if (n <= cap && p) return NNDEX_OK;
+    bump_alloc_epoch();
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
@@ -155,9 +161,15 @@ void CudaIndex::scan_event_end(cudaStream_t s, cudaEvent_t a) {
     ++scan_events_used;
 }
 
+void CudaIndex::drop_graphs() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
+}
+
 CudaIndex::~CudaIndex() {
     cudaSetDevice(device);
     cudaStreamSynchronize(stream);
+    drop_graphs();
     for (auto& p : scan_events) {
         cudaEventDestroy(p.first);
         cudaEventDestroy(p.second);
@@ -641,6 +653,117 @@ int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_si
     return NNDEX_OK;
 }
 
+// Enqueues one batch of the host-buffer search on `stream` (the queries already in h_q): status
+// resets, upload, prep, the path's scan and merge, and the downloads into the pinned buffers.
+int CudaIndex::enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path) {
+    int st;
+    cudaMemsetAsync(d_err, 0xFF, sizeof(unsigned long long), stream);
+    cudaMemsetAsync(d_status, 0, sizeof(uint32_t), stream);
+    cudaMemcpyAsync(d_qraw, h_q, n * dims * sizeof(float), cudaMemcpyHostToDevice, stream);
+    if ((st = enqueue_prep_queries(d_qraw, n, mode, path, stream))) return st;
+    if (path == 4) {
+        if ((st = ivf_search(*this, d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
+                             stream)))
+            return st;
+    } else if (path == 5) {
+        if ((st = ivf_search_tc(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
+                                stream)))
+            return st;
+    } else if (path == 1) {
+        if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
+                                     static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
+            return st;
+    } else {
+        if ((st = enqueue_tc(path == 3, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
+                             stream)))
+            return st;
+        if ((st = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
+            return st;
+    }
+    cudaMemcpyAsync(h_idx, d_idx, n * kcap * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(h_sim, d_sim, n * kcap * sizeof(float), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(h_cnt, d_cnt, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+    return NNDEX_OK;
+}
+
+// The batch through a CUDA graph when one is cached for this shape, capturing it when the same
+// shape came in the previous call (its buffers are then allocated, so nothing allocates during
+// the capture); otherwise directly. Paths 1 (FP32 scan) and 4 (IVF list scan) only: the others
+// read device results on the host in the middle of the batch.
+int CudaIndex::run_host_batch(uint64_t n, uint64_t kcap, int mode, int path) {
+    const bool graphable = use_graphs && !scan_timing && (path == 1 || path == 4) &&
+                           !(graph_failed_paths & (1u << path));
+    if (!graphable) return enqueue_host_batch(n, kcap, mode, path);
+    const uint64_t epoch = alloc_epoch();
+    auto same = [&](const GraphEntry& g) { return g.path == path && g.mode == mode && g.n == n && g.kcap == kcap; };
+    for (size_t i = 0; i < graphs.size(); ++i) {
+        if (!same(graphs[i])) continue;
+        if (graphs[i].epoch != epoch) {
+            cudaGraphExecDestroy(graphs[i].exec);
+            graphs.erase(graphs.begin() + static_cast<long>(i));
+            break;
+        }
+        const cudaError_t e = cudaGraphLaunch(graphs[i].exec, stream);
+        if (e != cudaSuccess) return cuda_error(e, "graph launch");
+        // the capture's statistics: counters added to this call's, the rest as captured
+        const nndex_cuda_search_stats acc = stats;
+        stats = graphs[i].stats;
+        stats.kernel_launches += acc.kernel_launches;
+        stats.rows_scanned += acc.rows_scanned;
+        stats.second_pass_queries += acc.second_pass_queries;
+        stats.fp32_fallback_queries += acc.fp32_fallback_queries;
+        stats.ivf_rows_streamed = acc.ivf_rows_streamed;
+        stats.ivf_rows_union = acc.ivf_rows_union;
+        count_launch(static_cast<uint32_t>(graphs[i].launches));
+        stats.graph = 2;
+        return NNDEX_OK;
+    }
+    if (!(same(graph_seen) && graph_seen.epoch == epoch)) {
+        graph_seen = GraphEntry{path, mode, n, kcap, epoch};
+        return enqueue_host_batch(n, kcap, mode, path);
+    }
+    // Second call of this shape with nothing reallocated in between: capture it.
+    const nndex_cuda_search_stats before = stats;
+    const uint64_t launches0 = kernel_launches_total();
+    cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return enqueue_host_batch(n, kcap, mode, path);
+    int st = enqueue_host_batch(n, kcap, mode, path);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (st == NNDEX_OK && e == cudaSuccess && alloc_epoch() == epoch)
+        e = cudaGraphInstantiate(&exec, graph, 0);
+    else if (e == cudaSuccess)
+        e = cudaErrorStreamCaptureInvalidated;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();  // a failed capture leaves no sticky error
+    if (e != cudaSuccess || !exec) {
+        // run it the ordinary way; a path that cannot be captured is not tried again
+        if (st == NNDEX_OK) graph_failed_paths |= 1u << path;
+        stats = before;
+        graph_seen = GraphEntry{};
+        return enqueue_host_batch(n, kcap, mode, path);
+    }
+    GraphEntry g{path, mode, n, kcap, epoch};
+    g.exec = exec;
+    g.launches = kernel_launches_total() - launches0;
+    g.stats = stats;  // counters as this batch's increments
+    g.stats.kernel_launches -= before.kernel_launches;
+    g.stats.rows_scanned -= before.rows_scanned;
+    g.stats.second_pass_queries -= before.second_pass_queries;
+    g.stats.fp32_fallback_queries -= before.fp32_fallback_queries;
+    if (graphs.size() >= 8) {
+        cudaGraphExecDestroy(graphs.front().exec);
+        graphs.erase(graphs.begin());
+    }
+    graphs.push_back(g);
+    if ((e = cudaGraphLaunch(exec, stream)) != cudaSuccess) return cuda_error(e, "graph launch");
+    stats.graph = 1;
+    return NNDEX_OK;
+}
+
 int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mode, uint64_t* idx_out,
                            float* sim_out, uint64_t* counts_out) {
     std::lock_guard<std::mutex> lock(mu);
@@ -660,35 +783,8 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         if ((st = ensure_query_capacity(n))) return st;
         if ((st = ensure_result_capacity(n, kcap))) return st;
         std::memcpy(h_q, queries + q0 * dims, n * dims * sizeof(float));
-        cudaMemsetAsync(d_err, 0xFF, sizeof(unsigned long long), stream);
-        cudaMemsetAsync(d_status, 0, sizeof(uint32_t), stream);
-        cudaMemcpyAsync(d_qraw, h_q, n * dims * sizeof(float), cudaMemcpyHostToDevice, stream);
-        if ((st = enqueue_prep_queries(d_qraw, n, mode, path, stream))) return st;
-        if (path == 4) {
-            if ((st = ivf_search(*this, d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim,
-                                 d_cnt, stream)))
-                return st;
-        } else if (path == 5) {
-            if ((st = ivf_search_tc(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
-                                    stream)))
-                return st;
-        } else if (path == 1) {
-            if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
-                                         static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
-                return st;
-        } else {
-            if ((st = enqueue_tc(path == 3, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim,
-                                 d_cnt, stream)))
-                return st;
-            if ((st = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
-                return st;
-        }
-        cudaMemcpyAsync(h_idx, d_idx, n * kcap * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
-        cudaMemcpyAsync(h_sim, d_sim, n * kcap * sizeof(float), cudaMemcpyDeviceToHost, stream);
-        cudaMemcpyAsync(h_cnt, d_cnt, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
         h_flags[1] = 0;
-        cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
-        cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+        if ((st = run_host_batch(n, kcap, mode, path))) return st;
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_error(e, "search");
         if ((st = check_device_words())) return st;
@@ -1248,6 +1344,7 @@ int nndex_cuda_set_precision(nndex_cuda_index* index, uint32_t precision, uint32
                          precision == NNDEX_PRECISION_BF16 ? "BF16" : "FP8",
                          precision == NNDEX_PRECISION_BF16 ? "BF16" : "FP8");
     ix->precision = precision;
+    ix->drop_graphs();
     ix->rerank_width = rerank_width;
     return NNDEX_OK;
 }
@@ -1328,6 +1425,7 @@ int nndex_cuda_ivf_restore(nndex_cuda_index* index, uint64_t nlist, const float*
     cudaSetDevice(ix->device);
     cudaError_t e = cudaDeviceSynchronize();  // searches in flight on any stream read the old IVF
     if (e != cudaSuccess) return cuda_error(e, "IVF restore");
+    ix->drop_graphs();
     const int st = ivf_restore(*ix, nlist, centroids, offsets, original_indices, init_rows);
     if (st == NNDEX_OK) ix->approx = true;
     return st;
@@ -1344,6 +1442,18 @@ int nndex_cuda_base_checksum(nndex_cuda_index* index, uint64_t* checksum) {
     return base_checksum(*ix, checksum);
 }
 
+int nndex_cuda_set_graphs(nndex_cuda_index* index, int enable) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    cudaSetDevice(ix->device);
+    cudaStreamSynchronize(ix->stream);
+    ix->use_graphs = enable != 0;
+    ix->drop_graphs();
+    return NNDEX_OK;
+}
+
 int nndex_cuda_set_nprobe(nndex_cuda_index* index, uint32_t nprobe) {
     clear_error();
     if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
@@ -1351,6 +1461,7 @@ int nndex_cuda_set_nprobe(nndex_cuda_index* index, uint32_t nprobe) {
     std::lock_guard<std::mutex> lock(ix->mu);
     ix->opts.nprobe = nprobe;
     ix->ivf_scratch.nprobe = nprobe;
+    ix->drop_graphs();
     return NNDEX_OK;
 }
 

@@ -17,6 +17,11 @@ constexpr uint64_t kMaxBatchChunk = 16384;
 // Rows a pass-2 query may collect before it is re-run on the FP32 scan.
 constexpr uint32_t kSecondPassCap = 8192;
 
+// Incremented whenever a scratch or staging buffer of any index is (re)allocated: a captured
+// CUDA graph is valid only while the epoch it was captured in lasts.
+uint64_t alloc_epoch();
+void bump_alloc_epoch();
+
 int set_error(int code, const char* fmt, ...);
 void clear_error();
 const char* last_error();
@@ -149,6 +154,23 @@ struct CudaIndex {
     IvfScratch ivf_scratch;
     int approx_override = -1;   // -1: the index's mode; 0: exact; 1: approx (server batches)
 
+    // CUDA graphs of the host-buffer search: the whole per-batch sequence (status resets, query
+    // upload, query prep, scan, merge, result downloads) works on buffers this index owns, so a
+    // shape seen twice in a row is captured once and replayed as one launch. A graph is dropped
+    // when any scratch buffer has been reallocated since its capture (alloc_epoch()).
+    struct GraphEntry {
+        int path = 0, mode = 0;
+        uint64_t n = 0, kcap = 0, epoch = 0;
+        cudaGraphExec_t exec = nullptr;
+        nndex_cuda_search_stats stats{};
+        uint64_t launches = 0;
+    };
+    std::vector<GraphEntry> graphs;
+    GraphEntry graph_seen;          // the last shape run without a graph (capture candidate)
+    bool use_graphs = true;
+    uint32_t graph_failed_paths = 0;  // paths whose capture failed (not tried again)
+    void drop_graphs();
+
     // scan-kernel timing (roofline reports)
     bool scan_timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> scan_events;
@@ -187,6 +209,8 @@ struct CudaIndex {
     // FP32 path (device outputs are patched in place). Synchronises the stream.
     int finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
     int stream_status();
+    int enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path);
+    int run_host_batch(uint64_t n, uint64_t kcap, int mode, int path);
     // Approximate mode with an IVF that gives a speedup (src/approx.rs:35-37 provides_speedup).
     bool uses_ivf() const {
         const bool want = approx_override < 0 ? approx : approx_override == 1;

@@ -13,6 +13,7 @@ namespace nndex {
 
 // Number of kernels launched by this library (process-wide).
 void count_launch(uint32_t n = 1);
+uint64_t kernel_launches_total();
 
 struct PrepArgs {
     const float* src = nullptr;  // rows × dims raw values (device)

@@ -433,6 +433,7 @@ namespace {
 template <class T>
 int grow(T*& p, size_t& cap, size_t n, const char* what) {
     if (n <= cap && p) return NNDEX_OK;
+    bump_alloc_epoch();
     cudaFree(p);
     p = nullptr;
     cap = 0;
@@ -468,6 +469,7 @@ cudaError_t launch_scan(const CUtensorMap& tmap, const IvfScanArgs& a, uint32_t 
 template <class T>
 int grow_pinned(T*& p, size_t& cap, size_t n, const char* what) {
     if (n <= cap && p) return NNDEX_OK;
+    bump_alloc_epoch();
     cudaFreeHost(p);
     p = nullptr;
     cap = 0;
@@ -563,6 +565,7 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "IVF merge launch");
         ix.stats.kernel_launches += 4;
     }
+    if (!w.h_probed) bump_alloc_epoch();
     if (!w.h_probed && cudaMallocHost(&w.h_probed, 8 * sizeof(unsigned long long)) != cudaSuccess)
         return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: pinned allocation failed");
     cudaMemcpyAsync(w.h_probed, w.d_counters + 3, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
@@ -616,6 +619,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     if ((st = grow(ix.d_cand_cnt, ix.cap_cand_cnt, nq, "tc workspace"))) return st;
     if ((st = grow(ix.d_cert, ix.cap_cert, nq, "tc workspace"))) return st;
     if ((st = grow(ix.d_kth, ix.cap_kth, nq, "tc workspace"))) return st;
+    if (!w.h_probed) bump_alloc_epoch();
     if (!w.h_probed && cudaMallocHost(&w.h_probed, 8 * sizeof(unsigned long long)) != cudaSuccess)
         return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: pinned allocation failed");
 

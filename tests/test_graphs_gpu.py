@@ -1,0 +1,84 @@
+"""CUDA-graph replay of the host-buffer search: a shape repeated in a row is captured once and
+replayed; results must equal direct launches bit for bit, for new query values every call, and
+after nprobe / precision changes (which drop the cached graphs)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from nndex_b200 import NNdex, _lib, kernel_launch_count
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a, b):
+    assert np.array_equal(a[0], b[0])
+    assert np.array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+
+
+def _mixture(rows, dims, seed):
+    rng = np.random.default_rng(seed)
+    c = rng.normal(size=(200, dims)).astype(np.float32)
+    x = c[rng.integers(0, 200, rows)] + 0.3 * rng.normal(size=(rows, dims)).astype(np.float32)
+    return x.astype(np.float32), rng
+
+
+@pytest.mark.parametrize("batch,k", [(1, 10), (16, 100), (40, 7)])
+def test_replayed_graphs_equal_direct_launches(batch, k):
+    base, rng = _mixture(50_000, 192, 1)
+    a = NNdex(base)
+    b = NNdex(base)
+    _lib.lib().nndex_cuda_set_graphs(b.handle, 0)
+    kinds = []
+    for step in range(6):
+        q = rng.normal(size=(batch, 192)).astype(np.float32)
+        ra, rb = a.search(q, k=k), b.search(q, k=k)
+        _bits(ra, rb)
+        kinds.append(a.last_search_stats()["graph"])
+        assert b.last_search_stats()["graph"] == 0
+    assert 1 in kinds and kinds[-1] == 2, kinds
+
+
+def test_replay_counts_its_kernels():
+    base, rng = _mixture(20_000, 64, 2)
+    a = NNdex(base)
+    q = rng.normal(size=(8, 64)).astype(np.float32)
+    for _ in range(4):  # the first call allocates, the next captures, then replays
+        a.search(q, k=5)
+    assert a.last_search_stats()["graph"] == 2
+    n0 = kernel_launch_count()
+    a.search(q, k=5)
+    assert kernel_launch_count() - n0 == a.last_search_stats()["kernel_launches"] > 0
+
+
+def test_ivf_list_scan_graphs_follow_nprobe():
+    base, rng = _mixture(60_000, 96, 3)
+    a = NNdex(base, approx=True, precision="fp32", seed=5)
+    b = NNdex(base, approx=True, precision="fp32", seed=5)
+    _lib.lib().nndex_cuda_set_graphs(b.handle, 0)
+    for nprobe in (4, 4, 4, 12, 12, 12, 4):
+        a.set_nprobe(nprobe) if nprobe != a.__dict__.get("_np") else None
+        a.__dict__["_np"] = nprobe
+        b.set_nprobe(nprobe)
+        q = rng.normal(size=(32, 96)).astype(np.float32)
+        _bits(a.search(q, k=10), b.search(q, k=10))
+        assert a.last_search_stats()["path"] == 4
+    assert a.last_search_stats()["graph"] in (0, 1, 2)
+
+
+def test_graphs_off_and_on_again():
+    base, rng = _mixture(10_000, 32, 4)
+    a = NNdex(base)
+    L = _lib.lib()
+    q = rng.normal(size=(4, 32)).astype(np.float32)
+    ref = a.search(q, k=3)
+    for _ in range(4):
+        _bits(a.search(q, k=3), ref)
+    assert a.last_search_stats()["graph"] == 2
+    assert L.nndex_cuda_set_graphs(a.handle, 0) == 0
+    _bits(a.search(q, k=3), ref)
+    assert a.last_search_stats()["graph"] == 0
+    assert L.nndex_cuda_set_graphs(a.handle, 1) == 0
+    for _ in range(3):
+        _bits(a.search(q, k=3), ref)
+    assert a.last_search_stats()["graph"] == 2
