@@ -237,15 +237,20 @@ def measured_peaks():
 
 
 def profiled_traffic(rows, dims, batch, k):
-    """DRAM bytes per scan launch from the committed ncu summary, scaled to this workload."""
-    path = os.path.join(ROOT, "profiles", "scan_fp32_traffic.json")
+    """DRAM bytes per scan launch from the committed ncu summary (profiles/scan_fp32_traffic.txt),
+    scaled to this workload by the rows streamed."""
+    path = os.path.join(ROOT, "profiles", "scan_fp32_traffic.txt")
     try:
-        d = json.load(open(path))
-    except (OSError, ValueError):
+        lines = open(path).read().splitlines()
+    except OSError:
         return None
-    for e in d.get("captures", []):
-        if e.get("batch") == batch and e.get("dims") == dims and e.get("k") == k:
-            return e["dram_bytes_per_launch"] * rows / e["rows"]
+    for line in lines:
+        f = line.split()
+        if not f or f[0].startswith("#") or len(f) < 6:
+            continue
+        r, d, b, kk, _kernel, dram = f[:6]
+        if int(d) == dims and int(b) == batch and int(kk) == k:
+            return int(dram) * rows / int(r)
     return None
 
 

@@ -70,9 +70,13 @@ __global__ void __launch_bounds__(ScanShape<QB, NCW>::kThreads, 1)
     const uint32_t c = blockIdx.x;
     const uint32_t q0 = blockIdx.y * QB;
     const uint32_t nqg = (nq - q0) < static_cast<uint32_t>(QB) ? (nq - q0) : static_cast<uint32_t>(QB);
-    const uint64_t row_begin = rows * c / G;
-    const uint64_t row_end = rows * (c + 1) / G;
-    const uint32_t ntiles = static_cast<uint32_t>((row_end - row_begin + TR - 1) / TR);
+    // Whole tiles per CTA: only the base's last tile reads rows past the end (zero padding / TMA
+    // fill), so no CTA streams rows that belong to the next one.
+    const uint64_t tiles_total = (rows + TR - 1) / TR;
+    const uint64_t row_begin = static_cast<uint64_t>(TR) * (tiles_total * c / G);
+    const uint64_t row_end_t = static_cast<uint64_t>(TR) * (tiles_total * (c + 1) / G);
+    const uint64_t row_end = row_end_t < rows ? row_end_t : rows;
+    const uint32_t ntiles = static_cast<uint32_t>(row_end > row_begin ? (row_end - row_begin + TR - 1) / TR : 0);
     const uint32_t nbox = dq / 32;
 
     if (tid == 0) {
@@ -183,9 +187,13 @@ __global__ void __launch_bounds__((W + 1) * 32, 1)
     const uint32_t c = blockIdx.x;
     const uint32_t q0 = blockIdx.y * QB;
     const uint32_t nqg = (nq - q0) < static_cast<uint32_t>(QB) ? (nq - q0) : static_cast<uint32_t>(QB);
-    const uint64_t row_begin = rows * c / G;
-    const uint64_t row_end = rows * (c + 1) / G;
-    const uint32_t ntiles = static_cast<uint32_t>((row_end - row_begin + TR - 1) / TR);
+    // Whole tiles per CTA: only the base's last tile reads rows past the end (zero padding / TMA
+    // fill), so no CTA streams rows that belong to the next one.
+    const uint64_t tiles_total = (rows + TR - 1) / TR;
+    const uint64_t row_begin = static_cast<uint64_t>(TR) * (tiles_total * c / G);
+    const uint64_t row_end_t = static_cast<uint64_t>(TR) * (tiles_total * (c + 1) / G);
+    const uint64_t row_end = row_end_t < rows ? row_end_t : rows;
+    const uint32_t ntiles = static_cast<uint32_t>(row_end > row_begin ? (row_end - row_begin + TR - 1) / TR : 0);
     const uint32_t nbox = dq / 32;
 
     if (tid == 0) {
