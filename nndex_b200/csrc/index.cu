@@ -183,6 +183,8 @@ CudaIndex::~CudaIndex() {
     cudaFree(d_cnt);
     cudaFree(d_err);
     cudaFree(d_status);
+    cudaFree(d_part_keys);
+    cudaFree(d_part_done);
     cudaFreeHost(h_q);
     cudaFreeHost(h_idx);
     cudaFreeHost(h_sim);
@@ -243,6 +245,21 @@ int CudaIndex::ensure_result_capacity(uint64_t nq, uint64_t kcap) {
     return NNDEX_OK;
 }
 
+// Workspace of the split merge (merge_parts(per_query, k) blocks per query), into m.
+int CudaIndex::merge_workspace(uint64_t per_query, uint32_t nq, uint32_t k, MergeArgs& m, cudaStream_t s) {
+    const uint32_t parts = merge_parts(per_query, k);
+    if (parts <= 1) return NNDEX_OK;
+    int st;
+    if ((st = grow_device(d_part_keys, cap_part_keys, static_cast<size_t>(nq) * parts * k, "merge workspace")))
+        return st;
+    const uint32_t* before = d_part_done;
+    if ((st = grow_device(d_part_done, cap_part_done, nq, "merge workspace"))) return st;
+    if (d_part_done != before) cudaMemsetAsync(d_part_done, 0, cap_part_done * sizeof(uint32_t), s);
+    m.part_keys = d_part_keys;
+    m.part_done = d_part_done;
+    return NNDEX_OK;
+}
+
 // Enqueue the exact FP32 top-k of `nq` normalised queries (d_queries, stride ds) into the
 // device outputs. Workspace is the index's own (grown on demand).
 int CudaIndex::enqueue_exact_fp32(const float* d_queries, uint32_t nq, uint32_t k, uint32_t out_stride,
@@ -279,6 +296,7 @@ int CudaIndex::enqueue_exact_fp32(const float* d_queries, uint32_t nq, uint32_t 
     m.idx_out = o_idx;
     m.sim_out = o_sim;
     m.count_out = o_cnt;
+    if ((st = merge_workspace(per_query, nq, k, m, s))) return st;
     e = launch_merge_topk(m, s);
     if (e != cudaSuccess) return cuda_error(e, "merge launch");
     stats.kernel_launches += 2;
@@ -484,6 +502,7 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     m.idx_out = d_cand_idx;
     m.sim_out = d_cand_sim;
     m.count_out = d_cand_cnt;
+    if ((st = merge_workspace(per_query, n, kp, m, s))) return st;
     if ((e = launch_merge_topk(m, s)) != cudaSuccess) return cuda_error(e, "merge launch");
     RerankArgs r;
     r.base = d_base;

@@ -149,6 +149,13 @@ struct CudaIndex {
     size_t cap_hcnt = 0;
     uint64_t* h_flags = nullptr;
 
+    // split cross-CTA merge (merge_topk_kernel with several blocks per query)
+    uint64_t* d_part_keys = nullptr;
+    size_t cap_part_keys = 0;
+    uint32_t* d_part_done = nullptr;
+    size_t cap_part_done = 0;
+    int merge_workspace(uint64_t per_query, uint32_t nq, uint32_t k, MergeArgs& m, cudaStream_t s);
+
     nndex_cuda_search_stats stats{};
     std::shared_ptr<const IvfIndex> ivf;  // approximate mode (NNDEX_FLAG_APPROX), built at creation
     IvfScratch ivf_scratch;

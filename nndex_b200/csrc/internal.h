@@ -74,7 +74,12 @@ struct MergeArgs {
     uint64_t* idx_out = nullptr;        // nq × out_stride
     float* sim_out = nullptr;
     uint32_t* count_out = nullptr;      // nq
+    // Optional split of each query's lists over several blocks (merge_parts(per_query, k) of them):
+    // part_keys holds nq × parts × k keys, part_done nq counters that start (and end) at zero.
+    uint64_t* part_keys = nullptr;
+    uint32_t* part_done = nullptr;
 };
+uint32_t merge_parts(uint64_t per_query, uint32_t k);
 cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream);
 
 // K3 tensor-core scan (BF16 / FP8), two passes, and K4 rerank.

@@ -275,23 +275,23 @@ __global__ void __launch_bounds__((W + 1) * 32, 1)
 }
 
 // ------------------------------------------------------------------------------------------
-// Cross-CTA merge: one block per query selects the k best of `per_query` candidate keys and
-// writes them sorted (similarity desc, index asc), padding the unused slots with (0, 0.0f)
-// (src/python_bindings.rs:477-483).
+// Cross-CTA merge: the k best of a query's candidate keys (one list of k per scan CTA), written
+// sorted (similarity desc, index asc), the unused slots padded with (0, 0.0f)
+// (src/python_bindings.rs:477-483). With `parts` > 1 the lists are split over that many blocks
+// per query: each selects the exact k best of its share into part_keys, and the block that
+// finishes last (a per-query counter) merges the parts·k survivors — the same result, with the
+// selection work spread over parts·nq blocks instead of nq.
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restrict__ ws_keys, uint64_t per_query,
-                                                         uint32_t k, uint32_t out_stride,
-                                                         uint64_t* __restrict__ idx_out,
-                                                         float* __restrict__ sim_out,
-                                                         uint32_t* __restrict__ count_out) {
-    __shared__ BlockSelectScratch s;
-    extern __shared__ uint64_t sorted[];
-    const uint32_t q = blockIdx.x;
-    const uint64_t* keys = ws_keys + static_cast<size_t>(q) * per_query;
+namespace {
+
+// The k best of keys[0..n) (0 = empty slot) into the outputs of query q, sorted.
+NNDEX_DEVICE_INLINE void merge_final(const uint64_t* keys, uint64_t n, uint32_t k, uint32_t q, uint32_t out_stride,
+                                     uint64_t* idx_out, float* sim_out, uint32_t* count_out, BlockSelectScratch& s,
+                                     uint64_t* sorted) {
     if (threadIdx.x == 0) s.count = 0;
     __syncthreads();
     uint32_t local = 0;
-    for (uint64_t i = threadIdx.x; i < per_query; i += blockDim.x) local += keys[i] != 0ull;
+    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) local += keys[i] != 0ull;
     atomicAdd(&s.count, local);
     __syncthreads();
     const uint32_t nvalid = s.count;
@@ -301,10 +301,10 @@ __global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restr
     while (p2 < kk) p2 <<= 1;
     if (kk > 0) {
         uint64_t kth = 1ull;
-        if (per_query > kk) kth = block_radix_kth(keys, per_query, kk, s);
+        if (n > kk) kth = block_radix_kth(keys, n, kk, s);
         if (threadIdx.x == 0) s.count = 0;
         __syncthreads();
-        for (uint64_t i = threadIdx.x; i < per_query; i += blockDim.x) {
+        for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
             const uint64_t key = keys[i];
             if (key != 0ull && key >= kth) {
                 const uint32_t pos = atomicAdd(&s.count, 1u);
@@ -316,6 +316,7 @@ __global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restr
         __syncthreads();
         block_bitonic_sort_desc(sorted, p2);
     }
+    __syncthreads();
     for (uint32_t j = threadIdx.x; j < out_stride; j += blockDim.x) {
         uint64_t idx = 0;
         float sim = 0.0f;
@@ -327,6 +328,64 @@ __global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restr
         sim_out[static_cast<size_t>(q) * out_stride + j] = sim;
     }
     if (threadIdx.x == 0 && count_out) count_out[q] = kk;
+}
+
+}  // namespace
+
+// grid (parts, nq); dynamic shared memory: p2(k) keys for the sort, plus parts·k keys when
+// parts > 1 (the survivors, staged for the final merge).
+__global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restrict__ ws_keys, uint64_t per_query,
+                                                         uint32_t k, uint32_t out_stride,
+                                                         uint64_t* __restrict__ idx_out,
+                                                         float* __restrict__ sim_out,
+                                                         uint32_t* __restrict__ count_out, uint32_t parts,
+                                                         uint64_t* __restrict__ part_keys,
+                                                         uint32_t* __restrict__ part_done) {
+    __shared__ BlockSelectScratch s;
+    __shared__ uint32_t last;
+    extern __shared__ uint64_t smem_keys[];
+    const uint32_t q = blockIdx.y;
+    const uint64_t* keys = ws_keys + static_cast<size_t>(q) * per_query;
+    uint32_t p2 = 1;
+    while (p2 < k) p2 <<= 1;
+    if (parts == 1) {
+        merge_final(keys, per_query, k, q, out_stride, idx_out, sim_out, count_out, s, smem_keys);
+        return;
+    }
+    // This block's share: lists [l0, l1) of k keys each.
+    const uint64_t lists = per_query / k;
+    const uint64_t l0 = lists * blockIdx.x / parts, l1 = lists * (blockIdx.x + 1) / parts;
+    const uint64_t n = (l1 - l0) * k;
+    const uint64_t* src = keys + l0 * k;
+    uint64_t* dst = part_keys + (static_cast<size_t>(q) * parts + blockIdx.x) * k;
+    uint64_t kth = 0ull;
+    if (n > k) kth = block_radix_kth(src, n, k, s);
+    if (threadIdx.x == 0) s.count = 0;
+    __syncthreads();
+    // Non-empty keys >= kth: exactly k of them when the share holds at least k (keys are distinct);
+    // all of them otherwise (kth is then an empty slot, 0). The rest of the part is padded with 0.
+    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint64_t key = src[i];
+        if (key != 0ull && key >= kth) {
+            const uint32_t pos = atomicAdd(&s.count, 1u);
+            if (pos < k) dst[pos] = key;
+        }
+    }
+    __syncthreads();
+    for (uint32_t j = s.count + threadIdx.x; j < k; j += blockDim.x) dst[j] = 0ull;
+    // Publish the part; the last block of this query merges them.
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&part_done[q], 1u) == parts - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    uint64_t* staged = smem_keys + p2;
+    const uint64_t* all = part_keys + static_cast<size_t>(q) * parts * k;
+    for (uint32_t i = threadIdx.x; i < parts * k; i += blockDim.x) staged[i] = __ldcg(all + i);
+    __syncthreads();
+    merge_final(staged, static_cast<uint64_t>(parts) * k, k, q, out_stride, idx_out, sim_out, count_out, s, smem_keys);
+    if (threadIdx.x == 0) part_done[q] = 0;  // ready for the next launch
 }
 
 // ------------------------------------------------------------------------------------------
@@ -530,11 +589,26 @@ cudaError_t launch_scan_fp32(const ScanArgs& a, const ScanPlan& p, cudaStream_t 
     }
 }
 
+uint32_t merge_parts(uint64_t per_query, uint32_t k) {
+    const uint64_t lists = k ? per_query / k : 0;
+    uint64_t parts = lists < 16 ? lists : 16;
+    while (parts > 1 && parts * k > 4096) --parts;  // survivors staged in shared memory
+    return parts < 1 ? 1u : static_cast<uint32_t>(parts);
+}
+
 cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream) {
     uint32_t p2 = 1;
     while (p2 < a.k) p2 <<= 1;
-    merge_topk_kernel<<<a.nq, 512, p2 * sizeof(uint64_t), stream>>>(a.ws_keys, a.per_query, a.k, a.out_stride,
-                                                                    a.idx_out, a.sim_out, a.count_out);
+    const uint32_t parts = (a.part_keys && a.part_done) ? merge_parts(a.per_query, a.k) : 1u;
+    const size_t smem = (p2 + (parts > 1 ? static_cast<size_t>(parts) * a.k : 0)) * sizeof(uint64_t);
+    if (smem > 40 * 1024) {  // with the static scratch, above the default 48 KB per block
+        cudaError_t e = cudaFuncSetAttribute(merge_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
+    merge_topk_kernel<<<dim3(parts, a.nq), 512, smem, stream>>>(a.ws_keys, a.per_query, a.k, a.out_stride, a.idx_out,
+                                                                a.sim_out, a.count_out, parts, a.part_keys,
+                                                                a.part_done);
     count_launch();
     return cudaGetLastError();
 }
