@@ -208,10 +208,11 @@ struct RingPos {
 
 template <int QB, int W, int ST>
 struct ScanConsumerWide {
-    static_assert(QB == 8 || QB == 16, "the wide consumer takes 8 or 16 queries");
+    static_assert(QB == 1 || QB == 2 || QB == 4 || QB == 8 || QB == 16, "the wide consumer takes 1-16 queries");
+    static constexpr int kGQ = QB < 4 ? QB : 4;  // queries per FMA group
     static constexpr int kTileRows = 16 * W;
     static constexpr uint32_t kStageBytes = kTileRows * 128;
-    static constexpr int kHalf = QB / 2;
+    static constexpr int kHalf = QB >= 2 ? QB / 2 : 1;  // values a lane inserts
     // Queries in shared memory slab-major: [dq / 32][QB][32] floats, so a slab's query chunks sit
     // at fixed offsets (b · 128 bytes) from the slab's base.
     static constexpr uint32_t kQSlabBytes = QB * 128;
@@ -256,26 +257,26 @@ struct ScanConsumerWide {
     template <int G0, int G1>
     NNDEX_DEVICE_INLINE static void fma_groups(float (&acc)[4][QB], const float4 (&x)[4], const float4* q) {
 #pragma unroll
-        for (int b0 = 4 * G0; b0 < 4 * G1; b0 += 4) {
-            float4 qv[4];
+        for (int b0 = kGQ * G0; b0 < kGQ * G1; b0 += kGQ) {
+            float4 qv[kGQ];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) qv[j] = q[(b0 + j) * 8];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][b0 + j] = fmaf(x[i].x, qv[j].x, acc[i][b0 + j]);
+            for (int j = 0; j < kGQ; ++j) qv[j] = q[(b0 + j) * 8];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][b0 + j] = fmaf(x[i].y, qv[j].y, acc[i][b0 + j]);
+                for (int j = 0; j < kGQ; ++j) acc[i][b0 + j] = fmaf(x[i].x, qv[j].x, acc[i][b0 + j]);
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][b0 + j] = fmaf(x[i].z, qv[j].z, acc[i][b0 + j]);
+                for (int j = 0; j < kGQ; ++j) acc[i][b0 + j] = fmaf(x[i].y, qv[j].y, acc[i][b0 + j]);
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][b0 + j] = fmaf(x[i].w, qv[j].w, acc[i][b0 + j]);
+                for (int j = 0; j < kGQ; ++j) acc[i][b0 + j] = fmaf(x[i].z, qv[j].z, acc[i][b0 + j]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < kGQ; ++j) acc[i][b0 + j] = fmaf(x[i].w, qv[j].w, acc[i][b0 + j]);
         }
     }
 
@@ -301,7 +302,7 @@ struct ScanConsumerWide {
             }
             load_rows(xn, nxt);
         }
-        fma_groups<1, QB / 4>(acc, x, q);
+        fma_groups<1, QB / kGQ>(acc, x, q);
         release(empty_bar, cur);
     }
 
@@ -356,11 +357,19 @@ struct ScanConsumerWide {
         float v2[2 * QB], v1[QB], v0[kHalf];
         halve<4 * QB>(v4, v2, 1, (dg & 1u) != 0);   // keeps rows {0,1} or {2,3}
         halve<2 * QB>(v2, v1, 2, (dg & 2u) != 0);   // keeps one row of those two
-        halve<QB>(v1, v0, 4, (dg & 4u) != 0);       // keeps queries [0, QB/2) or [QB/2, QB)
+        bool inserts = true;
+        if constexpr (QB >= 2) {
+            halve<QB>(v1, v0, 4, (dg & 4u) != 0);   // keeps queries [0, QB/2) or [QB/2, QB)
+        } else {
+            // one value left: the last step adds the partner's (S0 + S1 in both lanes: addition
+            // commutes) and the lane whose bit is clear inserts it
+            v0[0] = v1[0] + __shfl_xor_sync(0xffffffffu, v1[0], 4);
+            inserts = (dg & 4u) == 0;
+        }
         const uint32_t i_l = 2 * (dg & 1u) + ((dg >> 1) & 1u);
         const uint64_t r = tile_row0 + warp * 16 + rg + 4 * i_l;
-        const uint32_t b0 = kHalf * (dg >> 2);
-        if (r < row_end) {
+        const uint32_t b0 = QB >= 2 ? kHalf * (dg >> 2) : 0u;
+        if (r < row_end && inserts) {
             const uint32_t rk = row_key(r);
 #pragma unroll
             for (int t = 0; t < kHalf; ++t) {

@@ -176,7 +176,7 @@ __global__ void __launch_bounds__((W + 1) * 32, 1)
     uint32_t* hist = reinterpret_cast<uint32_t*>(cand + static_cast<size_t>(QB) * cap);
     uint64_t* thr = reinterpret_cast<uint64_t*>(hist + W * 256);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(thr + QB);
-    uint64_t* full_bar = reinterpret_cast<uint64_t*>(cnt + QB);
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(cnt + QB + (QB & 1));  // mbarriers: 8-byte aligned
     uint64_t* empty_bar = full_bar + ST;
     volatile uint32_t* abort_flag = reinterpret_cast<volatile uint32_t*>(empty_bar + ST);
 
@@ -451,7 +451,7 @@ size_t wide_smem_bytes(uint32_t qb, uint32_t w, uint32_t dq, uint32_t cap, uint3
     b += static_cast<size_t>(qb) * dq * 4;
     b += static_cast<size_t>(qb) * cap * 8;
     b += static_cast<size_t>(w) * 256 * 4;
-    b += qb * 8 + qb * 4;
+    b += qb * 8 + (qb + (qb & 1)) * 4;
     b += static_cast<size_t>(stages) * 16 + 16;
     return b;
 }
@@ -510,8 +510,8 @@ cudaError_t launch_wide(const ScanArgs& a, const ScanPlan& p, cudaStream_t strea
 // Tile-shape overrides for the autotuner and for measurement sweeps (0 = default):
 //   NNDEX_SCAN_STAGES   ring depth (2 or 4)        NNDEX_SCAN_QB   max queries per CTA (1..16)
 //   NNDEX_SCAN_CTAS     CTAs per query group      NNDEX_SCAN_CAP  candidate slots beyond k
-//   NNDEX_SCAN_WIDE     wide consumer warps at 8 / 16 queries per CTA: 7, 8, 11 or 16 (default 16
-//                       at 8 queries, 11 at 16); 1 = the 4-row × 8-query consumer instead
+//   NNDEX_SCAN_WIDE     wide consumer warps at 1..16 queries per CTA: 7, 8, 11 or 16 (default 16
+//                       up to 8 queries, 11 at 16); 1 = the 4-row × 8-query consumer instead
 static uint32_t env_u32(const char* name) {
     const char* v = getenv(name);
     return v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
@@ -542,12 +542,12 @@ bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t s
     // 8 or 16 queries per CTA: the wide consumer (16 rows × all queries per warp) when it fits.
     static const uint32_t o_wide = env_u32("NNDEX_SCAN_WIDE");
     plan.wide = 0;
-    if ((plan.qb == 8 || plan.qb == 16) && o_wide != 1) {
+    if (o_wide != 1) {
         // 16 consumer warps at 8 queries (96 registers, 4 warps per scheduler); 11 at 16 queries (3
         // per scheduler at up to 168 registers: the 64 accumulators need more than the 96 registers
         // that 17 warps leave)
         const uint32_t w = o_wide ? (o_wide == 16 || o_wide == 11 || o_wide == 7 ? o_wide : 8)
-                                  : (plan.qb == 8 ? 16 : 11);
+                                  : (plan.qb <= 8 ? 16 : 11);
         const uint32_t tr = 16 * w;
         const uint32_t wcap = ((k + (o_cap ? (o_cap > tr ? o_cap : tr + 32) : 2 * tr)) + 31) / 32 * 32;
         // ring depths with a kernel instance: 16 warps {4, 3, 2}, 8 warps {6, 4, 3, 2}
@@ -578,7 +578,15 @@ bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t s
 }
 
 cudaError_t launch_scan_fp32(const ScanArgs& a, const ScanPlan& p, cudaStream_t stream) {
-    if (p.wide) return p.qb == 16 ? launch_wide<16>(a, p, stream) : launch_wide<8>(a, p, stream);
+    if (p.wide) {
+        switch (p.qb) {
+            case 1: return launch_wide<1>(a, p, stream);
+            case 2: return launch_wide<2>(a, p, stream);
+            case 4: return launch_wide<4>(a, p, stream);
+            case 8: return launch_wide<8>(a, p, stream);
+            default: return launch_wide<16>(a, p, stream);
+        }
+    }
     switch (p.qb) {
         case 1: return launch_qb<1>(a, p, stream);
         case 2: return launch_qb<2>(a, p, stream);
