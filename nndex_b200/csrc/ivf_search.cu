@@ -27,10 +27,7 @@ namespace nndex {
 
 namespace {
 constexpr uint32_t kChunkRows = 4096;   // rows per list chunk (work-item granularity)
-constexpr int kNcw = 4;                 // consumer warps per half (as the FP32 scan)
-constexpr int kTileRows = kNcw * 32;    // 128 rows per tile
-constexpr int kStages = 4;
-constexpr uint32_t kStageBytes = kTileRows * 128;
+constexpr int kStages = 4;              // ring depth of the list scan
 
 NNDEX_DEVICE_INLINE uint8_t* align_1024(uint8_t* p) {
     const uint32_t a = smem_u32(p);
@@ -170,8 +167,8 @@ __global__ void __launch_bounds__(1024)
 }
 
 // ------------------------------------------------------------------------------------------
-// 3. Ragged list scan (persistent). Producer warp: TMA of 128-row × 128-byte slabs of the
-//    reordered rows. 2·kNcw consumer warps: the FP32 scan's mapping and FMA order.
+// 3. Ragged list scan (persistent). Producer warp: TMA of 128-row × 128-byte boxes of the
+//    reordered rows. Consumer warps: the FP32 scan's wide consumer, FMA order and addition tree.
 // ------------------------------------------------------------------------------------------
 struct IvfScanArgs {
     uint32_t dq = 0;             // row stride (floats), multiple of 32
@@ -191,20 +188,30 @@ struct IvfScanArgs {
     uint32_t* status = nullptr;
 };
 
+// Consumer warps of the list scan per queries per item: ScanConsumerWide (16 rows × all the item's
+// queries per warp, the FP32 scan's FMA order and addition tree); 8 warps of 128-row tiles at 16
+// queries, 16 warps of 256-row tiles (two 128-row boxes per slab) at 4 or 8.
 template <int QB>
-__global__ void __launch_bounds__(ScanShape<QB, kNcw>::kThreads, 1)
+struct IvfScanShape {
+    static constexpr int kW = QB >= 16 ? 8 : 16;
+    static constexpr int kThreads = (kW + 1) * 32;
+};
+
+template <int QB>
+__global__ void __launch_bounds__(IvfScanShape<QB>::kThreads, 1)
     ivf_scan_kernel(const __grid_constant__ CUtensorMap tmap, const IvfScanArgs a) {
-    using S = ScanShape<QB, kNcw>;
-    using Consumer = ScanConsumer<QB, kNcw, kStages>;
-    constexpr uint32_t kConsumers = S::kConsumers;
+    constexpr int W = IvfScanShape<QB>::kW;
+    using Consumer = ScanConsumerWide<QB, W, kStages>;
+    constexpr int TR = Consumer::kTileRows;
+    constexpr uint32_t kStage = Consumer::kStageBytes;
+    constexpr uint32_t kBoxes = TR / 128;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* stage_base = align_1024(smem_raw);
     const uint32_t dq = a.dq, cap = a.cap, k = a.k;
-    float* q_s = reinterpret_cast<float*>(stage_base + static_cast<size_t>(kStages) * kStageBytes);
+    float* q_s = reinterpret_cast<float*>(stage_base + static_cast<size_t>(kStages) * kStage);
     uint64_t* cand = reinterpret_cast<uint64_t*>(q_s + static_cast<size_t>(QB) * dq);
-    float* xchg = reinterpret_cast<float*>(cand + static_cast<size_t>(QB) * cap);
-    uint32_t* hist = reinterpret_cast<uint32_t*>(xchg + kConsumers * 32 * S::kXchg);
-    uint64_t* thr = reinterpret_cast<uint64_t*>(hist + kConsumers * 256);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(cand + static_cast<size_t>(QB) * cap);
+    uint64_t* thr = reinterpret_cast<uint64_t*>(hist + W * 256);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(thr + QB);
     uint32_t* qid = cnt + QB;
     uint32_t* slot = qid + QB;
@@ -219,18 +226,20 @@ __global__ void __launch_bounds__(ScanShape<QB, kNcw>::kThreads, 1)
     if (tid == 0) {
         for (int s = 0; s < kStages; ++s) {
             mbar_init(&full_bar[s], 1);
-            mbar_init(&empty_bar[s], kConsumers);
+            mbar_init(&empty_bar[s], W * 32);  // every consumer lane releases
         }
         *abort_flag = 0;
         fence_mbar_init();
     }
     __syncthreads();
 
-    constexpr uint32_t nthreads_c = kConsumers * 32;
-    const Consumer con(warp < kConsumers ? warp : 0, lane, stage_base, q_s, dq, xchg);
+    constexpr uint32_t nthreads_c = W * 32;
+    const Consumer con(warp < static_cast<uint32_t>(W) ? warp : 0, lane, stage_base, q_s);
     auto row_key = [&](uint64_t r) { return a.row_map[r]; };
 
-    uint32_t it = 0;  // ring position (producer and consumers walk the same sequence)
+    // Producer and consumers walk the same sequence of ring positions across items.
+    uint32_t it = 0;
+    RingPos<kStages> pos;
     for (;;) {
         if (tid == 0) {
             const unsigned long long w = *abort_flag ? total_items : atomicAdd(&a.counters[0], 1ull);
@@ -266,15 +275,15 @@ __global__ void __launch_bounds__(ScanShape<QB, kNcw>::kThreads, 1)
         const uint32_t nqg = static_cast<uint32_t>(item[2]);
         if (nqg == 0) break;
         const uint64_t row_begin = item[0], row_end = item[1];
-        const uint32_t ntiles = static_cast<uint32_t>((row_end - row_begin + kTileRows - 1) / kTileRows);
+        const uint32_t ntiles = static_cast<uint32_t>((row_end - row_begin + TR - 1) / TR);
 
-        if (warp == kConsumers) {
+        if (warp == static_cast<uint32_t>(W)) {
             // ---------------- producer ----------------
             if (lane == 0) {
                 const uint64_t policy = l2_policy_evict_first();
                 bool stop = false;
                 for (uint32_t t = 0; t < ntiles && !stop; ++t) {
-                    const int32_t y = static_cast<int32_t>(row_begin + static_cast<uint64_t>(t) * kTileRows);
+                    const int32_t y = static_cast<int32_t>(row_begin + static_cast<uint64_t>(t) * TR);
                     for (uint32_t bx = 0; bx < nbox; ++bx) {
                         const uint32_t s = it & (kStages - 1), u = it / kStages;
                         if (*abort_flag) {
@@ -287,9 +296,12 @@ __global__ void __launch_bounds__(ScanShape<QB, kNcw>::kThreads, 1)
                             stop = true;
                             break;
                         }
-                        mbar_arrive_expect_tx(&full_bar[s], kStageBytes);
-                        tma_load_2d_hint(stage_base + static_cast<size_t>(s) * kStageBytes, &tmap, &full_bar[s],
-                                         static_cast<int32_t>(bx * 32), y, policy);
+                        mbar_arrive_expect_tx(&full_bar[s], kStage);
+#pragma unroll
+                        for (uint32_t h = 0; h < kBoxes; ++h)
+                            tma_load_2d_hint(stage_base + static_cast<size_t>(s) * kStage + h * 128 * 128, &tmap,
+                                             &full_bar[s], static_cast<int32_t>(bx * 32),
+                                             y + static_cast<int32_t>(h * 128), policy);
                         ++it;
                     }
                 }
@@ -299,21 +311,21 @@ __global__ void __launch_bounds__(ScanShape<QB, kNcw>::kThreads, 1)
             // ---------------- consumers ----------------
             for (uint32_t i = tid; i < static_cast<uint32_t>(QB) * dq; i += nthreads_c) {
                 const uint32_t b = i / dq, d = i - b * dq;
-                q_s[i] = b < nqg ? a.queries[static_cast<uint64_t>(qid[b]) * dq + d] : 0.0f;
+                q_s[Consumer::q_slab_index(b, d)] = b < nqg ? a.queries[static_cast<uint64_t>(qid[b]) * dq + d] : 0.0f;
             }
             if (tid < static_cast<uint32_t>(QB)) {
                 cnt[tid] = 0;
                 thr[tid] = 0ull;
             }
             named_bar_sync(1, nthreads_c);
-            float acc[4][Consumer::QW];
+            float acc[4][QB];
             for (uint32_t t = 0; t < ntiles; ++t) {
-                con.accumulate(acc, nbox, it, full_bar, empty_bar, abort_flag, a.status);
-                con.insert(acc, row_begin + static_cast<uint64_t>(t) * kTileRows, row_end, nqg, row_key, thr, cnt, cand,
-                           cap, a.status);
-                scan_flush<QB, kNcw>(t + 1 == ntiles, nqg, k, cap, warp, lane, cnt, thr, cand, hist);
+                con.accumulate(acc, nbox, pos, full_bar, empty_bar, abort_flag, a.status);
+                con.insert(acc, row_begin + static_cast<uint64_t>(t) * TR, row_end, nqg, row_key, thr, cnt, cand, cap,
+                           a.status);
+                scan_flush_g<QB, W, TR>(t + 1 == ntiles, nqg, k, cap, warp, lane, cnt, thr, cand, hist);
             }
-            for (uint32_t b = warp; b < nqg; b += kConsumers) {
+            for (uint32_t b = warp; b < nqg; b += W) {
                 const uint32_t n = cnt[b] < k ? cnt[b] : k;
                 uint64_t* dst = a.ws + static_cast<uint64_t>(slot[b]) * k;
                 const uint64_t* src = cand + static_cast<size_t>(b) * cap;
@@ -322,7 +334,7 @@ __global__ void __launch_bounds__(ScanShape<QB, kNcw>::kThreads, 1)
         }
         __syncthreads();  // the item's shared state is consumed before the next fetch
     }
-    if (warp == kConsumers && lane == 0) {
+    if (warp == static_cast<uint32_t>(W) && lane == 0) {
         const uint32_t used = it < static_cast<uint32_t>(kStages) ? it : kStages;
         for (uint32_t s = 0; s < used; ++s) {
             const uint32_t uses = (it - s + kStages - 1) / kStages;
@@ -443,14 +455,16 @@ int grow(T*& p, size_t& cap, size_t n, const char* what) {
     return NNDEX_OK;
 }
 
+// Tile rows of the list scan at qb queries per item (IvfScanShape).
+uint32_t ivf_scan_tile_rows(uint32_t qb) { return qb >= 16 ? 8 * 16 : 16 * 16; }
+
 size_t ivf_scan_smem(uint32_t qb, uint32_t dq, uint32_t cap) {
-    const size_t consumers = scan_consumers(qb, kNcw);
+    const uint32_t w = qb >= 16 ? 8 : 16;
     size_t b = 1024;
-    b += static_cast<size_t>(kStages) * kStageBytes;
+    b += static_cast<size_t>(kStages) * ivf_scan_tile_rows(qb) * 128;
     b += static_cast<size_t>(qb) * dq * 4;
     b += static_cast<size_t>(qb) * cap * 8;
-    b += consumers * 32 * scan_xchg_per_lane(qb) * 4;
-    b += consumers * 256 * 4;
+    b += static_cast<size_t>(w) * 256 * 4;
     b += qb * 8 + (3 * qb + (qb & 1)) * 4;
     b += 4 * 8 + kStages * 16 + 16;
     return b;
@@ -461,7 +475,7 @@ cudaError_t launch_scan(const CUtensorMap& tmap, const IvfScanArgs& a, uint32_t 
     auto kern = ivf_scan_kernel<QB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    kern<<<grid, ScanShape<QB, kNcw>::kThreads, smem, s>>>(tmap, a);
+    kern<<<grid, IvfScanShape<QB>::kThreads, smem, s>>>(tmap, a);
     count_launch();
     return cudaGetLastError();
 }
@@ -493,8 +507,9 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
     // Queries per work item from the average number of queries probing a list.
     const double avg_q = static_cast<double>(nq) * np / nlist;
     uint32_t qb = avg_q >= 12.0 ? 16 : (avg_q >= 6.0 ? 8 : 4);
-    const uint32_t cap = ((k + 2 * kTileRows) + 31) / 32 * 32;
-    while (qb > 4 && ivf_scan_smem(qb, dq, cap) > ix.smem_optin) qb >>= 1;
+    auto cap_for = [&](uint32_t b) { return ((k + 2 * ivf_scan_tile_rows(b)) + 31) / 32 * 32; };
+    while (qb > 4 && ivf_scan_smem(qb, dq, cap_for(qb)) > ix.smem_optin) qb >>= 1;
+    const uint32_t cap = cap_for(qb);
     const size_t smem = ivf_scan_smem(qb, dq, cap);
     if (smem > ix.smem_optin)
         return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF scan needs %zu bytes of shared memory", smem);

@@ -214,7 +214,7 @@ def test_ivf_probed_fewer_rows_than_k():
 
 TC_CASES = [
     # name, rows, dims, nlist, nq, k, nprobe
-    ("mixture", 20_000, 64, 64, 200, 10, 0),
+    ("mixture", 20_000, 64, 64, 300, 10, 0),  # ≈ 14 queries per probed list: the tensor-core scan
     ("mixture", 20_000, 64, 64, 150, 1, 9),
     ("zipf", 30_000, 96, 150, 300, 100, 0),
     ("multichunk", 60_000, 128, 8, 96, 10, 3),  # lists of ≈ 7,500 rows: two 4,096-row chunks each
