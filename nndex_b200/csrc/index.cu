@@ -178,17 +178,12 @@ CudaIndex::~CudaIndex() {
     cudaFree(d_qraw);
     cudaFree(d_qn);
     cudaFree(d_ws);
-    cudaFree(d_idx);
-    cudaFree(d_sim);
-    cudaFree(d_cnt);
-    cudaFree(d_err);
-    cudaFree(d_status);
+    cudaFree(d_res);
+    cudaFree(d_err);  // d_status lives in the same allocation
     cudaFree(d_part_keys);
     cudaFree(d_part_done);
     cudaFreeHost(h_q);
-    cudaFreeHost(h_idx);
-    cudaFreeHost(h_sim);
-    cudaFreeHost(h_cnt);
+    cudaFreeHost(h_res);
     cudaFreeHost(h_flags);
     if (owns_base) cudaFree(d_base_bf16);
     if (owns_base) cudaFree(d_base_fp8);
@@ -236,12 +231,16 @@ int CudaIndex::ensure_query_capacity(uint64_t nq) {
 
 int CudaIndex::ensure_result_capacity(uint64_t nq, uint64_t kcap) {
     int st;
-    if ((st = grow_device(d_idx, cap_idx, nq * kcap, "result buffer"))) return st;
-    if ((st = grow_device(d_sim, cap_sim, nq * kcap, "result buffer"))) return st;
-    if ((st = grow_device(d_cnt, cap_cnt, nq, "result buffer"))) return st;
-    if ((st = grow_host(h_idx, cap_hidx, nq * kcap, "pinned result buffer"))) return st;
-    if ((st = grow_host(h_sim, cap_hsim, nq * kcap, "pinned result buffer"))) return st;
-    if ((st = grow_host(h_cnt, cap_hcnt, nq, "pinned result buffer"))) return st;
+    const size_t bi = nq * kcap * sizeof(uint64_t), bs = nq * kcap * sizeof(float), bc = nq * sizeof(uint32_t);
+    res_bytes = bi + bs + bc;
+    if ((st = grow_device(d_res, cap_res, res_bytes, "result buffer"))) return st;
+    if ((st = grow_host(h_res, cap_hres, res_bytes, "pinned result buffer"))) return st;
+    d_idx = reinterpret_cast<uint64_t*>(d_res);
+    d_sim = reinterpret_cast<float*>(d_res + bi);
+    d_cnt = reinterpret_cast<uint32_t*>(d_res + bi + bs);
+    h_idx = reinterpret_cast<uint64_t*>(h_res);
+    h_sim = reinterpret_cast<float*>(h_res + bi);
+    h_cnt = reinterpret_cast<uint32_t*>(h_res + bi + bs);
     return NNDEX_OK;
 }
 
@@ -707,11 +706,8 @@ int CudaIndex::enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path)
         if ((st = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
             return st;
     }
-    cudaMemcpyAsync(h_idx, d_idx, n * kcap * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(h_sim, d_sim, n * kcap * sizeof(float), cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(h_cnt, d_cnt, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(h_res, d_res, res_bytes, cudaMemcpyDeviceToHost, stream);  // idx, sim, cnt
+    cudaMemcpyAsync(h_flags, d_err, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);  // err, status
     return NNDEX_OK;
 }
 
@@ -810,8 +806,8 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         if ((st = ensure_query_capacity(n))) return st;
         if ((st = ensure_result_capacity(n, kcap))) return st;
         std::memcpy(h_q, queries + q0 * dims, n * dims * sizeof(float));
-        h_flags[1] = 0;
         if ((st = run_host_batch(n, kcap, mode, path))) return st;
+        cudaEventRecord(ev1, stream);  // before the wait: the device time ends with the last batch
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_error(e, "search");
         if ((st = check_device_words())) return st;
@@ -825,11 +821,9 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         if (counts_out)
             for (uint64_t i = 0; i < n; ++i) counts_out[q0 + i] = h_cnt[i];
     }
-    cudaEventRecord(ev1, stream);
     mark_done(stream);
-    cudaEventSynchronize(ev1);
     float ms = 0.0f;
-    cudaEventElapsedTime(&ms, ev0, ev1);
+    if (nq) cudaEventElapsedTime(&ms, ev0, ev1);
     stats.device_ms = ms;
     return NNDEX_OK;
 }
@@ -973,8 +967,8 @@ int index_begin(uint64_t rows, uint64_t dims, uint32_t flags, const nndex_cuda_o
         return fail(cuda_error(e, "cudaStreamCreate"));
     cudaEventCreate(&ix->ev0);
     cudaEventCreate(&ix->ev1);
-    if ((e = cudaMalloc(&ix->d_err, sizeof(unsigned long long))) != cudaSuccess) return fail(cuda_error(e, "alloc"));
-    if ((e = cudaMalloc(&ix->d_status, sizeof(uint32_t))) != cudaSuccess) return fail(cuda_error(e, "alloc"));
+    if ((e = cudaMalloc(&ix->d_err, 2 * sizeof(unsigned long long))) != cudaSuccess) return fail(cuda_error(e, "alloc"));
+    ix->d_status = reinterpret_cast<uint32_t*>(ix->d_err + 1);
     if ((e = cudaMallocHost(&ix->h_flags, 2 * sizeof(uint64_t))) != cudaSuccess) return fail(cuda_error(e, "alloc"));
     const size_t base_bytes = ix->rows_alloc * ix->ds * sizeof(float);
     if ((e = cudaMalloc(&ix->d_base, base_bytes)) != cudaSuccess) return fail(cuda_error(e, "base allocation"));
@@ -1174,12 +1168,12 @@ int make_view(const CudaIndex& src, CudaIndex** out) {
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreate(&v->ev0)) != cudaSuccess || (e = cudaEventCreate(&v->ev1)) != cudaSuccess ||
-        (e = cudaMalloc(&v->d_err, sizeof(unsigned long long))) != cudaSuccess ||
-        (e = cudaMalloc(&v->d_status, sizeof(uint32_t))) != cudaSuccess ||
+        (e = cudaMalloc(&v->d_err, 2 * sizeof(unsigned long long))) != cudaSuccess ||
         (e = cudaMallocHost(&v->h_flags, 2 * sizeof(uint64_t))) != cudaSuccess) {
         delete v;
         return cuda_error(e, "index view");
     }
+    v->d_status = reinterpret_cast<uint32_t*>(v->d_err + 1);
     cudaMemsetAsync(v->d_err, 0xFF, sizeof(unsigned long long), v->stream);
     cudaMemsetAsync(v->d_status, 0, sizeof(uint32_t), v->stream);
     cudaStreamSynchronize(v->stream);

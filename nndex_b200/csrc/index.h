@@ -131,22 +131,26 @@ struct CudaIndex {
     size_t cap_qn = 0;
     uint64_t* d_ws = nullptr;
     size_t cap_ws = 0;
+    // Results of the host-buffer search: idx (n·k u64), sim (n·k f32) and cnt (n u32) laid out
+    // back to back in one device buffer and one pinned buffer, so a single copy downloads them
+    // (ensure_result_capacity sets the three views for the batch's shape).
+    uint8_t* d_res = nullptr;
+    size_t cap_res = 0;
+    uint8_t* h_res = nullptr;
+    size_t cap_hres = 0;
     uint64_t* d_idx = nullptr;
-    size_t cap_idx = 0;
     float* d_sim = nullptr;
-    size_t cap_sim = 0;
     uint32_t* d_cnt = nullptr;
-    size_t cap_cnt = 0;
+    uint64_t* h_idx = nullptr;
+    float* h_sim = nullptr;
+    uint32_t* h_cnt = nullptr;
+    size_t res_bytes = 0;        // bytes of the current batch's results
+    // Status words, adjacent in one 16-byte allocation (d_status = the word after d_err), read back
+    // with one copy into h_flags.
     unsigned long long* d_err = nullptr;
     uint32_t* d_status = nullptr;
     float* h_q = nullptr;
     size_t cap_hq = 0;
-    uint64_t* h_idx = nullptr;
-    size_t cap_hidx = 0;
-    float* h_sim = nullptr;
-    size_t cap_hsim = 0;
-    uint32_t* h_cnt = nullptr;
-    size_t cap_hcnt = 0;
     uint64_t* h_flags = nullptr;
 
     // split cross-CTA merge (merge_topk_kernel with several blocks per query)
