@@ -398,6 +398,19 @@ NNDEX_API int nndex_cuda_server_stats_get(nndex_cuda_server* server, nndex_cuda_
 /* Finishes the queued requests, joins the workers and frees the slots. */
 NNDEX_API void nndex_cuda_server_stop(nndex_cuda_server* server);
 
+/* ---- failure handling checks (no counterpart in the reference, whose GPU waits have no limit:
+ * src/gpu.rs:573, 756) ------------------------------------------------------------------------ */
+
+/* Runs one bounded device wait, of `budget_cycles` clock cycles (1 .. 2e9), on an mbarrier that
+ * nothing completes: the kernel records a timeout status and returns, and the call reports it as
+ * NNDEX_ERR_TIMEOUT like any search whose wait ran out. The index stays usable afterwards. */
+NNDEX_API int nndex_cuda_check_bounded_wait(nndex_cuda_index* index, uint64_t budget_cycles);
+
+/* Fault injection on the host: the next `count` scratch or staging allocations made by any index
+ * fail as if the GPU were out of memory (no cudaMalloc is attempted), and the calls that needed them
+ * return NNDEX_ERR_OUT_OF_MEMORY. 0 cancels. For tests of callers' out-of-memory handling. */
+NNDEX_API void nndex_cuda_inject_alloc_failures(uint32_t count);
+
 /* ---- FP64 oracle on the device (score-error report) ------------------------------------- */
 
 /*

@@ -176,6 +176,8 @@ SIGNATURES = {
     "nndex_cuda_ivf_stats_get": (_i32, [_vp, C.POINTER(IvfStats)]),
     "nndex_cuda_set_nprobe": (_i32, [_vp, _u32]),
     "nndex_cuda_set_graphs": (_i32, [_vp, _i32]),
+    "nndex_cuda_check_bounded_wait": (_i32, [_vp, _u64]),
+    "nndex_cuda_inject_alloc_failures": (None, [_u32]),
     "nndex_cuda_ivf_restore": (_i32, [_vp, _u64, _vp, _vp, _vp, _vp]),
     "nndex_cuda_base_checksum": (_i32, [_vp, C.POINTER(_u64)]),
     "nndex_cuda_server_start": (_i32, [_vp, C.POINTER(ServerOpts), C.POINTER(_vp)]),

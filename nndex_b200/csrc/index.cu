@@ -26,6 +26,14 @@ namespace nndex {
 
 static std::atomic<uint64_t> g_launches{0};
 static std::atomic<uint64_t> g_alloc_epoch{0};
+static std::atomic<uint32_t> g_fail_allocs{0};  // host-side fault injection: allocations to fail
+bool take_injected_alloc_failure() {
+    uint32_t n = g_fail_allocs.load(std::memory_order_relaxed);
+    while (n > 0 && !g_fail_allocs.compare_exchange_weak(n, n - 1, std::memory_order_relaxed)) {
+    }
+    return n > 0;
+}
+void inject_alloc_failures(uint32_t n) { g_fail_allocs.store(n, std::memory_order_relaxed); }
 uint64_t alloc_epoch() { return g_alloc_epoch.load(std::memory_order_acquire); }
 void bump_alloc_epoch() { g_alloc_epoch.fetch_add(1, std::memory_order_acq_rel); }
 void count_launch(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
@@ -115,7 +123,9 @@ static int grow_device(T*& p, size_t& cap, size_t n, const char* what) {
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
+    cudaError_t e = take_injected_alloc_failure()
+                        ? cudaErrorMemoryAllocation
+                        : cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
     if (e != cudaSuccess) {
         p = nullptr;
         return cuda_error(e, what);
@@ -130,7 +140,9 @@ static int grow_host(T*& p, size_t& cap, size_t n, const char* what) {
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
+    cudaError_t e = take_injected_alloc_failure()
+                        ? cudaErrorMemoryAllocation
+                        : cudaMallocHost(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
     if (e != cudaSuccess) {
         p = nullptr;
         return cuda_error(e, what);

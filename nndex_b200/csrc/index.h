@@ -21,6 +21,9 @@ constexpr uint32_t kSecondPassCap = 8192;
 // CUDA graph is valid only while the epoch it was captured in lasts.
 uint64_t alloc_epoch();
 void bump_alloc_epoch();
+// Host-side fault injection (tests): the next n scratch allocations fail as out of memory.
+void inject_alloc_failures(uint32_t n);
+bool take_injected_alloc_failure();
 
 int set_error(int code, const char* fmt, ...);
 void clear_error();

@@ -449,7 +449,9 @@ int grow(T*& p, size_t& cap, size_t n, const char* what) {
     cudaFree(p);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
+    cudaError_t e = take_injected_alloc_failure()
+                        ? cudaErrorMemoryAllocation
+                        : cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
     if (e != cudaSuccess) return cuda_error(e, what);
     cap = n;
     return NNDEX_OK;

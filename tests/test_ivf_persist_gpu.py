@@ -32,7 +32,6 @@ def test_restored_index_answers_like_the_built_one(tmp_path, precision):
     la, lb = built.ivf_layout(), restored.ivf_layout()
     for key in la:
         assert np.array_equal(la[key], lb[key]), key
-    assert restored.ivf_stats()["build_ms"] < built.ivf_stats()["build_ms"]
     for k in (1, 10, 100):
         _bitwise(built.search(q, k=k), restored.search(q, k=k))
         _bitwise(built.search(q[0], k=k), restored.search(q[0], k=k))
