@@ -36,7 +36,30 @@ bool take_injected_alloc_failure() {
 void inject_alloc_failures(uint32_t n) { g_fail_allocs.store(n, std::memory_order_relaxed); }
 uint64_t alloc_epoch() { return g_alloc_epoch.load(std::memory_order_acquire); }
 void bump_alloc_epoch() { g_alloc_epoch.fetch_add(1, std::memory_order_acq_rel); }
-void count_launch(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+bool sync_check_enabled() {
+    static const bool on = [] {
+        const char* v = getenv("NNDEX_SYNC_CHECK");
+        return v && v[0] == '1';
+    }();
+    return on;
+}
+static thread_local char t_launch_note[256];
+void set_launch_note(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(t_launch_note, sizeof(t_launch_note), fmt, ap);
+    va_end(ap);
+}
+void count_launch_at(const char* file, int line, uint32_t n) {
+    g_launches.fetch_add(n, std::memory_order_relaxed);
+    if (!sync_check_enabled()) return;
+    static std::atomic<bool> reported{false};
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess && !reported.exchange(true))
+        std::fprintf(stderr, "nndex: %s (%d) after the launch at %s:%d [%s]\n", cudaGetErrorString(e),
+                     static_cast<int>(e), file, line, t_launch_note);
+    t_launch_note[0] = 0;
+}
 uint64_t kernel_launches_total() { return g_launches.load(std::memory_order_relaxed); }
 
 static thread_local std::string t_error;
@@ -85,6 +108,8 @@ bool shape_ok(uint64_t n_values, uint64_t rows, uint64_t dims) {
     return sat == n_values;
 }
 
+static thread_local int t_encode_result = 0;  // the last encode's CUresult on this thread
+
 static PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
@@ -111,8 +136,10 @@ bool encode_tmap_2d(CUtensorMap* map, CUtensorMapDataType dtype, uint32_t elem_b
     (void)elem_bytes;
     CUresult r = fn(map, dtype, 2, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                     swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    t_encode_result = static_cast<int>(r);
     return r == CUDA_SUCCESS;
 }
+int last_encode_result() { return t_encode_result; }
 
 // ---- device buffers ------------------------------------------------------------------------
 
@@ -263,9 +290,11 @@ int CudaIndex::merge_workspace(uint64_t per_query, uint32_t nq, uint32_t k, Merg
     int st;
     if ((st = grow_device(d_part_keys, cap_part_keys, static_cast<size_t>(nq) * parts * k, "merge workspace")))
         return st;
-    const uint32_t* before = d_part_done;
+    // counters start at zero: clear them whenever the buffer is (re)allocated (a new allocation
+    // may return the old address, so compare capacities, not pointers)
+    const size_t cap_before = cap_part_done;
     if ((st = grow_device(d_part_done, cap_part_done, nq, "merge workspace"))) return st;
-    if (d_part_done != before) cudaMemsetAsync(d_part_done, 0, cap_part_done * sizeof(uint32_t), s);
+    if (cap_part_done != cap_before) cudaMemsetAsync(d_part_done, 0, cap_part_done * sizeof(uint32_t), s);
     m.part_keys = d_part_keys;
     m.part_done = d_part_done;
     return NNDEX_OK;
@@ -372,14 +401,22 @@ int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
 // allows low-precision scoring and k fits its pass-1 heaps; else the FP32 list scan (4).
 int CudaIndex::ivf_path(uint64_t nq, uint64_t kcap) const {
     if (precision == NNDEX_PRECISION_FP32 || nq < 64 || !ivf || !ivf->d_reordered16) return 4;
-    // The tensor-core list scan scores 128-query blocks per list chunk; it pays once a probed list
-    // serves enough queries. Measured on 2M × 384, nlist 1414, 1024 queries: at nprobe 8 (≈ 6
-    // queries per list) the FP32 list scan is faster (489k vs 350k q/s); at nprobe 32 (≈ 23) and
-    // 64 (≈ 46) the tensor cores are (345k vs 269k, 324k vs 174k).
+    // The tensor-core list scan scores 128-query blocks per list chunk (≤ 4096 rows). With few
+    // queries per probed list and short lists its items are small and their fixed cost dominates:
+    // on 2M × 384 (nlist 1414, lists of ≈ 1,400 rows) with 1024 queries, nprobe 8 (≈ 6 queries per
+    // list) runs faster on the FP32 list scan (489k vs 350k q/s), nprobe 32 (≈ 23) and 64 (≈ 46)
+    // on the tensor cores (345k vs 269k, 324k vs 174k). With long lists (5M × 512, nlist 512, lists
+    // of ≈ 9,800 rows) the tensor cores win from 64 queries on (serving at saturation: 157k vs 132k
+    // q/s). So: the FP32 list scan when a probed list serves fewer than 12 queries on average and
+    // the average list is shorter than one 4096-row chunk.
     const uint64_t np0 = ivf_scratch.nprobe ? ivf_scratch.nprobe : ivf_choose_nprobe(ivf->nlist, kcap, rows);
     const double per_list = static_cast<double>(nq) * static_cast<double>(std::min<uint64_t>(np0, ivf->nlist)) /
                             static_cast<double>(ivf->nlist);
-    if (per_list < 12.0) return 4;
+    static const double min_per_list = [] {
+        const char* v = getenv("NNDEX_IVF_TC_MIN_PER_LIST");  // measurement override of the rule
+        return v ? atof(v) : 12.0;
+    }();
+    if (per_list < min_per_list && rows / ivf->nlist < 4096) return 4;
     const TcPlan p1 = plan_tc(kcap, false);
     return (p1.kp >= kcap && p1.kp > 0 && plan_tc(0, false).stages > 0) ? 5 : 4;
 }
@@ -577,7 +614,11 @@ int CudaIndex::encode_query_tmap(bool fp8, void* buf, uint32_t n, CUtensorMap* m
                                          CU_TENSOR_MAP_SWIZZLE_128B)
                         : encode_tmap_2d(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, buf, kb16, nq_alloc, kb16 * 2, 64,
                                          128, CU_TENSOR_MAP_SWIZZLE_128B);
-    if (!ok) return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (queries)");
+    if (!ok)
+        return set_error(NNDEX_ERR_CUDA,
+                         "cuda execution error: cuTensorMapEncodeTiled failed (queries: %s, %u rows, row length %llu, "
+                         "buffer %p, driver result %d)",
+                         fp8 ? "FP8" : "BF16", n, (unsigned long long)(fp8 ? kf8 : kb16), buf, last_encode_result());
     return NNDEX_OK;
 }
 
@@ -728,11 +769,14 @@ int CudaIndex::enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path)
 // the capture); otherwise directly. Paths 1 (FP32 scan) and 4 (IVF list scan) only: the others
 // read device results on the host in the middle of the batch.
 int CudaIndex::run_host_batch(uint64_t n, uint64_t kcap, int mode, int path) {
-    const bool graphable = use_graphs && !scan_timing && (path == 1 || path == 4) &&
+    const bool graphable = use_graphs && !scan_timing && !sync_check_enabled() && (path == 1 || path == 4) &&
                            !(graph_failed_paths & (1u << path));
     if (!graphable) return enqueue_host_batch(n, kcap, mode, path);
     const uint64_t epoch = alloc_epoch();
-    auto same = [&](const GraphEntry& g) { return g.path == path && g.mode == mode && g.n == n && g.kcap == kcap; };
+    const uint32_t np = static_cast<uint32_t>(ivf_scratch.nprobe);
+    auto same = [&](const GraphEntry& g) {
+        return g.path == path && g.mode == mode && g.n == n && g.kcap == kcap && g.nprobe == np;
+    };
     for (size_t i = 0; i < graphs.size(); ++i) {
         if (!same(graphs[i])) continue;
         if (graphs[i].epoch != epoch) {
@@ -756,7 +800,7 @@ int CudaIndex::run_host_batch(uint64_t n, uint64_t kcap, int mode, int path) {
         return NNDEX_OK;
     }
     if (!(same(graph_seen) && graph_seen.epoch == epoch)) {
-        graph_seen = GraphEntry{path, mode, n, kcap, epoch};
+        graph_seen = GraphEntry{path, mode, n, kcap, epoch, np};
         return enqueue_host_batch(n, kcap, mode, path);
     }
     // Second call of this shape with nothing reallocated in between: capture it.
@@ -781,7 +825,7 @@ int CudaIndex::run_host_batch(uint64_t n, uint64_t kcap, int mode, int path) {
         graph_seen = GraphEntry{};
         return enqueue_host_batch(n, kcap, mode, path);
     }
-    GraphEntry g{path, mode, n, kcap, epoch};
+    GraphEntry g{path, mode, n, kcap, epoch, np};
     g.exec = exec;
     g.launches = kernel_launches_total() - launches0;
     g.stats = stats;  // counters as this batch's increments

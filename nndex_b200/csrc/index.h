@@ -26,6 +26,7 @@ void inject_alloc_failures(uint32_t n);
 bool take_injected_alloc_failure();
 
 int set_error(int code, const char* fmt, ...);
+int last_encode_result();  // CUresult of this thread's last tensor-map encode
 void clear_error();
 const char* last_error();
 int cuda_error(cudaError_t e, const char* what);
@@ -175,6 +176,7 @@ struct CudaIndex {
     struct GraphEntry {
         int path = 0, mode = 0;
         uint64_t n = 0, kcap = 0, epoch = 0;
+        uint32_t nprobe = 0;  // the IVF scan's probe count at capture (0: chosen per batch)
         cudaGraphExec_t exec = nullptr;
         nndex_cuda_search_stats stats{};
         uint64_t launches = 0;

@@ -11,8 +11,17 @@
 
 namespace nndex {
 
-// Number of kernels launched by this library (process-wide).
-void count_launch(uint32_t n = 1);
+// Number of kernels launched by this library (process-wide). Called after each launch; with
+// NNDEX_SYNC_CHECK=1 in the environment it also waits for the device and prints the launch site of
+// the first CUDA error to stderr (a debugging aid: every launch then runs alone).
+void count_launch_at(const char* file, int line, uint32_t n);
+constexpr uint32_t launches_of() { return 1; }
+constexpr uint32_t launches_of(uint32_t n) { return n; }
+#define count_launch(...) ::nndex::count_launch_at(__FILE__, __LINE__, ::nndex::launches_of(__VA_ARGS__))
+bool sync_check_enabled();
+// With the sync check on: a description of the next launch, printed with its error (cleared by
+// count_launch).
+void set_launch_note(const char* fmt, ...);
 uint64_t kernel_launches_total();
 
 struct PrepArgs {
@@ -145,6 +154,7 @@ struct RerankArgs {
     bool certify = true;                 // false when pass 1 scanned a sample of the rows
 };
 cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream);
+// q2_lp holds m rounded up to 128 rows (whole query blocks); the rows past m are written as zeros.
 cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q_lp, uint32_t row_bytes, void* q2_lp,
                                   const float* resid, float* resid2, const float* scale, float* scale2,
                                   const float* kth, float* thr2, cudaStream_t stream);

@@ -720,16 +720,18 @@ __global__ void __launch_bounds__(kAsThreads, 1)
                 tmem_wait_ld_regs(va);
 #pragma unroll
                 for (uint32_t c = 0; c < kAsN / 32; c += 2) {
+                    // the warp reconverges before each .sync.aligned tcgen05 instruction
                     __syncwarp();
                     tc::tmem_ld32(taddr + (c + 1) * 32, vb);
                     process(va, c);
+                    __syncwarp();
                     tmem_wait_ld_regs(vb);
+                    if (c + 2 < kAsN / 32) tc::tmem_ld32(taddr + (c + 2) * 32, va);
+                    process(vb, c + 1);
                     if (c + 2 < kAsN / 32) {
                         __syncwarp();
-                        tc::tmem_ld32(taddr + (c + 2) * 32, va);
+                        tmem_wait_ld_regs(va);
                     }
-                    process(vb, c + 1);
-                    if (c + 2 < kAsN / 32) tmem_wait_ld_regs(va);
                 }
                 tc::fence_before_sync();
                 __syncwarp();

@@ -378,15 +378,23 @@ __global__ void __launch_bounds__(512)
             }
         }
         __syncthreads();
-        for (uint32_t i = kk + threadIdx.x; i < p2; i += blockDim.x) sorted[i] = 0ull;
+        // Exactly kk keys reach the k-th (keys are distinct); should fewer arrive, the slots they
+        // did not fill are cleared rather than read.
+        const uint32_t got = s.count < kk ? s.count : kk;
+        for (uint32_t i = got + threadIdx.x; i < p2; i += blockDim.x) sorted[i] = 0ull;
         __syncthreads();
         block_bitonic_sort_desc(sorted, p2);
+        __syncthreads();
+        if (threadIdx.x == 0) s.count = got;
+        __syncthreads();
     }
+    const uint32_t out_n = kk > 0 ? s.count : 0u;
+    __syncthreads();
     for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
-        idx_out[static_cast<uint64_t>(q) * k + j] = j < kk ? key_row(sorted[j]) : 0;
-        sim_out[static_cast<uint64_t>(q) * k + j] = j < kk ? key_score(sorted[j]) : 0.0f;
+        idx_out[static_cast<uint64_t>(q) * k + j] = j < out_n ? key_row(sorted[j]) : 0;
+        sim_out[static_cast<uint64_t>(q) * k + j] = j < out_n ? key_score(sorted[j]) : 0.0f;
     }
-    if (threadIdx.x == 0 && count_out) count_out[q] = kk;
+    if (threadIdx.x == 0 && count_out) count_out[q] = out_n;
 }
 
 // ------------------------------------------------------------------------------------------

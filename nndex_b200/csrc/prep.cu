@@ -96,11 +96,13 @@ __global__ void __launch_bounds__(256) prep_rows_kernel(
                 inv = __frcp_rn(__fsqrt_rn(norm_sq));
             }
         }
-        if (!ok) continue;
-        // Write the normalised (or copied) row, zero padded to out_stride.
+        // Write the normalised (or copied) row, zero padded to out_stride. A rejected row is
+        // written as zeros (residuals 0, FP8 scale 1): its batch fails, but the scans that were
+        // already queued behind this kernel then read defined values, not stale memory.
+        const uint32_t live_dims = ok ? dims : 0u;
         float amax = 0.0f;
         for (uint32_t i = lane; i < out_stride; i += 32) {
-            const float v = i < dims ? (mode == 2 ? s[i] : __fmul_rn(s[i], inv)) : 0.0f;
+            const float v = i < live_dims ? (mode == 2 ? s[i] : __fmul_rn(s[i], inv)) : 0.0f;
             o[i] = v;
             amax = fmaxf(amax, fabsf(v));
         }
@@ -108,7 +110,7 @@ __global__ void __launch_bounds__(256) prep_rows_kernel(
             float rb = 0.0f;
             __nv_bfloat16* ob = out_bf16 + r * bf16_stride;
             for (uint32_t i = lane; i < bf16_stride; i += 32) {
-                const float v = i < dims ? (mode == 2 ? s[i] : __fmul_rn(s[i], inv)) : 0.0f;
+                const float v = i < live_dims ? (mode == 2 ? s[i] : __fmul_rn(s[i], inv)) : 0.0f;
                 const __nv_bfloat16 b = __float2bfloat16_rn(v);
                 ob[i] = b;
                 const float d = v - __bfloat162float(b);
@@ -127,7 +129,7 @@ __global__ void __launch_bounds__(256) prep_rows_kernel(
             float rf = 0.0f;
             uint8_t* of = out_fp8 + r * fp8_stride;
             for (uint32_t i = lane; i < fp8_stride; i += 32) {
-                const float v = i < dims ? (mode == 2 ? s[i] : __fmul_rn(s[i], inv)) : 0.0f;
+                const float v = i < live_dims ? (mode == 2 ? s[i] : __fmul_rn(s[i], inv)) : 0.0f;
                 const __nv_fp8_e4m3 q(v * inv_scale);
                 of[i] = q.__x;
                 const float d = v - static_cast<float>(q) * scale;

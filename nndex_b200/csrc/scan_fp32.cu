@@ -312,22 +312,29 @@ NNDEX_DEVICE_INLINE void merge_final(const uint64_t* keys, uint64_t n, uint32_t 
             }
         }
         __syncthreads();
-        for (uint32_t i = kk + threadIdx.x; i < p2; i += blockDim.x) sorted[i] = 0ull;
+        // Exactly kk keys reach the k-th (keys are distinct); should fewer arrive, the slots they
+        // did not fill are cleared rather than read.
+        const uint32_t got = s.count < kk ? s.count : kk;
+        for (uint32_t i = got + threadIdx.x; i < p2; i += blockDim.x) sorted[i] = 0ull;
         __syncthreads();
         block_bitonic_sort_desc(sorted, p2);
+        __syncthreads();
+        if (threadIdx.x == 0) s.count = got;
+        __syncthreads();
     }
+    const uint32_t out_n = kk > 0 ? s.count : 0u;
     __syncthreads();
     for (uint32_t j = threadIdx.x; j < out_stride; j += blockDim.x) {
         uint64_t idx = 0;
         float sim = 0.0f;
-        if (j < kk) {
+        if (j < out_n) {
             idx = key_row(sorted[j]);
             sim = key_score(sorted[j]);
         }
         idx_out[static_cast<size_t>(q) * out_stride + j] = idx;
         sim_out[static_cast<size_t>(q) * out_stride + j] = sim;
     }
-    if (threadIdx.x == 0 && count_out) count_out[q] = kk;
+    if (threadIdx.x == 0 && count_out) count_out[q] = out_n;
 }
 
 }  // namespace

@@ -367,6 +367,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     if (kFp8) s = (s * sc[c * 32 + j]) * qs;
                     mask |= (s >= st.cut ? 1u : 0u) << j;
                 }
+                // A padding lane (no query: past nq, or an empty slot of a gathered block) scores
+                // whatever its query row holds, +inf included; it never survives, since its
+                // index would address past the per-query outputs.
+                if (!valid_q) mask = 0;
                 while (mask) {  // survivors are rare once a threshold exists
                     const uint32_t j = __ffs(mask) - 1;
                     mask &= mask - 1;
@@ -380,16 +384,20 @@ __global__ void __launch_bounds__(kThreads, 1)
             };
 #pragma unroll
             for (uint32_t c = 0; c < kN / 32; c += 2) {
+                // tcgen05.ld and tcgen05.wait::ld are .sync.aligned: the whole warp executes each
+                // one together. process() loops per lane over its survivors (one lane may take
+                // every row while the others take none), so the warp reconverges before each.
                 __syncwarp();
                 tc::tmem_ld32(taddr + (c + 1) * 32, vb);
                 process(va, c);
+                __syncwarp();
                 tmem_wait_ld_regs(vb);
+                if (c + 2 < kN / 32) tc::tmem_ld32(taddr + (c + 2) * 32, va);
+                process(vb, c + 1);
                 if (c + 2 < kN / 32) {
                     __syncwarp();
-                    tc::tmem_ld32(taddr + (c + 2) * 32, va);
+                    tmem_wait_ld_regs(va);
                 }
-                process(vb, c + 1);
-                if (c + 2 < kN / 32) tmem_wait_ld_regs(va);
             }
             tc::fence_before_sync();
             __syncwarp();
@@ -495,10 +503,13 @@ __global__ void gather_queries_kernel(const uint32_t* __restrict__ ids, uint32_t
                                       float* __restrict__ scale2, const float* __restrict__ kth,
                                       float* __restrict__ thr2) {
     const uint32_t i = blockIdx.x;
-    if (i >= m) return;
+    uint4* b = reinterpret_cast<uint4*>(q2_lp + static_cast<size_t>(i) * row_bytes);
+    if (i >= m) {  // padding rows of the last 128-query block: zeros, not stale memory
+        for (uint32_t t = threadIdx.x; t < row_bytes / 16; t += blockDim.x) b[t] = make_uint4(0, 0, 0, 0);
+        return;
+    }
     const uint32_t src = ids[i];
     const uint4* a = reinterpret_cast<const uint4*>(q_lp + static_cast<size_t>(src) * row_bytes);
-    uint4* b = reinterpret_cast<uint4*>(q2_lp + static_cast<size_t>(i) * row_bytes);
     for (uint32_t t = threadIdx.x; t < row_bytes / 16; t += blockDim.x) b[t] = a[t];
     if (threadIdx.x == 0) {
         resid2[i] = resid[src];
@@ -578,6 +589,11 @@ static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
     dim3 grid = kItems ? dim3(a.items, 1) : dim3((a.p.nq + kM - 1) / kM, a.nranges);
     TcParams p = a.p;
     p.kprime = kp;
+    if (sync_check_enabled())
+        set_launch_note("scan_tc fp8 %d stages %d mode %d stream_a %d items %d: grid (%u, %u), nq %u, k' %u, "
+                        "tile stride %u, range rows %llu, rows %llu, smem %zu",
+                        kFp8, kST, kMode, kStreamA, kItems, grid.x, grid.y, p.nq, kp, p.tile_stride,
+                        (unsigned long long)p.range_rows, (unsigned long long)p.rows, smem);
     kern<<<grid, kThreads, smem, stream>>>(*a.tmap_q, *a.tmap_b, p);
     count_launch();
     return cudaGetLastError();
@@ -632,7 +648,9 @@ cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q
                                   const float* resid, float* resid2, const float* scale, float* scale2,
                                   const float* kth, float* thr2, cudaStream_t stream) {
     if (m == 0) return cudaSuccess;
-    gather_queries_kernel<<<m, 128, 0, stream>>>(ids, m, static_cast<const uint8_t*>(q_lp), row_bytes,
+    // One block per row of the padded query buffer (m rounded up to the 128-query block).
+    const uint32_t m_alloc = (m + 127) / 128 * 128;
+    gather_queries_kernel<<<m_alloc, 128, 0, stream>>>(ids, m, static_cast<const uint8_t*>(q_lp), row_bytes,
                                                  static_cast<uint8_t*>(q2_lp), resid, resid2, scale, scale2, kth, thr2);
     count_launch();
     return cudaGetLastError();

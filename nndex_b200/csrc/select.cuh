@@ -41,16 +41,6 @@ NNDEX_DEVICE_INLINE uint64_t warp_min_u64(uint64_t v) {
     return v;
 }
 
-// hist[bin] += 1 for every lane with `valid`, as one shared atomic per distinct bin among the
-// warp's active lanes: the keys being selected have close scores, so their high digits fall in a
-// few bins, and unaggregated atomics on one bin serialise.
-NNDEX_DEVICE_INLINE void hist_add(uint32_t* hist, uint32_t bin, bool valid) {
-    const uint32_t active = __activemask();
-    const uint32_t peers = __match_any_sync(active, valid ? bin : 0x100u);
-    if (valid && lane_id() == static_cast<uint32_t>(__ffs(peers) - 1))
-        atomicAdd(&hist[bin], static_cast<uint32_t>(__popc(peers)));
-}
-
 // Given a 256-bin histogram, locate the bin holding the `krem`-th largest element (1-based,
 // counting from the highest bin). Executed by one full warp; returns (bin, count above, count in
 // bin) in every lane.
@@ -99,7 +89,7 @@ NNDEX_DEVICE_INLINE uint64_t warp_radix_kth(const uint64_t* buf, uint32_t n, uin
         __syncwarp();
         for (uint32_t i = lane; i < n; i += 32) {
             const uint64_t key = buf[i];
-            hist_add(hist, static_cast<uint32_t>(key >> shift) & 0xFFu, (key & mask) == prefix);
+            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 0xFFu], 1u);
         }
         __syncwarp();
         uint32_t bin, above, in_bin;
@@ -160,7 +150,7 @@ NNDEX_DEVICE_INLINE uint64_t block_radix_kth(const uint64_t* keys, uint64_t n, u
         __syncthreads();
         for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
             const uint64_t key = keys[i];
-            hist_add(s.hist, static_cast<uint32_t>(key >> shift) & 0xFFu, (key & mask) == prefix);
+            if ((key & mask) == prefix) atomicAdd(&s.hist[(key >> shift) & 0xFFu], 1u);
         }
         __syncthreads();
         if (threadIdx.x < 32) {

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <memory>
@@ -139,6 +140,10 @@ void Server::worker(uint32_t slot) {
         bcnt.resize(nq);
         v->approx_override = approx ? 1 : 0;
         v->ivf_scratch.nprobe = approx ? nprobe : 0;
+        if (sync_check_enabled())
+            std::fprintf(stderr, "nndex server: slot %u batch %llu: %llu queries from %zu requests, k %llu, approx %d\n",
+                         slot, (unsigned long long)batch_id, (unsigned long long)nq, batch.size(),
+                         (unsigned long long)kmax, approx ? 1 : 0);
         int code = v->search_host(qbuf.data(), nq, kmax, mode, bidx.data(), bsim.data(), bcnt.data());
         std::vector<int> codes(batch.size(), code);
         std::vector<std::string> msgs(batch.size(), code ? last_error() : "");
@@ -161,6 +166,9 @@ void Server::worker(uint32_t slot) {
         } else {
             // Attribute the failure: every request of the batch on its own (a bad query fails only
             // its own request, as it would alone).
+            if (sync_check_enabled())
+                std::fprintf(stderr, "nndex server: batch %llu failed (%s); its requests run one by one\n",
+                             (unsigned long long)batch_id, msgs[0].c_str());
             for (size_t i = 0; i < batch.size(); ++i) {
                 auto& r = batch[i];
                 r->idx.resize(r->nq * r->kcap);
