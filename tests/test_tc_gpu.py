@@ -118,3 +118,29 @@ def test_tc_alone_equals_in_batch():
         si, ss = index.search(q[lo:lo + 5].copy(), k=10)
         assert np.array_equal(si, bi[lo:lo + 5])
         assert np.array_equal(ss, bs[lo:lo + 5])
+
+
+def test_pass2_padding_lanes_ignore_stale_memory():
+    # Pass 2 scores whole 128-query blocks; the lanes past the last uncertified query are padding.
+    # Device memory freed by earlier work is refilled with BF16 +inf patterns first, so that new
+    # scratch buffers are likely to start with them. Against a base of strictly positive values a
+    # +inf query row scores +inf on every row. The padding lanes must still never survive: the
+    # result equals the FP32 path's.
+    import torch
+
+    rng = np.random.default_rng(21)
+    m = np.abs(mixture(rng, 40_000, 128, 128, 0.25)) + np.float32(0.05)
+    q = np.abs(mixture(np.random.default_rng(22), 200, 128, 128, 0.25)) + np.float32(0.05)
+    index = NNdex(m, precision="bf16")
+    index.set_precision("fp32")
+    fi, fs = index.search(q, k=10)
+    junk = torch.full((1 << 29,), 0x7F80, dtype=torch.int16, device="cuda")  # 1 GiB of BF16 +inf
+    torch.cuda.synchronize()
+    del junk
+    torch.cuda.empty_cache()
+    index.set_precision("bf16", rerank_width=10)  # k' = k: most queries need pass 2
+    ti, ts = index.search(q, k=10)
+    st = index.last_search_stats()
+    assert st["path"] == 2 and st["second_pass_queries"] > 0, st
+    assert np.array_equal(ti, fi)
+    assert np.max(np.abs(ts - fs)) <= 1e-5
