@@ -220,7 +220,7 @@ struct ScanConsumerWide {
 
     uint32_t lane, rg, dg, warp;
     uint32_t x_base0, x_base1;  // row chunk address (stage 0) for rows i = 0, 2 and i = 1, 3
-    const float4* q_base;       // this lane's chunk of query 0 in slab 0
+    uint32_t q_base;            // shared address of this lane's chunk of query 0 in slab 0
 
     NNDEX_DEVICE_INLINE ScanConsumerWide(uint32_t warp_, uint32_t lane_, const uint8_t* stage_base, const float* q_s)
         : lane(lane_), warp(warp_) {
@@ -230,7 +230,7 @@ struct ScanConsumerWide {
         const uint32_t row0 = warp * 16 + rg;
         x_base0 = smem_u32(stage_base) + row0 * 128 + ((dg ^ rg) * 16);
         x_base1 = smem_u32(stage_base) + (row0 + 4) * 128 + ((dg ^ (rg + 4)) * 16);
-        q_base = reinterpret_cast<const float4*>(q_s) + dg;
+        q_base = smem_u32(q_s) + dg * 16;
     }
 
     NNDEX_DEVICE_INLINE void load_rows(float4 (&x)[4], RingPos<ST> r) const {
@@ -250,17 +250,17 @@ struct ScanConsumerWide {
         }
     }
 
-    // acc += the products of rows x and queries [4·G0, 4·G1) at q (chunk dg), in component order.
-    // The queries are written once before the consumers start: plain loads, which the compiler
-    // may schedule among the FMAs. Four queries at a time: 16 independent FMAs separate the
-    // dependent ones of an accumulator.
+    // acc += the products of rows x and queries [4·G0, 4·G1) at shared address q (chunk dg), in
+    // component order. The queries are written once before the consumers start; explicit
+    // shared-memory loads (the address space is not left for the compiler to infer). Four queries
+    // at a time: 16 independent FMAs separate the dependent ones of an accumulator.
     template <int G0, int G1>
-    NNDEX_DEVICE_INLINE static void fma_groups(float (&acc)[4][QB], const float4 (&x)[4], const float4* q) {
+    NNDEX_DEVICE_INLINE static void fma_groups(float (&acc)[4][QB], const float4 (&x)[4], uint32_t q) {
 #pragma unroll
         for (int b0 = kGQ * G0; b0 < kGQ * G1; b0 += kGQ) {
             float4 qv[kGQ];
 #pragma unroll
-            for (int j = 0; j < kGQ; ++j) qv[j] = q[(b0 + j) * 8];
+            for (int j = 0; j < kGQ; ++j) qv[j] = lds128(q + (b0 + j) * 128);
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -289,7 +289,7 @@ struct ScanConsumerWide {
     // (and the row loads it guards) comes after them, so neither the test nor the loads' latency
     // holds up the FMA stream.
     NNDEX_DEVICE_INLINE void slab(float (&acc)[4][QB], const float4 (&x)[4], float4 (&xn)[4], bool more,
-                                  RingPos<ST> cur, const float4* q, uint64_t* full_bar, uint64_t* empty_bar,
+                                  RingPos<ST> cur, uint32_t q, uint64_t* full_bar, uint64_t* empty_bar,
                                   volatile uint32_t* abort_flag, uint32_t* status) const {
         const RingPos<ST> nxt = cur.next();
         const bool ready = !more || mbar_try_wait(&full_bar[nxt.s], nxt.phase);
@@ -317,16 +317,16 @@ struct ScanConsumerWide {
         float4 xa[4], xb[4];
         wait_full(full_bar, pos, abort_flag, status);
         load_rows(xa, pos);
-        const float4* q = q_base;
+        uint32_t q = q_base;
 #pragma unroll 1
         for (uint32_t bx = 0; bx < nbox; bx += 2) {
             slab(acc, xa, xb, bx + 1 < nbox, pos, q, full_bar, empty_bar, abort_flag, status);
             pos = pos.next();
-            q += kQSlabBytes / 16;
+            q += kQSlabBytes;
             if (bx + 1 >= nbox) break;
             slab(acc, xb, xa, bx + 2 < nbox, pos, q, full_bar, empty_bar, abort_flag, status);
             pos = pos.next();
-            q += kQSlabBytes / 16;
+            q += kQSlabBytes;
         }
     }
 
