@@ -367,7 +367,8 @@ def run_ours(args):
             "queries_per_s": total_q / (max_ms / 1e3),
             "scan_ms": scan_ms.value / max(scan_n.value, 1),
             "launches": n1 - n0,
-            "kernel": (f"scan_fp32_wide_kernel<{sst.scan_qb},{sst.scan_wide}>" if sst.scan_wide
+            "kernel": ("scan_tf32_kernel (FP32-accurate TF32 candidates + exact rerank)" if sst.path == 6
+                       else f"scan_fp32_wide_kernel<{sst.scan_qb},{sst.scan_wide}>" if sst.scan_wide
                        else f"scan_fp32_kernel<{sst.scan_qb},4>"),
         }
         if bi == 0:

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -233,6 +234,8 @@ CudaIndex::~CudaIndex() {
     cudaFree(d_q_fp8);
     cudaFree(d_q_scale);
     cudaFree(d_q_resid);
+    cudaFree(d_qtb);
+    cudaFree(d_qts);
     cudaFree(d_thr);
     cudaFree(d_cand_idx);
     cudaFree(d_cand_sim);
@@ -382,8 +385,12 @@ int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
         const TcPlan p1 = plan_tc(kcap, fp8);
         return p1.kp >= kcap && p1.kp > 0 && plan_tc(0, fp8).stages > 0;
     };
+    // 9–16 queries with NNDEX_TF32_SCAN=1: the TF32 candidate scan, which reads the same FP32 base
+    // and returns the same bits (opt-in: on 1M × 768 at 16 queries it is shared-memory-bound and
+    // slower than the FP32 scan, 0.85 against 0.77 ms per scan).
+    const int fp32_path = plan_tf32(nq, kcap).kp ? 6 : 1;
     switch (precision) {
-        case NNDEX_PRECISION_FP32: return 1;
+        case NNDEX_PRECISION_FP32: return fp32_path;
         case NNDEX_PRECISION_BF16: return (has16 && tc_ok(false)) ? 2 : 1;
         case NNDEX_PRECISION_FP8: return (has8 && tc_ok(true)) ? 3 : 1;
         default:
@@ -393,8 +400,40 @@ int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
                 if (has16 && tc_ok(false)) return 2;
                 if (has8 && tc_ok(true)) return 3;
             }
-            return 1;
+            return fp32_path;
     }
+}
+
+CudaIndex::Tf32Plan CudaIndex::plan_tf32(uint64_t nq, uint64_t kcap) const {
+    const char* opt = getenv("NNDEX_TF32_SCAN");  // 1: the TF32 candidate scan at 9–16 queries
+    const bool enabled = opt && opt[0] == '1';
+    Tf32Plan p;
+    if (!enabled || nq < 9 || nq > 16 || kcap == 0 || kcap > 128) return p;
+    // k′: twice k, at least k + 32, so that the k-th exact score clears the k′-th bound
+    const uint64_t kp = std::min<uint64_t>(256, std::max<uint64_t>(2 * kcap, kcap + 32));
+    if (rows < 4 * kp || rows > 0xFFFFFFFFull) return p;
+    // Room for three tiles of survivors above k′: a selection runs once ≥ 256 keys have
+    // accumulated since the last one, not after every tile.
+    const uint32_t cap = static_cast<uint32_t>(kp) + 3 * 128;
+    const uint32_t stages = tf32_stages_for(cap, smem_optin);
+    if (!stages) return p;
+    p.kp = static_cast<uint32_t>(kp);
+    p.cap = cap;
+    p.stages = stages;
+    return p;
+}
+
+// Upper bound of |FP32 scan-order score − s̃| for unit rows and queries (Σ|x_i q_i| ≤ 1):
+//   the split, three products each off by < 2⁻²⁰·|x_i q_i|:                 3·2⁻²⁰
+//   the FP32 scan's own rounding (eight chains of ds/8 FMAs, then 3 adds):  (ds/8 + 3)·2⁻²⁴
+//   the tensor core's FP32 accumulation, as for the BF16 scan (each of the 3·ds products
+//   added with up to one FP32 rounding, 4× margin):                          4·3·ds·2⁻²³
+//   and the rounding of s̃ + ε itself:                                      2⁻²³
+float CudaIndex::tf32_eps() const {
+    const double d = static_cast<double>(ds);
+    const double e = 3.0 * std::ldexp(1.0, -20) + (d / 8.0 + 3.0) * std::ldexp(1.0, -24) +
+                     12.0 * d * std::ldexp(1.0, -23) + std::ldexp(1.0, -23);
+    return static_cast<float>(e * 1.01);
 }
 
 // IVF batches: the tensor-core list scan (5) from a few dozen queries, when the index's precision
@@ -706,12 +745,17 @@ int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_si
         if (!h_ok2[i]) failed.push_back(h_ids[i]);
     stats.fp32_fallback_queries = static_cast<uint32_t>(failed.size());
     if (failed.empty()) return NNDEX_OK;
-
     // ---- FP32 scan for queries whose collected set overflowed ----
-    const uint32_t mf = static_cast<uint32_t>(failed.size());
+    return rerun_exact_fp32(failed, kcap, o_idx, o_sim, o_cnt, s);
+}
+
+int CudaIndex::rerun_exact_fp32(const std::vector<uint32_t>& qs, uint32_t kcap, uint64_t* o_idx, float* o_sim,
+                                uint32_t* o_cnt, cudaStream_t s) {
+    int st;
+    const uint32_t mf = static_cast<uint32_t>(qs.size());
     if ((st = grow_device(d_qsub, cap_qsub, static_cast<uint64_t>(mf) * ds, "fallback buffer"))) return st;
     for (uint32_t i = 0; i < mf; ++i)
-        cudaMemcpyAsync(d_qsub + static_cast<uint64_t>(i) * ds, d_qn + static_cast<uint64_t>(failed[i]) * ds,
+        cudaMemcpyAsync(d_qsub + static_cast<uint64_t>(i) * ds, d_qn + static_cast<uint64_t>(qs[i]) * ds,
                         ds * sizeof(float), cudaMemcpyDeviceToDevice, s);
     if ((st = grow_device(d_fb_idx, cap_fb_idx, static_cast<uint64_t>(mf) * kcap, "fallback buffer"))) return st;
     if ((st = grow_device(d_fb_sim, cap_fb_sim, static_cast<uint64_t>(mf) * kcap, "fallback buffer"))) return st;
@@ -720,16 +764,114 @@ int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_si
     if ((st = enqueue_exact_fp32(d_qsub, mf, kcap, kcap, d_fb_idx, d_fb_sim, d_fb_cnt, s))) return st;
     stats.path = path;
     for (uint32_t i = 0; i < mf; ++i) {
-        const uint64_t q = failed[i];
+        const uint64_t q = qs[i];
         cudaMemcpyAsync(o_idx + q * kcap, d_fb_idx + static_cast<uint64_t>(i) * kcap, kcap * sizeof(uint64_t),
                         cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(o_sim + q * kcap, d_fb_sim + static_cast<uint64_t>(i) * kcap, kcap * sizeof(float),
                         cudaMemcpyDeviceToDevice, s);
         if (o_cnt) cudaMemcpyAsync(o_cnt + q, d_fb_cnt + i, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     }
-    e = cudaStreamSynchronize(s);
+    const cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(e, "search");
     return NNDEX_OK;
+}
+
+// K12 (9–16 queries, FP32 precision): split the queries, the TF32 candidate scan, the merge of each
+// query's per-CTA candidates, and the exact rerank with its certificate into the outputs.
+int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                            cudaStream_t s) {
+    int st;
+    const Tf32Plan plan = plan_tf32(n, kcap);
+    if (!plan.kp) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: no TF32 scan plan for k=%u", kcap);
+    const uint32_t kp = plan.kp;
+    const uint32_t nq_alloc = (n + 15) / 16 * 16;
+    const uint32_t ctas = static_cast<uint32_t>(sm_count);
+    const uint64_t per_query = static_cast<uint64_t>(ctas) * kp;
+    if ((st = grow_device(d_qtb, cap_qtb, static_cast<uint64_t>(nq_alloc) * ds, "query buffer"))) return st;
+    if ((st = grow_device(d_qts, cap_qts, static_cast<uint64_t>(nq_alloc) * ds, "query buffer"))) return st;
+    if ((st = grow_device(d_ws, cap_ws, per_query * n, "scan workspace"))) return st;
+    if ((st = grow_device(d_cand_idx, cap_cand_idx, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
+    if ((st = grow_device(d_cand_sim, cap_cand_sim, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
+    if ((st = grow_device(d_cand_cnt, cap_cand_cnt, n, "tc workspace"))) return st;
+    if ((st = grow_device(d_cert, cap_cert, n, "tc workspace"))) return st;
+    if ((st = grow_device(d_kth, cap_kth, n, "tc workspace"))) return st;
+    CUtensorMap tmap_qb, tmap_qs;
+    if (!encode_tmap_2d(&tmap_qb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, d_qtb, ds, nq_alloc, ds * sizeof(float), 32, 16,
+                        CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !encode_tmap_2d(&tmap_qs, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, d_qts, ds, nq_alloc, ds * sizeof(float), 32, 16,
+                        CU_TENSOR_MAP_SWIZZLE_128B))
+        return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (split queries, driver "
+                                         "result %d)", last_encode_result());
+    cudaError_t e = launch_split_queries_tf32(d_qn, n, static_cast<uint32_t>(ds), nq_alloc, d_qtb, d_qts, s);
+    if (e != cudaSuccess) return cuda_error(e, "query split launch");
+    Tf32ScanArgs a;
+    a.nq = n;
+    a.nbox = static_cast<uint32_t>(ds / 32);
+    a.rows = rows;
+    a.kp = kp;
+    a.cap = plan.cap;
+    a.eps = tf32_eps();
+    a.ws_keys = d_ws;
+    a.status = d_status;
+    cudaEvent_t ev_a = nullptr;
+    scan_event_begin(s, ev_a);
+    e = launch_scan_tf32(tmap_f32, tmap_qb, tmap_qs, a, plan.stages, ctas, s);
+    scan_event_end(s, ev_a);
+    if (e != cudaSuccess) return cuda_error(e, "TF32 scan launch");
+    MergeArgs m;
+    m.ws_keys = d_ws;
+    m.nq = n;
+    m.per_query = per_query;
+    m.k = kp;
+    m.out_stride = kp;
+    m.idx_out = d_cand_idx;
+    m.sim_out = d_cand_sim;
+    m.count_out = d_cand_cnt;
+    if ((st = merge_workspace(per_query, n, kp, m, s))) return st;
+    if ((e = launch_merge_topk(m, s)) != cudaSuccess) return cuda_error(e, "merge launch");
+    RerankArgs r;
+    r.base = d_base;
+    r.ds = static_cast<uint32_t>(ds);
+    r.queries = d_qn;
+    r.cand_idx = d_cand_idx;
+    r.cand_sim = d_cand_sim;
+    r.cand_cnt = d_cand_cnt;
+    r.nq = n;
+    r.kp = kp;
+    r.k = kcap;
+    r.idx_out = o_idx;
+    r.sim_out = o_sim;
+    r.cnt_out = o_cnt;
+    r.cert_out = d_cert;
+    r.kth_out = d_kth;
+    r.certify = true;
+    if ((e = launch_rerank(r, s)) != cudaSuccess) return cuda_error(e, "rerank launch");
+    stats.kernel_launches += 4;
+    stats.path = 6;
+    stats.rerank_width = kp;
+    stats.rows_scanned += rows * n;
+    return NNDEX_OK;
+}
+
+int CudaIndex::finish_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                           cudaStream_t s) {
+    int st;
+    if ((st = grow_host(h_cert, cap_hcert, n, "pinned buffer"))) return st;
+    cudaMemcpyAsync(h_cert, d_cert, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    h_flags[1] = 0;
+    cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_error(e, "search");
+    if ((st = check_device_words())) return st;
+    last_tc_n = n;
+    std::vector<uint32_t> failed;
+    for (uint32_t i = 0; i < n; ++i)
+        if (!h_cert[i]) failed.push_back(i);
+    stats.certified = failed.empty() ? 1u : 0u;
+    stats.fp32_fallback_queries = static_cast<uint32_t>(failed.size());
+    if (failed.empty()) return NNDEX_OK;
+    return rerun_exact_fp32(failed, kcap, o_idx, o_sim, o_cnt, s);
 }
 
 // Enqueues one batch of the host-buffer search on `stream` (the queries already in h_q): status
@@ -751,6 +893,11 @@ int CudaIndex::enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path)
     } else if (path == 1) {
         if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
                                      static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
+            return st;
+    } else if (path == 6) {
+        if ((st = enqueue_tf32(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
+            return st;
+        if ((st = finish_tf32(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
             return st;
     } else {
         if ((st = enqueue_tc(path == 3, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
@@ -915,6 +1062,11 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
             if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
                                          static_cast<uint32_t>(kcap), oi, os, oc, s)))
                 return st;
+        } else if (path == 6) {
+            // the certificate's fallback needs the host: these batches synchronise
+            if ((st = enqueue_tf32(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s))) return st;
+            if ((st = finish_tf32(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s))) return st;
+            synced = true;
         } else {
             // The certificate's fallback needs the host: tensor-core batches always synchronise.
             if ((st = enqueue_tc(path == 3, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s)))
@@ -1435,7 +1587,8 @@ int nndex_cuda_last_candidates(nndex_cuda_index* index, uint64_t query_rows, uin
     cudaSetDevice(ix->device);
     const uint32_t kp = ix->stats.rerank_width;
     if (kprime) *kprime = kp;
-    if (eps_rows) *eps_rows = ix->stats.path == 3 ? ix->eps_fp8 : ix->eps_bf16;
+    if (eps_rows)
+        *eps_rows = ix->stats.path == 3 ? ix->eps_fp8 : ix->stats.path == 6 ? ix->tf32_eps() : ix->eps_bf16;
     if (kp == 0 || !ix->d_cand_idx) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: no low-precision search yet");
     const uint64_t n = query_rows * kp;
     if (n > capacity || n > ix->cap_cand_idx)

@@ -77,6 +77,10 @@ struct CudaIndex {
     size_t cap_q_fp8 = 0;
     float* d_q_scale = nullptr;
     size_t cap_q_scale = 0;
+    float* d_qtb = nullptr;  // K12: TF32 heads and remainders of the normalised queries
+    size_t cap_qtb = 0;
+    float* d_qts = nullptr;
+    size_t cap_qts = 0;
     float* d_q_resid = nullptr;
     size_t cap_q_resid = 0;
     unsigned long long* d_thr = nullptr;
@@ -205,8 +209,15 @@ struct CudaIndex {
                     uint64_t* counts_out);
     int search_device(const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out, float* d_sim_out,
                       uint32_t* d_cnt_out, cudaStream_t s, int synchronize);
-    // Path choice for a batch: 1 = FP32 scan, 2 = BF16 tensor-core scan, 3 = FP8 tensor-core scan.
+    // Path choice for a batch: 1 = FP32 scan, 2 = BF16 tensor-core scan, 3 = FP8 tensor-core scan,
+    // 6 = FP32-accurate TF32 candidate scan + exact rerank (9–16 queries).
     int choose_path(uint64_t nq, uint64_t kcap) const;
+    // K12's plan for k results: candidates per query and CTA (0: no plan), buffer, ring depth.
+    struct Tf32Plan {
+        uint32_t kp = 0, cap = 0, stages = 0;
+    };
+    Tf32Plan plan_tf32(uint64_t nq, uint64_t kcap) const;
+    float tf32_eps() const;
     int ivf_path(uint64_t nq, uint64_t kcap) const;
     struct TcPlan {
         uint32_t kp = 0;        // pass-1 heap entries per query (0: no plan)
@@ -224,6 +235,13 @@ struct CudaIndex {
     // After a tensor-core batch has completed: re-run the queries whose certificate failed on the
     // FP32 path (device outputs are patched in place). Synchronises the stream.
     int finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
+    int enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
+    // After a TF32 candidate batch: the queries whose certificate failed run on the FP32 scan.
+    // Synchronises the stream.
+    int finish_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
+    // The FP32 scan for the listed queries (rows of d_qn), written into their output slots.
+    int rerun_exact_fp32(const std::vector<uint32_t>& qs, uint32_t kcap, uint64_t* o_idx, float* o_sim,
+                         uint32_t* o_cnt, cudaStream_t s);
     int stream_status();
     int enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path);
     int run_host_batch(uint64_t n, uint64_t kcap, int mode, int path);

@@ -138,6 +138,28 @@ size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp
 uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, bool stream_a, size_t smem_limit);
 cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t stream);
 
+// K12: FP32-accurate candidate scan on the tensor cores (three TF32 products per K step), 16
+// queries per CTA; per query and CTA the kp best keys of (s̃ + eps, row) go to ws_keys.
+struct Tf32ScanArgs {
+    uint32_t nq = 0;
+    uint32_t nbox = 0;                 // 128-byte slabs per row (ds / 32)
+    uint64_t rows = 0;
+    uint32_t kp = 0;                   // candidates kept per query and CTA
+    uint32_t cap = 0;                  // candidate buffer per query, ≥ kp + 128
+    float eps = 0.0f;                  // bound on |FP32 scan-order score − s̃|
+    uint64_t* ws_keys = nullptr;       // nq × ctas × kp
+    uint32_t* status = nullptr;
+};
+size_t tf32_smem_bytes(uint32_t stages, uint32_t cap);
+uint32_t tf32_stages_for(uint32_t cap, size_t smem_limit);
+// tmap_x: the FP32 base, box {32 floats, 128 rows}, 128-byte swizzle; tmap_qb / tmap_qs: the split
+// queries (nq rounded up to 16 rows), box {32 floats, 16 rows}, 128-byte swizzle.
+cudaError_t launch_scan_tf32(const CUtensorMap& tmap_x, const CUtensorMap& tmap_qb, const CUtensorMap& tmap_qs,
+                             const Tf32ScanArgs& a, uint32_t stages, uint32_t ctas, cudaStream_t stream);
+// qb / qs (nq_alloc × ds): the TF32 head and the rest of each normalised query value; padding rows 0.
+cudaError_t launch_split_queries_tf32(const float* qn, uint32_t nq, uint32_t ds, uint32_t nq_alloc, float* qb,
+                                      float* qs, cudaStream_t stream);
+
 struct RerankArgs {
     const float* base = nullptr;  // FP32 base, stride ds
     uint32_t ds = 0;

@@ -401,6 +401,9 @@ NNDEX_DEVICE_INLINE void scan_flush_g(bool last, uint32_t nqg, uint32_t k, uint3
     for (int b = 0; b < QB; ++b)
         if (static_cast<uint32_t>(b) < nqg) need |= last ? (cnt[b] > k) : (cnt[b] + kTileRows > cap);
     if (!need) return;
+    // Every consumer has read the counts (and so made the same decision) before any warp
+    // rewrites them: a warp that read a count already compacted would skip the barrier below.
+    named_bar_sync(1, kConsumers * 32);
     for (uint32_t b = warp; b < nqg; b += kConsumers) {
         const uint32_t n = cnt[b] < cap ? cnt[b] : cap;
         if (n > k) {

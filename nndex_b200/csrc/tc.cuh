@@ -61,6 +61,26 @@ NNDEX_DEVICE_INLINE void mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, ui
     }
 }
 
+// D[tmem] (+)= A[smem] · B[smem]ᵀ with TF32 inputs (32-bit containers; the MMA uses the sign,
+// exponent and top 10 mantissa bits), issued by one thread.
+NNDEX_DEVICE_INLINE void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                  uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z)
+        : "memory");
+}
+
+// kind::tf32, F32 accumulate, both K-major (A and B format 2 = TF32).
+template <int M, int N>
+__host__ __device__ constexpr uint32_t instr_desc_tf32() {
+    return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+           (static_cast<uint32_t>(M >> 4) << 24);
+}
+
 // The mbarrier at `bar` receives one arrival when every tcgen05 operation this thread issued
 // before the commit has completed.
 NNDEX_DEVICE_INLINE void commit(uint64_t* bar) {
@@ -98,6 +118,26 @@ NNDEX_DEVICE_INLINE void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         : "memory");
 }
 NNDEX_DEVICE_INLINE void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Each thread of the warp reads 16 consecutive 32-bit columns of its own TMEM lane.
+NNDEX_DEVICE_INLINE void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr)
+        : "memory");
+}
+// tcgen05.wait::ld that also ties the 16 registers of the completed load.
+NNDEX_DEVICE_INLINE void tmem_wait_ld16(uint32_t (&v)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                   "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
+                   "+r"(v[15])
+                 :
+                 : "memory");
+}
 
 }  // namespace tc
 }  // namespace nndex

@@ -1,0 +1,79 @@
+"""FP32-accurate TF32 candidate scan (batches of 9-16 queries) against the FP32 scan and the FP64
+oracle (needs a B200).
+
+With NNDEX_TF32_SCAN=1, batches of 9 to 16 queries take the tensor-core candidate scan with the
+exact rerank; batches of 8 or fewer take the FP32 scan. A certified query's rows and scores are
+the FP32 scan's, bit for bit (the rerank sums in the FP32 scan's order); an uncertified one is
+re-run on the FP32 scan. So each query of a 16-query batch must equal its result from two
+8-query batches, bit for bit.
+"""
+import numpy as np
+import pytest
+
+from nndex_b200 import NNdex
+from oracle import oracle as O
+from tests._parity import assert_topk_matches
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def tf32_scan_on(monkeypatch):
+    # the TF32 candidate scan is opt-in (read on every search)
+    monkeypatch.setenv("NNDEX_TF32_SCAN", "1")
+
+
+def mixture(rng, rows, dims, centers, sigma, center_seed=77):
+    c = np.random.default_rng(center_seed).normal(size=(centers, dims)).astype(np.float32)
+    a = rng.integers(0, centers, size=rows)
+    return (c[a] + np.float32(sigma) * rng.normal(size=(rows, dims)).astype(np.float32)).astype(np.float32)
+
+
+CASES = [
+    # rows, dims, nq, k, data
+    (200_000, 768, 16, 100, "mixture"),
+    (100_003, 256, 16, 10, "mixture"),
+    (50_000, 100, 9, 1, "gauss"),      # dims padded to 128, 9 queries
+    (30_001, 128, 13, 128, "gauss"),   # rows not a multiple of the 128-row tile, largest k
+]
+
+
+@pytest.mark.parametrize("rows,dims,nq,k,data", CASES)
+def test_tf32_scan_equals_fp32_scan(rows, dims, nq, k, data):
+    rng = np.random.default_rng(rows + dims)
+    if data == "mixture":
+        m = mixture(rng, rows, dims, 256, 0.3)
+        q = mixture(np.random.default_rng(5), nq, dims, 256, 0.3)
+    else:
+        m = rng.normal(size=(rows, dims)).astype(np.float32)
+        q = rng.normal(size=(nq, dims)).astype(np.float32)
+    index = NNdex(m)
+    ti, ts = index.search(q, k=k)
+    st = index.last_search_stats()
+    assert st["path"] == 6, st
+    assert st["rerank_width"] >= k
+    parts = [index.search(q[lo:lo + 8].copy(), k=k) for lo in range(0, nq, 8)]
+    assert index.last_search_stats()["path"] == 1
+    fi = np.vstack([p[0] for p in parts])
+    fs = np.vstack([p[1] for p in parts])
+    np.testing.assert_array_equal(ti, fi)
+    np.testing.assert_array_equal(ts.view(np.uint32), fs.view(np.uint32))
+    # and against the FP64 oracle on a few queries
+    _, base = O.prepare_index(m, False)
+    _, qn = O.prepare_queries(q, False, base.shape[1])
+    for i in range(0, nq, 4):
+        assert_topk_matches(ti[i], ts[i], O.scores_f64(base, qn[i]), k, what=f"tf32 q{i}")
+
+
+def test_tf32_scan_certifies_the_benchmark_mixture():
+    # the C2 distribution (1,024 centres, sigma 0.3, unit rows) at k = 100: every query certifies,
+    # so no FP32 re-run
+    rng = np.random.default_rng(12)
+    m = mixture(rng, 300_000, 768, 1024, 0.3, center_seed=1)
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    q = mixture(np.random.default_rng(13), 16, 768, 1024, 0.3, center_seed=1)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    index = NNdex(m, normalized=True)
+    index.search(q, k=100)
+    st = index.last_search_stats()
+    assert st["path"] == 6 and st["fp32_fallback_queries"] == 0, st
