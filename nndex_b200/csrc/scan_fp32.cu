@@ -101,7 +101,9 @@ __global__ void __launch_bounds__(ScanShape<QB, NCW>::kThreads, 1)
         // ---------------- producer ----------------
         if (lane == 0) {
             tma_prefetch_desc(&tmap);
-            const uint64_t policy = l2_policy_evict_first();
+            // One query group streams each row once: evict first. Several groups read the same
+            // rows at about the same time (one wave, the groups' CTAs side by side): keep them.
+            const uint64_t policy = gridDim.y > 1 ? l2_policy_evict_normal() : l2_policy_evict_first();
             uint32_t it = 0;
             bool stop = false;
             for (uint32_t t = 0; t < ntiles && !stop; ++t) {
@@ -219,7 +221,9 @@ __global__ void __launch_bounds__((W + 1) * 32, 1)
         // ---------------- producer ----------------
         if (lane == 0) {
             tma_prefetch_desc(&tmap);
-            const uint64_t policy = l2_policy_evict_first();
+            // One query group streams each row once: evict first. Several groups read the same
+            // rows at about the same time (one wave, the groups' CTAs side by side): keep them.
+            const uint64_t policy = gridDim.y > 1 ? l2_policy_evict_normal() : l2_policy_evict_first();
             uint32_t it = 0;
             bool stop = false;
             for (uint32_t t = 0; t < ntiles && !stop; ++t) {
