@@ -751,7 +751,14 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     ix.stats.certified = m == 0 ? 1u : 0u;
     ix.stats.second_pass_queries = m;
     ix.stats.pass1_tile_stride = stride;
-    if (stride == 1 && m * 2 > nq) w.tc_stride = 4;
+    if (stride == 1 && m * 2 > nq) {
+        static const uint32_t sampled = [] {
+            const char* v = getenv("NNDEX_IVF_TC_STRIDE");  // measurement override of the sampled stride
+            const uint32_t x = v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
+            return x >= 2 && x <= 16 ? x : 4u;
+        }();
+        w.tc_stride = sampled;
+    }
     if (m == 0) return NNDEX_OK;
 
     // ---- pass 2: every probed row whose bound reaches T, for the uncertified queries ----
