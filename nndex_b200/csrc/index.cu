@@ -405,10 +405,10 @@ int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
 }
 
 CudaIndex::Tf32Plan CudaIndex::plan_tf32(uint64_t nq, uint64_t kcap) const {
-    const char* opt = getenv("NNDEX_TF32_SCAN");  // 1: the TF32 candidate scan at 9–16 queries
-    const bool enabled = opt && opt[0] == '1';
     Tf32Plan p;
-    if (!enabled || nq < 9 || nq > 16 || kcap == 0 || kcap > 128) return p;
+    if (nq < 9 || nq > 16 || kcap == 0 || kcap > 128) return p;
+    const char* opt = getenv("NNDEX_TF32_SCAN");  // 1: the TF32 candidate scan at 9–16 queries
+    if (!(opt && opt[0] == '1')) return p;
     // k′: twice k, at least k + 32, so that the k-th exact score clears the k′-th bound
     const uint64_t kp = std::min<uint64_t>(256, std::max<uint64_t>(2 * kcap, kcap + 32));
     if (rows < 4 * kp || rows > 0xFFFFFFFFull) return p;
