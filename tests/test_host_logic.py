@@ -50,3 +50,35 @@ def test_oracle_ivf_from_layout_equals_built():
     q = storage[:5]
     ra, rb = a.search(q, 10, 4), b.search(q, 10, 4)
     assert np.array_equal(ra[0], rb[0]) and np.array_equal(ra[1], rb[1])
+
+
+def test_tf32_split_error_term():
+    # The TF32 candidate scan's split: x = xb + xs with xb = x's top 10 mantissa bits (exact in
+    # TF32) and xs = x - xb (exact in FP32); likewise q. It computes xb·qb + xb·T(qs) + T(xs)·qb,
+    # where T keeps 10 mantissa bits (truncation or rounding). Each product is then off by less
+    # than 3·2^-20·|x_i q_i|: the split part of the certificate's bound. Checked in exact
+    # arithmetic (float64 holds these products exactly) on unit vectors, worst case over T.
+    rng = np.random.default_rng(3)
+
+    def head(v):
+        return (v.view(np.uint32) & np.uint32(0xFFFFE000)).view(np.float32)
+
+    def rne10(v):  # round to nearest, 10 mantissa bits
+        u = v.view(np.uint32).astype(np.uint64)
+        u = (u + 0xFFF + ((u >> 13) & 1)) & 0xFFFFE000
+        return u.astype(np.uint32).view(np.float32)
+
+    for _ in range(20):
+        x = rng.normal(size=768).astype(np.float32)
+        q = rng.normal(size=768).astype(np.float32)
+        x /= np.linalg.norm(x)
+        q /= np.linalg.norm(q)
+        xb, qb = head(x), head(q)
+        xs, qs = (x - xb).astype(np.float32), (q - qb).astype(np.float32)
+        assert np.array_equal(xb.astype(np.float64) + xs, x.astype(np.float64))  # the split is exact
+        for t in (head, rne10):
+            prod = (xb.astype(np.float64) * qb + xb.astype(np.float64) * t(qs) + t(xs).astype(np.float64) * qb)
+            err = np.abs(prod - x.astype(np.float64) * q.astype(np.float64))
+            bound = 3 * 2.0 ** -20 * np.abs(x.astype(np.float64) * q.astype(np.float64))
+            assert np.all(err <= bound)
+        assert np.abs((x.astype(np.float64) * q).sum()) <= 1 + 1e-6
