@@ -102,7 +102,9 @@ typedef struct nndex_cuda_devinfo {
 /* Search-side statistics of the last call on this index (per index, not thread-local). */
 typedef struct nndex_cuda_search_stats {
     uint32_t path;             /* 1 = FP32 scan, 2 = BF16 scan+rerank, 3 = FP8 scan+rerank,
-                                  4 = IVF probe + rerank                                     */
+                                  4 = IVF probe + rerank, 5 = IVF list scan on the tensor
+                                  cores + rerank, 6 = TF32 candidate scan + rerank
+                                  (NNDEX_TF32_SCAN=1, 9-16 queries)                           */
     uint32_t kernel_launches;  /* kernels this library launched for the call                */
     uint32_t rerank_width;     /* k' of a low-precision scan's first pass (0 otherwise)     */
     uint32_t certified;        /* 1 = every query certified after the first pass            */
@@ -110,7 +112,8 @@ typedef struct nndex_cuda_search_stats {
     uint32_t nprobe;           /* IVF lists probed per query                                */
     uint64_t rows_scanned;     /* base rows scored (sum over queries for IVF)               */
     double   device_ms;        /* CUDA-event time of the device part of the call            */
-    uint32_t fp32_fallback_queries; /* queries re-run on the FP32 scan (pass-2 overflow)   */
+    uint32_t fp32_fallback_queries; /* queries re-run on the FP32 scan (pass-2 overflow, or
+                                       an uncertified query of path 6)                       */
     uint32_t pass1_tile_stride;     /* first pass scanned every n-th 256-row tile (1 = all) */
     uint64_t ivf_rows_streamed;     /* IVF: rows read by the list scan (a list once per query group) */
     uint64_t ivf_rows_union;        /* IVF: rows in the union of the probed lists               */
