@@ -83,3 +83,29 @@ def test_ctypes_structs_match_the_c_compiler(tmp_path):
         for field, _ in cls._fields_:
             assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)
 
+
+
+def test_null_index_is_refused_without_touching_the_device():
+    # Every entry point that takes an index checks it before any CUDA call, so a wrapper that
+    # passes NULL gets NNDEX_ERR_INVALID_ARGUMENT and a message, also on a machine without a GPU.
+    L = _lib.lib()
+    u64, f32 = C.c_uint64(), C.c_float()
+    st = _lib.SearchStats()
+    calls = [
+        ("search", lambda: L.nndex_cuda_search(None, None, 0, 1, None, None, None)),
+        ("search_batch", lambda: L.nndex_cuda_search_batch(None, None, 0, 0, 1, None, None, None)),
+        ("search_batch_device", lambda: L.nndex_cuda_search_batch_device(None, None, 0, 0, 1, None, None, None,
+                                                                         None, 1)),
+        ("set_precision", lambda: L.nndex_cuda_set_precision(None, 0, 0)),
+        ("stream_status", lambda: L.nndex_cuda_stream_status(None)),
+        ("last_search_stats", lambda: L.nndex_cuda_last_search_stats(None, C.byref(st))),
+        ("rows", lambda: L.nndex_cuda_rows(None, C.byref(u64), C.byref(u64), C.byref(u64))),
+        ("base_checksum", lambda: L.nndex_cuda_base_checksum(None, C.byref(u64))),
+        ("set_nprobe", lambda: L.nndex_cuda_set_nprobe(None, 8)),
+        ("set_graphs", lambda: L.nndex_cuda_set_graphs(None, 1)),
+        ("set_scan_timing", lambda: L.nndex_cuda_set_scan_timing(None, 1)),
+    ]
+    for name, call in calls:
+        code = call()
+        assert code == _lib.NNDEX_ERR_INVALID_ARGUMENT, (name, code, _lib.last_error())
+        assert "null" in _lib.last_error(), (name, _lib.last_error())
