@@ -104,7 +104,12 @@ def test_null_index_is_refused_without_touching_the_device():
         ("set_nprobe", lambda: L.nndex_cuda_set_nprobe(None, 8)),
         ("set_graphs", lambda: L.nndex_cuda_set_graphs(None, 1)),
         ("set_scan_timing", lambda: L.nndex_cuda_set_scan_timing(None, 1)),
+        ("server_start", lambda: L.nndex_cuda_server_start(None, None, C.byref(C.c_void_p()))),
+        ("server_submit", lambda: L.nndex_cuda_server_submit(None, None, 1, 1, 1, 0, 0, C.byref(u64))),
+        ("server_poll", lambda: L.nndex_cuda_server_poll(None, 1, 0, None, None, None, None)),
+        ("server_stats", lambda: L.nndex_cuda_server_stats_get(None, C.byref(_lib.ServerStats()))),
     ]
+    L.nndex_cuda_server_stop(None)  # a no-op
     for name, call in calls:
         code = call()
         assert code == _lib.NNDEX_ERR_INVALID_ARGUMENT, (name, code, _lib.last_error())
