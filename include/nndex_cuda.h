@@ -293,9 +293,11 @@ NNDEX_API uint64_t nndex_cuda_kernel_launch_count(void);
  * synchronize = 1 (it returns after the results are written). Its scratch memory is one
  * file-scope device array of NNDEX_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
  * until exit; a batch whose normalised queries and candidate keys do not fit is rejected with
- * NNDEX_ERR_UNSUPPORTED. The first call on a device looks up the array's address (make it before
- * any stream capture). All calls share the array: calls that overlap on the GPU race. Indexes that
- * answer through an IVF (NNDEX_FLAG_APPROX) are rejected with NNDEX_ERR_UNSUPPORTED.
+ * NNDEX_ERR_UNSUPPORTED (batches above 16,384 queries run in pieces of 16,384, each of which must
+ * fit). Creating an index binds the array on the index's device (with lazy module loading that is
+ * when the GPU takes its memory), so a search never does. All calls share the array: calls that
+ * overlap on the GPU race. Indexes that answer through an IVF (NNDEX_FLAG_APPROX) are rejected
+ * with NNDEX_ERR_UNSUPPORTED.
  */
 NNDEX_API int nndex_cuda_search_batch_device_noalloc(nndex_cuda_index* index, const float* dev_queries,
                                                      uint64_t query_rows, uint64_t query_dims, uint64_t k,

@@ -8,6 +8,7 @@ include/nndex_cuda.h. nvcc cross-compiles for sm_100a without a GPU, so this run
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -43,17 +44,21 @@ def _stale() -> bool:
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
     if not force and not _stale():
         return OUT
-    objs = []
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
+    jobs = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         cmd = [NVCC, *ARCH, *FLAGS, *(extra or []), "-I", CSRC, "-I", os.path.join(ROOT, "include"),
                "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+        jobs.append((cmd, obj))
+    # one nvcc per source file, as many at once as there are host cores
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(subprocess.run, cmd, check=True) for cmd, _ in jobs]:
+            f.result()
+    objs = [obj for _, obj in jobs]
     tmp = OUT + ".tmp"
     cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart_static", "-ldl", "-lrt", "-lpthread",
            "-Xcompiler", "-fPIC"]

@@ -377,7 +377,7 @@ int CudaIndex::check_device_words() {
     return NNDEX_OK;
 }
 
-// ---- path choice (the autotuner's rules; see autotune notes in DESIGN) ---------------------
+// ---- path choice (rules by batch size, k and the index's copies) ----------------------------
 
 int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
     const bool has16 = d_base_bf16 != nullptr, has8 = d_base_fp8 != nullptr;
@@ -1148,6 +1148,9 @@ int index_begin(uint64_t rows, uint64_t dims, uint32_t flags, const nndex_cuda_o
     if (st) return st;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    // The no-allocation entry point's array is bound here, on the index's device: with lazy module
+    // loading its memory is taken when its address is first looked up.
+    if ((st = noalloc_bind(device))) return st;
 
     CudaIndex* ix = new (std::nothrow) CudaIndex();
     if (!ix) return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: host allocation failed");

@@ -260,6 +260,9 @@ void index_prep_rows(CudaIndex* ix, const float* d_src, uint64_t row0, uint64_t 
 int index_finish(CudaIndex* ix);  // deletes ix on failure
 int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out,
                           float* d_sim_out, uint32_t* d_cnt_out, cudaStream_t s);
+// Looks up the no-allocation array's address on `device` (current), which loads the module that
+// holds it; index creation calls it so that the array's memory is taken then, not at a first search.
+int noalloc_bind(int device);
 
 }  // namespace nndex
 

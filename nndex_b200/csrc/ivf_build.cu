@@ -14,10 +14,13 @@
 //     the minima and the threshold search are exact: every distance is a multiple of 2^-24, so FP64
 //     sums below 2^29 carry no rounding and any summation order gives the reference's value.
 //   * assignment: a tcgen05 FP16 GEMM rows × centroids (M = 128 rows in TMEM lanes, N = 256
-//     centroids) whose epilogue keeps each row's best four approximate scores. A row whose runner-up
-//     trails by more than twice its error bound has a certain argmax; a row with at most three
-//     scores inside that window is decided by exact dots with those candidates; the rest are
-//     re-scored exactly against every centroid (FP64, index order) with the reference's tie rule.
+//     centroids), run twice. Pass A keeps each row's best approximate score s1. Pass B repeats the
+//     GEMM and lists every centroid whose approximate score reaches s1 − 2e (e = the row's error
+//     bound); every other centroid scores strictly lower, exactly. A row with one listed centroid
+//     is assigned to it; a row with at most 32 is decided by one warp with exact FP64 dots against
+//     those candidates (highest f32 score, lowest index on a tie: the reference's strict `>` in
+//     index order); a row with more, or with a non-finite bound, is re-scored exactly against every
+//     centroid.
 //     FP16 (11-bit significand) suits unit rows and centroids: its error bound is 8× tighter than
 //     BF16's. Values in FP16's subnormal range count as lost in the residual, so the bound holds
 //     whether the tensor core keeps or flushes them; an overflow makes the bound infinite (or NaN),

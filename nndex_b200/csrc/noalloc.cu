@@ -14,9 +14,12 @@
 // words that must start clean are reset by each call. Calls whose work overlaps on the GPU (from
 // two threads, or on two streams) race on the array and must be serialised by the caller.
 //
-// Set-up: the first call on a device, with that device current, looks up the array's device
-// address with cudaGetSymbolAddress (host code cannot use the array's name as a device address)
-// and caches it. Make that first call on each device before any stream capture begins.
+// Set-up: creating an index looks up the array's device address on the index's device, with that
+// device current, through cudaGetSymbolAddress (host code cannot use the array's name as a device
+// address) and caches it. With lazy module loading (the CUDA default since 12.2) that lookup is
+// what loads the array onto the GPU, so its memory is taken when the index is created, alongside
+// the index's own allocations, and never by a search. Batches run in pieces of at most 16,384
+// queries (as the allocating entry point runs them), each reusing the array.
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
@@ -52,34 +55,46 @@ int scratch_address(int device, unsigned char** out) {
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 }  // namespace
 
+int noalloc_bind(int device) {
+    unsigned char* p = nullptr;
+    return scratch_address(device, &p);
+}
+
 int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out,
                           float* d_sim_out, uint32_t* d_cnt_out, cudaStream_t s) {
     std::lock_guard<std::mutex> lock(ix->mu);
     cudaError_t e = cudaSetDevice(ix->device);
     if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+    ix->stats = nndex_cuda_search_stats{};
     if (ix->uses_ivf())
         return set_error(NNDEX_ERR_UNSUPPORTED,
                          "cuda execution error: the no-allocation entry point serves exact indexes only");
     if (!s) s = cudaStreamLegacy;
-    ix->order_after_previous(s);
     const uint64_t kcap = std::min<uint64_t>(k, ix->rows);
-    ScanPlan plan;
-    if (kcap > kMaxFusedK ||
-        !plan_scan_fp32(static_cast<uint32_t>(nq), static_cast<uint32_t>(ix->ds), static_cast<uint32_t>(kcap),
-                        ix->sm_count, ix->smem_optin, plan))
-        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k=%llu above the fused top-k limit %u",
-                         (unsigned long long)kcap, kMaxFusedK);
+    // Batches run in pieces of at most kMaxBatchChunk queries, as the allocating entry point runs
+    // them (the merge's grid holds one row of blocks per query); every piece reuses the array, so
+    // the largest piece must fit.
+    const uint64_t chunk_max = std::min<uint64_t>(nq, kMaxBatchChunk);
+    const uint64_t chunk_last = nq - (nq - 1) / kMaxBatchChunk * kMaxBatchChunk;
     // Scratch layout: [status words | normalised queries | per-CTA candidate keys].
     const size_t words = 256;
-    const size_t qbytes = align256(static_cast<size_t>(nq) * ix->ds * sizeof(float));
-    const uint64_t per_query = static_cast<uint64_t>(plan.ctas_per_group) * kcap;
-    const size_t wsbytes = static_cast<size_t>(per_query) * nq * sizeof(uint64_t);
+    const size_t qbytes = align256(static_cast<size_t>(chunk_max) * ix->ds * sizeof(float));
+    size_t wsbytes = 0;
+    for (uint64_t n : {chunk_max, chunk_last}) {
+        ScanPlan plan;
+        if (kcap > kMaxFusedK ||
+            !plan_scan_fp32(static_cast<uint32_t>(n), static_cast<uint32_t>(ix->ds), static_cast<uint32_t>(kcap),
+                            ix->sm_count, ix->smem_optin, plan))
+            return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k=%llu above the fused top-k limit %u",
+                             (unsigned long long)kcap, kMaxFusedK);
+        wsbytes = std::max(wsbytes, static_cast<size_t>(plan.ctas_per_group) * kcap * n * sizeof(uint64_t));
+    }
     const size_t need = words + qbytes + wsbytes;
     if (need > NNDEX_NOALLOC_SCRATCH_BYTES)
         return set_error(NNDEX_ERR_UNSUPPORTED,
                          "cuda execution error: %llu queries with k=%llu need %zu bytes of scratch, above the %zu "
                          "bytes the no-allocation entry point holds; split the batch",
-                         (unsigned long long)nq, (unsigned long long)kcap, need,
+                         (unsigned long long)chunk_max, (unsigned long long)kcap, need,
                          static_cast<size_t>(NNDEX_NOALLOC_SCRATCH_BYTES));
     unsigned char* scratch = nullptr;
     int st = scratch_address(ix->device, &scratch);
@@ -89,41 +104,62 @@ int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, ui
     float* d_qn = reinterpret_cast<float*>(scratch + words);
     uint64_t* d_ws = reinterpret_cast<uint64_t*>(scratch + words + qbytes);
 
+    ix->order_after_previous(s);
+    // From here on work is enqueued on the shared array: every return marks the stream, so the
+    // next call (on any stream) is ordered after it.
+    auto fail = [&](int code) {
+        ix->mark_done(s);
+        return code;
+    };
     // The array keeps the previous call's contents: reset the words that must start clean.
     cudaMemsetAsync(d_err, 0xFF, sizeof(unsigned long long), s);
     cudaMemsetAsync(d_status, 0, sizeof(uint32_t), s);
-    PrepArgs p;
-    p.src = d_queries;
-    p.rows = nq;
-    p.dims = static_cast<uint32_t>(ix->dims);
-    p.out = d_qn;
-    p.out_stride = static_cast<uint32_t>(ix->ds);
-    p.mode = ix->normalized ? 2 : 0;
-    p.err = d_err;
-    p.sm_count = ix->sm_count;
-    launch_prep_rows(p, s);
-    ScanArgs a;
-    a.tmap = &ix->tmap_f32;
-    a.tmap_tile = &ix->tmap_f32_176;
-    a.tmap_112 = &ix->tmap_f32_112;
-    a.queries = d_qn;
-    a.nq = static_cast<uint32_t>(nq);
-    a.dq = static_cast<uint32_t>(ix->ds);
-    a.rows = ix->rows;
-    a.k = static_cast<uint32_t>(kcap);
-    a.ws_keys = d_ws;
-    a.status = d_status;
-    if ((e = launch_scan_fp32(a, plan, s)) != cudaSuccess) return cuda_error(e, "scan launch");
-    MergeArgs m;
-    m.ws_keys = d_ws;
-    m.nq = static_cast<uint32_t>(nq);
-    m.per_query = per_query;
-    m.k = static_cast<uint32_t>(kcap);
-    m.out_stride = static_cast<uint32_t>(kcap);
-    m.idx_out = d_idx_out;
-    m.sim_out = d_sim_out;
-    m.count_out = d_cnt_out;
-    if ((e = launch_merge_topk(m, s)) != cudaSuccess) return cuda_error(e, "merge launch");
+    for (uint64_t q0 = 0; q0 < nq; q0 += kMaxBatchChunk) {
+        const uint64_t n = std::min<uint64_t>(kMaxBatchChunk, nq - q0);
+        ScanPlan pl;
+        if (!plan_scan_fp32(static_cast<uint32_t>(n), static_cast<uint32_t>(ix->ds), static_cast<uint32_t>(kcap),
+                            ix->sm_count, ix->smem_optin, pl))
+            return fail(set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: no scan plan for %llu queries",
+                                  (unsigned long long)n));
+        const uint64_t per_query = static_cast<uint64_t>(pl.ctas_per_group) * kcap;
+        PrepArgs p;
+        p.src = d_queries + q0 * ix->dims;
+        p.rows = n;
+        p.dims = static_cast<uint32_t>(ix->dims);
+        p.out = d_qn;
+        p.out_stride = static_cast<uint32_t>(ix->ds);
+        p.mode = ix->normalized ? 2 : 0;
+        p.err = d_err;
+        p.sm_count = ix->sm_count;
+        launch_prep_rows(p, s);
+        ScanArgs a;
+        a.tmap = &ix->tmap_f32;
+        a.tmap_tile = &ix->tmap_f32_176;
+        a.tmap_112 = &ix->tmap_f32_112;
+        a.queries = d_qn;
+        a.nq = static_cast<uint32_t>(n);
+        a.dq = static_cast<uint32_t>(ix->ds);
+        a.rows = ix->rows;
+        a.k = static_cast<uint32_t>(kcap);
+        a.ws_keys = d_ws;
+        a.status = d_status;
+        if ((e = launch_scan_fp32(a, pl, s)) != cudaSuccess) return fail(cuda_error(e, "scan launch"));
+        MergeArgs m;
+        m.ws_keys = d_ws;
+        m.nq = static_cast<uint32_t>(n);
+        m.per_query = per_query;
+        m.k = static_cast<uint32_t>(kcap);
+        m.out_stride = static_cast<uint32_t>(kcap);
+        m.idx_out = d_idx_out + q0 * kcap;
+        m.sim_out = d_sim_out + q0 * kcap;
+        m.count_out = d_cnt_out ? d_cnt_out + q0 : nullptr;
+        if ((e = launch_merge_topk(m, s)) != cudaSuccess) return fail(cuda_error(e, "merge launch"));
+        ix->stats.kernel_launches += 3;
+        ix->stats.rows_scanned += ix->rows * n;
+        ix->stats.scan_qb = pl.qb;
+        ix->stats.scan_wide = pl.wide;
+    }
+    ix->stats.path = 1;
     // h_flags is pinned host memory the index allocated when it was created.
     ix->h_flags[1] = 0;
     cudaMemcpyAsync(&ix->h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);

@@ -136,7 +136,9 @@ def unit_cases() -> dict:
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the nndex reference checkout>")
+    ref = sys.argv[1]
     g = demo_golden(ref)
     rng = np.random.default_rng(42)
     m = rng.normal(size=(50000, 128)).astype(np.float32)

@@ -159,7 +159,7 @@ def test_ivf_recall_equals_reference_approx():
     # src/lib.rs:962-1021 (4096 × 64 uniform(-1, 1), k = 20, reference nlist/nprobe policy). The
     # reference asserts ≥ 14 of 20 for one ChaCha8 draw, which numpy cannot reproduce; on numpy draws
     # of the same distribution the restated reference IVF keeps ≈ 11 of 20 on average. The GPU index
-    # is the same index, so its overlap equals the restatement's on every draw (
+    # is the same index, so its overlap equals the restatement's on every draw (the acceptance bar:
     # recall no lower than the reference approx mode at the same nlist/nprobe/seed).
     gpu, ref_ov = [], []
     for seed in range(6):

@@ -1,6 +1,6 @@
 """Exact-search parity of the CUDA backend against the CPU oracle (needs a B200).
 
-Every call goes through nndex_b200.NNdex → libnndex_cuda.so's C ABI. Acceptance (north-star rule):
+Every call goes through nndex_b200.NNdex → libnndex_cuda.so's C ABI. Acceptance rule:
 scores within 1e-5 absolute of the FP64 score of the returned row, and indices bit-exact wherever
 the FP64 gap between neighbouring ranks exceeds 1e-5 (ties → lower index); see tests/_parity.py.
 """

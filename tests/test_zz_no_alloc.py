@@ -81,3 +81,23 @@ def test_noalloc_reports_query_errors():
                                                            out_s.data_ptr(), None, None)
     assert st == 0, _lib.last_error()
     assert out_i.cpu().numpy()[:, 0].tolist() == [0, 1]
+
+
+def test_noalloc_large_low_dim_batch_runs_in_pieces():
+    """70,000 queries of 8 dims at k = 1 fit the array but exceed one launch's row of merge blocks
+    (65,535): the batch runs in pieces of 16,384 queries like the allocating entry point's, with
+    the same results, and the call's statistics describe this call."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(77)
+    index = NNdex(rng.normal(size=(3000, 8)).astype(np.float32))
+    q = torch.from_numpy(rng.normal(size=(70_000, 8)).astype(np.float32)).cuda()
+    ai, asim, acnt = _call("alloc", index, q, 1, torch)
+    ni, nsim, ncnt = _call("noalloc", index, q, 1, torch)
+    assert np.array_equal(ni, ai)
+    assert np.max(np.abs(nsim - asim)) <= TOL
+    assert np.array_equal(ncnt, acnt) and np.all(ncnt == 1)
+    st = _lib.SearchStats()
+    assert _lib.lib().nndex_cuda_last_search_stats(index.handle, C.byref(st)) == 0
+    assert st.path == 1
+    assert st.kernel_launches == 3 * 5  # prep, scan and merge for each of 5 pieces
+    assert st.rows_scanned == 3000 * 70_000
