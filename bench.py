@@ -55,6 +55,9 @@ def parse_args(argv=None):
     p.add_argument("--extra-batches", default="1,4", help="batch sizes reported beside the headline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-batches", type=int, default=2)
+    p.add_argument("--c1", choices=["on", "off", "only"], default="on",
+                   help="the 50,000 x 128 plain exact section (single query and batch 64, k=10)")
+    p.add_argument("--c1-calls", type=int, default=300)
     p.add_argument("--mixed", choices=["on", "off", "only"], default="on",
                    help="also measure the mixed-precision workload (BF16/FP8 scan + FP32 rerank vs FP32)")
     p.add_argument("--mixed-rows", type=int, default=10_000_000)
@@ -64,7 +67,7 @@ def parse_args(argv=None):
     p.add_argument("--mixed-batch", type=int, default=4096)
     p.add_argument("--mixed-k", type=int, default=10)
     p.add_argument("--mixed-steps", type=int, default=5)
-    p.add_argument("--mixed-oracle-queries", type=int, default=32)
+    p.add_argument("--mixed-oracle-queries", type=int, default=512)
     p.add_argument("--ivf", choices=["on", "off", "only"], default="on",
                    help="also measure the IVF workload (GPU k-means build + probe + ragged list scan)")
     p.add_argument("--ivf-rows", type=int, default=2_000_000)
@@ -90,6 +93,8 @@ def parse_args(argv=None):
     p.add_argument("--serve-seconds", type=float, default=2.0)
     p.add_argument("--serve-slots", type=int, default=3)
     p.add_argument("--serve-nprobe", type=int, default=32)
+    p.add_argument("--serve-latency-ms", type=int, default=150,
+                   help="server latency budget: requests whose queue would take longer to drain are refused")
     return p.parse_args(argv)
 
 
@@ -286,6 +291,8 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     seed = replica_seed(args.seed, rank)
     L = _lib.lib()
+    if args.c1 == "only":
+        return {"c1": run_c1(args, dev, L, world)} if rank == 0 else None
     if args.mixed == "only":
         # the mixed-precision section alone (profiling runs of the tensor-core scan)
         mixed = run_mixed(args, dev, L, world)
@@ -361,13 +368,16 @@ def run_ours(args):
         L.nndex_cuda_scan_timing(h, C.byref(scan_ms), C.byref(scan_n))
         sst = _lib.SearchStats()
         L.nndex_cuda_last_search_stats(h, C.byref(sst))
+        serr = score_error_report(L, h, lambda: L.nndex_cuda_search_batch_device(
+            h, qall[:b].data_ptr(), b, args.dims, k, out_i.data_ptr(), out_s.data_ptr(), out_c.data_ptr(), sptr, 1))
         max_ms, total_q = aggregate(ms, b * args.steps, world, dev)
         results[b] = {
             "ms_per_step": max_ms / args.steps,
             "queries_per_s": total_q / (max_ms / 1e3),
             "scan_ms": scan_ms.value / max(scan_n.value, 1),
             "launches": n1 - n0,
-            "kernel": ("scan_tf32_kernel (FP32-accurate TF32 candidates + exact rerank)" if sst.path == 6
+            "score_error_vs_fp64": serr,
+            "kernel": ("scan_tf32_kernel (TF32 candidates + exact FP32 rerank)" if sst.path == 6
                        else f"scan_fp32_wide_kernel<{sst.scan_qb},{sst.scan_wide}>" if sst.scan_wide
                        else f"scan_fp32_kernel<{sst.scan_qb},4>"),
         }
@@ -415,6 +425,7 @@ def run_ours(args):
     L.nndex_cuda_destroy(h)
     del qall
     torch.cuda.empty_cache()
+    c1 = run_c1(args, dev, L, world) if args.c1 != "off" else None
     mixed = run_mixed(args, dev, L, world) if args.mixed != "off" else None
     ivf = run_ivf(args, dev, L, world) if args.ivf != "off" else None
     serve = run_serve(args, dev, L, world) if args.serve != "off" else None
@@ -454,16 +465,134 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
+        "c1": c1,
         "mixed_precision": mixed,
         "ivf": ivf,
         "serving": serve,
         "batches": {str(bb): {"queries_per_s": r["queries_per_s"], "ms_per_step": r["ms_per_step"],
                               "scan_ms": r["scan_ms"], "kernel": r["kernel"],
+                              "score_error_vs_fp64": r["score_error_vs_fp64"],
                               "hbm_gbs": (args.rows * args.dims * 4 + bb * args.dims * 4 + bb * k * 12)
                               / (r["scan_ms"] / 1e3) / 1e9}
                     for bb, r in results.items()},
     }
     return line
+
+
+# ---------------------------------------------------------------------------------------------
+# plain exact search on 50,000 x 128: the one configuration with published reference numbers
+# ---------------------------------------------------------------------------------------------
+
+def l2_copy_gbs(dev, nbytes=24 << 20, iters=200):
+    """Copy bandwidth (read + write bytes) of a buffer pair that stays in the 126 MB L2."""
+    import torch
+    a = torch.empty(nbytes // 4, dtype=torch.float32, device=dev).fill_(1.0)
+    b = torch.empty_like(a)
+    for _ in range(10):
+        b.copy_(a)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(iters):
+        b.copy_(a)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    return 2.0 * nbytes * iters / (e0.elapsed_time(e1) / 1e3) / 1e9
+
+
+def run_c1(args, dev, L, world):
+    """50,000 x 128 N(0, 1) (numpy default_rng(42)), normalized=false, k=10: the golden single query
+    of the reference's demo notebook and a batch of 64 from the same generator; host-buffer calls
+    (the reference-facing API) and device-resident calls, beside the reference's published CPU
+    latencies and the CPU restatement on this host."""
+    import numpy as np
+    import torch
+    from nndex_b200 import NNdex, _lib
+    from oracle import oracle as O
+    rng = np.random.default_rng(42)
+    m = rng.normal(size=(50_000, 128)).astype(np.float32)
+    q1 = rng.normal(size=(128,)).astype(np.float32)
+    q64 = rng.normal(size=(64, 128)).astype(np.float32)
+    k = 10
+    index = NNdex(m, gpu_device_index=dev.index)
+    gi, _ = index.search(q1, k=5)
+    golden = gi.tolist() == [43576, 14100, 15993, 35409, 38916]
+    if not golden:
+        raise RuntimeError(f"50k x 128 golden query answered {gi.tolist()}")
+    out = {"golden_top5_matches": golden}
+    # host-buffer calls: wall time per call (the latency a caller sees)
+    for name, q in (("batch_1", q1), ("batch_64", q64)):
+        for _ in range(20):
+            index.search(q, k=k)
+        lat = []
+        for _ in range(args.c1_calls):
+            t0 = time.perf_counter()
+            index.search(q, k=k)
+            lat.append((time.perf_counter() - t0) * 1e3)
+        lat = np.array(lat)
+        nq = 1 if q.ndim == 1 else q.shape[0]
+        out[name] = {"host_call_ms_p50": float(np.median(lat)), "host_call_ms_p99": float(np.percentile(lat, 99)),
+                     "host_queries_per_s": nq / (np.median(lat) / 1e3)}
+    # device-resident: CUDA events over back-to-back calls on one stream (the base stays in L2)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = C.c_void_p(stream.cuda_stream)
+    l2 = l2_copy_gbs(dev)
+    peak, peak_kind = measured_peaks()
+    h = index.handle
+    for name, q in (("batch_1", q1.reshape(1, -1)), ("batch_64", q64)):
+        nq = q.shape[0]
+        qd = torch.from_numpy(q).to(dev)
+        oi = torch.empty((nq, k), dtype=torch.int64, device=dev)
+        os_ = torch.empty((nq, k), dtype=torch.float32, device=dev)
+
+        def call():
+            if L.nndex_cuda_search_batch_device(h, qd.data_ptr(), nq, 128, k, oi.data_ptr(), os_.data_ptr(), None,
+                                                sptr, 0) != 0:
+                raise RuntimeError(_lib.last_error())
+        for _ in range(20):
+            call()
+        torch.cuda.synchronize(dev)
+        L.nndex_cuda_set_scan_timing(h, 1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(args.c1_calls):
+                call()
+            e1.record(stream)
+        torch.cuda.synchronize(dev)
+        L.nndex_cuda_set_scan_timing(h, 0)
+        scan_ms, scan_n = C.c_double(0.0), C.c_uint64(0)
+        L.nndex_cuda_scan_timing(h, C.byref(scan_ms), C.byref(scan_n))
+        ms = e0.elapsed_time(e1) / args.c1_calls
+        scan = scan_ms.value / max(scan_n.value, 1)
+        gbs = 50_000 * 128 * 4 / (scan / 1e3) / 1e9
+        st = index.last_search_stats()
+        out[name].update({"device_ms_per_call": ms, "device_queries_per_s": nq / (ms / 1e3), "scan_ms": scan,
+                          "path": st["path"], "scan_gbs": gbs, "frac_of_hbm": gbs / peak,
+                          "frac_of_l2_copy": gbs / l2})
+    # the CPU restatement on this host: single query (ParallelChunked) and the batch (Gemm)
+    st_, base = O.prepare_index(m, False)
+    _, qn1 = O.prepare_queries(q1.reshape(1, -1), False, base.shape[1])
+    _, qn64 = O.prepare_queries(q64, False, base.shape[1])
+    ts = []
+    for _ in range(30):
+        t0 = time.perf_counter()
+        O.bench_search_single(base, qn1[0], k)
+        ts.append(time.perf_counter() - t0)
+    tb = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        O.bench_search_batch(base, qn64, k)
+        tb.append(time.perf_counter() - t0)
+    out["cpu_restatement"] = {"single_ms_p50": float(np.median(ts)) * 1e3,
+                              "batch_64_queries_per_s": 64 / float(np.median(tb)), "cores": O.num_threads()}
+    out["published_reference_cpu_single_ms"] = {
+        "accuracy_vs_numpy notebook (k=20, seed 7)": 0.31, "python_bindings_demo notebook (k=5, seed 42)": 0.28962,
+        "hardware": "unstated"}
+    out["roofline"] = {"bytes_per_batch": 50_000 * 128 * 4, "l2_copy_gbs_measured": l2, "hbm_peak_gbs": peak,
+                       "hbm_peak_kind": peak_kind,
+                       "note": "the 25.6 MB base stays in the 126 MB L2 across calls: a latency case"}
+    del index
+    return out
 
 
 # ---------------------------------------------------------------------------------------------
@@ -554,9 +683,10 @@ def run_mixed(args, dev, L, world):
         max_ms, total_q = aggregate(ms, nq * steps, world, dev)
         got = oi[:sample]
         hits = sum(len(set(got[i].tolist()) & set(ref_i[i].tolist())) for i in range(sample))
-        # score error of the returned results against the FP64 oracle
-        ps = (q[:sample].double().unsqueeze(1) * base[got].double()).sum(-1)
-        err = (os_[:sample].double() - ps).abs().max().item()
+        # every result's score error against the FP64 oracle, from the library's own report (one
+        # untimed batch with the report on)
+        serr = score_error_report(L, h, lambda: L.nndex_cuda_search_batch_device(
+            h, q.data_ptr(), nq, dims, k, oi.data_ptr(), os_.data_ptr(), None, sptr, 1))
         scan_total = scan_ms.value  # all scan-kernel launches of the timed batches
         out[name] = {
             "queries_per_s": total_q / (max_ms / 1e3),
@@ -566,7 +696,8 @@ def run_mixed(args, dev, L, world):
             "scan_tflops": flops / (scan_total / 1e3) / 1e12,
             "pass1_tile_stride": int(stats.pass1_tile_stride),
             "recall_at_k_vs_fp64": hits / (sample * k),
-            "max_score_error_vs_fp64": err,
+            "score_error_vs_fp64": serr,
+            "algorithmic_tflops": 2.0 * rows * dims * nq / (max_ms / steps / 1e3) / 1e12,
             "rerank_width": int(stats.rerank_width),
             "second_pass_queries_per_batch": second / steps,
             "fp32_fallback_queries_per_batch": fallbacks / steps,
@@ -579,16 +710,21 @@ def run_mixed(args, dev, L, world):
     for name in ("bf16", "fp8"):
         out[name]["speedup_vs_fp32"] = out[name]["queries_per_s"] / fp32
     bf16_peak = measured_bf16_peak()
+    alg = {name: out[name]["algorithmic_tflops"] for name in ("bf16", "fp8")}
     return {
         "workload": f"exact top-{k}, base {rows}x{dims} ({args.mixed_centers}-centre Gaussian mixture, "
                     f"sigma={args.mixed_sigma}, unit rows), batch {nq}; BF16/FP8 tensor-core scan + FP32 rerank "
                     f"vs the FP32 scan; recall on {sample} queries vs a float64 brute force",
         "results": out,
-        "roofline": {"bound": "tensor", "kernel": "scan_tc_kernel (BF16, both passes)",
-                     "achieved_bf16_tflops": out["bf16"]["scan_tflops"],
-                     "peak_bf16_tflops": bf16_peak[0], "frac_bf16": out["bf16"]["scan_tflops"] / bf16_peak[0],
-                     "peak_kind": bf16_peak[1],
-                     "flops": "2*N*D*(batch/pass1_tile_stride + second_pass_queries) per batch"},
+        "roofline": {"bound": "tensor", "kernel": "scan_tc_kernel",
+                     "flops": "algorithmic 2*N*D*batch per batch, over the whole batch time (both passes, "
+                              "merge, rerank)",
+                     "achieved_bf16_tflops": alg["bf16"], "peak_bf16_tflops": bf16_peak[0],
+                     "frac_bf16": alg["bf16"] / bf16_peak[0],
+                     "achieved_fp8_tflops": alg["fp8"], "peak_fp8_tflops": 2 * bf16_peak[0],
+                     "frac_fp8": alg["fp8"] / (2 * bf16_peak[0]),
+                     "peak_kind": bf16_peak[1] + "; FP8 peak taken as twice the BF16 figure",
+                     "executed_scan_tflops": {name: out[name]["scan_tflops"] for name in ("bf16", "fp8")}},
     }
 
 
@@ -685,6 +821,8 @@ def run_ivf(args, dev, L, world):
         got = oi.cpu().tolist()
         hits = sum(len(set(got[i]) & exact_sets[i]) for i in range(nq))
         tc = stats.path == 5
+        serr = score_error_report(L, h, lambda: L.nndex_cuda_search_batch_device(
+            h, q.data_ptr(), nq, dims, k, oi.data_ptr(), os_.data_ptr(), cnt.data_ptr(), sptr, 1))
         scan_avg = scan_ms.value / args.ivf_steps  # all scan launches of a batch (the tensor-core scan: 2 passes)
         passes = (scan_n.value / args.ivf_steps) if tc else 1.0
         streamed_b = stats.ivf_rows_streamed * dims * (2 if tc else 4) * passes
@@ -696,6 +834,7 @@ def run_ivf(args, dev, L, world):
             "queries_per_s": total_q / (max_ms / 1e3),
             "ms_per_batch": max_ms / args.ivf_steps,
             "recall_at_k_vs_exact": hits / (nq * k),
+            "score_error_vs_fp64": serr,
             "rows_probed_per_query": stats.rows_scanned / nq,
             "rows_streamed": stats.ivf_rows_streamed,
             "rows_union": stats.ivf_rows_union,
@@ -815,6 +954,7 @@ def run_serve(args, dev, L, world):
     L.nndex_cuda_ivf_stats_get(h, C.byref(bst))
     so = _lib.ServerOpts()
     so.slots = args.serve_slots
+    so.latency_budget_ms = args.serve_latency_ms
     srv = C.c_void_p()
     if L.nndex_cuda_server_start(h, C.byref(so), C.byref(srv)) != 0:
         raise RuntimeError(_lib.last_error())
@@ -833,6 +973,7 @@ def run_serve(args, dev, L, world):
         starts = rng.integers(0, pool.shape[0] - 256, size=nreq)
         tickets = [None] * nreq
         lat = []
+        batches_seen = {}  # batch id → (slot, start_ns, done_ns, queries)
         done_q = [0]
         refused = [0]
         first_last = [None, None]
@@ -854,10 +995,13 @@ def run_serve(args, dev, L, world):
                 if st != 0:
                     raise RuntimeError(_lib.last_error())
                 lat.append((info.done_ns - info.submit_ns) / 1e6)
+                batches_seen[info.batch_id] = (info.slot, info.start_ns, info.done_ns, info.batch_queries)
                 done_q[0] += n
                 first_last[0] = info.submit_ns if first_last[0] is None else min(first_last[0], info.submit_ns)
                 first_last[1] = info.done_ns if first_last[1] is None else max(first_last[1], info.done_ns)
 
+        s0 = _lib.ServerStats()
+        L.nndex_cuda_server_stats_get(srv, C.byref(s0))
         th = threading.Thread(target=collect)
         th.start()
         tk = C.c_uint64(0)
@@ -877,7 +1021,16 @@ def run_serve(args, dev, L, world):
                 refused[0] += 1
             ready.release()
         th.join()
+        s1 = _lib.ServerStats()
+        L.nndex_cuda_server_stats_get(srv, C.byref(s1))
         elapsed = (first_last[1] - first_last[0]) / 1e9 if first_last[1] else float("nan")
+        # per-slot timeline: batches, mean batch time and the share of the phase each slot was busy
+        slots_tl = {}
+        for sl, b0, b1, bq in batches_seen.values():
+            d = slots_tl.setdefault(sl, [0, 0.0, 0])
+            d[0] += 1
+            d[1] += (b1 - b0) / 1e6
+            d[2] += bq
         lat_a = np.array(lat) if lat else np.array([float("nan")])
         if name is None:
             continue
@@ -889,6 +1042,11 @@ def run_serve(args, dev, L, world):
             "latency_ms_p50": float(np.percentile(lat_a, 50)),
             "latency_ms_p99": float(np.percentile(lat_a, 99)),
             "latency_ms_max": float(lat_a.max()),
+            "refused_by_latency_budget": int(s1.refused_latency - s0.refused_latency),
+            "us_per_query_estimate": float(s1.us_per_query),
+            "slots": {str(sl): {"batches": d[0], "mean_batch_ms": d[1] / d[0], "mean_batch_queries": d[2] / d[0],
+                                "busy_frac": d[1] / 1e3 / elapsed if elapsed > 0 else None}
+                      for sl, d in sorted(slots_tl.items())},
         }
     sst = _lib.ServerStats()
     L.nndex_cuda_server_stats_get(srv, C.byref(sst))
@@ -898,7 +1056,8 @@ def run_serve(args, dev, L, world):
         "workload": f"serving: base {rows}x{dims} ({args.serve_centers}-centre mixture, sigma={args.serve_sigma}, "
                     f"unit rows; FP32 + BF16 copies + IVF nlist={bst.nlist}), Poisson arrivals, requests of "
                     f"U{{1..256}} queries, k in {{1,10,100}}, 50/50 exact / IVF(nprobe={args.serve_nprobe}), "
-                    f"{args.serve_slots} slots, admission by free HBM",
+                    f"{args.serve_slots} slots, admission by free HBM and a {args.serve_latency_ms} ms "
+                    f"queue-drain budget",
         "create_s_with_ivf_build": create_s,
         "by_offered_rate": out,
         "batches": sst.batches,
@@ -906,6 +1065,19 @@ def run_serve(args, dev, L, world):
         "max_queued_queries": sst.max_queued_queries,
         "slot_bytes": sst.slot_bytes,
     }
+
+
+def score_error_report(L, h, search):
+    """Runs `search` once with the library's per-result error report on; max and mean error of all
+    its results against the FP64 oracle."""
+    from nndex_b200 import _lib
+    L.nndex_cuda_set_error_report(h, 1)
+    if search() != 0:
+        raise RuntimeError(_lib.last_error())
+    st = _lib.SearchStats()
+    L.nndex_cuda_last_search_stats(h, C.byref(st))
+    L.nndex_cuda_set_error_report(h, 0)
+    return {"max": st.max_score_error, "mean": st.mean_score_error, "results": "every result of one batch"}
 
 
 def measured_bf16_peak():

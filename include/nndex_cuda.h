@@ -104,7 +104,7 @@ typedef struct nndex_cuda_search_stats {
     uint32_t path;             /* 1 = FP32 scan, 2 = BF16 scan+rerank, 3 = FP8 scan+rerank,
                                   4 = IVF probe + rerank, 5 = IVF list scan on the tensor
                                   cores + rerank, 6 = TF32 candidate scan + rerank
-                                  (NNDEX_TF32_SCAN=1, 9-16 queries)                           */
+                                  (9-16 queries of a batch)                                    */
     uint32_t kernel_launches;  /* kernels this library launched for the call                */
     uint32_t rerank_width;     /* k' of a low-precision scan's first pass (0 otherwise)     */
     uint32_t certified;        /* 1 = every query certified after the first pass            */
@@ -122,7 +122,13 @@ typedef struct nndex_cuda_search_stats {
                                        consumer warps of 16 rows × all queries (wide consumer)  */
     uint32_t graph;                 /* host-buffer search: 0 = direct launches, 1 = captured as a
                                        CUDA graph by this call, 2 = a cached graph replayed      */
-    uint32_t reserved;
+    uint32_t score_errors;          /* 1 = the call measured every result's score error        */
+    double   max_score_error;       /* largest |score − FP64 score| over the call's results     */
+    double   mean_score_error;      /* their mean (both 0 unless score_errors)                  */
+    uint32_t tuned;                 /* plan of the call's last batch: 0 = by the rules, 1 = the
+                                       autotuner timed the candidates on it, 2 = from the tuner's
+                                       cache                                                     */
+    uint32_t tune_candidates;       /* plans the autotuner compared for that shape (0 = none)    */
 } nndex_cuda_search_stats;
 
 /* IVF build statistics (approximate mode; zero when the index has no IVF). */
@@ -344,6 +350,30 @@ NNDEX_API int nndex_cuda_base_checksum(nndex_cuda_index* index, uint64_t* checks
  * the cached graphs. enable = 0 turns capture off (and drops them). */
 NNDEX_API int nndex_cuda_set_graphs(nndex_cuda_index* index, int enable);
 
+/*
+ * The autotuner (replaces src/profiles.rs:65-185, which maps a shape to a CPU strategy by fixed
+ * thresholds). mode 1 (the default): the first batch of each shape — exact or IVF, queries and k
+ * rounded up to powers of two, nprobe and precision — runs every plan that returns the same
+ * results (the FP32 scan or the TF32 candidate scan for small batches; BF16 or FP8 tensor-core
+ * scans with pass-1 tile strides 1, 8 and 32 for large ones; the FP32 or the tensor-core IVF list
+ * scan), times each, and keeps the fastest for later batches of that shape. mode 0: the fixed
+ * rules. Results are identical under every plan; only speed differs.
+ */
+NNDEX_API int nndex_cuda_set_autotune(nndex_cuda_index* index, int mode);
+/*
+ * The tuner's cache as text, to keep across processes: a header line naming the device, the
+ * matrix shape and flags, then one line per shape with its plan and time. *len receives the size
+ * (with the terminating 0); with buf NULL or too small only *len is written
+ * (NNDEX_ERR_INVALID_ARGUMENT when buf is too small).
+ */
+NNDEX_API int nndex_cuda_autotune_export(nndex_cuda_index* index, char* buf, uint64_t capacity, uint64_t* len);
+/* Installs a cache exported for the same device model, shape and flags (NNDEX_ERR_INVALID_ARGUMENT
+ * otherwise: a plan measured elsewhere is not trusted). Replaces entries of the same shapes. */
+NNDEX_API int nndex_cuda_autotune_import(nndex_cuda_index* index, const char* text);
+/* Parses exported text without an index or a GPU: NNDEX_OK and the entry count, or
+ * NNDEX_ERR_INVALID_ARGUMENT and the first bad line in the error message. */
+NNDEX_API int nndex_cuda_autotune_validate(const char* text, uint64_t* entries);
+
 /* Lists probed per query by later approx searches (0 = choose_nprobe, src/approx.rs:318-336);
  * no counterpart in the reference, whose nprobe is always the policy's. */
 NNDEX_API int nndex_cuda_set_nprobe(nndex_cuda_index* index, uint32_t nprobe);
@@ -368,7 +398,10 @@ typedef struct nndex_cuda_server_opts {
     uint32_t max_batch_queries;  /* queries per batch, 0 = 4096                                 */
     uint64_t queue_capacity;     /* queries waiting, 0 = 1 << 20                                */
     uint64_t slot_bytes;         /* device memory per slot, 0 = free HBM × 0.5 / slots          */
-    uint32_t reserved[8];
+    uint32_t latency_budget_ms;  /* refuse a request when the queue ahead of it would take longer
+                                    than this to drain (estimated from the batches served so far),
+                                    0 = no latency bound                                         */
+    uint32_t reserved[7];
 } nndex_cuda_server_opts;
 typedef struct nndex_cuda_request_info {
     uint64_t submit_ns, start_ns, done_ns;   /* steady-clock times: queued, batch launched, done */
@@ -383,6 +416,8 @@ typedef struct nndex_cuda_server_stats {
     uint64_t queued_queries, max_queued_queries;
     uint32_t slots, max_batch_queries;
     uint64_t slot_bytes;
+    uint64_t refused_latency;      /* of `refused`: refused by the latency budget               */
+    double us_per_query;           /* the drain-time estimate's cost of a query in one slot     */
 } nndex_cuda_server_stats;
 
 NNDEX_API int nndex_cuda_server_start(nndex_cuda_index* index, const nndex_cuda_server_opts* opts,
@@ -426,6 +461,22 @@ NNDEX_API void nndex_cuda_inject_alloc_failures(uint32_t count);
 NNDEX_API int nndex_cuda_fp64_scores(nndex_cuda_index* index, const float* dev_queries_normalized,
                            uint64_t query_rows, const uint64_t* dev_pairs_query,
                            const uint64_t* dev_pairs_row, uint64_t n, double* dev_out);
+
+/*
+ * Per-result score errors (no counterpart in the reference, whose results carry no error): while
+ * enabled, every search also scores each returned (query, row) pair in FP64 on the device — the
+ * stored FP32 row against the query as the index normalised it, the exact value the returned FP32
+ * score approximates — and records |returned score − FP64 score| per result. The extra work is one
+ * FP64 dot product per result. The no-allocation entry point records none. Enabling or disabling
+ * drops the cached CUDA graphs (and the host-buffer search is not captured while enabled).
+ */
+NNDEX_API int nndex_cuda_set_error_report(nndex_cuda_index* index, int enable);
+/*
+ * The last search's per-result errors: query_rows × min(k, rows) doubles in result order (0 where a
+ * query returned fewer results). query_rows and k must be the last search's. Waits for the search.
+ */
+NNDEX_API int nndex_cuda_last_score_errors(nndex_cuda_index* index, uint64_t query_rows, uint64_t k,
+                                           double* errors_out);
 
 #ifdef __cplusplus
 }

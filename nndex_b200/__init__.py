@@ -130,7 +130,8 @@ class NNdex:
     def __init__(self, data: Any, normalized: bool = False, approx: bool = False, backend: str = "cuda",
                  enable_cache: bool = True, gpu_device_index: int | None = None, *, precision: str = "fp32",
                  nlist: int = 0, nprobe: int = 0, kmeans_iters: int = 0, seed: int | None = None,
-                 rerank_width: int = 0, low_precision_copies: tuple = (), ivf: Any = None):
+                 rerank_width: int = 0, low_precision_copies: tuple = (), ivf: Any = None,
+                 autotune: bool = True):
         self._h = None
         flags, opts = self._options(backend, normalized, approx, gpu_device_index, precision, nlist, nprobe,
                                     kmeans_iters, seed, rerank_width, low_precision_copies, ivf)
@@ -143,6 +144,8 @@ class NNdex:
         if st != 0:
             raise ValueError(_lib.last_error())
         self._adopt(h, rows, dims, normalized, approx, enable_cache)
+        if not autotune:
+            self.set_autotune(False)
         if ivf is not None:
             self.load_ivf(ivf)
 
@@ -257,6 +260,36 @@ class NNdex:
         _check(_lib.lib().nndex_cuda_last_candidates(self._h, query_rows, idx.ctypes.data, sim.ctypes.data, idx.size,
                                                      C.byref(kp), C.byref(eps), cert.ctypes.data))
         return idx[:, :kp.value], sim[:, :kp.value], float(eps.value), cert.astype(bool)
+
+    def set_autotune(self, enable: bool = True) -> None:
+        """Plan choice for later searches: measured once per batch shape (the default) or the fixed
+        rules (nndex_cuda_set_autotune). Results are the same either way."""
+        _check(_lib.lib().nndex_cuda_set_autotune(self._h, 1 if enable else 0))
+
+    def autotune_export(self) -> str:
+        """The autotuner's cache as text (nndex_cuda_autotune_export)."""
+        n = C.c_uint64(0)
+        _check(_lib.lib().nndex_cuda_autotune_export(self._h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(_lib.lib().nndex_cuda_autotune_export(self._h, buf, n.value, C.byref(n)))
+        return buf.value.decode()
+
+    def autotune_import(self, text: str) -> None:
+        """Installs a cache exported for the same device model, shape and flags."""
+        _check(_lib.lib().nndex_cuda_autotune_import(self._h, text.encode()))
+
+    def set_error_report(self, enable: bool = True) -> None:
+        """Record, for every result of later searches, |score − FP64 score| (see
+        nndex_cuda_set_error_report); last_score_errors returns them, last_search_stats their max and
+        mean."""
+        _check(_lib.lib().nndex_cuda_set_error_report(self._h, 1 if enable else 0))
+
+    def last_score_errors(self, query_rows: int, k: int) -> np.ndarray:
+        """The last search's per-result score errors, query_rows × min(k, rows) (0 past a query's count)."""
+        kk = max(min(int(k), self._rows), 1)
+        out = np.zeros((query_rows, kk), dtype=np.float64)
+        _check(_lib.lib().nndex_cuda_last_score_errors(self._h, query_rows, int(k), out.ctypes.data))
+        return out
 
     def last_search_stats(self) -> dict:
         s = _lib.SearchStats()
@@ -464,13 +497,14 @@ class Server:
     """
 
     def __init__(self, index: NNdex, slots: int = 2, max_batch_queries: int = 4096,
-                 queue_capacity: int = 1 << 20, slot_bytes: int = 0):
+                 queue_capacity: int = 1 << 20, slot_bytes: int = 0, latency_budget_ms: int = 0):
         self._index = index  # keeps the index alive while the server runs
         o = _lib.ServerOpts()
         o.slots = slots
         o.max_batch_queries = max_batch_queries
         o.queue_capacity = queue_capacity
         o.slot_bytes = slot_bytes
+        o.latency_budget_ms = latency_budget_ms
         h = C.c_void_p()
         _check(_lib.lib().nndex_cuda_server_start(index.handle, C.byref(o), C.byref(h)))
         self._h = h

@@ -84,7 +84,11 @@ class SearchStats(C.Structure):
         ("scan_qb", C.c_uint32),
         ("scan_wide", C.c_uint32),
         ("graph", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("score_errors", C.c_uint32),
+        ("max_score_error", C.c_double),
+        ("mean_score_error", C.c_double),
+        ("tuned", C.c_uint32),
+        ("tune_candidates", C.c_uint32),
     ]
 
 
@@ -110,7 +114,8 @@ class ServerOpts(C.Structure):
         ("max_batch_queries", C.c_uint32),
         ("queue_capacity", C.c_uint64),
         ("slot_bytes", C.c_uint64),
-        ("reserved", C.c_uint32 * 8),
+        ("latency_budget_ms", C.c_uint32),
+        ("reserved", C.c_uint32 * 7),
     ]
 
 
@@ -138,6 +143,8 @@ class ServerStats(C.Structure):
         ("slots", C.c_uint32),
         ("max_batch_queries", C.c_uint32),
         ("slot_bytes", C.c_uint64),
+        ("refused_latency", C.c_uint64),
+        ("us_per_query", C.c_double),
     ]
 
 
@@ -171,6 +178,12 @@ SIGNATURES = {
     "nndex_cuda_set_scan_timing": (_i32, [_vp, _i32]),
     "nndex_cuda_scan_timing": (_i32, [_vp, C.POINTER(C.c_double), C.POINTER(_u64)]),
     "nndex_cuda_fp64_scores": (_i32, [_vp, _vp, _u64, _vp, _vp, _u64, _vp]),
+    "nndex_cuda_set_error_report": (_i32, [_vp, _i32]),
+    "nndex_cuda_set_autotune": (_i32, [_vp, _i32]),
+    "nndex_cuda_autotune_export": (_i32, [_vp, C.c_char_p, _u64, C.POINTER(_u64)]),
+    "nndex_cuda_autotune_import": (_i32, [_vp, C.c_char_p]),
+    "nndex_cuda_autotune_validate": (_i32, [C.c_char_p, C.POINTER(_u64)]),
+    "nndex_cuda_last_score_errors": (_i32, [_vp, _u64, _u64, _vp]),
     "nndex_cuda_search_batch_device_noalloc": (_i32, [_vp, _vp, _u64, _u64, _u64, _vp, _vp, _vp, _vp]),
     "nndex_cuda_ivf_layout": (_i32, [_vp, C.POINTER(_u64), _vp, _vp, _vp, _vp]),
     "nndex_cuda_ivf_stats_get": (_i32, [_vp, C.POINTER(IvfStats)]),

@@ -9,6 +9,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -234,8 +235,10 @@ CudaIndex::~CudaIndex() {
     cudaFree(d_q_fp8);
     cudaFree(d_q_scale);
     cudaFree(d_q_resid);
-    cudaFree(d_qtb);
-    cudaFree(d_qts);
+    if (owns_base) cudaFree(d_tfnorm);
+    cudaFree(d_serr);
+    cudaFree(d_serr_acc);
+    cudaFreeHost(h_serr_acc);
     cudaFree(d_thr);
     cudaFree(d_cand_idx);
     cudaFree(d_cand_sim);
@@ -385,9 +388,9 @@ int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
         const TcPlan p1 = plan_tc(kcap, fp8);
         return p1.kp >= kcap && p1.kp > 0 && plan_tc(0, fp8).stages > 0;
     };
-    // 9–16 queries with NNDEX_TF32_SCAN=1: the TF32 candidate scan, which reads the same FP32 base
-    // and returns the same bits (opt-in: on 1M × 768 at 16 queries it is shared-memory-bound and
-    // slower than the FP32 scan, 0.85 against 0.77 ms per scan).
+    // Small batches (plan_tf32's range): the TF32 candidate scan, which reads the same FP32 base and
+    // returns the same bits as the FP32 scan at the HBM rate, where the FP32 scan is bound by its
+    // FMA issue.
     const int fp32_path = plan_tf32(nq, kcap).kp ? 6 : 1;
     switch (precision) {
         case NNDEX_PRECISION_FP32: return fp32_path;
@@ -406,11 +409,19 @@ int CudaIndex::choose_path(uint64_t nq, uint64_t kcap) const {
 
 CudaIndex::Tf32Plan CudaIndex::plan_tf32(uint64_t nq, uint64_t kcap) const {
     Tf32Plan p;
-    if (nq < 9 || nq > 16 || kcap == 0 || kcap > 128) return p;
-    const char* opt = getenv("NNDEX_TF32_SCAN");  // 1: the TF32 candidate scan at 9–16 queries
-    if (!(opt && opt[0] == '1')) return p;
-    // k′: twice k, at least k + 32, so that the k-th exact score clears the k′-th bound
-    const uint64_t kp = std::min<uint64_t>(256, std::max<uint64_t>(2 * kcap, kcap + 32));
+    static const uint32_t min_q = [] {
+        const char* v = getenv("NNDEX_TF32_MIN_QUERIES");  // measurement override of the batch rule
+        return v ? static_cast<uint32_t>(atoi(v)) : 9u;
+    }();
+    static const bool off = [] {
+        const char* v = getenv("NNDEX_TF32_SCAN");  // 0: small batches always take the FP32 scan
+        return v && v[0] == '0';
+    }();
+    if (off || !d_tfnorm || nq < std::max<uint32_t>(min_q, 1) || nq > 16 || kcap == 0 || kcap > 448) return p;
+    // k′: 2.5 k rounded up to 32, at least k + 64 and at most 512, so that the exact k-th score
+    // clears the k′-th bound on clustered data (on a 1,024-centre mixture of 1M × 768 rows the
+    // 100th and 256th scores of a query are ≈ 2.4e-3 apart, twice the bound's typical ε)
+    const uint64_t kp = std::min<uint64_t>(512, (std::max<uint64_t>(kcap * 5 / 2, kcap + 64) + 31) / 32 * 32);
     if (rows < 4 * kp || rows > 0xFFFFFFFFull) return p;
     // Room for three tiles of survivors above k′: a selection runs once ≥ 256 keys have
     // accumulated since the last one, not after every tile.
@@ -423,17 +434,20 @@ CudaIndex::Tf32Plan CudaIndex::plan_tf32(uint64_t nq, uint64_t kcap) const {
     return p;
 }
 
-// Upper bound of |FP32 scan-order score − s̃| for unit rows and queries (Σ|x_i q_i| ≤ 1):
-//   the split, three products each off by < 2⁻²⁰·|x_i q_i|:                 3·2⁻²⁰
+// C of K12's bound, per unit ‖q‖‖x‖:
+//   the tensor core's FP32 accumulation of ds exact TF32 products (each added with up to one FP32
+//   rounding, 4× margin, as for the BF16 scan):                              4·ds·2⁻²³
 //   the FP32 scan's own rounding (eight chains of ds/8 FMAs, then 3 adds):  (ds/8 + 3)·2⁻²⁴
-//   the tensor core's FP32 accumulation, as for the BF16 scan (each of the 3·ds products
-//   added with up to one FP32 rounding, 4× margin):                          4·3·ds·2⁻²³
-//   and the rounding of s̃ + ε itself:                                      2⁻²³
-float CudaIndex::tf32_eps() const {
+//   the rounding of u = s̃ + ε:                                             2⁻²²
+float CudaIndex::tf32_c_norm() const {
     const double d = static_cast<double>(ds);
-    const double e = 3.0 * std::ldexp(1.0, -20) + (d / 8.0 + 3.0) * std::ldexp(1.0, -24) +
-                     12.0 * d * std::ldexp(1.0, -23) + std::ldexp(1.0, -23);
-    return static_cast<float>(e * 1.01);
+    return static_cast<float>((4.0 * d * std::ldexp(1.0, -23) + (d / 8.0 + 3.0) * std::ldexp(1.0, -24) +
+                               std::ldexp(1.0, -22)) * 1.01);
+}
+
+// For unit rows and queries ‖d_v‖ < 2⁻¹⁰: ε < 2·2⁻¹⁰ + 2⁻²⁰ + C.
+float CudaIndex::tf32_eps() const {
+    return static_cast<float>((2.0 * std::ldexp(1.0, -10) + std::ldexp(1.0, -20) + tf32_c_norm()) * 1.01);
 }
 
 // IVF batches: the tensor-core list scan (5) from a few dozen queries, when the index's precision
@@ -556,7 +570,9 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     const uint64_t per_query = nranges * kp;
     // Autotuned: when the last batch rarely certified in pass 1, pass 1 only has to produce each
     // query's threshold T, and a sample of the rows (every 8th tile) gives a valid one.
-    const uint32_t stride = (tc_sample_stride > 1 && rows >= 256ull * 64) ? tc_sample_stride : 1;
+    // The tuner's plan may fix it instead (only bases of ≥ 64 tiles are sampled).
+    const uint32_t want = forced_stride ? forced_stride : tc_sample_stride;
+    const uint32_t stride = (want > 1 && rows >= 256ull * 64) ? want : 1;
     if ((st = grow_device(d_thr, cap_thr, n, "tc workspace"))) return st;
     if ((st = grow_device(d_ws, cap_ws, per_query * n, "tc workspace"))) return st;
     if ((st = grow_device(d_cand_idx, cap_cand_idx, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
@@ -683,9 +699,12 @@ int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_si
         if (!h_cert[i]) h_ids[m++] = i;
     stats.certified = m == 0 ? 1u : 0u;
     stats.second_pass_queries = m;
-    // Autotune pass 1 for the next batch: a full pass 1 pays off only when it certifies most queries.
-    if (last_tc_stride == 1) tc_sample_stride = (m * 2 > n) ? 8u : 1u;
-    else if (m * 2 <= n) tc_sample_stride = 1;
+    // The rule for the next batch (when no tuned plan fixes the stride): a full pass 1 pays off only
+    // when it certifies most queries.
+    if (!forced_stride) {
+        if (last_tc_stride == 1) tc_sample_stride = (m * 2 > n) ? 8u : 1u;
+        else if (m * 2 <= n) tc_sample_stride = 1;
+    }
     if (m == 0) return NNDEX_OK;
 
     // ---- pass 2 ----
@@ -776,46 +795,44 @@ int CudaIndex::rerun_exact_fp32(const std::vector<uint32_t>& qs, uint32_t kcap, 
     return NNDEX_OK;
 }
 
-// K12 (9–16 queries, FP32 precision): split the queries, the TF32 candidate scan, the merge of each
-// query's per-CTA candidates, and the exact rerank with its certificate into the outputs.
+// K12 (small batches, FP32 precision): the TF32 candidate scan, the merge of each query's per-CTA
+// candidates, and the exact rerank with its certificate into the outputs.
 int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
                             cudaStream_t s) {
     int st;
     const Tf32Plan plan = plan_tf32(n, kcap);
     if (!plan.kp) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: no TF32 scan plan for k=%u", kcap);
     const uint32_t kp = plan.kp;
-    const uint32_t nq_alloc = (n + 15) / 16 * 16;
     const uint32_t ctas = static_cast<uint32_t>(sm_count);
     const uint64_t per_query = static_cast<uint64_t>(ctas) * kp;
-    if ((st = grow_device(d_qtb, cap_qtb, static_cast<uint64_t>(nq_alloc) * ds, "query buffer"))) return st;
-    if ((st = grow_device(d_qts, cap_qts, static_cast<uint64_t>(nq_alloc) * ds, "query buffer"))) return st;
     if ((st = grow_device(d_ws, cap_ws, per_query * n, "scan workspace"))) return st;
     if ((st = grow_device(d_cand_idx, cap_cand_idx, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
     if ((st = grow_device(d_cand_sim, cap_cand_sim, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
     if ((st = grow_device(d_cand_cnt, cap_cand_cnt, n, "tc workspace"))) return st;
     if ((st = grow_device(d_cert, cap_cert, n, "tc workspace"))) return st;
     if ((st = grow_device(d_kth, cap_kth, n, "tc workspace"))) return st;
-    CUtensorMap tmap_qb, tmap_qs;
-    if (!encode_tmap_2d(&tmap_qb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, d_qtb, ds, nq_alloc, ds * sizeof(float), 32, 16,
-                        CU_TENSOR_MAP_SWIZZLE_128B) ||
-        !encode_tmap_2d(&tmap_qs, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, d_qts, ds, nq_alloc, ds * sizeof(float), 32, 16,
+    // The queries straight from the prepared buffer: rows past n read as zeros.
+    CUtensorMap tmap_q;
+    if (!encode_tmap_2d(&tmap_q, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, d_qn, ds, n, ds * sizeof(float), 32, 16,
                         CU_TENSOR_MAP_SWIZZLE_128B))
-        return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (split queries, driver "
+        return set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (queries, driver "
                                          "result %d)", last_encode_result());
-    cudaError_t e = launch_split_queries_tf32(d_qn, n, static_cast<uint32_t>(ds), nq_alloc, d_qtb, d_qts, s);
-    if (e != cudaSuccess) return cuda_error(e, "query split launch");
     Tf32ScanArgs a;
     a.nq = n;
     a.nbox = static_cast<uint32_t>(ds / 32);
+    a.ds = static_cast<uint32_t>(ds);
     a.rows = rows;
     a.kp = kp;
     a.cap = plan.cap;
-    a.eps = tf32_eps();
+    a.queries = d_qn;
+    a.row_norms = d_tfnorm;
+    a.c_norm = tf32_c_norm();
+    a.evict_first = n <= 16;
     a.ws_keys = d_ws;
     a.status = d_status;
     cudaEvent_t ev_a = nullptr;
     scan_event_begin(s, ev_a);
-    e = launch_scan_tf32(tmap_f32, tmap_qb, tmap_qs, a, plan.stages, ctas, s);
+    cudaError_t e = launch_scan_tf32(tmap_f32, tmap_q, a, plan.stages, ctas, s);
     scan_event_end(s, ev_a);
     if (e != cudaSuccess) return cuda_error(e, "TF32 scan launch");
     MergeArgs m;
@@ -846,7 +863,7 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     r.kth_out = d_kth;
     r.certify = true;
     if ((e = launch_rerank(r, s)) != cudaSuccess) return cuda_error(e, "rerank launch");
-    stats.kernel_launches += 4;
+    stats.kernel_launches += 3;
     stats.path = 6;
     stats.rerank_width = kp;
     stats.rows_scanned += rows * n;
@@ -872,6 +889,50 @@ int CudaIndex::finish_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_
     stats.fp32_fallback_queries = static_cast<uint32_t>(failed.size());
     if (failed.empty()) return NNDEX_OK;
     return rerun_exact_fp32(failed, kcap, o_idx, o_sim, o_cnt, s);
+}
+
+int CudaIndex::tune_host(uint64_t n, uint64_t kcap, int mode, TunePlan* plan) {
+    std::vector<TunePlan> cands = tune_candidates(n, kcap);
+    const nndex_cuda_search_stats before = stats;
+    const bool report = error_report;
+    error_report = false;  // the timed runs record no score errors
+    double best_ms = 0.0;
+    int best = -1, last_err = NNDEX_OK;
+    for (size_t c = 0; c < cands.size(); ++c) {
+        double ms = 0.0;
+        int cst = NNDEX_OK;
+        for (int rep = 0; rep < 2 && cst == NNDEX_OK; ++rep) {
+            forced_stride = cands[c].stride;
+            const auto t0 = std::chrono::steady_clock::now();
+            cst = enqueue_host_batch(n, kcap, mode, cands[c].path);
+            const cudaError_t e = cudaStreamSynchronize(stream);
+            if (cst == NNDEX_OK && e != cudaSuccess) cst = cuda_error(e, "search");
+            if (cst == NNDEX_OK) cst = check_device_words();
+            ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+        forced_stride = 0;
+        if (cst != NNDEX_OK) {
+            last_err = cst;
+            continue;
+        }
+        if (best < 0 || ms < best_ms) {
+            best = static_cast<int>(c);
+            best_ms = ms;
+        }
+    }
+    error_report = report;
+    if (best < 0) return last_err;
+    clear_error();
+    TuneEntry ent;
+    ent.plan = cands[best];
+    ent.ms = best_ms;
+    ent.candidates = static_cast<uint32_t>(cands.size());
+    tune_cache[tune_key(n, kcap)] = ent;
+    stats = before;
+    stats.tuned = 1;
+    stats.tune_candidates = ent.candidates;
+    *plan = ent.plan;
+    return NNDEX_OK;
 }
 
 // Enqueues one batch of the host-buffer search on `stream` (the queries already in h_q): status
@@ -906,6 +967,8 @@ int CudaIndex::enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path)
         if ((st = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
             return st;
     }
+    if (error_report)
+        serr_record(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream);
     cudaMemcpyAsync(h_res, d_res, res_bytes, cudaMemcpyDeviceToHost, stream);  // idx, sim, cnt
     cudaMemcpyAsync(h_flags, d_err, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);  // err, status
     return NNDEX_OK;
@@ -916,7 +979,8 @@ int CudaIndex::enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path)
 // the capture); otherwise directly. Paths 1 (FP32 scan) and 4 (IVF list scan) only: the others
 // read device results on the host in the middle of the batch.
 int CudaIndex::run_host_batch(uint64_t n, uint64_t kcap, int mode, int path) {
-    const bool graphable = use_graphs && !scan_timing && !sync_check_enabled() && (path == 1 || path == 4) &&
+    const bool graphable = use_graphs && !scan_timing && !error_report && !sync_check_enabled() &&
+                           (path == 1 || path == 4) &&
                            !(graph_failed_paths & (1u << path));
     if (!graphable) return enqueue_host_batch(n, kcap, mode, path);
     const uint64_t epoch = alloc_epoch();
@@ -1000,16 +1064,33 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
     if (kcap > kMaxFusedK)
         return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k=%llu above the fused top-k limit %u",
                          (unsigned long long)kcap, kMaxFusedK);
+    int st0;
+    if (error_report && (st0 = serr_begin(nq, kcap, stream))) return st0;
     cudaEventRecord(ev0, stream);
     const uint64_t chunk = kMaxBatchChunk;
     for (uint64_t q0 = 0; q0 < nq; q0 += chunk) {
         const uint64_t n = std::min<uint64_t>(chunk, nq - q0);
-        const int path = uses_ivf() ? ivf_path(n, kcap) : choose_path(n, kcap);
         int st;
         if ((st = ensure_query_capacity(n))) return st;
         if ((st = ensure_result_capacity(n, kcap))) return st;
         std::memcpy(h_q, queries + q0 * dims, n * dims * sizeof(float));
-        if ((st = run_host_batch(n, kcap, mode, path))) return st;
+        bool measure = false;
+        TunePlan plan = plan_for(n, kcap, &measure);
+        if (measure) {
+            if ((st = tune_host(n, kcap, mode, &plan))) return st;
+        } else if (autotune) {
+            auto it = tune_cache.find(tune_key(n, kcap));
+            if (it != tune_cache.end()) {
+                stats.tuned = 2;
+                stats.tune_candidates = it->second.candidates;
+            }
+        }
+        const int path = plan.path;
+        serr_off = q0;
+        forced_stride = plan.stride;
+        st = run_host_batch(n, kcap, mode, path);
+        forced_stride = 0;
+        if (st) return st;
         cudaEventRecord(ev1, stream);  // before the wait: the device time ends with the last batch
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_error(e, "search");
@@ -1031,6 +1112,29 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
     return NNDEX_OK;
 }
 
+// One piece of a device-buffer search (≤ kMaxBatchChunk queries) on `path`: query prep, the path's
+// scan and merge into the outputs. *synced is set when the path waited for the stream.
+int CudaIndex::run_device_chunk(const float* dq, uint64_t n, uint64_t kcap, int path, uint64_t* oi, float* os,
+                                uint32_t* oc, cudaStream_t s, bool* synced) {
+    int st;
+    if ((st = enqueue_prep_queries(dq, n, normalized ? 2 : 0, path, s))) return st;
+    const uint32_t n32 = static_cast<uint32_t>(n), k32 = static_cast<uint32_t>(kcap);
+    if (path == 4) return ivf_search(*this, d_qn, n32, k32, oi, os, oc, s);
+    if (path == 5) {
+        *synced = true;
+        return ivf_search_tc(*this, n32, k32, oi, os, oc, s);
+    }
+    if (path == 1) return enqueue_exact_fp32(d_qn, n32, k32, k32, oi, os, oc, s);
+    // the certificates' fallbacks need the host: these paths synchronise
+    *synced = true;
+    if (path == 6) {
+        if ((st = enqueue_tf32(n32, k32, oi, os, oc, s))) return st;
+        return finish_tf32(n32, k32, oi, os, oc, s);
+    }
+    if ((st = enqueue_tc(path == 3, n32, k32, oi, os, oc, s))) return st;
+    return finish_tc(n32, k32, oi, os, oc, s);
+}
+
 int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out,
                              float* d_sim_out, uint32_t* d_cnt_out, cudaStream_t s, int synchronize) {
     std::lock_guard<std::mutex> lock(mu);
@@ -1041,38 +1145,72 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
     const uint64_t kcap = std::min<uint64_t>(k, rows);
     int st;
     if ((st = ensure_query_capacity(std::min<uint64_t>(nq, kMaxBatchChunk)))) return st;
+    if (error_report && (st = serr_begin(nq, kcap, s))) return st;
     cudaMemsetAsync(d_err, 0xFF, sizeof(unsigned long long), s);
     cudaMemsetAsync(d_status, 0, sizeof(uint32_t), s);
     bool synced = false;
     for (uint64_t q0 = 0; q0 < nq; q0 += kMaxBatchChunk) {
         const uint64_t n = std::min<uint64_t>(kMaxBatchChunk, nq - q0);
-        const int path = uses_ivf() ? ivf_path(n, kcap) : choose_path(n, kcap);
-        if ((st = enqueue_prep_queries(d_queries + q0 * dims, n, normalized ? 2 : 0, path, s))) return st;
         uint64_t* oi = d_idx_out + q0 * kcap;
         float* os = d_sim_out + q0 * kcap;
         uint32_t* oc = d_cnt_out ? d_cnt_out + q0 : nullptr;
-        if (path == 4) {
-            if ((st = ivf_search(*this, d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s)))
-                return st;
-        } else if (path == 5) {
-            if ((st = ivf_search_tc(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s)))
-                return st;
+        const float* dq = d_queries + q0 * dims;
+        bool measure = false;
+        TunePlan plan = plan_for(n, kcap, &measure);
+        if (measure) {
+            // the first batch of this shape: time every candidate plan on it, keep the fastest
+            std::vector<TunePlan> cands = tune_candidates(n, kcap);
+            const nndex_cuda_search_stats before = stats;
+            double best_ms = 0.0;
+            int best = -1, last_err = NNDEX_OK;
+            for (size_t c = 0; c < cands.size(); ++c) {
+                double ms = 0.0;
+                int cst = NNDEX_OK;
+                for (int rep = 0; rep < 2 && cst == NNDEX_OK; ++rep) {
+                    forced_stride = cands[c].stride;
+                    bool sy = false;
+                    const auto t0 = std::chrono::steady_clock::now();
+                    cst = run_device_chunk(dq, n, kcap, cands[c].path, oi, os, oc, s, &sy);
+                    const cudaError_t e = cudaStreamSynchronize(s);
+                    if (cst == NNDEX_OK && e != cudaSuccess) cst = cuda_error(e, "search");
+                    ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                }
+                forced_stride = 0;
+                if (cst != NNDEX_OK) {
+                    last_err = cst;
+                    continue;
+                }
+                if (best < 0 || ms < best_ms) {
+                    best = static_cast<int>(c);
+                    best_ms = ms;
+                }
+            }
+            if (best < 0) return last_err;
+            clear_error();
+            TuneEntry ent;
+            ent.plan = cands[best];
+            ent.ms = best_ms;
+            ent.candidates = static_cast<uint32_t>(cands.size());
+            tune_cache[tune_key(n, kcap)] = ent;
+            stats = before;
+            stats.tuned = 1;
+            stats.tune_candidates = ent.candidates;
+            plan = ent.plan;
             synced = true;
-        } else if (path == 1) {
-            if ((st = enqueue_exact_fp32(d_qn, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap),
-                                         static_cast<uint32_t>(kcap), oi, os, oc, s)))
-                return st;
-        } else if (path == 6) {
-            // the certificate's fallback needs the host: these batches synchronise
-            if ((st = enqueue_tf32(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s))) return st;
-            if ((st = finish_tf32(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s))) return st;
-            synced = true;
-        } else {
-            // The certificate's fallback needs the host: tensor-core batches always synchronise.
-            if ((st = enqueue_tc(path == 3, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s)))
-                return st;
-            if ((st = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s))) return st;
-            synced = true;
+        } else if (autotune) {
+            auto it = tune_cache.find(tune_key(n, kcap));
+            if (it != tune_cache.end()) {
+                stats.tuned = 2;
+                stats.tune_candidates = it->second.candidates;
+            }
+        }
+        forced_stride = plan.stride;
+        st = run_device_chunk(dq, n, kcap, plan.path, oi, os, oc, s, &synced);
+        forced_stride = 0;
+        if (st) return st;
+        if (error_report) {
+            serr_off = q0;
+            serr_record(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), oi, os, oc, s);
         }
     }
     if (synchronize || synced) {
@@ -1090,6 +1228,48 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
         return check_device_words();
     }
     mark_done(s);
+    return NNDEX_OK;
+}
+
+// Score-error report: buffers for the call's nq × kcap results and a cleared accumulator.
+int CudaIndex::serr_begin(uint64_t nq, uint64_t kcap, cudaStream_t s) {
+    int st;
+    if ((st = grow_device(d_serr, cap_serr, nq * kcap, "score-error buffer"))) return st;
+    if (!d_serr_acc) {
+        cudaError_t e;
+        if ((e = cudaMalloc(&d_serr_acc, 3 * sizeof(unsigned long long))) != cudaSuccess ||
+            (e = cudaMallocHost(&h_serr_acc, 3 * sizeof(unsigned long long))) != cudaSuccess)
+            return cuda_error(e, "score-error buffer");
+    }
+    cudaMemsetAsync(d_serr_acc, 0, 3 * sizeof(unsigned long long), s);
+    serr_nq = nq;
+    serr_k = kcap;
+    serr_off = 0;
+    serr_stream = s;
+    serr_pending = true;
+    stats.score_errors = 1;
+    return NNDEX_OK;
+}
+
+// The errors of one piece of the call (its first query at serr_off; queries normalised in d_qn).
+void CudaIndex::serr_record(uint32_t n, uint32_t kcap, const uint64_t* idx, const float* sim, const uint32_t* cnt,
+                            cudaStream_t s) {
+    launch_score_errors(d_base, ds, d_qn, n, kcap, idx, sim, cnt, d_serr + serr_off * kcap, d_serr_acc, s);
+    stats.kernel_launches += 1;
+}
+
+// Max and mean error into the statistics, once per call (waits for the call's stream).
+int CudaIndex::serr_fetch_stats() {
+    if (!serr_pending) return NNDEX_OK;
+    cudaMemcpyAsync(h_serr_acc, d_serr_acc, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, serr_stream);
+    const cudaError_t e = cudaStreamSynchronize(serr_stream);
+    if (e != cudaSuccess) return cuda_error(e, "score errors");
+    serr_pending = false;
+    double mx, sum;
+    std::memcpy(&mx, &h_serr_acc[0], sizeof(double));
+    std::memcpy(&sum, &h_serr_acc[1], sizeof(double));
+    stats.max_score_error = mx;
+    stats.mean_score_error = h_serr_acc[2] ? sum / static_cast<double>(h_serr_acc[2]) : 0.0;
     return NNDEX_OK;
 }
 
@@ -1271,6 +1451,16 @@ int index_finish(CudaIndex* ix) {
         !encode_tmap_2d(&ix->tmap_fp8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ix->d_base_fp8, ix->kf8, ix->rows_alloc,
                         ix->kf8, 128, 256, CU_TENSOR_MAP_SWIZZLE_128B))
         return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (FP8)"));
+    // Row norms of K12's bound (8 bytes per row, one pass over the base). Without them (no memory)
+    // small batches take the FP32 scan.
+    if (cudaMalloc(&ix->d_tfnorm, ix->rows * sizeof(float2)) == cudaSuccess) {
+        if ((e = launch_tf32_row_norms(ix->d_base, ix->rows, static_cast<uint32_t>(ix->ds), ix->d_tfnorm,
+                                       static_cast<uint32_t>(ix->sm_count), ix->stream)) != cudaSuccess)
+            return fail(cuda_error(e, "row norms launch"));
+    } else {
+        ix->d_tfnorm = nullptr;
+        cudaGetLastError();
+    }
     if (ix->approx) {
         // src/approx.rs:46-100, built once at construction instead of on the first approx search.
         const int st = ivf_build(*ix);
@@ -1370,6 +1560,7 @@ int make_view(const CudaIndex& src, CudaIndex** out) {
     v->eps_fp8 = src.eps_fp8;
     v->d_res16 = src.d_res16;
     v->d_res8 = src.d_res8;
+    v->d_tfnorm = src.d_tfnorm;
     v->tmap_bf16 = src.tmap_bf16;
     v->tmap_fp8 = src.tmap_fp8;
     v->rerank_width = src.rerank_width;
@@ -1617,7 +1808,48 @@ int nndex_cuda_stream_status(nndex_cuda_index* index) {
 int nndex_cuda_last_search_stats(const nndex_cuda_index* index, nndex_cuda_search_stats* out) {
     clear_error();
     if (!index || !out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null argument");
-    *out = index->impl->stats;
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    if (ix->serr_pending) {
+        cudaSetDevice(ix->device);
+        const int st = ix->serr_fetch_stats();
+        if (st) return st;
+    }
+    *out = ix->stats;
+    return NNDEX_OK;
+}
+
+int nndex_cuda_set_error_report(nndex_cuda_index* index, int enable) {
+    clear_error();
+    if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    cudaSetDevice(ix->device);
+    cudaStreamSynchronize(ix->stream);
+    ix->error_report = enable != 0;
+    ix->drop_graphs();
+    return NNDEX_OK;
+}
+
+int nndex_cuda_last_score_errors(nndex_cuda_index* index, uint64_t query_rows, uint64_t k, double* errors_out) {
+    clear_error();
+    if (!index || !errors_out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null argument");
+    CudaIndex* ix = index->impl;
+    std::lock_guard<std::mutex> lock(ix->mu);
+    const uint64_t kcap = std::min<uint64_t>(k, ix->rows);
+    if (!ix->stats.score_errors || !ix->d_serr)
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: the last search recorded no score errors "
+                                                     "(nndex_cuda_set_error_report)");
+    if (query_rows != ix->serr_nq || kcap != ix->serr_k)
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT,
+                         "cuda execution error: the last search had %llu queries at k=%llu, not %llu at k=%llu",
+                         (unsigned long long)ix->serr_nq, (unsigned long long)ix->serr_k,
+                         (unsigned long long)query_rows, (unsigned long long)kcap);
+    cudaSetDevice(ix->device);
+    cudaError_t e = cudaStreamSynchronize(ix->serr_stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(errors_out, ix->d_serr, query_rows * kcap * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(e, "score errors");
     return NNDEX_OK;
 }
 

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <memory>
+#include <map>
 #include <mutex>
 #include <unordered_map>
 #include <utility>
@@ -77,10 +78,7 @@ struct CudaIndex {
     size_t cap_q_fp8 = 0;
     float* d_q_scale = nullptr;
     size_t cap_q_scale = 0;
-    float* d_qtb = nullptr;  // K12: TF32 heads and remainders of the normalised queries
-    size_t cap_qtb = 0;
-    float* d_qts = nullptr;
-    size_t cap_qts = 0;
+    float2* d_tfnorm = nullptr;  // K12: per row {‖x‖, ‖x − tf32_head(x)‖}, rounded up (shared by views)
     float* d_q_resid = nullptr;
     size_t cap_q_resid = 0;
     unsigned long long* d_thr = nullptr;
@@ -104,7 +102,8 @@ struct CudaIndex {
     uint32_t* d_fb_cnt = nullptr;
     size_t cap_fb_cnt = 0;
     uint32_t last_tc_n = 0;  // queries of the last tensor-core batch (diagnostics)
-    uint32_t tc_sample_stride = 1;  // autotuned pass-1 tile stride (1 = full pass 1)
+    uint32_t tc_sample_stride = 1;  // pass-1 tile stride by the certification rule (1 = full pass 1)
+    uint32_t forced_stride = 0;     // the tuned plan's pass-1 tile stride for the current batch (0 = rule)
     uint32_t last_tc_stride = 1;
     float* d_kth = nullptr;  // pass 1: exact k-th score per query
     size_t cap_kth = 0;
@@ -191,6 +190,21 @@ struct CudaIndex {
     uint32_t graph_failed_paths = 0;  // paths whose capture failed (not tried again)
     void drop_graphs();
 
+    // per-result score errors (nndex_cuda_set_error_report): |result − FP64 score| per result of the
+    // last call, and {max as double bits, sum, count} for its statistics
+    bool error_report = false;
+    double* d_serr = nullptr;
+    size_t cap_serr = 0;
+    unsigned long long* d_serr_acc = nullptr;
+    unsigned long long* h_serr_acc = nullptr;  // pinned copy of d_serr_acc
+    uint64_t serr_nq = 0, serr_k = 0, serr_off = 0;  // the last call's shape; the current piece's first query
+    cudaStream_t serr_stream = nullptr;
+    bool serr_pending = false;  // statistics not yet read back
+    int serr_begin(uint64_t nq, uint64_t kcap, cudaStream_t s);
+    void serr_record(uint32_t n, uint32_t kcap, const uint64_t* idx, const float* sim, const uint32_t* cnt,
+                     cudaStream_t s);
+    int serr_fetch_stats();
+
     // scan-kernel timing (roofline reports)
     bool scan_timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> scan_events;
@@ -209,16 +223,43 @@ struct CudaIndex {
                     uint64_t* counts_out);
     int search_device(const float* d_queries, uint64_t nq, uint64_t k, uint64_t* d_idx_out, float* d_sim_out,
                       uint32_t* d_cnt_out, cudaStream_t s, int synchronize);
+    int run_device_chunk(const float* dq, uint64_t n, uint64_t kcap, int path, uint64_t* oi, float* os,
+                         uint32_t* oc, cudaStream_t s, bool* synced);
     // Path choice for a batch: 1 = FP32 scan, 2 = BF16 tensor-core scan, 3 = FP8 tensor-core scan,
-    // 6 = FP32-accurate TF32 candidate scan + exact rerank (9–16 queries).
+    // 6 = TF32 tensor-core candidate scan + exact FP32 rerank (small batches of an FP32 index).
     int choose_path(uint64_t nq, uint64_t kcap) const;
     // K12's plan for k results: candidates per query and CTA (0: no plan), buffer, ring depth.
     struct Tf32Plan {
         uint32_t kp = 0, cap = 0, stages = 0;
     };
     Tf32Plan plan_tf32(uint64_t nq, uint64_t kcap) const;
-    float tf32_eps() const;
+    float tf32_c_norm() const;  // C of K12's bound: ε = ‖q‖(‖d_x‖ + C‖x‖) + ‖d_q‖(‖x‖ + ‖d_x‖)
+    float tf32_eps() const;     // the largest ε for unit rows and queries
     int ivf_path(uint64_t nq, uint64_t kcap) const;
+
+    // Autotuner (autotune.cu): for each batch shape (exact or IVF, queries and k rounded up to
+    // powers of two, nprobe, precision) the plans that return the same results are timed once on
+    // the first batch of that shape, and the fastest is kept. A plan is a path and, for the
+    // tensor-core scan, its pass-1 tile stride.
+    struct TunePlan {
+        int path = 0;
+        uint32_t stride = 0;  // 0 = the certification rule
+    };
+    struct TuneEntry {
+        TunePlan plan;
+        double ms = 0.0;      // its wall time per batch when measured
+        uint32_t candidates = 0;
+    };
+    int autotune = 1;  // 0 = rules only, 1 = measure once per shape
+    std::map<uint64_t, TuneEntry> tune_cache;
+    uint64_t tune_key(uint64_t nq, uint64_t kcap) const;
+    std::vector<TunePlan> tune_candidates(uint64_t nq, uint64_t kcap) const;
+    TunePlan rule_plan(uint64_t nq, uint64_t kcap) const;
+    // The plan for a batch: cached, or by the rules; *measure when the tuner should time the
+    // candidates on this batch first.
+    TunePlan plan_for(uint64_t nq, uint64_t kcap, bool* measure) const;
+    // The first host-buffer batch of a shape: every candidate plan timed on it (the queries in h_q).
+    int tune_host(uint64_t n, uint64_t kcap, int mode, TunePlan* plan);
     struct TcPlan {
         uint32_t kp = 0;        // pass-1 heap entries per query (0: no plan)
         uint32_t stages = 0;    // ring depth

@@ -143,22 +143,26 @@ cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t str
 struct Tf32ScanArgs {
     uint32_t nq = 0;
     uint32_t nbox = 0;                 // 128-byte slabs per row (ds / 32)
+    uint32_t ds = 0;                   // floats per stored row
     uint64_t rows = 0;
     uint32_t kp = 0;                   // candidates kept per query and CTA
     uint32_t cap = 0;                  // candidate buffer per query, ≥ kp + 128
-    float eps = 0.0f;                  // bound on |FP32 scan-order score − s̃|
+    const float* queries = nullptr;    // nq × ds normalised queries (their norms are taken in-kernel)
+    const float2* row_norms = nullptr; // per row {‖x‖, ‖x − tf32_head(x)‖}, rounded up
+    float c_norm = 0.0f;               // C of ε: accumulation and rounding terms per unit ‖q‖‖x‖
+    bool evict_first = true;           // L2 policy of the base loads (one query block: stream once)
     uint64_t* ws_keys = nullptr;       // nq × ctas × kp
     uint32_t* status = nullptr;
 };
 size_t tf32_smem_bytes(uint32_t stages, uint32_t cap);
 uint32_t tf32_stages_for(uint32_t cap, size_t smem_limit);
-// tmap_x: the FP32 base, box {32 floats, 128 rows}, 128-byte swizzle; tmap_qb / tmap_qs: the split
-// queries (nq rounded up to 16 rows), box {32 floats, 16 rows}, 128-byte swizzle.
-cudaError_t launch_scan_tf32(const CUtensorMap& tmap_x, const CUtensorMap& tmap_qb, const CUtensorMap& tmap_qs,
-                             const Tf32ScanArgs& a, uint32_t stages, uint32_t ctas, cudaStream_t stream);
-// qb / qs (nq_alloc × ds): the TF32 head and the rest of each normalised query value; padding rows 0.
-cudaError_t launch_split_queries_tf32(const float* qn, uint32_t nq, uint32_t ds, uint32_t nq_alloc, float* qb,
-                                      float* qs, cudaStream_t stream);
+// tmap_x: the FP32 base, box {32 floats, 128 rows}, 128-byte swizzle; tmap_q: the normalised
+// queries (nq rows; the rows past nq read as zeros), box {32 floats, 16 rows}, 128-byte swizzle.
+cudaError_t launch_scan_tf32(const CUtensorMap& tmap_x, const CUtensorMap& tmap_q, const Tf32ScanArgs& a,
+                             uint32_t stages, uint32_t ctas, cudaStream_t stream);
+// Per row of the base (stride ds): {‖x‖, ‖x − tf32_head(x)‖}, FP64 sums rounded up.
+cudaError_t launch_tf32_row_norms(const float* base, uint64_t rows, uint32_t ds, float2* out, uint32_t sm_count,
+                                  cudaStream_t stream);
 
 struct RerankArgs {
     const float* base = nullptr;  // FP32 base, stride ds
@@ -190,6 +194,11 @@ cudaError_t launch_max_reduce(const float* v, uint64_t n, unsigned int* out, cud
 constexpr uint32_t kMaxFusedK = 2048;
 
 // FP64 scores of (query, row) pairs: base rows of stride ds, queries of stride dims.
+// |sim − FP64 score| of each of nq × k results (rows idx, stride k; cnt may be null = k each) into
+// out, and acc = {max as double bits, sum as double, count} accumulated atomically.
+void launch_score_errors(const float* base, uint64_t ds, const float* queries, uint32_t nq, uint32_t k,
+                         const uint64_t* idx, const float* sim, const uint32_t* cnt, double* out,
+                         unsigned long long* acc, cudaStream_t stream);
 void launch_fp64_pairs(const float* base, uint64_t ds, const float* queries, uint64_t dims,
                        const uint64_t* pq, const uint64_t* pr, uint64_t n, double* out,
                        cudaStream_t stream);

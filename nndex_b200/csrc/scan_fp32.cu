@@ -418,6 +418,37 @@ __global__ void fp64_pairs_kernel(const float* __restrict__ base, uint64_t ds, c
     if (lane == 0) out[warp] = acc;
 }
 
+// Score error of each result: one warp per (query, slot) pair, |returned score − FP64 score of the
+// stored row with the normalised query|; slots past the query's count get 0. acc = {max (as the
+// bits of a non-negative double, which order like the values), sum, count}.
+__global__ void score_error_kernel(const float* __restrict__ base, uint64_t ds, const float* __restrict__ queries,
+                                   uint32_t nq, uint32_t k, const uint64_t* __restrict__ idx,
+                                   const float* __restrict__ sim, const uint32_t* __restrict__ cnt,
+                                   double* __restrict__ out, unsigned long long* __restrict__ acc) {
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (warp >= static_cast<uint64_t>(nq) * k) return;
+    const uint32_t q = static_cast<uint32_t>(warp / k), j = static_cast<uint32_t>(warp % k);
+    const uint32_t n = cnt ? cnt[q] : k;
+    if (j >= n) {
+        if (lane == 0) out[warp] = 0.0;
+        return;
+    }
+    const float* x = base + idx[warp] * ds;
+    const float* qv = queries + static_cast<uint64_t>(q) * ds;
+    double a = 0.0;
+    for (uint64_t d = lane; d < ds; d += 32) a = fma(static_cast<double>(x[d]), static_cast<double>(qv[d]), a);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) {
+        const double e = fabs(static_cast<double>(sim[warp]) - a);
+        out[warp] = e;
+        atomicMax(&acc[0], static_cast<unsigned long long>(__double_as_longlong(e)));
+        atomicAdd(reinterpret_cast<double*>(&acc[1]), e);
+        atomicAdd(&acc[2], 1ull);
+    }
+}
+
 // ------------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------------
@@ -630,6 +661,17 @@ cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream) {
                                                                 a.part_done);
     count_launch();
     return cudaGetLastError();
+}
+
+void launch_score_errors(const float* base, uint64_t ds, const float* queries, uint32_t nq, uint32_t k,
+                         const uint64_t* idx, const float* sim, const uint32_t* cnt, double* out,
+                         unsigned long long* acc, cudaStream_t stream) {
+    const uint64_t n = static_cast<uint64_t>(nq) * k;
+    if (n == 0) return;
+    const uint64_t blocks = (n * 32 + 255) / 256;
+    score_error_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(base, ds, queries, nq, k, idx, sim, cnt, out,
+                                                                        acc);
+    count_launch();
 }
 
 void launch_fp64_pairs(const float* base, uint64_t ds, const float* queries, uint64_t dims, const uint64_t* pq,

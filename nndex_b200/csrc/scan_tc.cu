@@ -74,7 +74,7 @@ size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp
     b += stream_a ? static_cast<size_t>(stages) * (kAChunk + kBChunk)
                   : static_cast<size_t>(nchunks) * kAChunk + static_cast<size_t>(stages) * kBChunk;
     b += static_cast<size_t>(kprime) * kM * 8;
-    b += fp8 ? 2 * kN * 4 : 0;
+    b += fp8 ? 2 * kN * 4 + 2 * 4 * 8 : 0;  // row scales and per-warp (min, max) of two tiles
     b += (2 * stages + 5) * 8 + 16;
     return b;
 }
@@ -166,7 +166,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint8_t* b_smem = a_smem + (kStreamA ? 0 : static_cast<size_t>(p.nchunks) * kAChunk);
     uint64_t* heap = reinterpret_cast<uint64_t*>(b_smem + static_cast<size_t>(kST) * kStage);
     float* scale_s = reinterpret_cast<float*>(heap + static_cast<size_t>(p.kprime) * kM);  // FP8: [2][256]
-    uint64_t* full_bar = reinterpret_cast<uint64_t*>(scale_s + (kFp8 ? 2 * kN : 0));
+    float2* scale_mm = reinterpret_cast<float2*>(scale_s + (kFp8 ? 2 * kN : 0));          // FP8: [2][4]
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(scale_mm + (kFp8 ? 2 * 4 : 0));
     uint64_t* empty_bar = full_bar + kST;
     uint64_t* a_full = empty_bar + kST;
     uint64_t* tfull = a_full + 1;
@@ -334,19 +335,42 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t buf = t & 1u, ub = t >> 1;
             const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * tile_step;
             const float* sc = scale_s + (t & 1u) * kN;
+            float smin = 0.0f, smax = 0.0f;
             if (kFp8) {
-                // Row scales of this tile, shared by the 128 queries (each applies its own scale).
+                // Row scales of this tile, shared by the 128 queries (each applies its own scale),
+                // and their extremes over the tile's rows.
                 float* w = scale_s + (t & 1u) * kN;
-                for (uint32_t j = et; j < static_cast<uint32_t>(kN); j += 128)
-                    w[j] = (tile_row0 + j < row_end) ? p.row_scale[tile_row0 + j] : 0.0f;
+                float lo = INFINITY, hi = 0.0f;
+                for (uint32_t j = et; j < static_cast<uint32_t>(kN); j += 128) {
+                    const bool in = tile_row0 + j < row_end;
+                    const float v = in ? p.row_scale[tile_row0 + j] : 0.0f;
+                    w[j] = v;
+                    if (in) {
+                        lo = fminf(lo, v);
+                        hi = fmaxf(hi, v);
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    lo = fminf(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+                    hi = fmaxf(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+                }
+                if (lane == 0) scale_mm[(t & 1u) * 4 + (warp - 2)] = make_float2(lo, hi);
                 named_bar_sync(2, 128);
+                smin = INFINITY;
+#pragma unroll
+                for (int w4 = 0; w4 < 4; ++w4) {
+                    const float2 m = scale_mm[(t & 1u) * 4 + w4];
+                    smin = fminf(smin, m.x);
+                    smax = fmaxf(smax, m.y);
+                }
             }
             if (!*abort_flag && !mbar_wait_bounded(&tfull[buf], ub & 1u, kWaitBudgetCycles)) {
                 *abort_flag = 1;
                 record_status(p.status, kStatusTimeout);
             }
             tc::fence_after_sync();
-            if (kMode == 0 && (t & 15u) == 15u && valid_q) {
+            if (kMode == 0 && (t & 3u) == 3u && valid_q) {
                 const unsigned long long g = p.thr_global[q];
                 if (g > st.thr_key) {
                     st.thr_key = g;
@@ -359,7 +383,31 @@ __global__ void __launch_bounds__(kThreads, 1)
             __syncwarp();
             tc::tmem_ld32(taddr, va);
             tmem_wait_ld_regs(va);
+            // The cut in the domain of the accumulator's raw scores. FP8 scores are scaled by the row's
+            // and the query's scales (both positive): a score can reach the cut only if its raw value
+            // reaches cut / (largest row scale · query scale) when cut ≥ 0, or cut / (smallest row
+            // scale · query scale) when cut < 0; 2⁻²⁰ of slack covers the roundings of both sides.
+            float raw_cut = st.cut;
+            if (kFp8) {
+                const float den = (st.cut >= 0.0f ? smax : smin) * qs;
+                raw_cut = (den > 0.0f) ? st.cut / den : -INFINITY;
+                raw_cut -= fabsf(raw_cut) * 9.5367431640625e-07f;
+                if (!(raw_cut == raw_cut)) raw_cut = -INFINITY;  // an infinite cut filters nothing here
+            }
             auto process = [&](const uint32_t(&v)[32], uint32_t c) {
+                // A padding lane (no query: past nq, or an empty slot of a gathered block) scores
+                // whatever its query row holds, +inf included; it never survives, since its
+                // index would address past the per-query outputs.
+                if (!valid_q) return;
+                // Almost every group of 32 scores is rejected by its largest one (a 5-level tree).
+                float m16[16];
+#pragma unroll
+                for (uint32_t j = 0; j < 16; ++j) m16[j] = fmaxf(__uint_as_float(v[j]), __uint_as_float(v[j + 16]));
+#pragma unroll
+                for (uint32_t w = 8; w > 0; w >>= 1)
+#pragma unroll
+                    for (uint32_t j = 0; j < w; ++j) m16[j] = fmaxf(m16[j], m16[j + w]);
+                if (!(m16[0] >= raw_cut)) return;
                 uint32_t mask = 0;
 #pragma unroll
                 for (uint32_t j = 0; j < 32; ++j) {
@@ -367,10 +415,6 @@ __global__ void __launch_bounds__(kThreads, 1)
                     if (kFp8) s = (s * sc[c * 32 + j]) * qs;
                     mask |= (s >= st.cut ? 1u : 0u) << j;
                 }
-                // A padding lane (no query: past nq, or an empty slot of a gathered block) scores
-                // whatever its query row holds, +inf included; it never survives, since its
-                // index would address past the per-query outputs.
-                if (!valid_q) mask = 0;
                 while (mask) {  // survivors are rare once a threshold exists
                     const uint32_t j = __ffs(mask) - 1;
                     mask &= mask - 1;

@@ -19,6 +19,13 @@
 // share is estimated from its queries and k (normalised queries, results, scan workspace, IVF
 // slots). A batch only grows while its estimate fits, a request that cannot fit any batch is refused,
 // and the queue is bounded in queries (NNDEX_ERR_ADMISSION: the caller may retry later).
+//
+// Admission by latency. With a latency budget, a request is also refused when the queries queued
+// ahead of it, with its own, would take longer than the budget to drain: slots run in parallel, so
+// the drain time is queued queries × (seconds per query in one slot) / slots, the per-query cost
+// being a moving average over the batches served (their wall time from launch to results). Under
+// overload the queue then stops growing, and the latency of admitted requests stays near the budget
+// plus one batch instead of rising without limit.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -74,6 +81,7 @@ struct Server {
     uint64_t next_ticket = 1, next_batch = 1;
     bool stopping = false;
     nndex_cuda_server_stats st{};
+    double spq = 0.0;  // moving average of one slot's wall seconds per query (0 until a batch ran)
 
     // Device bytes a batch of nq queries at k (capped) needs in a slot.
     uint64_t batch_bytes(uint64_t nq, uint64_t kcap, bool approx, uint32_t nprobe) const {
@@ -183,6 +191,9 @@ void Server::worker(uint32_t slot) {
         const uint32_t path = v->stats.path;
         {
             std::lock_guard<std::mutex> lk(mu);
+            const double per = static_cast<double>(t_done - t_start) * 1e-9 / static_cast<double>(nq);
+            spq = spq > 0.0 ? 0.9 * spq + 0.1 * per : per;
+            st.us_per_query = spq * 1e6;
             for (size_t i = 0; i < batch.size(); ++i) {
                 auto& r = batch[i];
                 r->status = codes[i];
@@ -299,6 +310,18 @@ int nndex_cuda_server_submit(nndex_cuda_server* server, const float* host_querie
             s->st.refused += 1;
             return set_error(NNDEX_ERR_ADMISSION, "cuda execution error: queue full (%llu queries waiting)",
                              (unsigned long long)s->st.queued_queries);
+        }
+        if (s->opts.latency_budget_ms && s->spq > 0.0) {
+            const double drain_ms =
+                static_cast<double>(s->st.queued_queries + r->nq) * s->spq * 1e3 / static_cast<double>(s->opts.slots);
+            if (drain_ms > static_cast<double>(s->opts.latency_budget_ms)) {
+                s->st.refused += 1;
+                s->st.refused_latency += 1;
+                return set_error(NNDEX_ERR_ADMISSION,
+                                 "cuda execution error: %llu queries waiting would take %.1f ms to drain, above the "
+                                 "%u ms latency budget",
+                                 (unsigned long long)s->st.queued_queries, drain_ms, s->opts.latency_budget_ms);
+            }
         }
         r->ticket = s->next_ticket++;
         r->info.submit_ns = now_ns();

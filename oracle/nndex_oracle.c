@@ -586,6 +586,63 @@ OR_API void or_kmeans_plusplus_init(const float* m, uint64_t rows, uint64_t dims
 }
 
 /*
+ * The assignment step of src/approx.rs:446-493 for `n` rows of `m` (their indices in `row_ids`):
+ * the strict `>` argmax of dot_small over the centroids, so the lowest centroid index wins ties.
+ */
+OR_API void or_kmeans_assign_rows(const float* m, uint64_t dims, const uint64_t* row_ids, uint64_t n,
+                                  const float* centroids, uint64_t nlist, uint32_t* assign) {
+#pragma omp parallel for schedule(dynamic, 256)
+    for (uint64_t i = 0; i < n; ++i) {
+        const float* row = m + row_ids[i] * dims;
+        uint32_t best_c = 0;
+        float best_s = -INFINITY;
+        for (uint64_t c = 0; c < nlist; ++c) {
+            float s = or_dot_small(row, centroids + c * dims, dims);
+            if (s > best_s) {
+                best_s = s;
+                best_c = (uint32_t)c;
+            }
+        }
+        assign[i] = best_c;
+    }
+}
+
+/*
+ * The update step of src/approx.rs:495-531 from an assignment: FP64 sums in row order, mean,
+ * renormalise with the 1e-30 guard, empty cluster → zero centroid; written into `centroids`.
+ */
+OR_API void or_kmeans_update(const float* m, uint64_t rows, uint64_t dims, uint64_t nlist,
+                             const uint32_t* assign, float* centroids) {
+    double* sums = (double*)calloc(nlist * dims, sizeof(double));
+    uint64_t* sizes = (uint64_t*)calloc(nlist, sizeof(uint64_t));
+    for (uint64_t r = 0; r < rows; ++r) {
+        uint32_t c = assign[r];
+        sizes[c] += 1;
+        const float* row = m + r * dims;
+        double* s = sums + (uint64_t)c * dims;
+        for (uint64_t d = 0; d < dims; ++d) s[d] += (double)row[d];
+    }
+    for (uint64_t c = 0; c < nlist; ++c) {
+        float* out = centroids + c * dims;
+        if (sizes[c] == 0) {
+            for (uint64_t d = 0; d < dims; ++d) out[d] = 0.0f;
+            continue;
+        }
+        double inv_count = 1.0 / (double)sizes[c];
+        const double* s = sums + c * dims;
+        double norm_sq = 0.0;
+        for (uint64_t d = 0; d < dims; ++d) {
+            double scaled = s[d] * inv_count;
+            norm_sq += scaled * scaled;
+        }
+        double inv_norm = norm_sq > 1e-30 ? 1.0 / sqrt(norm_sq) : 1.0;
+        for (uint64_t d = 0; d < dims; ++d) out[d] = (float)(s[d] * inv_count * inv_norm);
+    }
+    free(sums);
+    free(sizes);
+}
+
+/*
  * src/approx.rs:434-535 spherical_kmeans for `iters` iterations: assignment by strict `>`
  * argmax of dot_small (lowest centroid index wins ties), FP64 sums in row order, mean,
  * renormalise with the 1e-30 guard, empty cluster → zero centroid. `assign` receives the
@@ -593,51 +650,13 @@ OR_API void or_kmeans_plusplus_init(const float* m, uint64_t rows, uint64_t dims
  */
 OR_API void or_spherical_kmeans(const float* m, uint64_t rows, uint64_t dims, uint64_t nlist,
                                 uint64_t iters, float* centroids, uint32_t* assign) {
-    double* sums = (double*)malloc(sizeof(double) * nlist * dims);
-    uint64_t* sizes = (uint64_t*)malloc(sizeof(uint64_t) * nlist);
+    uint64_t* all = (uint64_t*)malloc(sizeof(uint64_t) * rows);
+    for (uint64_t r = 0; r < rows; ++r) all[r] = r;
     for (uint64_t it = 0; it < iters; ++it) {
-#pragma omp parallel for schedule(dynamic, 256)
-        for (uint64_t r = 0; r < rows; ++r) {
-            const float* row = m + r * dims;
-            uint32_t best_c = 0;
-            float best_s = -INFINITY;
-            for (uint64_t c = 0; c < nlist; ++c) {
-                float s = or_dot_small(row, centroids + c * dims, dims);
-                if (s > best_s) {
-                    best_s = s;
-                    best_c = (uint32_t)c;
-                }
-            }
-            assign[r] = best_c;
-        }
-        memset(sums, 0, sizeof(double) * nlist * dims);
-        memset(sizes, 0, sizeof(uint64_t) * nlist);
-        for (uint64_t r = 0; r < rows; ++r) {
-            uint32_t c = assign[r];
-            sizes[c] += 1;
-            const float* row = m + r * dims;
-            double* s = sums + (uint64_t)c * dims;
-            for (uint64_t d = 0; d < dims; ++d) s[d] += (double)row[d];
-        }
-        for (uint64_t c = 0; c < nlist; ++c) {
-            float* out = centroids + c * dims;
-            if (sizes[c] == 0) {
-                for (uint64_t d = 0; d < dims; ++d) out[d] = 0.0f;
-                continue;
-            }
-            double inv_count = 1.0 / (double)sizes[c];
-            const double* s = sums + c * dims;
-            double norm_sq = 0.0;
-            for (uint64_t d = 0; d < dims; ++d) {
-                double scaled = s[d] * inv_count;
-                norm_sq += scaled * scaled;
-            }
-            double inv_norm = norm_sq > 1e-30 ? 1.0 / sqrt(norm_sq) : 1.0;
-            for (uint64_t d = 0; d < dims; ++d) out[d] = (float)(s[d] * inv_count * inv_norm);
-        }
+        or_kmeans_assign_rows(m, dims, all, rows, centroids, nlist, assign);
+        or_kmeans_update(m, rows, dims, nlist, assign, centroids);
     }
-    free(sums);
-    free(sizes);
+    free(all);
 }
 
 typedef struct or_ivf {
@@ -858,10 +877,109 @@ OR_API uint64_t or_bench_search_single(const float* base, uint64_t rows, uint64_
 }
 
 /*
+ * Score blocks for the batch baseline: S[q][r] = dot(query q, row r) for a block of rows × queries,
+ * by a register-blocked FP32 micro-kernel (4 rows × 4 queries of vector accumulators along D, the
+ * matrixmultiply role in the reference's sgemm), chosen at run time: AVX-512 (16 lanes, 16 zmm
+ * accumulators) where the host has it, else AVX2 (8 lanes, 2 rows × 4 queries). Timing only: the
+ * summation order is the kernel's, not the reference's.
+ */
+#if defined(__x86_64__)
+#include <immintrin.h>
+
+__attribute__((target("avx512f"))) static void micro_4x4_avx512(const float* r0, const float* r1, const float* r2,
+                                                                const float* r3, const float* const* q,
+                                                                uint64_t dp, float out[4][4]) {
+    __m512 acc[4][4];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) acc[i][j] = _mm512_setzero_ps();
+    const float* rr[4] = {r0, r1, r2, r3};
+    uint64_t d = 0;
+    for (; d + 16 <= dp; d += 16) {
+        __m512 x[4], y[4];
+        for (int i = 0; i < 4; ++i) x[i] = _mm512_loadu_ps(rr[i] + d);
+        for (int j = 0; j < 4; ++j) y[j] = _mm512_loadu_ps(q[j] + d);
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) acc[i][j] = _mm512_fmadd_ps(x[i], y[j], acc[i][j]);
+    }
+    if (d < dp) {  /* padded dims are a multiple of 8: one masked half step */
+        const __mmask16 m = (__mmask16)((1u << (dp - d)) - 1u);
+        __m512 x[4], y[4];
+        for (int i = 0; i < 4; ++i) x[i] = _mm512_maskz_loadu_ps(m, rr[i] + d);
+        for (int j = 0; j < 4; ++j) y[j] = _mm512_maskz_loadu_ps(m, q[j] + d);
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) acc[i][j] = _mm512_fmadd_ps(x[i], y[j], acc[i][j]);
+    }
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) out[i][j] = _mm512_reduce_add_ps(acc[i][j]);
+}
+
+__attribute__((target("avx2,fma"))) static void micro_2x4_avx2(const float* r0, const float* r1,
+                                                               const float* const* q, uint64_t dp, float out[2][4]) {
+    __m256 acc[2][4];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 4; ++j) acc[i][j] = _mm256_setzero_ps();
+    for (uint64_t d = 0; d + 8 <= dp; d += 8) {
+        const __m256 x0 = _mm256_loadu_ps(r0 + d), x1 = _mm256_loadu_ps(r1 + d);
+        for (int j = 0; j < 4; ++j) {
+            const __m256 y = _mm256_loadu_ps(q[j] + d);
+            acc[0][j] = _mm256_fmadd_ps(x0, y, acc[0][j]);
+            acc[1][j] = _mm256_fmadd_ps(x1, y, acc[1][j]);
+        }
+    }
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 4; ++j) {
+            __m128 v = _mm_add_ps(_mm256_castps256_ps128(acc[i][j]), _mm256_extractf128_ps(acc[i][j], 1));
+            v = _mm_add_ps(v, _mm_movehl_ps(v, v));
+            v = _mm_add_ss(v, _mm_shuffle_ps(v, v, 1));
+            out[i][j] = _mm_cvtss_f32(v);
+        }
+}
+
+static int host_has_avx512(void) {
+    static int v = -1;
+    if (v < 0) v = __builtin_cpu_supports("avx512f") ? 1 : 0;
+    return v;
+}
+#endif
+
+/* Scores of rows [rb, re) of `base` against queries [qb, qe) into scores[q * ld + (r - rofs)]. */
+static void score_block(const float* base, uint64_t dp, uint64_t rb, uint64_t re, uint64_t rofs, const float* qs,
+                        uint64_t qb, uint64_t qe, float* scores, uint64_t ld) {
+    uint64_t q = qb;
+#if defined(__x86_64__)
+    const int wide = host_has_avx512();
+    for (; q + 4 <= qe; q += 4) {
+        const float* qp[4] = {qs + q * dp, qs + (q + 1) * dp, qs + (q + 2) * dp, qs + (q + 3) * dp};
+        uint64_t r = rb;
+        if (wide) {
+            for (; r + 4 <= re; r += 4) {
+                float o[4][4];
+                micro_4x4_avx512(base + r * dp, base + (r + 1) * dp, base + (r + 2) * dp, base + (r + 3) * dp, qp, dp, o);
+                for (int i = 0; i < 4; ++i)
+                    for (int j = 0; j < 4; ++j) scores[(q + j) * ld + (r + i - rofs)] = o[i][j];
+            }
+        } else {
+            for (; r + 2 <= re; r += 2) {
+                float o[2][4];
+                micro_2x4_avx2(base + r * dp, base + (r + 1) * dp, qp, dp, o);
+                for (int i = 0; i < 2; ++i)
+                    for (int j = 0; j < 4; ++j) scores[(q + j) * ld + (r + i - rofs)] = o[i][j];
+            }
+        }
+        for (; r < re; ++r)
+            for (int j = 0; j < 4; ++j) scores[(q + j) * ld + (r - rofs)] = fast_dot(base + r * dp, qp[j], dp);
+    }
+#endif
+    for (; q < qe; ++q)
+        for (uint64_t r = rb; r < re; ++r) scores[q * ld + (r - rofs)] = fast_dot(base + r * dp, qs + q * dp, dp);
+}
+
+/*
  * Batch: src/cpu.rs:256-284 Gemm (score matrix in blocks, then topk_from_scores per query) or
  * src/cpu.rs:291-341 GemmChunked (64 MB base chunks streamed into per-query accumulators), as
- * src/profiles.rs:151-185 picks for (rows, dims, nq). The score block is computed by a
- * register-blocked FP32 kernel (the matrixmultiply role).
+ * src/profiles.rs:151-185 picks for (rows, dims, nq). Each thread scores a block of 64 rows against
+ * every query (the block stays in its core's cache while the queries pass over it, so the base is
+ * read from memory once per batch) with the register-blocked micro-kernel of score_block.
  */
 OR_API void or_bench_search_batch(const float* base, uint64_t rows, uint64_t dp, const float* qs,
                                   uint64_t nq, uint64_t k, uint64_t* idx, float* sim) {
@@ -875,15 +993,15 @@ OR_API void or_bench_search_batch(const float* base, uint64_t rows, uint64_t dp,
     for (uint64_t q = 0; q < nq; ++q) accs[q] = or_topk_new(k);
     for (uint64_t r0 = 0; r0 < rows; r0 += chunk_rows) {
         uint64_t nr = rows - r0 < chunk_rows ? rows - r0 : chunk_rows;
-        const uint64_t RB = 64, QB = 8;
-#pragma omp parallel for collapse(2) schedule(dynamic, 1)
-        for (uint64_t rb = 0; rb < nr; rb += RB)
+        const uint64_t RB = 64, QB = 64;
+#pragma omp parallel for schedule(dynamic, 1)
+        for (uint64_t rb = 0; rb < nr; rb += RB) {
+            uint64_t re = rb + RB < nr ? rb + RB : nr;
             for (uint64_t qb = 0; qb < nq; qb += QB) {
-                uint64_t re = rb + RB < nr ? rb + RB : nr, qe = qb + QB < nq ? qb + QB : nq;
-                for (uint64_t r = rb; r < re; ++r)
-                    for (uint64_t q = qb; q < qe; ++q)
-                        scores[q * chunk_rows + r] = fast_dot(base + (r0 + r) * dp, qs + q * dp, dp);
+                uint64_t qe = qb + QB < nq ? qb + QB : nq;
+                score_block(base, dp, r0 + rb, r0 + re, r0, qs, qb, qe, scores, chunk_rows);
             }
+        }
         if (!chunked) {
 #pragma omp parallel for schedule(dynamic, 1)
             for (uint64_t q = 0; q < nq; ++q) {

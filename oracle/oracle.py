@@ -70,6 +70,8 @@ def lib():
         "or_pick_medoid_row": (_u64, [_f32p, _u64, _u64]),
         "or_kmeans_plusplus_init": (None, [_f32p, _u64, _u64, _u64, C.c_int, _u64, _f32p, _u64p]),
         "or_spherical_kmeans": (None, [_f32p, _u64, _u64, _u64, _u64, _f32p, _u32p]),
+        "or_kmeans_assign_rows": (None, [_f32p, _u64, _u64p, _u64, _f32p, _u64, _u32p]),
+        "or_kmeans_update": (None, [_f32p, _u64, _u64, _u64, _u32p, _f32p]),
         "or_ivf_build": (C.c_void_p, [_f32p, _u64, _u64, _u64, _u64, C.c_int, _u64]),
         "or_ivf_from_layout": (C.c_void_p, [_f32p, _u64, _u64, _u64, _f32p, _u64p, _u64p]),
         "or_ivf_free": (None, [C.c_void_p]),
@@ -278,6 +280,37 @@ def choose_nlist(rows: int) -> int:
 
 def choose_nprobe(nlist: int, k: int, rows: int) -> int:
     return int(lib().or_choose_nprobe(nlist, k, rows))
+
+
+def kmeans_plusplus_init(storage: np.ndarray, nlist: int, seed: int | None = None):
+    """src/approx.rs:357-406: the first `nlist` k-means++ picks (the medoid first) and their rows.
+    The picks do not depend on how many follow, so a small nlist gives a prefix of a larger one's."""
+    m = _c(storage, np.float32)
+    rows, dims = m.shape
+    cent = np.zeros((nlist, dims), np.float32)
+    chosen = np.zeros(nlist, np.uint64)
+    lib().or_kmeans_plusplus_init(m, rows, dims, nlist, 0 if seed is None else 1, 0 if seed is None else seed,
+                                  cent, chosen)
+    return chosen, cent
+
+
+def kmeans_assign_rows(storage: np.ndarray, row_ids: np.ndarray, centroids: np.ndarray) -> np.ndarray:
+    """src/approx.rs:446-493: the assignment of the given rows (strict `>` argmax of dot_small)."""
+    m = _c(storage, np.float32)
+    ids = _c(row_ids, np.uint64)
+    cent = _c(centroids, np.float32)
+    out = np.zeros(ids.shape[0], np.uint32)
+    lib().or_kmeans_assign_rows(m, m.shape[1], ids, ids.shape[0], cent, cent.shape[0], out)
+    return out
+
+
+def kmeans_update(storage: np.ndarray, assign: np.ndarray, nlist: int) -> np.ndarray:
+    """src/approx.rs:495-531: the centroids one update makes from an assignment."""
+    m = _c(storage, np.float32)
+    a = _c(assign, np.uint32)
+    out = np.zeros((nlist, m.shape[1]), np.float32)
+    lib().or_kmeans_update(m, m.shape[0], m.shape[1], nlist, a, out)
+    return out
 
 
 class IvfIndex:

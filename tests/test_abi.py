@@ -40,7 +40,7 @@ def test_structs_match_header_layout():
     # sizes of the C structs as the header lays them out (x86-64)
     assert C.sizeof(_lib.Opts) == 4 + 4 * 5 + 8 + 4 + 4 * 7
     assert C.sizeof(_lib.DevInfo) == 8 + 256 + 64 + 64 + 32 + 32 + 4 * 3 + 4 + 8 + 8
-    assert C.sizeof(_lib.SearchStats) == 4 * 6 + 8 + 8 + 8 + 8 + 8 + 4 * 4
+    assert C.sizeof(_lib.SearchStats) == 4 * 6 + 8 + 8 + 8 + 8 + 8 + 4 * 4 + 8 + 8 + 4 * 2
 
 
 def test_last_error_is_empty_string_initially():
@@ -104,6 +104,8 @@ def test_null_index_is_refused_without_touching_the_device():
         ("set_nprobe", lambda: L.nndex_cuda_set_nprobe(None, 8)),
         ("set_graphs", lambda: L.nndex_cuda_set_graphs(None, 1)),
         ("set_scan_timing", lambda: L.nndex_cuda_set_scan_timing(None, 1)),
+        ("set_error_report", lambda: L.nndex_cuda_set_error_report(None, 1)),
+        ("last_score_errors", lambda: L.nndex_cuda_last_score_errors(None, 1, 1, None)),
         ("server_start", lambda: L.nndex_cuda_server_start(None, None, C.byref(C.c_void_p()))),
         ("server_submit", lambda: L.nndex_cuda_server_submit(None, None, 1, 1, 1, 0, 0, C.byref(u64))),
         ("server_poll", lambda: L.nndex_cuda_server_poll(None, 1, 0, None, None, None, None)),

@@ -1,8 +1,11 @@
 """Host-side logic of the Python mirror (no GPU): argument parsing and marshalling rules."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
 import nndex_b200 as nb
+from nndex_b200 import _lib
 
 
 def test_parse_backend():
@@ -82,3 +85,25 @@ def test_tf32_split_error_term():
             bound = 3 * 2.0 ** -20 * np.abs(x.astype(np.float64) * q.astype(np.float64))
             assert np.all(err <= bound)
         assert np.abs((x.astype(np.float64) * q).sum()) <= 1 + 1e-6
+
+
+def test_autotune_cache_text_is_validated_without_a_gpu():
+    # the tuner's export format: a header naming device, shape and flags, then one line per shape
+    L = _lib.lib()
+    n = C.c_uint64(0)
+    good = (b"nndex-autotune v1 device=NVIDIA_B200 rows=1000000 dims=768 flags=1\n"
+            b"shape ivf=0 nq=16 k=128 precision=0 nprobe=0 plan path=6 stride=0 ms=0.512\n"
+            b"shape ivf=1 nq=1024 k=16 precision=3 nprobe=32 plan path=5 stride=0 ms=2.5\n\n")
+    assert L.nndex_cuda_autotune_validate(good, C.byref(n)) == 0 and n.value == 2
+    bad = [
+        b"shape ivf=0 nq=16 k=128 precision=0 nprobe=0 plan path=6 stride=0 ms=0.5\n",  # no header
+        good + b"shape ivf=0 nq=12 k=128 precision=0 nprobe=0 plan path=1 stride=0 ms=1\n",  # nq not 2^n
+        good + b"shape ivf=0 nq=16 k=16 precision=0 nprobe=0 plan path=4 stride=0 ms=1\n",  # IVF path, exact shape
+        good + b"shape ivf=1 nq=16 k=16 precision=0 nprobe=8 plan path=2 stride=0 ms=1\n",  # exact path, IVF shape
+        good + b"shape ivf=0 nq=16 k=16 precision=0 nprobe=0 plan path=9 stride=0 ms=1\n",  # no such path
+        good + b"garbage\n",
+    ]
+    for text in bad:
+        assert L.nndex_cuda_autotune_validate(text, C.byref(n)) == _lib.NNDEX_ERR_INVALID_ARGUMENT, text
+        assert "autotune text" in _lib.last_error()
+    assert L.nndex_cuda_autotune_validate(None, C.byref(n)) == _lib.NNDEX_ERR_INVALID_ARGUMENT

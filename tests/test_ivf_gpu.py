@@ -226,7 +226,7 @@ def test_ivf_tensor_core_scan_equals_fp32_scan(name, rows, dims, nlist, nq, k, n
     # the tensor-core list scan (certified BF16 candidates + exact FP32 rerank) returns the FP32 list
     # scan's result: the same probed rows, the same exact scores, bit for bit
     m = make_data("zipf" if name == "zipf" else "mixture", rows, dims)
-    index = NNdex(m, approx=True, precision="auto", nlist=nlist, kmeans_iters=3, seed=42, nprobe=nprobe)
+    index = NNdex(m, approx=True, precision="auto", nlist=nlist, kmeans_iters=3, seed=42, nprobe=nprobe, autotune=False)
     q = make_data("mixture", nq, dims, seed=13)
     ti, ts = index.search(q, k=k)
     st = index.last_search_stats()

@@ -25,10 +25,10 @@ def _bitwise(a, b):
 @pytest.mark.parametrize("precision", ["fp32", "auto"])
 def test_restored_index_answers_like_the_built_one(tmp_path, precision):
     base, q = _mixture(60_000, 128, 300, seed=11)
-    built = NNdex(base, approx=True, precision=precision, seed=7)
+    built = NNdex(base, approx=True, precision=precision, seed=7, autotune=False)
     path = tmp_path / "ivf.npz"
     built.save_ivf(str(path))
-    restored = NNdex(base, approx=True, precision=precision, ivf=str(path))
+    restored = NNdex(base, approx=True, precision=precision, ivf=str(path), autotune=False)
     la, lb = built.ivf_layout(), restored.ivf_layout()
     for key in la:
         assert np.array_equal(la[key], lb[key]), key

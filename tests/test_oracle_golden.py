@@ -244,3 +244,19 @@ def test_ivf_structure_valid():
     assert ivf.nlist == O.choose_nlist(rows)
     small = O.IvfIndex(np.ones((100, 32), np.float32))
     assert not small.provides_speedup()
+
+
+def test_kmeans_steps_restate_the_build():
+    # the exported steps recompose the build: k-means++ picks are a prefix of a larger nlist's, the
+    # last assignment is the argmax over the previous centroids, and the centroids are one update
+    rng = np.random.default_rng(9)
+    m = rng.normal(size=(3000, 24)).astype(np.float32)
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    full = O.IvfIndex(m, nlist=20, iters=3, seed=42)
+    prev = O.IvfIndex(m, nlist=20, iters=2, seed=42)
+    chosen, _ = O.kmeans_plusplus_init(m, 7, seed=42)
+    np.testing.assert_array_equal(full.init_rows[:7], chosen)
+    a = O.kmeans_assign_rows(m, np.arange(3000, dtype=np.uint64), prev.centroids)
+    np.testing.assert_array_equal(a, full.assignments)
+    np.testing.assert_array_equal(O.kmeans_update(m, a, 20).view(np.uint32), full.centroids.view(np.uint32))
+    np.testing.assert_array_equal(full.original_indices, np.argsort(a, kind="stable"))

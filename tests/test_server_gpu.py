@@ -111,3 +111,34 @@ def test_poll_without_waiting_and_unknown_ticket(index):
         assert r[0].shape == (3, 5)
         with pytest.raises(KeyError):
             s.poll(t)
+
+
+def test_latency_budget_refuses_when_the_queue_would_drain_too_slowly(index):
+    # the per-query cost from a first server sets a budget that one request meets with room to
+    # spare; a burst queued at once then overflows it and part of it is refused, while the
+    # admitted requests still get the index's own answers
+    reqs = requests(60, index.dims, seed=11)
+    with Server(index, slots=1) as s:
+        for q, k, approx in reqs[:4]:
+            s.result(s.submit(q, k=k, approx=approx))
+        us = s.stats()["us_per_query"]
+    assert us > 0
+    budget = max(1, int(np.ceil(3 * 256 * us / 1000)))
+    with Server(index, slots=1, latency_budget_ms=budget) as s:
+        q0, k0, a0 = reqs[0]
+        s.result(s.submit(q0, k=k0, approx=a0))
+        admitted, refused = [], 0
+        for q, k, approx in reqs[1:]:
+            try:
+                admitted.append((s.submit(q, k=k, approx=approx), q, k, approx))
+            except NNdexError as e:
+                assert e.code == NNDEX_ERR_ADMISSION and "latency budget" in str(e)
+                refused += 1
+        results = [(s.result(t), q, k, approx) for t, q, k, approx in admitted]
+        st = s.stats()
+    assert refused > 0 and st["refused_latency"] == refused, (refused, st, budget)
+    assert admitted, "nothing admitted"
+    for (ri, rs), q, k, approx in results:
+        if not approx:
+            ei, es = index.search(q, k=k)
+            np.testing.assert_array_equal(ri, np.atleast_2d(ei))

@@ -131,7 +131,7 @@ def test_pass2_padding_lanes_ignore_stale_memory():
     rng = np.random.default_rng(21)
     m = np.abs(mixture(rng, 40_000, 128, 128, 0.25)) + np.float32(0.05)
     q = np.abs(mixture(np.random.default_rng(22), 200, 128, 128, 0.25)) + np.float32(0.05)
-    index = NNdex(m, precision="bf16")
+    index = NNdex(m, precision="bf16", autotune=False)
     index.set_precision("fp32")
     fi, fs = index.search(q, k=10)
     junk = torch.full((1 << 29,), 0x7F80, dtype=torch.int16, device="cuda")  # 1 GiB of BF16 +inf

@@ -1,11 +1,11 @@
-"""FP32-accurate TF32 candidate scan (batches of 9-16 queries) against the FP32 scan and the FP64
-oracle (needs a B200).
+"""TF32 candidate scan (batches of 9-16 queries of an FP32 index) against the FP32 scan and the
+FP64 oracle (needs a B200).
 
-With NNDEX_TF32_SCAN=1, batches of 9 to 16 queries take the tensor-core candidate scan with the
-exact rerank; batches of 8 or fewer take the FP32 scan. A certified query's rows and scores are
-the FP32 scan's, bit for bit (the rerank sums in the FP32 scan's order); an uncertified one is
-re-run on the FP32 scan. So each query of a 16-query batch must equal its result from two
-8-query batches, bit for bit.
+Batches of 9 to 16 queries take the tensor-core candidate scan (one TF32 product per row and
+query, ranked by an upper bound) with the exact rerank; batches of 8 or fewer take the FP32 scan. A
+certified query's rows and scores are the FP32 scan's, bit for bit (the rerank sums in the FP32
+scan's order); an uncertified one is re-run on the FP32 scan. So each query of a 16-query batch
+must equal its result from two 8-query batches, bit for bit.
 """
 import numpy as np
 import pytest
@@ -15,12 +15,6 @@ from oracle import oracle as O
 from tests._parity import assert_topk_matches
 
 pytestmark = pytest.mark.gpu
-
-
-@pytest.fixture(autouse=True)
-def tf32_scan_on(monkeypatch):
-    # the TF32 candidate scan is opt-in (read on every search)
-    monkeypatch.setenv("NNDEX_TF32_SCAN", "1")
 
 
 def mixture(rng, rows, dims, centers, sigma, center_seed=77):
@@ -47,7 +41,7 @@ def test_tf32_scan_equals_fp32_scan(rows, dims, nq, k, data):
     else:
         m = rng.normal(size=(rows, dims)).astype(np.float32)
         q = rng.normal(size=(nq, dims)).astype(np.float32)
-    index = NNdex(m)
+    index = NNdex(m, autotune=False)
     ti, ts = index.search(q, k=k)
     st = index.last_search_stats()
     assert st["path"] == 6, st
@@ -73,7 +67,44 @@ def test_tf32_scan_certifies_the_benchmark_mixture():
     m /= np.linalg.norm(m, axis=1, keepdims=True)
     q = mixture(np.random.default_rng(13), 16, 768, 1024, 0.3, center_seed=1)
     q /= np.linalg.norm(q, axis=1, keepdims=True)
-    index = NNdex(m, normalized=True)
+    index = NNdex(m, normalized=True, autotune=False)
     index.search(q, k=100)
     st = index.last_search_stats()
     assert st["path"] == 6 and st["fp32_fallback_queries"] == 0, st
+
+
+def _equal_to_fp32_scan(index, q, k):
+    ti, ts = index.search(q, k=k)
+    st = index.last_search_stats()
+    parts = [index.search(q[lo:lo + 8].copy(), k=k) for lo in range(0, len(q), 8)]
+    assert index.last_search_stats()["path"] == 1
+    np.testing.assert_array_equal(ti, np.vstack([p[0] for p in parts]))
+    np.testing.assert_array_equal(ts.view(np.uint32), np.vstack([p[1] for p in parts]).view(np.uint32))
+    return st
+
+
+def test_tf32_scan_bound_follows_row_and_query_norms():
+    # normalized=true keeps the caller's rows and queries as they are: norms from 0.01 to 100, so
+    # the bound must scale with ‖q‖‖x‖ (a unit-norm bound would drop true neighbours)
+    rng = np.random.default_rng(31)
+    m = mixture(rng, 60_000, 192, 128, 0.3)
+    m *= (10.0 ** rng.uniform(-2, 2, size=(60_000, 1))).astype(np.float32)
+    q = mixture(np.random.default_rng(32), 16, 192, 128, 0.3)
+    q *= (10.0 ** np.random.default_rng(33).uniform(-2, 2, size=(16, 1))).astype(np.float32)
+    index = NNdex(m, normalized=True, autotune=False)
+    st = _equal_to_fp32_scan(index, q, 50)
+    assert st["path"] == 6, st
+
+
+def test_tf32_scan_ties_fall_back_to_the_fp32_scan():
+    # 3,000 copies of one row: the k-th and the k'-th scores are equal, the certificate cannot
+    # hold, and the queries are re-run on the FP32 scan (lowest row index first among the ties)
+    rng = np.random.default_rng(41)
+    m = rng.normal(size=(20_000, 64)).astype(np.float32)
+    m[5_000:8_000] = m[5_000]
+    q = np.repeat(m[5_000:5_001], 12, axis=0) + np.float32(1e-3) * rng.normal(size=(12, 64)).astype(np.float32)
+    index = NNdex(m, autotune=False)
+    st = _equal_to_fp32_scan(index, q, 20)
+    assert st["path"] == 6 and st["fp32_fallback_queries"] == 12, st
+    ti, _ = index.search(q, k=20)
+    assert ti[0].tolist() == list(range(5_000, 5_020))
