@@ -239,6 +239,9 @@ CudaIndex::~CudaIndex() {
     cudaFree(d_serr);
     cudaFree(d_serr_acc);
     cudaFreeHost(h_serr_acc);
+    cudaFree(d_fbq);
+    cudaFree(d_fbn);
+    cudaFreeHost(h_fbn);
     cudaFree(d_thr);
     cudaFree(d_cand_idx);
     cudaFree(d_cand_sim);
@@ -677,94 +680,101 @@ int CudaIndex::encode_query_tmap(bool fp8, void* buf, uint32_t n, CUtensorMap* m
     return NNDEX_OK;
 }
 
-// After pass 1: queries whose certificate held are final. The others run pass 2 (collect every row
-// whose upper bound reaches their exact k-th score, rerank exactly); a query whose collected set
-// overflows is re-run on the FP32 scan. Synchronises the stream.
-int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
-                         cudaStream_t s) {
-    int st;
-    if ((st = grow_host(h_cert, cap_hcert, n, "pinned buffer"))) return st;
-    cudaMemcpyAsync(h_cert, d_cert, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    h_flags[1] = 0;
-    cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cuda_error(e, "search");
-    if ((st = check_device_words())) return st;
-    last_tc_n = n;
-    const bool fp8 = stats.path == 3;
-    uint32_t m = 0;
-    if ((st = grow_host(h_ids, cap_hids, n, "pinned buffer"))) return st;
-    for (uint32_t i = 0; i < n; ++i)
-        if (!h_cert[i]) h_ids[m++] = i;
-    stats.certified = m == 0 ? 1u : 0u;
-    stats.second_pass_queries = m;
-    // The rule for the next batch (when no tuned plan fixes the stride): a full pass 1 pays off only
-    // when it certifies most queries.
-    if (!forced_stride) {
-        if (last_tc_stride == 1) tc_sample_stride = (m * 2 > n) ? 8u : 1u;
-        else if (m * 2 <= n) tc_sample_stride = 1;
-    }
-    if (m == 0) return NNDEX_OK;
+int CudaIndex::ensure_fbn() {
+    if (d_fbn) return NNDEX_OK;
+    cudaError_t e;
+    if ((e = cudaMalloc(&d_fbn, 4 * sizeof(uint32_t))) != cudaSuccess ||
+        (e = cudaMallocHost(&h_fbn, 4 * sizeof(uint32_t))) != cudaSuccess)
+        return cuda_error(e, "fallback buffer");
+    return NNDEX_OK;
+}
 
-    // ---- pass 2 ----
+// After pass 1: queries whose certificate held are final. The others run pass 2 (collect every row
+// whose upper bound reaches their exact k-th score, rerank exactly) — all on the device, sized for
+// the worst case (every query uncertified), the kernels reading the count that the compaction left.
+int CudaIndex::enqueue_tc_pass2(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim,
+                                uint32_t* o_cnt, cudaStream_t s) {
+    int st;
     const uint32_t cap2 = kSecondPassCap;
     const uint64_t row_bytes = fp8 ? kf8 : kb16 * 2;
-    const uint64_t m_alloc = (m + 127) / 128 * 128;
-    if ((st = grow_device(d_ids, cap_ids, m, "pass-2 buffer"))) return st;
-    if ((st = grow_device(d_q2_lp, cap_q2_lp, m_alloc * row_bytes, "pass-2 buffer"))) return st;
-    if ((st = grow_device(d_q2_resid, cap_q2_resid, m, "pass-2 buffer"))) return st;
-    if ((st = grow_device(d_q2_scale, cap_q2_scale, m, "pass-2 buffer"))) return st;
-    if ((st = grow_device(d_q2_thr, cap_q2_thr, m, "pass-2 buffer"))) return st;
-    if ((st = grow_device(d_rows2, cap_rows2, static_cast<uint64_t>(m) * cap2, "pass-2 buffer"))) return st;
-    if ((st = grow_device(d_cnt2, cap_cnt2, m, "pass-2 buffer"))) return st;
-    if ((st = grow_device(d_ok2, cap_ok2, m, "pass-2 buffer"))) return st;
-    cudaMemcpyAsync(d_ids, h_ids, m * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
-    e = launch_gather_queries(d_ids, m, fp8 ? static_cast<const void*>(d_q_fp8) : static_cast<const void*>(d_q_bf16),
-                              static_cast<uint32_t>(row_bytes), d_q2_lp, d_q_resid, d_q2_resid,
-                              fp8 ? d_q_scale : nullptr, d_q2_scale, d_kth, d_q2_thr, s);
+    const uint64_t n_alloc = (n + 127) / 128 * 128;
+    if ((st = ensure_fbn())) return st;
+    if ((st = grow_device(d_ids, cap_ids, n, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_q2_lp, cap_q2_lp, n_alloc * row_bytes, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_q2_resid, cap_q2_resid, n, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_q2_scale, cap_q2_scale, n, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_q2_thr, cap_q2_thr, n, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_rows2, cap_rows2, static_cast<uint64_t>(n) * cap2, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_cnt2, cap_cnt2, n, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_ok2, cap_ok2, n, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_tcfail, cap_tcfail, n, "pass-2 buffer"))) return st;
+    uint32_t* d_m = d_fbn + 1;      // uncertified queries
+    uint32_t* d_fail = d_fbn + 2;   // of them, collections that overflowed
+    launch_compact_zero_flags(d_cert, n, d_ids, d_m, s);
+    cudaError_t e = launch_gather_queries(d_ids, n, fp8 ? static_cast<const void*>(d_q_fp8)
+                                                         : static_cast<const void*>(d_q_bf16),
+                                          static_cast<uint32_t>(row_bytes), d_q2_lp, d_q_resid, d_q2_resid,
+                                          fp8 ? d_q_scale : nullptr, d_q2_scale, d_kth, d_q2_thr, s, d_m);
     if (e != cudaSuccess) return cuda_error(e, "gather launch");
-    cudaMemsetAsync(d_cnt2, 0, m * sizeof(uint32_t), s);
+    cudaMemsetAsync(d_cnt2, 0, n * sizeof(uint32_t), s);
     CUtensorMap tmap_q2;
-    if ((st = encode_query_tmap(fp8, d_q2_lp, m, &tmap_q2))) return st;
-    uint64_t nranges = 0, range_rows = 0;
-    tc_ranges((m + 127) / 128, nranges, range_rows);
+    if ((st = encode_query_tmap(fp8, d_q2_lp, n, &tmap_q2))) return st;
     TcArgs a;
     a.tmap_q = &tmap_q2;
     a.tmap_b = fp8 ? &tmap_fp8 : &tmap_bf16;
-    a.nranges = static_cast<uint32_t>(nranges);
     const TcPlan plan2 = plan_tc(0, fp8);
     a.stages = plan2.stages;
     a.stream_a = plan2.stream_a;
-    fill_tc_params(fp8, m, range_rows, a.p);
+    fill_tc_params(fp8, n, 0, a.p);
     a.p.q_resid = d_q2_resid;
     a.p.q_scale = fp8 ? d_q2_scale : nullptr;
     a.p.q_thr = d_q2_thr;
     a.p.cand_rows = d_rows2;
     a.p.cand_cnt = d_cnt2;
     a.p.cap2 = cap2;
+    a.p.live_q = d_m;
+    a.p.sm_count = static_cast<uint32_t>(sm_count);
+    // (query block, row range) items for any count ≤ n: at most 4 per SM plus one per block
+    a.live_items = 4u * static_cast<uint32_t>(sm_count) + static_cast<uint32_t>(n_alloc / 128) + 1u;
     cudaEvent_t ev_a = nullptr;
     scan_event_begin(s, ev_a);
     e = launch_scan_tc(a, fp8, 1, s);
     scan_event_end(s, ev_a);
     if (e != cudaSuccess) return cuda_error(e, "tensor-core scan launch (pass 2)");
-    e = launch_rerank_collected(d_base, static_cast<uint32_t>(ds), d_qn, d_ids, m, d_rows2, d_cnt2, cap2, kcap, o_idx,
-                                o_sim, o_cnt, d_ok2, s);
+    e = launch_rerank_collected(d_base, static_cast<uint32_t>(ds), d_qn, d_ids, n, d_rows2, d_cnt2, cap2, kcap, o_idx,
+                                o_sim, o_cnt, d_ok2, s, false, d_m);
     if (e != cudaSuccess) return cuda_error(e, "rerank launch (pass 2)");
-    stats.kernel_launches += 3;
-    if ((st = grow_host(h_ok2, cap_hok2, m, "pinned buffer"))) return st;
-    cudaMemcpyAsync(h_ok2, d_ok2, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    h_flags[1] = 0;
-    cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    e = cudaStreamSynchronize(s);
+    launch_compact_zero_flags(d_ok2, n, d_tcfail, d_fail, s, d_m);
+    stats.kernel_launches += 5;
+    last_tc_n = n;
+    return NNDEX_OK;
+}
+
+int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                         cudaStream_t s) {
+    const uint32_t m = h_fbn[1], failed_n = h_fbn[2];
+    stats.certified = m == 0 ? 1u : 0u;
+    stats.second_pass_queries = m;
+    // The rule for the next batch (when no tuned plan fixes the stride): a full pass 1 pays off only
+    // when it certifies most queries.
+    if (!forced_stride) {
+        const uint32_t before = tc_sample_stride;
+        if (last_tc_stride == 1) tc_sample_stride = (m * 2 > n) ? 8u : 1u;
+        else if (m * 2 <= n) tc_sample_stride = 1;
+        if (tc_sample_stride != before) drop_graphs();  // a captured batch keeps its stride
+    }
+    stats.fp32_fallback_queries = failed_n;
+    if (failed_n == 0) return NNDEX_OK;
+    // ---- the FP32 scan for queries whose collected set overflowed ----
+    int st;
+    if ((st = grow_host(h_ids, cap_hids, n, "pinned buffer"))) return st;
+    if ((st = grow_host(h_ok2, cap_hok2, n, "pinned buffer"))) return st;
+    cudaMemcpyAsync(h_ids, d_ids, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h_ok2, d_tcfail, failed_n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_error(e, "search");
-    if ((st = check_device_words())) return st;
-    std::vector<uint32_t> failed;
-    for (uint32_t i = 0; i < m; ++i)
-        if (!h_ok2[i]) failed.push_back(h_ids[i]);
-    stats.fp32_fallback_queries = static_cast<uint32_t>(failed.size());
-    if (failed.empty()) return NNDEX_OK;
-    // ---- FP32 scan for queries whose collected set overflowed ----
+    std::vector<uint32_t> failed(failed_n);
+    for (uint32_t i = 0; i < failed_n; ++i) failed[i] = h_ids[h_ok2[i]];
     return rerun_exact_fp32(failed, kcap, o_idx, o_sim, o_cnt, s);
 }
 
@@ -805,7 +815,23 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     const uint32_t kp = plan.kp;
     const uint32_t ctas = static_cast<uint32_t>(sm_count);
     const uint64_t per_query = static_cast<uint64_t>(ctas) * kp;
-    if ((st = grow_device(d_ws, cap_ws, per_query * n, "scan workspace"))) return st;
+    // the FP32 scan that re-runs uncertified queries shares the candidate workspace
+    ScanPlan fb_plan;
+    if (!plan_scan_fp32(n, static_cast<uint32_t>(ds), kcap, sm_count, smem_optin, fb_plan))
+        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: no FP32 scan plan for k=%u", kcap);
+    const uint64_t fb_per_query = static_cast<uint64_t>(fb_plan.ctas_per_group) * kcap;
+    if ((st = grow_device(d_ws, cap_ws, std::max(per_query, fb_per_query) * n, "scan workspace"))) return st;
+    if ((st = grow_device(d_qsub, cap_qsub, static_cast<uint64_t>(n) * ds, "fallback buffer"))) return st;
+    if ((st = grow_device(d_fb_idx, cap_fb_idx, static_cast<uint64_t>(n) * kcap, "fallback buffer"))) return st;
+    if ((st = grow_device(d_fb_sim, cap_fb_sim, static_cast<uint64_t>(n) * kcap, "fallback buffer"))) return st;
+    if ((st = grow_device(d_fb_cnt, cap_fb_cnt, n, "fallback buffer"))) return st;
+    if ((st = grow_device(d_fbq, cap_fbq, n, "fallback buffer"))) return st;
+    if (!d_fbn) {
+        cudaError_t e0;
+        if ((e0 = cudaMalloc(&d_fbn, 4 * sizeof(uint32_t))) != cudaSuccess ||
+            (e0 = cudaMallocHost(&h_fbn, 4 * sizeof(uint32_t))) != cudaSuccess)
+            return cuda_error(e0, "fallback buffer");
+    }
     if ((st = grow_device(d_cand_idx, cap_cand_idx, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
     if ((st = grow_device(d_cand_sim, cap_cand_sim, static_cast<uint64_t>(n) * kp, "tc workspace"))) return st;
     if ((st = grow_device(d_cand_cnt, cap_cand_cnt, n, "tc workspace"))) return st;
@@ -863,33 +889,58 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     r.kth_out = d_kth;
     r.certify = true;
     if ((e = launch_rerank(r, s)) != cudaSuccess) return cuda_error(e, "rerank launch");
-    stats.kernel_launches += 3;
+    // Uncertified queries re-run on the FP32 scan, on the device: compaction, gather, the scan and
+    // its merge (both return at once when every query certified), scatter into the outputs.
+    launch_compact_zero_flags(d_cert, n, d_fbq, d_fbn, s);
+    launch_gather_rows(d_qn, static_cast<uint32_t>(ds), d_fbq, d_fbn, n, d_qsub, s);
+    ScanArgs fa;
+    fa.tmap = &tmap_f32;
+    fa.tmap_tile = &tmap_f32_176;
+    fa.tmap_112 = &tmap_f32_112;
+    fa.queries = d_qsub;
+    fa.nq = n;
+    fa.dq = static_cast<uint32_t>(ds);
+    fa.rows = rows;
+    fa.k = kcap;
+    fa.ws_keys = d_ws;
+    fa.status = d_status;
+    fa.live = d_fbn;
+    if ((e = launch_scan_fp32(fa, fb_plan, s)) != cudaSuccess) return cuda_error(e, "fallback scan launch");
+    MergeArgs fm;
+    fm.ws_keys = d_ws;
+    fm.nq = n;
+    fm.per_query = fb_per_query;
+    fm.k = kcap;
+    fm.out_stride = kcap;
+    fm.idx_out = d_fb_idx;
+    fm.sim_out = d_fb_sim;
+    fm.count_out = d_fb_cnt;
+    fm.live = d_fbn;
+    if ((st = merge_workspace(fb_per_query, n, kcap, fm, s))) return st;
+    if ((e = launch_merge_topk(fm, s)) != cudaSuccess) return cuda_error(e, "fallback merge launch");
+    launch_scatter_results(d_fb_idx, d_fb_sim, d_fb_cnt, d_fbq, d_fbn, n, kcap, o_idx, o_sim, o_cnt, s);
+    last_tc_n = n;
+    fbn_stream = s;
+    fbn_pending = true;
+    stats.kernel_launches += 8;
     stats.path = 6;
     stats.rerank_width = kp;
     stats.rows_scanned += rows * n;
     return NNDEX_OK;
 }
 
-int CudaIndex::finish_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
-                           cudaStream_t s) {
-    int st;
-    if ((st = grow_host(h_cert, cap_hcert, n, "pinned buffer"))) return st;
-    cudaMemcpyAsync(h_cert, d_cert, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    h_flags[1] = 0;
-    cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    const cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cuda_error(e, "search");
-    if ((st = check_device_words())) return st;
-    last_tc_n = n;
-    std::vector<uint32_t> failed;
-    for (uint32_t i = 0; i < n; ++i)
-        if (!h_cert[i]) failed.push_back(i);
-    stats.certified = failed.empty() ? 1u : 0u;
-    stats.fp32_fallback_queries = static_cast<uint32_t>(failed.size());
-    if (failed.empty()) return NNDEX_OK;
-    return rerun_exact_fp32(failed, kcap, o_idx, o_sim, o_cnt, s);
+// The device-side fallback's count into the statistics (waits for its stream once).
+int CudaIndex::fetch_fallback_stats() {
+    if (!fbn_pending) return NNDEX_OK;
+    cudaMemcpyAsync(h_fbn, d_fbn, sizeof(uint32_t), cudaMemcpyDeviceToHost, fbn_stream);
+    const cudaError_t e = cudaStreamSynchronize(fbn_stream);
+    if (e != cudaSuccess) return cuda_error(e, "fallback count");
+    fbn_pending = false;
+    stats.fp32_fallback_queries = h_fbn[0];
+    stats.certified = h_fbn[0] == 0 ? 1u : 0u;
+    return NNDEX_OK;
 }
+
 
 int CudaIndex::tune_host(uint64_t n, uint64_t kcap, int mode, TunePlan* plan) {
     std::vector<TunePlan> cands = tune_candidates(n, kcap);
@@ -908,6 +959,8 @@ int CudaIndex::tune_host(uint64_t n, uint64_t kcap, int mode, TunePlan* plan) {
             const cudaError_t e = cudaStreamSynchronize(stream);
             if (cst == NNDEX_OK && e != cudaSuccess) cst = cuda_error(e, "search");
             if (cst == NNDEX_OK) cst = check_device_words();
+            if (cst == NNDEX_OK && (cands[c].path == 2 || cands[c].path == 3))
+                cst = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream);
             ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         }
         forced_stride = 0;
@@ -958,14 +1011,15 @@ int CudaIndex::enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path)
     } else if (path == 6) {
         if ((st = enqueue_tf32(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
             return st;
-        if ((st = finish_tf32(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
-            return st;
     } else {
         if ((st = enqueue_tc(path == 3, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
                              stream)))
             return st;
-        if ((st = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
+        if ((st = enqueue_tc_pass2(path == 3, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim,
+                                   d_cnt, stream)))
             return st;
+        // pass 2's counts come back with the results (finish_tc reads them once the batch is done)
+        cudaMemcpyAsync(h_fbn, d_fbn, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
     }
     if (error_report)
         serr_record(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream);
@@ -976,11 +1030,14 @@ int CudaIndex::enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path)
 
 // The batch through a CUDA graph when one is cached for this shape, capturing it when the same
 // shape came in the previous call (its buffers are then allocated, so nothing allocates during
-// the capture); otherwise directly. Paths 1 (FP32 scan) and 4 (IVF list scan) only: the others
-// read device results on the host in the middle of the batch.
+// the capture); otherwise directly. Every path whose batch needs no host decision in its middle:
+// the FP32 scan (1), the tensor-core scans (2, 3: pass 2 and its compaction run on the device; the
+// rare FP32 re-run of an overflowed collection follows the batch), the IVF list scan (4) and the
+// TF32 candidate scan (6, its certificate's fallback on the device). The tensor-core IVF list scan
+// (5) plans its pass 2 on the host.
 int CudaIndex::run_host_batch(uint64_t n, uint64_t kcap, int mode, int path) {
     const bool graphable = use_graphs && !scan_timing && !error_report && !sync_check_enabled() &&
-                           (path == 1 || path == 4) &&
+                           (path == 1 || path == 2 || path == 3 || path == 4 || path == 6) &&
                            !(graph_failed_paths & (1u << path));
     if (!graphable) return enqueue_host_batch(n, kcap, mode, path);
     const uint64_t epoch = alloc_epoch();
@@ -1008,6 +1065,10 @@ int CudaIndex::run_host_batch(uint64_t n, uint64_t kcap, int mode, int path) {
         stats.ivf_rows_union = acc.ivf_rows_union;
         count_launch(static_cast<uint32_t>(graphs[i].launches));
         stats.graph = 2;
+        if (path == 6) {  // the replayed fallback's count is read back with the statistics
+            fbn_stream = stream;
+            fbn_pending = true;
+        }
         return NNDEX_OK;
     }
     if (!(same(graph_seen) && graph_seen.epoch == epoch)) {
@@ -1095,6 +1156,15 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_error(e, "search");
         if ((st = check_device_words())) return st;
+        if (path == 2 || path == 3) {
+            // pass 2 ran on the device; a query whose collection overflowed is re-run now
+            if ((st = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
+                return st;
+            if (stats.fp32_fallback_queries) {
+                cudaMemcpyAsync(h_res, d_res, res_bytes, cudaMemcpyDeviceToHost, stream);
+                if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_error(e, "search");
+            }
+        }
         if (path == 4) {
             stats.rows_scanned += ivf_scratch.h_probed[0];
             stats.ivf_rows_streamed += ivf_scratch.h_probed[1];
@@ -1128,10 +1198,18 @@ int CudaIndex::run_device_chunk(const float* dq, uint64_t n, uint64_t kcap, int 
     // the certificates' fallbacks need the host: these paths synchronise
     *synced = true;
     if (path == 6) {
-        if ((st = enqueue_tf32(n32, k32, oi, os, oc, s))) return st;
-        return finish_tf32(n32, k32, oi, os, oc, s);
+        *synced = false;  // the certificate's fallback runs on the device
+        return enqueue_tf32(n32, k32, oi, os, oc, s);
     }
     if ((st = enqueue_tc(path == 3, n32, k32, oi, os, oc, s))) return st;
+    if ((st = enqueue_tc_pass2(path == 3, n32, k32, oi, os, oc, s))) return st;
+    cudaMemcpyAsync(h_fbn, d_fbn, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    h_flags[1] = 0;
+    cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_error(e, "search");
+    if ((st = check_device_words())) return st;
     return finish_tc(n32, k32, oi, os, oc, s);
 }
 
@@ -1787,13 +1865,13 @@ int nndex_cuda_last_candidates(nndex_cuda_index* index, uint64_t query_rows, uin
     const uint64_t n = query_rows * kp;
     if (n > capacity || n > ix->cap_cand_idx)
         return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: candidate buffer too small");
-    cudaError_t e = cudaStreamSynchronize(ix->stream);
+    cudaError_t e = cudaDeviceSynchronize();  // the search may have run on any stream
     if (e == cudaSuccess && idx_out) e = cudaMemcpy(idx_out, ix->d_cand_idx, n * sizeof(uint64_t), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && approx_out) e = cudaMemcpy(approx_out, ix->d_cand_sim, n * sizeof(float), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && certified_out) {
         if (query_rows > ix->last_tc_n)
             return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: more rows than the last batch");
-        std::memcpy(certified_out, ix->h_cert, query_rows * sizeof(uint32_t));
+        e = cudaMemcpy(certified_out, ix->d_cert, query_rows * sizeof(uint32_t), cudaMemcpyDeviceToHost);
     }
     if (e != cudaSuccess) return cuda_error(e, "candidates");
     return NNDEX_OK;
@@ -1810,9 +1888,10 @@ int nndex_cuda_last_search_stats(const nndex_cuda_index* index, nndex_cuda_searc
     if (!index || !out) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null argument");
     CudaIndex* ix = index->impl;
     std::lock_guard<std::mutex> lock(ix->mu);
-    if (ix->serr_pending) {
+    if (ix->serr_pending || ix->fbn_pending) {
         cudaSetDevice(ix->device);
-        const int st = ix->serr_fetch_stats();
+        int st = ix->serr_fetch_stats();
+        if (!st) st = ix->fetch_fallback_stats();
         if (st) return st;
     }
     *out = ix->stats;

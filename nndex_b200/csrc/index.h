@@ -205,6 +205,19 @@ struct CudaIndex {
                      cudaStream_t s);
     int serr_fetch_stats();
 
+    // Counters a device-side certificate fallback leaves on the device ({queries re-run on the FP32
+    // scan, spare}), read back with the statistics.
+    uint32_t* d_fbq = nullptr;  // the re-run queries' indices
+    size_t cap_fbq = 0;
+    uint32_t* d_fbn = nullptr;  // {TF32 re-runs, TC pass-2 queries, TC pass-2 overflows, spare}
+    uint32_t* h_fbn = nullptr;  // pinned copy
+    uint32_t* d_tcfail = nullptr;  // TC pass 2: positions (in d_ids) of the queries whose collection overflowed
+    size_t cap_tcfail = 0;
+    int ensure_fbn();
+    cudaStream_t fbn_stream = nullptr;
+    bool fbn_pending = false;
+    int fetch_fallback_stats();
+
     // scan-kernel timing (roofline reports)
     bool scan_timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> scan_events;
@@ -273,13 +286,16 @@ struct CudaIndex {
     int enqueue_prep_queries(const float* d_raw, uint64_t n, int mode, int path, cudaStream_t s);
     int enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
                    cudaStream_t s);
-    // After a tensor-core batch has completed: re-run the queries whose certificate failed on the
-    // FP32 path (device outputs are patched in place). Synchronises the stream.
+    // Pass 2 of a tensor-core batch on the device, after enqueue_tc: the uncertified queries are
+    // compacted and gathered, their rows collected against T and reranked, and the queries whose
+    // collection overflowed compacted for the host (d_fbn[1..2], d_tcfail). No host round trip.
+    int enqueue_tc_pass2(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                         cudaStream_t s);
+    // Once the stream has completed a tensor-core batch (h_fbn read back with it): statistics, the
+    // pass-1 stride rule, and the FP32 re-run of any query whose collection overflowed (device
+    // outputs patched in place; synchronises the stream again only then).
     int finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
     int enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
-    // After a TF32 candidate batch: the queries whose certificate failed run on the FP32 scan.
-    // Synchronises the stream.
-    int finish_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s);
     // The FP32 scan for the listed queries (rows of d_qn), written into their output slots.
     int rerun_exact_fp32(const std::vector<uint32_t>& qs, uint32_t kcap, uint64_t* o_idx, float* o_sim,
                          uint32_t* o_cnt, cudaStream_t s);

@@ -67,6 +67,7 @@ struct ScanArgs {
     const uint32_t* row_map = nullptr;  // optional: stored position → original row index
     uint64_t* ws_keys = nullptr;        // nq × ctas_per_group × k
     uint32_t* status = nullptr;
+    const uint32_t* live = nullptr;     // optional: a device count; 0 makes the whole launch return
 };
 
 // Picks queries-per-CTA, grid and candidate capacity for (nq, dq, k) within the shared-memory
@@ -87,6 +88,7 @@ struct MergeArgs {
     // part_keys holds nq × parts × k keys, part_done nq counters that start (and end) at zero.
     uint64_t* part_keys = nullptr;
     uint32_t* part_done = nullptr;
+    const uint32_t* live = nullptr;     // optional: a device count; queries at or past it are skipped
 };
 uint32_t merge_parts(uint64_t per_query, uint32_t k);
 cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream);
@@ -123,6 +125,11 @@ struct TcParams {
     const uint32_t* row_map = nullptr;        // reordered row → original row
     uint32_t it_nlist = 0;
     uint32_t it_chunk_rows = 0;
+    // Pass 2 with a device-side query count (no host round trip after pass 1): live_q[0] queries of
+    // the gathered block are live; the 1-D grid's CTA b takes work item b of (query block, row
+    // range), the ranges derived from the count as the host derives them (tc_ranges with sm_count).
+    const uint32_t* live_q = nullptr;
+    uint32_t sm_count = 0;
 };
 struct TcArgs {
     const CUtensorMap* tmap_q = nullptr;  // quantised queries [nq_alloc × K], box {128 B, 128 rows}
@@ -132,6 +139,7 @@ struct TcArgs {
     uint32_t stages = 4;                  // base ring depth (2..4)
     bool stream_a = false;                // pass 1: query slabs staged per ring stage, not resident
     uint32_t items = 0;                   // IVF item mode: number of work items (grid), 0 = off
+    uint32_t live_items = 0;              // pass 2 with p.live_q: CTAs launched (an upper bound)
 };
 size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8, bool stream_a);
 // Deepest base ring (4, 3 or 2 stages) that fits k′ heaps in `smem_limit`; 0 if none fits.
@@ -164,6 +172,16 @@ cudaError_t launch_scan_tf32(const CUtensorMap& tmap_x, const CUtensorMap& tmap_
 cudaError_t launch_tf32_row_norms(const float* base, uint64_t rows, uint32_t ds, float2* out, uint32_t sm_count,
                                   cudaStream_t stream);
 
+// Device-side certificate fallback: compaction of the zero flags (one block), a gather of their rows
+// (zeros past the count), and a scatter of re-run results back to their queries' slots.
+void launch_compact_zero_flags(const uint32_t* flags, uint32_t n, uint32_t* ids, uint32_t* count, cudaStream_t s,
+                               const uint32_t* live = nullptr);
+void launch_gather_rows(const float* src, uint32_t ds, const uint32_t* ids, const uint32_t* count, uint32_t n,
+                        float* dst, cudaStream_t s);
+void launch_scatter_results(const uint64_t* fb_idx, const float* fb_sim, const uint32_t* fb_cnt, const uint32_t* ids,
+                            const uint32_t* count, uint32_t n, uint32_t k, uint64_t* idx, float* sim, uint32_t* cnt,
+                            cudaStream_t s);
+
 struct RerankArgs {
     const float* base = nullptr;  // FP32 base, stride ds
     uint32_t ds = 0;
@@ -183,11 +201,11 @@ cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream);
 // q2_lp holds m rounded up to 128 rows (whole query blocks); the rows past m are written as zeros.
 cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q_lp, uint32_t row_bytes, void* q2_lp,
                                   const float* resid, float* resid2, const float* scale, float* scale2,
-                                  const float* kth, float* thr2, cudaStream_t stream);
+                                  const float* kth, float* thr2, cudaStream_t stream, const uint32_t* live = nullptr);
 cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float* queries, const uint32_t* ids,
                                     uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
                                     uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
-                                    cudaStream_t stream, bool by_query = false);
+                                    cudaStream_t stream, bool by_query = false, const uint32_t* live = nullptr);
 cudaError_t launch_max_reduce(const float* v, uint64_t n, unsigned int* out, cudaStream_t stream);
 
 // Maximum k the fused scan kernels select in shared memory.

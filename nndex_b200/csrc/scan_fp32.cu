@@ -43,7 +43,8 @@ __global__ void __launch_bounds__(ScanShape<QB, NCW>::kThreads, 1)
     scan_fp32_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restrict__ queries, uint32_t nq,
                      uint32_t dq, uint64_t rows, uint32_t k, uint32_t cap,
                      const uint32_t* __restrict__ row_map, uint64_t* __restrict__ ws_keys,
-                     uint32_t* __restrict__ status) {
+                     uint32_t* __restrict__ status, const uint32_t* __restrict__ live) {
+    if (live && *live == 0) return;  // a fallback launch with nothing to re-run
     using S = ScanShape<QB, NCW>;
     using Consumer = ScanConsumer<QB, NCW, ST>;
     constexpr int TR = S::kTileRows;
@@ -163,7 +164,8 @@ __global__ void __launch_bounds__((W + 1) * 32, 1)
     scan_fp32_wide_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restrict__ queries, uint32_t nq,
                           uint32_t dq, uint64_t rows, uint32_t k, uint32_t cap,
                           const uint32_t* __restrict__ row_map, uint64_t* __restrict__ ws_keys,
-                          uint32_t* __restrict__ status) {
+                          uint32_t* __restrict__ status, const uint32_t* __restrict__ live) {
+    if (live && *live == 0) return;  // a fallback launch with nothing to re-run
     using Consumer = ScanConsumerWide<QB, W, ST>;
     constexpr int TR = Consumer::kTileRows;
     constexpr uint32_t kStageBytes = Consumer::kStageBytes;
@@ -351,7 +353,9 @@ __global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restr
                                                          float* __restrict__ sim_out,
                                                          uint32_t* __restrict__ count_out, uint32_t parts,
                                                          uint64_t* __restrict__ part_keys,
-                                                         uint32_t* __restrict__ part_done) {
+                                                         uint32_t* __restrict__ part_done,
+                                                         const uint32_t* __restrict__ live) {
+    if (live && blockIdx.y >= *live) return;  // a fallback merge: only the queries re-run
     __shared__ BlockSelectScratch s;
     __shared__ uint32_t last;
     extern __shared__ uint64_t smem_keys[];
@@ -477,7 +481,7 @@ cudaError_t launch_qb_st(const ScanArgs& a, const ScanPlan& p, cudaStream_t stre
     if (e != cudaSuccess) return e;
     dim3 grid(p.ctas_per_group, p.groups);
     kern<<<grid, ScanShape<QB, kNcw>::kThreads, p.smem_bytes, stream>>>(*a.tmap, a.queries, a.nq, a.dq, a.rows, a.k, p.cap,
-                                                              a.row_map, a.ws_keys, a.status);
+                                                              a.row_map, a.ws_keys, a.status, a.live);
     count_launch();
     return cudaGetLastError();
 }
@@ -509,7 +513,7 @@ cudaError_t launch_wide_st(const ScanArgs& a, const ScanPlan& p, cudaStream_t st
     if (!tm) return cudaErrorInvalidValue;
     dim3 grid(p.ctas_per_group, p.groups);
     kern<<<grid, (W + 1) * 32, p.smem_bytes, stream>>>(*tm, a.queries, a.nq, a.dq, a.rows, a.k, p.cap, a.row_map,
-                                                       a.ws_keys, a.status);
+                                                       a.ws_keys, a.status, a.live);
     count_launch();
     return cudaGetLastError();
 }
@@ -658,7 +662,7 @@ cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream) {
     }
     merge_topk_kernel<<<dim3(parts, a.nq), 512, smem, stream>>>(a.ws_keys, a.per_query, a.k, a.out_stride, a.idx_out,
                                                                 a.sim_out, a.count_out, parts, a.part_keys,
-                                                                a.part_done);
+                                                                a.part_done, a.live);
     count_launch();
     return cudaGetLastError();
 }

@@ -177,9 +177,28 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     uint32_t q0 = blockIdx.x * kM;
-    const uint32_t range = blockIdx.y, nranges = gridDim.y;
-    uint64_t row_begin = static_cast<uint64_t>(range) * p.range_rows;
-    uint64_t row_end = (row_begin + p.range_rows) < p.rows ? (row_begin + p.range_rows) : p.rows;
+    uint32_t range = blockIdx.y, nranges = gridDim.y;
+    uint64_t range_rows = p.range_rows;
+    uint32_t nq_live = p.nq;
+    if (!kItems && p.live_q) {
+        // The device count decides the grid's shape: the same ranges tc_ranges gives the host for
+        // this many query blocks; CTAs past the work items return before any set-up.
+        nq_live = *p.live_q;
+        const uint64_t nqb = (nq_live + kM - 1) / kM;
+        if (nqb == 0) return;
+        uint64_t nr = (4ull * p.sm_count + nqb - 1) / nqb;
+        const uint64_t nr_max = (p.rows + 2047) / 2048;
+        nr = nr < 1 ? 1 : (nr > nr_max ? nr_max : nr);
+        range_rows = (p.rows + nr - 1) / nr;
+        range_rows = (range_rows + 255) / 256 * 256;
+        nr = (p.rows + range_rows - 1) / range_rows;
+        if (blockIdx.x >= nqb * nr) return;
+        q0 = static_cast<uint32_t>(blockIdx.x / nr) * kM;
+        range = static_cast<uint32_t>(blockIdx.x % nr);
+        nranges = static_cast<uint32_t>(nr);
+    }
+    uint64_t row_begin = static_cast<uint64_t>(range) * range_rows;
+    uint64_t row_end = (row_begin + range_rows) < p.rows ? (row_begin + range_rows) : p.rows;
     uint32_t chunk = 0;  // item mode: the chunk of the list (its output slot offset)
     if (kItems) {
         const uint32_t wi = blockIdx.x;
@@ -314,7 +333,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t quarter = warp & 3u;
         const uint32_t lrow = quarter * 32 + lane;
         const uint32_t q = kItems ? p.it_lane_qid[q0 + lrow] : q0 + lrow;
-        const bool valid_q = kItems ? q != 0xFFFFFFFFu : q < p.nq;
+        const bool valid_q = kItems ? q != 0xFFFFFFFFu : q < nq_live;
         const uint32_t et = threadIdx.x - 64;  // 0..127
         const float qs = (kFp8 && valid_q) ? p.q_scale[q] : 1.0f;
         const float rq = valid_q ? p.q_resid[q] : 0.0f;
@@ -545,8 +564,12 @@ __global__ void gather_queries_kernel(const uint32_t* __restrict__ ids, uint32_t
                                       uint32_t row_bytes, uint8_t* __restrict__ q2_lp, const float* __restrict__ resid,
                                       float* __restrict__ resid2, const float* __restrict__ scale,
                                       float* __restrict__ scale2, const float* __restrict__ kth,
-                                      float* __restrict__ thr2) {
+                                      float* __restrict__ thr2, const uint32_t* __restrict__ live) {
     const uint32_t i = blockIdx.x;
+    if (live) {  // the count is on the device: rows past its 128-query block are not used
+        m = *live;
+        if (i >= (m + 127) / 128 * 128) return;
+    }
     uint4* b = reinterpret_cast<uint4*>(q2_lp + static_cast<size_t>(i) * row_bytes);
     if (i >= m) {  // padding rows of the last 128-query block: zeros, not stale memory
         for (uint32_t t = threadIdx.x; t < row_bytes / 16; t += blockDim.x) b[t] = make_uint4(0, 0, 0, 0);
@@ -567,10 +590,11 @@ __global__ void __launch_bounds__(256)
                             const uint32_t* __restrict__ ids, const uint32_t* __restrict__ rows2,
                             const uint32_t* __restrict__ cnt2, uint32_t cap2, uint32_t k, uint64_t* __restrict__ idx_out,
                             float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out,
-                            uint32_t* __restrict__ ok_out, int by_query) {
+                            uint32_t* __restrict__ ok_out, int by_query, const uint32_t* __restrict__ live) {
     extern __shared__ uint64_t keys[];
     __shared__ BlockSelectScratch sel;
     const uint32_t i = blockIdx.x;
+    if (live && i >= *live) return;
     const uint32_t q = ids[i];
     const uint32_t qrow = by_query ? q : i;  // collected rows indexed by query, or by position in ids
     const uint32_t total = cnt2[qrow];
@@ -630,7 +654,8 @@ static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
     const size_t smem = tc_smem_bytes(a.p.nchunks, kp, kST, kFp8, kStreamA);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    dim3 grid = kItems ? dim3(a.items, 1) : dim3((a.p.nq + kM - 1) / kM, a.nranges);
+    dim3 grid = kItems ? dim3(a.items, 1)
+                       : (a.p.live_q ? dim3(a.live_items, 1) : dim3((a.p.nq + kM - 1) / kM, a.nranges));
     TcParams p = a.p;
     p.kprime = kp;
     if (sync_check_enabled())
@@ -690,12 +715,14 @@ cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream) {
 
 cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q_lp, uint32_t row_bytes, void* q2_lp,
                                   const float* resid, float* resid2, const float* scale, float* scale2,
-                                  const float* kth, float* thr2, cudaStream_t stream) {
+                                  const float* kth, float* thr2, cudaStream_t stream, const uint32_t* live) {
     if (m == 0) return cudaSuccess;
-    // One block per row of the padded query buffer (m rounded up to the 128-query block).
+    // One block per row of the padded query buffer (m rounded up to the 128-query block; with a
+    // device count `live`, m is its bound).
     const uint32_t m_alloc = (m + 127) / 128 * 128;
     gather_queries_kernel<<<m_alloc, 128, 0, stream>>>(ids, m, static_cast<const uint8_t*>(q_lp), row_bytes,
-                                                 static_cast<uint8_t*>(q2_lp), resid, resid2, scale, scale2, kth, thr2);
+                                                 static_cast<uint8_t*>(q2_lp), resid, resid2, scale, scale2, kth, thr2,
+                                                 live);
     count_launch();
     return cudaGetLastError();
 }
@@ -703,7 +730,7 @@ cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q
 cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float* queries, const uint32_t* ids,
                                     uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
                                     uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
-                                    cudaStream_t stream, bool by_query) {
+                                    cudaStream_t stream, bool by_query, const uint32_t* live) {
     if (m == 0) return cudaSuccess;
     uint32_t p2 = 1;
     while (p2 < cap2) p2 <<= 1;
@@ -712,9 +739,96 @@ cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float*
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     kern<<<m, 256, smem, stream>>>(base, ds, queries, ids, rows2, cnt2, cap2, k, idx_out, sim_out, cnt_out, ok_out,
-                                   by_query ? 1 : 0);
+                                   by_query ? 1 : 0, live);
     count_launch();
     return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// Device-side fallback of a certificate: the queries whose certificate failed are compacted,
+// gathered, re-run on the FP32 scan (whose launch returns at once when there are none) and their
+// results scattered back, all on the stream, with no host round trip.
+// ------------------------------------------------------------------------------------------
+
+// One block of 1024 threads: ids[0..m) = the indices i < n with flags[i] == 0, in order; count[0] = m.
+// With `live`, only the first live[0] flags count.
+__global__ void __launch_bounds__(1024) compact_zero_flags_kernel(const uint32_t* __restrict__ flags, uint32_t n,
+                                                                  uint32_t* __restrict__ ids,
+                                                                  uint32_t* __restrict__ count,
+                                                                  const uint32_t* __restrict__ live) {
+    __shared__ uint32_t warp_sum[32];
+    __shared__ uint32_t base;
+    if (live && *live < n) n = *live;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (uint32_t i0 = 0; i0 < n; i0 += 1024) {
+        const uint32_t i = i0 + threadIdx.x;
+        const bool take = i < n && flags[i] == 0;
+        const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, take);
+        if (lane == 0) warp_sum[warp] = __popc(ballot);
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+        for (uint32_t w = 0; w < 32; ++w) {
+            const uint32_t v = warp_sum[w];
+            before += w < warp ? v : 0u;
+            total += v;
+        }
+        if (take) ids[base + before + __popc(ballot & ((1u << lane) - 1u))] = i;
+        __syncthreads();
+        if (threadIdx.x == 0) base += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) count[0] = base;
+}
+
+// Row i of dst (stride ds floats) = row ids[i] of src for i < count[0], zeros for the rest of n.
+__global__ void gather_rows_kernel(const float* __restrict__ src, uint32_t ds, const uint32_t* __restrict__ ids,
+                                   const uint32_t* __restrict__ count, float* __restrict__ dst) {
+    const uint32_t i = blockIdx.x;
+    float4* d = reinterpret_cast<float4*>(dst + static_cast<size_t>(i) * ds);
+    if (i >= count[0]) {
+        for (uint32_t t = threadIdx.x; t < ds / 4; t += blockDim.x) d[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const float4* a = reinterpret_cast<const float4*>(src + static_cast<size_t>(ids[i]) * ds);
+    for (uint32_t t = threadIdx.x; t < ds / 4; t += blockDim.x) d[t] = a[t];
+}
+
+// The results of re-run query i (< count[0]) into the slots of query ids[i].
+__global__ void scatter_results_kernel(const uint64_t* __restrict__ fb_idx, const float* __restrict__ fb_sim,
+                                       const uint32_t* __restrict__ fb_cnt, const uint32_t* __restrict__ ids,
+                                       const uint32_t* __restrict__ count, uint32_t k, uint64_t* __restrict__ idx,
+                                       float* __restrict__ sim, uint32_t* __restrict__ cnt) {
+    const uint32_t i = blockIdx.x;
+    if (i >= count[0]) return;
+    const uint32_t q = ids[i];
+    for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
+        idx[static_cast<size_t>(q) * k + j] = fb_idx[static_cast<size_t>(i) * k + j];
+        sim[static_cast<size_t>(q) * k + j] = fb_sim[static_cast<size_t>(i) * k + j];
+    }
+    if (threadIdx.x == 0 && cnt) cnt[q] = fb_cnt[i];
+}
+
+void launch_compact_zero_flags(const uint32_t* flags, uint32_t n, uint32_t* ids, uint32_t* count, cudaStream_t s,
+                               const uint32_t* live) {
+    compact_zero_flags_kernel<<<1, 1024, 0, s>>>(flags, n, ids, count, live);
+    count_launch();
+}
+
+void launch_gather_rows(const float* src, uint32_t ds, const uint32_t* ids, const uint32_t* count, uint32_t n,
+                        float* dst, cudaStream_t s) {
+    if (n == 0) return;
+    gather_rows_kernel<<<n, 128, 0, s>>>(src, ds, ids, count, dst);
+    count_launch();
+}
+
+void launch_scatter_results(const uint64_t* fb_idx, const float* fb_sim, const uint32_t* fb_cnt, const uint32_t* ids,
+                            const uint32_t* count, uint32_t n, uint32_t k, uint64_t* idx, float* sim, uint32_t* cnt,
+                            cudaStream_t s) {
+    if (n == 0) return;
+    scatter_results_kernel<<<n, 128, 0, s>>>(fb_idx, fb_sim, fb_cnt, ids, count, k, idx, sim, cnt);
+    count_launch();
 }
 
 // Largest row residual norm (the ε of the certificate), by a grid-stride max.
