@@ -82,3 +82,22 @@ def test_graphs_off_and_on_again():
     for _ in range(3):
         _bits(a.search(q, k=3), ref)
     assert a.last_search_stats()["graph"] == 2
+
+
+@pytest.mark.parametrize("precision,batch,path", [("fp32", 16, 6), ("bf16", 200, 2), ("fp8", 200, 3)])
+def test_certified_paths_are_captured_and_replayed(precision, batch, path):
+    # the TF32 candidate scan and the tensor-core scans decide their fallbacks on the device, so
+    # their host-buffer batches are captured too; replays equal direct launches bit for bit
+    base, rng = _mixture(60_000, 128, 5)
+    a = NNdex(base, precision=precision, autotune=False)
+    b = NNdex(base, precision=precision, autotune=False)
+    _lib.lib().nndex_cuda_set_graphs(b.handle, 0)
+    centres, _ = _mixture(200, 128, 5)  # points near the base's clusters
+    kinds = []
+    for step in range(6):
+        q = (centres[rng.integers(0, 200, batch)] + 0.3 * rng.normal(size=(batch, 128))).astype(np.float32)
+        _bits(a.search(q, k=10), b.search(q, k=10))
+        st = a.last_search_stats()
+        assert st["path"] == path, st
+        kinds.append(st["graph"])
+    assert 2 in kinds, kinds

@@ -144,3 +144,22 @@ def test_pass2_padding_lanes_ignore_stale_memory():
     assert st["path"] == 2 and st["second_pass_queries"] > 0, st
     assert np.array_equal(ti, fi)
     assert np.max(np.abs(ts - fs)) <= 1e-5
+
+
+def test_overflowing_collection_reruns_on_the_fp32_scan():
+    # 10,000 copies of one row: pass 1 cannot certify (the k-th and k'-th scores tie), pass 2
+    # collects every copy — more than its 8,192-row buffer — so the device marks each query for the
+    # FP32 scan, which returns the lowest rows among the ties
+    rng = np.random.default_rng(31)
+    m = rng.normal(size=(30_000, 64)).astype(np.float32)
+    m[10_000:20_000] = m[10_000]
+    q = (np.repeat(m[10_000:10_001], 130, axis=0) + np.float32(1e-3) * rng.normal(size=(130, 64))).astype(np.float32)
+    index = NNdex(m, precision="bf16", autotune=False)
+    ti, ts = index.search(q, k=10)
+    st = index.last_search_stats()
+    assert st["path"] == 2 and st["second_pass_queries"] == 130 and st["fp32_fallback_queries"] == 130, st
+    assert ti[0].tolist() == list(range(10_000, 10_010))
+    index.set_precision("fp32")
+    fi, fs = index.search(q, k=10)
+    np.testing.assert_array_equal(ti, fi)
+    np.testing.assert_array_equal(ts.view(np.uint32), fs.view(np.uint32))
