@@ -68,6 +68,8 @@ def parse_args(argv=None):
     p.add_argument("--mixed-k", type=int, default=10)
     p.add_argument("--mixed-steps", type=int, default=5)
     p.add_argument("--mixed-oracle-queries", type=int, default=512)
+    p.add_argument("--mixed-stride", type=int, default=0,
+                   help="fix the tensor-core scans' pass-1 tile stride (installed as the tuner's plan); 0 = tuned")
     p.add_argument("--ivf", choices=["on", "off", "only"], default="on",
                    help="also measure the IVF workload (GPU k-means build + probe + ragged list scan)")
     p.add_argument("--ivf-rows", type=int, default=2_000_000)
@@ -93,8 +95,8 @@ def parse_args(argv=None):
     p.add_argument("--serve-seconds", type=float, default=2.0)
     p.add_argument("--serve-slots", type=int, default=3)
     p.add_argument("--serve-nprobe", type=int, default=32)
-    p.add_argument("--serve-latency-ms", type=int, default=150,
-                   help="server latency budget: requests whose queue would take longer to drain are refused")
+    p.add_argument("--serve-latency-ms", type=int, default=100,
+                   help="server latency budget: requests are refused while the oldest queued one has waited longer")
     return p.parse_args(argv)
 
 
@@ -241,9 +243,10 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(rows, dims, batch, k):
+def profiled_traffic(rows, dims, batch, k, kernel=""):
     """DRAM bytes per scan launch from the committed ncu summary (profiles/scan_fp32_traffic.txt),
-    scaled to this workload by the rows streamed."""
+    scaled to this workload by the rows streamed; the line must be for the same kernel family."""
+    family = kernel.split("<")[0].split(" ")[0]
     path = os.path.join(ROOT, "profiles", "scan_fp32_traffic.txt")
     try:
         lines = open(path).read().splitlines()
@@ -253,8 +256,8 @@ def profiled_traffic(rows, dims, batch, k):
         f = line.split()
         if not f or f[0].startswith("#") or len(f) < 6:
             continue
-        r, d, b, kk, _kernel, dram = f[:6]
-        if int(d) == dims and int(b) == batch and int(kk) == k:
+        r, d, b, kk, kern, dram = f[:6]
+        if int(d) == dims and int(b) == batch and int(kk) == k and kern.split("<")[0] == family:
             return int(dram) * rows / int(r)
     return None
 
@@ -435,7 +438,7 @@ def run_ours(args):
     bytes_per_launch = args.rows * args.dims * 4 + args.batch * args.dims * 4 + args.batch * k * 12
     achieved = bytes_per_launch / (head["scan_ms"] / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profiled_traffic(args.rows, args.dims, args.batch, k)
+    traffic = profiled_traffic(args.rows, args.dims, args.batch, k, head["kernel"])
     line = {
         "metric": METRIC,
         "value": head["queries_per_s"],
@@ -642,6 +645,18 @@ def run_mixed(args, dev, L, world):
     os_ = torch.empty((nq, k), dtype=torch.float32, device=dev)
     stats = _lib.SearchStats()
     out = {}
+    if args.mixed_stride:
+        # the tuner's cache with the given stride for both tensor-core precisions at this shape
+        n = C.c_uint64(0)
+        L.nndex_cuda_autotune_export(h, None, 0, C.byref(n))
+        buf = C.create_string_buffer(n.value)
+        L.nndex_cuda_autotune_export(h, buf, n.value, C.byref(n))
+        nqb, kb = 1 << (nq - 1).bit_length(), 1 << (k - 1).bit_length()
+        text = buf.value.decode() + "".join(
+            f"shape ivf=0 nq={nqb} k={kb} precision={p} nprobe=0 plan path={p} stride={args.mixed_stride} ms=0\n"
+            for p in (2, 3))
+        if L.nndex_cuda_autotune_import(h, text.encode()) != 0:
+            raise RuntimeError(_lib.last_error())
     sample = min(args.mixed_oracle_queries, nq)
     ref_i, ref_s = fp64_topk(base, q[:sample], k)
     for name, prec in (("fp32", NNDEX_PRECISION_FP32), ("bf16", NNDEX_PRECISION_BF16), ("fp8", NNDEX_PRECISION_FP8)):

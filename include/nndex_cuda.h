@@ -357,7 +357,9 @@ NNDEX_API int nndex_cuda_set_graphs(nndex_cuda_index* index, int enable);
  * results (the FP32 scan or the TF32 candidate scan for small batches; BF16 or FP8 tensor-core
  * scans with pass-1 tile strides 1, 8 and 32 for large ones; the FP32 or the tensor-core IVF list
  * scan), times each, and keeps the fastest for later batches of that shape. mode 0: the fixed
- * rules. Results are identical under every plan; only speed differs.
+ * rules. mode 2: the cached plans, and the rules for shapes not in the cache (no batch pays for
+ * measurements; the serving loop's slots run so, with the cache the index had when the server
+ * started). Results are identical under every plan; only speed differs.
  */
 NNDEX_API int nndex_cuda_set_autotune(nndex_cuda_index* index, int mode);
 /*
@@ -398,9 +400,9 @@ typedef struct nndex_cuda_server_opts {
     uint32_t max_batch_queries;  /* queries per batch, 0 = 4096                                 */
     uint64_t queue_capacity;     /* queries waiting, 0 = 1 << 20                                */
     uint64_t slot_bytes;         /* device memory per slot, 0 = free HBM × 0.5 / slots          */
-    uint32_t latency_budget_ms;  /* refuse a request when the queue ahead of it would take longer
-                                    than this to drain (estimated from the batches served so far),
-                                    0 = no latency bound                                         */
+    uint32_t latency_budget_ms;  /* refuse a request while the oldest queued request has waited
+                                    longer than this (the queue is backed up), 0 = no latency
+                                    bound                                                        */
     uint32_t reserved[7];
 } nndex_cuda_server_opts;
 typedef struct nndex_cuda_request_info {
@@ -417,7 +419,8 @@ typedef struct nndex_cuda_server_stats {
     uint32_t slots, max_batch_queries;
     uint64_t slot_bytes;
     uint64_t refused_latency;      /* of `refused`: refused by the latency budget               */
-    double us_per_query;           /* the drain-time estimate's cost of a query in one slot     */
+    double us_per_query;           /* moving average of a slot's wall time per query (batches'
+                                      launch to results), for reports                           */
 } nndex_cuda_server_stats;
 
 NNDEX_API int nndex_cuda_server_start(nndex_cuda_index* index, const nndex_cuda_server_opts* opts,

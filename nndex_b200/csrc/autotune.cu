@@ -201,7 +201,7 @@ CudaIndex::TunePlan CudaIndex::plan_for(uint64_t nq, uint64_t kcap, bool* measur
     if (autotune) {
         auto it = tune_cache.find(tune_key(nq, kcap));
         if (it != tune_cache.end()) return it->second.plan;
-        if (tune_candidates(nq, kcap).size() > 1) *measure = true;
+        if (autotune == 1 && tune_candidates(nq, kcap).size() > 1) *measure = true;
     }
     return rule_plan(nq, kcap);
 }
@@ -215,7 +215,7 @@ extern "C" {
 int nndex_cuda_set_autotune(nndex_cuda_index* index, int mode) {
     clear_error();
     if (!index) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: null index");
-    if (mode < 0 || mode > 1) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: autotune mode %d", mode);
+    if (mode < 0 || mode > 2) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: autotune mode %d", mode);
     CudaIndex* ix = index->impl;
     std::lock_guard<std::mutex> lock(ix->mu);
     ix->autotune = mode;

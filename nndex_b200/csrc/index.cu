@@ -1643,6 +1643,10 @@ int make_view(const CudaIndex& src, CudaIndex** out) {
     v->tmap_fp8 = src.tmap_fp8;
     v->rerank_width = src.rerank_width;
     v->tc_sample_stride = src.tc_sample_stride;
+    // a view (a serving slot) never stops a batch to time plans: the source's measured plans, else
+    // the rules
+    v->tune_cache = src.tune_cache;
+    v->autotune = src.autotune ? 2 : 0;
     v->ivf = src.ivf;
     v->ivf_scratch.nprobe = src.ivf_scratch.nprobe;
     cudaError_t e;

@@ -263,7 +263,7 @@ struct CudaIndex {
         double ms = 0.0;      // its wall time per batch when measured
         uint32_t candidates = 0;
     };
-    int autotune = 1;  // 0 = rules only, 1 = measure once per shape
+    int autotune = 1;  // 0 = rules only, 1 = measure once per shape, 2 = cached plans, else rules
     std::map<uint64_t, TuneEntry> tune_cache;
     uint64_t tune_key(uint64_t nq, uint64_t kcap) const;
     std::vector<TunePlan> tune_candidates(uint64_t nq, uint64_t kcap) const;

@@ -113,32 +113,29 @@ def test_poll_without_waiting_and_unknown_ticket(index):
             s.poll(t)
 
 
-def test_latency_budget_refuses_when_the_queue_would_drain_too_slowly(index):
-    # the per-query cost from a first server sets a budget that one request meets with room to
-    # spare; a burst queued at once then overflows it and part of it is refused, while the
-    # admitted requests still get the index's own answers
-    reqs = requests(60, index.dims, seed=11)
-    with Server(index, slots=1) as s:
-        for q, k, approx in reqs[:4]:
-            s.result(s.submit(q, k=k, approx=approx))
-        us = s.stats()["us_per_query"]
-    assert us > 0
-    budget = max(1, int(np.ceil(3 * 256 * us / 1000)))
-    with Server(index, slots=1, latency_budget_ms=budget) as s:
-        q0, k0, a0 = reqs[0]
-        s.result(s.submit(q0, k=k0, approx=a0))
-        admitted, refused = [], 0
-        for q, k, approx in reqs[1:]:
-            try:
-                admitted.append((s.submit(q, k=k, approx=approx), q, k, approx))
-            except NNdexError as e:
-                assert e.code == NNDEX_ERR_ADMISSION and "latency budget" in str(e)
-                refused += 1
-        results = [(s.result(t), q, k, approx) for t, q, k, approx in admitted]
+def test_latency_budget_refuses_while_the_queue_is_backed_up(index):
+    # one slot taking 64 queries per batch and 400 queued requests of 64: the queue takes many
+    # batches to drain, so after a few milliseconds its oldest request has waited longer than a
+    # 2 ms budget and a new request is refused; the admitted ones still get the index's answers
+    import time
+    rng = np.random.default_rng(11)
+    qs = [mixture(rng, 64, index.dims) for _ in range(400)]
+    with Server(index, slots=1, max_batch_queries=64, latency_budget_ms=2) as s:
+        tickets = [s.submit(q, k=10) for q in qs[:1]]
+        time.sleep(0.2)  # the first batch runs alone (any one-off set-up), the queue is empty again
+        s.result(tickets[0])
+        tickets = [s.submit(q, k=10) for q in qs]  # the burst arrives faster than the budget
+        time.sleep(0.008)
+        with pytest.raises(NNdexError) as err:
+            s.submit(qs[0], k=10)
+        assert err.value.code == NNDEX_ERR_ADMISSION and "latency budget" in str(err.value)
+        results = [s.result(t) for t in tickets]
         st = s.stats()
-    assert refused > 0 and st["refused_latency"] == refused, (refused, st, budget)
-    assert admitted, "nothing admitted"
-    for (ri, rs), q, k, approx in results:
-        if not approx:
-            ei, es = index.search(q, k=k)
-            np.testing.assert_array_equal(ri, np.atleast_2d(ei))
+        assert st["refused_latency"] >= 1 and st["us_per_query"] > 0
+        # drained: nothing waits now, so a request is admitted again
+        s.result(s.submit(qs[1], k=10))
+    with Server(index, slots=1) as alone:
+        for j in (0, 199, 399):
+            ai, asim = alone.result(alone.submit(qs[j], k=10))
+            np.testing.assert_array_equal(results[j][0], ai)
+            np.testing.assert_array_equal(results[j][1].view(np.uint32), asim.view(np.uint32))
