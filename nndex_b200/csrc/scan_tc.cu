@@ -40,7 +40,13 @@ constexpr int kM = 128;               // queries per CTA (TMEM lanes)
 constexpr int kN = 256;               // base rows per tile (MMA N)
 constexpr uint32_t kAChunk = kM * 128;
 constexpr uint32_t kBChunk = kN * 128;
-constexpr int kThreads = 192;         // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+// Warps: 0 TMA, 1 MMA, then the epilogue: 4 warps in pass 1 (one thread owns a query's heap), 8 in
+// pass 2 (two warps per TMEM lane quarter, each reading half of the tile's columns: collection has
+// no per-query state beyond the threshold, and the epilogue, not the MMA, bounds the pass).
+template <int kMode>
+constexpr uint32_t epi_warps() { return kMode == 1 ? 8u : 4u; }
+template <int kMode>
+constexpr int tc_threads() { return 64 + 32 * static_cast<int>(epi_warps<kMode>()); }
 constexpr uint32_t kTmemCols = 512;   // two 256-column FP32 accumulators
 
 NNDEX_DEVICE_INLINE uint8_t* align_1024(uint8_t* p) {
@@ -74,7 +80,7 @@ size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp
     b += stream_a ? static_cast<size_t>(stages) * (kAChunk + kBChunk)
                   : static_cast<size_t>(nchunks) * kAChunk + static_cast<size_t>(stages) * kBChunk;
     b += static_cast<size_t>(kprime) * kM * 8;
-    b += fp8 ? 2 * kN * 4 + 2 * 4 * 8 : 0;  // row scales and per-warp (min, max) of two tiles
+    b += fp8 ? 2 * kN * 4 + 2 * 8 * 8 : 0;  // row scales and per-warp (min, max) of two tiles
     b += (2 * stages + 5) * 8 + 16;
     return b;
 }
@@ -155,7 +161,7 @@ NNDEX_DEVICE_INLINE void epi_survivor(const TcParams& p, EpiState& st, uint64_t*
 // queries probing one list and its rows one chunk of that list's reordered rows; keys and collected
 // rows carry original row indices, and pass-1 heaps go to the (query, chunk) output slots.
 template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     scan_tc_kernel(const __grid_constant__ CUtensorMap tmap_q, const __grid_constant__ CUtensorMap tmap_b,
                    const TcParams p) {
     constexpr uint32_t kElems = kFp8 ? 128 : 64;  // K elements per 128-byte slab
@@ -166,8 +172,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint8_t* b_smem = a_smem + (kStreamA ? 0 : static_cast<size_t>(p.nchunks) * kAChunk);
     uint64_t* heap = reinterpret_cast<uint64_t*>(b_smem + static_cast<size_t>(kST) * kStage);
     float* scale_s = reinterpret_cast<float*>(heap + static_cast<size_t>(p.kprime) * kM);  // FP8: [2][256]
-    float2* scale_mm = reinterpret_cast<float2*>(scale_s + (kFp8 ? 2 * kN : 0));          // FP8: [2][4]
-    uint64_t* full_bar = reinterpret_cast<uint64_t*>(scale_mm + (kFp8 ? 2 * 4 : 0));
+    float2* scale_mm = reinterpret_cast<float2*>(scale_s + (kFp8 ? 2 * kN : 0));          // FP8: [2][8]
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(scale_mm + (kFp8 ? 2 * 8 : 0));
     uint64_t* empty_bar = full_bar + kST;
     uint64_t* a_full = empty_bar + kST;
     uint64_t* tfull = a_full + 1;
@@ -228,7 +234,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_init(a_full, 1);
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 4);
+            mbar_init(&tempty[b], epi_warps<kMode>());
         }
         *abort_flag = 0;
         fence_mbar_init();
@@ -329,12 +335,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
         }
     } else {
-        // ---------------- epilogue: 4 warps, one query per thread ----------------
+        // ---------------- epilogue: one query per thread (pass 2: two threads, half a tile each) ----
+        constexpr uint32_t kEpiW = epi_warps<kMode>();
+        constexpr uint32_t kChunks = (kN / 32) / (kEpiW / 4);  // 32-column chunks per thread
+        const uint32_t ew = warp - 2;
+        const uint32_t c_begin = (ew / 4) * kChunks;
         const uint32_t quarter = warp & 3u;
         const uint32_t lrow = quarter * 32 + lane;
         const uint32_t q = kItems ? p.it_lane_qid[q0 + lrow] : q0 + lrow;
         const bool valid_q = kItems ? q != 0xFFFFFFFFu : q < nq_live;
-        const uint32_t et = threadIdx.x - 64;  // 0..127
+        const uint32_t et = threadIdx.x - 64;  // 0 .. kEpiW·32 − 1
         const float qs = (kFp8 && valid_q) ? p.q_scale[q] : 1.0f;
         const float rq = valid_q ? p.q_resid[q] : 0.0f;
         const float b_mul = 1.0f + rq, b_add = rq + p.eps_acc;
@@ -360,7 +370,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 // and their extremes over the tile's rows.
                 float* w = scale_s + (t & 1u) * kN;
                 float lo = INFINITY, hi = 0.0f;
-                for (uint32_t j = et; j < static_cast<uint32_t>(kN); j += 128) {
+                for (uint32_t j = et; j < static_cast<uint32_t>(kN); j += kEpiW * 32) {
                     const bool in = tile_row0 + j < row_end;
                     const float v = in ? p.row_scale[tile_row0 + j] : 0.0f;
                     w[j] = v;
@@ -374,12 +384,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                     lo = fminf(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
                     hi = fmaxf(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
                 }
-                if (lane == 0) scale_mm[(t & 1u) * 4 + (warp - 2)] = make_float2(lo, hi);
-                named_bar_sync(2, 128);
+                if (lane == 0) scale_mm[(t & 1u) * 8 + ew] = make_float2(lo, hi);
+                named_bar_sync(2, kEpiW * 32);
                 smin = INFINITY;
 #pragma unroll
-                for (int w4 = 0; w4 < 4; ++w4) {
-                    const float2 m = scale_mm[(t & 1u) * 4 + w4];
+                for (uint32_t w4 = 0; w4 < kEpiW; ++w4) {
+                    const float2 m = scale_mm[(t & 1u) * 8 + w4];
                     smin = fminf(smin, m.x);
                     smax = fmaxf(smax, m.y);
                 }
@@ -400,7 +410,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t taddr = taddr0 + buf * kN;
             uint32_t va[32], vb[32];
             __syncwarp();
-            tc::tmem_ld32(taddr, va);
+            tc::tmem_ld32(taddr + c_begin * 32, va);
             tmem_wait_ld_regs(va);
             // The cut in the domain of the accumulator's raw scores. FP8 scores are scaled by the row's
             // and the query's scales (both positive): a score can reach the cut only if its raw value
@@ -446,7 +456,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             };
 #pragma unroll
-            for (uint32_t c = 0; c < kN / 32; c += 2) {
+            for (uint32_t cc = 0; cc < kChunks; cc += 2) {
+                const uint32_t c = c_begin + cc;
                 // tcgen05.ld and tcgen05.wait::ld are .sync.aligned: the whole warp executes each
                 // one together. process() loops per lane over its survivors (one lane may take
                 // every row while the others take none), so the warp reconverges before each.
@@ -455,9 +466,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 process(va, c);
                 __syncwarp();
                 tmem_wait_ld_regs(vb);
-                if (c + 2 < kN / 32) tc::tmem_ld32(taddr + (c + 2) * 32, va);
+                if (cc + 2 < kChunks) tc::tmem_ld32(taddr + (c + 2) * 32, va);
                 process(vb, c + 1);
-                if (c + 2 < kN / 32) {
+                if (cc + 2 < kChunks) {
                     __syncwarp();
                     tmem_wait_ld_regs(va);
                 }
@@ -513,7 +524,7 @@ NNDEX_DEVICE_INLINE float dot_scan_order(const float* __restrict__ x, const floa
 // ------------------------------------------------------------------------------------------
 // K4 (pass 1): exact FP32 rerank of the k′ candidates + top-k + certificate + T. One block per query.
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(1024)
     rerank_kernel(const float* __restrict__ base, uint32_t ds, const float* __restrict__ queries,
                   const uint64_t* __restrict__ cand_idx, const float* __restrict__ cand_bound,
                   const uint32_t* __restrict__ cand_cnt, uint32_t kp, uint32_t k, uint64_t* __restrict__ idx_out,
@@ -663,7 +674,7 @@ static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
                         "tile stride %u, range rows %llu, rows %llu, smem %zu",
                         kFp8, kST, kMode, kStreamA, kItems, grid.x, grid.y, p.nq, kp, p.tile_stride,
                         (unsigned long long)p.range_rows, (unsigned long long)p.rows, smem);
-    kern<<<grid, kThreads, smem, stream>>>(*a.tmap_q, *a.tmap_b, p);
+    kern<<<grid, tc_threads<kMode>(), smem, stream>>>(*a.tmap_q, *a.tmap_b, p);
     count_launch();
     return cudaGetLastError();
 }
@@ -706,7 +717,10 @@ cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t str
 cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream) {
     uint32_t p2 = 1;
     while (p2 < a.kp) p2 <<= 1;
-    rerank_kernel<<<a.nq, 256, p2 * sizeof(uint64_t), stream>>>(a.base, a.ds, a.queries, a.cand_idx, a.cand_sim,
+    // One block per query; a small batch leaves most SMs idle, so its blocks take 1024 threads (128
+    // candidates re-scored at once instead of 32) to keep more row loads in flight.
+    const uint32_t threads = a.nq < 64 ? 1024u : 256u;
+    rerank_kernel<<<a.nq, threads, p2 * sizeof(uint64_t), stream>>>(a.base, a.ds, a.queries, a.cand_idx, a.cand_sim,
                                                                a.cand_cnt, a.kp, a.k, a.idx_out, a.sim_out,
                                                                a.cnt_out, a.cert_out, a.kth_out, a.certify ? 1 : 0);
     count_launch();

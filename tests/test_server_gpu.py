@@ -114,28 +114,36 @@ def test_poll_without_waiting_and_unknown_ticket(index):
 
 
 def test_latency_budget_refuses_while_the_queue_is_backed_up(index):
-    # one slot taking 64 queries per batch and 400 queued requests of 64: the queue takes many
-    # batches to drain, so after a few milliseconds its oldest request has waited longer than a
-    # 2 ms budget and a new request is refused; the admitted ones still get the index's answers
+    # one slot taking 64 queries per batch and a burst of 1,000 requests of 64: the queue takes
+    # many batches to drain, so a few tens of milliseconds later its oldest request has waited
+    # longer than a 10 ms budget and new requests are refused; the admitted ones still get the
+    # answers they get alone, and once the queue has drained requests are admitted again
     import time
     rng = np.random.default_rng(11)
-    qs = [mixture(rng, 64, index.dims) for _ in range(400)]
-    with Server(index, slots=1, max_batch_queries=64, latency_budget_ms=2) as s:
-        tickets = [s.submit(q, k=10) for q in qs[:1]]
-        time.sleep(0.2)  # the first batch runs alone (any one-off set-up), the queue is empty again
-        s.result(tickets[0])
-        tickets = [s.submit(q, k=10) for q in qs]  # the burst arrives faster than the budget
-        time.sleep(0.008)
-        with pytest.raises(NNdexError) as err:
-            s.submit(qs[0], k=10)
-        assert err.value.code == NNDEX_ERR_ADMISSION and "latency budget" in str(err.value)
-        results = [s.result(t) for t in tickets]
+    qs = [mixture(rng, 64, index.dims) for _ in range(1000)]
+
+    def submit_or_refused(s, q):
+        try:
+            return s.submit(q, k=10)
+        except NNdexError as e:
+            assert e.code == NNDEX_ERR_ADMISSION and "latency budget" in str(e), str(e)
+            return None
+
+    with Server(index, slots=1, max_batch_queries=64, latency_budget_ms=10) as s:
+        s.result(s.submit(qs[0], k=10))  # any one-off set-up runs alone
+        tickets = [submit_or_refused(s, q) for q in qs]
+        time.sleep(0.03)
+        late = submit_or_refused(s, qs[0])
+        results = {j: s.result(t) for j, t in enumerate(tickets) if t is not None}
+        if late is not None:
+            s.result(late)
         st = s.stats()
-        assert st["refused_latency"] >= 1 and st["us_per_query"] > 0
-        # drained: nothing waits now, so a request is admitted again
-        s.result(s.submit(qs[1], k=10))
+        assert st["refused_latency"] >= 1, st
+        assert st["refused_latency"] == st["refused"] == sum(t is None for t in tickets) + (late is None)
+        s.result(s.submit(qs[1], k=10))  # drained: admitted again
+    assert results, "nothing admitted"
     with Server(index, slots=1) as alone:
-        for j in (0, 199, 399):
+        for j in list(results)[:3]:
             ai, asim = alone.result(alone.submit(qs[j], k=10))
             np.testing.assert_array_equal(results[j][0], ai)
             np.testing.assert_array_equal(results[j][1].view(np.uint32), asim.view(np.uint32))
