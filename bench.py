@@ -54,6 +54,8 @@ def parse_args(argv=None):
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--extra-batches", default="1,4", help="batch sizes reported beside the headline")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--autotune", choices=["on", "off"], default="on",
+                   help="off: the fixed path rules for the headline index (profiling a given kernel)")
     p.add_argument("--cpu-sample-batches", type=int, default=2)
     p.add_argument("--c1", choices=["on", "off", "only"], default="on",
                    help="the 50,000 x 128 plain exact section (single query and batch 64, k=10)")
@@ -315,6 +317,8 @@ def run_ours(args):
                                          NNDEX_FLAG_NORMALIZED, C.byref(opts), C.byref(h))
     if st != 0:
         raise RuntimeError(_lib.last_error())
+    if args.autotune == "off":
+        L.nndex_cuda_set_autotune(h, 0)
     base_host = base.cpu().numpy() if (rank == 0 and not args.no_cpu_baseline) else None
     del base
     torch.cuda.empty_cache()

@@ -199,8 +199,10 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         range_rows = (range_rows + 255) / 256 * 256;
         nr = (p.rows + range_rows - 1) / range_rows;
         if (blockIdx.x >= nqb * nr) return;
-        q0 = static_cast<uint32_t>(blockIdx.x / nr) * kM;
-        range = static_cast<uint32_t>(blockIdx.x % nr);
+        // consecutive CTAs take the query blocks of one row range, as the 2-D grid orders them: the
+        // CTAs resident together read the same base tiles, which then come from L2 after the first
+        q0 = static_cast<uint32_t>(blockIdx.x % nqb) * kM;
+        range = static_cast<uint32_t>(blockIdx.x / nqb);
         nranges = static_cast<uint32_t>(nr);
     }
     uint64_t row_begin = static_cast<uint64_t>(range) * range_rows;

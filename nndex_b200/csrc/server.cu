@@ -21,12 +21,13 @@
 // and the queue is bounded in queries (NNDEX_ERR_ADMISSION: the caller may retry later).
 //
 // Admission by latency. With a latency budget, a request is also refused while the oldest queued
-// request has waited longer than the budget: the queue is then backed up, and a new request would
-// wait at least as long. Under overload the queue stops growing at about one budget's worth of
-// work, and the latency of admitted requests stays near the budget plus one batch instead of rising
-// without limit; at loads the slots keep up with, nothing waits that long and nothing is refused.
-// (A cost model of the queue — queries × seconds per query — misjudges it both ways, because a
-// batch's cost per query falls steeply with its size.)
+// request has waited longer than the budget (the queue is backed up: a newcomer would wait at least
+// as long), or when the queries ahead of it would take longer than the budget to drain at the cost
+// per query of large batches (a moving average over batches of at least a quarter of the batch
+// limit: a long queue is served in such batches). Small batches cost far more per query, so their
+// cost is not used: at light loads the queue is short and only its age matters. Under overload the
+// queue stops growing at about one budget's worth of work, and the latency of admitted requests
+// stays near the budget plus one batch instead of rising without limit.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -82,7 +83,8 @@ struct Server {
     uint64_t next_ticket = 1, next_batch = 1;
     bool stopping = false;
     nndex_cuda_server_stats st{};
-    double spq = 0.0;  // moving average of one slot's wall seconds per query (0 until a batch ran)
+    double spq = 0.0;      // moving average of one slot's wall seconds per query (0 until a batch ran)
+    double spq_big = 0.0;  // the same over large batches (≥ a quarter of max_batch_queries) only
 
     // Device bytes a batch of nq queries at k (capped) needs in a slot.
     uint64_t batch_bytes(uint64_t nq, uint64_t kcap, bool approx, uint32_t nprobe) const {
@@ -194,6 +196,7 @@ void Server::worker(uint32_t slot) {
             std::lock_guard<std::mutex> lk(mu);
             const double per = static_cast<double>(t_done - t_start) * 1e-9 / static_cast<double>(nq);
             spq = spq > 0.0 ? 0.9 * spq + 0.1 * per : per;
+            if (nq * 4 >= opts.max_batch_queries) spq_big = spq_big > 0.0 ? 0.9 * spq_big + 0.1 * per : per;
             st.us_per_query = spq * 1e6;
             for (size_t i = 0; i < batch.size(); ++i) {
                 auto& r = batch[i];
@@ -313,14 +316,19 @@ int nndex_cuda_server_submit(nndex_cuda_server* server, const float* host_querie
                              (unsigned long long)s->st.queued_queries);
         }
         if (s->opts.latency_budget_ms && !s->queue.empty()) {
+            const double budget = static_cast<double>(s->opts.latency_budget_ms);
             const double age_ms = static_cast<double>(now_ns() - s->queue.front()->info.submit_ns) * 1e-6;
-            if (age_ms > static_cast<double>(s->opts.latency_budget_ms)) {
+            // the wait ahead of this request at the cost per query of large batches (what a long
+            // queue is served in)
+            const double drain_ms = static_cast<double>(s->st.queued_queries + r->nq) * s->spq_big * 1e3 /
+                                    static_cast<double>(s->opts.slots);
+            if (age_ms > budget || drain_ms > budget) {
                 s->st.refused += 1;
                 s->st.refused_latency += 1;
                 return set_error(NNDEX_ERR_ADMISSION,
-                                 "cuda execution error: the oldest of %llu queued queries has waited %.1f ms, above the "
-                                 "%u ms latency budget",
-                                 (unsigned long long)s->st.queued_queries, age_ms, s->opts.latency_budget_ms);
+                                 "cuda execution error: %llu queued queries (the oldest waiting %.1f ms, about %.1f ms "
+                                 "to drain) exceed the %u ms latency budget",
+                                 (unsigned long long)s->st.queued_queries, age_ms, drain_ms, s->opts.latency_budget_ms);
             }
         }
         r->ticket = s->next_ticket++;
