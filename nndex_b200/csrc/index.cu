@@ -961,6 +961,9 @@ int CudaIndex::tune_host(uint64_t n, uint64_t kcap, int mode, TunePlan* plan) {
             if (cst == NNDEX_OK) cst = check_device_words();
             if (cst == NNDEX_OK && (cands[c].path == 2 || cands[c].path == 3))
                 cst = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream);
+            if (cst == NNDEX_OK && cands[c].path == 5)
+                cst = ivf_finish_tc(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
+                                    stream);
             ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         }
         forced_stride = 0;
@@ -1030,14 +1033,13 @@ int CudaIndex::enqueue_host_batch(uint64_t n, uint64_t kcap, int mode, int path)
 
 // The batch through a CUDA graph when one is cached for this shape, capturing it when the same
 // shape came in the previous call (its buffers are then allocated, so nothing allocates during
-// the capture); otherwise directly. Every path whose batch needs no host decision in its middle:
-// the FP32 scan (1), the tensor-core scans (2, 3: pass 2 and its compaction run on the device; the
+// the capture); otherwise directly. No path needs a host decision in the middle of its batch: the
+// FP32 scan (1), the tensor-core scans (2, 3, 5: pass 2 and its compaction run on the device; the
 // rare FP32 re-run of an overflowed collection follows the batch), the IVF list scan (4) and the
-// TF32 candidate scan (6, its certificate's fallback on the device). The tensor-core IVF list scan
-// (5) plans its pass 2 on the host.
+// TF32 candidate scan (6, its certificate's fallback on the device).
 int CudaIndex::run_host_batch(uint64_t n, uint64_t kcap, int mode, int path) {
     const bool graphable = use_graphs && !scan_timing && !error_report && !sync_check_enabled() &&
-                           (path == 1 || path == 2 || path == 3 || path == 4 || path == 6) &&
+                           path >= 1 && path <= 6 &&
                            !(graph_failed_paths & (1u << path));
     if (!graphable) return enqueue_host_batch(n, kcap, mode, path);
     const uint64_t epoch = alloc_epoch();
@@ -1156,10 +1158,13 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_error(e, "search");
         if ((st = check_device_words())) return st;
-        if (path == 2 || path == 3) {
+        if (path == 2 || path == 3 || path == 5) {
             // pass 2 ran on the device; a query whose collection overflowed is re-run now
-            if ((st = finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt, stream)))
-                return st;
+            st = path == 5 ? ivf_finish_tc(*this, static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim,
+                                           d_cnt, stream)
+                           : finish_tc(static_cast<uint32_t>(n), static_cast<uint32_t>(kcap), d_idx, d_sim, d_cnt,
+                                       stream);
+            if (st) return st;
             if (stats.fp32_fallback_queries) {
                 cudaMemcpyAsync(h_res, d_res, res_bytes, cudaMemcpyDeviceToHost, stream);
                 if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_error(e, "search");
@@ -1192,7 +1197,14 @@ int CudaIndex::run_device_chunk(const float* dq, uint64_t n, uint64_t kcap, int 
     if (path == 4) return ivf_search(*this, d_qn, n32, k32, oi, os, oc, s);
     if (path == 5) {
         *synced = true;
-        return ivf_search_tc(*this, n32, k32, oi, os, oc, s);
+        if ((st = ivf_search_tc(*this, n32, k32, oi, os, oc, s))) return st;
+        h_flags[1] = 0;
+        cudaMemcpyAsync(&h_flags[0], d_err, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&h_flags[1], d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        const cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_error(e, "IVF search");
+        if ((st = check_device_words())) return st;
+        return ivf_finish_tc(*this, n32, k32, oi, os, oc, s);
     }
     if (path == 1) return enqueue_exact_fp32(d_qn, n32, k32, k32, oi, os, oc, s);
     // the certificates' fallbacks need the host: these paths synchronise

@@ -86,8 +86,13 @@ int base_checksum(CudaIndex& ix, uint64_t* out);
 int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim,
                uint32_t* o_cnt, cudaStream_t s);
 // The same result on the tensor cores: BF16 list scan with certified candidates, exact FP32 rerank
-// (the queries of ix.d_qn and their BF16 copies ix.d_q_bf16 / ix.d_q_resid). Synchronises the stream.
+// (the queries of ix.d_qn and their BF16 copies ix.d_q_bf16 / ix.d_q_resid). Enqueues without a host
+// round trip; ivf_finish_tc completes the batch once the stream has.
 int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                  cudaStream_t s);
+// After the stream has completed an ivf_search_tc batch: statistics, the pass-1 stride rule, and an
+// FP32 list-scan re-run of queries whose collection overflowed (patched into the outputs).
+int ivf_finish_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
                   cudaStream_t s);
 
 // src/approx.rs:305-311 choose_nlist and 318-336 choose_nprobe.

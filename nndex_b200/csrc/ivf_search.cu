@@ -604,9 +604,13 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
 // reordered BF16 rows and leaves the k′ best upper bounds per (query, chunk) in its slot; the merge
 // keeps the k′ best per query over its slots and K4 re-scores them exactly in FP32: the exact k-th
 // score T, and a certificate when T beats the k′-th bound (no other probed row can reach the top k).
-// Pass 2, for the other queries: every probed row whose bound reaches T, re-scored exactly; a query
-// whose collection overflows runs on the FP32 list scan. The result equals the FP32 list scan's
-// (the same probed rows, the same exact scores, bit for bit).
+// Pass 2, for the other queries: every probed row whose bound reaches T, re-scored exactly. The
+// result equals the FP32 list scan's (the same probed rows, the same exact scores, bit for bit).
+//
+// Everything is enqueued without a host round trip: the grid is the largest item count the plan
+// can produce (its CTAs past the plan's own count return at once), the uncertified queries are
+// compacted on the device (pass 2 returns at once when there are none), and the queries whose
+// collection overflowed are compacted for ivf_finish_tc, which runs once the stream has completed.
 int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
                   cudaStream_t s) {
     const IvfIndex& v = *ix.ivf;
@@ -623,6 +627,11 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     const uint64_t max_chunks = (v.max_list + kChunkRows - 1) / kChunkRows;
     const uint64_t pairs = static_cast<uint64_t>(nq) * np;
     const uint64_t max_blocks = nlist + (pairs + 127) / 128;
+    // Σ over lists of (query groups × chunks) ≤ (pairs / 128) · max_chunks + Σ chunks ≤ … + rows / chunk + nlist
+    const uint64_t max_items = (pairs + 127) / 128 * max_chunks + ix.rows / kChunkRows + nlist + 1;
+    if (max_items > 0x7FFFFFFFull)
+        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF batch of %u queries × %u lists too large", nq, np);
+    const uint32_t cap2 = kSecondPassCap;
     int st;
     if ((st = grow(w.d_probes, w.cap_probes, pairs, "IVF probe buffer"))) return st;
     if ((st = grow(w.d_list_cnt, w.cap_list_cnt, nlist, "IVF plan buffer"))) return st;
@@ -644,6 +653,13 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     if ((st = grow(ix.d_cand_cnt, ix.cap_cand_cnt, nq, "tc workspace"))) return st;
     if ((st = grow(ix.d_cert, ix.cap_cert, nq, "tc workspace"))) return st;
     if ((st = grow(ix.d_kth, ix.cap_kth, nq, "tc workspace"))) return st;
+    if ((st = grow(ix.d_ids, ix.cap_ids, nq, "pass-2 buffer"))) return st;
+    if ((st = grow(ix.d_q2_thr, ix.cap_q2_thr, nq, "pass-2 buffer"))) return st;
+    if ((st = grow(ix.d_rows2, ix.cap_rows2, static_cast<size_t>(nq) * cap2, "pass-2 buffer"))) return st;
+    if ((st = grow(ix.d_cnt2, ix.cap_cnt2, nq, "pass-2 buffer"))) return st;
+    if ((st = grow(ix.d_ok2, ix.cap_ok2, nq, "pass-2 buffer"))) return st;
+    if ((st = grow(ix.d_tcfail, ix.cap_tcfail, nq, "pass-2 buffer"))) return st;
+    if ((st = ix.ensure_fbn())) return st;
     if (!w.h_probed) bump_alloc_epoch();
     if (!w.h_probed && cudaMallocHost(&w.h_probed, 8 * sizeof(unsigned long long)) != cudaSuccess)
         return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: pinned allocation failed");
@@ -665,17 +681,10 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     count_launch(3);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "IVF plan launch");
-    cudaMemcpyAsync(w.h_probed, w.d_counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "IVF plan");
-    const uint64_t items = w.h_probed[1], blocks = w.h_probed[6];
-    const unsigned long long rows_probed = w.h_probed[3], streamed = w.h_probed[4], uni = w.h_probed[5];
-    if (items == 0 || blocks > max_blocks)
-        return set_error(NNDEX_ERR_CUDA, "cuda execution error: IVF plan produced %llu items, %llu query blocks",
-                         (unsigned long long)items, (unsigned long long)blocks);
 
     // ---- pass 1 ----
     CUtensorMap tmap_q;
-    if ((st = ix.encode_query_tmap(false, w.d_g16, static_cast<uint32_t>(blocks * 128), &tmap_q))) return st;
+    if ((st = ix.encode_query_tmap(false, w.d_g16, static_cast<uint32_t>(max_blocks * 128), &tmap_q))) return st;
     cudaMemsetAsync(ix.d_thr, 0, nq * sizeof(unsigned long long), s);
     TcArgs a;
     a.tmap_q = &tmap_q;
@@ -683,7 +692,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     a.nranges = 1;
     a.stages = plan.stages;
     a.stream_a = plan.stream_a;
-    a.items = static_cast<uint32_t>(items);
+    a.items = static_cast<uint32_t>(max_items);
     ix.fill_tc_params(false, nq, 0, a.p);
     a.p.row_resid = v.d_res16;
     a.p.eps_rows = v.eps16;
@@ -691,8 +700,9 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     a.p.kprime = kp;
     a.p.thr_global = ix.d_thr;
     a.p.ws_keys = w.d_ws;
-    // Autotuned like the exact path's pass 1: when pass 1 rarely certifies, it only has to give each
-    // query its threshold T, and every 4th tile of its lists gives a valid one.
+    // Like the exact path's pass 1: when pass 1 rarely certifies, it only has to give each query its
+    // threshold T, and every 4th tile of its lists gives a valid one (the rule lives in
+    // ivf_finish_tc).
     const uint32_t stride = w.tc_stride;
     a.p.tile_stride = stride;
     a.p.it_item_off = w.d_item_off;
@@ -731,44 +741,11 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     r.kth_out = ix.d_kth;
     r.certify = stride == 1;
     if ((e = launch_rerank(r, s)) != cudaSuccess) return cuda_error(e, "rerank launch");
-    if ((st = grow_pinned(ix.h_cert, ix.cap_hcert, nq, "pinned buffer"))) return st;
-    cudaMemcpyAsync(ix.h_cert, ix.d_cert, nq * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    ix.h_flags[1] = 0;
-    cudaMemcpyAsync(&ix.h_flags[1], ix.d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "IVF search");
-    if (ix.h_flags[1] != 0) return ix.check_device_words();
-    ix.stats.kernel_launches += 6;
-    ix.stats.path = 5;
-    ix.stats.nprobe = np;
-    ix.stats.rerank_width = kp;
-    ix.stats.rows_scanned = rows_probed;
-    ix.stats.ivf_rows_streamed = streamed;
-    ix.stats.ivf_rows_union = uni;
-    if ((st = grow_pinned(ix.h_ids, ix.cap_hids, nq, "pinned buffer"))) return st;
-    uint32_t m = 0;
-    for (uint32_t i = 0; i < nq; ++i)
-        if (!ix.h_cert[i]) ix.h_ids[m++] = i;
-    ix.stats.certified = m == 0 ? 1u : 0u;
-    ix.stats.second_pass_queries = m;
-    ix.stats.pass1_tile_stride = stride;
-    if (stride == 1 && m * 2 > nq) {
-        static const uint32_t sampled = [] {
-            const char* v = getenv("NNDEX_IVF_TC_STRIDE");  // measurement override of the sampled stride
-            const uint32_t x = v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
-            return x >= 2 && x <= 16 ? x : 4u;
-        }();
-        w.tc_stride = sampled;
-    }
-    if (m == 0) return NNDEX_OK;
 
     // ---- pass 2: every probed row whose bound reaches T, for the uncertified queries ----
-    const uint32_t cap2 = kSecondPassCap;
-    if ((st = grow(ix.d_ids, ix.cap_ids, m, "pass-2 buffer"))) return st;
-    if ((st = grow(ix.d_q2_thr, ix.cap_q2_thr, nq, "pass-2 buffer"))) return st;
-    if ((st = grow(ix.d_rows2, ix.cap_rows2, static_cast<size_t>(nq) * cap2, "pass-2 buffer"))) return st;
-    if ((st = grow(ix.d_cnt2, ix.cap_cnt2, nq, "pass-2 buffer"))) return st;
-    if ((st = grow(ix.d_ok2, ix.cap_ok2, m, "pass-2 buffer"))) return st;
-    cudaMemcpyAsync(ix.d_ids, ix.h_ids, m * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    uint32_t* d_m = ix.d_fbn + 1;     // uncertified queries
+    uint32_t* d_fail = ix.d_fbn + 2;  // of them, collections that overflowed
+    launch_compact_zero_flags(ix.d_cert, nq, ix.d_ids, d_m, s);
     ivf_pass2_thr_kernel<<<(nq + 255) / 256, 256, 0, s>>>(ix.d_cert, ix.d_kth, nq, ix.d_q2_thr);
     count_launch();
     cudaMemsetAsync(ix.d_cnt2, 0, nq * sizeof(uint32_t), s);
@@ -780,28 +757,61 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     a.p.cand_rows = ix.d_rows2;
     a.p.cand_cnt = ix.d_cnt2;
     a.p.cap2 = cap2;
+    a.p.live_q = d_m;  // item mode: the whole pass returns at once when every query certified
     ix.scan_event_begin(s, ev_a);
     e = launch_scan_tc(a, false, 1, s);
     ix.scan_event_end(s, ev_a);
     if (e != cudaSuccess) return cuda_error(e, "IVF tensor-core scan launch (pass 2)");
-    e = launch_rerank_collected(ix.d_base, static_cast<uint32_t>(ix.ds), ix.d_qn, ix.d_ids, m, ix.d_rows2, ix.d_cnt2,
-                                cap2, k, o_idx, o_sim, o_cnt, ix.d_ok2, s, true);
+    e = launch_rerank_collected(ix.d_base, static_cast<uint32_t>(ix.ds), ix.d_qn, ix.d_ids, nq, ix.d_rows2, ix.d_cnt2,
+                                cap2, k, o_idx, o_sim, o_cnt, ix.d_ok2, s, true, d_m);
     if (e != cudaSuccess) return cuda_error(e, "rerank launch (pass 2)");
-    ix.stats.kernel_launches += 3;
-    if ((st = grow_pinned(ix.h_ok2, ix.cap_hok2, m, "pinned buffer"))) return st;
-    cudaMemcpyAsync(ix.h_ok2, ix.d_ok2, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    ix.h_flags[1] = 0;
-    cudaMemcpyAsync(&ix.h_flags[1], ix.d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "IVF search");
-    if (ix.h_flags[1] != 0) return ix.check_device_words();
-    std::vector<uint32_t> failed;
-    for (uint32_t i = 0; i < m; ++i)
-        if (!ix.h_ok2[i]) failed.push_back(ix.h_ids[i]);
-    ix.stats.fp32_fallback_queries = static_cast<uint32_t>(failed.size());
-    if (failed.empty()) return NNDEX_OK;
+    launch_compact_zero_flags(ix.d_ok2, nq, ix.d_tcfail, d_fail, s, d_m);
+    // the plan's totals and the pass counts come back with the results
+    cudaMemcpyAsync(w.h_probed, w.d_counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(ix.h_fbn, ix.d_fbn, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    ix.last_tc_n = nq;
+    ix.stats.kernel_launches += 11;
+    ix.stats.path = 5;
+    ix.stats.nprobe = np;
+    ix.stats.rerank_width = kp;
+    ix.stats.pass1_tile_stride = stride;
+    return NNDEX_OK;
+}
 
+// After the stream has completed an ivf_search_tc batch: statistics, the pass-1 stride rule, and
+// the FP32 list scan for queries whose collection overflowed (outputs patched in place; it
+// synchronises the stream again only then).
+int ivf_finish_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float* o_sim, uint32_t* o_cnt,
+                  cudaStream_t s) {
+    IvfScratch& w = ix.ivf_scratch;
+    const uint32_t m = ix.h_fbn[1], failed_n = ix.h_fbn[2];
+    ix.stats.rows_scanned = w.h_probed[3];
+    ix.stats.ivf_rows_streamed = w.h_probed[4];
+    ix.stats.ivf_rows_union = w.h_probed[5];
+    ix.stats.certified = m == 0 ? 1u : 0u;
+    ix.stats.second_pass_queries = m;
+    ix.stats.fp32_fallback_queries = failed_n;
+    if (w.tc_stride == 1 && m * 2 > nq) {
+        static const uint32_t sampled = [] {
+            const char* v = getenv("NNDEX_IVF_TC_STRIDE");  // measurement override of the sampled stride
+            const uint32_t x = v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
+            return x >= 2 && x <= 16 ? x : 4u;
+        }();
+        w.tc_stride = sampled;
+        ix.drop_graphs();  // a captured batch keeps its stride
+    }
+    if (failed_n == 0) return NNDEX_OK;
     // ---- FP32 list scan for the queries whose collection overflowed ----
-    const uint32_t mf = static_cast<uint32_t>(failed.size());
+    int st;
+    if ((st = grow_pinned(ix.h_ids, ix.cap_hids, nq, "pinned buffer"))) return st;
+    if ((st = grow_pinned(ix.h_ok2, ix.cap_hok2, nq, "pinned buffer"))) return st;
+    cudaMemcpyAsync(ix.h_ids, ix.d_ids, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(ix.h_ok2, ix.d_tcfail, failed_n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaError_t e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "IVF search");
+    std::vector<uint32_t> failed(failed_n);
+    for (uint32_t i = 0; i < failed_n; ++i) failed[i] = ix.h_ids[ix.h_ok2[i]];
+    const uint32_t mf = failed_n;
     if ((st = grow(ix.d_qsub, ix.cap_qsub, static_cast<size_t>(mf) * ix.ds, "fallback buffer"))) return st;
     for (uint32_t i = 0; i < mf; ++i)
         cudaMemcpyAsync(ix.d_qsub + static_cast<uint64_t>(i) * ix.ds, ix.d_qn + static_cast<uint64_t>(failed[i]) * ix.ds,

@@ -210,6 +210,10 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     uint32_t chunk = 0;  // item mode: the chunk of the list (its output slot offset)
     if (kItems) {
         const uint32_t wi = blockIdx.x;
+        // the grid is an upper bound of the plan's items; pass 2 has nothing to do when every
+        // query certified (the device count of the others is zero)
+        if (wi >= p.it_item_off[p.it_nlist]) return;
+        if (kMode == 1 && p.live_q && *p.live_q == 0) return;
         uint32_t lo = 0, hi = p.it_nlist;  // the last list whose first item is ≤ wi
         while (hi - lo > 1) {
             const uint32_t mid = (lo + hi) >> 1;

@@ -101,3 +101,21 @@ def test_certified_paths_are_captured_and_replayed(precision, batch, path):
         assert st["path"] == path, st
         kinds.append(st["graph"])
     assert 2 in kinds, kinds
+
+
+def test_ivf_tensor_core_batches_are_captured_and_replayed():
+    # the tensor-core IVF list scan plans, certifies and collects on the device too
+    base, rng = _mixture(60_000, 128, 6)
+    kw = dict(approx=True, precision="auto", nlist=32, kmeans_iters=3, seed=2, nprobe=8, autotune=False)
+    a = NNdex(base, **kw)
+    b = NNdex(base, **kw)
+    _lib.lib().nndex_cuda_set_graphs(b.handle, 0)
+    centres, _ = _mixture(200, 128, 6)
+    kinds = []
+    for step in range(6):
+        q = (centres[rng.integers(0, 200, 200)] + 0.3 * rng.normal(size=(200, 128))).astype(np.float32)
+        _bits(a.search(q, k=10), b.search(q, k=10))
+        st = a.last_search_stats()
+        assert st["path"] == 5, st
+        kinds.append(st["graph"])
+    assert 2 in kinds, kinds
