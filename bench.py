@@ -1083,6 +1083,10 @@ def run_serve(args, dev, L, world):
         "mean_batch_queries": sst.queries_done / max(sst.batches, 1),
         "max_queued_queries": sst.max_queued_queries,
         "slot_bytes": sst.slot_bytes,
+        "fp32_fallback_queries": sst.fp32_fallback_queries,
+        "slowest_batch": {"ms": sst.slowest_batch_ms, "queries": sst.slowest_batch_queries,
+                          "k": sst.slowest_batch_k, "path": sst.slowest_batch_path,
+                          "approx": bool(sst.slowest_batch_approx)},
     }
 
 

@@ -421,6 +421,12 @@ typedef struct nndex_cuda_server_stats {
     uint64_t refused_latency;      /* of `refused`: refused by the latency budget               */
     double us_per_query;           /* moving average of a slot's wall time per query (batches'
                                       launch to results), for reports                           */
+    uint64_t fp32_fallback_queries;  /* queries of all batches re-run on an FP32 scan            */
+    double slowest_batch_ms;         /* the slowest batch so far: its wall time,                */
+    uint32_t slowest_batch_queries;  /*   its queries,                                           */
+    uint32_t slowest_batch_k;        /*   the k it ran at,                                       */
+    uint32_t slowest_batch_path;     /*   its path (nndex_cuda_search_stats::path)               */
+    uint32_t slowest_batch_approx;   /*   and whether it was an IVF batch                        */
 } nndex_cuda_server_stats;
 
 NNDEX_API int nndex_cuda_server_start(nndex_cuda_index* index, const nndex_cuda_server_opts* opts,

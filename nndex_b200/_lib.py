@@ -145,6 +145,12 @@ class ServerStats(C.Structure):
         ("slot_bytes", C.c_uint64),
         ("refused_latency", C.c_uint64),
         ("us_per_query", C.c_double),
+        ("fp32_fallback_queries", C.c_uint64),
+        ("slowest_batch_ms", C.c_double),
+        ("slowest_batch_queries", C.c_uint32),
+        ("slowest_batch_k", C.c_uint32),
+        ("slowest_batch_path", C.c_uint32),
+        ("slowest_batch_approx", C.c_uint32),
     ]
 
 

@@ -191,6 +191,7 @@ void Server::worker(uint32_t slot) {
             }
         }
         const uint64_t t_done = now_ns();
+        v->fetch_fallback_stats();  // the TF32 path's device-side re-run count
         const uint32_t path = v->stats.path;
         {
             std::lock_guard<std::mutex> lk(mu);
@@ -198,6 +199,15 @@ void Server::worker(uint32_t slot) {
             spq = spq > 0.0 ? 0.9 * spq + 0.1 * per : per;
             if (nq * 4 >= opts.max_batch_queries) spq_big = spq_big > 0.0 ? 0.9 * spq_big + 0.1 * per : per;
             st.us_per_query = spq * 1e6;
+            st.fp32_fallback_queries += v->stats.fp32_fallback_queries;
+            const double ms = static_cast<double>(t_done - t_start) * 1e-6;
+            if (ms > st.slowest_batch_ms) {
+                st.slowest_batch_ms = ms;
+                st.slowest_batch_queries = static_cast<uint32_t>(nq);
+                st.slowest_batch_k = static_cast<uint32_t>(kmax);
+                st.slowest_batch_path = path;
+                st.slowest_batch_approx = approx ? 1u : 0u;
+            }
             for (size_t i = 0; i < batch.size(); ++i) {
                 auto& r = batch[i];
                 r->status = codes[i];
