@@ -231,6 +231,7 @@ CudaIndex::~CudaIndex() {
     if (owns_base) cudaFree(d_res16);
     if (owns_base) cudaFree(d_res8);
     if (owns_base) cudaFree(d_row_scale);
+    if (owns_base) cudaFree(d_tile_scale);
     cudaFree(d_q_bf16);
     cudaFree(d_q_fp8);
     cudaFree(d_q_scale);
@@ -659,6 +660,7 @@ void CudaIndex::fill_tc_params(bool fp8, uint32_t n, uint64_t range_rows, TcPara
     p.rows = rows;
     p.range_rows = range_rows;
     p.row_scale = fp8 ? d_row_scale : nullptr;
+    p.tile_scale = fp8 ? d_tile_scale : nullptr;
     p.row_resid = fp8 ? d_res8 : d_res16;
     p.eps_rows = fp8 ? eps_fp8 : eps_bf16;
     // FP32 accumulation of kb exact products (|Σ| ≤ 1 + ε): kb·2^-23, with a 4× margin.
@@ -1541,6 +1543,12 @@ int index_finish(CudaIndex* ix) {
         !encode_tmap_2d(&ix->tmap_fp8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ix->d_base_fp8, ix->kf8, ix->rows_alloc,
                         ix->kf8, 128, 256, CU_TENSOR_MAP_SWIZZLE_128B))
         return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (FP8)"));
+    if (ix->d_row_scale) {
+        // FP8 scan: the scale extremes of each 256-row tile (its epilogue's per-tile cut)
+        if ((e = cudaMalloc(&ix->d_tile_scale, ix->rows_alloc / 256 * sizeof(float2))) != cudaSuccess)
+            return fail(cuda_error(e, "FP8 tile scales"));
+        launch_tile_scale(ix->d_row_scale, ix->rows, ix->rows_alloc / 256, ix->d_tile_scale, ix->stream);
+    }
     // Row norms of K12's bound (8 bytes per row, one pass over the base). Without them (no memory)
     // small batches take the FP32 scan.
     if (cudaMalloc(&ix->d_tfnorm, ix->rows * sizeof(float2)) == cudaSuccess) {
@@ -1646,6 +1654,7 @@ int make_view(const CudaIndex& src, CudaIndex** out) {
     v->d_base_bf16 = src.d_base_bf16;
     v->d_base_fp8 = src.d_base_fp8;
     v->d_row_scale = src.d_row_scale;
+    v->d_tile_scale = src.d_tile_scale;
     v->eps_bf16 = src.eps_bf16;
     v->eps_fp8 = src.eps_fp8;
     v->d_res16 = src.d_res16;

@@ -67,6 +67,7 @@ struct CudaIndex {
     __nv_bfloat16* d_base_bf16 = nullptr;      // rows_alloc × kb16
     uint8_t* d_base_fp8 = nullptr;             // rows_alloc × kf8 (E4M3)
     float* d_row_scale = nullptr;              // rows_alloc: FP8 dequantisation scale per row
+    float2* d_tile_scale = nullptr;            // rows_alloc / 256: FP8 {min, max} scale per 256-row tile
     float eps_bf16 = 0.0f, eps_fp8 = 0.0f;     // max row residual norm ‖x − x̂‖
     float* d_res16 = nullptr;                  // rows: ‖x − x̂‖ of the BF16 copy
     float* d_res8 = nullptr;                   // rows: ‖x − x̂‖ of the FP8 copy

@@ -103,6 +103,7 @@ struct TcParams {
     uint64_t range_rows = 0;              // rows per CTA range (multiple of 256)
     uint32_t tile_stride = 1;             // scan every tile_stride-th 256-row tile (pass-1 sampling)
     const float* row_scale = nullptr;     // FP8 only
+    const float2* tile_scale = nullptr;   // FP8 only: per 256-row tile, {min, max} of its rows' scales
     const float* q_scale = nullptr;       // FP8 only
     const float* row_resid = nullptr;     // ‖x − x̂‖ per row
     const float* q_resid = nullptr;       // ‖q − q̂‖ per query
@@ -207,6 +208,8 @@ cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float*
                                     uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
                                     cudaStream_t stream, bool by_query = false, const uint32_t* live = nullptr);
 cudaError_t launch_max_reduce(const float* v, uint64_t n, unsigned int* out, cudaStream_t stream);
+// FP8: {min, max} row scale of each 256-row tile (tiles = rows_alloc / 256).
+void launch_tile_scale(const float* row_scale, uint64_t rows, uint64_t tiles, float2* out, cudaStream_t s);
 
 // Maximum k the fused scan kernels select in shared memory.
 constexpr uint32_t kMaxFusedK = 2048;

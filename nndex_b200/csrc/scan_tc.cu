@@ -80,7 +80,6 @@ size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp
     b += stream_a ? static_cast<size_t>(stages) * (kAChunk + kBChunk)
                   : static_cast<size_t>(nchunks) * kAChunk + static_cast<size_t>(stages) * kBChunk;
     b += static_cast<size_t>(kprime) * kM * 8;
-    b += fp8 ? 2 * kN * 4 + 2 * 8 * 8 : 0;  // row scales and per-warp (min, max) of two tiles
     b += (2 * stages + 5) * 8 + 16;
     return b;
 }
@@ -171,9 +170,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     uint8_t* a_smem = smem;  // resident query slabs (kStreamA: none)
     uint8_t* b_smem = a_smem + (kStreamA ? 0 : static_cast<size_t>(p.nchunks) * kAChunk);
     uint64_t* heap = reinterpret_cast<uint64_t*>(b_smem + static_cast<size_t>(kST) * kStage);
-    float* scale_s = reinterpret_cast<float*>(heap + static_cast<size_t>(p.kprime) * kM);  // FP8: [2][256]
-    float2* scale_mm = reinterpret_cast<float2*>(scale_s + (kFp8 ? 2 * kN : 0));          // FP8: [2][8]
-    uint64_t* full_bar = reinterpret_cast<uint64_t*>(scale_mm + (kFp8 ? 2 * 8 : 0));
+    uint64_t* full_bar = heap + static_cast<size_t>(p.kprime) * kM;
     uint64_t* empty_bar = full_bar + kST;
     uint64_t* a_full = empty_bar + kST;
     uint64_t* tfull = a_full + 1;
@@ -350,7 +347,6 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         const uint32_t lrow = quarter * 32 + lane;
         const uint32_t q = kItems ? p.it_lane_qid[q0 + lrow] : q0 + lrow;
         const bool valid_q = kItems ? q != 0xFFFFFFFFu : q < nq_live;
-        const uint32_t et = threadIdx.x - 64;  // 0 .. kEpiW·32 − 1
         const float qs = (kFp8 && valid_q) ? p.q_scale[q] : 1.0f;
         const float rq = valid_q ? p.q_resid[q] : 0.0f;
         const float b_mul = 1.0f + rq, b_add = rq + p.eps_acc;
@@ -369,36 +365,14 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         for (uint32_t t = 0; t < ntiles; ++t) {
             const uint32_t buf = t & 1u, ub = t >> 1;
             const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * tile_step;
-            const float* sc = scale_s + (t & 1u) * kN;
+            // FP8: the extremes of the row scales over this tile's rows (computed once per index), so
+            // no thread needs the tile's 256 scales unless a score may survive
             float smin = 0.0f, smax = 0.0f;
+            const float* sc = kFp8 ? p.row_scale + tile_row0 : nullptr;
             if (kFp8) {
-                // Row scales of this tile, shared by the 128 queries (each applies its own scale),
-                // and their extremes over the tile's rows.
-                float* w = scale_s + (t & 1u) * kN;
-                float lo = INFINITY, hi = 0.0f;
-                for (uint32_t j = et; j < static_cast<uint32_t>(kN); j += kEpiW * 32) {
-                    const bool in = tile_row0 + j < row_end;
-                    const float v = in ? p.row_scale[tile_row0 + j] : 0.0f;
-                    w[j] = v;
-                    if (in) {
-                        lo = fminf(lo, v);
-                        hi = fmaxf(hi, v);
-                    }
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    lo = fminf(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
-                    hi = fmaxf(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
-                }
-                if (lane == 0) scale_mm[(t & 1u) * 8 + ew] = make_float2(lo, hi);
-                named_bar_sync(2, kEpiW * 32);
-                smin = INFINITY;
-#pragma unroll
-                for (uint32_t w4 = 0; w4 < kEpiW; ++w4) {
-                    const float2 m = scale_mm[(t & 1u) * 8 + w4];
-                    smin = fminf(smin, m.x);
-                    smax = fmaxf(smax, m.y);
-                }
+                const float2 mm = p.tile_scale[tile_row0 / kN];
+                smin = mm.x;
+                smax = mm.y;
             }
             if (!*abort_flag && !mbar_wait_bounded(&tfull[buf], ub & 1u, kWaitBudgetCycles)) {
                 *abort_flag = 1;
@@ -848,6 +822,35 @@ void launch_scatter_results(const uint64_t* fb_idx, const float* fb_sim, const u
                             cudaStream_t s) {
     if (n == 0) return;
     scatter_results_kernel<<<n, 128, 0, s>>>(fb_idx, fb_sim, fb_cnt, ids, count, k, idx, sim, cnt);
+    count_launch();
+}
+
+// FP8: per 256-row tile of the base, {smallest, largest} scale over the tile's rows (rows past the
+// base excluded; a tile without rows gets {+inf, 0}). One warp per tile.
+__global__ void tile_scale_kernel(const float* __restrict__ row_scale, uint64_t rows, uint64_t tiles,
+                                  float2* __restrict__ out) {
+    const uint64_t t = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (t >= tiles) return;
+    float lo = INFINITY, hi = 0.0f;
+    for (uint32_t j = lane; j < 256; j += 32) {
+        const uint64_t r = t * 256 + j;
+        if (r < rows) {
+            lo = fminf(lo, row_scale[r]);
+            hi = fmaxf(hi, row_scale[r]);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+    }
+    if (lane == 0) out[t] = make_float2(lo, hi);
+}
+
+void launch_tile_scale(const float* row_scale, uint64_t rows, uint64_t tiles, float2* out, cudaStream_t s) {
+    if (tiles == 0) return;
+    tile_scale_kernel<<<static_cast<uint32_t>((tiles * 32 + 255) / 256), 256, 0, s>>>(row_scale, rows, tiles, out);
     count_launch();
 }
 
