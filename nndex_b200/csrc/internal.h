@@ -206,7 +206,8 @@ cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q
 cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float* queries, const uint32_t* ids,
                                     uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
                                     uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
-                                    cudaStream_t stream, bool by_query = false, const uint32_t* live = nullptr);
+                                    cudaStream_t stream, bool by_query = false, const uint32_t* live = nullptr,
+                                    const uint32_t* row_map = nullptr);
 cudaError_t launch_max_reduce(const float* v, uint64_t n, unsigned int* out, cudaStream_t stream);
 // FP8: {min, max} row scale of each 256-row tile (tiles = rows_alloc / 256).
 void launch_tile_scale(const float* row_scale, uint64_t rows, uint64_t tiles, float2* out, cudaStream_t s);

@@ -763,7 +763,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     ix.scan_event_end(s, ev_a);
     if (e != cudaSuccess) return cuda_error(e, "IVF tensor-core scan launch (pass 2)");
     e = launch_rerank_collected(ix.d_base, static_cast<uint32_t>(ix.ds), ix.d_qn, ix.d_ids, nq, ix.d_rows2, ix.d_cnt2,
-                                cap2, k, o_idx, o_sim, o_cnt, ix.d_ok2, s, true, d_m);
+                                cap2, k, o_idx, o_sim, o_cnt, ix.d_ok2, s, true, d_m, v.d_row_map);
     if (e != cudaSuccess) return cuda_error(e, "rerank launch (pass 2)");
     launch_compact_zero_flags(ix.d_ok2, nq, ix.d_tcfail, d_fail, s, d_m);
     // the plan's totals and the pass counts come back with the results

@@ -45,6 +45,9 @@ constexpr uint32_t kBChunk = kN * 128;
 // no per-query state beyond the threshold, and the epilogue, not the MMA, bounds the pass).
 template <int kMode>
 constexpr uint32_t epi_warps() { return kMode == 1 ? 8u : 4u; }
+// Pass 2: rows that pass the cut are staged per epilogue thread and appended to the query's
+// collection kPass2Stage at a time (one atomic per group instead of one per row).
+constexpr uint32_t kPass2Stage = 8;
 template <int kMode>
 constexpr int tc_threads() { return 64 + 32 * static_cast<int>(epi_warps<kMode>()); }
 constexpr uint32_t kTmemCols = 512;   // two 256-column FP32 accumulators
@@ -80,6 +83,7 @@ size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp
     b += stream_a ? static_cast<size_t>(stages) * (kAChunk + kBChunk)
                   : static_cast<size_t>(nchunks) * kAChunk + static_cast<size_t>(stages) * kBChunk;
     b += static_cast<size_t>(kprime) * kM * 8;
+    if (kprime == 0) b += static_cast<size_t>(kPass2Stage) * 8 * 32 * 4;  // pass 2: survivor staging
     b += (2 * stages + 5) * 8 + 16;
     return b;
 }
@@ -170,7 +174,8 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     uint8_t* a_smem = smem;  // resident query slabs (kStreamA: none)
     uint8_t* b_smem = a_smem + (kStreamA ? 0 : static_cast<size_t>(p.nchunks) * kAChunk);
     uint64_t* heap = reinterpret_cast<uint64_t*>(b_smem + static_cast<size_t>(kST) * kStage);
-    uint64_t* full_bar = heap + static_cast<size_t>(p.kprime) * kM;
+    uint32_t* stage2 = reinterpret_cast<uint32_t*>(heap + static_cast<size_t>(p.kprime) * kM);  // pass 2
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(stage2 + (kMode == 1 ? kPass2Stage * 8 * 32 : 0));
     uint64_t* empty_bar = full_bar + kST;
     uint64_t* a_full = empty_bar + kST;
     uint64_t* tfull = a_full + 1;
@@ -347,6 +352,15 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         const uint32_t lrow = quarter * 32 + lane;
         const uint32_t q = kItems ? p.it_lane_qid[q0 + lrow] : q0 + lrow;
         const bool valid_q = kItems ? q != 0xFFFFFFFFu : q < nq_live;
+        // pass 2: this thread's staged rows and its append of them to the query's collection
+        uint32_t* my_stage = stage2 + (ew * 32 + lane) * kPass2Stage;
+        uint32_t staged = 0;
+        auto flush_stage = [&]() {
+            const uint32_t pos = atomicAdd(&p.cand_cnt[q], staged);
+            for (uint32_t i = 0; i < staged; ++i)
+                if (pos + i < p.cap2) p.cand_rows[static_cast<size_t>(q) * p.cap2 + pos + i] = my_stage[i];
+            staged = 0;
+        };
         const float qs = (kFp8 && valid_q) ? p.q_scale[q] : 1.0f;
         const float rq = valid_q ? p.q_resid[q] : 0.0f;
         const float b_mul = 1.0f + rq, b_add = rq + p.eps_acc;
@@ -429,6 +443,14 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
                     mask &= mask - 1;
                     const uint64_t row = tile_row0 + c * 32 + j;
                     if (row >= row_end) continue;
+                    if (kMode == 1) {
+                        // pass 2 keeps every row that passed the cut (the largest bound slack over
+                        // all rows: a superset of the rows whose own bound reaches T); in item mode
+                        // the row is a reordered position, mapped to its row by the rerank
+                        my_stage[staged++] = static_cast<uint32_t>(row);
+                        if (staged == kPass2Stage) flush_stage();
+                        continue;
+                    }
                     float s = pick(v, j);
                     if (kFp8) s = (s * sc[c * 32 + j]) * qs;
                     const float u = fmaf(p.row_resid[row], b_mul, s + b_add);
@@ -457,6 +479,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[buf]);
         }
+        if (kMode == 1 && staged) flush_stage();
         if (kMode == 0 && valid_q) {
             uint64_t* dst = kItems ? p.ws_keys + static_cast<size_t>(p.it_lane_slot[q0 + lrow] + chunk) * p.kprime
                                    : p.ws_keys + (static_cast<size_t>(q) * nranges + range) * p.kprime;
@@ -581,7 +604,8 @@ __global__ void __launch_bounds__(256)
                             const uint32_t* __restrict__ ids, const uint32_t* __restrict__ rows2,
                             const uint32_t* __restrict__ cnt2, uint32_t cap2, uint32_t k, uint64_t* __restrict__ idx_out,
                             float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out,
-                            uint32_t* __restrict__ ok_out, int by_query, const uint32_t* __restrict__ live) {
+                            uint32_t* __restrict__ ok_out, int by_query, const uint32_t* __restrict__ live,
+                            const uint32_t* __restrict__ row_map) {
     extern __shared__ uint64_t keys[];
     __shared__ BlockSelectScratch sel;
     const uint32_t i = blockIdx.x;
@@ -600,7 +624,8 @@ __global__ void __launch_bounds__(256)
     for (uint32_t j0 = 0; j0 < n; j0 += nslots) {
         const uint32_t j = j0 + slot;
         const bool live = j < n;
-        const uint64_t row = live ? rows2[static_cast<size_t>(qrow) * cap2 + j] : 0;
+        const uint32_t pos = live ? rows2[static_cast<size_t>(qrow) * cap2 + j] : 0u;
+        const uint64_t row = row_map && live ? row_map[pos] : pos;
         const float acc = dot_scan_order(base + row * ds, qv, nbox, ch, live);
         if (ch == 0 && live) keys[j] = make_key(acc, static_cast<uint32_t>(row));
     }
@@ -724,7 +749,8 @@ cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q
 cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float* queries, const uint32_t* ids,
                                     uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
                                     uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
-                                    cudaStream_t stream, bool by_query, const uint32_t* live) {
+                                    cudaStream_t stream, bool by_query, const uint32_t* live,
+                                    const uint32_t* row_map) {
     if (m == 0) return cudaSuccess;
     uint32_t p2 = 1;
     while (p2 < cap2) p2 <<= 1;
@@ -733,7 +759,7 @@ cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float*
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     kern<<<m, 256, smem, stream>>>(base, ds, queries, ids, rows2, cnt2, cap2, k, idx_out, sim_out, cnt_out, ok_out,
-                                   by_query ? 1 : 0, live);
+                                   by_query ? 1 : 0, live, row_map);
     count_launch();
     return cudaGetLastError();
 }

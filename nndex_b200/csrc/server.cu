@@ -104,6 +104,11 @@ struct Server {
     ~Server();
 };
 
+// A batch runs at its largest k, and a search's cost grows with k (candidate widths, collections,
+// merges): requests share a batch only within one class of k, so k = 1 and k = 10 requests never
+// pay for a k = 100 neighbour.
+static int k_class(uint64_t k) { return k <= 16 ? 0 : (k <= 128 ? 1 : 2); }
+
 void Server::worker(uint32_t slot) {
     CudaIndex* v = views[slot];
     std::vector<float> qbuf;
@@ -121,10 +126,12 @@ void Server::worker(uint32_t slot) {
             if (queue.empty()) return;  // stopping, and nothing left to run
             approx = queue.front()->approx;
             nprobe = queue.front()->nprobe;
+            const int kclass = k_class(queue.front()->kcap);
             for (auto it = queue.begin(); it != queue.end();) {
                 const Request& r = **it;
                 const uint64_t k2 = std::max(kmax, r.kcap);
-                if (r.approx == approx && r.nprobe == nprobe && nq + r.nq <= opts.max_batch_queries &&
+                if (r.approx == approx && r.nprobe == nprobe && k_class(r.kcap) == kclass &&
+                    nq + r.nq <= opts.max_batch_queries &&
                     batch_bytes(nq + r.nq, k2, approx, nprobe) <= opts.slot_bytes) {
                     nq += r.nq;
                     kmax = k2;
