@@ -129,6 +129,8 @@ typedef struct nndex_cuda_search_stats {
                                        autotuner timed the candidates on it, 2 = from the tuner's
                                        cache                                                     */
     uint32_t tune_candidates;       /* plans the autotuner compared for that shape (0 = none)    */
+    uint64_t pass2_rows;            /* tensor-core paths: rows the second pass collected (summed
+                                       over its queries) and re-scored in FP32                  */
 } nndex_cuda_search_stats;
 
 /* IVF build statistics (approximate mode; zero when the index has no IVF). */

@@ -89,6 +89,7 @@ class SearchStats(C.Structure):
         ("mean_score_error", C.c_double),
         ("tuned", C.c_uint32),
         ("tune_candidates", C.c_uint32),
+        ("pass2_rows", C.c_uint64),
     ]
 
 

@@ -36,6 +36,26 @@ bool take_injected_alloc_failure() {
     return n > 0;
 }
 void inject_alloc_failures(uint32_t n) { g_fail_allocs.store(n, std::memory_order_relaxed); }
+static thread_local cudaStream_t t_scratch_stream = nullptr;
+void set_scratch_stream(cudaStream_t s) { t_scratch_stream = s; }
+cudaStream_t scratch_stream() { return t_scratch_stream; }
+cudaError_t regrow_raw(void** p, size_t bytes) {
+    if (bytes == 0) bytes = 1;
+    cudaStream_t s = t_scratch_stream;
+    if (!s) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        return cudaMalloc(p, bytes);
+    }
+    // never inside a stream capture: the allocation would become a node of a graph that may be
+    // discarded (the caller then runs the batch without a graph)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+        return cudaErrorStreamCaptureUnsupported;
+    if (*p) cudaFreeAsync(*p, s);
+    *p = nullptr;
+    return cudaMallocAsync(p, bytes, s);
+}
 uint64_t alloc_epoch() { return g_alloc_epoch.load(std::memory_order_acquire); }
 void bump_alloc_epoch() { g_alloc_epoch.fetch_add(1, std::memory_order_acq_rel); }
 bool sync_check_enabled() {
@@ -149,16 +169,16 @@ template <class T>
 static int grow_device(T*& p, size_t& cap, size_t n, const char* what) {
     if (n <= cap && p) return NNDEX_OK;
     bump_alloc_epoch();
-    if (p) cudaFree(p);
-    p = nullptr;
     cap = 0;
-    cudaError_t e = take_injected_alloc_failure()
-                        ? cudaErrorMemoryAllocation
-                        : cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
+    void* raw = p;
+    cudaError_t e = take_injected_alloc_failure() ? cudaErrorMemoryAllocation
+                                                  : regrow_raw(&raw, std::max<size_t>(n, 1) * sizeof(T));
+    if (e == cudaErrorMemoryAllocation && raw) cudaFree(raw);  // an injected failure frees it too
     if (e != cudaSuccess) {
         p = nullptr;
         return cuda_error(e, what);
     }
+    p = static_cast<T*>(raw);
     cap = n;
     return NNDEX_OK;
 }
@@ -766,9 +786,19 @@ int CudaIndex::finish_tc(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o_si
         if (tc_sample_stride != before) drop_graphs();  // a captured batch keeps its stride
     }
     stats.fp32_fallback_queries = failed_n;
+    int st;
+    if (m) {
+        // rows collected by pass 2 (the counts of its m queries, after the batch)
+        if ((st = grow_host(h_ok2, cap_hok2, n, "pinned buffer"))) return st;
+        cudaMemcpyAsync(h_ok2, d_cnt2, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        const cudaError_t e0 = cudaStreamSynchronize(s);
+        if (e0 != cudaSuccess) return cuda_error(e0, "search");
+        uint64_t total = 0;
+        for (uint32_t i = 0; i < m; ++i) total += std::min<uint32_t>(h_ok2[i], kSecondPassCap);
+        stats.pass2_rows += total;
+    }
     if (failed_n == 0) return NNDEX_OK;
     // ---- the FP32 scan for queries whose collected set overflowed ----
-    int st;
     if ((st = grow_host(h_ids, cap_hids, n, "pinned buffer"))) return st;
     if ((st = grow_host(h_ok2, cap_hok2, n, "pinned buffer"))) return st;
     cudaMemcpyAsync(h_ids, d_ids, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);

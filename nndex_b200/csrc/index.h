@@ -25,6 +25,15 @@ void bump_alloc_epoch();
 // Host-side fault injection (tests): the next n scratch allocations fail as out of memory.
 void inject_alloc_failures(uint32_t n);
 bool take_injected_alloc_failure();
+// Scratch growth. By default a buffer that must grow is freed with cudaFree (which waits for the
+// whole device) and reallocated with cudaMalloc. A serving slot instead grows its buffers in
+// stream order on its own stream (cudaFreeAsync / cudaMallocAsync), so a slot meeting a larger
+// batch does not wait for the batches the other slots are running; every buffer it grows is then
+// stream-ordered memory from the start (a slot is a fresh view). The stream is per thread.
+void set_scratch_stream(cudaStream_t s);
+cudaStream_t scratch_stream();
+// Frees `p` and allocates `bytes` (0 → 1) into it under the current thread's growth mode.
+cudaError_t regrow_raw(void** p, size_t bytes);
 
 int set_error(int code, const char* fmt, ...);
 int last_encode_result();  // CUresult of this thread's last tensor-map encode

@@ -454,13 +454,16 @@ template <class T>
 int grow(T*& p, size_t& cap, size_t n, const char* what) {
     if (n <= cap && p) return NNDEX_OK;
     bump_alloc_epoch();
-    cudaFree(p);
-    p = nullptr;
     cap = 0;
-    cudaError_t e = take_injected_alloc_failure()
-                        ? cudaErrorMemoryAllocation
-                        : cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
-    if (e != cudaSuccess) return cuda_error(e, what);
+    void* raw = p;
+    cudaError_t e = take_injected_alloc_failure() ? cudaErrorMemoryAllocation
+                                                  : regrow_raw(&raw, std::max<size_t>(n, 1) * sizeof(T));
+    if (e == cudaErrorMemoryAllocation && raw) cudaFree(raw);  // an injected failure frees it too
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return cuda_error(e, what);
+    }
+    p = static_cast<T*>(raw);
     cap = n;
     return NNDEX_OK;
 }
@@ -791,6 +794,20 @@ int ivf_finish_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     ix.stats.certified = m == 0 ? 1u : 0u;
     ix.stats.second_pass_queries = m;
     ix.stats.fp32_fallback_queries = failed_n;
+    int st;
+    if (m) {
+        // rows collected by pass 2 (the counts of the uncertified queries, read after the batch)
+        if ((st = grow_pinned(ix.h_ok2, ix.cap_hok2, nq, "pinned buffer"))) return st;
+        if ((st = grow_pinned(ix.h_ids, ix.cap_hids, nq, "pinned buffer"))) return st;
+        cudaMemcpyAsync(ix.h_ok2, ix.d_cnt2, nq * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(ix.h_ids, ix.d_cert, nq * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        const cudaError_t e0 = cudaStreamSynchronize(s);
+        if (e0 != cudaSuccess) return cuda_error(e0, "IVF search");
+        uint64_t total = 0;
+        for (uint32_t i = 0; i < nq; ++i)
+            if (!ix.h_ids[i]) total += std::min<uint32_t>(ix.h_ok2[i], kSecondPassCap);
+        ix.stats.pass2_rows += total;
+    }
     if (w.tc_stride == 1 && m * 2 > nq) {
         static const uint32_t sampled = [] {
             const char* v = getenv("NNDEX_IVF_TC_STRIDE");  // measurement override of the sampled stride
@@ -802,7 +819,6 @@ int ivf_finish_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     }
     if (failed_n == 0) return NNDEX_OK;
     // ---- FP32 list scan for the queries whose collection overflowed ----
-    int st;
     if ((st = grow_pinned(ix.h_ids, ix.cap_hids, nq, "pinned buffer"))) return st;
     if ((st = grow_pinned(ix.h_ok2, ix.cap_hok2, nq, "pinned buffer"))) return st;
     cudaMemcpyAsync(ix.h_ids, ix.d_ids, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);

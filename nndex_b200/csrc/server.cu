@@ -111,6 +111,7 @@ static int k_class(uint64_t k) { return k <= 16 ? 0 : (k <= 128 ? 1 : 2); }
 
 void Server::worker(uint32_t slot) {
     CudaIndex* v = views[slot];
+    set_scratch_stream(v->stream);  // this slot's buffers grow in stream order (see set_scratch_stream)
     std::vector<float> qbuf;
     std::vector<uint64_t> bidx, bcnt;
     std::vector<float> bsim;
