@@ -68,6 +68,7 @@ bool parse_entry(const char* line, uint64_t* key, CudaIndex::TuneEntry* e) {
         path < 1 || path > 6 || stride > 64 || !(ms >= 0.0))
         return false;
     if (ivf ? (path != 4 && path != 5) : (path == 4 || path == 5)) return false;
+    if (path == 4 && stride) return false;
     f.ivf = ivf;
     f.nq = nq;
     f.k = k;
@@ -164,8 +165,12 @@ std::vector<CudaIndex::TunePlan> CudaIndex::tune_candidates(uint64_t nq, uint64_
         c.push_back({4, 0});
         const TcPlan p1 = plan_tc(kcap, false);
         if (precision != NNDEX_PRECISION_FP32 && nq >= 64 && ivf->d_reordered16 && p1.kp >= kcap && p1.kp > 0 &&
-            plan_tc(0, false).stages > 0)
-            c.push_back({5, 0});
+            plan_tc(0, false).stages > 0) {
+            // the tensor-core list scan with a full pass 1, or on every 4th or 16th tile of its lists
+            c.push_back({5, 1});
+            c.push_back({5, 4});
+            c.push_back({5, 16});
+        }
         return c;
     }
     const bool tf32 = plan_tf32(nq, kcap).kp != 0;

@@ -706,7 +706,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     // Like the exact path's pass 1: when pass 1 rarely certifies, it only has to give each query its
     // threshold T, and every 4th tile of its lists gives a valid one (the rule lives in
     // ivf_finish_tc).
-    const uint32_t stride = w.tc_stride;
+    const uint32_t stride = ix.forced_stride ? ix.forced_stride : w.tc_stride;  // a tuned plan may fix it
     a.p.tile_stride = stride;
     a.p.it_item_off = w.d_item_off;
     a.p.it_list_cnt = w.d_list_cnt;
@@ -808,7 +808,7 @@ int ivf_finish_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
             if (!ix.h_ids[i]) total += std::min<uint32_t>(ix.h_ok2[i], kSecondPassCap);
         ix.stats.pass2_rows += total;
     }
-    if (w.tc_stride == 1 && m * 2 > nq) {
+    if (!ix.forced_stride && w.tc_stride == 1 && m * 2 > nq) {
         static const uint32_t sampled = [] {
             const char* v = getenv("NNDEX_IVF_TC_STRIDE");  // measurement override of the sampled stride
             const uint32_t x = v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
