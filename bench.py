@@ -72,6 +72,8 @@ def parse_args(argv=None):
     p.add_argument("--mixed-oracle-queries", type=int, default=512)
     p.add_argument("--mixed-stride", type=int, default=0,
                    help="fix the tensor-core scans' pass-1 tile stride (installed as the tuner's plan); 0 = tuned")
+    p.add_argument("--mixed-qb", type=int, default=0, choices=[0, 1, 2],
+                   help="fix the tensor-core pass 2's query blocks per CTA (installed as the tuner's plan); 0 = tuned")
     p.add_argument("--ivf", choices=["on", "off", "only"], default="on",
                    help="also measure the IVF workload (GPU k-means build + probe + ragged list scan)")
     p.add_argument("--ivf-rows", type=int, default=2_000_000)
@@ -649,15 +651,16 @@ def run_mixed(args, dev, L, world):
     os_ = torch.empty((nq, k), dtype=torch.float32, device=dev)
     stats = _lib.SearchStats()
     out = {}
-    if args.mixed_stride:
-        # the tuner's cache with the given stride for both tensor-core precisions at this shape
+    if args.mixed_stride or args.mixed_qb:
+        # the tuner's cache with the given stride / blocks for both tensor-core precisions at this shape
         n = C.c_uint64(0)
         L.nndex_cuda_autotune_export(h, None, 0, C.byref(n))
         buf = C.create_string_buffer(n.value)
         L.nndex_cuda_autotune_export(h, buf, n.value, C.byref(n))
         nqb, kb = 1 << (nq - 1).bit_length(), 1 << (k - 1).bit_length()
         text = buf.value.decode() + "".join(
-            f"shape ivf=0 nq={nqb} k={kb} precision={p} nprobe=0 plan path={p} stride={args.mixed_stride} ms=0\n"
+            f"shape ivf=0 nq={nqb} k={kb} precision={p} nprobe=0 plan path={p} stride={args.mixed_stride} "
+            f"qb={args.mixed_qb} ms=0\n"
             for p in (2, 3))
         if L.nndex_cuda_autotune_import(h, text.encode()) != 0:
             raise RuntimeError(_lib.last_error())
@@ -679,6 +682,7 @@ def run_mixed(args, dev, L, world):
         second = 0
         fallbacks = 0
         flops = 0.0
+        p2rows = 0
         for _ in range(steps):
             if L.nndex_cuda_search_batch_device(h, q.data_ptr(), nq, dims, k, oi.data_ptr(), os_.data_ptr(), None,
                                                 sptr, 1) != 0:
@@ -687,6 +691,7 @@ def run_mixed(args, dev, L, world):
             if stats.path in (2, 3):
                 second += stats.second_pass_queries
                 fallbacks += stats.fp32_fallback_queries
+                p2rows += stats.pass2_rows
                 # tensor-core FLOPs executed: pass 1 over 1/stride of the rows, pass 2 over all rows
                 flops += 2.0 * rows * dims * (nq / max(stats.pass1_tile_stride, 1) + stats.second_pass_queries)
             else:
@@ -719,6 +724,8 @@ def run_mixed(args, dev, L, world):
             "algorithmic_tflops": 2.0 * rows * dims * nq / (max_ms / steps / 1e3) / 1e12,
             "rerank_width": int(stats.rerank_width),
             "second_pass_queries_per_batch": second / steps,
+            "pass2_rows_per_query": p2rows / second if second else 0.0,
+            "pass2_query_blocks": int(stats.pass2_query_blocks),
             "fp32_fallback_queries_per_batch": fallbacks / steps,
             "kernel_launches_per_batch": (n1 - n0) / steps,
         }
@@ -849,6 +856,7 @@ def run_ivf(args, dev, L, world):
         per[name] = {
             "path": "tensor-core list scan" if stats.path == 5 else "FP32 list scan",
             "second_pass_queries": stats.second_pass_queries,
+            "pass2_rows_per_query": stats.pass2_rows / stats.second_pass_queries if stats.second_pass_queries else 0.0,
             "fp32_fallback_queries": stats.fp32_fallback_queries,
             "queries_per_s": total_q / (max_ms / 1e3),
             "ms_per_batch": max_ms / args.ivf_steps,

@@ -131,6 +131,9 @@ typedef struct nndex_cuda_search_stats {
     uint32_t tune_candidates;       /* plans the autotuner compared for that shape (0 = none)    */
     uint64_t pass2_rows;            /* tensor-core paths: rows the second pass collected (summed
                                        over its queries) and re-scored in FP32                  */
+    uint32_t pass2_query_blocks;    /* paths 2/3: 128-query blocks per CTA of the second pass
+                                       (2 = two blocks against 128-row base tiles; 0 = no pass) */
+    uint32_t reserved0;
 } nndex_cuda_search_stats;
 
 /* IVF build statistics (approximate mode; zero when the index has no IVF). */

@@ -90,6 +90,8 @@ class SearchStats(C.Structure):
         ("tuned", C.c_uint32),
         ("tune_candidates", C.c_uint32),
         ("pass2_rows", C.c_uint64),
+        ("pass2_query_blocks", C.c_uint32),
+        ("reserved0", C.c_uint32),
     ]
 
 

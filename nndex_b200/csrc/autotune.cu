@@ -29,7 +29,7 @@ uint32_t ceil_log2(uint64_t v) {
     while ((1ull << l) < v) ++l;
     return l;
 }
-constexpr const char* kHeader = "nndex-autotune v1";
+constexpr const char* kHeader = "nndex-autotune v2";
 
 // One shape of the key, as its fields.
 struct ShapeFields {
@@ -60,15 +60,17 @@ bool parse_entry(const char* line, uint64_t* key, CudaIndex::TuneEntry* e) {
     ShapeFields f;
     unsigned long long nq = 0, k = 0;
     int path = 0;
-    unsigned stride = 0, ivf = 0, prec = 0, nprobe = 0;
+    unsigned stride = 0, qb = 0, ivf = 0, prec = 0, nprobe = 0;
     double ms = 0.0;
-    int n = std::sscanf(line, "shape ivf=%u nq=%llu k=%llu precision=%u nprobe=%u plan path=%d stride=%u ms=%lf",
-                        &ivf, &nq, &k, &prec, &nprobe, &path, &stride, &ms);
-    if (n != 8 || ivf > 1 || !is_pow2(nq) || nq > kMaxBatchChunk || !is_pow2(k) || k > (1ull << 20) || prec > 3 ||
-        path < 1 || path > 6 || stride > 64 || !(ms >= 0.0))
+    int n = std::sscanf(line,
+                        "shape ivf=%u nq=%llu k=%llu precision=%u nprobe=%u plan path=%d stride=%u qb=%u ms=%lf",
+                        &ivf, &nq, &k, &prec, &nprobe, &path, &stride, &qb, &ms);
+    if (n != 9 || ivf > 1 || !is_pow2(nq) || nq > kMaxBatchChunk || !is_pow2(k) || k > (1ull << 20) || prec > 3 ||
+        path < 1 || path > 6 || stride > 64 || qb > 2 || !(ms >= 0.0))
         return false;
     if (ivf ? (path != 4 && path != 5) : (path == 4 || path == 5)) return false;
     if (path == 4 && stride) return false;
+    if (qb && path != 2 && path != 3) return false;  // only the exact tensor-core pass 2 has two blocks
     f.ivf = ivf;
     f.nq = nq;
     f.k = k;
@@ -77,6 +79,7 @@ bool parse_entry(const char* line, uint64_t* key, CudaIndex::TuneEntry* e) {
     *key = pack_key(f);
     e->plan.path = path;
     e->plan.stride = stride;
+    e->plan.qb = qb;
     e->ms = ms;
     return true;
 }
@@ -155,10 +158,16 @@ std::vector<CudaIndex::TunePlan> CudaIndex::tune_candidates(uint64_t nq, uint64_
         return p1.kp >= kcap && p1.kp > 0 && plan_tc(0, fp8).stages > 0;
     };
     auto add_tc = [&](int path) {
-        c.push_back({path, 1});
-        if (rows >= 256ull * 64) {  // sampled pass 1 (every 8th or 32nd tile) on large bases
-            c.push_back({path, 8});
-            c.push_back({path, 32});
+        // pass 2 with one or two query blocks per CTA, where a batch has two blocks and they fit
+        const bool pair = nq > 128 && tc_pair_stages_for(tc_chunks(path == 3), path == 3, smem_optin) > 0;
+        for (uint32_t stride : {1u, 8u, 32u}) {
+            if (stride > 1 && rows < 256ull * 64) break;  // sampled pass 1 (every 8th or 32nd tile) on large bases
+            if (pair) {
+                c.push_back({path, stride, 1});
+                c.push_back({path, stride, 2});
+            } else {
+                c.push_back({path, stride, 0});
+            }
         }
     };
     if (uses_ivf()) {
@@ -237,9 +246,9 @@ int nndex_cuda_autotune_export(nndex_cuda_index* index, char* buf, uint64_t capa
         const ShapeFields f = unpack_key(kv.first);
         char line[256];
         std::snprintf(line, sizeof(line),
-                      "shape ivf=%u nq=%llu k=%llu precision=%u nprobe=%u plan path=%d stride=%u ms=%.6f\n", f.ivf,
-                      (unsigned long long)f.nq, (unsigned long long)f.k, f.precision, f.nprobe, kv.second.plan.path,
-                      kv.second.plan.stride, kv.second.ms);
+                      "shape ivf=%u nq=%llu k=%llu precision=%u nprobe=%u plan path=%d stride=%u qb=%u ms=%.6f\n",
+                      f.ivf, (unsigned long long)f.nq, (unsigned long long)f.k, f.precision, f.nprobe,
+                      kv.second.plan.path, kv.second.plan.stride, kv.second.plan.qb, kv.second.ms);
         out += line;
     }
     *len = out.size() + 1;

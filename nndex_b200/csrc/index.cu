@@ -747,6 +747,19 @@ int CudaIndex::enqueue_tc_pass2(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o
     const TcPlan plan2 = plan_tc(0, fp8);
     a.stages = plan2.stages;
     a.stream_a = plan2.stream_a;
+    // Two query blocks per CTA (where both fit beside a ring: D ≤ 256 in BF16, 512 in FP8) read half
+    // the base bytes per FLOP but run M = 128, N = 128 MMAs, which read as many query bytes from
+    // shared memory as base bytes. On 10M × 256 at 4,096 queries that made FP8 7 % faster and BF16
+    // 7 % slower, so the rule takes it for FP8 and the autotuner times both.
+    const uint32_t want_qb = forced_qb ? forced_qb : (fp8 ? 2u : 1u);
+    const uint32_t pair_stages = (want_qb == 2 && n > 128) ? tc_pair_stages_for(tc_chunks(fp8), fp8, smem_optin) : 0;
+    if (pair_stages) {
+        a.qb = 2;
+        a.stages = pair_stages;
+        a.stream_a = false;
+        a.tmap_b = fp8 ? &tmap_fp8_h : &tmap_bf16_h;
+    }
+    stats.pass2_query_blocks = a.qb;
     fill_tc_params(fp8, n, 0, a.p);
     a.p.q_resid = d_q2_resid;
     a.p.q_scale = fp8 ? d_q2_scale : nullptr;
@@ -763,8 +776,8 @@ int CudaIndex::enqueue_tc_pass2(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o
     e = launch_scan_tc(a, fp8, 1, s);
     scan_event_end(s, ev_a);
     if (e != cudaSuccess) return cuda_error(e, "tensor-core scan launch (pass 2)");
-    e = launch_rerank_collected(d_base, static_cast<uint32_t>(ds), d_qn, d_ids, n, d_rows2, d_cnt2, cap2, kcap, o_idx,
-                                o_sim, o_cnt, d_ok2, s, false, d_m);
+    e = launch_rerank_collected(d_base, static_cast<uint32_t>(ds), d_qn, d_ids, n, d_rows2, d_cnt2, cap2, kcap,
+                                d_q2_thr, o_idx, o_sim, o_cnt, d_ok2, s, false, d_m);
     if (e != cudaSuccess) return cuda_error(e, "rerank launch (pass 2)");
     launch_compact_zero_flags(d_ok2, n, d_tcfail, d_fail, s, d_m);
     stats.kernel_launches += 5;
@@ -986,6 +999,7 @@ int CudaIndex::tune_host(uint64_t n, uint64_t kcap, int mode, TunePlan* plan) {
         int cst = NNDEX_OK;
         for (int rep = 0; rep < 2 && cst == NNDEX_OK; ++rep) {
             forced_stride = cands[c].stride;
+            forced_qb = cands[c].qb;
             const auto t0 = std::chrono::steady_clock::now();
             cst = enqueue_host_batch(n, kcap, mode, cands[c].path);
             const cudaError_t e = cudaStreamSynchronize(stream);
@@ -999,6 +1013,7 @@ int CudaIndex::tune_host(uint64_t n, uint64_t kcap, int mode, TunePlan* plan) {
             ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         }
         forced_stride = 0;
+        forced_qb = 0;
         if (cst != NNDEX_OK) {
             last_err = cst;
             continue;
@@ -1183,8 +1198,10 @@ int CudaIndex::search_host(const float* queries, uint64_t nq, uint64_t k, int mo
         const int path = plan.path;
         serr_off = q0;
         forced_stride = plan.stride;
+        forced_qb = plan.qb;
         st = run_host_batch(n, kcap, mode, path);
         forced_stride = 0;
+        forced_qb = 0;
         if (st) return st;
         cudaEventRecord(ev1, stream);  // before the wait: the device time ends with the last batch
         cudaError_t e = cudaStreamSynchronize(stream);
@@ -1290,6 +1307,7 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
                 int cst = NNDEX_OK;
                 for (int rep = 0; rep < 2 && cst == NNDEX_OK; ++rep) {
                     forced_stride = cands[c].stride;
+                    forced_qb = cands[c].qb;
                     bool sy = false;
                     const auto t0 = std::chrono::steady_clock::now();
                     cst = run_device_chunk(dq, n, kcap, cands[c].path, oi, os, oc, s, &sy);
@@ -1298,6 +1316,7 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
                     ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
                 }
                 forced_stride = 0;
+                forced_qb = 0;
                 if (cst != NNDEX_OK) {
                     last_err = cst;
                     continue;
@@ -1327,8 +1346,10 @@ int CudaIndex::search_device(const float* d_queries, uint64_t nq, uint64_t k, ui
             }
         }
         forced_stride = plan.stride;
+        forced_qb = plan.qb;
         st = run_device_chunk(dq, n, kcap, plan.path, oi, os, oc, s, &synced);
         forced_stride = 0;
+        forced_qb = 0;
         if (st) return st;
         if (error_report) {
             serr_off = q0;
@@ -1566,12 +1587,16 @@ int index_finish(CudaIndex* ix) {
                         ix->ds * sizeof(float), 32, 112, CU_TENSOR_MAP_SWIZZLE_128B))
         return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed"));
     if (ix->d_base_bf16 &&
-        !encode_tmap_2d(&ix->tmap_bf16, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ix->d_base_bf16, ix->kb16, ix->rows_alloc,
-                        ix->kb16 * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B))
+        (!encode_tmap_2d(&ix->tmap_bf16, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ix->d_base_bf16, ix->kb16,
+                         ix->rows_alloc, ix->kb16 * 2, 64, 256, CU_TENSOR_MAP_SWIZZLE_128B) ||
+         !encode_tmap_2d(&ix->tmap_bf16_h, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ix->d_base_bf16, ix->kb16,
+                         ix->rows_alloc, ix->kb16 * 2, 64, 128, CU_TENSOR_MAP_SWIZZLE_128B)))
         return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (BF16)"));
     if (ix->d_base_fp8 &&
-        !encode_tmap_2d(&ix->tmap_fp8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ix->d_base_fp8, ix->kf8, ix->rows_alloc,
-                        ix->kf8, 128, 256, CU_TENSOR_MAP_SWIZZLE_128B))
+        (!encode_tmap_2d(&ix->tmap_fp8, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ix->d_base_fp8, ix->kf8, ix->rows_alloc,
+                         ix->kf8, 128, 256, CU_TENSOR_MAP_SWIZZLE_128B) ||
+         !encode_tmap_2d(&ix->tmap_fp8_h, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ix->d_base_fp8, ix->kf8, ix->rows_alloc,
+                         ix->kf8, 128, 128, CU_TENSOR_MAP_SWIZZLE_128B)))
         return fail(set_error(NNDEX_ERR_CUDA, "cuda execution error: cuTensorMapEncodeTiled failed (FP8)"));
     if (ix->d_row_scale) {
         // FP8 scan: the scale extremes of each 256-row tile (its epilogue's per-tile cut)
@@ -1692,6 +1717,8 @@ int make_view(const CudaIndex& src, CudaIndex** out) {
     v->d_tfnorm = src.d_tfnorm;
     v->tmap_bf16 = src.tmap_bf16;
     v->tmap_fp8 = src.tmap_fp8;
+    v->tmap_bf16_h = src.tmap_bf16_h;
+    v->tmap_fp8_h = src.tmap_fp8_h;
     v->rerank_width = src.rerank_width;
     v->tc_sample_stride = src.tc_sample_stride;
     // a view (a serving slot) never stops a batch to time plans: the source's measured plans, else

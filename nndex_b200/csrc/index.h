@@ -81,6 +81,7 @@ struct CudaIndex {
     float* d_res16 = nullptr;                  // rows: ‖x − x̂‖ of the BF16 copy
     float* d_res8 = nullptr;                   // rows: ‖x − x̂‖ of the FP8 copy
     CUtensorMap tmap_bf16{}, tmap_fp8{};
+    CUtensorMap tmap_bf16_h{}, tmap_fp8_h{};   // the same with 128-row boxes (two-block pass 2)
     // per-search buffers of the tensor-core path
     __nv_bfloat16* d_q_bf16 = nullptr;
     size_t cap_q_bf16 = 0;
@@ -114,6 +115,7 @@ struct CudaIndex {
     uint32_t last_tc_n = 0;  // queries of the last tensor-core batch (diagnostics)
     uint32_t tc_sample_stride = 1;  // pass-1 tile stride by the certification rule (1 = full pass 1)
     uint32_t forced_stride = 0;     // the tuned plan's pass-1 tile stride for the current batch (0 = rule)
+    uint32_t forced_qb = 0;         // the tuned plan's pass-2 query blocks per CTA (0 = rule)
     uint32_t last_tc_stride = 1;
     float* d_kth = nullptr;  // pass 1: exact k-th score per query
     size_t cap_kth = 0;
@@ -267,6 +269,7 @@ struct CudaIndex {
     struct TunePlan {
         int path = 0;
         uint32_t stride = 0;  // 0 = the certification rule
+        uint32_t qb = 0;      // tensor-core pass 2: query blocks per CTA (1 or 2; 0 = the rule)
     };
     struct TuneEntry {
         TunePlan plan;

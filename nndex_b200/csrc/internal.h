@@ -135,16 +135,21 @@ struct TcParams {
 struct TcArgs {
     const CUtensorMap* tmap_q = nullptr;  // quantised queries [nq_alloc × K], box {128 B, 128 rows}
     const CUtensorMap* tmap_b = nullptr;  // quantised base [rows_alloc × K], box {128 B, 256 rows}
+                                          // (qb = 2: box {128 B, 128 rows})
     TcParams p;
     uint32_t nranges = 0;
     uint32_t stages = 4;                  // base ring depth (2..4)
     bool stream_a = false;                // pass 1: query slabs staged per ring stage, not resident
     uint32_t items = 0;                   // IVF item mode: number of work items (grid), 0 = off
     uint32_t live_items = 0;              // pass 2 with p.live_q: CTAs launched (an upper bound)
+    uint32_t qb = 1;                      // pass 2: query blocks per CTA (2: 128-row base tiles)
 };
-size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8, bool stream_a);
+size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8, bool stream_a, uint32_t qb = 1);
 // Deepest base ring (4, 3 or 2 stages) that fits k′ heaps in `smem_limit`; 0 if none fits.
 uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, bool stream_a, size_t smem_limit);
+// Pass 2 with two resident query blocks per CTA: the deepest ring (5 or 4 stages of 128-row slabs)
+// that fits beside both blocks' query slabs; 0 if none (large D).
+uint32_t tc_pair_stages_for(uint32_t nchunks, bool fp8, size_t smem_limit);
 cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t stream);
 
 // K12: FP32-accurate candidate scan on the tensor cores (three TF32 products per K step), 16
@@ -203,11 +208,13 @@ cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream);
 cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q_lp, uint32_t row_bytes, void* q2_lp,
                                   const float* resid, float* resid2, const float* scale, float* scale2,
                                   const float* kth, float* thr2, cudaStream_t stream, const uint32_t* live = nullptr);
-cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float* queries, const uint32_t* ids,
+// Pass 2's exact rerank. thr: each query's T (indexed like cnt2). vecs: the base by row, or with
+// row_map (IVF) the list-ordered copy by collected position.
+cudaError_t launch_rerank_collected(const float* vecs, uint32_t ds, const float* queries, const uint32_t* ids,
                                     uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
-                                    uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
-                                    cudaStream_t stream, bool by_query = false, const uint32_t* live = nullptr,
-                                    const uint32_t* row_map = nullptr);
+                                    const float* thr, uint64_t* idx_out, float* sim_out, uint32_t* cnt_out,
+                                    uint32_t* ok_out, cudaStream_t stream, bool by_query = false,
+                                    const uint32_t* live = nullptr, const uint32_t* row_map = nullptr);
 cudaError_t launch_max_reduce(const float* v, uint64_t n, unsigned int* out, cudaStream_t stream);
 // FP8: {min, max} row scale of each 256-row tile (tiles = rows_alloc / 256).
 void launch_tile_scale(const float* row_scale, uint64_t rows, uint64_t tiles, float2* out, cudaStream_t s);

@@ -1,12 +1,13 @@
 // ivf_search.cu — K8/K9: IVF probe and the ragged list scan with exact FP32 rerank.
 //
 // Replaces candidate_clusters(_batch) (src/approx.rs:159-300) and search_approx /
-// search_batch_approx (src/cpu.rs:425-502). A batch runs as four launches and no host round trip:
+// search_batch_approx (src/cpu.rs:425-502). A batch runs as five launches and no host round trip:
 //   1. probe: per query, dot_small against every centroid (FP64 in index order, f32 result — the
-//      reference's value) and the nprobe best clusters (score desc, lower index on ties).
-//   2. plan (one block): the (list, query) pairs grouped by list, each list cut into chunks of at
-//      most kChunkRows rows, and work items (list chunk × group of up to QB queries probing it),
-//      with every (query, list chunk) owning one output slot of k keys.
+//      reference's value) and the nprobe best clusters (score desc, lower index on ties); up to 8
+//      queries per block share each read of the centroids.
+//   2. plan (a one-block scan, then one warp per query): the (list, query) pairs grouped by list,
+//      each list cut into chunks of at most kChunkRows rows, and work items (list chunk × group of up
+//      to QB queries probing it), with every (query, list chunk) owning one output slot of k keys.
 //   3. scan: persistent CTAs take work items from a global counter. A list chunk streams through
 //      shared memory by TMA once per item while up to QB queries are scored against it with the
 //      FP32 scan's exact FMA order (so an IVF score is bit-identical to the exact path's score of
@@ -63,80 +64,161 @@ NNDEX_DEVICE_INLINE void block_exclusive_scan(uint32_t* v, uint32_t n, uint32_t*
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
-// 1. Probe: one block per query.
+// 1. Probe: QB queries per block of 8 warps (QB ≤ 8, as many as shared memory holds), so the
+//    centroid matrix is read from L2 once per QB queries. A thread scores its centroids against
+//    all QB queries (FP64 FMA in index order, the queries held as doubles in shared memory); warp j
+//    then selects query j's nprobe best lists (a radix select over its keys), writes them, and
+//    counts them into the plan: queries per list, and the query's output slots (one per chunk of a
+//    probed list) and probed rows.
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
-    ivf_probe_kernel(const float* __restrict__ queries, uint32_t ds, uint32_t dp, const float* __restrict__ cent_t,
-                     uint64_t ct_stride, uint32_t nlist, uint32_t np, uint32_t* __restrict__ probes) {
-    extern __shared__ uint8_t smem_raw[];
-    float* qs = reinterpret_cast<float*>(smem_raw);
-    uint64_t* keys = reinterpret_cast<uint64_t*>(qs + ds);
-    __shared__ BlockSelectScratch sel;
-    const uint32_t q = blockIdx.x;
-    for (uint32_t d = threadIdx.x; d < ds; d += blockDim.x) qs[d] = queries[static_cast<uint64_t>(q) * ds + d];
-    __syncthreads();
-    for (uint32_t c = threadIdx.x; c < nlist; c += blockDim.x) {
-        double s = 0.0;
-        for (uint32_t d = 0; d < dp; ++d)
-            s = fma(static_cast<double>(cent_t[static_cast<uint64_t>(d) * ct_stride + c]), static_cast<double>(qs[d]), s);
-        keys[c] = make_key(fold_zero(__double2float_rn(s)), c);
+// The k-th largest of n distinct keys, by one warp (8 passes of 8 bits; `hist` 256 words of the
+// warp's own).
+NNDEX_DEVICE_INLINE uint64_t warp_radix_kth(const uint64_t* keys, uint32_t n, uint32_t k, uint32_t* hist,
+                                            uint32_t lane) {
+    uint64_t prefix = 0, mask = 0;
+    uint32_t krem = k;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (uint32_t i = lane; i < 256; i += 32) hist[i] = 0;
+        __syncwarp();
+        for (uint32_t i = lane; i < n; i += 32) {
+            const uint64_t key = keys[i];
+            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+        }
+        __syncwarp();
+        // lane L owns bins 255 − 8L down to 248 − 8L: counts above a bin accumulate from lane 0
+        uint32_t c[8], local = 0;
+#pragma unroll
+        for (uint32_t b = 0; b < 8; ++b) {
+            c[b] = hist[255u - (lane * 8u + b)];
+            local += c[b];
+        }
+        uint32_t incl = local;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += x;
+        }
+        const uint32_t excl = incl - local;
+        const uint32_t owner = __ffs(__ballot_sync(0xFFFFFFFFu, excl < krem && krem <= incl)) - 1;
+        uint32_t bin = 0, above = excl;
+        if (lane == owner) {
+#pragma unroll
+            for (uint32_t b = 0; b < 8; ++b) {
+                if (above + c[b] >= krem) {
+                    bin = 255u - (lane * 8u + b);
+                    break;
+                }
+                above += c[b];
+            }
+        }
+        bin = __shfl_sync(0xFFFFFFFFu, bin, owner);
+        above = __shfl_sync(0xFFFFFFFFu, above, owner);
+        prefix |= static_cast<uint64_t>(bin) << shift;
+        mask |= 0xFFull << shift;
+        krem -= above;
+        __syncwarp();
+    }
+    return prefix;
+}
+
+constexpr uint32_t kProbeThreads = 256;
+
+size_t probe_smem(uint32_t qb, uint64_t dp, uint64_t nlist) {
+    return static_cast<size_t>(qb) * (dp * 8 + nlist * 8 + 256 * 4);
+}
+
+template <int QB>
+__global__ void __launch_bounds__(kProbeThreads)
+    ivf_probe_kernel(const float* __restrict__ queries, uint32_t nq, uint32_t ds, uint32_t dp,
+                     const float* __restrict__ cent_t, uint64_t ct_stride, uint32_t nlist, uint32_t np,
+                     const uint32_t* __restrict__ offsets, uint32_t* __restrict__ probes,
+                     uint32_t* __restrict__ list_cnt, uint32_t* __restrict__ q_slot_off,
+                     unsigned long long* __restrict__ counters) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    double* qd = reinterpret_cast<double*>(smem_raw);                 // [dp][QB]
+    uint64_t* keys = reinterpret_cast<uint64_t*>(qd + static_cast<size_t>(dp) * QB);  // [QB][nlist]
+    uint32_t* hist = reinterpret_cast<uint32_t*>(keys + static_cast<size_t>(QB) * nlist);  // [QB][256]
+    const uint32_t q0 = blockIdx.x * QB;
+    const uint32_t nb = (nq - q0) < QB ? (nq - q0) : QB;
+    for (uint32_t i = threadIdx.x; i < dp * QB; i += blockDim.x) {
+        const uint32_t d = i / QB, j = i % QB;
+        qd[i] = j < nb ? static_cast<double>(queries[static_cast<uint64_t>(q0 + j) * ds + d]) : 0.0;
     }
     __syncthreads();
-    uint64_t kth = 0;
-    if (np < nlist) kth = block_radix_kth(keys, nlist, np, sel);
-    if (threadIdx.x == 0) sel.count = 0;
-    __syncthreads();
     for (uint32_t c = threadIdx.x; c < nlist; c += blockDim.x) {
-        const uint64_t key = keys[c];
-        if (key >= kth) {
-            const uint32_t pos = atomicAdd(&sel.count, 1u);
-            if (pos < np) probes[static_cast<uint64_t>(q) * np + pos] = key_row(key);
+        double acc[QB];
+#pragma unroll
+        for (int j = 0; j < QB; ++j) acc[j] = 0.0;
+        const float* col = cent_t + c;
+#pragma unroll 4
+        for (uint32_t d = 0; d < dp; ++d) {
+            const double cv = static_cast<double>(__ldg(col + static_cast<uint64_t>(d) * ct_stride));
+            const double* qv = qd + static_cast<size_t>(d) * QB;
+#pragma unroll
+            for (int j = 0; j < QB; ++j) acc[j] = fma(cv, qv[j], acc[j]);
         }
+#pragma unroll
+        for (int j = 0; j < QB; ++j) keys[static_cast<size_t>(j) * nlist + c] = make_key(fold_zero(__double2float_rn(acc[j])), c);
+    }
+    __syncthreads();
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    if (warp >= nb) return;
+    const uint32_t q = q0 + warp;
+    const uint64_t* kq = keys + static_cast<size_t>(warp) * nlist;
+    const uint64_t kth = np < nlist ? warp_radix_kth(kq, nlist, np, hist + warp * 256u, lane) : 0ull;
+    uint32_t base = 0, slots = 0;
+    unsigned long long rows = 0;
+    for (uint32_t c0 = 0; c0 < nlist; c0 += 32) {
+        const uint32_t c = c0 + lane;
+        const bool take = c < nlist && kq[c] >= kth;
+        const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, take);
+        if (take) {
+            const uint32_t pos = base + __popc(ballot & ((1u << lane) - 1u));
+            if (pos < np) {
+                probes[static_cast<uint64_t>(q) * np + pos] = c;
+                atomicAdd(&list_cnt[c], 1u);
+                const uint32_t len = offsets[c + 1] - offsets[c];
+                slots += (len + kChunkRows - 1) / kChunkRows;
+                rows += len;
+            }
+        }
+        base += __popc(ballot);
+    }
+#pragma unroll
+    for (uint32_t o = 16; o > 0; o >>= 1) {
+        slots += __shfl_xor_sync(0xFFFFFFFFu, slots, o);
+        rows += __shfl_xor_sync(0xFFFFFFFFu, rows, o);
+    }
+    if (lane == 0) {
+        q_slot_off[q] = slots;
+        atomicAdd(&counters[3], rows);  // zeroed once per search: Σ over sub-batches
     }
 }
 
 // ------------------------------------------------------------------------------------------
-// 2. Plan: one block.
+// 2. Plan, from the probe's counts. (a) One block: per list its work items (chunks × groups of qb
+//    queries) and gathered query blocks, and the exclusive scans that place each list's queries,
+//    items and blocks and each query's slots. (b) One warp per query: its (list, query) pairs
+//    written into their lists, each with the query's slot of the list's first chunk.
 //    counters[0] work-item counter (the scan's), [1] items, [2] slots; summed over the sub-batches of
 //    a search: [3] Σ rows probed per query, [4] rows streamed by the scan, [5] rows of probed lists;
 //    [6] gathered query blocks (qblock_off given: the tensor-core scan's groups of qb queries).
 //    Groups of a list are consecutive blocks from qblock_off[l].
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024)
-    ivf_plan_kernel(const uint32_t* __restrict__ probes, uint32_t nq, uint32_t np, uint32_t nlist,
-                    const uint32_t* __restrict__ offsets, uint32_t qb, uint32_t* __restrict__ list_cnt,
-                    uint32_t* __restrict__ list_fill, uint32_t* __restrict__ list_qoff, uint32_t* __restrict__ item_off,
-                    uint32_t* __restrict__ list_q, uint32_t* __restrict__ list_slot, uint32_t* __restrict__ q_slot_off,
-                    unsigned long long* __restrict__ counters, uint32_t* __restrict__ qblock_off) {
+    ivf_plan_scan_kernel(uint32_t nq, uint32_t nlist, const uint32_t* __restrict__ offsets, uint32_t qb,
+                         const uint32_t* __restrict__ list_cnt, uint32_t* __restrict__ list_qoff,
+                         uint32_t* __restrict__ item_off, uint32_t* __restrict__ q_slot_off,
+                         unsigned long long* __restrict__ counters, uint32_t* __restrict__ qblock_off) {
     __shared__ uint32_t part[1024];
-    __shared__ unsigned long long probed;
-    if (threadIdx.x == 0) probed = 0;
-    __syncthreads();
-    auto chunks = [&](uint32_t l) {
-        const uint32_t len = offsets[l + 1] - offsets[l];
-        return (len + kChunkRows - 1) / kChunkRows;
-    };
-    unsigned long long my_rows = 0;
-    for (uint32_t q = threadIdx.x; q < nq; q += blockDim.x) {
-        uint32_t slots = 0;
-        for (uint32_t j = 0; j < np; ++j) {
-            const uint32_t l = probes[static_cast<uint64_t>(q) * np + j];
-            atomicAdd(&list_cnt[l], 1u);
-            slots += chunks(l);
-            my_rows += offsets[l + 1] - offsets[l];
-        }
-        q_slot_off[q] = slots;
-    }
-    atomicAdd(&probed, my_rows);
-    __syncthreads();
     unsigned long long my_stream = 0, my_union = 0;
     for (uint32_t l = threadIdx.x; l < nlist; l += blockDim.x) {
         const uint32_t c = list_cnt[l];
         const uint32_t groups = (c + qb - 1) / qb;
-        item_off[l] = chunks(l) * groups;
+        const uint32_t len = offsets[l + 1] - offsets[l];
+        item_off[l] = (len + kChunkRows - 1) / kChunkRows * groups;
         list_qoff[l] = c;
         if (qblock_off) qblock_off[l] = groups;
-        const uint32_t len = offsets[l + 1] - offsets[l];
         my_stream += static_cast<unsigned long long>(len) * groups;
         my_union += c ? len : 0u;
     }
@@ -147,22 +229,40 @@ __global__ void __launch_bounds__(1024)
     block_exclusive_scan(item_off, nlist, part);
     block_exclusive_scan(q_slot_off, nq, part);
     if (qblock_off) block_exclusive_scan(qblock_off, nlist, part);
-    for (uint32_t q = threadIdx.x; q < nq; q += blockDim.x) {
-        uint32_t rel = q_slot_off[q];
-        for (uint32_t j = 0; j < np; ++j) {
-            const uint32_t l = probes[static_cast<uint64_t>(q) * np + j];
-            const uint32_t pos = list_qoff[l] + atomicAdd(&list_fill[l], 1u);
-            list_q[pos] = q;
-            list_slot[pos] = rel;
-            rel += chunks(l);
-        }
-    }
     if (threadIdx.x == 0) {
         counters[0] = 0;
         counters[1] = item_off[nlist];
         counters[2] = q_slot_off[nq];
-        counters[3] += probed;  // zeroed once per search: Σ over sub-batches
         if (qblock_off) counters[6] = qblock_off[nlist];
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    ivf_plan_fill_kernel(const uint32_t* __restrict__ probes, uint32_t nq, uint32_t np,
+                         const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ list_qoff,
+                         uint32_t* __restrict__ list_fill, const uint32_t* __restrict__ q_slot_off,
+                         uint32_t* __restrict__ list_q, uint32_t* __restrict__ list_slot) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (q >= nq) return;
+    uint32_t run = q_slot_off[q];  // the query's slots, its probed lists' chunks in probe order
+    for (uint32_t j0 = 0; j0 < np; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        const bool on = j < np;
+        const uint32_t l = on ? probes[static_cast<uint64_t>(q) * np + j] : 0u;
+        const uint32_t c = on ? (offsets[l + 1] - offsets[l] + kChunkRows - 1) / kChunkRows : 0u;
+        uint32_t incl = c;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += x;
+        }
+        if (on) {
+            const uint32_t pos = list_qoff[l] + atomicAdd(&list_fill[l], 1u);
+            list_q[pos] = q;
+            list_slot[pos] = run + incl - c;
+        }
+        run += __shfl_sync(0xFFFFFFFFu, incl, 31);
     }
 }
 
@@ -493,6 +593,58 @@ cudaError_t launch_scan(const CUtensorMap& tmap, const IvfScanArgs& a, uint32_t 
     return cudaGetLastError();
 }
 
+// Queries per probe block: the most (8, 4, 2 or 1) whose queries, keys and histograms fit in
+// shared memory; 0 if not even one query's do.
+uint32_t probe_qb(uint64_t dp, uint64_t nlist, size_t smem_optin) {
+    for (uint32_t qb = 8; qb >= 1; qb >>= 1)
+        if (probe_smem(qb, dp, nlist) <= smem_optin) return qb;
+    return 0;
+}
+
+struct ProbeLaunch {
+    const float* queries;
+    uint32_t nq, ds, dp, nlist, np;
+    const float* cent_t;
+    uint64_t ct_stride;
+    const uint32_t* offsets;
+    uint32_t* probes;
+    uint32_t* list_cnt;
+    uint32_t* q_slot_off;
+    unsigned long long* counters;
+};
+
+template <int QB>
+cudaError_t launch_probe_qb(const ProbeLaunch& a, cudaStream_t s) {
+    auto kern = ivf_probe_kernel<QB>;
+    const size_t smem = probe_smem(QB, a.dp, a.nlist);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    kern<<<(a.nq + QB - 1) / QB, kProbeThreads, smem, s>>>(a.queries, a.nq, a.ds, a.dp, a.cent_t, a.ct_stride, a.nlist,
+                                                          a.np, a.offsets, a.probes, a.list_cnt, a.q_slot_off,
+                                                          a.counters);
+    return cudaGetLastError();
+}
+
+// Probe + plan of n queries: three launches (probe with its counts, the plan's scans, the pairs).
+cudaError_t launch_probe_plan(uint32_t pqb, const ProbeLaunch& a, uint32_t qb, IvfScratch& w, uint32_t* qblock_off,
+                              cudaStream_t s) {
+    cudaError_t e;
+    switch (pqb) {
+        case 8: e = launch_probe_qb<8>(a, s); break;
+        case 4: e = launch_probe_qb<4>(a, s); break;
+        case 2: e = launch_probe_qb<2>(a, s); break;
+        case 1: e = launch_probe_qb<1>(a, s); break;
+        default: return cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess) return e;
+    ivf_plan_scan_kernel<<<1, 1024, 0, s>>>(a.nq, a.nlist, a.offsets, qb, w.d_list_cnt, w.d_list_qoff, w.d_item_off,
+                                            w.d_q_slot_off, w.d_counters, qblock_off);
+    ivf_plan_fill_kernel<<<(a.nq + 7) / 8, 256, 0, s>>>(a.probes, a.nq, a.np, a.offsets, w.d_list_qoff, w.d_list_fill,
+                                                         w.d_q_slot_off, w.d_list_q, w.d_list_slot);
+    count_launch(3);
+    return cudaGetLastError();
+}
+
 template <class T>
 int grow_pinned(T*& p, size_t& cap, size_t n, const char* what) {
     if (n <= cap && p) return NNDEX_OK;
@@ -526,8 +678,8 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
     const size_t smem = ivf_scan_smem(qb, dq, cap);
     if (smem > ix.smem_optin)
         return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF scan needs %zu bytes of shared memory", smem);
-    if (static_cast<size_t>(ix.ds) * 4 + static_cast<size_t>(nlist) * 8 > ix.smem_optin)
-        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF probe shared memory above the limit");
+    const uint32_t pqb = probe_qb(ix.dp, nlist, ix.smem_optin);
+    if (!pqb) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF probe shared memory above the limit");
     const uint64_t max_chunks = (v.max_list + kChunkRows - 1) / kChunkRows;
     int st;
     // Sub-batches so the slot workspace (Σ slots × k keys) stays bounded.
@@ -559,8 +711,6 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
     a.counters = w.d_counters;
     a.ws = w.d_ws;
     a.status = ix.d_status;
-    const size_t probe_smem = static_cast<size_t>(ix.ds) * 4 + static_cast<size_t>(nlist) * 8;
-    cudaFuncSetAttribute(ivf_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(probe_smem));
     uint32_t p2 = 1;
     while (p2 < k) p2 <<= 1;
     cudaMemsetAsync(w.d_counters, 0, 8 * sizeof(unsigned long long), s);
@@ -569,14 +719,11 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
         const float* qn = queries + static_cast<uint64_t>(q0) * ix.ds;
         cudaMemsetAsync(w.d_list_cnt, 0, nlist * sizeof(uint32_t), s);
         cudaMemsetAsync(w.d_list_fill, 0, nlist * sizeof(uint32_t), s);
-        ivf_probe_kernel<<<n, 256, probe_smem, s>>>(qn, dq, static_cast<uint32_t>(ix.dp), v.d_cent_t, v.nlist_pad, nlist,
-                                                    np, w.d_probes);
-        ivf_plan_kernel<<<1, 1024, 0, s>>>(w.d_probes, n, np, nlist, v.d_offsets, qb, w.d_list_cnt, w.d_list_fill,
-                                           w.d_list_qoff, w.d_item_off, w.d_list_q, w.d_list_slot, w.d_q_slot_off,
-                                           w.d_counters, nullptr);
-        count_launch(2);
+        const ProbeLaunch pl{qn, n, dq, static_cast<uint32_t>(ix.dp), nlist, np, v.d_cent_t, v.nlist_pad,
+                             v.d_offsets, w.d_probes, w.d_list_cnt, w.d_q_slot_off, w.d_counters};
+        cudaError_t e = launch_probe_plan(pqb, pl, qb, w, nullptr, s);
+        if (e != cudaSuccess) return cuda_error(e, "IVF probe launch");
         a.queries = qn;
-        cudaError_t e;
         cudaEvent_t ev_a = nullptr;
         ix.scan_event_begin(s, ev_a);
         switch (qb) {
@@ -591,7 +738,7 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
                                                                o_cnt ? o_cnt + q0 : nullptr);
         count_launch();
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "IVF merge launch");
-        ix.stats.kernel_launches += 4;
+        ix.stats.kernel_launches += 5;
     }
     if (!w.h_probed) bump_alloc_epoch();
     if (!w.h_probed && cudaMallocHost(&w.h_probed, 8 * sizeof(unsigned long long)) != cudaSuccess)
@@ -625,8 +772,8 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     const CudaIndex::TcPlan plan = ix.plan_tc(k, false), plan2 = ix.plan_tc(0, false);
     if (plan.kp < k || !plan.stages || !plan2.stages) return ivf_search(ix, ix.d_qn, nq, k, o_idx, o_sim, o_cnt, s);
     const uint32_t kp = plan.kp;
-    if (static_cast<size_t>(ix.ds) * 4 + static_cast<size_t>(nlist) * 8 > ix.smem_optin)
-        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF probe shared memory above the limit");
+    const uint32_t pqb = probe_qb(ix.dp, nlist, ix.smem_optin);
+    if (!pqb) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF probe shared memory above the limit");
     const uint64_t max_chunks = (v.max_list + kChunkRows - 1) / kChunkRows;
     const uint64_t pairs = static_cast<uint64_t>(nq) * np;
     const uint64_t max_blocks = nlist + (pairs + 127) / 128;
@@ -668,21 +815,18 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
         return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: pinned allocation failed");
 
     // ---- probe + plan (groups of 128 queries) + gathered query blocks ----
-    const size_t probe_smem = static_cast<size_t>(ix.ds) * 4 + static_cast<size_t>(nlist) * 8;
-    cudaFuncSetAttribute(ivf_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(probe_smem));
     cudaMemsetAsync(w.d_counters, 0, 8 * sizeof(unsigned long long), s);
     cudaMemsetAsync(w.d_list_cnt, 0, nlist * sizeof(uint32_t), s);
     cudaMemsetAsync(w.d_list_fill, 0, nlist * sizeof(uint32_t), s);
-    ivf_probe_kernel<<<nq, 256, probe_smem, s>>>(ix.d_qn, static_cast<uint32_t>(ix.ds), static_cast<uint32_t>(ix.dp),
-                                                 v.d_cent_t, v.nlist_pad, nlist, np, w.d_probes);
-    ivf_plan_kernel<<<1, 1024, 0, s>>>(w.d_probes, nq, np, nlist, v.d_offsets, 128, w.d_list_cnt, w.d_list_fill,
-                                       w.d_list_qoff, w.d_item_off, w.d_list_q, w.d_list_slot, w.d_q_slot_off,
-                                       w.d_counters, w.d_qblock_off);
+    const ProbeLaunch pl{ix.d_qn, nq, static_cast<uint32_t>(ix.ds), static_cast<uint32_t>(ix.dp), nlist, np,
+                         v.d_cent_t, v.nlist_pad, v.d_offsets, w.d_probes, w.d_list_cnt, w.d_q_slot_off, w.d_counters};
+    cudaError_t e = launch_probe_plan(pqb, pl, 128, w, w.d_qblock_off, s);
+    if (e != cudaSuccess) return cuda_error(e, "IVF probe launch");
     ivf_gather_tc_kernel<<<nlist, 256, 0, s>>>(ix.d_q_bf16, static_cast<uint32_t>(v.kb16), w.d_list_cnt, w.d_list_qoff,
                                                w.d_list_q, w.d_list_slot, w.d_qblock_off, w.d_g16, w.d_lane_qid,
                                                w.d_lane_slot);
-    count_launch(3);
-    cudaError_t e = cudaGetLastError();
+    count_launch();
+    e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "IVF plan launch");
 
     // ---- pass 1 ----
@@ -765,15 +909,16 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     e = launch_scan_tc(a, false, 1, s);
     ix.scan_event_end(s, ev_a);
     if (e != cudaSuccess) return cuda_error(e, "IVF tensor-core scan launch (pass 2)");
-    e = launch_rerank_collected(ix.d_base, static_cast<uint32_t>(ix.ds), ix.d_qn, ix.d_ids, nq, ix.d_rows2, ix.d_cnt2,
-                                cap2, k, o_idx, o_sim, o_cnt, ix.d_ok2, s, true, d_m, v.d_row_map);
+    e = launch_rerank_collected(v.d_reordered, static_cast<uint32_t>(ix.ds), ix.d_qn, ix.d_ids, nq, ix.d_rows2,
+                                ix.d_cnt2, cap2, k, ix.d_q2_thr, o_idx, o_sim, o_cnt, ix.d_ok2, s, true, d_m,
+                                v.d_row_map);
     if (e != cudaSuccess) return cuda_error(e, "rerank launch (pass 2)");
     launch_compact_zero_flags(ix.d_ok2, nq, ix.d_tcfail, d_fail, s, d_m);
     // the plan's totals and the pass counts come back with the results
     cudaMemcpyAsync(w.h_probed, w.d_counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(ix.h_fbn, ix.d_fbn, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     ix.last_tc_n = nq;
-    ix.stats.kernel_launches += 11;
+    ix.stats.kernel_launches += 12;
     ix.stats.path = 5;
     ix.stats.nprobe = np;
     ix.stats.rerank_width = kp;

@@ -78,10 +78,10 @@ NNDEX_DEVICE_INLINE float pick(const uint32_t (&v)[32], uint32_t j) {
 }
 }  // namespace
 
-size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8, bool stream_a) {
+size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8, bool stream_a, uint32_t qb) {
     size_t b = 1024;
     b += stream_a ? static_cast<size_t>(stages) * (kAChunk + kBChunk)
-                  : static_cast<size_t>(nchunks) * kAChunk + static_cast<size_t>(stages) * kBChunk;
+                  : static_cast<size_t>(qb) * nchunks * kAChunk + static_cast<size_t>(stages) * (kBChunk / qb);
     b += static_cast<size_t>(kprime) * kM * 8;
     if (kprime == 0) b += static_cast<size_t>(kPass2Stage) * 8 * 32 * 4;  // pass 2: survivor staging
     b += (2 * stages + 5) * 8 + 16;
@@ -91,6 +91,12 @@ size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp
 uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, bool stream_a, size_t smem_limit) {
     for (uint32_t st = 4; st >= 2; --st)
         if (tc_smem_bytes(nchunks, kprime, st, fp8, stream_a) <= smem_limit) return st;
+    return 0;
+}
+
+uint32_t tc_pair_stages_for(uint32_t nchunks, bool fp8, size_t smem_limit) {
+    for (uint32_t st = 5; st >= 4; --st)
+        if (tc_smem_bytes(nchunks, 0, st, fp8, false, 2) <= smem_limit) return st;
     return 0;
 }
 
@@ -163,16 +169,23 @@ NNDEX_DEVICE_INLINE void epi_survivor(const TcParams& p, EpiState& st, uint64_t*
 // kItems: the IVF list scan (TcParams' item fields): the CTA's queries are a gathered block of the
 // queries probing one list and its rows one chunk of that list's reordered rows; keys and collected
 // rows carry original row indices, and pass-1 heaps go to the (query, chunk) output slots.
-template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems>
+// kQB = 2 (pass 2 only): two resident query blocks per CTA (256 queries) against 128-row base tiles.
+// Each slab of a base tile feeds two MMAs (M = 128, N = 128), one per block, into the two halves of
+// the 256-column accumulator, so a CTA reads half the base bytes per FLOP: the pass is otherwise
+// bound by how fast L2 feeds the base tiles (1 byte per 128 FLOPs). The tile map's box is 128 rows.
+template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems, int kQB>
 __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     scan_tc_kernel(const __grid_constant__ CUtensorMap tmap_q, const __grid_constant__ CUtensorMap tmap_b,
                    const TcParams p) {
-    constexpr uint32_t kElems = kFp8 ? 128 : 64;  // K elements per 128-byte slab
-    constexpr uint32_t kStage = kStreamA ? kAChunk + kBChunk : kBChunk;
+    static_assert(kQB == 1 || (kQB == 2 && kMode == 1 && !kStreamA && !kItems), "two query blocks: pass 2 only");
+    constexpr uint32_t kNT = kQB == 2 ? kN / 2 : kN;  // base rows per tile (MMA N)
+    constexpr uint32_t kQC = kM * kQB;                // queries per CTA
+    constexpr uint32_t kElems = kFp8 ? 128 : 64;      // K elements per 128-byte slab
+    constexpr uint32_t kStage = kStreamA ? kAChunk + kBChunk : kNT * 128;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = align_1024(smem_raw);
-    uint8_t* a_smem = smem;  // resident query slabs (kStreamA: none)
-    uint8_t* b_smem = a_smem + (kStreamA ? 0 : static_cast<size_t>(p.nchunks) * kAChunk);
+    uint8_t* a_smem = smem;  // resident query slabs (kStreamA: none), block-major
+    uint8_t* b_smem = a_smem + (kStreamA ? 0 : static_cast<size_t>(kQB) * p.nchunks * kAChunk);
     uint64_t* heap = reinterpret_cast<uint64_t*>(b_smem + static_cast<size_t>(kST) * kStage);
     uint32_t* stage2 = reinterpret_cast<uint32_t*>(heap + static_cast<size_t>(p.kprime) * kM);  // pass 2
     uint64_t* full_bar = reinterpret_cast<uint64_t*>(stage2 + (kMode == 1 ? kPass2Stage * 8 * 32 : 0));
@@ -184,7 +197,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     volatile uint32_t* abort_flag = tmem_slot + 1;
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    uint32_t q0 = blockIdx.x * kM;
+    uint32_t q0 = blockIdx.x * kQC;
     uint32_t range = blockIdx.y, nranges = gridDim.y;
     uint64_t range_rows = p.range_rows;
     uint32_t nq_live = p.nq;
@@ -192,7 +205,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         // The device count decides the grid's shape: the same ranges tc_ranges gives the host for
         // this many query blocks; CTAs past the work items return before any set-up.
         nq_live = *p.live_q;
-        const uint64_t nqb = (nq_live + kM - 1) / kM;
+        const uint64_t nqb = (nq_live + kQC - 1) / kQC;
         if (nqb == 0) return;
         uint64_t nr = (4ull * p.sm_count + nqb - 1) / nqb;
         const uint64_t nr_max = (p.rows + 2047) / 2048;
@@ -203,7 +216,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         if (blockIdx.x >= nqb * nr) return;
         // consecutive CTAs take the query blocks of one row range, as the 2-D grid orders them: the
         // CTAs resident together read the same base tiles, which then come from L2 after the first
-        q0 = static_cast<uint32_t>(blockIdx.x % nqb) * kM;
+        q0 = static_cast<uint32_t>(blockIdx.x % nqb) * kQC;
         range = static_cast<uint32_t>(blockIdx.x / nqb);
         nranges = static_cast<uint32_t>(nr);
     }
@@ -229,7 +242,10 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         const uint64_t le = p.it_offsets[lo + 1];
         row_end = (row_begin + p.it_chunk_rows) < le ? (row_begin + p.it_chunk_rows) : le;
     }
-    const uint64_t tile_step = static_cast<uint64_t>(kN) * p.tile_stride;
+    // query blocks with at least one query: a second block past the last query is neither loaded
+    // nor multiplied (its epilogue lanes have no query)
+    const uint32_t nblk = (kQB == 2 && q0 + kM >= nq_live) ? 1u : static_cast<uint32_t>(kQB);
+    const uint64_t tile_step = static_cast<uint64_t>(kNT) * p.tile_stride;
     const uint32_t ntiles =
         row_end > row_begin ? static_cast<uint32_t>((row_end - row_begin + tile_step - 1) / tile_step) : 0;
     const uint32_t nchunks = p.nchunks;
@@ -264,10 +280,11 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
             // Base tiles are read by every query block of the same row range at about the same
             // time: keep them in L2 with the default policy (no evict-first hint).
             if (!kStreamA) {
-                mbar_arrive_expect_tx(a_full, nchunks * kAChunk);
-                for (uint32_t c = 0; c < nchunks; ++c)
-                    tma_load_2d(a_smem + static_cast<size_t>(c) * kAChunk, &tmap_q, a_full,
-                                static_cast<int32_t>(c * kElems), static_cast<int32_t>(q0));
+                mbar_arrive_expect_tx(a_full, nblk * nchunks * kAChunk);
+                for (uint32_t b = 0; b < nblk; ++b)
+                    for (uint32_t c = 0; c < nchunks; ++c)
+                        tma_load_2d(a_smem + static_cast<size_t>(b * nchunks + c) * kAChunk, &tmap_q, a_full,
+                                    static_cast<int32_t>(c * kElems), static_cast<int32_t>(q0 + b * kM));
             }
             uint32_t it = 0;
             bool stop = false;
@@ -306,7 +323,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            constexpr uint32_t idesc = tc::instr_desc<kFp8, kM, kN>();
+            constexpr uint32_t idesc = tc::instr_desc<kFp8, kM, kNT>();
             if (!kStreamA && !mbar_wait_bounded(a_full, 0, kWaitBudgetCycles)) {
                 *abort_flag = 1;
                 record_status(p.status, kStatusTimeout);
@@ -321,7 +338,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
                     record_status(p.status, kStatusTimeout);
                 }
                 tc::fence_after_sync();
-                const uint32_t d = tmem_base + buf * kN;
+                const uint32_t d = tmem_base + buf * kN;  // kQB = 2: block b in columns [b·128, b·128 + 128)
                 for (uint32_t c = 0; c < nchunks; ++c, ++it) {
                     const uint32_t s = it % kST, u = it / kST;
                     if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], u & 1u, kWaitBudgetCycles)) {
@@ -331,11 +348,14 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
                     tc::fence_after_sync();
                     if (!*abort_flag) {
                         const uint32_t b_addr = b_addr0 + s * kStage;
-                        const uint32_t a_addr = kStreamA ? b_addr + kBChunk : a_addr0 + c * kAChunk;
+                        for (uint32_t b = 0; b < nblk; ++b) {
+                            const uint32_t a_addr =
+                                kStreamA ? b_addr + kBChunk : a_addr0 + (b * nchunks + c) * kAChunk;
 #pragma unroll
-                        for (uint32_t kk = 0; kk < 4; ++kk)
-                            tc::mma<kFp8>(d, tc::smem_desc_sw128(a_addr + kk * 32), tc::smem_desc_sw128(b_addr + kk * 32),
-                                          idesc, (c | kk) != 0u ? 1u : 0u);
+                            for (uint32_t kk = 0; kk < 4; ++kk)
+                                tc::mma<kFp8>(d + b * kNT, tc::smem_desc_sw128(a_addr + kk * 32),
+                                              tc::smem_desc_sw128(b_addr + kk * 32), idesc, (c | kk) != 0u ? 1u : 0u);
+                        }
                     }
                     tc::commit(&empty_bar[s]);  // frees the slab once the MMAs above have read it
                 }
@@ -345,12 +365,14 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     } else {
         // ---------------- epilogue: one query per thread (pass 2: two threads, half a tile each) ----
         constexpr uint32_t kEpiW = epi_warps<kMode>();
-        constexpr uint32_t kChunks = (kN / 32) / (kEpiW / 4);  // 32-column chunks per thread
+        constexpr uint32_t kWPB = kEpiW / 4 / kQB;            // warps per (TMEM lane quarter, query block)
+        constexpr uint32_t kChunks = (kNT / 32) / kWPB;       // 32-column chunks per thread
         const uint32_t ew = warp - 2;
-        const uint32_t c_begin = (ew / 4) * kChunks;
+        const uint32_t blk = (ew / 4) / kWPB;                 // the thread's query block
+        const uint32_t c_begin = ((ew / 4) % kWPB) * kChunks;
         const uint32_t quarter = warp & 3u;
         const uint32_t lrow = quarter * 32 + lane;
-        const uint32_t q = kItems ? p.it_lane_qid[q0 + lrow] : q0 + lrow;
+        const uint32_t q = kItems ? p.it_lane_qid[q0 + lrow] : q0 + blk * kM + lrow;
         const bool valid_q = kItems ? q != 0xFFFFFFFFu : q < nq_live;
         // pass 2: this thread's staged rows and its append of them to the query's collection
         uint32_t* my_stage = stage2 + (ew * 32 + lane) * kPass2Stage;
@@ -384,7 +406,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
             float smin = 0.0f, smax = 0.0f;
             const float* sc = kFp8 ? p.row_scale + tile_row0 : nullptr;
             if (kFp8) {
-                const float2 mm = p.tile_scale[tile_row0 / kN];
+                const float2 mm = p.tile_scale[tile_row0 / kN];  // a 128-row tile lies in one 256-row tile
                 smin = mm.x;
                 smax = mm.y;
             }
@@ -401,7 +423,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
                     st.cut = st.thr_f - slack;
                 }
             }
-            const uint32_t taddr = taddr0 + buf * kN;
+            const uint32_t taddr = taddr0 + buf * kN + blk * kNT;
             uint32_t va[32], vb[32];
             __syncwarp();
             tc::tmem_ld32(taddr + c_begin * 32, va);
@@ -503,15 +525,34 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
 // by slab with FMA; then ((c0+c1)+(c2+c3)) + ((c4+c5)+(c6+c7)). Called by 8 consecutive lanes (one
 // per ch); every lane returns the full sum. So a query's scores are bit-identical on every path.
 // ------------------------------------------------------------------------------------------
+// kU slabs' loads are issued before their FMAs (a row is a gather: its loads must overlap); the FMAs
+// stay in slab order.
+template <uint32_t kU>
 NNDEX_DEVICE_INLINE float dot_scan_order(const float* __restrict__ x, const float* __restrict__ y, uint32_t nbox,
                                          uint32_t ch, bool live) {
     float acc = 0.0f;
     if (live) {
         const float* xa = x + ch * 4;
         const float* ya = y + ch * 4;
-        for (uint32_t bx = 0; bx < nbox; ++bx) {
-            const float4 a = *reinterpret_cast<const float4*>(xa + bx * 32);
-            const float4 b = *reinterpret_cast<const float4*>(ya + bx * 32);
+        uint32_t bx = 0;
+        for (; bx + kU <= nbox; bx += kU) {
+            float4 a[kU], b[kU];
+#pragma unroll
+            for (uint32_t u = 0; u < kU; ++u) {
+                a[u] = __ldg(reinterpret_cast<const float4*>(xa + (bx + u) * 32));
+                b[u] = __ldg(reinterpret_cast<const float4*>(ya + (bx + u) * 32));
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < kU; ++u) {
+                acc = fmaf(a[u].x, b[u].x, acc);
+                acc = fmaf(a[u].y, b[u].y, acc);
+                acc = fmaf(a[u].z, b[u].z, acc);
+                acc = fmaf(a[u].w, b[u].w, acc);
+            }
+        }
+        for (; bx < nbox; ++bx) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(xa + bx * 32));
+            const float4 b = __ldg(reinterpret_cast<const float4*>(ya + bx * 32));
             acc = fmaf(a.x, b.x, acc);
             acc = fmaf(a.y, b.y, acc);
             acc = fmaf(a.z, b.z, acc);
@@ -527,7 +568,7 @@ NNDEX_DEVICE_INLINE float dot_scan_order(const float* __restrict__ x, const floa
 // ------------------------------------------------------------------------------------------
 // K4 (pass 1): exact FP32 rerank of the k′ candidates + top-k + certificate + T. One block per query.
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(1024, 1)
     rerank_kernel(const float* __restrict__ base, uint32_t ds, const float* __restrict__ queries,
                   const uint64_t* __restrict__ cand_idx, const float* __restrict__ cand_bound,
                   const uint32_t* __restrict__ cand_cnt, uint32_t kp, uint32_t k, uint64_t* __restrict__ idx_out,
@@ -546,7 +587,7 @@ __global__ void __launch_bounds__(1024)
         const uint32_t j = j0 + slot;
         const bool live = j < n;
         const uint64_t row = live ? cand_idx[static_cast<size_t>(q) * kp + j] : 0;
-        const float acc = dot_scan_order(base + row * ds, qv, nbox, ch, live);
+        const float acc = dot_scan_order<4>(base + row * ds, qv, nbox, ch, live);
         if (ch == 0 && j < p2) keys[j] = live ? make_key(acc, static_cast<uint32_t>(row)) : 0ull;
     }
     __syncthreads();
@@ -599,56 +640,83 @@ __global__ void gather_queries_kernel(const uint32_t* __restrict__ ids, uint32_t
     }
 }
 
+// Scores of one round that the block keeps in shared memory beside the carried best k.
+constexpr uint32_t kRerankRound = 2048;
+
+// One block per uncertified query: re-scores its collected rows exactly (the FP32 scan's order) and
+// writes their top-k. Only rows whose exact score reaches T (the exact k-th score of pass 1, a lower
+// bound of the true k-th) can be in the top-k, and the k rows that gave T are among the collected
+// ones, so only those rows are kept; when more than a round of them accumulate, the best k are
+// selected and the round starts over. `vecs` holds the vectors: the base by row, or (IVF) the
+// list-ordered copy by collected position.
 __global__ void __launch_bounds__(256)
-    rerank_collected_kernel(const float* __restrict__ base, uint32_t ds, const float* __restrict__ queries,
+    rerank_collected_kernel(const float* __restrict__ vecs, uint32_t ds, const float* __restrict__ queries,
                             const uint32_t* __restrict__ ids, const uint32_t* __restrict__ rows2,
                             const uint32_t* __restrict__ cnt2, uint32_t cap2, uint32_t k, uint64_t* __restrict__ idx_out,
                             float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out,
                             uint32_t* __restrict__ ok_out, int by_query, const uint32_t* __restrict__ live,
-                            const uint32_t* __restrict__ row_map) {
-    extern __shared__ uint64_t keys[];
+                            const uint32_t* __restrict__ row_map, const float* __restrict__ thr) {
+    extern __shared__ uint64_t keys[];  // kRerankRound + (k rounded up to a power of two)
     __shared__ BlockSelectScratch sel;
+    __shared__ uint32_t fill;
     const uint32_t i = blockIdx.x;
     if (live && i >= *live) return;
     const uint32_t q = ids[i];
-    const uint32_t qrow = by_query ? q : i;  // collected rows indexed by query, or by position in ids
+    const uint32_t qrow = by_query ? q : i;  // collected rows and T indexed by query, or by position in ids
     const uint32_t total = cnt2[qrow];
     if (total > cap2) {  // the collected set overflowed: this query goes to the FP32 scan
         if (threadIdx.x == 0) ok_out[i] = 0;
         return;
     }
     const uint32_t n = total;
+    const float t = thr[qrow];
     const uint32_t ch = threadIdx.x & 7u, slot = threadIdx.x >> 3, nslots = blockDim.x >> 3;
     const float* qv = queries + static_cast<size_t>(q) * ds;
     const uint32_t nbox = ds / 32;
+    uint32_t p2k = 1;
+    while (p2k < k) p2k <<= 1;
+    const uint32_t capacity = kRerankRound + p2k;
+    if (threadIdx.x == 0) fill = 0;
+    __syncthreads();
+    // keeps the best kk of keys[0, m) in keys[0, kk) (order not yet defined)
+    auto keep_best = [&](uint32_t m, uint32_t kk) {
+        const uint64_t kth = block_radix_kth(keys, m, kk, sel);
+        if (threadIdx.x == 0) sel.count = 0;
+        __syncthreads();
+        for (uint32_t j0 = 0; j0 < m; j0 += blockDim.x) {
+            const uint32_t j = j0 + threadIdx.x;
+            const uint64_t key = j < m ? keys[j] : 0ull;
+            __syncthreads();
+            if (j < m && key >= kth) {
+                const uint32_t pos = atomicAdd(&sel.count, 1u);
+                keys[pos] = key;  // pos ≤ j: never overwrites a key not yet read
+            }
+            __syncthreads();
+        }
+    };
     for (uint32_t j0 = 0; j0 < n; j0 += nslots) {
         const uint32_t j = j0 + slot;
-        const bool live = j < n;
-        const uint32_t pos = live ? rows2[static_cast<size_t>(qrow) * cap2 + j] : 0u;
-        const uint64_t row = row_map && live ? row_map[pos] : pos;
-        const float acc = dot_scan_order(base + row * ds, qv, nbox, ch, live);
-        if (ch == 0 && live) keys[j] = make_key(acc, static_cast<uint32_t>(row));
-    }
-    __syncthreads();
-    const uint32_t kk = n < k ? n : k;
-    uint64_t kth = 1;
-    if (n > kk && kk > 0) kth = block_radix_kth(keys, n, kk, sel);
-    // Keep the kk best in place (order does not matter yet), then sort them.
-    if (threadIdx.x == 0) sel.count = 0;
-    __syncthreads();
-    for (uint32_t j0 = 0; j0 < n; j0 += blockDim.x) {
-        const uint32_t j = j0 + threadIdx.x;
-        const uint64_t key = j < n ? keys[j] : 0ull;
+        const bool on = j < n;
+        const uint32_t pos = on ? rows2[static_cast<size_t>(qrow) * cap2 + j] : 0u;
+        const uint32_t row = row_map && on ? row_map[pos] : pos;
+        const float acc = dot_scan_order<4>(vecs + static_cast<size_t>(row_map ? pos : row) * ds, qv, nbox, ch, on);
+        if (ch == 0 && on && acc >= t) keys[atomicAdd(&fill, 1u)] = make_key(acc, row);
         __syncthreads();
-        if (j < n && key >= kth) {
-            const uint32_t pos = atomicAdd(&sel.count, 1u);
-            keys[pos] = key;  // pos ≤ j: never overwrites a key not yet read
+        const uint32_t f = fill;
+        __syncthreads();  // every thread has read the count before the next round appends
+        if (f + nslots > capacity) {  // no room for another round: keep the best k (f > k here)
+            keep_best(f, k);
+            if (threadIdx.x == 0) fill = k;
+            __syncthreads();
         }
-        __syncthreads();
     }
+    const uint32_t m = fill;
+    const uint32_t kk = m < k ? m : k;
+    if (m > kk) keep_best(m, kk);
     uint32_t p2 = 1;
     while (p2 < kk) p2 <<= 1;
     for (uint32_t j = kk + threadIdx.x; j < p2; j += blockDim.x) keys[j] = 0ull;
+    __syncthreads();
     block_bitonic_sort_desc(keys, p2);
     for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
         idx_out[static_cast<size_t>(q) * k + j] = j < kk ? key_row(keys[j]) : 0;
@@ -663,21 +731,21 @@ __global__ void __launch_bounds__(256)
 // ------------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------------
-template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems = false>
+template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems = false, int kQB = 1>
 static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
-    auto kern = scan_tc_kernel<kFp8, kST, kMode, kStreamA, kItems>;
+    auto kern = scan_tc_kernel<kFp8, kST, kMode, kStreamA, kItems, kQB>;
     const uint32_t kp = kMode == 0 ? a.p.kprime : 0;
-    const size_t smem = tc_smem_bytes(a.p.nchunks, kp, kST, kFp8, kStreamA);
+    const size_t smem = tc_smem_bytes(a.p.nchunks, kp, kST, kFp8, kStreamA, kQB);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     dim3 grid = kItems ? dim3(a.items, 1)
-                       : (a.p.live_q ? dim3(a.live_items, 1) : dim3((a.p.nq + kM - 1) / kM, a.nranges));
+                       : (a.p.live_q ? dim3(a.live_items, 1) : dim3((a.p.nq + kM * kQB - 1) / (kM * kQB), a.nranges));
     TcParams p = a.p;
     p.kprime = kp;
     if (sync_check_enabled())
-        set_launch_note("scan_tc fp8 %d stages %d mode %d stream_a %d items %d: grid (%u, %u), nq %u, k' %u, "
-                        "tile stride %u, range rows %llu, rows %llu, smem %zu",
-                        kFp8, kST, kMode, kStreamA, kItems, grid.x, grid.y, p.nq, kp, p.tile_stride,
+        set_launch_note("scan_tc fp8 %d stages %d mode %d stream_a %d items %d query blocks %d: grid (%u, %u), nq %u, "
+                        "k' %u, tile stride %u, range rows %llu, rows %llu, smem %zu",
+                        kFp8, kST, kMode, kStreamA, kItems, kQB, grid.x, grid.y, p.nq, kp, p.tile_stride,
                         (unsigned long long)p.range_rows, (unsigned long long)p.rows, smem);
     kern<<<grid, tc_threads<kMode>(), smem, stream>>>(*a.tmap_q, *a.tmap_b, p);
     count_launch();
@@ -711,6 +779,17 @@ cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t str
         if (mode == 0) return a.stream_a ? launch_tc_items<0, true>(a, stream) : launch_tc_items<0, false>(a, stream);
         return a.stream_a ? launch_tc_items<1, true>(a, stream) : launch_tc_items<1, false>(a, stream);
     }
+    if (mode == 1 && a.qb == 2) {
+        if (a.stream_a || a.p.range_rows % kN) return cudaErrorInvalidValue;
+        switch (a.stages) {
+            case 5: return fp8 ? launch_tc_impl<true, 5, 1, false, false, 2>(a, stream)
+                               : launch_tc_impl<false, 5, 1, false, false, 2>(a, stream);
+            case 4: return fp8 ? launch_tc_impl<true, 4, 1, false, false, 2>(a, stream)
+                               : launch_tc_impl<false, 4, 1, false, false, 2>(a, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    if (a.qb != 1) return cudaErrorInvalidValue;
     if (mode == 0) {
         if (a.stream_a) return fp8 ? launch_tc_stages<true, 0, true>(a, stream) : launch_tc_stages<false, 0, true>(a, stream);
         return fp8 ? launch_tc_stages<true, 0, false>(a, stream) : launch_tc_stages<false, 0, false>(a, stream);
@@ -746,20 +825,21 @@ cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q
     return cudaGetLastError();
 }
 
-cudaError_t launch_rerank_collected(const float* base, uint32_t ds, const float* queries, const uint32_t* ids,
+cudaError_t launch_rerank_collected(const float* vecs, uint32_t ds, const float* queries, const uint32_t* ids,
                                     uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
-                                    uint64_t* idx_out, float* sim_out, uint32_t* cnt_out, uint32_t* ok_out,
-                                    cudaStream_t stream, bool by_query, const uint32_t* live,
+                                    const float* thr, uint64_t* idx_out, float* sim_out, uint32_t* cnt_out,
+                                    uint32_t* ok_out, cudaStream_t stream, bool by_query, const uint32_t* live,
                                     const uint32_t* row_map) {
     if (m == 0) return cudaSuccess;
-    uint32_t p2 = 1;
-    while (p2 < cap2) p2 <<= 1;
-    const size_t smem = std::max<size_t>(p2, 2 * k) * sizeof(uint64_t);
+    if (k == 0 || k > kRerankRound) return cudaErrorInvalidValue;
+    uint32_t p2k = 1;
+    while (p2k < k) p2k <<= 1;
+    const size_t smem = (kRerankRound + p2k) * sizeof(uint64_t);
     auto kern = rerank_collected_kernel;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    kern<<<m, 256, smem, stream>>>(base, ds, queries, ids, rows2, cnt2, cap2, k, idx_out, sim_out, cnt_out, ok_out,
-                                   by_query ? 1 : 0, live, row_map);
+    kern<<<m, 256, smem, stream>>>(vecs, ds, queries, ids, rows2, cnt2, cap2, k, idx_out, sim_out, cnt_out, ok_out,
+                                   by_query ? 1 : 0, live, row_map, thr);
     count_launch();
     return cudaGetLastError();
 }

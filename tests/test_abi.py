@@ -40,7 +40,7 @@ def test_structs_match_header_layout():
     # sizes of the C structs as the header lays them out (x86-64)
     assert C.sizeof(_lib.Opts) == 4 + 4 * 5 + 8 + 4 + 4 * 7
     assert C.sizeof(_lib.DevInfo) == 8 + 256 + 64 + 64 + 32 + 32 + 4 * 3 + 4 + 8 + 8
-    assert C.sizeof(_lib.SearchStats) == 4 * 6 + 8 + 8 + 8 + 8 + 8 + 4 * 4 + 8 + 8 + 4 * 2 + 8
+    assert C.sizeof(_lib.SearchStats) == 4 * 6 + 8 + 8 + 8 + 8 + 8 + 4 * 4 + 8 + 8 + 4 * 2 + 8 + 4 * 2
 
 
 def test_last_error_is_empty_string_initially():

@@ -91,16 +91,21 @@ def test_autotune_cache_text_is_validated_without_a_gpu():
     # the tuner's export format: a header naming device, shape and flags, then one line per shape
     L = _lib.lib()
     n = C.c_uint64(0)
-    good = (b"nndex-autotune v1 device=NVIDIA_B200 rows=1000000 dims=768 flags=1\n"
-            b"shape ivf=0 nq=16 k=128 precision=0 nprobe=0 plan path=6 stride=0 ms=0.512\n"
-            b"shape ivf=1 nq=1024 k=16 precision=3 nprobe=32 plan path=5 stride=0 ms=2.5\n\n")
+    good = (b"nndex-autotune v2 device=NVIDIA_B200 rows=1000000 dims=768 flags=1\n"
+            b"shape ivf=0 nq=16 k=128 precision=0 nprobe=0 plan path=6 stride=0 qb=0 ms=0.512\n"
+            b"shape ivf=1 nq=1024 k=16 precision=3 nprobe=32 plan path=5 stride=0 qb=0 ms=2.5\n\n")
     assert L.nndex_cuda_autotune_validate(good, C.byref(n)) == 0 and n.value == 2
+    two = good + b"shape ivf=0 nq=256 k=16 precision=1 nprobe=0 plan path=2 stride=8 qb=2 ms=20.5\n"
+    assert L.nndex_cuda_autotune_validate(two, C.byref(n)) == 0 and n.value == 3
     bad = [
-        b"shape ivf=0 nq=16 k=128 precision=0 nprobe=0 plan path=6 stride=0 ms=0.5\n",  # no header
-        good + b"shape ivf=0 nq=12 k=128 precision=0 nprobe=0 plan path=1 stride=0 ms=1\n",  # nq not 2^n
-        good + b"shape ivf=0 nq=16 k=16 precision=0 nprobe=0 plan path=4 stride=0 ms=1\n",  # IVF path, exact shape
-        good + b"shape ivf=1 nq=16 k=16 precision=0 nprobe=8 plan path=2 stride=0 ms=1\n",  # exact path, IVF shape
-        good + b"shape ivf=0 nq=16 k=16 precision=0 nprobe=0 plan path=9 stride=0 ms=1\n",  # no such path
+        b"shape ivf=0 nq=16 k=128 precision=0 nprobe=0 plan path=6 stride=0 qb=0 ms=0.5\n",  # no header
+        good + b"shape ivf=0 nq=12 k=128 precision=0 nprobe=0 plan path=1 stride=0 qb=0 ms=1\n",  # nq not 2^n
+        good + b"shape ivf=0 nq=16 k=16 precision=0 nprobe=0 plan path=4 stride=0 qb=0 ms=1\n",  # IVF path, exact shape
+        good + b"shape ivf=1 nq=16 k=16 precision=0 nprobe=8 plan path=2 stride=0 qb=0 ms=1\n",  # exact path, IVF shape
+        good + b"shape ivf=0 nq=16 k=16 precision=0 nprobe=0 plan path=9 stride=0 qb=0 ms=1\n",  # no such path
+        good + b"shape ivf=0 nq=16 k=16 precision=0 nprobe=0 plan path=1 stride=0 qb=2 ms=1\n",  # qb off path 2/3
+        good + b"shape ivf=0 nq=256 k=16 precision=1 nprobe=0 plan path=2 stride=8 qb=3 ms=1\n",  # qb above 2
+        good + b"shape ivf=0 nq=256 k=16 precision=1 nprobe=0 plan path=2 stride=8 ms=1\n",  # no qb field
         good + b"garbage\n",
     ]
     for text in bad:

@@ -163,3 +163,48 @@ def test_overflowing_collection_reruns_on_the_fp32_scan():
     fi, fs = index.search(q, k=10)
     np.testing.assert_array_equal(ti, fi)
     np.testing.assert_array_equal(ts.view(np.uint32), fs.view(np.uint32))
+
+
+@pytest.mark.parametrize("precision,certifying,uncertified,qb", [
+    ("bf16", 250, 50, 2),    # 50 live queries of 300: the CTA's second query block is empty
+    ("bf16", 100, 200, 2),   # 200 live: the second block is partly filled
+    ("bf16", 100, 600, 2),   # 600 live: three CTA query pairs, the last with one block
+    ("bf16", 100, 200, 1),
+    ("fp8", 150, 170, 2),
+    ("fp8", 150, 170, 1),
+])
+def test_pass2_query_blocks_per_cta(precision, certifying, uncertified, qb):
+    # Pass 2 of a batch of more than 128 queries can put two query blocks in each CTA against
+    # 128-row base tiles (the plan's qb, fixed here through the autotuner's cache). The number of
+    # live queries decides on the device how many blocks a CTA loads and multiplies. Queries equal
+    # to a base row of a mixture certify in pass 1 (their top-1 scores 1, their cluster about 0.94);
+    # a query with 40 near-duplicate rows (scores about 1e-4 apart, inside the bound slack) cannot
+    # certify with k' = 32 and takes pass 2. Results equal the oracle's and the FP32 path's.
+    rng = np.random.default_rng(certifying + uncertified)
+    dims = 128
+    mix = mixture(rng, 8_000, dims, 256, 0.25)
+    vs = rng.normal(size=(100, dims)).astype(np.float32)
+    groups = (np.repeat(vs, 40, axis=0) + np.float32(1e-2) * rng.normal(size=(4_000, dims))).astype(np.float32)
+    m = np.concatenate([mix, groups]).astype(np.float32)
+    q = np.concatenate([mix[rng.choice(8_000, certifying, replace=False)],
+                        vs[rng.integers(0, 100, size=uncertified)]]).astype(np.float32)
+    q = q[rng.permutation(q.shape[0])].copy()
+    index = NNdex(m, precision=precision)
+    code = 2 if precision == "bf16" else 3
+    nqb = 1 << (q.shape[0] - 1).bit_length()
+    index.autotune_import(index.autotune_export() +
+                          f"shape ivf=0 nq={nqb} k=1 precision={code} nprobe=0 plan path={code} stride=1 qb={qb} ms=0\n")
+    _check(index, m, q, 1, f"{precision} pass 2 with {qb} query blocks per CTA")
+    st = index.last_search_stats()
+    # (FP8's wider bound may leave a few of the other queries uncertified too)
+    if precision == "bf16":
+        assert st["second_pass_queries"] == uncertified, st
+    else:
+        assert uncertified <= st["second_pass_queries"] <= uncertified + certifying // 10, st
+    assert st["pass2_query_blocks"] == qb and st["tuned"] == 2, st
+    assert st["fp32_fallback_queries"] == 0, st
+    ti, ts = index.search(q, k=1)
+    index.set_precision("fp32")
+    fi, fs = index.search(q, k=1)
+    np.testing.assert_array_equal(ti, fi)
+    np.testing.assert_array_equal(ts.view(np.uint32), fs.view(np.uint32))
