@@ -51,6 +51,7 @@ struct IvfScratch {
     uint32_t nprobe = 0;                // 0 = choose_nprobe per search
     uint32_t tc_stride = 1;             // tensor-core scan: pass 1 on every n-th tile (autotuned)
     uint32_t* d_probes = nullptr;       size_t cap_probes = 0;
+    float* d_pscore = nullptr;          size_t cap_pscore = 0;     // B·nlist: centroid scores of the probe
     uint32_t* d_list_cnt = nullptr;     size_t cap_list_cnt = 0;   // nlist: queries probing each list
     uint32_t* d_list_fill = nullptr;    size_t cap_list_fill = 0;
     uint32_t* d_list_qoff = nullptr;    size_t cap_list_qoff = 0;  // nlist + 1

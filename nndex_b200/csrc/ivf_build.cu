@@ -975,6 +975,7 @@ IvfScratch::~IvfScratch() {
     cudaFree(d_lane_qid);
     cudaFree(d_lane_slot);
     cudaFree(d_probes);
+    cudaFree(d_pscore);
     cudaFree(d_list_cnt);
     cudaFree(d_list_fill);
     cudaFree(d_list_qoff);

@@ -1,10 +1,10 @@
 // ivf_search.cu — K8/K9: IVF probe and the ragged list scan with exact FP32 rerank.
 //
 // Replaces candidate_clusters(_batch) (src/approx.rs:159-300) and search_approx /
-// search_batch_approx (src/cpu.rs:425-502). A batch runs as five launches and no host round trip:
-//   1. probe: per query, dot_small against every centroid (FP64 in index order, f32 result — the
-//      reference's value) and the nprobe best clusters (score desc, lower index on ties); up to 8
-//      queries per block share each read of the centroids.
+// search_batch_approx (src/cpu.rs:425-502). A batch runs as six launches and no host round trip:
+//   1. probe (two launches): per query, dot_small against every centroid (FP64 in index order, f32
+//      result — the reference's value; up to 8 queries share each read of a centroid) and the nprobe
+//      best clusters (score desc, lower index on ties).
 //   2. plan (a one-block scan, then one warp per query): the (list, query) pairs grouped by list,
 //      each list cut into chunks of at most kChunkRows rows, and work items (list chunk × group of up
 //      to QB queries probing it), with every (query, list chunk) owning one output slot of k keys.
@@ -64,16 +64,17 @@ NNDEX_DEVICE_INLINE void block_exclusive_scan(uint32_t* v, uint32_t n, uint32_t*
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
-// 1. Probe: QB queries per block of 8 warps (QB ≤ 8, as many as shared memory holds), so the
-//    centroid matrix is read from L2 once per QB queries. A thread scores its centroids against
-//    all QB queries (FP64 FMA in index order, the queries held as doubles in shared memory); warp j
-//    then selects query j's nprobe best lists (a radix select over its keys), writes them, and
-//    counts them into the plan: queries per list, and the query's output slots (one per chunk of a
-//    probed list) and probed rows.
+// 1. Probe, in two launches.
+//    (a) Scores: a block scores 256 centroids against up to 8 queries (FP64 FMA in index order, f32
+//        result, the queries held as doubles in shared memory), so each centroid read from L2
+//        serves 8 queries and the grid (query groups × centroid chunks) fills every SM.
+//    (b) Selection: one warp per query reads its scores (from L2) and selects its nprobe best lists
+//        (a radix select over the keys (score, list)), writes them, and counts them into the plan:
+//        queries per list, the query's output slots (one per chunk of a probed list), probed rows.
 // ------------------------------------------------------------------------------------------
-// The k-th largest of n distinct keys, by one warp (8 passes of 8 bits; `hist` 256 words of the
-// warp's own).
-NNDEX_DEVICE_INLINE uint64_t warp_radix_kth(const uint64_t* keys, uint32_t n, uint32_t k, uint32_t* hist,
+// The k-th largest of the n distinct keys (score, index i) of scores[0, n), by one warp (8 passes of
+// 8 bits; `hist` 256 words of the warp's own).
+NNDEX_DEVICE_INLINE uint64_t warp_radix_kth(const float* scores, uint32_t n, uint32_t k, uint32_t* hist,
                                             uint32_t lane) {
     uint64_t prefix = 0, mask = 0;
     uint32_t krem = k;
@@ -81,7 +82,7 @@ NNDEX_DEVICE_INLINE uint64_t warp_radix_kth(const uint64_t* keys, uint32_t n, ui
         for (uint32_t i = lane; i < 256; i += 32) hist[i] = 0;
         __syncwarp();
         for (uint32_t i = lane; i < n; i += 32) {
-            const uint64_t key = keys[i];
+            const uint64_t key = make_key(scores[i], i);
             if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
         }
         __syncwarp();
@@ -121,23 +122,17 @@ NNDEX_DEVICE_INLINE uint64_t warp_radix_kth(const uint64_t* keys, uint32_t n, ui
     return prefix;
 }
 
-constexpr uint32_t kProbeThreads = 256;
+constexpr uint32_t kProbeThreads = 256;  // centroids per scoring block
 
-size_t probe_smem(uint32_t qb, uint64_t dp, uint64_t nlist) {
-    return static_cast<size_t>(qb) * (dp * 8 + nlist * 8 + 256 * 4);
-}
+static size_t probe_smem(uint32_t qb, uint64_t dp) { return static_cast<size_t>(qb) * dp * 8; }
 
 template <int QB>
 __global__ void __launch_bounds__(kProbeThreads)
-    ivf_probe_kernel(const float* __restrict__ queries, uint32_t nq, uint32_t ds, uint32_t dp,
-                     const float* __restrict__ cent_t, uint64_t ct_stride, uint32_t nlist, uint32_t np,
-                     const uint32_t* __restrict__ offsets, uint32_t* __restrict__ probes,
-                     uint32_t* __restrict__ list_cnt, uint32_t* __restrict__ q_slot_off,
-                     unsigned long long* __restrict__ counters) {
+    ivf_probe_score_kernel(const float* __restrict__ queries, uint32_t nq, uint32_t ds, uint32_t dp,
+                           const float* __restrict__ cent_t, uint64_t ct_stride, uint32_t nlist,
+                           float* __restrict__ scores) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    double* qd = reinterpret_cast<double*>(smem_raw);                 // [dp][QB]
-    uint64_t* keys = reinterpret_cast<uint64_t*>(qd + static_cast<size_t>(dp) * QB);  // [QB][nlist]
-    uint32_t* hist = reinterpret_cast<uint32_t*>(keys + static_cast<size_t>(QB) * nlist);  // [QB][256]
+    double* qd = reinterpret_cast<double*>(smem_raw);  // [dp][QB]
     const uint32_t q0 = blockIdx.x * QB;
     const uint32_t nb = (nq - q0) < QB ? (nq - q0) : QB;
     for (uint32_t i = threadIdx.x; i < dp * QB; i += blockDim.x) {
@@ -145,32 +140,40 @@ __global__ void __launch_bounds__(kProbeThreads)
         qd[i] = j < nb ? static_cast<double>(queries[static_cast<uint64_t>(q0 + j) * ds + d]) : 0.0;
     }
     __syncthreads();
-    for (uint32_t c = threadIdx.x; c < nlist; c += blockDim.x) {
-        double acc[QB];
+    const uint32_t c = blockIdx.y * kProbeThreads + threadIdx.x;
+    if (c >= nlist) return;
+    double acc[QB];
 #pragma unroll
-        for (int j = 0; j < QB; ++j) acc[j] = 0.0;
-        const float* col = cent_t + c;
-#pragma unroll 4
-        for (uint32_t d = 0; d < dp; ++d) {
-            const double cv = static_cast<double>(__ldg(col + static_cast<uint64_t>(d) * ct_stride));
-            const double* qv = qd + static_cast<size_t>(d) * QB;
+    for (int j = 0; j < QB; ++j) acc[j] = 0.0;
+    const float* col = cent_t + c;
+#pragma unroll 8
+    for (uint32_t d = 0; d < dp; ++d) {
+        const double cv = static_cast<double>(__ldg(col + static_cast<uint64_t>(d) * ct_stride));
+        const double* qv = qd + static_cast<size_t>(d) * QB;
 #pragma unroll
-            for (int j = 0; j < QB; ++j) acc[j] = fma(cv, qv[j], acc[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < QB; ++j) keys[static_cast<size_t>(j) * nlist + c] = make_key(fold_zero(__double2float_rn(acc[j])), c);
+        for (int j = 0; j < QB; ++j) acc[j] = fma(cv, qv[j], acc[j]);
     }
-    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < QB; ++j)
+        if (j < static_cast<int>(nb)) scores[static_cast<uint64_t>(q0 + j) * nlist + c] = fold_zero(__double2float_rn(acc[j]));
+}
+
+__global__ void __launch_bounds__(256)
+    ivf_probe_select_kernel(const float* __restrict__ scores, uint32_t nq, uint32_t nlist, uint32_t np,
+                            const uint32_t* __restrict__ offsets, uint32_t* __restrict__ probes,
+                            uint32_t* __restrict__ list_cnt, uint32_t* __restrict__ q_slot_off,
+                            unsigned long long* __restrict__ counters) {
+    __shared__ uint32_t hist_all[8][256];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    if (warp >= nb) return;
-    const uint32_t q = q0 + warp;
-    const uint64_t* kq = keys + static_cast<size_t>(warp) * nlist;
-    const uint64_t kth = np < nlist ? warp_radix_kth(kq, nlist, np, hist + warp * 256u, lane) : 0ull;
+    const uint32_t q = blockIdx.x * 8 + warp;
+    if (q >= nq) return;
+    const float* sq = scores + static_cast<uint64_t>(q) * nlist;
+    const uint64_t kth = np < nlist ? warp_radix_kth(sq, nlist, np, hist_all[warp], lane) : 0ull;
     uint32_t base = 0, slots = 0;
     unsigned long long rows = 0;
     for (uint32_t c0 = 0; c0 < nlist; c0 += 32) {
         const uint32_t c = c0 + lane;
-        const bool take = c < nlist && kq[c] >= kth;
+        const bool take = c < nlist && make_key(sq[c], c) >= kth;
         const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, take);
         if (take) {
             const uint32_t pos = base + __popc(ballot & ((1u << lane) - 1u));
@@ -593,11 +596,11 @@ cudaError_t launch_scan(const CUtensorMap& tmap, const IvfScanArgs& a, uint32_t 
     return cudaGetLastError();
 }
 
-// Queries per probe block: the most (8, 4, 2 or 1) whose queries, keys and histograms fit in
-// shared memory; 0 if not even one query's do.
-uint32_t probe_qb(uint64_t dp, uint64_t nlist, size_t smem_optin) {
+// Queries per probe scoring block: the most (8, 4, 2 or 1) held as doubles in shared memory; 0 if
+// not even one fits.
+uint32_t probe_qb(uint64_t dp, size_t smem_optin) {
     for (uint32_t qb = 8; qb >= 1; qb >>= 1)
-        if (probe_smem(qb, dp, nlist) <= smem_optin) return qb;
+        if (probe_smem(qb, dp) <= smem_optin) return qb;
     return 0;
 }
 
@@ -607,6 +610,7 @@ struct ProbeLaunch {
     const float* cent_t;
     uint64_t ct_stride;
     const uint32_t* offsets;
+    float* scores;  // nq × nlist
     uint32_t* probes;
     uint32_t* list_cnt;
     uint32_t* q_slot_off;
@@ -615,19 +619,20 @@ struct ProbeLaunch {
 
 template <int QB>
 cudaError_t launch_probe_qb(const ProbeLaunch& a, cudaStream_t s) {
-    auto kern = ivf_probe_kernel<QB>;
-    const size_t smem = probe_smem(QB, a.dp, a.nlist);
+    auto kern = ivf_probe_score_kernel<QB>;
+    const size_t smem = probe_smem(QB, a.dp);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    kern<<<(a.nq + QB - 1) / QB, kProbeThreads, smem, s>>>(a.queries, a.nq, a.ds, a.dp, a.cent_t, a.ct_stride, a.nlist,
-                                                          a.np, a.offsets, a.probes, a.list_cnt, a.q_slot_off,
-                                                          a.counters);
+    const dim3 grid((a.nq + QB - 1) / QB, (a.nlist + kProbeThreads - 1) / kProbeThreads);
+    kern<<<grid, kProbeThreads, smem, s>>>(a.queries, a.nq, a.ds, a.dp, a.cent_t, a.ct_stride, a.nlist, a.scores);
     return cudaGetLastError();
 }
 
-// Probe + plan of n queries: three launches (probe with its counts, the plan's scans, the pairs).
+// Probe + plan of n queries: four launches (centroid scores, the selection with its counts, the
+// plan's scans, the pairs).
 cudaError_t launch_probe_plan(uint32_t pqb, const ProbeLaunch& a, uint32_t qb, IvfScratch& w, uint32_t* qblock_off,
                               cudaStream_t s) {
+    if ((a.nlist + kProbeThreads - 1) / kProbeThreads > 65535u) return cudaErrorInvalidValue;
     cudaError_t e;
     switch (pqb) {
         case 8: e = launch_probe_qb<8>(a, s); break;
@@ -637,11 +642,13 @@ cudaError_t launch_probe_plan(uint32_t pqb, const ProbeLaunch& a, uint32_t qb, I
         default: return cudaErrorInvalidValue;
     }
     if (e != cudaSuccess) return e;
+    ivf_probe_select_kernel<<<(a.nq + 7) / 8, 256, 0, s>>>(a.scores, a.nq, a.nlist, a.np, a.offsets, a.probes,
+                                                           a.list_cnt, a.q_slot_off, a.counters);
     ivf_plan_scan_kernel<<<1, 1024, 0, s>>>(a.nq, a.nlist, a.offsets, qb, w.d_list_cnt, w.d_list_qoff, w.d_item_off,
                                             w.d_q_slot_off, w.d_counters, qblock_off);
     ivf_plan_fill_kernel<<<(a.nq + 7) / 8, 256, 0, s>>>(a.probes, a.nq, a.np, a.offsets, w.d_list_qoff, w.d_list_fill,
                                                          w.d_q_slot_off, w.d_list_q, w.d_list_slot);
-    count_launch(3);
+    count_launch(4);
     return cudaGetLastError();
 }
 
@@ -678,7 +685,7 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
     const size_t smem = ivf_scan_smem(qb, dq, cap);
     if (smem > ix.smem_optin)
         return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF scan needs %zu bytes of shared memory", smem);
-    const uint32_t pqb = probe_qb(ix.dp, nlist, ix.smem_optin);
+    const uint32_t pqb = probe_qb(ix.dp, ix.smem_optin);
     if (!pqb) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF probe shared memory above the limit");
     const uint64_t max_chunks = (v.max_list + kChunkRows - 1) / kChunkRows;
     int st;
@@ -687,6 +694,7 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
     uint64_t per_query = std::max<uint64_t>(1, static_cast<uint64_t>(np) * max_chunks * k * 8);
     uint32_t sub = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(nq, ws_budget / per_query)));
     if ((st = grow(w.d_probes, w.cap_probes, static_cast<size_t>(sub) * np, "IVF probe buffer"))) return st;
+    if ((st = grow(w.d_pscore, w.cap_pscore, static_cast<size_t>(sub) * nlist, "IVF probe buffer"))) return st;
     if ((st = grow(w.d_list_cnt, w.cap_list_cnt, nlist, "IVF plan buffer"))) return st;
     if ((st = grow(w.d_list_fill, w.cap_list_fill, nlist, "IVF plan buffer"))) return st;
     if ((st = grow(w.d_list_qoff, w.cap_list_qoff, nlist + 1, "IVF plan buffer"))) return st;
@@ -719,8 +727,9 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
         const float* qn = queries + static_cast<uint64_t>(q0) * ix.ds;
         cudaMemsetAsync(w.d_list_cnt, 0, nlist * sizeof(uint32_t), s);
         cudaMemsetAsync(w.d_list_fill, 0, nlist * sizeof(uint32_t), s);
-        const ProbeLaunch pl{qn, n, dq, static_cast<uint32_t>(ix.dp), nlist, np, v.d_cent_t, v.nlist_pad,
-                             v.d_offsets, w.d_probes, w.d_list_cnt, w.d_q_slot_off, w.d_counters};
+        const ProbeLaunch pl{qn,          n,          dq,           static_cast<uint32_t>(ix.dp), nlist, np,
+                             v.d_cent_t,  v.nlist_pad, v.d_offsets, w.d_pscore, w.d_probes, w.d_list_cnt,
+                             w.d_q_slot_off, w.d_counters};
         cudaError_t e = launch_probe_plan(pqb, pl, qb, w, nullptr, s);
         if (e != cudaSuccess) return cuda_error(e, "IVF probe launch");
         a.queries = qn;
@@ -738,7 +747,7 @@ int ivf_search(CudaIndex& ix, const float* queries, uint32_t nq, uint32_t k, uin
                                                                o_cnt ? o_cnt + q0 : nullptr);
         count_launch();
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "IVF merge launch");
-        ix.stats.kernel_launches += 5;
+        ix.stats.kernel_launches += 6;
     }
     if (!w.h_probed) bump_alloc_epoch();
     if (!w.h_probed && cudaMallocHost(&w.h_probed, 8 * sizeof(unsigned long long)) != cudaSuccess)
@@ -772,7 +781,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     const CudaIndex::TcPlan plan = ix.plan_tc(k, false), plan2 = ix.plan_tc(0, false);
     if (plan.kp < k || !plan.stages || !plan2.stages) return ivf_search(ix, ix.d_qn, nq, k, o_idx, o_sim, o_cnt, s);
     const uint32_t kp = plan.kp;
-    const uint32_t pqb = probe_qb(ix.dp, nlist, ix.smem_optin);
+    const uint32_t pqb = probe_qb(ix.dp, ix.smem_optin);
     if (!pqb) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: IVF probe shared memory above the limit");
     const uint64_t max_chunks = (v.max_list + kChunkRows - 1) / kChunkRows;
     const uint64_t pairs = static_cast<uint64_t>(nq) * np;
@@ -784,6 +793,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     const uint32_t cap2 = kSecondPassCap;
     int st;
     if ((st = grow(w.d_probes, w.cap_probes, pairs, "IVF probe buffer"))) return st;
+    if ((st = grow(w.d_pscore, w.cap_pscore, static_cast<size_t>(nq) * nlist, "IVF probe buffer"))) return st;
     if ((st = grow(w.d_list_cnt, w.cap_list_cnt, nlist, "IVF plan buffer"))) return st;
     if ((st = grow(w.d_list_fill, w.cap_list_fill, nlist, "IVF plan buffer"))) return st;
     if ((st = grow(w.d_list_qoff, w.cap_list_qoff, nlist + 1, "IVF plan buffer"))) return st;
@@ -818,8 +828,9 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     cudaMemsetAsync(w.d_counters, 0, 8 * sizeof(unsigned long long), s);
     cudaMemsetAsync(w.d_list_cnt, 0, nlist * sizeof(uint32_t), s);
     cudaMemsetAsync(w.d_list_fill, 0, nlist * sizeof(uint32_t), s);
-    const ProbeLaunch pl{ix.d_qn, nq, static_cast<uint32_t>(ix.ds), static_cast<uint32_t>(ix.dp), nlist, np,
-                         v.d_cent_t, v.nlist_pad, v.d_offsets, w.d_probes, w.d_list_cnt, w.d_q_slot_off, w.d_counters};
+    const ProbeLaunch pl{ix.d_qn,   nq,          static_cast<uint32_t>(ix.ds), static_cast<uint32_t>(ix.dp),
+                         nlist,      np,          v.d_cent_t,  v.nlist_pad, v.d_offsets, w.d_pscore, w.d_probes,
+                         w.d_list_cnt, w.d_q_slot_off, w.d_counters};
     cudaError_t e = launch_probe_plan(pqb, pl, 128, w, w.d_qblock_off, s);
     if (e != cudaSuccess) return cuda_error(e, "IVF probe launch");
     ivf_gather_tc_kernel<<<nlist, 256, 0, s>>>(ix.d_q_bf16, static_cast<uint32_t>(v.kb16), w.d_list_cnt, w.d_list_qoff,
@@ -918,7 +929,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     cudaMemcpyAsync(w.h_probed, w.d_counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(ix.h_fbn, ix.d_fbn, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     ix.last_tc_n = nq;
-    ix.stats.kernel_launches += 12;
+    ix.stats.kernel_launches += 13;
     ix.stats.path = 5;
     ix.stats.nprobe = np;
     ix.stats.rerank_width = kp;
