@@ -857,6 +857,7 @@ def run_ivf(args, dev, L, world):
             "path": "tensor-core list scan" if stats.path == 5 else "FP32 list scan",
             "second_pass_queries": stats.second_pass_queries,
             "pass2_rows_per_query": stats.pass2_rows / stats.second_pass_queries if stats.second_pass_queries else 0.0,
+            "pass1_tile_stride": int(stats.pass1_tile_stride) if tc else None,
             "fp32_fallback_queries": stats.fp32_fallback_queries,
             "queries_per_s": total_q / (max_ms / 1e3),
             "ms_per_batch": max_ms / args.ivf_steps,

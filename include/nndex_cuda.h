@@ -264,7 +264,8 @@ NNDEX_API int nndex_cuda_search_batch_device(nndex_cuda_index* index, const floa
 NNDEX_API int nndex_cuda_set_precision(nndex_cuda_index* index, uint32_t precision, uint32_t rerank_width);
 
 /*
- * Candidates of the last low-precision search on this index (diagnostics and error reports):
+ * Candidates of the last exact low-precision search on this index (paths 2, 3 and 6; diagnostics
+ * and error reports):
  * for each of `query_rows` queries, the k' rows ranked by approximate (BF16/FP8) score, with those
  * approximate scores, the bound eps the exactness certificate used for this index's copy (max row
  * residual) and, per query, whether its certificate held (0 = re-run on the FP32 scan). Host

@@ -273,6 +273,8 @@ CudaIndex::~CudaIndex() {
     cudaFree(d_fb_sim);
     cudaFree(d_fb_cnt);
     cudaFree(d_kth);
+    cudaFree(d_floor);
+    cudaFree(d_rslots);
     cudaFree(d_ids);
     cudaFree(d_q2_lp);
     cudaFree(d_q2_resid);
@@ -730,6 +732,9 @@ int CudaIndex::enqueue_tc_pass2(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o
     if ((st = grow_device(d_cnt2, cap_cnt2, n, "pass-2 buffer"))) return st;
     if ((st = grow_device(d_ok2, cap_ok2, n, "pass-2 buffer"))) return st;
     if ((st = grow_device(d_tcfail, cap_tcfail, n, "pass-2 buffer"))) return st;
+    if ((st = grow_device(d_rslots, cap_rslots, static_cast<uint64_t>(n) * rerank_chunks(cap2) * kcap,
+                          "pass-2 buffer")))
+        return st;
     uint32_t* d_m = d_fbn + 1;      // uncertified queries
     uint32_t* d_fail = d_fbn + 2;   // of them, collections that overflowed
     launch_compact_zero_flags(d_cert, n, d_ids, d_m, s);
@@ -777,10 +782,10 @@ int CudaIndex::enqueue_tc_pass2(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o
     scan_event_end(s, ev_a);
     if (e != cudaSuccess) return cuda_error(e, "tensor-core scan launch (pass 2)");
     e = launch_rerank_collected(d_base, static_cast<uint32_t>(ds), d_qn, d_ids, n, d_rows2, d_cnt2, cap2, kcap,
-                                d_q2_thr, o_idx, o_sim, o_cnt, d_ok2, s, false, d_m);
+                                d_q2_thr, d_rslots, o_idx, o_sim, o_cnt, d_ok2, s, false, d_m);
     if (e != cudaSuccess) return cuda_error(e, "rerank launch (pass 2)");
     launch_compact_zero_flags(d_ok2, n, d_tcfail, d_fail, s, d_m);
-    stats.kernel_launches += 5;
+    stats.kernel_launches += 6;
     last_tc_n = n;
     return NNDEX_OK;
 }
@@ -867,9 +872,6 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     const uint64_t fb_per_query = static_cast<uint64_t>(fb_plan.ctas_per_group) * kcap;
     if ((st = grow_device(d_ws, cap_ws, std::max(per_query, fb_per_query) * n, "scan workspace"))) return st;
     if ((st = grow_device(d_qsub, cap_qsub, static_cast<uint64_t>(n) * ds, "fallback buffer"))) return st;
-    if ((st = grow_device(d_fb_idx, cap_fb_idx, static_cast<uint64_t>(n) * kcap, "fallback buffer"))) return st;
-    if ((st = grow_device(d_fb_sim, cap_fb_sim, static_cast<uint64_t>(n) * kcap, "fallback buffer"))) return st;
-    if ((st = grow_device(d_fb_cnt, cap_fb_cnt, n, "fallback buffer"))) return st;
     if ((st = grow_device(d_fbq, cap_fbq, n, "fallback buffer"))) return st;
     if (!d_fbn) {
         cudaError_t e0;
@@ -882,6 +884,7 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     if ((st = grow_device(d_cand_cnt, cap_cand_cnt, n, "tc workspace"))) return st;
     if ((st = grow_device(d_cert, cap_cert, n, "tc workspace"))) return st;
     if ((st = grow_device(d_kth, cap_kth, n, "tc workspace"))) return st;
+    if ((st = grow_device(d_floor, cap_floor, n, "tc workspace"))) return st;
     // The queries straight from the prepared buffer: rows past n read as zeros.
     CUtensorMap tmap_q;
     if (!encode_tmap_2d(&tmap_q, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, d_qn, ds, n, ds * sizeof(float), 32, 16,
@@ -900,7 +903,9 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     a.c_norm = tf32_c_norm();
     a.evict_first = n <= 16;
     a.ws_keys = d_ws;
+    a.floor_keys = d_floor;
     a.status = d_status;
+    cudaMemsetAsync(d_floor, 0, n * sizeof(unsigned long long), s);
     cudaEvent_t ev_a = nullptr;
     scan_event_begin(s, ev_a);
     cudaError_t e = launch_scan_tf32(tmap_f32, tmap_q, a, plan.stages, ctas, s);
@@ -915,6 +920,7 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     m.idx_out = d_cand_idx;
     m.sim_out = d_cand_sim;
     m.count_out = d_cand_cnt;
+    m.floor_keys = d_floor;
     if ((st = merge_workspace(per_query, n, kp, m, s))) return st;
     if ((e = launch_merge_topk(m, s)) != cudaSuccess) return cuda_error(e, "merge launch");
     RerankArgs r;
@@ -933,10 +939,13 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     r.cert_out = d_cert;
     r.kth_out = d_kth;
     r.certify = true;
+    r.fb_ids = d_fbq;
+    r.fb_count = d_fbn;
+    cudaMemsetAsync(d_fbn, 0, sizeof(uint32_t), s);
     if ((e = launch_rerank(r, s)) != cudaSuccess) return cuda_error(e, "rerank launch");
-    // Uncertified queries re-run on the FP32 scan, on the device: compaction, gather, the scan and
-    // its merge (both return at once when every query certified), scatter into the outputs.
-    launch_compact_zero_flags(d_cert, n, d_fbq, d_fbn, s);
+    // Uncertified queries re-run on the FP32 scan, on the device: the rerank listed them, then a
+    // gather, the scan and its merge (all return at once when every query certified), the merge
+    // writing each result into the query's own output row.
     launch_gather_rows(d_qn, static_cast<uint32_t>(ds), d_fbq, d_fbn, n, d_qsub, s);
     ScanArgs fa;
     fa.tmap = &tmap_f32;
@@ -957,17 +966,17 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     fm.per_query = fb_per_query;
     fm.k = kcap;
     fm.out_stride = kcap;
-    fm.idx_out = d_fb_idx;
-    fm.sim_out = d_fb_sim;
-    fm.count_out = d_fb_cnt;
+    fm.idx_out = o_idx;
+    fm.sim_out = o_sim;
+    fm.count_out = o_cnt;
     fm.live = d_fbn;
+    fm.out_rows = d_fbq;
     if ((st = merge_workspace(fb_per_query, n, kcap, fm, s))) return st;
     if ((e = launch_merge_topk(fm, s)) != cudaSuccess) return cuda_error(e, "fallback merge launch");
-    launch_scatter_results(d_fb_idx, d_fb_sim, d_fb_cnt, d_fbq, d_fbn, n, kcap, o_idx, o_sim, o_cnt, s);
     last_tc_n = n;
     fbn_stream = s;
     fbn_pending = true;
-    stats.kernel_launches += 8;
+    stats.kernel_launches += 6;
     stats.path = 6;
     stats.rerank_width = kp;
     stats.rows_scanned += rows * n;
@@ -1944,6 +1953,9 @@ int nndex_cuda_last_candidates(nndex_cuda_index* index, uint64_t query_rows, uin
     if (eps_rows)
         *eps_rows = ix->stats.path == 3 ? ix->eps_fp8 : ix->stats.path == 6 ? ix->tf32_eps() : ix->eps_bf16;
     if (kp == 0 || !ix->d_cand_idx) return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: no low-precision search yet");
+    if (ix->stats.path == 5)
+        return set_error(NNDEX_ERR_UNSUPPORTED,
+                         "cuda execution error: the IVF list scan's candidates are list positions, not exported");
     const uint64_t n = query_rows * kp;
     if (n > capacity || n > ix->cap_cand_idx)
         return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: candidate buffer too small");

@@ -118,6 +118,10 @@ struct CudaIndex {
     uint32_t forced_qb = 0;         // the tuned plan's pass-2 query blocks per CTA (0 = rule)
     uint32_t last_tc_stride = 1;
     float* d_kth = nullptr;  // pass 1: exact k-th score per query
+    unsigned long long* d_floor = nullptr;  // TF32 scan: per query, a key its k'-th candidate reaches
+    size_t cap_floor = 0;
+    uint64_t* d_rslots = nullptr;  // pass 2: each rerank work item's best k keys
+    size_t cap_rslots = 0;
     size_t cap_kth = 0;
     // pass 2 (threshold collection) buffers
     uint32_t* d_ids = nullptr;

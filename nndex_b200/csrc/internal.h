@@ -89,6 +89,10 @@ struct MergeArgs {
     uint64_t* part_keys = nullptr;
     uint32_t* part_done = nullptr;
     const uint32_t* live = nullptr;     // optional: a device count; queries at or past it are skipped
+    // optional, per query: a key the k-th best is known to reach (the scan's largest full-list
+    // minimum); smaller keys are dropped before the selection
+    const unsigned long long* floor_keys = nullptr;
+    const uint32_t* out_rows = nullptr;  // optional: query q's results go to output row out_rows[q]
 };
 uint32_t merge_parts(uint64_t per_query, uint32_t k);
 cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream);
@@ -166,6 +170,10 @@ struct Tf32ScanArgs {
     float c_norm = 0.0f;               // C of ε: accumulation and rounding terms per unit ‖q‖‖x‖
     bool evict_first = true;           // L2 policy of the base loads (one query block: stream once)
     uint64_t* ws_keys = nullptr;       // nq × ctas × kp
+    // optional, nq keys zeroed before the launch: the largest over CTAs of the smallest key of a
+    // full (kp-key) list. Every row a CTA did not list has a smaller key than its list's smallest,
+    // so the global kp-th key reaches it.
+    unsigned long long* floor_keys = nullptr;
     uint32_t* status = nullptr;
 };
 size_t tf32_smem_bytes(uint32_t stages, uint32_t cap);
@@ -189,7 +197,7 @@ void launch_scatter_results(const uint64_t* fb_idx, const float* fb_sim, const u
                             cudaStream_t s);
 
 struct RerankArgs {
-    const float* base = nullptr;  // FP32 base, stride ds
+    const float* base = nullptr;  // FP32 base, stride ds (with row_map: the list-ordered copy)
     uint32_t ds = 0;
     const float* queries = nullptr;  // FP32 normalised queries, stride ds
     const uint64_t* cand_idx = nullptr;  // nq × kp, sorted by upper bound
@@ -202,18 +210,26 @@ struct RerankArgs {
     uint32_t* cert_out = nullptr;
     float* kth_out = nullptr;            // exact k-th score per query (pass-2 threshold)
     bool certify = true;                 // false when pass 1 scanned a sample of the rows
+    // optional: an uncertified query appends its index to fb_ids at fb_count[0] (zeroed before)
+    uint32_t* fb_ids = nullptr;
+    uint32_t* fb_count = nullptr;
+    // optional (IVF): candidates are list positions; base is read by position, results carry
+    // row_map[position]
+    const uint32_t* row_map = nullptr;
 };
 cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream);
 // q2_lp holds m rounded up to 128 rows (whole query blocks); the rows past m are written as zeros.
 cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q_lp, uint32_t row_bytes, void* q2_lp,
                                   const float* resid, float* resid2, const float* scale, float* scale2,
                                   const float* kth, float* thr2, cudaStream_t stream, const uint32_t* live = nullptr);
-// Pass 2's exact rerank. thr: each query's T (indexed like cnt2). vecs: the base by row, or with
-// row_map (IVF) the list-ordered copy by collected position.
+// Pass 2's exact rerank (two launches: work items of collected rows, then a merge per query).
+// thr: each query's T (indexed like cnt2). vecs: the base by row, or with row_map (IVF) the
+// list-ordered copy by collected position. slot_keys: m × rerank_chunks(cap2) × k keys of scratch.
+uint32_t rerank_chunks(uint32_t cap2);
 cudaError_t launch_rerank_collected(const float* vecs, uint32_t ds, const float* queries, const uint32_t* ids,
                                     uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
-                                    const float* thr, uint64_t* idx_out, float* sim_out, uint32_t* cnt_out,
-                                    uint32_t* ok_out, cudaStream_t stream, bool by_query = false,
+                                    const float* thr, uint64_t* slot_keys, uint64_t* idx_out, float* sim_out,
+                                    uint32_t* cnt_out, uint32_t* ok_out, cudaStream_t stream, bool by_query = false,
                                     const uint32_t* live = nullptr, const uint32_t* row_map = nullptr);
 cudaError_t launch_max_reduce(const float* v, uint64_t n, unsigned int* out, cudaStream_t stream);
 // FP8: {min, max} row scale of each 256-row tile (tiles = rows_alloc / 256).

@@ -461,7 +461,8 @@ __global__ void __launch_bounds__(512)
     __syncthreads();
     uint32_t local = 0;
     for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) local += keys[i] != 0ull;
-    atomicAdd(&s.count, local);
+    local = __reduce_add_sync(0xffffffffu, local);
+    if (lane_id() == 0) atomicAdd(&s.count, local);
     __syncthreads();
     const uint32_t nvalid = s.count;
     const uint32_t kk = nvalid < k ? nvalid : k;
@@ -473,12 +474,12 @@ __global__ void __launch_bounds__(512)
         if (n > kk) kth = block_radix_kth(keys, n, kk, s);
         if (threadIdx.x == 0) s.count = 0;
         __syncthreads();
-        for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
-            const uint64_t key = keys[i];
-            if (key != 0ull && key >= kth) {
-                const uint32_t pos = atomicAdd(&s.count, 1u);
-                if (pos < kk) sorted[pos] = key;
-            }
+        for (uint64_t i0 = 0; i0 < n; i0 += blockDim.x) {
+            const uint64_t i = i0 + threadIdx.x;
+            const uint64_t key = i < n ? keys[i] : 0ull;
+            const bool take = key != 0ull && key >= kth;
+            const uint32_t pos = warp_append(&s.count, take);
+            if (take && pos < kk) sorted[pos] = key;
         }
         __syncthreads();
         // Exactly kk keys reach the k-th (keys are distinct); should fewer arrive, the slots they
@@ -819,6 +820,8 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     if ((st = grow(ix.d_cnt2, ix.cap_cnt2, nq, "pass-2 buffer"))) return st;
     if ((st = grow(ix.d_ok2, ix.cap_ok2, nq, "pass-2 buffer"))) return st;
     if ((st = grow(ix.d_tcfail, ix.cap_tcfail, nq, "pass-2 buffer"))) return st;
+    if ((st = grow(ix.d_rslots, ix.cap_rslots, static_cast<size_t>(nq) * rerank_chunks(cap2) * k, "pass-2 buffer")))
+        return st;
     if ((st = ix.ensure_fbn())) return st;
     if (!w.h_probed) bump_alloc_epoch();
     if (!w.h_probed && cudaMallocHost(&w.h_probed, 8 * sizeof(unsigned long long)) != cudaSuccess)
@@ -883,7 +886,8 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
                                                             ix.d_cand_cnt);
     count_launch();
     RerankArgs r;
-    r.base = ix.d_base;
+    r.base = v.d_reordered;  // the slot keys hold list positions
+    r.row_map = v.d_row_map;
     r.ds = static_cast<uint32_t>(ix.ds);
     r.queries = ix.d_qn;
     r.cand_idx = ix.d_cand_idx;
@@ -921,15 +925,15 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     ix.scan_event_end(s, ev_a);
     if (e != cudaSuccess) return cuda_error(e, "IVF tensor-core scan launch (pass 2)");
     e = launch_rerank_collected(v.d_reordered, static_cast<uint32_t>(ix.ds), ix.d_qn, ix.d_ids, nq, ix.d_rows2,
-                                ix.d_cnt2, cap2, k, ix.d_q2_thr, o_idx, o_sim, o_cnt, ix.d_ok2, s, true, d_m,
-                                v.d_row_map);
+                                ix.d_cnt2, cap2, k, ix.d_q2_thr, ix.d_rslots, o_idx, o_sim, o_cnt, ix.d_ok2, s, true,
+                                d_m, v.d_row_map);
     if (e != cudaSuccess) return cuda_error(e, "rerank launch (pass 2)");
     launch_compact_zero_flags(ix.d_ok2, nq, ix.d_tcfail, d_fail, s, d_m);
     // the plan's totals and the pass counts come back with the results
     cudaMemcpyAsync(w.h_probed, w.d_counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(ix.h_fbn, ix.d_fbn, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     ix.last_tc_n = nq;
-    ix.stats.kernel_launches += 13;
+    ix.stats.kernel_launches += 14;
     ix.stats.path = 5;
     ix.stats.nprobe = np;
     ix.stats.rerank_width = kp;

@@ -298,7 +298,8 @@ NNDEX_DEVICE_INLINE void merge_final(const uint64_t* keys, uint64_t n, uint32_t 
     __syncthreads();
     uint32_t local = 0;
     for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) local += keys[i] != 0ull;
-    atomicAdd(&s.count, local);
+    local = __reduce_add_sync(0xffffffffu, local);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(&s.count, local);
     __syncthreads();
     const uint32_t nvalid = s.count;
     const uint32_t kk = nvalid < k ? nvalid : k;
@@ -310,12 +311,12 @@ NNDEX_DEVICE_INLINE void merge_final(const uint64_t* keys, uint64_t n, uint32_t 
         if (n > kk) kth = block_radix_kth(keys, n, kk, s);
         if (threadIdx.x == 0) s.count = 0;
         __syncthreads();
-        for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
-            const uint64_t key = keys[i];
-            if (key != 0ull && key >= kth) {
-                const uint32_t pos = atomicAdd(&s.count, 1u);
-                if (pos < kk) sorted[pos] = key;
-            }
+        for (uint64_t i0 = 0; i0 < n; i0 += blockDim.x) {
+            const uint64_t i = i0 + threadIdx.x;
+            const uint64_t key = i < n ? keys[i] : 0ull;
+            const bool take = key != 0ull && key >= kth;
+            const uint32_t pos = warp_append(&s.count, take);
+            if (take && pos < kk) sorted[pos] = key;
         }
         __syncthreads();
         // Exactly kk keys reach the k-th (keys are distinct); should fewer arrive, the slots they
@@ -354,7 +355,9 @@ __global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restr
                                                          uint32_t* __restrict__ count_out, uint32_t parts,
                                                          uint64_t* __restrict__ part_keys,
                                                          uint32_t* __restrict__ part_done,
-                                                         const uint32_t* __restrict__ live) {
+                                                         const uint32_t* __restrict__ live,
+                                                         const unsigned long long* __restrict__ floor_keys,
+                                                         const uint32_t* __restrict__ out_rows) {
     if (live && blockIdx.y >= *live) return;  // a fallback merge: only the queries re-run
     __shared__ BlockSelectScratch s;
     __shared__ uint32_t last;
@@ -363,8 +366,9 @@ __global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restr
     const uint64_t* keys = ws_keys + static_cast<size_t>(q) * per_query;
     uint32_t p2 = 1;
     while (p2 < k) p2 <<= 1;
+    const uint32_t oq = out_rows ? out_rows[q] : q;  // the output row of this query's results
     if (parts == 1) {
-        merge_final(keys, per_query, k, q, out_stride, idx_out, sim_out, count_out, s, smem_keys);
+        merge_final(keys, per_query, k, oq, out_stride, idx_out, sim_out, count_out, s, smem_keys);
         return;
     }
     // This block's share: lists [l0, l1) of k keys each.
@@ -373,20 +377,43 @@ __global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restr
     const uint64_t n = (l1 - l0) * k;
     const uint64_t* src = keys + l0 * k;
     uint64_t* dst = part_keys + (static_cast<size_t>(q) * parts + blockIdx.x) * k;
-    uint64_t kth = 0ull;
-    if (n > k) kth = block_radix_kth(src, n, k, s);
-    if (threadIdx.x == 0) s.count = 0;
-    __syncthreads();
-    // Non-empty keys >= kth: exactly k of them when the share holds at least k (keys are distinct);
-    // all of them otherwise (kth is then an empty slot, 0). The rest of the part is padded with 0.
-    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint64_t key = src[i];
-        if (key != 0ull && key >= kth) {
-            const uint32_t pos = atomicAdd(&s.count, 1u);
-            if (pos < k) dst[pos] = key;
+    // With a floor (a key the query's k-th best reaches), one pass keeps the share's keys at or
+    // above it; when no more than k remain they are the share's candidates, with no selection.
+    bool kept = false;
+    if (floor_keys) {
+        const uint64_t fl = floor_keys[q];
+        if (threadIdx.x == 0) s.count = 0;
+        __syncthreads();
+        if (fl) {
+            for (uint64_t i0 = 0; i0 < n; i0 += blockDim.x) {
+                const uint64_t i = i0 + threadIdx.x;
+                const uint64_t key = i < n ? src[i] : 0ull;
+                const bool take = i < n && key >= fl;
+                const uint32_t pos = warp_append(&s.count, take);
+                if (take && pos < k) dst[pos] = key;
+            }
         }
+        __syncthreads();
+        kept = fl && s.count <= k;
+        __syncthreads();
     }
-    __syncthreads();
+    if (!kept) {
+        uint64_t kth = 0ull;
+        if (n > k) kth = block_radix_kth(src, n, k, s);
+        if (threadIdx.x == 0) s.count = 0;
+        __syncthreads();
+        // Non-empty keys >= kth: exactly k of them when the share holds at least k (keys are
+        // distinct); all of them otherwise (kth is then an empty slot, 0). The rest of the part is
+        // padded with 0.
+        for (uint64_t i0 = 0; i0 < n; i0 += blockDim.x) {
+            const uint64_t i = i0 + threadIdx.x;
+            const uint64_t key = i < n ? src[i] : 0ull;
+            const bool take = key != 0ull && key >= kth;
+            const uint32_t pos = warp_append(&s.count, take);
+            if (take && pos < k) dst[pos] = key;
+        }
+        __syncthreads();
+    }
     for (uint32_t j = s.count + threadIdx.x; j < k; j += blockDim.x) dst[j] = 0ull;
     // Publish the part; the last block of this query merges them.
     __threadfence();
@@ -395,11 +422,21 @@ __global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restr
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // the parts' non-empty keys, packed (their order does not matter to the selection)
     uint64_t* staged = smem_keys + p2;
     const uint64_t* all = part_keys + static_cast<size_t>(q) * parts * k;
-    for (uint32_t i = threadIdx.x; i < parts * k; i += blockDim.x) staged[i] = __ldcg(all + i);
+    if (threadIdx.x == 0) s.count = 0;
     __syncthreads();
-    merge_final(staged, static_cast<uint64_t>(parts) * k, k, q, out_stride, idx_out, sim_out, count_out, s, smem_keys);
+    for (uint32_t i0 = 0; i0 < parts * k; i0 += blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        const uint64_t key = i < parts * k ? __ldcg(all + i) : 0ull;
+        const uint32_t pos = warp_append(&s.count, key != 0ull);
+        if (key != 0ull) staged[pos] = key;
+    }
+    __syncthreads();
+    const uint32_t m = s.count;
+    __syncthreads();
+    merge_final(staged, m, k, oq, out_stride, idx_out, sim_out, count_out, s, smem_keys);
     if (threadIdx.x == 0) part_done[q] = 0;  // ready for the next launch
 }
 
@@ -662,7 +699,7 @@ cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream) {
     }
     merge_topk_kernel<<<dim3(parts, a.nq), 512, smem, stream>>>(a.ws_keys, a.per_query, a.k, a.out_stride, a.idx_out,
                                                                 a.sim_out, a.count_out, parts, a.part_keys,
-                                                                a.part_done, a.live);
+                                                                a.part_done, a.live, a.floor_keys, a.out_rows);
     count_launch();
     return cudaGetLastError();
 }

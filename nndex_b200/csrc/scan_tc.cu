@@ -387,6 +387,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         const float rq = valid_q ? p.q_resid[q] : 0.0f;
         const float b_mul = 1.0f + rq, b_add = rq + p.eps_acc;
         const float slack = fmaf(p.eps_rows, b_mul, b_add);  // the largest u_r − s̃_r over all rows
+        const bool per_row_bound = p.tile_stride == 1;
         EpiState st;
         st.n = 0;
         if (kMode == 0) {
@@ -475,8 +476,11 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
                     }
                     float s = pick(v, j);
                     if (kFp8) s = (s * sc[c * 32 + j]) * qs;
-                    const float u = fmaf(p.row_resid[row], b_mul, s + b_add);
-                    epi_survivor<kMode>(p, st, heap, lrow, q, u, kItems ? p.row_map[row] : row, slack);
+                    // The row's own bound when pass 1 may certify (every tile scanned); a sampled
+                    // pass 1 only yields T, and the largest slack spares a dependent load per
+                    // survivor. In item mode the key holds the list position (the rerank maps it).
+                    const float u = per_row_bound ? fmaf(p.row_resid[row], b_mul, s + b_add) : s + slack;
+                    epi_survivor<kMode>(p, st, heap, lrow, q, u, row, slack);
                 }
             };
 #pragma unroll
@@ -573,7 +577,8 @@ __global__ void __launch_bounds__(1024, 1)
                   const uint64_t* __restrict__ cand_idx, const float* __restrict__ cand_bound,
                   const uint32_t* __restrict__ cand_cnt, uint32_t kp, uint32_t k, uint64_t* __restrict__ idx_out,
                   float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out, uint32_t* __restrict__ cert_out,
-                  float* __restrict__ kth_out, int certify) {
+                  float* __restrict__ kth_out, int certify, uint32_t* __restrict__ fb_ids,
+                  uint32_t* __restrict__ fb_count, const uint32_t* __restrict__ row_map) {
     extern __shared__ uint64_t keys[];
     const uint32_t q = blockIdx.x;
     const uint32_t ch = threadIdx.x & 7u, slot = threadIdx.x >> 3;  // 8 lanes per candidate
@@ -586,9 +591,10 @@ __global__ void __launch_bounds__(1024, 1)
     for (uint32_t j0 = 0; j0 < p2; j0 += nslots) {
         const uint32_t j = j0 + slot;
         const bool live = j < n;
-        const uint64_t row = live ? cand_idx[static_cast<size_t>(q) * kp + j] : 0;
-        const float acc = dot_scan_order<4>(base + row * ds, qv, nbox, ch, live);
-        if (ch == 0 && j < p2) keys[j] = live ? make_key(acc, static_cast<uint32_t>(row)) : 0ull;
+        const uint64_t cand = live ? cand_idx[static_cast<size_t>(q) * kp + j] : 0;
+        const uint32_t row = row_map && live ? row_map[cand] : static_cast<uint32_t>(cand);
+        const float acc = dot_scan_order<4>(base + cand * ds, qv, nbox, ch, live);
+        if (ch == 0 && j < p2) keys[j] = live ? make_key(acc, row) : 0ull;
     }
     __syncthreads();
     block_bitonic_sort_desc(keys, p2);
@@ -605,6 +611,7 @@ __global__ void __launch_bounds__(1024, 1)
         if (certify && n >= kp && kk > 0)
             ok = key_score(keys[kk - 1]) > cand_bound[static_cast<size_t>(q) * kp + kp - 1] ? 1u : 0u;
         cert_out[q] = ok;
+        if (fb_count && !ok) fb_ids[atomicAdd(fb_count, 1u)] = q;  // for the FP32 scan
         // T: the exact k-th score among the candidates, a lower bound of the true k-th; with fewer
         // than k candidates (a sampled pass 1 over few rows) there is no bound.
         kth_out[q] = kk == k ? key_score(keys[kk - 1]) : -INFINITY;
@@ -640,79 +647,105 @@ __global__ void gather_queries_kernel(const uint32_t* __restrict__ ids, uint32_t
     }
 }
 
-// Scores of one round that the block keeps in shared memory beside the carried best k.
-constexpr uint32_t kRerankRound = 2048;
+// Pass 2's exact rerank runs as work items of up to kRerankChunk collected rows, so that a query
+// with thousands of collected rows is spread over many blocks instead of one.
+constexpr uint32_t kRerankChunk = 512;
 
-// One block per uncertified query: re-scores its collected rows exactly (the FP32 scan's order) and
-// writes their top-k. Only rows whose exact score reaches T (the exact k-th score of pass 1, a lower
-// bound of the true k-th) can be in the top-k, and the k rows that gave T are among the collected
-// ones, so only those rows are kept; when more than a round of them accumulate, the best k are
-// selected and the round starts over. `vecs` holds the vectors: the base by row, or (IVF) the
-// list-ordered copy by collected position.
+// Keeps the best kk of keys[0, m) (distinct) in keys[0, kk), in no particular order.
+NNDEX_DEVICE_INLINE void block_keep_best(uint64_t* keys, uint32_t m, uint32_t kk, BlockSelectScratch& sel) {
+    const uint64_t kth = block_radix_kth(keys, m, kk, sel);
+    if (threadIdx.x == 0) sel.count = 0;
+    __syncthreads();
+    for (uint32_t j0 = 0; j0 < m; j0 += blockDim.x) {
+        const uint32_t j = j0 + threadIdx.x;
+        const uint64_t key = j < m ? keys[j] : 0ull;
+        __syncthreads();
+        const bool take = j < m && key >= kth;
+        const uint32_t pos = warp_append(&sel.count, take);
+        if (take) keys[pos] = key;  // pos ≤ j: never overwrites a key not yet read
+        __syncthreads();
+    }
+}
+
+// Work item (i, c): rows [c·kRerankChunk, (c + 1)·kRerankChunk) of the collection of uncertified
+// query i (ids[i]), re-scored exactly in the FP32 scan's order. Only rows whose exact score reaches T
+// (the exact k-th score of pass 1, a lower bound of the true k-th) can be in the top-k, and the k
+// rows that gave T are among the collected ones, so only those are kept; the item's best k of them
+// go to its slot. `vecs` holds the vectors: the base by row, or (IVF) the list-ordered copy by
+// collected position. Items past a query's collection (or of an overflowed one) return at once.
 __global__ void __launch_bounds__(256)
-    rerank_collected_kernel(const float* __restrict__ vecs, uint32_t ds, const float* __restrict__ queries,
-                            const uint32_t* __restrict__ ids, const uint32_t* __restrict__ rows2,
-                            const uint32_t* __restrict__ cnt2, uint32_t cap2, uint32_t k, uint64_t* __restrict__ idx_out,
-                            float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out,
-                            uint32_t* __restrict__ ok_out, int by_query, const uint32_t* __restrict__ live,
-                            const uint32_t* __restrict__ row_map, const float* __restrict__ thr) {
-    extern __shared__ uint64_t keys[];  // kRerankRound + (k rounded up to a power of two)
+    rerank_chunk_kernel(const float* __restrict__ vecs, uint32_t ds, const float* __restrict__ queries,
+                        const uint32_t* __restrict__ ids, const uint32_t* __restrict__ rows2,
+                        const uint32_t* __restrict__ cnt2, uint32_t cap2, uint32_t k, int by_query,
+                        const uint32_t* __restrict__ live, const uint32_t* __restrict__ row_map,
+                        const float* __restrict__ thr, uint64_t* __restrict__ slot_keys) {
+    __shared__ uint64_t keys[kRerankChunk];
     __shared__ BlockSelectScratch sel;
     __shared__ uint32_t fill;
-    const uint32_t i = blockIdx.x;
+    const uint32_t i = blockIdx.x, c = blockIdx.y;
     if (live && i >= *live) return;
     const uint32_t q = ids[i];
     const uint32_t qrow = by_query ? q : i;  // collected rows and T indexed by query, or by position in ids
     const uint32_t total = cnt2[qrow];
-    if (total > cap2) {  // the collected set overflowed: this query goes to the FP32 scan
-        if (threadIdx.x == 0) ok_out[i] = 0;
-        return;
-    }
-    const uint32_t n = total;
+    const uint32_t j_begin = c * kRerankChunk;
+    if (total > cap2 || j_begin >= total) return;
+    const uint32_t j_end = (total - j_begin) < kRerankChunk ? total : j_begin + kRerankChunk;
     const float t = thr[qrow];
     const uint32_t ch = threadIdx.x & 7u, slot = threadIdx.x >> 3, nslots = blockDim.x >> 3;
     const float* qv = queries + static_cast<size_t>(q) * ds;
     const uint32_t nbox = ds / 32;
-    uint32_t p2k = 1;
-    while (p2k < k) p2k <<= 1;
-    const uint32_t capacity = kRerankRound + p2k;
     if (threadIdx.x == 0) fill = 0;
     __syncthreads();
-    // keeps the best kk of keys[0, m) in keys[0, kk) (order not yet defined)
-    auto keep_best = [&](uint32_t m, uint32_t kk) {
-        const uint64_t kth = block_radix_kth(keys, m, kk, sel);
-        if (threadIdx.x == 0) sel.count = 0;
-        __syncthreads();
-        for (uint32_t j0 = 0; j0 < m; j0 += blockDim.x) {
-            const uint32_t j = j0 + threadIdx.x;
-            const uint64_t key = j < m ? keys[j] : 0ull;
-            __syncthreads();
-            if (j < m && key >= kth) {
-                const uint32_t pos = atomicAdd(&sel.count, 1u);
-                keys[pos] = key;  // pos ≤ j: never overwrites a key not yet read
-            }
-            __syncthreads();
-        }
-    };
-    for (uint32_t j0 = 0; j0 < n; j0 += nslots) {
+    for (uint32_t j0 = j_begin; j0 < j_end; j0 += nslots) {
         const uint32_t j = j0 + slot;
-        const bool on = j < n;
+        const bool on = j < j_end;
         const uint32_t pos = on ? rows2[static_cast<size_t>(qrow) * cap2 + j] : 0u;
         const uint32_t row = row_map && on ? row_map[pos] : pos;
         const float acc = dot_scan_order<4>(vecs + static_cast<size_t>(row_map ? pos : row) * ds, qv, nbox, ch, on);
-        if (ch == 0 && on && acc >= t) keys[atomicAdd(&fill, 1u)] = make_key(acc, row);
-        __syncthreads();
-        const uint32_t f = fill;
-        __syncthreads();  // every thread has read the count before the next round appends
-        if (f + nslots > capacity) {  // no room for another round: keep the best k (f > k here)
-            keep_best(f, k);
-            if (threadIdx.x == 0) fill = k;
-            __syncthreads();
-        }
+        const bool take = ch == 0 && on && acc >= t;
+        const uint32_t at = warp_append(&fill, take);
+        if (take) keys[at] = make_key(acc, row);
     }
+    __syncthreads();
     const uint32_t m = fill;
     const uint32_t kk = m < k ? m : k;
-    if (m > kk) keep_best(m, kk);
+    if (m > kk) block_keep_best(keys, m, kk, sel);
+    uint64_t* out = slot_keys + (static_cast<size_t>(i) * gridDim.y + c) * k;
+    for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) out[j] = j < kk ? keys[j] : 0ull;
+}
+
+// Per uncertified query i: the best k over its items' slots, sorted, into the query's outputs (a
+// collection that overflowed its buffer marks the query for the FP32 scan instead).
+__global__ void __launch_bounds__(256)
+    rerank_merge_kernel(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ cnt2, uint32_t cap2,
+                        uint32_t k, int by_query, const uint32_t* __restrict__ live,
+                        const uint64_t* __restrict__ slot_keys, uint32_t chunks, uint64_t* __restrict__ idx_out,
+                        float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out, uint32_t* __restrict__ ok_out) {
+    extern __shared__ uint64_t keys[];  // chunks·k keys, at least p2(k)
+    __shared__ BlockSelectScratch sel;
+    const uint32_t i = blockIdx.x;
+    if (live && i >= *live) return;
+    const uint32_t q = ids[i];
+    const uint32_t total = cnt2[by_query ? q : i];
+    if (total > cap2) {  // the collected set overflowed: this query goes to the FP32 scan
+        if (threadIdx.x == 0) ok_out[i] = 0;
+        return;
+    }
+    const uint32_t items = (total + kRerankChunk - 1) / kRerankChunk;
+    const uint64_t* src = slot_keys + static_cast<size_t>(i) * chunks * k;
+    if (threadIdx.x == 0) sel.count = 0;
+    __syncthreads();
+    for (uint32_t j0 = 0; j0 < items * k; j0 += blockDim.x) {
+        const uint32_t j = j0 + threadIdx.x;
+        const uint64_t key = j < items * k ? src[j] : 0ull;
+        const uint32_t at = warp_append(&sel.count, key != 0ull);
+        if (key != 0ull) keys[at] = key;
+    }
+    __syncthreads();
+    const uint32_t m = sel.count;
+    __syncthreads();
+    const uint32_t kk = m < k ? m : k;
+    if (m > kk) block_keep_best(keys, m, kk, sel);
     uint32_t p2 = 1;
     while (p2 < kk) p2 <<= 1;
     for (uint32_t j = kk + threadIdx.x; j < p2; j += blockDim.x) keys[j] = 0ull;
@@ -806,7 +839,8 @@ cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream) {
     const uint32_t threads = a.nq < 64 ? 1024u : 256u;
     rerank_kernel<<<a.nq, threads, p2 * sizeof(uint64_t), stream>>>(a.base, a.ds, a.queries, a.cand_idx, a.cand_sim,
                                                                a.cand_cnt, a.kp, a.k, a.idx_out, a.sim_out,
-                                                               a.cnt_out, a.cert_out, a.kth_out, a.certify ? 1 : 0);
+                                                               a.cnt_out, a.cert_out, a.kth_out, a.certify ? 1 : 0,
+                                                               a.fb_ids, a.fb_count, a.row_map);
     count_launch();
     return cudaGetLastError();
 }
@@ -825,22 +859,27 @@ cudaError_t launch_gather_queries(const uint32_t* ids, uint32_t m, const void* q
     return cudaGetLastError();
 }
 
+uint32_t rerank_chunks(uint32_t cap2) { return (cap2 + kRerankChunk - 1) / kRerankChunk; }
+
 cudaError_t launch_rerank_collected(const float* vecs, uint32_t ds, const float* queries, const uint32_t* ids,
                                     uint32_t m, const uint32_t* rows2, const uint32_t* cnt2, uint32_t cap2, uint32_t k,
-                                    const float* thr, uint64_t* idx_out, float* sim_out, uint32_t* cnt_out,
-                                    uint32_t* ok_out, cudaStream_t stream, bool by_query, const uint32_t* live,
-                                    const uint32_t* row_map) {
+                                    const float* thr, uint64_t* slot_keys, uint64_t* idx_out, float* sim_out,
+                                    uint32_t* cnt_out, uint32_t* ok_out, cudaStream_t stream, bool by_query,
+                                    const uint32_t* live, const uint32_t* row_map) {
     if (m == 0) return cudaSuccess;
-    if (k == 0 || k > kRerankRound) return cudaErrorInvalidValue;
-    uint32_t p2k = 1;
-    while (p2k < k) p2k <<= 1;
-    const size_t smem = (kRerankRound + p2k) * sizeof(uint64_t);
-    auto kern = rerank_collected_kernel;
+    const uint32_t chunks = rerank_chunks(cap2);
+    if (k == 0 || k > kRerankChunk || chunks > 65535u) return cudaErrorInvalidValue;
+    rerank_chunk_kernel<<<dim3(m, chunks), 256, 0, stream>>>(vecs, ds, queries, ids, rows2, cnt2, cap2, k,
+                                                            by_query ? 1 : 0, live, row_map, thr, slot_keys);
+    uint32_t p2 = 1;
+    while (p2 < k) p2 <<= 1;
+    const size_t smem = std::max<size_t>(static_cast<size_t>(chunks) * k, p2) * sizeof(uint64_t);
+    auto kern = rerank_merge_kernel;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    kern<<<m, 256, smem, stream>>>(vecs, ds, queries, ids, rows2, cnt2, cap2, k, idx_out, sim_out, cnt_out, ok_out,
-                                   by_query ? 1 : 0, live, row_map, thr);
-    count_launch();
+    kern<<<m, 256, smem, stream>>>(ids, cnt2, cap2, k, by_query ? 1 : 0, live, slot_keys, chunks, idx_out, sim_out,
+                                   cnt_out, ok_out);
+    count_launch(2);
     return cudaGetLastError();
 }
 

@@ -276,7 +276,20 @@ __global__ void __launch_bounds__(kTfThreads, 1)
             const uint32_t n = cnt[b] < p.kp ? cnt[b] : p.kp;
             uint64_t* dst = p.ws_keys + (static_cast<size_t>(q0 + b) * G + c) * p.kp;
             const uint64_t* src = cand + static_cast<size_t>(b) * p.cap;
-            for (uint32_t j = lane; j < p.kp; j += 32) dst[j] = j < n ? src[j] : 0ull;
+            unsigned long long mn = ~0ull;
+            for (uint32_t j = lane; j < p.kp; j += 32) {
+                const uint64_t key = j < n ? src[j] : 0ull;
+                dst[j] = key;
+                mn = key < mn ? key : mn;
+            }
+            if (p.floor_keys && n == p.kp) {  // a full list: every row it left out has a smaller key
+#pragma unroll
+                for (uint32_t o = 16; o > 0; o >>= 1) {
+                    const unsigned long long x = __shfl_xor_sync(0xFFFFFFFFu, mn, o);
+                    mn = x < mn ? x : mn;
+                }
+                if (lane == 0) atomicMax(&p.floor_keys[q0 + b], mn);
+            }
         }
     }
     // ---------------- teardown: release TMEM ----------------

@@ -77,6 +77,18 @@ NNDEX_DEVICE_INLINE void warp_find_bin(const uint32_t* hist, uint32_t krem, uint
     in_bin = __shfl_sync(0xffffffffu, n, src);
 }
 
+// A slot from *counter (shared or global) for each lane with `take`, one atomic per warp; all 32
+// lanes call it. Slots are consecutive in lane order within the warp.
+NNDEX_DEVICE_INLINE uint32_t warp_append(uint32_t* counter, bool take) {
+    const uint32_t ballot = __ballot_sync(0xffffffffu, take);
+    if (ballot == 0u) return 0u;
+    const uint32_t leader = static_cast<uint32_t>(__ffs(ballot) - 1);
+    uint32_t base = 0;
+    if (lane_id() == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(ballot)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + static_cast<uint32_t>(__popc(ballot & ((1u << lane_id()) - 1u)));
+}
+
 // Exact k-th largest key among buf[0..n) (requires 1 <= k <= n), by one warp. `hist` is a
 // 256-entry per-warp scratch in shared memory. buf may live in shared or global memory.
 NNDEX_DEVICE_INLINE uint64_t warp_radix_kth(const uint64_t* buf, uint32_t n, uint32_t k, uint32_t* hist) {
