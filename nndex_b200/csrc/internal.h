@@ -122,6 +122,7 @@ struct TcParams {
     // IVF item mode (the list scan on the tensor cores): CTA b runs work item b of the IVF plan —
     // one chunk of one list's reordered rows against one gathered block of ≤ 128 queries probing it.
     const uint32_t* it_item_off = nullptr;    // nlist + 1: first work item of each list
+    const uint32_t* it_item_list = nullptr;   // items: the list of each work item
     const uint32_t* it_list_cnt = nullptr;    // nlist: queries probing each list
     const uint32_t* it_offsets = nullptr;     // nlist + 1: each list's reordered row range
     const uint32_t* it_qblock_off = nullptr;  // nlist + 1: first gathered query block of each list

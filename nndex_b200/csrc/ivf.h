@@ -56,6 +56,7 @@ struct IvfScratch {
     uint32_t* d_list_fill = nullptr;    size_t cap_list_fill = 0;
     uint32_t* d_list_qoff = nullptr;    size_t cap_list_qoff = 0;  // nlist + 1
     uint32_t* d_item_off = nullptr;     size_t cap_item_off = 0;   // nlist + 1
+    uint32_t* d_item_list = nullptr;    size_t cap_item_list = 0;  // tensor-core scan: list of each work item
     uint32_t* d_list_q = nullptr;       size_t cap_list_q = 0;     // B·nprobe: query of each (list, query) pair
     uint32_t* d_list_slot = nullptr;    size_t cap_list_slot = 0;  // B·nprobe: its first output slot
     uint32_t* d_q_slot_off = nullptr;   size_t cap_q_slot_off = 0; // B + 1

@@ -980,6 +980,7 @@ IvfScratch::~IvfScratch() {
     cudaFree(d_list_fill);
     cudaFree(d_list_qoff);
     cudaFree(d_item_off);
+    cudaFree(d_item_list);
     cudaFree(d_list_q);
     cudaFree(d_list_slot);
     cudaFree(d_q_slot_off);

@@ -512,10 +512,13 @@ __global__ void __launch_bounds__(256)
                          const uint32_t* __restrict__ list_qoff, const uint32_t* __restrict__ list_q,
                          const uint32_t* __restrict__ list_slot, const uint32_t* __restrict__ qblock_off,
                          __nv_bfloat16* __restrict__ g16, uint32_t* __restrict__ lane_qid,
-                         uint32_t* __restrict__ lane_slot) {
+                         uint32_t* __restrict__ lane_slot, const uint32_t* __restrict__ item_off,
+                         uint32_t* __restrict__ item_list) {
     const uint32_t l = blockIdx.x;
     const uint32_t cnt = list_cnt[l];
     if (cnt == 0) return;
+    // the list of each of this list's work items (so a scan CTA finds its list with one load)
+    for (uint32_t i = item_off[l] + threadIdx.x; i < item_off[l + 1]; i += blockDim.x) item_list[i] = l;
     const uint32_t n = (cnt + 127) / 128 * 128;
     const uint64_t row0 = static_cast<uint64_t>(qblock_off[l]) * 128;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nwarps = blockDim.x >> 5;
@@ -808,6 +811,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     if ((st = grow(w.d_g16, w.cap_g16, max_blocks * 128 * v.kb16, "IVF query blocks"))) return st;
     if ((st = grow(w.d_lane_qid, w.cap_lane_qid, max_blocks * 128, "IVF query blocks"))) return st;
     if ((st = grow(w.d_lane_slot, w.cap_lane_slot, max_blocks * 128, "IVF query blocks"))) return st;
+    if ((st = grow(w.d_item_list, w.cap_item_list, max_items, "IVF plan buffer"))) return st;
     if ((st = grow(ix.d_thr, ix.cap_thr, nq, "tc workspace"))) return st;
     if ((st = grow(ix.d_cand_idx, ix.cap_cand_idx, static_cast<size_t>(nq) * kp, "tc workspace"))) return st;
     if ((st = grow(ix.d_cand_sim, ix.cap_cand_sim, static_cast<size_t>(nq) * kp, "tc workspace"))) return st;
@@ -838,7 +842,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     if (e != cudaSuccess) return cuda_error(e, "IVF probe launch");
     ivf_gather_tc_kernel<<<nlist, 256, 0, s>>>(ix.d_q_bf16, static_cast<uint32_t>(v.kb16), w.d_list_cnt, w.d_list_qoff,
                                                w.d_list_q, w.d_list_slot, w.d_qblock_off, w.d_g16, w.d_lane_qid,
-                                               w.d_lane_slot);
+                                               w.d_lane_slot, w.d_item_off, w.d_item_list);
     count_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "IVF plan launch");
@@ -867,6 +871,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     const uint32_t stride = ix.forced_stride ? ix.forced_stride : w.tc_stride;  // a tuned plan may fix it
     a.p.tile_stride = stride;
     a.p.it_item_off = w.d_item_off;
+    a.p.it_item_list = w.d_item_list;
     a.p.it_list_cnt = w.d_list_cnt;
     a.p.it_offsets = v.d_offsets;
     a.p.it_qblock_off = w.d_qblock_off;

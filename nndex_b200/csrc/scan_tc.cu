@@ -229,11 +229,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         // query certified (the device count of the others is zero)
         if (wi >= p.it_item_off[p.it_nlist]) return;
         if (kMode == 1 && p.live_q && *p.live_q == 0) return;
-        uint32_t lo = 0, hi = p.it_nlist;  // the last list whose first item is ≤ wi
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (p.it_item_off[mid] <= wi) lo = mid; else hi = mid;
-        }
+        const uint32_t lo = p.it_item_list[wi];  // the item's list
         const uint32_t groups = (p.it_list_cnt[lo] + kM - 1) / kM;
         const uint32_t local = wi - p.it_item_off[lo];
         chunk = local / groups;
