@@ -620,6 +620,7 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     a.p.q_resid = d_q_resid;
     a.p.q_scale = fp8 ? d_q_scale : nullptr;
     a.p.kprime = kp;
+    a.p.heap_k = stride > 1 ? std::max(1u, std::min(kp, kcap)) : kp;  // a sampled pass 1 only yields T
     a.p.thr_global = d_thr;
     a.p.ws_keys = d_ws;
     a.p.tile_stride = stride;

@@ -101,7 +101,10 @@ cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream);
 struct TcParams {
     uint32_t nq = 0;
     uint32_t nchunks = 0;                 // K bytes / 128
-    uint32_t kprime = 0;                  // pass 1 heap size
+    uint32_t kprime = 0;                  // pass 1: keys per (query, range or item) slot
+    // pass 1 heap size (≤ kprime; the slot's rest is zero): kprime when pass 1 may certify; a
+    // sampled pass 1 only has to yield T, for which each slot's best k suffice
+    uint32_t heap_k = 0;
     uint32_t cap2 = 0;                    // pass 2 rows collected per query
     uint64_t rows = 0;
     uint64_t range_rows = 0;              // rows per CTA range (multiple of 256)

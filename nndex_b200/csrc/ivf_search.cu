@@ -870,6 +870,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     // ivf_finish_tc).
     const uint32_t stride = ix.forced_stride ? ix.forced_stride : w.tc_stride;  // a tuned plan may fix it
     a.p.tile_stride = stride;
+    a.p.heap_k = stride > 1 ? std::max(1u, std::min(kp, k)) : kp;  // a sampled pass 1 only yields T
     a.p.it_item_off = w.d_item_off;
     a.p.it_item_list = w.d_item_list;
     a.p.it_list_cnt = w.d_list_cnt;

@@ -47,7 +47,7 @@ template <int kMode>
 constexpr uint32_t epi_warps() { return kMode == 1 ? 8u : 4u; }
 // Pass 2: rows that pass the cut are staged per epilogue thread and appended to the query's
 // collection kPass2Stage at a time (one atomic per group instead of one per row).
-constexpr uint32_t kPass2Stage = 8;
+constexpr uint32_t kPass2Stage = 16;
 template <int kMode>
 constexpr int tc_threads() { return 64 + 32 * static_cast<int>(epi_warps<kMode>()); }
 constexpr uint32_t kTmemCols = 512;   // two 256-column FP32 accumulators
@@ -117,7 +117,7 @@ NNDEX_DEVICE_INLINE void epi_survivor(const TcParams& p, EpiState& st, uint64_t*
     if (kMode == 0) {
         const uint64_t key = make_key(u, static_cast<uint32_t>(row));
         if (key <= st.thr_key) return;
-        const uint32_t kp = p.kprime;
+        const uint32_t kp = p.heap_k;
         if (st.n < kp) {
             uint32_t i = st.n++;
             while (i > 0) {
@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
             uint64_t* dst = kItems ? p.ws_keys + static_cast<size_t>(p.it_lane_slot[q0 + lrow] + chunk) * p.kprime
                                    : p.ws_keys + (static_cast<size_t>(q) * nranges + range) * p.kprime;
             for (uint32_t i = 0; i < p.kprime; ++i) dst[i] = i < st.n ? heap[i * kM + lrow] : 0ull;
-            if (st.n == p.kprime) atomicMax(&p.thr_global[q], static_cast<unsigned long long>(heap[lrow]));
+            if (st.n == p.heap_k) atomicMax(&p.thr_global[q], static_cast<unsigned long long>(heap[lrow]));
         }
     }
     // ---------------- teardown: release TMEM ----------------
@@ -764,6 +764,7 @@ template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems = false, int
 static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
     auto kern = scan_tc_kernel<kFp8, kST, kMode, kStreamA, kItems, kQB>;
     const uint32_t kp = kMode == 0 ? a.p.kprime : 0;
+    if (kMode == 0 && (a.p.heap_k == 0 || a.p.heap_k > kp)) return cudaErrorInvalidValue;
     const size_t smem = tc_smem_bytes(a.p.nchunks, kp, kST, kFp8, kStreamA, kQB);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
