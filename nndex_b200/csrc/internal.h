@@ -126,6 +126,7 @@ struct TcParams {
     // one chunk of one list's reordered rows against one gathered block of ≤ 128 queries probing it.
     const uint32_t* it_item_off = nullptr;    // nlist + 1: first work item of each list
     const uint32_t* it_item_list = nullptr;   // items: the list of each work item
+    unsigned long long* it_next = nullptr;    // zeroed before the launch: the next item to take
     const uint32_t* it_list_cnt = nullptr;    // nlist: queries probing each list
     const uint32_t* it_offsets = nullptr;     // nlist + 1: each list's reordered row range
     const uint32_t* it_qblock_off = nullptr;  // nlist + 1: first gathered query block of each list

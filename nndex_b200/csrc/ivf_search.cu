@@ -806,7 +806,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     if ((st = grow(w.d_list_q, w.cap_list_q, pairs, "IVF plan buffer"))) return st;
     if ((st = grow(w.d_list_slot, w.cap_list_slot, pairs, "IVF plan buffer"))) return st;
     if ((st = grow(w.d_q_slot_off, w.cap_q_slot_off, nq + 1, "IVF plan buffer"))) return st;
-    if ((st = grow(w.d_counters, w.cap_counters, 8, "IVF plan buffer"))) return st;
+    if ((st = grow(w.d_counters, w.cap_counters, 10, "IVF plan buffer"))) return st;
     if ((st = grow(w.d_ws, w.cap_ws, pairs * max_chunks * kp, "IVF slot workspace"))) return st;
     if ((st = grow(w.d_g16, w.cap_g16, max_blocks * 128 * v.kb16, "IVF query blocks"))) return st;
     if ((st = grow(w.d_lane_qid, w.cap_lane_qid, max_blocks * 128, "IVF query blocks"))) return st;
@@ -832,7 +832,8 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
         return set_error(NNDEX_ERR_OUT_OF_MEMORY, "cuda execution error: pinned allocation failed");
 
     // ---- probe + plan (groups of 128 queries) + gathered query blocks ----
-    cudaMemsetAsync(w.d_counters, 0, 8 * sizeof(unsigned long long), s);
+    // [8] and [9]: the work-item counters of the two tensor-core passes
+    cudaMemsetAsync(w.d_counters, 0, 10 * sizeof(unsigned long long), s);
     cudaMemsetAsync(w.d_list_cnt, 0, nlist * sizeof(uint32_t), s);
     cudaMemsetAsync(w.d_list_fill, 0, nlist * sizeof(uint32_t), s);
     const ProbeLaunch pl{ix.d_qn,   nq,          static_cast<uint32_t>(ix.ds), static_cast<uint32_t>(ix.dp),
@@ -881,6 +882,8 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     a.p.row_map = v.d_row_map;
     a.p.it_nlist = nlist;
     a.p.it_chunk_rows = kChunkRows;
+    a.p.sm_count = static_cast<uint32_t>(ix.sm_count);  // the persistent item grid
+    a.p.it_next = w.d_counters + 8;                      // its CTAs take items from this counter
     cudaEvent_t ev_a = nullptr;
     ix.scan_event_begin(s, ev_a);
     e = launch_scan_tc(a, false, 0, s);
@@ -926,6 +929,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     a.p.cand_cnt = ix.d_cnt2;
     a.p.cap2 = cap2;
     a.p.live_q = d_m;  // item mode: the whole pass returns at once when every query certified
+    a.p.it_next = w.d_counters + 9;
     ix.scan_event_begin(s, ev_a);
     e = launch_scan_tc(a, false, 1, s);
     ix.scan_event_end(s, ev_a);

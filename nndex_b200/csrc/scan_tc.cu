@@ -84,7 +84,7 @@ size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp
                   : static_cast<size_t>(qb) * nchunks * kAChunk + static_cast<size_t>(stages) * (kBChunk / qb);
     b += static_cast<size_t>(kprime) * kM * 8;
     if (kprime == 0) b += static_cast<size_t>(kPass2Stage) * 8 * 32 * 4;  // pass 2: survivor staging
-    b += (2 * stages + 5) * 8 + 16;
+    b += (2 * stages + 10) * 8 + 16;
     return b;
 }
 
@@ -191,13 +191,17 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     uint64_t* full_bar = reinterpret_cast<uint64_t*>(stage2 + (kMode == 1 ? kPass2Stage * 8 * 32 : 0));
     uint64_t* empty_bar = full_bar + kST;
     uint64_t* a_full = empty_bar + kST;
-    uint64_t* tfull = a_full + 1;
+    uint64_t* a_free = a_full + 1;  // item mode: the MMAs of the last item have read its query block
+    uint64_t* wfull = a_free + 1;   // item mode: the next item's id is in witem[slot]
+    uint64_t* wempty = wfull + 2;   // item mode: the MMA and epilogue warps have read witem[slot]
+    uint64_t* tfull = wempty + 2;
     uint64_t* tempty = tfull + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
     volatile uint32_t* abort_flag = tmem_slot + 1;
+    volatile uint32_t* witem = tmem_slot + 2;  // [2]
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    uint32_t q0 = blockIdx.x * kQC;
+    uint32_t grid_q0 = blockIdx.x * kQC;
     uint32_t range = blockIdx.y, nranges = gridDim.y;
     uint64_t range_rows = p.range_rows;
     uint32_t nq_live = p.nq;
@@ -216,34 +220,53 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         if (blockIdx.x >= nqb * nr) return;
         // consecutive CTAs take the query blocks of one row range, as the 2-D grid orders them: the
         // CTAs resident together read the same base tiles, which then come from L2 after the first
-        q0 = static_cast<uint32_t>(blockIdx.x % nqb) * kQC;
+        grid_q0 = static_cast<uint32_t>(blockIdx.x % nqb) * kQC;
         range = static_cast<uint32_t>(blockIdx.x / nqb);
         nranges = static_cast<uint32_t>(nr);
     }
-    uint64_t row_begin = static_cast<uint64_t>(range) * range_rows;
-    uint64_t row_end = (row_begin + range_rows) < p.rows ? (row_begin + range_rows) : p.rows;
-    uint32_t chunk = 0;  // item mode: the chunk of the list (its output slot offset)
+    // The CTA's work: one (query block, row range) in the grid modes. In item mode the CTA is
+    // persistent: its producer thread takes the plan's items (each a chunk of one list × one
+    // gathered query block) from a global counter and hands each item's id to the MMA and epilogue
+    // warps through two shared-memory slots; TMEM, barriers and the base ring stay across items,
+    // so the next item's base tiles stream while the last one's epilogue drains.
+    constexpr uint32_t kNoItem = 0xFFFFFFFFu;
+    uint32_t total = 0;
     if (kItems) {
-        const uint32_t wi = blockIdx.x;
-        // the grid is an upper bound of the plan's items; pass 2 has nothing to do when every
-        // query certified (the device count of the others is zero)
-        if (wi >= p.it_item_off[p.it_nlist]) return;
+        total = p.it_item_off[p.it_nlist];
+        // pass 2 has nothing to do when every query certified (the device count of the others is 0)
         if (kMode == 1 && p.live_q && *p.live_q == 0) return;
-        const uint32_t lo = p.it_item_list[wi];  // the item's list
-        const uint32_t groups = (p.it_list_cnt[lo] + kM - 1) / kM;
-        const uint32_t local = wi - p.it_item_off[lo];
-        chunk = local / groups;
-        q0 = (p.it_qblock_off[lo] + local % groups) * kM;
-        row_begin = p.it_offsets[lo] + static_cast<uint64_t>(chunk) * p.it_chunk_rows;
-        const uint64_t le = p.it_offsets[lo + 1];
-        row_end = (row_begin + p.it_chunk_rows) < le ? (row_begin + p.it_chunk_rows) : le;
+        if (total == 0) return;
     }
-    // query blocks with at least one query: a second block past the last query is neither loaded
-    // nor multiplied (its epilogue lanes have no query)
-    const uint32_t nblk = (kQB == 2 && q0 + kM >= nq_live) ? 1u : static_cast<uint32_t>(kQB);
     const uint64_t tile_step = static_cast<uint64_t>(kNT) * p.tile_stride;
-    const uint32_t ntiles =
-        row_end > row_begin ? static_cast<uint32_t>((row_end - row_begin + tile_step - 1) / tile_step) : 0;
+    struct Work {
+        uint32_t q0, chunk, ntiles, nblk;
+        uint64_t row_begin, row_end;
+    };
+    auto work_of = [&](uint32_t wi) {
+        Work w;
+        w.chunk = 0;  // item mode: the chunk of the list (its output slot offset)
+        if (kItems) {
+            const uint32_t lo = p.it_item_list[wi];  // the item's list
+            const uint32_t groups = (p.it_list_cnt[lo] + kM - 1) / kM;
+            const uint32_t local = wi - p.it_item_off[lo];
+            w.chunk = local / groups;
+            w.q0 = (p.it_qblock_off[lo] + local % groups) * kM;
+            w.row_begin = p.it_offsets[lo] + static_cast<uint64_t>(w.chunk) * p.it_chunk_rows;
+            const uint64_t le = p.it_offsets[lo + 1];
+            w.row_end = (w.row_begin + p.it_chunk_rows) < le ? (w.row_begin + p.it_chunk_rows) : le;
+        } else {
+            w.q0 = grid_q0;
+            w.row_begin = static_cast<uint64_t>(range) * range_rows;
+            w.row_end = (w.row_begin + range_rows) < p.rows ? (w.row_begin + range_rows) : p.rows;
+        }
+        // query blocks with at least one query: a second block past the last query is neither
+        // loaded nor multiplied (its epilogue lanes have no query)
+        w.nblk = (kQB == 2 && w.q0 + kM >= nq_live) ? 1u : static_cast<uint32_t>(kQB);
+        w.ntiles = w.row_end > w.row_begin
+                       ? static_cast<uint32_t>((w.row_end - w.row_begin + tile_step - 1) / tile_step)
+                       : 0u;
+        return w;
+    };
     const uint32_t nchunks = p.nchunks;
 
     if (threadIdx.x == 0) {
@@ -252,6 +275,11 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
             mbar_init(&empty_bar[s], 1);
         }
         mbar_init(a_full, 1);
+        mbar_init(a_free, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&wfull[b], 1);
+            mbar_init(&wempty[b], 1 + epi_warps<kMode>());
+        }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
             mbar_init(&tempty[b], epi_warps<kMode>());
@@ -275,40 +303,70 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
             tma_prefetch_desc(&tmap_b);
             // Base tiles are read by every query block of the same row range at about the same
             // time: keep them in L2 with the default policy (no evict-first hint).
-            if (!kStreamA) {
-                mbar_arrive_expect_tx(a_full, nblk * nchunks * kAChunk);
-                for (uint32_t b = 0; b < nblk; ++b)
-                    for (uint32_t c = 0; c < nchunks; ++c)
-                        tma_load_2d(a_smem + static_cast<size_t>(b * nchunks + c) * kAChunk, &tmap_q, a_full,
-                                    static_cast<int32_t>(c * kElems), static_cast<int32_t>(q0 + b * kM));
-            }
-            uint32_t it = 0;
+            uint32_t it = 0, a_loads = 0;
             bool stop = false;
-            for (uint32_t t = 0; t < ntiles && !stop; ++t) {
-                const int32_t y = static_cast<int32_t>(row_begin + static_cast<uint64_t>(t) * tile_step);
-                for (uint32_t c = 0; c < nchunks; ++c) {
-                    const uint32_t s = it % kST, u = it / kST;
-                    if (u > 0 && !mbar_wait_bounded(&empty_bar[s], (u - 1) & 1u, kWaitBudgetCycles)) {
+            for (uint32_t j = 0; !stop; ++j) {
+                uint32_t wi = 0;
+                if (kItems) {
+                    // take the next item; its slot is free once both readers took the item before
+                    const uint32_t slot = j & 1u;
+                    if (j >= 2 && !mbar_wait_bounded(&wempty[slot], ((j >> 1) - 1) & 1u, kWaitBudgetCycles)) {
+                        *abort_flag = 1;
+                        record_status(p.status, kStatusTimeout);
+                        break;
+                    }
+                    const unsigned long long g = atomicAdd(p.it_next, 1ull);
+                    wi = g < total ? static_cast<uint32_t>(g) : kNoItem;
+                    witem[slot] = wi;
+                    mbar_arrive(&wfull[slot]);
+                    if (wi == kNoItem) break;
+                } else if (j > 0) {
+                    break;
+                }
+                const Work w = work_of(wi);
+                if (!kStreamA) {
+                    // the previous item's MMAs have read its query block (a_free) before this one's
+                    // replaces it
+                    if (j > 0 && !mbar_wait_bounded(a_free, (j - 1) & 1u, kWaitBudgetCycles)) {
                         *abort_flag = 1;
                         record_status(p.status, kStatusTimeout);
                         stop = true;
                         break;
                     }
-                    if (*abort_flag) {
-                        stop = true;
-                        break;
+                    mbar_arrive_expect_tx(a_full, w.nblk * nchunks * kAChunk);
+                    for (uint32_t b = 0; b < w.nblk; ++b)
+                        for (uint32_t c = 0; c < nchunks; ++c)
+                            tma_load_2d(a_smem + static_cast<size_t>(b * nchunks + c) * kAChunk, &tmap_q, a_full,
+                                        static_cast<int32_t>(c * kElems), static_cast<int32_t>(w.q0 + b * kM));
+                    ++a_loads;
+                }
+                for (uint32_t t = 0; t < w.ntiles && !stop; ++t) {
+                    const int32_t y = static_cast<int32_t>(w.row_begin + static_cast<uint64_t>(t) * tile_step);
+                    for (uint32_t c = 0; c < nchunks; ++c) {
+                        const uint32_t s = it % kST, u = it / kST;
+                        if (u > 0 && !mbar_wait_bounded(&empty_bar[s], (u - 1) & 1u, kWaitBudgetCycles)) {
+                            *abort_flag = 1;
+                            record_status(p.status, kStatusTimeout);
+                            stop = true;
+                            break;
+                        }
+                        if (*abort_flag) {
+                            stop = true;
+                            break;
+                        }
+                        uint8_t* stage = b_smem + static_cast<size_t>(s) * kStage;
+                        mbar_arrive_expect_tx(&full_bar[s], kStage);
+                        if (kStreamA)
+                            tma_load_2d(stage + kBChunk, &tmap_q, &full_bar[s], static_cast<int32_t>(c * kElems),
+                                        static_cast<int32_t>(w.q0));
+                        tma_load_2d(stage, &tmap_b, &full_bar[s], static_cast<int32_t>(c * kElems), y);
+                        ++it;
                     }
-                    uint8_t* stage = b_smem + static_cast<size_t>(s) * kStage;
-                    mbar_arrive_expect_tx(&full_bar[s], kStage);
-                    if (kStreamA)
-                        tma_load_2d(stage + kBChunk, &tmap_q, &full_bar[s], static_cast<int32_t>(c * kElems),
-                                    static_cast<int32_t>(q0));
-                    tma_load_2d(stage, &tmap_b, &full_bar[s], static_cast<int32_t>(c * kElems), y);
-                    ++it;
                 }
             }
             // Drain every copy this thread issued before the CTA may exit.
-            if (!kStreamA && !mbar_wait_bounded(a_full, 0, kWaitBudgetCycles)) record_status(p.status, kStatusTimeout);
+            if (!kStreamA && a_loads > 0 && !mbar_wait_bounded(a_full, (a_loads - 1) & 1u, kWaitBudgetCycles))
+                record_status(p.status, kStatusTimeout);
             const uint32_t used = it < static_cast<uint32_t>(kST) ? it : kST;
             for (uint32_t s = 0; s < used; ++s) {
                 const uint32_t uses = (it - s + kST - 1) / kST;
@@ -320,42 +378,67 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             constexpr uint32_t idesc = tc::instr_desc<kFp8, kM, kNT>();
-            if (!kStreamA && !mbar_wait_bounded(a_full, 0, kWaitBudgetCycles)) {
-                *abort_flag = 1;
-                record_status(p.status, kStatusTimeout);
-            }
-            tc::fence_after_sync();
             const uint32_t a_addr0 = smem_u32(a_smem), b_addr0 = smem_u32(b_smem);
-            uint32_t it = 0;
-            for (uint32_t t = 0; t < ntiles; ++t) {
-                const uint32_t buf = t & 1u, ub = t >> 1;
-                if (ub > 0 && !*abort_flag && !mbar_wait_bounded(&tempty[buf], (ub - 1) & 1u, kWaitBudgetCycles)) {
+            uint32_t it = 0, tg = 0;  // slabs and tiles over all of the CTA's work
+            for (uint32_t j = 0;; ++j) {
+                uint32_t wi = 0;
+                if (kItems) {
+                    const uint32_t slot = j & 1u;
+                    if (*abort_flag || !mbar_wait_bounded(&wfull[slot], (j >> 1) & 1u, kWaitBudgetCycles)) {
+                        if (!*abort_flag) {
+                            *abort_flag = 1;
+                            record_status(p.status, kStatusTimeout);
+                        }
+                        break;
+                    }
+                    wi = witem[slot];
+                    mbar_arrive(&wempty[slot]);
+                    if (wi == kNoItem) break;
+                    // another item: the previous one's MMAs are all issued, and its query block may
+                    // be replaced once they complete (never committed after the CTA's last item,
+                    // which nothing waits for)
+                    if (!kStreamA && j > 0) tc::commit(a_free);
+                } else if (j > 0) {
+                    break;
+                }
+                const Work w = work_of(wi);
+                if (!kStreamA && !*abort_flag && !mbar_wait_bounded(a_full, j & 1u, kWaitBudgetCycles)) {
                     *abort_flag = 1;
                     record_status(p.status, kStatusTimeout);
                 }
                 tc::fence_after_sync();
-                const uint32_t d = tmem_base + buf * kN;  // kQB = 2: block b in columns [b·128, b·128 + 128)
-                for (uint32_t c = 0; c < nchunks; ++c, ++it) {
-                    const uint32_t s = it % kST, u = it / kST;
-                    if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], u & 1u, kWaitBudgetCycles)) {
+                for (uint32_t t = 0; t < w.ntiles; ++t, ++tg) {
+                    const uint32_t buf = tg & 1u, ub = tg >> 1;
+                    if (ub > 0 && !*abort_flag &&
+                        !mbar_wait_bounded(&tempty[buf], (ub - 1) & 1u, kWaitBudgetCycles)) {
                         *abort_flag = 1;
                         record_status(p.status, kStatusTimeout);
                     }
                     tc::fence_after_sync();
-                    if (!*abort_flag) {
-                        const uint32_t b_addr = b_addr0 + s * kStage;
-                        for (uint32_t b = 0; b < nblk; ++b) {
-                            const uint32_t a_addr =
-                                kStreamA ? b_addr + kBChunk : a_addr0 + (b * nchunks + c) * kAChunk;
-#pragma unroll
-                            for (uint32_t kk = 0; kk < 4; ++kk)
-                                tc::mma<kFp8>(d + b * kNT, tc::smem_desc_sw128(a_addr + kk * 32),
-                                              tc::smem_desc_sw128(b_addr + kk * 32), idesc, (c | kk) != 0u ? 1u : 0u);
+                    const uint32_t d = tmem_base + buf * kN;  // kQB = 2: block b in columns [b·128, b·128 + 128)
+                    for (uint32_t c = 0; c < nchunks; ++c, ++it) {
+                        const uint32_t s = it % kST, u = it / kST;
+                        if (!*abort_flag && !mbar_wait_bounded(&full_bar[s], u & 1u, kWaitBudgetCycles)) {
+                            *abort_flag = 1;
+                            record_status(p.status, kStatusTimeout);
                         }
+                        tc::fence_after_sync();
+                        if (!*abort_flag) {
+                            const uint32_t b_addr = b_addr0 + s * kStage;
+                            for (uint32_t b = 0; b < w.nblk; ++b) {
+                                const uint32_t a_addr =
+                                    kStreamA ? b_addr + kBChunk : a_addr0 + (b * nchunks + c) * kAChunk;
+#pragma unroll
+                                for (uint32_t kk = 0; kk < 4; ++kk)
+                                    tc::mma<kFp8>(d + b * kNT, tc::smem_desc_sw128(a_addr + kk * 32),
+                                                  tc::smem_desc_sw128(b_addr + kk * 32), idesc,
+                                                  (c | kk) != 0u ? 1u : 0u);
+                            }
+                        }
+                        tc::commit(&empty_bar[s]);  // frees the slab once the MMAs above have read it
                     }
-                    tc::commit(&empty_bar[s]);  // frees the slab once the MMAs above have read it
+                    tc::commit(&tfull[buf]);  // the accumulator is complete
                 }
-                tc::commit(&tfull[buf]);  // the accumulator is complete
             }
         }
     } else {
@@ -368,145 +451,171 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         const uint32_t c_begin = ((ew / 4) % kWPB) * kChunks;
         const uint32_t quarter = warp & 3u;
         const uint32_t lrow = quarter * 32 + lane;
-        const uint32_t q = kItems ? p.it_lane_qid[q0 + lrow] : q0 + blk * kM + lrow;
-        const bool valid_q = kItems ? q != 0xFFFFFFFFu : q < nq_live;
         // pass 2: this thread's staged rows and its append of them to the query's collection
         uint32_t* my_stage = stage2 + (ew * 32 + lane) * kPass2Stage;
-        uint32_t staged = 0;
-        auto flush_stage = [&]() {
-            const uint32_t pos = atomicAdd(&p.cand_cnt[q], staged);
-            for (uint32_t i = 0; i < staged; ++i)
-                if (pos + i < p.cap2) p.cand_rows[static_cast<size_t>(q) * p.cap2 + pos + i] = my_stage[i];
-            staged = 0;
-        };
-        const float qs = (kFp8 && valid_q) ? p.q_scale[q] : 1.0f;
-        const float rq = valid_q ? p.q_resid[q] : 0.0f;
-        const float b_mul = 1.0f + rq, b_add = rq + p.eps_acc;
-        const float slack = fmaf(p.eps_rows, b_mul, b_add);  // the largest u_r − s̃_r over all rows
-        const bool per_row_bound = p.tile_stride == 1;
-        EpiState st;
-        st.n = 0;
-        if (kMode == 0) {
-            st.thr_key = valid_q ? p.thr_global[q] : ~0ull;
-            st.thr_f = !valid_q ? INFINITY : (st.thr_key ? key_score(st.thr_key) : -INFINITY);
-        } else {
-            st.thr_key = 0;
-            st.thr_f = valid_q ? p.q_thr[q] : INFINITY;
-        }
-        st.cut = st.thr_f - slack;
         const uint32_t taddr0 = tmem_base + ((quarter * 32u) << 16);
-        for (uint32_t t = 0; t < ntiles; ++t) {
-            const uint32_t buf = t & 1u, ub = t >> 1;
-            const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * tile_step;
-            // FP8: the extremes of the row scales over this tile's rows (computed once per index), so
-            // no thread needs the tile's 256 scales unless a score may survive
-            float smin = 0.0f, smax = 0.0f;
-            const float* sc = kFp8 ? p.row_scale + tile_row0 : nullptr;
-            if (kFp8) {
-                const float2 mm = p.tile_scale[tile_row0 / kN];  // a 128-row tile lies in one 256-row tile
-                smin = mm.x;
-                smax = mm.y;
-            }
-            if (!*abort_flag && !mbar_wait_bounded(&tfull[buf], ub & 1u, kWaitBudgetCycles)) {
-                *abort_flag = 1;
-                record_status(p.status, kStatusTimeout);
-            }
-            tc::fence_after_sync();
-            if (kMode == 0 && (t & 3u) == 3u && valid_q) {
-                const unsigned long long g = p.thr_global[q];
-                if (g > st.thr_key) {
-                    st.thr_key = g;
-                    st.thr_f = key_score(g);
-                    st.cut = st.thr_f - slack;
-                }
-            }
-            const uint32_t taddr = taddr0 + buf * kN + blk * kNT;
-            uint32_t va[32], vb[32];
-            __syncwarp();
-            tc::tmem_ld32(taddr + c_begin * 32, va);
-            tmem_wait_ld_regs(va);
-            // The cut in the domain of the accumulator's raw scores. FP8 scores are scaled by the row's
-            // and the query's scales (both positive): a score can reach the cut only if its raw value
-            // reaches cut / (largest row scale · query scale) when cut ≥ 0, or cut / (smallest row
-            // scale · query scale) when cut < 0; 2⁻²⁰ of slack covers the roundings of both sides.
-            float raw_cut = st.cut;
-            if (kFp8) {
-                const float den = (st.cut >= 0.0f ? smax : smin) * qs;
-                raw_cut = (den > 0.0f) ? st.cut / den : -INFINITY;
-                raw_cut -= fabsf(raw_cut) * 9.5367431640625e-07f;
-                if (!(raw_cut == raw_cut)) raw_cut = -INFINITY;  // an infinite cut filters nothing here
-            }
-            auto process = [&](const uint32_t(&v)[32], uint32_t c) {
-                // A padding lane (no query: past nq, or an empty slot of a gathered block) scores
-                // whatever its query row holds, +inf included; it never survives, since its
-                // index would address past the per-query outputs.
-                if (!valid_q) return;
-                // Almost every group of 32 scores is rejected by its largest one (a 5-level tree).
-                float m16[16];
-#pragma unroll
-                for (uint32_t j = 0; j < 16; ++j) m16[j] = fmaxf(__uint_as_float(v[j]), __uint_as_float(v[j + 16]));
-#pragma unroll
-                for (uint32_t w = 8; w > 0; w >>= 1)
-#pragma unroll
-                    for (uint32_t j = 0; j < w; ++j) m16[j] = fmaxf(m16[j], m16[j + w]);
-                if (!(m16[0] >= raw_cut)) return;
-                uint32_t mask = 0;
-#pragma unroll
-                for (uint32_t j = 0; j < 32; ++j) {
-                    float s = __uint_as_float(v[j]);
-                    if (kFp8) s = (s * sc[c * 32 + j]) * qs;
-                    mask |= (s >= st.cut ? 1u : 0u) << j;
-                }
-                while (mask) {  // survivors are rare once a threshold exists
-                    const uint32_t j = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const uint64_t row = tile_row0 + c * 32 + j;
-                    if (row >= row_end) continue;
-                    if (kMode == 1) {
-                        // pass 2 keeps every row that passed the cut (the largest bound slack over
-                        // all rows: a superset of the rows whose own bound reaches T); in item mode
-                        // the row is a reordered position, mapped to its row by the rerank
-                        my_stage[staged++] = static_cast<uint32_t>(row);
-                        if (staged == kPass2Stage) flush_stage();
-                        continue;
+        const bool per_row_bound = p.tile_stride == 1;
+        uint32_t tg = 0;  // tiles over all of the CTA's work
+        for (uint32_t jw = 0;; ++jw) {
+            uint32_t wi = 0;
+            if (kItems) {
+                // lane 0 takes the item and the warp follows its decision (no lane leaves alone)
+                const uint32_t slot = jw & 1u;
+                uint32_t got = kNoItem;
+                if (lane == 0) {
+                    if (!*abort_flag && mbar_wait_bounded(&wfull[slot], (jw >> 1) & 1u, kWaitBudgetCycles)) {
+                        got = witem[slot];
+                        mbar_arrive(&wempty[slot]);
+                    } else if (!*abort_flag) {
+                        *abort_flag = 1;
+                        record_status(p.status, kStatusTimeout);
                     }
-                    float s = pick(v, j);
-                    if (kFp8) s = (s * sc[c * 32 + j]) * qs;
-                    // The row's own bound when pass 1 may certify (every tile scanned); a sampled
-                    // pass 1 only yields T, and the largest slack spares a dependent load per
-                    // survivor. In item mode the key holds the list position (the rerank maps it).
-                    const float u = per_row_bound ? fmaf(p.row_resid[row], b_mul, s + b_add) : s + slack;
-                    epi_survivor<kMode>(p, st, heap, lrow, q, u, row, slack);
                 }
-            };
-#pragma unroll
-            for (uint32_t cc = 0; cc < kChunks; cc += 2) {
-                const uint32_t c = c_begin + cc;
-                // tcgen05.ld and tcgen05.wait::ld are .sync.aligned: the whole warp executes each
-                // one together. process() loops per lane over its survivors (one lane may take
-                // every row while the others take none), so the warp reconverges before each.
-                __syncwarp();
-                tc::tmem_ld32(taddr + (c + 1) * 32, vb);
-                process(va, c);
-                __syncwarp();
-                tmem_wait_ld_regs(vb);
-                if (cc + 2 < kChunks) tc::tmem_ld32(taddr + (c + 2) * 32, va);
-                process(vb, c + 1);
-                if (cc + 2 < kChunks) {
-                    __syncwarp();
-                    tmem_wait_ld_regs(va);
-                }
+                wi = __shfl_sync(0xffffffffu, got, 0);
+                if (wi == kNoItem) break;
+            } else if (jw > 0) {
+                break;
             }
-            tc::fence_before_sync();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&tempty[buf]);
-        }
-        if (kMode == 1 && staged) flush_stage();
-        if (kMode == 0 && valid_q) {
-            uint64_t* dst = kItems ? p.ws_keys + static_cast<size_t>(p.it_lane_slot[q0 + lrow] + chunk) * p.kprime
-                                   : p.ws_keys + (static_cast<size_t>(q) * nranges + range) * p.kprime;
-            for (uint32_t i = 0; i < p.kprime; ++i) dst[i] = i < st.n ? heap[i * kM + lrow] : 0ull;
-            if (st.n == p.heap_k) atomicMax(&p.thr_global[q], static_cast<unsigned long long>(heap[lrow]));
+            const Work w = work_of(wi);
+            const uint32_t q0 = w.q0;
+            const uint64_t row_begin = w.row_begin, row_end = w.row_end;
+            const uint32_t q = kItems ? p.it_lane_qid[q0 + lrow] : q0 + blk * kM + lrow;
+            const bool valid_q = kItems ? q != 0xFFFFFFFFu : q < nq_live;
+            uint32_t staged = 0;
+            auto flush_stage = [&]() {
+                const uint32_t pos = atomicAdd(&p.cand_cnt[q], staged);
+                for (uint32_t i = 0; i < staged; ++i)
+                    if (pos + i < p.cap2) p.cand_rows[static_cast<size_t>(q) * p.cap2 + pos + i] = my_stage[i];
+                staged = 0;
+            };
+            const float qs = (kFp8 && valid_q) ? p.q_scale[q] : 1.0f;
+            const float rq = valid_q ? p.q_resid[q] : 0.0f;
+            const float b_mul = 1.0f + rq, b_add = rq + p.eps_acc;
+            const float slack = fmaf(p.eps_rows, b_mul, b_add);  // the largest u_r − s̃_r over all rows
+            EpiState st;
+            st.n = 0;
+            if (kMode == 0) {
+                st.thr_key = valid_q ? p.thr_global[q] : ~0ull;
+                st.thr_f = !valid_q ? INFINITY : (st.thr_key ? key_score(st.thr_key) : -INFINITY);
+            } else {
+                st.thr_key = 0;
+                st.thr_f = valid_q ? p.q_thr[q] : INFINITY;
+            }
+            st.cut = st.thr_f - slack;
+            for (uint32_t t = 0; t < w.ntiles; ++t, ++tg) {
+                const uint32_t buf = tg & 1u, ub = tg >> 1;
+                const uint64_t tile_row0 = row_begin + static_cast<uint64_t>(t) * tile_step;
+                // FP8: the extremes of the row scales over this tile's rows (computed once per index),
+                // so no thread needs the tile's 256 scales unless a score may survive
+                float smin = 0.0f, smax = 0.0f;
+                const float* sc = kFp8 ? p.row_scale + tile_row0 : nullptr;
+                if (kFp8) {
+                    const float2 mm = p.tile_scale[tile_row0 / kN];  // a 128-row tile lies in one 256-row tile
+                    smin = mm.x;
+                    smax = mm.y;
+                }
+                if (!*abort_flag && !mbar_wait_bounded(&tfull[buf], ub & 1u, kWaitBudgetCycles)) {
+                    *abort_flag = 1;
+                    record_status(p.status, kStatusTimeout);
+                }
+                tc::fence_after_sync();
+                if (kMode == 0 && (t & 3u) == 3u && valid_q) {
+                    const unsigned long long g = p.thr_global[q];
+                    if (g > st.thr_key) {
+                        st.thr_key = g;
+                        st.thr_f = key_score(g);
+                        st.cut = st.thr_f - slack;
+                    }
+                }
+                const uint32_t taddr = taddr0 + buf * kN + blk * kNT;
+                uint32_t va[32], vb[32];
+                __syncwarp();
+                tc::tmem_ld32(taddr + c_begin * 32, va);
+                tmem_wait_ld_regs(va);
+                // The cut in the domain of the accumulator's raw scores. FP8 scores are scaled by the
+                // row's and the query's scales (both positive): a score can reach the cut only if its
+                // raw value reaches cut / (largest row scale · query scale) when cut ≥ 0, or cut /
+                // (smallest row scale · query scale) when cut < 0; 2⁻²⁰ of slack covers the roundings
+                // of both sides.
+                float raw_cut = st.cut;
+                if (kFp8) {
+                    const float den = (st.cut >= 0.0f ? smax : smin) * qs;
+                    raw_cut = (den > 0.0f) ? st.cut / den : -INFINITY;
+                    raw_cut -= fabsf(raw_cut) * 9.5367431640625e-07f;
+                    if (!(raw_cut == raw_cut)) raw_cut = -INFINITY;  // an infinite cut filters nothing here
+                }
+                auto process = [&](const uint32_t(&v)[32], uint32_t c) {
+                    // A padding lane (no query: past nq, or an empty slot of a gathered block) scores
+                    // whatever its query row holds, +inf included; it never survives, since its
+                    // index would address past the per-query outputs.
+                    if (!valid_q) return;
+                    // Almost every group of 32 scores is rejected by its largest one (a 5-level tree).
+                    float m16[16];
+#pragma unroll
+                    for (uint32_t j = 0; j < 16; ++j) m16[j] = fmaxf(__uint_as_float(v[j]), __uint_as_float(v[j + 16]));
+#pragma unroll
+                    for (uint32_t h = 8; h > 0; h >>= 1)
+#pragma unroll
+                        for (uint32_t j = 0; j < h; ++j) m16[j] = fmaxf(m16[j], m16[j + h]);
+                    if (!(m16[0] >= raw_cut)) return;
+                    uint32_t mask = 0;
+#pragma unroll
+                    for (uint32_t j = 0; j < 32; ++j) {
+                        float s = __uint_as_float(v[j]);
+                        if (kFp8) s = (s * sc[c * 32 + j]) * qs;
+                        mask |= (s >= st.cut ? 1u : 0u) << j;
+                    }
+                    while (mask) {  // survivors are rare once a threshold exists
+                        const uint32_t j = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        const uint64_t row = tile_row0 + c * 32 + j;
+                        if (row >= row_end) continue;
+                        if (kMode == 1) {
+                            // pass 2 keeps every row that passed the cut (the largest bound slack over
+                            // all rows: a superset of the rows whose own bound reaches T); in item mode
+                            // the row is a reordered position, mapped to its row by the rerank
+                            my_stage[staged++] = static_cast<uint32_t>(row);
+                            if (staged == kPass2Stage) flush_stage();
+                            continue;
+                        }
+                        float s = pick(v, j);
+                        if (kFp8) s = (s * sc[c * 32 + j]) * qs;
+                        // The row's own bound when pass 1 may certify (every tile scanned); a sampled
+                        // pass 1 only yields T, and the largest slack spares a dependent load per
+                        // survivor. In item mode the key holds the list position (the rerank maps it).
+                        const float u = per_row_bound ? fmaf(p.row_resid[row], b_mul, s + b_add) : s + slack;
+                        epi_survivor<kMode>(p, st, heap, lrow, q, u, row, slack);
+                    }
+                };
+#pragma unroll
+                for (uint32_t cc = 0; cc < kChunks; cc += 2) {
+                    const uint32_t c = c_begin + cc;
+                    // tcgen05.ld and tcgen05.wait::ld are .sync.aligned: the whole warp executes each
+                    // one together. process() loops per lane over its survivors (one lane may take
+                    // every row while the others take none), so the warp reconverges before each.
+                    __syncwarp();
+                    tc::tmem_ld32(taddr + (c + 1) * 32, vb);
+                    process(va, c);
+                    __syncwarp();
+                    tmem_wait_ld_regs(vb);
+                    if (cc + 2 < kChunks) tc::tmem_ld32(taddr + (c + 2) * 32, va);
+                    process(vb, c + 1);
+                    if (cc + 2 < kChunks) {
+                        __syncwarp();
+                        tmem_wait_ld_regs(va);
+                    }
+                }
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[buf]);
+            }
+            if (kMode == 1 && staged) flush_stage();
+            if (kMode == 0 && valid_q) {
+                uint64_t* dst = kItems ? p.ws_keys + static_cast<size_t>(p.it_lane_slot[q0 + lrow] + w.chunk) * p.kprime
+                                       : p.ws_keys + (static_cast<size_t>(q) * nranges + range) * p.kprime;
+                for (uint32_t i = 0; i < p.kprime; ++i) dst[i] = i < st.n ? heap[i * kM + lrow] : 0ull;
+                if (st.n == p.heap_k) atomicMax(&p.thr_global[q], static_cast<unsigned long long>(heap[lrow]));
+            }
         }
     }
     // ---------------- teardown: release TMEM ----------------
@@ -770,6 +879,14 @@ static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
     if (e != cudaSuccess) return e;
     dim3 grid = kItems ? dim3(a.items, 1)
                        : (a.p.live_q ? dim3(a.live_items, 1) : dim3((a.p.nq + kM * kQB - 1) / (kM * kQB), a.nranges));
+    if (kItems) {
+        // persistent: as many CTAs as fit on the device at once, each looping over items
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, tc_threads<kMode>(), smem);
+        if (e != cudaSuccess) return e;
+        const uint64_t resident = static_cast<uint64_t>(per_sm > 0 ? per_sm : 1) * (a.p.sm_count ? a.p.sm_count : 1u);
+        grid.x = static_cast<uint32_t>(a.items < resident ? a.items : resident);
+    }
     TcParams p = a.p;
     p.kprime = kp;
     if (sync_check_enabled())
