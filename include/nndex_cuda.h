@@ -362,7 +362,7 @@ NNDEX_API int nndex_cuda_set_graphs(nndex_cuda_index* index, int enable);
  * rounded up to powers of two, nprobe and precision — runs every plan that returns the same
  * results (the FP32 scan or the TF32 candidate scan for small batches; BF16 or FP8 tensor-core
  * scans with pass-1 tile strides 1, 8 and 32 for large ones; the FP32 or the tensor-core IVF list
- * scan, the latter with pass-1 strides 1, 4 and 16), times each, and keeps the fastest for later
+ * scan, the latter with pass-1 strides 1, 2, 4 and 16), times each, and keeps the fastest for later
  * batches of that shape. mode 0: the fixed
  * rules. mode 2: the cached plans, and the rules for shapes not in the cache (no batch pays for
  * measurements; the serving loop's slots run so, with the cache the index had when the server

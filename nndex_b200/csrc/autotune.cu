@@ -175,8 +175,10 @@ std::vector<CudaIndex::TunePlan> CudaIndex::tune_candidates(uint64_t nq, uint64_
         const TcPlan p1 = plan_tc(kcap, false);
         if (precision != NNDEX_PRECISION_FP32 && nq >= 64 && ivf->d_reordered16 && p1.kp >= kcap && p1.kp > 0 &&
             plan_tc(0, false).stages > 0) {
-            // the tensor-core list scan with a full pass 1, or on every 4th or 16th tile of its lists
+            // the tensor-core list scan with a full pass 1, or on every 2nd, 4th or 16th tile of its
+            // lists (a denser sample gives a tighter T and fewer rows to re-score)
             c.push_back({5, 1});
+            c.push_back({5, 2});
             c.push_back({5, 4});
             c.push_back({5, 16});
         }
