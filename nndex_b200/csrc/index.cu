@@ -597,7 +597,10 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
     // Autotuned: when the last batch rarely certified in pass 1, pass 1 only has to produce each
     // query's threshold T, and a sample of the rows (every 8th tile) gives a valid one.
     // The tuner's plan may fix it instead (only bases of ≥ 64 tiles are sampled).
-    const uint32_t want = forced_stride ? forced_stride : tc_sample_stride;
+    // At k ≥ 64 the rules start sampled: a full pass 1 then carries the largest heaps and almost
+    // never certifies (the k′ the shared memory allows is little above k), and the rule's state is
+    // shared with the index's small-k batches, which may keep it at 1.
+    const uint32_t want = forced_stride ? forced_stride : (kcap >= 64 ? 8u : tc_sample_stride);
     const uint32_t stride = (want > 1 && rows >= 256ull * 64) ? want : 1;
     if ((st = grow_device(d_thr, cap_thr, n, "tc workspace"))) return st;
     if ((st = grow_device(d_ws, cap_ws, per_query * n, "tc workspace"))) return st;

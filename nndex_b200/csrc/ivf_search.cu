@@ -600,6 +600,16 @@ cudaError_t launch_scan(const CUtensorMap& tmap, const IvfScanArgs& a, uint32_t 
     return cudaGetLastError();
 }
 
+// The sampled pass-1 stride of the tensor-core list scan's rules.
+uint32_t ivf_sampled_stride() {
+    static const uint32_t sampled = [] {
+        const char* v = getenv("NNDEX_IVF_TC_STRIDE");  // measurement override of the sampled stride
+        const uint32_t x = v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
+        return x >= 2 && x <= 16 ? x : 4u;
+    }();
+    return sampled;
+}
+
 // Queries per probe scoring block: the most (8, 4, 2 or 1) held as doubles in shared memory; 0 if
 // not even one fits.
 uint32_t probe_qb(uint64_t dp, size_t smem_optin) {
@@ -869,7 +879,9 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     // Like the exact path's pass 1: when pass 1 rarely certifies, it only has to give each query its
     // threshold T, and every 4th tile of its lists gives a valid one (the rule lives in
     // ivf_finish_tc).
-    const uint32_t stride = ix.forced_stride ? ix.forced_stride : w.tc_stride;  // a tuned plan may fix it
+    // a tuned plan may fix the stride; at k ≥ 64 the rules start sampled (a full pass 1 then carries
+    // the largest heaps and almost never certifies)
+    const uint32_t stride = ix.forced_stride ? ix.forced_stride : (k >= 64 ? ivf_sampled_stride() : w.tc_stride);
     a.p.tile_stride = stride;
     a.p.heap_k = stride > 1 ? std::max(1u, std::min(kp, k)) : kp;  // a sampled pass 1 only yields T
     a.p.it_item_off = w.d_item_off;
@@ -882,8 +894,7 @@ int ivf_search_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
     a.p.row_map = v.d_row_map;
     a.p.it_nlist = nlist;
     a.p.it_chunk_rows = kChunkRows;
-    a.p.sm_count = static_cast<uint32_t>(ix.sm_count);  // the persistent item grid
-    a.p.it_next = w.d_counters + 8;                      // its CTAs take items from this counter
+    a.p.it_next = w.d_counters + 8;  // the CTAs take items from this counter
     cudaEvent_t ev_a = nullptr;
     ix.scan_event_begin(s, ev_a);
     e = launch_scan_tc(a, false, 0, s);
@@ -978,13 +989,9 @@ int ivf_finish_tc(CudaIndex& ix, uint32_t nq, uint32_t k, uint64_t* o_idx, float
             if (!ix.h_ids[i]) total += std::min<uint32_t>(ix.h_ok2[i], kSecondPassCap);
         ix.stats.pass2_rows += total;
     }
-    if (!ix.forced_stride && w.tc_stride == 1 && m * 2 > nq) {
-        static const uint32_t sampled = [] {
-            const char* v = getenv("NNDEX_IVF_TC_STRIDE");  // measurement override of the sampled stride
-            const uint32_t x = v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
-            return x >= 2 && x <= 16 ? x : 4u;
-        }();
-        w.tc_stride = sampled;
+    // the rule learns from batches that ran its own stride (a full pass 1 that certified few)
+    if (!ix.forced_stride && w.tc_stride == 1 && ix.stats.pass1_tile_stride == 1 && m * 2 > nq) {
+        w.tc_stride = ivf_sampled_stride();
         ix.drop_graphs();  // a captured batch keeps its stride
     }
     if (failed_n == 0) return NNDEX_OK;

@@ -224,12 +224,15 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         range = static_cast<uint32_t>(blockIdx.x / nqb);
         nranges = static_cast<uint32_t>(nr);
     }
-    // The CTA's work: one (query block, row range) in the grid modes. In item mode the CTA is
-    // persistent: its producer thread takes the plan's items (each a chunk of one list × one
-    // gathered query block) from a global counter and hands each item's id to the MMA and epilogue
-    // warps through two shared-memory slots; TMEM, barriers and the base ring stay across items,
-    // so the next item's base tiles stream while the last one's epilogue drains.
+    // The CTA's work: one (query block, row range) in the grid modes. In item mode its producer
+    // thread takes up to kItemsPerCta of the plan's items (each a chunk of one list × one gathered
+    // query block) from a global counter and hands each item's id to the MMA and epilogue warps
+    // through two shared-memory slots; TMEM, barriers and the base ring stay across them, so the
+    // next item's base tiles stream while the last one's epilogue drains. (With one CTA per SM
+    // taking every item, the kernel held all SMs until its last item and other streams' kernels
+    // waited behind it.)
     constexpr uint32_t kNoItem = 0xFFFFFFFFu;
+    constexpr uint32_t kItemsPerCta = 4;
     uint32_t total = 0;
     if (kItems) {
         total = p.it_item_off[p.it_nlist];
@@ -315,7 +318,7 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
                         record_status(p.status, kStatusTimeout);
                         break;
                     }
-                    const unsigned long long g = atomicAdd(p.it_next, 1ull);
+                    const unsigned long long g = j < kItemsPerCta ? atomicAdd(p.it_next, 1ull) : ~0ull;
                     wi = g < total ? static_cast<uint32_t>(g) : kNoItem;
                     witem[slot] = wi;
                     mbar_arrive(&wfull[slot]);
@@ -879,14 +882,8 @@ static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
     if (e != cudaSuccess) return e;
     dim3 grid = kItems ? dim3(a.items, 1)
                        : (a.p.live_q ? dim3(a.live_items, 1) : dim3((a.p.nq + kM * kQB - 1) / (kM * kQB), a.nranges));
-    if (kItems) {
-        // persistent: as many CTAs as fit on the device at once, each looping over items
-        int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, tc_threads<kMode>(), smem);
-        if (e != cudaSuccess) return e;
-        const uint64_t resident = static_cast<uint64_t>(per_sm > 0 ? per_sm : 1) * (a.p.sm_count ? a.p.sm_count : 1u);
-        grid.x = static_cast<uint32_t>(a.items < resident ? a.items : resident);
-    }
+    // item mode: one CTA per item of the bound; each takes up to kItemsPerCta items from the counter
+    // and exits, so CTAs of other streams' kernels get SMs between them
     TcParams p = a.p;
     p.kprime = kp;
     if (sync_check_enabled())
