@@ -677,6 +677,57 @@ NNDEX_DEVICE_INLINE float dot_scan_order(const float* __restrict__ x, const floa
     return acc;
 }
 
+// The same sum with the query in shared memory (`ys`): kU of the row's slabs are in flight per lane.
+template <uint32_t kU>
+NNDEX_DEVICE_INLINE float dot_scan_order_sq(const float* __restrict__ x, const float* ys, uint32_t nbox, uint32_t ch,
+                                            bool live) {
+    float acc = 0.0f;
+    if (live) {
+        const float* xa = x + ch * 4;
+        const float* ya = ys + ch * 4;
+        uint32_t bx = 0;
+        for (; bx + kU <= nbox; bx += kU) {
+            float4 a[kU];
+#pragma unroll
+            for (uint32_t u = 0; u < kU; ++u) a[u] = __ldg(reinterpret_cast<const float4*>(xa + (bx + u) * 32));
+#pragma unroll
+            for (uint32_t u = 0; u < kU; ++u) {
+                const float4 b = *reinterpret_cast<const float4*>(ya + (bx + u) * 32);
+                acc = fmaf(a[u].x, b.x, acc);
+                acc = fmaf(a[u].y, b.y, acc);
+                acc = fmaf(a[u].z, b.z, acc);
+                acc = fmaf(a[u].w, b.w, acc);
+            }
+        }
+        if (kU > 4 && bx + 4 <= nbox) {  // a half batch before the last slabs (D = 384: 8 + 4)
+            float4 a[4];
+#pragma unroll
+            for (uint32_t u = 0; u < 4; ++u) a[u] = __ldg(reinterpret_cast<const float4*>(xa + (bx + u) * 32));
+#pragma unroll
+            for (uint32_t u = 0; u < 4; ++u) {
+                const float4 b = *reinterpret_cast<const float4*>(ya + (bx + u) * 32);
+                acc = fmaf(a[u].x, b.x, acc);
+                acc = fmaf(a[u].y, b.y, acc);
+                acc = fmaf(a[u].z, b.z, acc);
+                acc = fmaf(a[u].w, b.w, acc);
+            }
+            bx += 4;
+        }
+        for (; bx < nbox; ++bx) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(xa + bx * 32));
+            const float4 b = *reinterpret_cast<const float4*>(ya + bx * 32);
+            acc = fmaf(a.x, b.x, acc);
+            acc = fmaf(a.y, b.y, acc);
+            acc = fmaf(a.z, b.z, acc);
+            acc = fmaf(a.w, b.w, acc);
+        }
+    }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+    return acc;
+}
+
 // ------------------------------------------------------------------------------------------
 // K4 (pass 1): exact FP32 rerank of the k′ candidates + top-k + certificate + T. One block per query.
 // ------------------------------------------------------------------------------------------
@@ -802,6 +853,9 @@ __global__ void __launch_bounds__(256)
     const uint32_t ch = threadIdx.x & 7u, slot = threadIdx.x >> 3, nslots = blockDim.x >> 3;
     const float* qv = queries + static_cast<size_t>(q) * ds;
     const uint32_t nbox = ds / 32;
+    // the query in shared memory, so the registers hold eight of a row's slabs in flight
+    extern __shared__ __align__(16) float q_s[];
+    for (uint32_t d = threadIdx.x; d < ds; d += blockDim.x) q_s[d] = qv[d];
     if (threadIdx.x == 0) fill = 0;
     __syncthreads();
     for (uint32_t j0 = j_begin; j0 < j_end; j0 += nslots) {
@@ -809,7 +863,7 @@ __global__ void __launch_bounds__(256)
         const bool on = j < j_end;
         const uint32_t pos = on ? rows2[static_cast<size_t>(qrow) * cap2 + j] : 0u;
         const uint32_t row = row_map && on ? row_map[pos] : pos;
-        const float acc = dot_scan_order<4>(vecs + static_cast<size_t>(row_map ? pos : row) * ds, qv, nbox, ch, on);
+        const float acc = dot_scan_order_sq<8>(vecs + static_cast<size_t>(row_map ? pos : row) * ds, q_s, nbox, ch, on);
         const bool take = ch == 0 && on && acc >= t;
         const uint32_t at = warp_append(&fill, take);
         if (take) keys[at] = make_key(acc, row);
@@ -980,8 +1034,14 @@ cudaError_t launch_rerank_collected(const float* vecs, uint32_t ds, const float*
     if (m == 0) return cudaSuccess;
     const uint32_t chunks = rerank_chunks(cap2);
     if (k == 0 || k > kRerankChunk || chunks > 65535u) return cudaErrorInvalidValue;
-    rerank_chunk_kernel<<<dim3(m, chunks), 256, 0, stream>>>(vecs, ds, queries, ids, rows2, cnt2, cap2, k,
-                                                            by_query ? 1 : 0, live, row_map, thr, slot_keys);
+    const size_t qsmem = static_cast<size_t>(ds) * sizeof(float);
+    if (qsmem > 48 * 1024) {
+        const cudaError_t ea = cudaFuncSetAttribute(rerank_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    static_cast<int>(qsmem));
+        if (ea != cudaSuccess) return ea;
+    }
+    rerank_chunk_kernel<<<dim3(m, chunks), 256, qsmem, stream>>>(vecs, ds, queries, ids, rows2, cnt2, cap2, k,
+                                                                by_query ? 1 : 0, live, row_map, thr, slot_keys);
     uint32_t p2 = 1;
     while (p2 < k) p2 <<= 1;
     const size_t smem = std::max<size_t>(static_cast<size_t>(chunks) * k, p2) * sizeof(uint64_t);
