@@ -449,12 +449,17 @@ CudaIndex::Tf32Plan CudaIndex::plan_tf32(uint64_t nq, uint64_t kcap) const {
     // 100th and 256th scores of a query are ≈ 2.4e-3 apart, twice the bound's typical ε)
     const uint64_t kp = std::min<uint64_t>(512, (std::max<uint64_t>(kcap * 5 / 2, kcap + 64) + 31) / 32 * 32);
     if (rows < 4 * kp || rows > 0xFFFFFFFFull) return p;
-    // Room for three tiles of survivors above k′: a selection runs once ≥ 256 keys have
+    // Each CTA lists a quarter of k′ (at least 32): the k′ best of a query come from all 148 CTAs,
+    // and the rows a full list left out score below the largest full-list minimum (the floor),
+    // which the certificate then also has to clear.
+    const uint32_t kp_cta = static_cast<uint32_t>(std::max<uint64_t>(32, (kp / 4 + 31) / 32 * 32));
+    // Room for three tiles of survivors above the list: a selection runs once ≥ 256 keys have
     // accumulated since the last one, not after every tile.
-    const uint32_t cap = static_cast<uint32_t>(kp) + 3 * 128;
+    const uint32_t cap = kp_cta + 3 * 128;
     const uint32_t stages = tf32_stages_for(cap, smem_optin);
     if (!stages) return p;
     p.kp = static_cast<uint32_t>(kp);
+    p.kp_cta = kp_cta;
     p.cap = cap;
     p.stages = stages;
     return p;
@@ -868,7 +873,7 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     if (!plan.kp) return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: no TF32 scan plan for k=%u", kcap);
     const uint32_t kp = plan.kp;
     const uint32_t ctas = static_cast<uint32_t>(sm_count);
-    const uint64_t per_query = static_cast<uint64_t>(ctas) * kp;
+    const uint64_t per_query = static_cast<uint64_t>(ctas) * plan.kp_cta;
     // the FP32 scan that re-runs uncertified queries shares the candidate workspace
     ScanPlan fb_plan;
     if (!plan_scan_fp32(n, static_cast<uint32_t>(ds), kcap, sm_count, smem_optin, fb_plan))
@@ -900,7 +905,7 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     a.nbox = static_cast<uint32_t>(ds / 32);
     a.ds = static_cast<uint32_t>(ds);
     a.rows = rows;
-    a.kp = kp;
+    a.kp = plan.kp_cta;
     a.cap = plan.cap;
     a.queries = d_qn;
     a.row_norms = d_tfnorm;
@@ -924,7 +929,6 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     m.idx_out = d_cand_idx;
     m.sim_out = d_cand_sim;
     m.count_out = d_cand_cnt;
-    m.floor_keys = d_floor;
     if ((st = merge_workspace(per_query, n, kp, m, s))) return st;
     if ((e = launch_merge_topk(m, s)) != cudaSuccess) return cuda_error(e, "merge launch");
     RerankArgs r;
@@ -943,6 +947,7 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     r.cert_out = d_cert;
     r.kth_out = d_kth;
     r.certify = true;
+    r.floor_keys = d_floor;  // rows the CTAs' lists left out score below it
     r.fb_ids = d_fbq;
     r.fb_count = d_fbn;
     cudaMemsetAsync(d_fbn, 0, sizeof(uint32_t), s);

@@ -259,7 +259,9 @@ struct CudaIndex {
     int choose_path(uint64_t nq, uint64_t kcap) const;
     // K12's plan for k results: candidates per query and CTA (0: no plan), buffer, ring depth.
     struct Tf32Plan {
-        uint32_t kp = 0, cap = 0, stages = 0;
+        uint32_t kp = 0;      // candidates per query after the merge (k′)
+        uint32_t kp_cta = 0;  // candidates per query and CTA
+        uint32_t cap = 0, stages = 0;
     };
     Tf32Plan plan_tf32(uint64_t nq, uint64_t kcap) const;
     float tf32_c_norm() const;  // C of K12's bound: ε = ‖q‖(‖d_x‖ + C‖x‖) + ‖d_q‖(‖x‖ + ‖d_x‖)

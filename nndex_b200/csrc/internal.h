@@ -89,9 +89,6 @@ struct MergeArgs {
     uint64_t* part_keys = nullptr;
     uint32_t* part_done = nullptr;
     const uint32_t* live = nullptr;     // optional: a device count; queries at or past it are skipped
-    // optional, per query: a key the k-th best is known to reach (the scan's largest full-list
-    // minimum); smaller keys are dropped before the selection
-    const unsigned long long* floor_keys = nullptr;
     const uint32_t* out_rows = nullptr;  // optional: query q's results go to output row out_rows[q]
 };
 uint32_t merge_parts(uint64_t per_query, uint32_t k);
@@ -177,7 +174,7 @@ struct Tf32ScanArgs {
     uint64_t* ws_keys = nullptr;       // nq × ctas × kp
     // optional, nq keys zeroed before the launch: the largest over CTAs of the smallest key of a
     // full (kp-key) list. Every row a CTA did not list has a smaller key than its list's smallest,
-    // so the global kp-th key reaches it.
+    // so every row outside the lists stays below it (the certificate must clear it).
     unsigned long long* floor_keys = nullptr;
     uint32_t* status = nullptr;
 };
@@ -221,6 +218,9 @@ struct RerankArgs {
     // optional (IVF): candidates are list positions; base is read by position, results carry
     // row_map[position]
     const uint32_t* row_map = nullptr;
+    // optional, per query: a key every row outside the candidate lists stays below (their largest
+    // full-list minimum); the certificate must clear it too
+    const unsigned long long* floor_keys = nullptr;
 };
 cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream);
 // q2_lp holds m rounded up to 128 rows (whole query blocks); the rows past m are written as zeros.

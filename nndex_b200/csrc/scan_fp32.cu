@@ -356,7 +356,6 @@ __global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restr
                                                          uint64_t* __restrict__ part_keys,
                                                          uint32_t* __restrict__ part_done,
                                                          const uint32_t* __restrict__ live,
-                                                         const unsigned long long* __restrict__ floor_keys,
                                                          const uint32_t* __restrict__ out_rows) {
     if (live && blockIdx.y >= *live) return;  // a fallback merge: only the queries re-run
     __shared__ BlockSelectScratch s;
@@ -371,33 +370,12 @@ __global__ void __launch_bounds__(512) merge_topk_kernel(const uint64_t* __restr
         merge_final(keys, per_query, k, oq, out_stride, idx_out, sim_out, count_out, s, smem_keys);
         return;
     }
-    // This block's share: lists [l0, l1) of k keys each.
-    const uint64_t lists = per_query / k;
-    const uint64_t l0 = lists * blockIdx.x / parts, l1 = lists * (blockIdx.x + 1) / parts;
-    const uint64_t n = (l1 - l0) * k;
-    const uint64_t* src = keys + l0 * k;
+    // This block's share of the query's keys.
+    const uint64_t i0 = per_query * blockIdx.x / parts, i1 = per_query * (blockIdx.x + 1) / parts;
+    const uint64_t n = i1 - i0;
+    const uint64_t* src = keys + i0;
     uint64_t* dst = part_keys + (static_cast<size_t>(q) * parts + blockIdx.x) * k;
-    // With a floor (a key the query's k-th best reaches), one pass keeps the share's keys at or
-    // above it; when no more than k remain they are the share's candidates, with no selection.
-    bool kept = false;
-    if (floor_keys) {
-        const uint64_t fl = floor_keys[q];
-        if (threadIdx.x == 0) s.count = 0;
-        __syncthreads();
-        if (fl) {
-            for (uint64_t i0 = 0; i0 < n; i0 += blockDim.x) {
-                const uint64_t i = i0 + threadIdx.x;
-                const uint64_t key = i < n ? src[i] : 0ull;
-                const bool take = i < n && key >= fl;
-                const uint32_t pos = warp_append(&s.count, take);
-                if (take && pos < k) dst[pos] = key;
-            }
-        }
-        __syncthreads();
-        kept = fl && s.count <= k;
-        __syncthreads();
-    }
-    if (!kept) {
+    {
         uint64_t kth = 0ull;
         if (n > k) kth = block_radix_kth(src, n, k, s);
         if (threadIdx.x == 0) s.count = 0;
@@ -699,7 +677,7 @@ cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream) {
     }
     merge_topk_kernel<<<dim3(parts, a.nq), 512, smem, stream>>>(a.ws_keys, a.per_query, a.k, a.out_stride, a.idx_out,
                                                                 a.sim_out, a.count_out, parts, a.part_keys,
-                                                                a.part_done, a.live, a.floor_keys, a.out_rows);
+                                                                a.part_done, a.live, a.out_rows);
     count_launch();
     return cudaGetLastError();
 }

@@ -637,49 +637,10 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
 // by slab with FMA; then ((c0+c1)+(c2+c3)) + ((c4+c5)+(c6+c7)). Called by 8 consecutive lanes (one
 // per ch); every lane returns the full sum. So a query's scores are bit-identical on every path.
 // ------------------------------------------------------------------------------------------
-// kU slabs' loads are issued before their FMAs (a row is a gather: its loads must overlap); the FMAs
-// stay in slab order.
+// The query is in shared memory (`ys`): kU of the row's slabs (a gather) are loaded before their
+// FMAs, which stay in slab order.
 template <uint32_t kU>
-NNDEX_DEVICE_INLINE float dot_scan_order(const float* __restrict__ x, const float* __restrict__ y, uint32_t nbox,
-                                         uint32_t ch, bool live) {
-    float acc = 0.0f;
-    if (live) {
-        const float* xa = x + ch * 4;
-        const float* ya = y + ch * 4;
-        uint32_t bx = 0;
-        for (; bx + kU <= nbox; bx += kU) {
-            float4 a[kU], b[kU];
-#pragma unroll
-            for (uint32_t u = 0; u < kU; ++u) {
-                a[u] = __ldg(reinterpret_cast<const float4*>(xa + (bx + u) * 32));
-                b[u] = __ldg(reinterpret_cast<const float4*>(ya + (bx + u) * 32));
-            }
-#pragma unroll
-            for (uint32_t u = 0; u < kU; ++u) {
-                acc = fmaf(a[u].x, b[u].x, acc);
-                acc = fmaf(a[u].y, b[u].y, acc);
-                acc = fmaf(a[u].z, b[u].z, acc);
-                acc = fmaf(a[u].w, b[u].w, acc);
-            }
-        }
-        for (; bx < nbox; ++bx) {
-            const float4 a = __ldg(reinterpret_cast<const float4*>(xa + bx * 32));
-            const float4 b = __ldg(reinterpret_cast<const float4*>(ya + bx * 32));
-            acc = fmaf(a.x, b.x, acc);
-            acc = fmaf(a.y, b.y, acc);
-            acc = fmaf(a.z, b.z, acc);
-            acc = fmaf(a.w, b.w, acc);
-        }
-    }
-    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-    acc += __shfl_xor_sync(0xffffffffu, acc, 4);
-    return acc;
-}
-
-// The same sum with the query in shared memory (`ys`): kU of the row's slabs are in flight per lane.
-template <uint32_t kU>
-NNDEX_DEVICE_INLINE float dot_scan_order_sq(const float* __restrict__ x, const float* ys, uint32_t nbox, uint32_t ch,
+NNDEX_DEVICE_INLINE float dot_scan_order(const float* __restrict__ x, const float* ys, uint32_t nbox, uint32_t ch,
                                             bool live) {
     float acc = 0.0f;
     if (live) {
@@ -737,8 +698,9 @@ __global__ void __launch_bounds__(1024, 1)
                   const uint32_t* __restrict__ cand_cnt, uint32_t kp, uint32_t k, uint64_t* __restrict__ idx_out,
                   float* __restrict__ sim_out, uint32_t* __restrict__ cnt_out, uint32_t* __restrict__ cert_out,
                   float* __restrict__ kth_out, int certify, uint32_t* __restrict__ fb_ids,
-                  uint32_t* __restrict__ fb_count, const uint32_t* __restrict__ row_map) {
-    extern __shared__ uint64_t keys[];
+                  uint32_t* __restrict__ fb_count, const uint32_t* __restrict__ row_map,
+                  const unsigned long long* __restrict__ floor_keys) {
+    extern __shared__ uint64_t keys[];  // p2(kp) keys, then the query (ds floats)
     const uint32_t q = blockIdx.x;
     const uint32_t ch = threadIdx.x & 7u, slot = threadIdx.x >> 3;  // 8 lanes per candidate
     const uint32_t nslots = blockDim.x >> 3;
@@ -747,12 +709,16 @@ __global__ void __launch_bounds__(1024, 1)
     while (p2 < kp) p2 <<= 1;
     const float* qv = queries + static_cast<size_t>(q) * ds;
     const uint32_t nbox = ds / 32;
+    // the query in shared memory, so the registers hold eight of a row's slabs in flight
+    float* q_s = reinterpret_cast<float*>(keys + p2);
+    for (uint32_t d = threadIdx.x; d < ds; d += blockDim.x) q_s[d] = qv[d];
+    __syncthreads();
     for (uint32_t j0 = 0; j0 < p2; j0 += nslots) {
         const uint32_t j = j0 + slot;
         const bool live = j < n;
         const uint64_t cand = live ? cand_idx[static_cast<size_t>(q) * kp + j] : 0;
         const uint32_t row = row_map && live ? row_map[cand] : static_cast<uint32_t>(cand);
-        const float acc = dot_scan_order<4>(base + cand * ds, qv, nbox, ch, live);
+        const float acc = dot_scan_order<8>(base + cand * ds, q_s, nbox, ch, live);
         if (ch == 0 && j < p2) keys[j] = live ? make_key(acc, row) : 0ull;
     }
     __syncthreads();
@@ -766,9 +732,16 @@ __global__ void __launch_bounds__(1024, 1)
         if (cnt_out) cnt_out[q] = kk;
         // Every row outside the k′ candidates has an exact score ≤ the k′-th upper bound; an exact
         // k-th score above it proves the top-k exact.
+        // Rows outside the candidates: those the merge left out (bound ≤ the k′-th bound, when it
+        // had k′) and those a full per-CTA list left out (bound ≤ the floor). With neither, every
+        // row was a candidate and the result is exact as it stands.
         uint32_t ok = certify ? 1u : 0u;
-        if (certify && n >= kp && kk > 0)
-            ok = key_score(keys[kk - 1]) > cand_bound[static_cast<size_t>(q) * kp + kp - 1] ? 1u : 0u;
+        const unsigned long long fk = floor_keys ? floor_keys[q] : 0ull;
+        if (certify && kk > 0 && (n >= kp || fk)) {
+            float bound = n >= kp ? cand_bound[static_cast<size_t>(q) * kp + kp - 1] : -INFINITY;
+            if (fk) bound = fmaxf(bound, key_score(fk));
+            ok = key_score(keys[kk - 1]) > bound ? 1u : 0u;
+        }
         cert_out[q] = ok;
         if (fb_count && !ok) fb_ids[atomicAdd(fb_count, 1u)] = q;  // for the FP32 scan
         // T: the exact k-th score among the candidates, a lower bound of the true k-th; with fewer
@@ -863,7 +836,7 @@ __global__ void __launch_bounds__(256)
         const bool on = j < j_end;
         const uint32_t pos = on ? rows2[static_cast<size_t>(qrow) * cap2 + j] : 0u;
         const uint32_t row = row_map && on ? row_map[pos] : pos;
-        const float acc = dot_scan_order_sq<8>(vecs + static_cast<size_t>(row_map ? pos : row) * ds, q_s, nbox, ch, on);
+        const float acc = dot_scan_order<8>(vecs + static_cast<size_t>(row_map ? pos : row) * ds, q_s, nbox, ch, on);
         const bool take = ch == 0 && on && acc >= t;
         const uint32_t at = warp_append(&fill, take);
         if (take) keys[at] = make_key(acc, row);
@@ -1002,10 +975,16 @@ cudaError_t launch_rerank(const RerankArgs& a, cudaStream_t stream) {
     // One block per query; a small batch leaves most SMs idle, so its blocks take 1024 threads (128
     // candidates re-scored at once instead of 32) to keep more row loads in flight.
     const uint32_t threads = a.nq < 64 ? 1024u : 256u;
-    rerank_kernel<<<a.nq, threads, p2 * sizeof(uint64_t), stream>>>(a.base, a.ds, a.queries, a.cand_idx, a.cand_sim,
+    const size_t smem = p2 * sizeof(uint64_t) + static_cast<size_t>(a.ds) * sizeof(float);
+    if (smem > 48 * 1024) {
+        const cudaError_t ea =
+            cudaFuncSetAttribute(rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (ea != cudaSuccess) return ea;
+    }
+    rerank_kernel<<<a.nq, threads, smem, stream>>>(a.base, a.ds, a.queries, a.cand_idx, a.cand_sim,
                                                                a.cand_cnt, a.kp, a.k, a.idx_out, a.sim_out,
                                                                a.cnt_out, a.cert_out, a.kth_out, a.certify ? 1 : 0,
-                                                               a.fb_ids, a.fb_count, a.row_map);
+                                                               a.fb_ids, a.fb_count, a.row_map, a.floor_keys);
     count_launch();
     return cudaGetLastError();
 }
