@@ -101,12 +101,13 @@ NNDEX_DEVICE_INLINE uint64_t warp_radix_kth(const float* scores, uint32_t n, uin
         }
         const uint32_t excl = incl - local;
         const uint32_t owner = __ffs(__ballot_sync(0xFFFFFFFFu, excl < krem && krem <= incl)) - 1;
-        uint32_t bin = 0, above = excl;
+        uint32_t bin = 0, above = excl, in_bin = 0;
         if (lane == owner) {
 #pragma unroll
             for (uint32_t b = 0; b < 8; ++b) {
                 if (above + c[b] >= krem) {
                     bin = 255u - (lane * 8u + b);
+                    in_bin = c[b];
                     break;
                 }
                 above += c[b];
@@ -114,18 +115,32 @@ NNDEX_DEVICE_INLINE uint64_t warp_radix_kth(const float* scores, uint32_t n, uin
         }
         bin = __shfl_sync(0xFFFFFFFFu, bin, owner);
         above = __shfl_sync(0xFFFFFFFFu, above, owner);
+        in_bin = __shfl_sync(0xFFFFFFFFu, in_bin, owner);
         prefix |= static_cast<uint64_t>(bin) << shift;
         mask |= 0xFFull << shift;
         krem -= above;
         __syncwarp();
+        if (in_bin == krem) {
+            // every key of this bin is selected: the k-th is the smallest of them
+            uint64_t m = ~0ull;
+            for (uint32_t i = lane; i < n; i += 32) {
+                const uint64_t key = make_key(scores[i], i);
+                if ((key & mask) == prefix && key < m) m = key;
+            }
+            return warp_min_u64(m);
+        }
     }
     return prefix;
 }
 
-constexpr uint32_t kProbeThreads = 256;  // centroids per scoring block
+constexpr uint32_t kProbeCentroids = 256;  // centroids per scoring block
+constexpr uint32_t kProbeThreads = 128;    // two centroids per thread
 
 static size_t probe_smem(uint32_t qb, uint64_t dp) { return static_cast<size_t>(qb) * dp * 8; }
 
+// Each thread scores two centroids (c and c + 128) against the block's QB queries: every query
+// value read from shared memory feeds two FMAs (one FMA per read left the kernel waiting on its
+// shared-memory loads, the FP64 pipe 36 % busy).
 template <int QB>
 __global__ void __launch_bounds__(kProbeThreads)
     ivf_probe_score_kernel(const float* __restrict__ queries, uint32_t nq, uint32_t ds, uint32_t dp,
@@ -140,22 +155,33 @@ __global__ void __launch_bounds__(kProbeThreads)
         qd[i] = j < nb ? static_cast<double>(queries[static_cast<uint64_t>(q0 + j) * ds + d]) : 0.0;
     }
     __syncthreads();
-    const uint32_t c = blockIdx.y * kProbeThreads + threadIdx.x;
-    if (c >= nlist) return;
-    double acc[QB];
+    const uint32_t c0 = blockIdx.y * kProbeCentroids + threadIdx.x, c1 = c0 + kProbeThreads;
+    if (c0 >= nlist) return;
+    const bool two = c1 < nlist;
+    double a0[QB], a1[QB];
 #pragma unroll
-    for (int j = 0; j < QB; ++j) acc[j] = 0.0;
-    const float* col = cent_t + c;
-#pragma unroll 8
+    for (int j = 0; j < QB; ++j) a0[j] = a1[j] = 0.0;
+    const float* col0 = cent_t + c0;
+    const float* col1 = cent_t + (two ? c1 : c0);
+#pragma unroll 4
     for (uint32_t d = 0; d < dp; ++d) {
-        const double cv = static_cast<double>(__ldg(col + static_cast<uint64_t>(d) * ct_stride));
+        const double v0 = static_cast<double>(__ldg(col0 + static_cast<uint64_t>(d) * ct_stride));
+        const double v1 = static_cast<double>(__ldg(col1 + static_cast<uint64_t>(d) * ct_stride));
         const double* qv = qd + static_cast<size_t>(d) * QB;
 #pragma unroll
-        for (int j = 0; j < QB; ++j) acc[j] = fma(cv, qv[j], acc[j]);
+        for (int j = 0; j < QB; ++j) {
+            const double x = qv[j];
+            a0[j] = fma(v0, x, a0[j]);
+            a1[j] = fma(v1, x, a1[j]);
+        }
     }
 #pragma unroll
     for (int j = 0; j < QB; ++j)
-        if (j < static_cast<int>(nb)) scores[static_cast<uint64_t>(q0 + j) * nlist + c] = fold_zero(__double2float_rn(acc[j]));
+        if (j < static_cast<int>(nb)) {
+            float* row = scores + static_cast<uint64_t>(q0 + j) * nlist;
+            row[c0] = fold_zero(__double2float_rn(a0[j]));
+            if (two) row[c1] = fold_zero(__double2float_rn(a1[j]));
+        }
 }
 
 __global__ void __launch_bounds__(256)
@@ -637,7 +663,7 @@ cudaError_t launch_probe_qb(const ProbeLaunch& a, cudaStream_t s) {
     const size_t smem = probe_smem(QB, a.dp);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    const dim3 grid((a.nq + QB - 1) / QB, (a.nlist + kProbeThreads - 1) / kProbeThreads);
+    const dim3 grid((a.nq + QB - 1) / QB, (a.nlist + kProbeCentroids - 1) / kProbeCentroids);
     kern<<<grid, kProbeThreads, smem, s>>>(a.queries, a.nq, a.ds, a.dp, a.cent_t, a.ct_stride, a.nlist, a.scores);
     return cudaGetLastError();
 }
@@ -646,7 +672,7 @@ cudaError_t launch_probe_qb(const ProbeLaunch& a, cudaStream_t s) {
 // plan's scans, the pairs).
 cudaError_t launch_probe_plan(uint32_t pqb, const ProbeLaunch& a, uint32_t qb, IvfScratch& w, uint32_t* qblock_off,
                               cudaStream_t s) {
-    if ((a.nlist + kProbeThreads - 1) / kProbeThreads > 65535u) return cudaErrorInvalidValue;
+    if ((a.nlist + kProbeCentroids - 1) / kProbeCentroids > 65535u) return cudaErrorInvalidValue;
     cudaError_t e;
     switch (pqb) {
         case 8: e = launch_probe_qb<8>(a, s); break;

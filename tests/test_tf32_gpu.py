@@ -108,3 +108,26 @@ def test_tf32_scan_ties_fall_back_to_the_fp32_scan():
     assert st["path"] == 6 and st["fp32_fallback_queries"] == 12, st
     ti, _ = index.search(q, k=20)
     assert ti[0].tolist() == list(range(5_000, 5_020))
+
+
+@pytest.mark.parametrize("k", [10, 100])
+def test_tf32_scan_rows_sorted_by_cluster(k):
+    # Each CTA lists a quarter of k′ per query; rows outside the lists are covered by the floor
+    # (the largest full-list minimum) in the certificate. With the base sorted by cluster, a query's
+    # neighbours crowd into a few CTAs, whose lists leave true candidates out: the results must
+    # still equal the FP32 scan's, bit for bit, certified or re-run.
+    rng = np.random.default_rng(61 + k)
+    centers = np.random.default_rng(62).normal(size=(64, 256)).astype(np.float32)
+    assign = np.sort(rng.integers(0, 64, size=150_000))
+    m = (centers[assign] + np.float32(0.2) * rng.normal(size=(150_000, 256)).astype(np.float32)).astype(np.float32)
+    q = (centers[rng.integers(0, 64, size=16)] + np.float32(0.2) * rng.normal(size=(16, 256))).astype(np.float32)
+    index = NNdex(m, autotune=False)
+    st = _equal_to_fp32_scan(index, q, k)
+    assert st["path"] == 6, st
+    # and against the FP64 oracle
+    idx, sim = index.search(q, k=k)
+    stb, base = O.prepare_index(m, False)
+    assert stb == 0
+    _, qn = O.prepare_queries(q, False, base.shape[1])
+    for i in range(q.shape[0]):
+        assert_topk_matches(idx[i], sim[i], O.scores_f64(base, qn[i]), k, what=f"sorted k={k} q{i}")
