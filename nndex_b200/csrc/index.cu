@@ -182,21 +182,25 @@ static int grow_device(T*& p, size_t& cap, size_t n, const char* what) {
     cap = n;
     return NNDEX_OK;
 }
+// Pinned buffers grow geometrically from 4,096 elements: releasing one (cudaFreeHost) waits for
+// the device, which in a serving slot means waiting for the other slots' batches too, so they are
+// replaced as rarely as possible.
 template <class T>
 static int grow_host(T*& p, size_t& cap, size_t n, const char* what) {
     if (n <= cap && p) return NNDEX_OK;
     bump_alloc_epoch();
     if (p) cudaFreeHost(p);
     p = nullptr;
+    const size_t want = std::max<size_t>({n, cap * 2, 4096});
     cap = 0;
     cudaError_t e = take_injected_alloc_failure()
                         ? cudaErrorMemoryAllocation
-                        : cudaMallocHost(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
+                        : cudaMallocHost(reinterpret_cast<void**>(&p), want * sizeof(T));
     if (e != cudaSuccess) {
         p = nullptr;
         return cuda_error(e, what);
     }
-    cap = n;
+    cap = want;
     return NNDEX_OK;
 }
 

@@ -694,14 +694,17 @@ cudaError_t launch_probe_plan(uint32_t pqb, const ProbeLaunch& a, uint32_t qb, I
 
 template <class T>
 int grow_pinned(T*& p, size_t& cap, size_t n, const char* what) {
+    // geometric from 4,096 elements: releasing a pinned buffer waits for the device (in a serving
+    // slot, for the other slots' batches too)
     if (n <= cap && p) return NNDEX_OK;
     bump_alloc_epoch();
     cudaFreeHost(p);
     p = nullptr;
+    const size_t want = std::max<size_t>({n, cap * 2, 4096});
     cap = 0;
-    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T));
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), want * sizeof(T));
     if (e != cudaSuccess) return cuda_error(e, what);
-    cap = n;
+    cap = want;
     return NNDEX_OK;
 }
 
