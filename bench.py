@@ -984,8 +984,10 @@ def run_serve(args, dev, L, world):
     so.slots = args.serve_slots
     so.latency_budget_ms = args.serve_latency_ms
     srv = C.c_void_p()
+    t_start = time.perf_counter()
     if L.nndex_cuda_server_start(h, C.byref(so), C.byref(srv)) != 0:
         raise RuntimeError(_lib.last_error())
+    start_s = time.perf_counter() - t_start  # the slots' warm-up batches included
     rng = np.random.default_rng(seed)
     mean_size = (1 + 256) / 2
     out = {}
@@ -1087,6 +1089,7 @@ def run_serve(args, dev, L, world):
                     f"{args.serve_slots} slots, admission by free HBM and a {args.serve_latency_ms} ms "
                     f"queue-drain budget",
         "create_s_with_ivf_build": create_s,
+        "server_start_s_with_warmup": start_s,
         "by_offered_rate": out,
         "batches": sst.batches,
         "mean_batch_queries": sst.queries_done / max(sst.batches, 1),

@@ -286,6 +286,55 @@ int nndex_cuda_server_start(nndex_cuda_index* index, const nndex_cuda_server_opt
     srv->st.slots = o.slots;
     srv->st.max_batch_queries = o.max_batch_queries;
     srv->st.slot_bytes = o.slot_bytes;
+    // Warm-up, before any request: every slot runs each kind of batch once (exact and, with an IVF,
+    // approximate at the default nprobe; k = 1, 10 and 100; 16, 256 and the largest batch a slot
+    // admits), on the index's first rows as queries. CUDA loads a kernel on its first launch (about
+    // 130 ms for the first tensor-core batch), and a slot's buffers grow with its largest batch;
+    // both would otherwise fall on the first requests of each kind while the other slots run on.
+    const uint64_t wn = std::min<uint64_t>(o.max_batch_queries, ix->rows);
+    if (wn) {
+        std::vector<float> wq(wn * ix->dims);
+        cudaError_t e = cudaMemcpy2D(wq.data(), ix->dims * sizeof(float), ix->d_base, ix->ds * sizeof(float),
+                                     ix->dims * sizeof(float), wn, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_error(e, "server warm-up");
+        const int mode = ix->normalized ? 2 : 0;
+        Server* sv = srv.get();
+        std::vector<std::thread> warm;
+        for (uint32_t i = 0; i < o.slots; ++i)
+            warm.emplace_back([sv, &wq, wn, mode, i] {
+                CudaIndex* v = sv->views[i];
+                const CudaIndex* x = sv->ix;
+                cudaSetDevice(x->device);
+                set_scratch_stream(v->stream);
+                std::vector<uint64_t> bi, bc;
+                std::vector<float> bs;
+                for (int approx = 0; approx <= (x->ivf ? 1 : 0); ++approx)
+                    for (uint64_t k : {1ull, 10ull, 100ull}) {
+                        const uint64_t kc = std::min<uint64_t>(k, x->rows);
+                        uint32_t np = 0;
+                        if (approx) {
+                            const uint64_t d = x->ivf_scratch.nprobe ? x->ivf_scratch.nprobe
+                                                                     : ivf_choose_nprobe(x->ivf->nlist, kc, x->rows);
+                            np = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(d, x->ivf->nlist)));
+                        }
+                        uint64_t top = wn;
+                        while (top > 1 && sv->batch_bytes(top, kc, approx, np) > sv->opts.slot_bytes) top /= 2;
+                        for (uint64_t n : {uint64_t{16}, uint64_t{256}, top}) {
+                            const uint64_t nq = std::min<uint64_t>(n, top);
+                            bi.resize(nq * kc);
+                            bs.resize(nq * kc);
+                            bc.resize(nq);
+                            v->approx_override = approx;
+                            v->ivf_scratch.nprobe = np;
+                            v->search_host(wq.data(), nq, kc, mode, bi.data(), bs.data(), bc.data());
+                        }
+                    }
+                v->approx_override = -1;
+                v->ivf_scratch.nprobe = x->ivf_scratch.nprobe;
+                clear_error();
+            });
+        for (auto& t : warm) t.join();
+    }
     Server* s = srv.get();
     for (uint32_t i = 0; i < o.slots; ++i) s->workers.emplace_back([s, i] { s->worker(i); });
     *out = new nndex_cuda_server{srv.release()};
