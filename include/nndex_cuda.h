@@ -132,7 +132,8 @@ typedef struct nndex_cuda_search_stats {
     uint64_t pass2_rows;            /* tensor-core paths: rows the second pass collected (summed
                                        over its queries) and re-scored in FP32                  */
     uint32_t pass2_query_blocks;    /* paths 2/3: 128-query blocks per CTA of the second pass
-                                       (2 = two blocks against 128-row base tiles; 0 = no pass) */
+                                       (2 = two blocks against 128-row base tiles; 3 = one block
+                                       per CTA of a CTA pair sharing 256-row tiles; 0 = no pass) */
     uint32_t reserved0;
 } nndex_cuda_search_stats;
 

@@ -111,6 +111,28 @@ NNDEX_DEVICE_INLINE bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long 
     return true;
 }
 
+// ---- thread-block clusters -------------------------------------------------------------
+
+NNDEX_DEVICE_INLINE uint32_t cluster_ctarank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// The shared::cluster address of the variable at `p` in the cluster's CTA `rank`.
+NNDEX_DEVICE_INLINE uint32_t cluster_map(const void* p, uint32_t rank) {
+    uint32_t a;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+    return a;
+}
+// One arrival on an mbarrier of any CTA of the cluster (release at cluster scope).
+NNDEX_DEVICE_INLINE void mbar_arrive_cluster(uint32_t bar_cluster) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+// Every thread of every CTA of the cluster (all of them execute it).
+NNDEX_DEVICE_INLINE void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 // ≈1 s at B200 clocks: far above any legitimate wait in these kernels.
 constexpr long long kWaitBudgetCycles = 2000000000ll;
 
@@ -127,6 +149,17 @@ NNDEX_DEVICE_INLINE void tma_load_2d(void* dst, const void* tmap, uint64_t* bar,
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
         " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(tmap)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// CTA pair (cta_group::2): the box lands in this CTA's shared memory at `dst` and its bytes complete
+// on the mbarrier at shared::cluster address `bar_cluster` (the pair's even CTA's barrier). No
+// multicast: each CTA loads its own box.
+NNDEX_DEVICE_INLINE void tma_load_2d_pair(void* dst, const void* tmap, uint32_t bar_cluster, int32_t x, int32_t y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(bar_cluster), "r"(x), "r"(y)
         : "memory");
 }
 

@@ -769,11 +769,15 @@ int CudaIndex::enqueue_tc_pass2(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o
     // the base bytes per FLOP but run M = 128, N = 128 MMAs, which read as many query bytes from
     // shared memory as base bytes. On 10M × 256 at 4,096 queries that made FP8 7 % faster and BF16
     // 7 % slower, so the rule takes it for FP8 and the autotuner times both.
+    // CTA pairs (qb = 3): two CTAs, one query block each, share every 256-row base tile through
+    // M = 256 MMAs, so each SM reads half the base bytes per FLOP without narrowing the MMA.
     const uint32_t want_qb = forced_qb ? forced_qb : (fp8 ? 2u : 1u);
     const uint32_t pair_stages = (want_qb == 2 && n > 128) ? tc_pair_stages_for(tc_chunks(fp8), fp8, smem_optin) : 0;
-    if (pair_stages) {
-        a.qb = 2;
-        a.stages = pair_stages;
+    const uint32_t cta_pair_stages =
+        (want_qb == 3 && n > 128) ? tc_cta_pair_stages_for(tc_chunks(fp8), fp8, smem_optin) : 0;
+    if (pair_stages || cta_pair_stages) {
+        a.qb = pair_stages ? 2 : 3;
+        a.stages = pair_stages ? pair_stages : cta_pair_stages;
         a.stream_a = false;
         a.tmap_b = fp8 ? &tmap_fp8_h : &tmap_bf16_h;
     }

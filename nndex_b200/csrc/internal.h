@@ -148,7 +148,8 @@ struct TcArgs {
     bool stream_a = false;                // pass 1: query slabs staged per ring stage, not resident
     uint32_t items = 0;                   // IVF item mode: number of work items (grid), 0 = off
     uint32_t live_items = 0;              // pass 2 with p.live_q: CTAs launched (an upper bound)
-    uint32_t qb = 1;                      // pass 2: query blocks per CTA (2: 128-row base tiles)
+    uint32_t qb = 1;                      // pass 2: query blocks per CTA (2: 128-row base tiles;
+                                          // 3: one per CTA of a CTA pair, 128 of the pair's 256 rows)
 };
 size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8, bool stream_a, uint32_t qb = 1);
 // Deepest base ring (4, 3 or 2 stages) that fits k′ heaps in `smem_limit`; 0 if none fits.
@@ -156,6 +157,8 @@ uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, bool stream_
 // Pass 2 with two resident query blocks per CTA: the deepest ring (5 or 4 stages of 128-row slabs)
 // that fits beside both blocks' query slabs; 0 if none (large D).
 uint32_t tc_pair_stages_for(uint32_t nchunks, bool fp8, size_t smem_limit);
+// Ring stages of a CTA-pair pass 2 (TcArgs::qb = 3) that fit, 0 when none does.
+uint32_t tc_cta_pair_stages_for(uint32_t nchunks, bool fp8, size_t smem_limit);
 cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t stream);
 
 // K12: FP32-accurate candidate scan on the tensor cores (three TF32 products per K step), 16

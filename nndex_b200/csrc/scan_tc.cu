@@ -79,9 +79,12 @@ NNDEX_DEVICE_INLINE float pick(const uint32_t (&v)[32], uint32_t j) {
 }  // namespace
 
 size_t tc_smem_bytes(uint32_t nchunks, uint32_t kprime, uint32_t stages, bool fp8, bool stream_a, uint32_t qb) {
+    // qb: 1 = one resident query block and 256-row stages, 2 = two blocks and 128-row stages,
+    // 3 = one block per CTA of a CTA pair and 128-row stages (the pair's tile is 256 rows)
+    const size_t a_blocks = qb == 2 ? 2 : 1, stage_b = qb == 1 ? kBChunk : kBChunk / 2;
     size_t b = 1024;
     b += stream_a ? static_cast<size_t>(stages) * (kAChunk + kBChunk)
-                  : static_cast<size_t>(qb) * nchunks * kAChunk + static_cast<size_t>(stages) * (kBChunk / qb);
+                  : a_blocks * nchunks * kAChunk + static_cast<size_t>(stages) * stage_b;
     b += static_cast<size_t>(kprime) * kM * 8;
     if (kprime == 0) b += static_cast<size_t>(kPass2Stage) * 8 * 32 * 4;  // pass 2: survivor staging
     b += (2 * stages + 10) * 8 + 16;
@@ -97,6 +100,12 @@ uint32_t tc_stages_for(uint32_t nchunks, uint32_t kprime, bool fp8, bool stream_
 uint32_t tc_pair_stages_for(uint32_t nchunks, bool fp8, size_t smem_limit) {
     for (uint32_t st = 5; st >= 4; --st)
         if (tc_smem_bytes(nchunks, 0, st, fp8, false, 2) <= smem_limit) return st;
+    return 0;
+}
+
+uint32_t tc_cta_pair_stages_for(uint32_t nchunks, bool fp8, size_t smem_limit) {
+    for (uint32_t st : {8u, 6u})
+        if (tc_smem_bytes(nchunks, 0, st, fp8, false, 3) <= smem_limit) return st;
     return 0;
 }
 
@@ -173,15 +182,24 @@ NNDEX_DEVICE_INLINE void epi_survivor(const TcParams& p, EpiState& st, uint64_t*
 // Each slab of a base tile feeds two MMAs (M = 128, N = 128), one per block, into the two halves of
 // the 256-column accumulator, so a CTA reads half the base bytes per FLOP: the pass is otherwise
 // bound by how fast L2 feeds the base tiles (1 byte per 128 FLOPs). The tile map's box is 128 rows.
-template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems, int kQB>
+// kPair (pass 2 only): CTA pairs (a cluster of two) share each 256-row base tile: each CTA loads
+// its own query block and 128 of the tile's rows, and the even CTA issues M = 256, N = 256 MMAs
+// (cta_group::2) over both CTAs' shared memory into both CTAs' TMEM, so each SM reads half the base
+// bytes per FLOP at the full MMA shape. The barriers that gate MMAs (slabs landed, query blocks
+// landed, accumulators drained) are the even CTA's, armed for both CTAs' bytes and arrivals; the
+// MMA completions arrive on both CTAs' barriers (slab free, accumulator ready). The tile map's box
+// is 128 rows.
+template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems, int kQB, bool kPair = false>
 __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     scan_tc_kernel(const __grid_constant__ CUtensorMap tmap_q, const __grid_constant__ CUtensorMap tmap_b,
                    const TcParams p) {
     static_assert(kQB == 1 || (kQB == 2 && kMode == 1 && !kStreamA && !kItems), "two query blocks: pass 2 only");
+    static_assert(!kPair || (kQB == 1 && kMode == 1 && !kStreamA && !kItems), "CTA pairs: pass 2 only");
     constexpr uint32_t kNT = kQB == 2 ? kN / 2 : kN;  // base rows per tile (MMA N)
+    constexpr uint32_t kLoadRows = kPair ? kN / 2 : kNT;  // base rows per tile this CTA loads
     constexpr uint32_t kQC = kM * kQB;                // queries per CTA
     constexpr uint32_t kElems = kFp8 ? 128 : 64;      // K elements per 128-byte slab
-    constexpr uint32_t kStage = kStreamA ? kAChunk + kBChunk : kNT * 128;
+    constexpr uint32_t kStage = kStreamA ? kAChunk + kBChunk : kLoadRows * 128;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = align_1024(smem_raw);
     uint8_t* a_smem = smem;  // resident query slabs (kStreamA: none), block-major
@@ -201,6 +219,8 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     volatile uint32_t* witem = tmem_slot + 2;  // [2]
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t rank = kPair ? cluster_ctarank() : 0u;  // the CTA's place in its pair
+    const bool leader = rank == 0;                          // pairs: the even CTA issues the MMAs
     uint32_t grid_q0 = blockIdx.x * kQC;
     uint32_t range = blockIdx.y, nranges = gridDim.y;
     uint64_t range_rows = p.range_rows;
@@ -217,11 +237,21 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         range_rows = (p.rows + nr - 1) / nr;
         range_rows = (range_rows + 255) / 256 * 256;
         nr = (p.rows + range_rows - 1) / range_rows;
-        if (blockIdx.x >= nqb * nr) return;
-        // consecutive CTAs take the query blocks of one row range, as the 2-D grid orders them: the
-        // CTAs resident together read the same base tiles, which then come from L2 after the first
-        grid_q0 = static_cast<uint32_t>(blockIdx.x % nqb) * kQC;
-        range = static_cast<uint32_t>(blockIdx.x / nqb);
+        if (kPair) {
+            // pairs of query blocks (the last one may have no queries: its CTA still loads its half
+            // of the base tiles); both CTAs of a pair return here, or neither
+            const uint64_t npairs = (nqb + 1) / 2, pair = blockIdx.x >> 1;
+            if (pair >= npairs * nr) return;
+            grid_q0 = static_cast<uint32_t>((pair % npairs) * 2 + rank) * kQC;
+            range = static_cast<uint32_t>(pair / npairs);
+        } else {
+            if (blockIdx.x >= nqb * nr) return;
+            // consecutive CTAs take the query blocks of one row range, as the 2-D grid orders them:
+            // the CTAs resident together read the same base tiles, which then come from L2 after
+            // the first
+            grid_q0 = static_cast<uint32_t>(blockIdx.x % nqb) * kQC;
+            range = static_cast<uint32_t>(blockIdx.x / nqb);
+        }
         nranges = static_cast<uint32_t>(nr);
     }
     // The CTA's work: one (query block, row range) in the grid modes. In item mode its producer
@@ -285,17 +315,24 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], epi_warps<kMode>());
+            mbar_init(&tempty[b], (kPair ? 2 : 1) * epi_warps<kMode>());  // pairs: both CTAs' epilogues
         }
         *abort_flag = 0;
         fence_mbar_init();
     }
     if (warp == 1) {
-        tc::tmem_alloc(tmem_slot, kTmemCols);
-        tc::tmem_relinquish();
+        if constexpr (kPair) {
+            tc::tmem_alloc_pair(tmem_slot, kTmemCols);
+            tc::tmem_relinquish_pair();
+        } else {
+            tc::tmem_alloc(tmem_slot, kTmemCols);
+            tc::tmem_relinquish();
+        }
     }
     tc::fence_before_sync();
-    __syncthreads();
+    // pairs: the other CTA's barriers are initialised before any copy or arrival reaches them
+    if (kPair) cluster_sync_all();
+    else __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem_base = *tmem_slot;
 
@@ -336,11 +373,21 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
                         stop = true;
                         break;
                     }
-                    mbar_arrive_expect_tx(a_full, w.nblk * nchunks * kAChunk);
-                    for (uint32_t b = 0; b < w.nblk; ++b)
+                    if constexpr (kPair) {
+                        // both CTAs' query blocks complete on the even CTA's barrier
+                        if (leader) mbar_arrive_expect_tx(a_full, 2u * nchunks * kAChunk);
+                        const uint32_t a_bar = cluster_map(a_full, 0);
                         for (uint32_t c = 0; c < nchunks; ++c)
-                            tma_load_2d(a_smem + static_cast<size_t>(b * nchunks + c) * kAChunk, &tmap_q, a_full,
-                                        static_cast<int32_t>(c * kElems), static_cast<int32_t>(w.q0 + b * kM));
+                            tma_load_2d_pair(a_smem + static_cast<size_t>(c) * kAChunk, &tmap_q, a_bar,
+                                             static_cast<int32_t>(c * kElems), static_cast<int32_t>(w.q0));
+                    } else {
+                        mbar_arrive_expect_tx(a_full, w.nblk * nchunks * kAChunk);
+                        for (uint32_t b = 0; b < w.nblk; ++b)
+                            for (uint32_t c = 0; c < nchunks; ++c)
+                                tma_load_2d(a_smem + static_cast<size_t>(b * nchunks + c) * kAChunk, &tmap_q,
+                                            a_full, static_cast<int32_t>(c * kElems),
+                                            static_cast<int32_t>(w.q0 + b * kM));
+                    }
                     ++a_loads;
                 }
                 for (uint32_t t = 0; t < w.ntiles && !stop; ++t) {
@@ -358,29 +405,51 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
                             break;
                         }
                         uint8_t* stage = b_smem + static_cast<size_t>(s) * kStage;
-                        mbar_arrive_expect_tx(&full_bar[s], kStage);
-                        if (kStreamA)
-                            tma_load_2d(stage + kBChunk, &tmap_q, &full_bar[s], static_cast<int32_t>(c * kElems),
-                                        static_cast<int32_t>(w.q0));
-                        tma_load_2d(stage, &tmap_b, &full_bar[s], static_cast<int32_t>(c * kElems), y);
+                        if constexpr (kPair) {
+                            // this CTA's 128 rows of the pair's 256-row tile; both halves complete on
+                            // the even CTA's barrier, which expects both
+                            if (leader) mbar_arrive_expect_tx(&full_bar[s], 2u * kStage);
+                            tma_load_2d_pair(stage, &tmap_b, cluster_map(&full_bar[s], 0),
+                                             static_cast<int32_t>(c * kElems),
+                                             y + static_cast<int32_t>(rank * kLoadRows));
+                        } else {
+                            mbar_arrive_expect_tx(&full_bar[s], kStage);
+                            if (kStreamA)
+                                tma_load_2d(stage + kBChunk, &tmap_q, &full_bar[s], static_cast<int32_t>(c * kElems),
+                                            static_cast<int32_t>(w.q0));
+                            tma_load_2d(stage, &tmap_b, &full_bar[s], static_cast<int32_t>(c * kElems), y);
+                        }
                         ++it;
                     }
                 }
             }
-            // Drain every copy this thread issued before the CTA may exit.
-            if (!kStreamA && a_loads > 0 && !mbar_wait_bounded(a_full, (a_loads - 1) & 1u, kWaitBudgetCycles))
+            // Drain every copy this thread issued before the CTA may exit. (Pairs: the odd CTA's copies
+            // complete on the even CTA's barriers, which the even CTA drains; neither CTA leaves the
+            // closing cluster barrier before the other reaches it.)
+            if (!kStreamA && a_loads > 0 && leader &&
+                !mbar_wait_bounded(a_full, (a_loads - 1) & 1u, kWaitBudgetCycles))
                 record_status(p.status, kStatusTimeout);
-            const uint32_t used = it < static_cast<uint32_t>(kST) ? it : kST;
+            const uint32_t used = !leader ? 0u : (it < static_cast<uint32_t>(kST) ? it : kST);
             for (uint32_t s = 0; s < used; ++s) {
                 const uint32_t uses = (it - s + kST - 1) / kST;
                 if (!mbar_wait_bounded(&full_bar[s], (uses - 1) & 1u, kWaitBudgetCycles))
                     record_status(p.status, kStatusTimeout);
             }
+            if (kPair) {
+                // the even CTA's MMA completions also arrive on this CTA's slab barriers: wait for the
+                // last one of every slab before the CTA may leave
+                const uint32_t used_e = it < static_cast<uint32_t>(kST) ? it : kST;
+                for (uint32_t s = 0; s < used_e; ++s) {
+                    const uint32_t uses = (it - s + kST - 1) / kST;
+                    if (!mbar_wait_bounded(&empty_bar[s], (uses - 1) & 1u, kWaitBudgetCycles))
+                        record_status(p.status, kStatusTimeout);
+                }
+            }
         }
     } else if (warp == 1) {
-        // ---------------- MMA issuer ----------------
-        if (lane == 0) {
-            constexpr uint32_t idesc = tc::instr_desc<kFp8, kM, kNT>();
+        // ---------------- MMA issuer (pairs: the even CTA's, for both) ----------------
+        if (lane == 0 && leader) {
+            constexpr uint32_t idesc = tc::instr_desc<kFp8, kPair ? 2 * kM : kM, kNT>();
             const uint32_t a_addr0 = smem_u32(a_smem), b_addr0 = smem_u32(b_smem);
             uint32_t it = 0, tg = 0;  // slabs and tiles over all of the CTA's work
             for (uint32_t j = 0;; ++j) {
@@ -432,15 +501,25 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
                                 const uint32_t a_addr =
                                     kStreamA ? b_addr + kBChunk : a_addr0 + (b * nchunks + c) * kAChunk;
 #pragma unroll
-                                for (uint32_t kk = 0; kk < 4; ++kk)
-                                    tc::mma<kFp8>(d + b * kNT, tc::smem_desc_sw128(a_addr + kk * 32),
-                                                  tc::smem_desc_sw128(b_addr + kk * 32), idesc,
-                                                  (c | kk) != 0u ? 1u : 0u);
+                                for (uint32_t kk = 0; kk < 4; ++kk) {
+                                    if constexpr (kPair)
+                                        tc::mma_pair<kFp8>(d, tc::smem_desc_sw128(a_addr + kk * 32),
+                                                           tc::smem_desc_sw128(b_addr + kk * 32), idesc,
+                                                           (c | kk) != 0u ? 1u : 0u);
+                                    else
+                                        tc::mma<kFp8>(d + b * kNT, tc::smem_desc_sw128(a_addr + kk * 32),
+                                                      tc::smem_desc_sw128(b_addr + kk * 32), idesc,
+                                                      (c | kk) != 0u ? 1u : 0u);
+                                }
                             }
                         }
-                        tc::commit(&empty_bar[s]);  // frees the slab once the MMAs above have read it
+                        // frees the slab (pairs: in both CTAs) once the MMAs above have read it
+                        if constexpr (kPair) tc::commit_pair(&empty_bar[s], 0x3);
+                        else tc::commit(&empty_bar[s]);
                     }
-                    tc::commit(&tfull[buf]);  // the accumulator is complete
+                    // the accumulator is complete (pairs: both CTAs' halves)
+                    if constexpr (kPair) tc::commit_pair(&tfull[buf], 0x3);
+                    else tc::commit(&tfull[buf]);
                 }
             }
         }
@@ -610,7 +689,10 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
                 }
                 tc::fence_before_sync();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&tempty[buf]);
+                if (lane == 0) {
+                    if (kPair) mbar_arrive_cluster(cluster_map(&tempty[buf], 0));  // the MMA issuer's barrier
+                    else mbar_arrive(&tempty[buf]);
+                }
             }
             if (kMode == 1 && staged) flush_stage();
             if (kMode == 0 && valid_q) {
@@ -623,11 +705,14 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     }
     // ---------------- teardown: release TMEM ----------------
     tc::fence_before_sync();
-    __syncthreads();
+    // pairs: both CTAs are done with each other's shared memory, barriers and TMEM
+    if (kPair) cluster_sync_all();
+    else __syncthreads();
     if (warp == 1) {
         __syncwarp();
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem_base, kTmemCols);
+        if constexpr (kPair) tc::tmem_dealloc_pair(tmem_base, kTmemCols);
+        else tc::tmem_dealloc(tmem_base, kTmemCols);
     }
 }
 
@@ -899,16 +984,20 @@ __global__ void __launch_bounds__(256)
 // ------------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------------
-template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems = false, int kQB = 1>
+template <bool kFp8, int kST, int kMode, bool kStreamA, bool kItems = false, int kQB = 1, bool kPair = false>
 static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
-    auto kern = scan_tc_kernel<kFp8, kST, kMode, kStreamA, kItems, kQB>;
+    auto kern = scan_tc_kernel<kFp8, kST, kMode, kStreamA, kItems, kQB, kPair>;
     const uint32_t kp = kMode == 0 ? a.p.kprime : 0;
     if (kMode == 0 && (a.p.heap_k == 0 || a.p.heap_k > kp)) return cudaErrorInvalidValue;
-    const size_t smem = tc_smem_bytes(a.p.nchunks, kp, kST, kFp8, kStreamA, kQB);
+    const size_t smem = tc_smem_bytes(a.p.nchunks, kp, kST, kFp8, kStreamA, kPair ? 3 : kQB);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     dim3 grid = kItems ? dim3(a.items, 1)
                        : (a.p.live_q ? dim3(a.live_items, 1) : dim3((a.p.nq + kM * kQB - 1) / (kM * kQB), a.nranges));
+    if (kPair) {
+        // two CTAs per (pair of query blocks, row range): live_items bounds the pairs
+        grid.x = a.p.live_q ? 2u * a.live_items : (grid.x + 1u) / 2u * 2u;
+    }
     // item mode: one CTA per item of the bound; each takes up to kItemsPerCta items from the counter
     // and exits, so CTAs of other streams' kernels get SMs between them
     TcParams p = a.p;
@@ -918,6 +1007,23 @@ static cudaError_t launch_tc_impl(const TcArgs& a, cudaStream_t stream) {
                         "k' %u, tile stride %u, range rows %llu, rows %llu, smem %zu",
                         kFp8, kST, kMode, kStreamA, kItems, kQB, grid.x, grid.y, p.nq, kp, p.tile_stride,
                         (unsigned long long)p.range_rows, (unsigned long long)p.rows, smem);
+    if (kPair) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = dim3(tc_threads<kMode>());
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, kern, *a.tmap_q, *a.tmap_b, p);
+        count_launch();
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     kern<<<grid, tc_threads<kMode>(), smem, stream>>>(*a.tmap_q, *a.tmap_b, p);
     count_launch();
     return cudaGetLastError();
@@ -957,6 +1063,16 @@ cudaError_t launch_scan_tc(const TcArgs& a, bool fp8, int mode, cudaStream_t str
                                : launch_tc_impl<false, 5, 1, false, false, 2>(a, stream);
             case 4: return fp8 ? launch_tc_impl<true, 4, 1, false, false, 2>(a, stream)
                                : launch_tc_impl<false, 4, 1, false, false, 2>(a, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    if (mode == 1 && a.qb == 3) {
+        if (a.stream_a || a.p.range_rows % kN) return cudaErrorInvalidValue;
+        switch (a.stages) {
+            case 8: return fp8 ? launch_tc_impl<true, 8, 1, false, false, 1, true>(a, stream)
+                               : launch_tc_impl<false, 8, 1, false, false, 1, true>(a, stream);
+            case 6: return fp8 ? launch_tc_impl<true, 6, 1, false, false, 1, true>(a, stream)
+                               : launch_tc_impl<false, 6, 1, false, false, 1, true>(a, stream);
             default: return cudaErrorInvalidValue;
         }
     }

@@ -61,6 +61,31 @@ NNDEX_DEVICE_INLINE void mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, ui
     }
 }
 
+// CTA-pair MMA (cta_group::2), issued by one thread of the pair's even CTA: M = 256 query rows, 128
+// in each CTA's shared memory at the same offset (the descriptors' addresses), and N base rows, N/2
+// in each CTA's shared memory; each CTA's TMEM receives its own 128 rows × N columns at tmem_d,
+// columns [0, N/2) from the even CTA's B rows and [N/2, N) from the odd CTA's.
+template <bool kFp8>
+NNDEX_DEVICE_INLINE void mma_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                  uint32_t accumulate) {
+    const uint32_t z = 0;
+    if constexpr (kFp8) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f8f6f4 [%0], %1, %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}"
+            ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}"
+            ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z)
+            : "memory");
+    }
+}
+
 // D[tmem] (+)= A[smem] · B[smem]ᵀ with TF32 inputs (32-bit containers; the MMA uses the sign,
 // exponent and top 10 mantissa bits), issued by one thread.
 NNDEX_DEVICE_INLINE void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -88,6 +113,16 @@ NNDEX_DEVICE_INLINE void commit(uint64_t* bar) {
                  : "memory");
 }
 
+// CTA pair: the mbarrier at the same offset `bar` in every CTA of `cta_mask` receives one arrival
+// when the pair's tcgen05 operations issued by this thread before the commit have completed.
+NNDEX_DEVICE_INLINE void commit_pair(uint64_t* bar, uint16_t cta_mask) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"(cta_mask)
+        : "memory");
+}
+
 NNDEX_DEVICE_INLINE void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 NNDEX_DEVICE_INLINE void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -102,6 +137,19 @@ NNDEX_DEVICE_INLINE void tmem_relinquish() {
 }
 NNDEX_DEVICE_INLINE void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// CTA pair: one warp of each CTA (the same warp) allocates the same columns in both CTAs' TMEM.
+NNDEX_DEVICE_INLINE void tmem_alloc_pair(uint32_t* dst_smem, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+                 "r"(ncols)
+                 : "memory");
+}
+NNDEX_DEVICE_INLINE void tmem_relinquish_pair() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+NNDEX_DEVICE_INLINE void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
 // Each thread of the warp reads 32 consecutive 32-bit columns of its own TMEM lane.

@@ -97,6 +97,8 @@ def test_autotune_cache_text_is_validated_without_a_gpu():
     assert L.nndex_cuda_autotune_validate(good, C.byref(n)) == 0 and n.value == 2
     two = good + b"shape ivf=0 nq=256 k=16 precision=1 nprobe=0 plan path=2 stride=8 qb=2 ms=20.5\n"
     assert L.nndex_cuda_autotune_validate(two, C.byref(n)) == 0 and n.value == 3
+    pair = two + b"shape ivf=0 nq=512 k=16 precision=1 nprobe=0 plan path=2 stride=8 qb=3 ms=30.5\n"  # CTA pairs
+    assert L.nndex_cuda_autotune_validate(pair, C.byref(n)) == 0 and n.value == 4
     bad = [
         b"shape ivf=0 nq=16 k=128 precision=0 nprobe=0 plan path=6 stride=0 qb=0 ms=0.5\n",  # no header
         good + b"shape ivf=0 nq=12 k=128 precision=0 nprobe=0 plan path=1 stride=0 qb=0 ms=1\n",  # nq not 2^n
@@ -104,7 +106,7 @@ def test_autotune_cache_text_is_validated_without_a_gpu():
         good + b"shape ivf=1 nq=16 k=16 precision=0 nprobe=8 plan path=2 stride=0 qb=0 ms=1\n",  # exact path, IVF shape
         good + b"shape ivf=0 nq=16 k=16 precision=0 nprobe=0 plan path=9 stride=0 qb=0 ms=1\n",  # no such path
         good + b"shape ivf=0 nq=16 k=16 precision=0 nprobe=0 plan path=1 stride=0 qb=2 ms=1\n",  # qb off path 2/3
-        good + b"shape ivf=0 nq=256 k=16 precision=1 nprobe=0 plan path=2 stride=8 qb=3 ms=1\n",  # qb above 2
+        good + b"shape ivf=0 nq=256 k=16 precision=1 nprobe=0 plan path=2 stride=8 qb=4 ms=1\n",  # qb above 3
         good + b"shape ivf=0 nq=256 k=16 precision=1 nprobe=0 plan path=2 stride=8 ms=1\n",  # no qb field
         good + b"garbage\n",
     ]

@@ -172,11 +172,17 @@ def test_overflowing_collection_reruns_on_the_fp32_scan():
     ("bf16", 100, 200, 1),
     ("fp8", 150, 170, 2),
     ("fp8", 150, 170, 1),
+    ("bf16", 250, 50, 3),    # CTA pairs: one pair, the odd CTA's block empty
+    ("bf16", 100, 200, 3),   # one pair, both blocks partly filled
+    ("bf16", 100, 600, 3),   # five blocks: three pairs, the last CTA's block empty
+    ("fp8", 150, 170, 3),
 ])
 def test_pass2_query_blocks_per_cta(precision, certifying, uncertified, qb):
     # Pass 2 of a batch of more than 128 queries can put two query blocks in each CTA against
-    # 128-row base tiles (the plan's qb, fixed here through the autotuner's cache). The number of
-    # live queries decides on the device how many blocks a CTA loads and multiplies. Queries equal
+    # 128-row base tiles, or run CTA pairs (qb 3: one block per CTA, M = 256 MMAs over both CTAs'
+    # shared memory, each CTA loading half of every 256-row tile) — the plan's qb, fixed here
+    # through the autotuner's cache. The number of live queries decides on the device how many
+    # blocks (or pairs) there are; a block without queries still loads its half of the tiles. Queries equal
     # to a base row of a mixture certify in pass 1 (their top-1 scores 1, their cluster about 0.94);
     # a query with 40 near-duplicate rows (scores about 1e-4 apart, inside the bound slack) cannot
     # certify with k' = 32 and takes pass 2. Results equal the oracle's and the FP32 path's.
