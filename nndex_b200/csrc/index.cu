@@ -681,11 +681,7 @@ int CudaIndex::enqueue_tc(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o_idx, 
 // Row ranges of the tensor-core grid: about four waves of CTAs, each range a multiple of the
 // 256-row tile. Concurrent CTAs share ranges, so a base tile is read from HBM about once.
 void CudaIndex::tc_ranges(uint32_t nqb, uint64_t& nranges, uint64_t& range_rows) const {
-    nranges = (4ull * sm_count + nqb - 1) / nqb;
-    nranges = std::max<uint64_t>(1, std::min<uint64_t>(nranges, (rows + 2047) / 2048));
-    range_rows = (rows + nranges - 1) / nranges;
-    range_rows = (range_rows + 255) / 256 * 256;
-    nranges = (rows + range_rows - 1) / range_rows;
+    tc_range_split(rows, nqb, static_cast<uint64_t>(sm_count), nranges, range_rows);
 }
 
 void CudaIndex::fill_tc_params(bool fp8, uint32_t n, uint64_t range_rows, TcParams& p) const {
@@ -791,8 +787,9 @@ int CudaIndex::enqueue_tc_pass2(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o
     a.p.cap2 = cap2;
     a.p.live_q = d_m;
     a.p.sm_count = static_cast<uint32_t>(sm_count);
-    // (query block, row range) items for any count ≤ n: at most 4 per SM plus one per block
-    a.live_items = 4u * static_cast<uint32_t>(sm_count) + static_cast<uint32_t>(n_alloc / 128) + 1u;
+    // (query block, row range) items for any count ≤ n: at most 8 per SM plus one per block
+    // (tc_range_split: at most 8 rounds, or one range per block)
+    a.live_items = 8u * static_cast<uint32_t>(sm_count) + static_cast<uint32_t>(n_alloc / 128) + 1u;
     cudaEvent_t ev_a = nullptr;
     scan_event_begin(s, ev_a);
     e = launch_scan_tc(a, fp8, 1, s);

@@ -95,6 +95,39 @@ uint32_t merge_parts(uint64_t per_query, uint32_t k);
 cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream);
 
 // K3 tensor-core scan (BF16 / FP8), two passes, and K4 rerank.
+
+// Row ranges of a tensor-core scan grid of `groups` CTAs per range (its query blocks, or a pair's
+// two CTAs per pair). One CTA fits an SM, and every range but the last holds the same number of
+// 256-row tiles, so the launch takes ceil(groups × ranges / sms) rounds of one range's tiles: the
+// split minimises that product over 1 to 8 rounds. (Four ranges per SM with 32 query blocks made
+// 608 CTAs on 148 SMs: 4.1 rounds, the fifth with 16 CTAs and 132 SMs idle.) A range holds at
+// least 2,048 rows. The host derives pass 1's grid with it, pass 2's CTAs from the live query count.
+__host__ __device__ inline void tc_range_split(uint64_t rows, uint64_t groups, uint64_t sms, uint64_t& nranges,
+                                               uint64_t& range_rows) {
+    const uint64_t tiles = (rows + 255) / 256;
+    if (tiles == 0 || groups == 0 || sms == 0) {
+        nranges = 1;
+        range_rows = 256;
+        return;
+    }
+    uint64_t nr_max = (rows + 2047) / 2048;
+    if (nr_max < 1) nr_max = 1;
+    uint64_t best_tpr = tiles, best_cost = ~0ull;
+    for (uint64_t m = 1; m <= 8; ++m) {
+        uint64_t nr = m * sms / groups;
+        nr = nr < 1 ? 1 : (nr > nr_max ? nr_max : nr);
+        const uint64_t tpr = (tiles + nr - 1) / nr;  // tiles per range
+        const uint64_t used = (tiles + tpr - 1) / tpr;
+        const uint64_t cost = (groups * used + sms - 1) / sms * tpr;
+        if (cost < best_cost) {  // ties keep the fewer rounds
+            best_cost = cost;
+            best_tpr = tpr;
+        }
+    }
+    range_rows = best_tpr * 256;
+    nranges = (rows + range_rows - 1) / range_rows;
+}
+
 struct TcParams {
     uint32_t nq = 0;
     uint32_t nchunks = 0;                 // K bytes / 128

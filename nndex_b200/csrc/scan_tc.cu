@@ -226,17 +226,13 @@ __global__ void __launch_bounds__(tc_threads<kMode>(), 1)
     uint64_t range_rows = p.range_rows;
     uint32_t nq_live = p.nq;
     if (!kItems && p.live_q) {
-        // The device count decides the grid's shape: the same ranges tc_ranges gives the host for
-        // this many query blocks; CTAs past the work items return before any set-up.
+        // The device count decides the grid's shape (tc_range_split, as the host splits pass 1);
+        // CTAs past the work items return before any set-up.
         nq_live = *p.live_q;
         const uint64_t nqb = (nq_live + kQC - 1) / kQC;
         if (nqb == 0) return;
-        uint64_t nr = (4ull * p.sm_count + nqb - 1) / nqb;
-        const uint64_t nr_max = (p.rows + 2047) / 2048;
-        nr = nr < 1 ? 1 : (nr > nr_max ? nr_max : nr);
-        range_rows = (p.rows + nr - 1) / nr;
-        range_rows = (range_rows + 255) / 256 * 256;
-        nr = (p.rows + range_rows - 1) / range_rows;
+        uint64_t nr = 0;
+        tc_range_split(p.rows, kPair ? (nqb + 1) / 2 * 2 : nqb, p.sm_count, nr, range_rows);
         if (kPair) {
             // pairs of query blocks (the last one may have no queries: its CTA still loads its half
             // of the base tiles); both CTAs of a pair return here, or neither
