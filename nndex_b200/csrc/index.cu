@@ -341,7 +341,7 @@ int CudaIndex::merge_workspace(uint64_t per_query, uint32_t nq, uint32_t k, Merg
 int CudaIndex::enqueue_exact_fp32(const float* d_queries, uint32_t nq, uint32_t k, uint32_t out_stride,
                                   uint64_t* o_idx, float* o_sim, uint32_t* o_cnt, cudaStream_t s) {
     ScanPlan plan;
-    if (!plan_scan_fp32(nq, static_cast<uint32_t>(ds), k, sm_count, smem_optin, plan))
+    if (!plan_scan_fp32(nq, static_cast<uint32_t>(ds), k, rows, sm_count, smem_optin, plan))
         return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k=%u above the fused top-k limit %u", k,
                          kMaxFusedK);
     const uint64_t per_query = static_cast<uint64_t>(plan.ctas_per_group) * k;
@@ -881,7 +881,7 @@ int CudaIndex::enqueue_tf32(uint32_t n, uint32_t kcap, uint64_t* o_idx, float* o
     const uint64_t per_query = static_cast<uint64_t>(ctas) * plan.kp_cta;
     // the FP32 scan that re-runs uncertified queries shares the candidate workspace
     ScanPlan fb_plan;
-    if (!plan_scan_fp32(n, static_cast<uint32_t>(ds), kcap, sm_count, smem_optin, fb_plan))
+    if (!plan_scan_fp32(n, static_cast<uint32_t>(ds), kcap, rows, sm_count, smem_optin, fb_plan))
         return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: no FP32 scan plan for k=%u", kcap);
     const uint64_t fb_per_query = static_cast<uint64_t>(fb_plan.ctas_per_group) * kcap;
     if ((st = grow_device(d_ws, cap_ws, std::max(per_query, fb_per_query) * n, "scan workspace"))) return st;

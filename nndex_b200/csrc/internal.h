@@ -72,7 +72,8 @@ struct ScanArgs {
 
 // Picks queries-per-CTA, grid and candidate capacity for (nq, dq, k) within the shared-memory
 // budget. Returns false when k is above what the fused kernel supports.
-bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t smem_limit, ScanPlan& plan);
+bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, uint64_t rows, int sm_count, size_t smem_limit,
+                    ScanPlan& plan);
 cudaError_t launch_scan_fp32(const ScanArgs& a, const ScanPlan& plan, cudaStream_t stream);
 
 struct MergeArgs {

@@ -84,7 +84,7 @@ int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, ui
         ScanPlan plan;
         if (kcap > kMaxFusedK ||
             !plan_scan_fp32(static_cast<uint32_t>(n), static_cast<uint32_t>(ix->ds), static_cast<uint32_t>(kcap),
-                            ix->sm_count, ix->smem_optin, plan))
+                            ix->rows, ix->sm_count, ix->smem_optin, plan))
             return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: k=%llu above the fused top-k limit %u",
                              (unsigned long long)kcap, kMaxFusedK);
         wsbytes = std::max(wsbytes, static_cast<size_t>(plan.ctas_per_group) * kcap * n * sizeof(uint64_t));
@@ -118,7 +118,7 @@ int search_device_noalloc(CudaIndex* ix, const float* d_queries, uint64_t nq, ui
         const uint64_t n = std::min<uint64_t>(kMaxBatchChunk, nq - q0);
         ScanPlan pl;
         if (!plan_scan_fp32(static_cast<uint32_t>(n), static_cast<uint32_t>(ix->ds), static_cast<uint32_t>(kcap),
-                            ix->sm_count, ix->smem_optin, pl))
+                            ix->rows, ix->sm_count, ix->smem_optin, pl))
             return fail(set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: no scan plan for %llu queries",
                                   (unsigned long long)n));
         const uint64_t per_query = static_cast<uint64_t>(pl.ctas_per_group) * kcap;

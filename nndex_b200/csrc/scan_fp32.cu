@@ -20,9 +20,11 @@
 // buffer could overflow on the next tile, a warp radix-selects its exact k best, compacts, and
 // raises `thr`. Each CTA writes its k best keys per query; merge_topk_kernel selects the global k
 // best and sorts them (similarity desc, index asc).
+#include <algorithm>
 #include <cstdlib>
 
 #include "common.cuh"
+
 #include "internal.h"
 #include "scan_core.cuh"
 #include "select.cuh"
@@ -578,7 +580,8 @@ static uint32_t env_u32(const char* name) {
     return v ? static_cast<uint32_t>(strtoul(v, nullptr, 10)) : 0u;
 }
 
-bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t smem_limit, ScanPlan& plan) {
+bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, uint64_t rows, int sm_count, size_t smem_limit,
+                    ScanPlan& plan) {
     if (k == 0 || k > kMaxFusedK || nq == 0) return false;
     static const uint32_t o_stages = env_u32("NNDEX_SCAN_STAGES"), o_qb = env_u32("NNDEX_SCAN_QB"),
                           o_ctas = env_u32("NNDEX_SCAN_CTAS"), o_cap = env_u32("NNDEX_SCAN_CAP");
@@ -631,8 +634,27 @@ bool plan_scan_fp32(uint32_t nq, uint32_t dq, uint32_t k, int sm_count, size_t s
         }
     }
     plan.groups = (nq + plan.qb - 1) / plan.qb;
-    uint32_t per = static_cast<uint32_t>(sm_count) / plan.groups;
-    if (per < 1) per = 1;
+    // CTAs per query group (each taking 1/per of the rows): a CTA fills an SM, so the launch takes
+    // ceil(groups × per / SMs) rounds of 1/per of the base. The rule fills the SMs once (per = SMs /
+    // groups); where that leaves a last round part-empty by more than 5 %, per minimises rounds / per
+    // over at most 8 rounds, with at least 2,048 rows per CTA (256 groups of one CTA, at 4,096
+    // queries, took 2 rounds where 1.73 was the ideal; 4 CTAs per group take 1.75).
+    const uint64_t sms = static_cast<uint64_t>(sm_count > 0 ? sm_count : 1);
+    const uint64_t base_per = std::max<uint64_t>(1, sms / plan.groups);
+    const uint64_t base_rounds = (plan.groups * base_per + sms - 1) / sms;
+    uint64_t per_cap = std::min<uint64_t>(8 * sms / plan.groups, rows / 2048);
+    per_cap = std::min<uint64_t>(std::max<uint64_t>(per_cap, base_per), 1024);
+    uint64_t best = base_per, best_rounds = base_rounds;
+    for (uint64_t c = 1; c <= per_cap; ++c) {
+        const uint64_t r = (plan.groups * c + sms - 1) / sms;
+        if (r * best < best_rounds * c) {  // r / c < best_rounds / best
+            best = c;
+            best_rounds = r;
+        }
+    }
+    // keep the rule unless the split is ≥ 5 % faster: best_rounds / best ≤ 0.95 · base_rounds / base_per
+    uint32_t per = static_cast<uint32_t>(base_per);
+    if (best_rounds * base_per * 100 <= base_rounds * best * 95) per = static_cast<uint32_t>(best);
     if (o_ctas) per = o_ctas;
     plan.ctas_per_group = per;
     return true;
