@@ -319,9 +319,9 @@ int CudaIndex::ensure_result_capacity(uint64_t nq, uint64_t kcap) {
     return NNDEX_OK;
 }
 
-// Workspace of the split merge (merge_parts(per_query, k) blocks per query), into m.
+// Workspace of the split merge (merge_parts(per_query, k, nq) blocks per query), into m.
 int CudaIndex::merge_workspace(uint64_t per_query, uint32_t nq, uint32_t k, MergeArgs& m, cudaStream_t s) {
-    const uint32_t parts = merge_parts(per_query, k);
+    const uint32_t parts = merge_parts(per_query, k, nq);
     if (parts <= 1) return NNDEX_OK;
     int st;
     if ((st = grow_device(d_part_keys, cap_part_keys, static_cast<size_t>(nq) * parts * k, "merge workspace")))

@@ -85,14 +85,14 @@ struct MergeArgs {
     uint64_t* idx_out = nullptr;        // nq × out_stride
     float* sim_out = nullptr;
     uint32_t* count_out = nullptr;      // nq
-    // Optional split of each query's lists over several blocks (merge_parts(per_query, k) of them):
+    // Optional split of each query's lists over several blocks (merge_parts(per_query, k, nq) of them):
     // part_keys holds nq × parts × k keys, part_done nq counters that start (and end) at zero.
     uint64_t* part_keys = nullptr;
     uint32_t* part_done = nullptr;
     const uint32_t* live = nullptr;     // optional: a device count; queries at or past it are skipped
     const uint32_t* out_rows = nullptr;  // optional: query q's results go to output row out_rows[q]
 };
-uint32_t merge_parts(uint64_t per_query, uint32_t k);
+uint32_t merge_parts(uint64_t per_query, uint32_t k, uint32_t nq);
 cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream);
 
 // K3 tensor-core scan (BF16 / FP8), two passes, and K4 rerank.

@@ -680,17 +680,22 @@ cudaError_t launch_scan_fp32(const ScanArgs& a, const ScanPlan& p, cudaStream_t 
     }
 }
 
-uint32_t merge_parts(uint64_t per_query, uint32_t k) {
+uint32_t merge_parts(uint64_t per_query, uint32_t k, uint32_t nq) {
     const uint64_t lists = k ? per_query / k : 0;
     uint64_t parts = lists < 16 ? lists : 16;
     while (parts > 1 && parts * k > 4096) --parts;  // survivors staged in shared memory
+    // Splitting a query's lists over blocks only helps while the queries alone leave SMs idle: about
+    // 1,024 blocks in all. (At 4,096 queries, 16 parts made 65,536 blocks, each a full block radix
+    // select over about 74 keys: 2.0 ms, against 0.04 ms for the rerank that follows.)
+    const uint64_t by_blocks = nq ? (1024 + nq - 1) / nq : 1;
+    if (parts > by_blocks) parts = by_blocks;
     return parts < 1 ? 1u : static_cast<uint32_t>(parts);
 }
 
 cudaError_t launch_merge_topk(const MergeArgs& a, cudaStream_t stream) {
     uint32_t p2 = 1;
     while (p2 < a.k) p2 <<= 1;
-    const uint32_t parts = (a.part_keys && a.part_done) ? merge_parts(a.per_query, a.k) : 1u;
+    const uint32_t parts = (a.part_keys && a.part_done) ? merge_parts(a.per_query, a.k, a.nq) : 1u;
     const size_t smem = (p2 + (parts > 1 ? static_cast<size_t>(parts) * a.k : 0)) * sizeof(uint64_t);
     if (smem > 40 * 1024) {  // with the static scratch, above the default 48 KB per block
         cudaError_t e = cudaFuncSetAttribute(merge_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
