@@ -147,3 +147,31 @@ def test_latency_budget_refuses_while_the_queue_is_backed_up(index):
             ai, asim = alone.result(alone.submit(qs[j], k=10))
             np.testing.assert_array_equal(results[j][0], ai)
             np.testing.assert_array_equal(results[j][1].view(np.uint32), asim.view(np.uint32))
+
+
+
+def test_warm_up_leaves_no_trace_but_loaded_kernels(index):
+    # Server start runs one batch of every kind on each slot (exact and approximate; k = 1, 10 and
+    # 100; small to the largest admitted batch) before it takes requests. None of them shows in the
+    # request statistics; each slot then serves both kinds with the request's own mode and nprobe
+    # (the warm-up restores the slot's), so results equal later ones and the index's own approximate
+    # search. The first batch's time is bounded well below the ~130 ms a fresh process's first
+    # tensor-core batch spends loading kernels (here earlier tests may have loaded them already).
+    q, _, _ = requests(1, index.dims, seed=13)[0]
+    q = np.vstack([q] * (200 // q.shape[0] + 1))[:200]  # 200 queries: the tensor-core path
+    with Server(index, slots=2, max_batch_queries=512) as s:
+        st = s.stats()
+        assert st["batches"] == 0 and st["queries_done"] == 0 and st["requests_done"] == 0, st
+        (ei, es), info = s.result(s.submit(q, k=10, approx=False), with_info=True)
+        ai, asim = s.result(s.submit(q, k=10, approx=True, nprobe=8))
+        assert (info["done_ns"] - info["start_ns"]) / 1e6 < 100.0, info
+        ei2, es2 = s.result(s.submit(q, k=10, approx=False))
+    np.testing.assert_array_equal(ei, ei2)
+    np.testing.assert_array_equal(es.view(np.uint32), es2.view(np.uint32))
+    index.set_nprobe(8)
+    try:
+        xi, xs = index.search(q, k=10)  # an approx index searches its IVF
+    finally:
+        index.set_nprobe(0)
+    np.testing.assert_array_equal(ai, xi)
+    np.testing.assert_array_equal(asim.view(np.uint32), xs.view(np.uint32))
