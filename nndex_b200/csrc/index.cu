@@ -763,11 +763,12 @@ int CudaIndex::enqueue_tc_pass2(bool fp8, uint32_t n, uint32_t kcap, uint64_t* o
     a.stream_a = plan2.stream_a;
     // Two query blocks per CTA (where both fit beside a ring: D ≤ 256 in BF16, 512 in FP8) read half
     // the base bytes per FLOP but run M = 128, N = 128 MMAs, which read as many query bytes from
-    // shared memory as base bytes. On 10M × 256 at 4,096 queries that made FP8 7 % faster and BF16
-    // 7 % slower, so the rule takes it for FP8 and the autotuner times both.
+    // shared memory as base bytes. On 10M × 256 at 4,096 queries that made BF16 7 % slower, and FP8
+    // 7 % faster only while the row ranges left SMs idle in a last partial round (the autotuner has
+    // taken one block for FP8 since): the rule takes one block, and the autotuner times both.
     // CTA pairs (qb = 3): two CTAs, one query block each, share every 256-row base tile through
     // M = 256 MMAs, so each SM reads half the base bytes per FLOP without narrowing the MMA.
-    const uint32_t want_qb = forced_qb ? forced_qb : (fp8 ? 2u : 1u);
+    const uint32_t want_qb = forced_qb ? forced_qb : 1u;
     const uint32_t pair_stages = (want_qb == 2 && n > 128) ? tc_pair_stages_for(tc_chunks(fp8), fp8, smem_optin) : 0;
     const uint32_t cta_pair_stages =
         (want_qb == 3 && n > 128) ? tc_cta_pair_stages_for(tc_chunks(fp8), fp8, smem_optin) : 0;
