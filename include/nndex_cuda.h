@@ -468,6 +468,21 @@ NNDEX_API int nndex_cuda_check_bounded_wait(nndex_cuda_index* index, uint64_t bu
  * return NNDEX_ERR_OUT_OF_MEMORY. 0 cancels. For tests of callers' out-of-memory handling. */
 NNDEX_API void nndex_cuda_inject_alloc_failures(uint32_t count);
 
+/* ---- launch planning (host only: no GPU, no index) ------------------------------------------ */
+
+/* The row ranges the tensor-core scan splits `rows` rows into for `groups` CTAs per range (its
+ * 128-query blocks, or the two CTAs of a pair per pair) on `sm_count` SMs, one CTA per SM at a
+ * time: *range_rows (a multiple of 256, at least 2,048 rows unless the base is smaller) and
+ * *nranges minimise ceil(groups × nranges / sm_count) × the tiles of a range over 1 to 8 rounds. */
+NNDEX_API int nndex_cuda_plan_tc_ranges(uint64_t rows, uint64_t groups, uint32_t sm_count, uint64_t* nranges,
+                                        uint64_t* range_rows);
+/* The FP32 scan's grid for `nq` queries at `k` over `rows` stored rows of `dims` values on
+ * `sm_count` SMs with `smem_limit` bytes of shared memory per block: *qb queries per CTA, *groups
+ * query groups and *ctas_per_group CTAs per group (each a contiguous share of the rows). */
+NNDEX_API int nndex_cuda_plan_fp32_scan(uint32_t nq, uint32_t dims, uint32_t k, uint64_t rows, uint32_t sm_count,
+                                        uint64_t smem_limit, uint32_t* qb, uint32_t* groups,
+                                        uint32_t* ctas_per_group);
+
 /* ---- FP64 oracle on the device (score-error report) ------------------------------------- */
 
 /*

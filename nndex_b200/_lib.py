@@ -200,6 +200,9 @@ SIGNATURES = {
     "nndex_cuda_set_graphs": (_i32, [_vp, _i32]),
     "nndex_cuda_check_bounded_wait": (_i32, [_vp, _u64]),
     "nndex_cuda_inject_alloc_failures": (None, [_u32]),
+    "nndex_cuda_plan_tc_ranges": (_i32, [_u64, _u64, _u32, C.POINTER(_u64), C.POINTER(_u64)]),
+    "nndex_cuda_plan_fp32_scan": (_i32, [_u32, _u32, _u32, _u64, _u32, _u64, C.POINTER(_u32), C.POINTER(_u32),
+                                         C.POINTER(_u32)]),
     "nndex_cuda_ivf_restore": (_i32, [_vp, _u64, _vp, _vp, _vp, _vp]),
     "nndex_cuda_base_checksum": (_i32, [_vp, C.POINTER(_u64)]),
     "nndex_cuda_server_start": (_i32, [_vp, C.POINTER(ServerOpts), C.POINTER(_vp)]),

@@ -7,6 +7,8 @@
 // wait on an mbarrier that nothing ever completes, so a test can watch the budget run out.
 // nndex_cuda_inject_alloc_failures makes the next scratch allocations fail on the host side (no
 // cudaMalloc is attempted), so out-of-memory handling can be tested without exhausting a GPU.
+// nndex_cuda_plan_tc_ranges and nndex_cuda_plan_fp32_scan return the grids the scans would launch
+// (host arithmetic only), so the planning rules are tested without a GPU.
 #include "common.cuh"
 #include "index.h"
 #include "internal.h"
@@ -55,5 +57,29 @@ int nndex_cuda_check_bounded_wait(nndex_cuda_index* index, uint64_t budget_cycle
 }
 
 void nndex_cuda_inject_alloc_failures(uint32_t count) { inject_alloc_failures(count); }
+
+int nndex_cuda_plan_tc_ranges(uint64_t rows, uint64_t groups, uint32_t sm_count, uint64_t* nranges,
+                              uint64_t* range_rows) {
+    clear_error();
+    if (!nranges || !range_rows || rows == 0 || groups == 0 || sm_count == 0)
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: plan needs rows, groups and SMs");
+    tc_range_split(rows, groups, sm_count, *nranges, *range_rows);
+    return NNDEX_OK;
+}
+
+int nndex_cuda_plan_fp32_scan(uint32_t nq, uint32_t dims, uint32_t k, uint64_t rows, uint32_t sm_count,
+                              uint64_t smem_limit, uint32_t* qb, uint32_t* groups, uint32_t* ctas_per_group) {
+    clear_error();
+    if (!qb || !groups || !ctas_per_group || dims == 0 || sm_count == 0)
+        return set_error(NNDEX_ERR_INVALID_ARGUMENT, "cuda execution error: plan needs dims and SMs");
+    ScanPlan plan;
+    const uint32_t ds = (dims + 31) / 32 * 32;  // the stored row stride
+    if (!plan_scan_fp32(nq, ds, k, rows, static_cast<int>(sm_count), static_cast<size_t>(smem_limit), plan))
+        return set_error(NNDEX_ERR_UNSUPPORTED, "cuda execution error: no FP32 scan plan for nq=%u k=%u", nq, k);
+    *qb = plan.qb;
+    *groups = plan.groups;
+    *ctas_per_group = plan.ctas_per_group;
+    return NNDEX_OK;
+}
 
 }  // extern "C"

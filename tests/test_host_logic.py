@@ -114,3 +114,49 @@ def test_autotune_cache_text_is_validated_without_a_gpu():
         assert L.nndex_cuda_autotune_validate(text, C.byref(n)) == _lib.NNDEX_ERR_INVALID_ARGUMENT, text
         assert "autotune text" in _lib.last_error()
     assert L.nndex_cuda_autotune_validate(None, C.byref(n)) == _lib.NNDEX_ERR_INVALID_ARGUMENT
+
+
+def test_launch_planners_fill_the_sms_in_whole_rounds():
+    # The scans' grids, computed on the host without a GPU: one CTA fills an SM, so a launch takes
+    # ceil(CTAs / SMs) rounds, and the planners avoid a last round that leaves most SMs idle.
+    L = _lib.lib()
+    nr, rr = C.c_uint64(), C.c_uint64()
+
+    def ranges(rows, groups, sms=148):
+        assert L.nndex_cuda_plan_tc_ranges(rows, groups, sms, C.byref(nr), C.byref(rr)) == 0
+        return nr.value, rr.value
+
+    # 4,096 queries (32 blocks) over 10M rows: 37 ranges, 1,184 CTAs in exactly 8 rounds (four ranges
+    # per SM gave 19 ranges: 608 CTAs, a fifth round of 16)
+    assert ranges(10_000_000, 32) == (37, 270_336)
+    assert ranges(10_000_000, 1) == (148, 67_584)  # one block: a range per SM
+    assert ranges(12_000, 3) == (6, 2_048)  # a small base: ranges of at least 2,048 rows
+    for rows in (3_000, 50_000, 1_000_000, 10_000_000, 123_457):
+        for groups in (1, 2, 3, 7, 16, 32, 33, 100, 148, 300, 2_000):
+            n, r = ranges(rows, groups)
+            assert r % 256 == 0 and (n - 1) * r < rows <= n * r, (rows, groups, n, r)
+            tiles = -(-rows // 256)
+            old = max(1, min(-(-4 * 148 // groups), -(-rows // 2048)))  # four ranges per SM
+            old_r = -(-(-(-rows // old)) // 256) * 256
+            old_n = -(-rows // old_r)
+            cost = -(-groups * n // 148) * (r // 256)
+            assert cost <= -(-groups * old_n // 148) * (old_r // 256), (rows, groups)
+            assert n * groups <= max(8 * 148, groups), (rows, groups)  # within the launch's item bound
+            assert tiles >= 1
+    assert L.nndex_cuda_plan_tc_ranges(0, 1, 148, C.byref(nr), C.byref(rr)) == _lib.NNDEX_ERR_INVALID_ARGUMENT
+
+    qb, groups, ctas = C.c_uint32(), C.c_uint32(), C.c_uint32()
+
+    def fp32(nq, dims, k, rows, sms=148, smem=232_448):
+        assert L.nndex_cuda_plan_fp32_scan(nq, dims, k, rows, sms, smem, C.byref(qb), C.byref(groups),
+                                           C.byref(ctas)) == 0
+        return qb.value, groups.value, ctas.value
+
+    assert fp32(1, 128, 10, 50_000) == (1, 1, 148)  # a single query: one group over every SM
+    assert fp32(64, 128, 10, 50_000) == (16, 4, 37)  # C1's batch: the rule's fill, kept
+    # 4,096 queries: 256 groups of 16; four CTAs per group take 7 rounds of 148 (1.75 bases) where
+    # one took 2 (the second with 40 SMs idle)
+    assert fp32(4096, 256, 10, 10_000_000) == (16, 256, 4)
+    assert fp32(4096, 256, 10, 5_000)[2] == 1  # too few rows to split: one CTA per group
+    assert L.nndex_cuda_plan_fp32_scan(16, 0, 10, 100, 148, 232_448, C.byref(qb), C.byref(groups),
+                                       C.byref(ctas)) == _lib.NNDEX_ERR_INVALID_ARGUMENT
